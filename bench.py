@@ -1,0 +1,322 @@
+#!/usr/bin/env python
+"""FDTD throughput benchmark of the B200 engine (one JSON line on rank 0).
+
+Workload (opensol_b200/workloads.py, roofline_2d): the 8192 x 8192 E_z grid incl. 20 CPML cells per side, dx = 20 nm,
+2000 seeded dielectric cylinders, a 1550 nm Gaussian line source and four 16-frequency flux lines.  One bench step
+is one whole simulation of 10,000 Yee steps (fields, psi and spectra reset first), so
+
+    value = cell-updates per second = 8192^2 x 10,000 x steps x ranks / device time      [Gcell-updates/s]
+
+measured with CUDA events on the stream the engine launches on, max over ranks.  The fields (3 x 268 MB) exceed the
+126 MB L2, so no flush is needed between steps.  e2e = the same metric through the public API from host inputs:
+Simulation built and painted on the host beforehand, then per step the upload of the materials (pinned host memory),
+the 10,000 steps and the read-back of all four flux spectra.
+
+--impl reference times the CPU restatement of open_sol's step (the oracle, C + OpenMP on every host core) on a
+bounded sample of the same grid.  With torchrun (N > 1) each rank runs an independent replica (the path does not
+shard; no collective touches the data).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_CELL_UPDATE = 28          # 3 float32 fields read + written, one float32 material word read
+SIM_STEPS = 10_000
+CPU_SAMPLE_STEPS = 24
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument('--gpus', type=int, default=1)
+    p.add_argument('--steps', type=int, default=5)
+    p.add_argument('--warmup', type=int, default=3)
+    p.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    p.add_argument('--sim-steps', type=int, default=SIM_STEPS)
+    p.add_argument('--no-cpu-baseline', action='store_true')
+    p.add_argument('--no-e2e', action='store_true')
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get('RANK', 0)), int(os.environ.get('WORLD_SIZE', 1)), int(os.environ.get('LOCAL_RANK', 0))
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)['hbm_gbs']), 'measured'
+    return 6650.0, 'fallback'
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix='.csv')
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', f'--id={self.index}', f'--query-gpu={self.QUERY}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=open(self.path, 'w'), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(',')]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        except OSError:
+            pass
+        if not rows:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled']}
+        sm = [float(r[1]) for r in rows if r[1].replace('.', '').isdigit()]
+        sm_max = [float(r[2]) for r in rows if r[2].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({name for r in rows for name, v in zip(names, r[5:9]) if v.lower() == 'active'})
+        return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': max(sm_max) if sm_max else None,
+                'reasons': reasons, 'samples': len(rows)}
+
+
+def build_sim(device, amplitude=1.0, pinned=False):
+    import opensol_b200 as ob
+    from opensol_b200 import workloads
+    sim = ob.Simulation(**workloads.roofline_2d_sim_args(), verbose=False, device=device, pinned_host=pinned)
+    monitors = workloads.apply(sim, workloads.roofline_2d_ops(amplitude=amplitude))
+    return sim, monitors
+
+
+def launches_per_sim(engine, n_steps):
+    """Kernels one n_steps chunk launches from step 0: the per-step field kernels plus one DFT launch per monitor
+    per sample."""
+    samples = n_steps // engine.sample_interval
+    return engine.kernels_per_step * n_steps + samples * len(engine._monitors)
+
+
+def cpu_baseline(sample_steps=CPU_SAMPLE_STEPS):
+    """The oracle (CPU restatement of open_sol's step, C + OpenMP) on the same 8192^2 workload: a bounded sample of
+    sample_steps Yee steps after a 2-step warm-up."""
+    from oracle.fdtd2d import OracleEz2D
+    from opensol_b200 import workloads
+    subprocess.run(['make', '-s', '-C', os.path.join(ROOT, 'oracle')], check=True)
+    o = OracleEz2D(**workloads.roofline_2d_sim_args())
+    workloads.apply(o, workloads.roofline_2d_ops())
+    o.finalize()
+    o.run(n_steps=2)
+    t0 = time.perf_counter()
+    o.run(n_steps=sample_steps)
+    wall = time.perf_counter() - t0
+    cells = o.domain.nx * o.domain.ny
+    return {'value': cells * sample_steps / wall / 1e9, 'unit': 'Gcell-updates/s',
+            'cores': os.cpu_count(), 'kind': 'port',
+            'sample': f'{sample_steps} Yee steps of the 8192x8192 roofline grid after 2 warm-up steps, '
+                      f'C restatement with OpenMP on {os.cpu_count()} threads',
+            'wall_s': wall}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle.fdtd2d import OracleEz2D
+    from opensol_b200 import workloads
+    subprocess.run(['make', '-s', '-C', os.path.join(ROOT, 'oracle')], check=True)
+    o = OracleEz2D(**workloads.roofline_2d_sim_args())
+    workloads.apply(o, workloads.roofline_2d_ops())
+    o.finalize()
+    cells = o.domain.nx * o.domain.ny
+    sample = 4
+    for _ in range(args.warmup):
+        o.run(n_steps=sample)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        o.run(n_steps=sample)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = cells * sample * args.steps / total / 1e9
+    line = {
+        'impl': 'reference', 'metric': 'FDTD Gcell-updates/s', 'value': value, 'unit': 'Gcell-updates/s',
+        'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total / args.steps * 1e3,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+        'config': config_block(args, 'replicas'),
+        'cpu_baseline': {'value': value, 'unit': 'Gcell-updates/s', 'cores': os.cpu_count(), 'kind': 'port',
+                         'sample': f'{sample} Yee steps of the 8192x8192 roofline grid per bench step (oracle: C '
+                                   f'restatement of open_sol\'s CPU step, OpenMP on {os.cpu_count()} threads)'},
+        'e2e': {'value': value, 'unit': 'Gcell-updates/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_block(args, parallelism):
+    return {'workload': 'roofline_2d: 2D E_z FDTD, 8192x8192 total grid incl. 20 CPML cells/side, dx 20 nm, 2000 '
+                        'seeded cylinders eps_r U(2,12), 1550 nm Gaussian line source, 4 x 16-frequency flux lines, '
+                        f'{args.sim_steps} Yee steps per bench step',
+            'grid': [8192, 8192], 'sim_steps': args.sim_steps, 'parallelism': parallelism,
+            'l2': 'inputs larger than L2 (fields 3 x 268 MB), no flush'}
+
+
+def run_b200(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300), device_id=torch.device('cuda', local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def reduce_max(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    sim, monitors = build_sim(local)
+    sim.em.finalize()
+    engine = sim.em.engine
+    stream = torch.cuda.current_stream()
+    engine.set_stream(stream.cuda_stream)
+    cells = engine.nx * engine.ny
+    engine.reset()
+    tables = engine.chunk_tables(args.sim_steps)
+    for _ in range(args.warmup):
+        engine.reset()
+        engine.advance(args.sim_steps, tables)
+    torch.cuda.synchronize()
+
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    advance_ms = []
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            engine.reset()
+            engine.advance(args.sim_steps, tables)
+            advance_ms.append(engine.last_advance_ms())
+        stop.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    device_ms = reduce_max(start.elapsed_time(stop))
+    value = world * cells * args.sim_steps * args.steps / (device_ms / 1e3) / 1e9
+    flux = [m.flux() for m in monitors]
+    assert all(float(abs(f).max()) > 0 for f in flux), 'flux is zero: the run did no work'
+
+    # dominant kernel: the fused step kernel(s); algorithmic bytes per launch over its mean launch time
+    kernel_ms_per_step = reduce_max(statistics.mean(advance_ms)) / args.sim_steps
+    per_launch_units = cells * engine.steps_per_launch
+    kernel_launch_ms = kernel_ms_per_step * engine.steps_per_launch
+    achieved = BYTES_PER_CELL_UPDATE * per_launch_units / (kernel_launch_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
+                'traffic': None, 'peak_source': f'{peak_kind} hbm_gbs', 'kernel': engine.kernel_name,
+                'algorithmic_bytes_per_launch': BYTES_PER_CELL_UPDATE * per_launch_units,
+                'launch_ms': kernel_launch_ms}
+    traffic_path = os.path.join(ROOT, 'profiles', 'traffic.json')
+    if os.path.exists(traffic_path):
+        with open(traffic_path) as f:
+            t = json.load(f).get(engine.kernel_name)
+        if t:
+            roofline['traffic'] = t['bytes_per_launch_scaled']
+            roofline['traffic_note'] = t['note']
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, local, world, barrier, reduce_max)
+
+    line = {
+        'metric': 'FDTD Gcell-updates/s', 'value': value, 'unit': 'Gcell-updates/s', 'n_gpus': world,
+        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': device_ms / args.steps, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+        'config': config_block(args, 'replicas' if world > 1 else 'single'),
+        'roofline': roofline,
+        'gpu_launches': launches_per_sim(engine, args.sim_steps) * args.steps,
+        'clocks': clocks.summary(),
+    }
+    if e2e is not None:
+        line['e2e'] = e2e
+    sim.clear()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line['cpu_baseline'] = cpu_baseline()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_e2e(args, device, world, barrier, reduce_max):
+    """Public-API runs from host inputs: per step the pinned host materials are uploaded, the 10,000 steps run and
+    the four monitors' spectra come back (flux())."""
+    import torch
+    n = max(1, min(args.steps, 3))
+    sims = [build_sim(device, pinned=True) for _ in range(n + 1)]
+    h2d = d2h = 0
+    sim, mons = sims[0]
+    sim.run(n_steps=args.sim_steps, verbose=False, print_every=0)   # warm-up run
+    [m.flux() for m in mons]
+    sim.clear()
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for sim, mons in sims[1:]:
+        sim.run(n_steps=args.sim_steps, verbose=False, print_every=0)
+        [m.flux() for m in mons]
+        h2d = sim.em.engine.h2d_bytes
+        d2h = sum(m.n_freqs * m.n_cells * 2 * 16 for m in mons)
+        sim.clear()
+    torch.cuda.synchronize()
+    wall = reduce_max(time.perf_counter() - t0)
+    barrier()
+    cells = 8192 * 8192
+    return {'value': world * cells * args.sim_steps * n / wall / 1e9, 'unit': 'Gcell-updates/s',
+            'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h), 'steps': n,
+            'timing': 'host wall clock around Simulation.run + flux(), synchronized, max over ranks'}
+
+
+def main():
+    args = parse_args()
+    if args.impl == 'reference':
+        run_reference(args)
+        return
+    run_b200(args)
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,141 @@
+/*
+ * opensol_fdtd.h -- C ABI of the B200 FDTD engine (libopensol_fdtd.so).
+ *
+ * Plain pointers and sizes only.  Every entry point returns an int status (OS_OK = 0) and never aborts; the message
+ * of the last failure on the calling thread is read with os_fdtd_last_error.  A handle owns its device buffers and
+ * one CUDA stream; calls on one handle come from one host thread.  Host pointers are copied in (the caller may reuse
+ * them on return); "_device" variants take device pointers the caller keeps alive.
+ *
+ * Arrays are C-contiguous row-major exactly as open_sol holds them: 2D (nx, ny) with idx = i * ny + j, 3D
+ * (nx, ny, nz) with idx = (i * ny + j) * nz + k.  All field arithmetic is float32, evaluated in open_sol's order with
+ * no fused multiply-add, so results equal open_sol's CPU backend bit for bit.
+ *
+ * Each function names the open_sol interface it replaces (file:line inside the open_sol project).
+ */
+#ifndef OPENSOL_FDTD_H
+#define OPENSOL_FDTD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    OS_OK = 0,
+    OS_ERR_INVALID = 1,     /* bad argument or configuration (open_sol raises ValueError / TypeError there) */
+    OS_ERR_CUDA = 2,        /* a CUDA call failed (RuntimeError) */
+    OS_ERR_NO_MEMORY = 3,   /* device allocation failed */
+    OS_ERR_STATE = 4        /* call out of order (e.g. advance before coefficients are set) */
+};
+
+/* CPML side bits, open_sol FACES order (open_sol/core/constants.py:18). */
+enum { OS_SIDE_X_LO = 1, OS_SIDE_X_HI = 2, OS_SIDE_Y_LO = 4, OS_SIDE_Y_HI = 8, OS_SIDE_Z_LO = 16, OS_SIDE_Z_HI = 32 };
+
+/* Field components of os_fdtd2d_read_field / write_field. */
+enum { OS_EZ = 0, OS_HX = 1, OS_HY = 2 };
+
+/* Copies the calling thread's last error message (NUL-terminated, truncated to n) into buf; returns its length. */
+int os_fdtd_last_error(char *buf, size_t n);
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int os_fdtd_version(void);
+
+/* Page-locked host memory for material arrays and read-back buffers (cudaHostAlloc), so host<->device copies run at
+ * full PCIe / C2C rate.  No open_sol counterpart (open_sol's cupy pool allocates device memory only). */
+int os_fdtd_host_alloc(size_t bytes, void **out);
+int os_fdtd_host_free(void *ptr);
+
+/* ----------------------------------------------------------------------------------------------------------------
+ * 2D E_z polarisation engine (E_z, H_x, H_y): replaces FDTDEngine2D_Ez (open_sol/physics/em/solvers/fdtd_ez_2d.py:11)
+ * with its BoundaryManager / CPMLSided state (open_sol/physics/em/boundaries.py:376, 689).
+ * ---------------------------------------------------------------------------------------------------------------- */
+typedef struct OsFdtd2D OsFdtd2D;
+
+typedef struct {
+    int32_t nx, ny;              /* total grid incl. CPML cells (Domain.uniform pads them: core/domain.py:180-197) */
+    int32_t periodic_x, periodic_y;
+    int32_t npml;                /* CPML cells per active side (BoundaryConfig.cpml_npml) */
+    int32_t cpml_sides;          /* OS_SIDE_* bits of the CPML faces */
+    int32_t device;              /* CUDA device ordinal */
+} OsGrid2D;
+
+/* Zeroed fields, psi slabs and spectra on `device`: FDTDEngine2D_Ez.__init__ (fdtd_ez_2d.py:20-52) plus
+ * CPMLSided.__init__ (boundaries.py:694-730).  Refuses a grid that cannot hold its CPML layers plus two rows
+ * (cpml_axis_profiles, boundaries.py:604-608). */
+int os_fdtd2d_create(const OsGrid2D *grid, OsFdtd2D **out);
+int os_fdtd2d_destroy(OsFdtd2D *h);
+
+/* Kappa-folded 1D curl spacings (nx,) (nx,) (ny,) (ny,): _curl_spacings (fdtd_2d_base.py:76-84). */
+int os_fdtd2d_set_spacings(OsFdtd2D *h, const float *inv_dx_e, const float *inv_dx_h, const float *inv_dy_e,
+                           const float *inv_dy_h);
+
+/* E / H update coefficients from the float32 material arrays (nx, ny): e_coefficients / h_coefficients
+ * (fdtd_ez_2d_kernels.py:314-353) evaluated on the device.  sigma_e NULL = lossless (ca = 1 is not stored); mu_r and
+ * sigma_m NULL = vacuum permeability everywhere (da = 1, db = dt / mu0 uniform, not stored). */
+int os_fdtd2d_set_materials(OsFdtd2D *h, const float *eps_r, const float *sigma_e, const float *mu_r,
+                            const float *sigma_m, float dt, float eps0, float mu0);
+
+/* The same from precomputed coefficient arrays (nx, ny): ca NULL = 1; da/db NULL = the uniform values. */
+int os_fdtd2d_set_coefficients(OsFdtd2D *h, const float *ca, const float *cb, const float *da, const float *db,
+                               float da_uniform, float db_uniform);
+
+/* Copies the device cb (nx, ny) to the host: the calibration input of SheetCurrentCalibration.apply
+ * (physics/em/sources.py:582-602). */
+int os_fdtd2d_read_cb(OsFdtd2D *h, float *cb);
+
+/* One CPML side (a single OS_SIDE_* bit): psi recursion rows b, a and bulk curl spacing of its cell-centre (_e) and
+ * hi-face (_h) rows, npml each (_cpml_row_set, boundaries.py:671-686; rows from cpml_side_rows, :570-576). */
+int os_fdtd2d_set_cpml_side(OsFdtd2D *h, int32_t side, const float *b_e, const float *a_e, const float *inv_e,
+                            const float *b_h, const float *a_h, const float *inv_h);
+
+/* Soft E_z line source: axis 0 = line along x at y-cell `position`, 1 = along y at x-cell `position`, half-open
+ * span [lo, hi), calibrated float32 profile (hi - lo,): LineSource (core/sources.py:190-229).  At most 16. */
+int os_fdtd2d_add_line_source(OsFdtd2D *h, int32_t axis, int32_t position, int32_t lo, int32_t hi,
+                              const float *profile, int32_t *source_id);
+int os_fdtd2d_set_line_profile(OsFdtd2D *h, int32_t source_id, const float *profile);
+
+/* Flux line: E_z and the tangential H (H_y for normal_axis 0, H_x for 1) on cells [lo, hi) of x-cell (normal 0) or
+ * y-cell (normal 1) `position`, nf frequencies, complex128 running DFTs: FluxMonitor (physics/em/monitors.py:325). */
+int os_fdtd2d_add_flux_line(OsFdtd2D *h, int32_t normal_axis, int32_t position, int32_t lo, int32_t hi, int32_t nf,
+                            int32_t *monitor_id);
+
+/* Steps between DFT samples (dft_sample_interval, physics/em/monitors.py:177-191). */
+int os_fdtd2d_set_sample_interval(OsFdtd2D *h, int64_t sample_interval);
+
+/* n_steps Yee steps (FDTDEngine2D_Ez.advance, fdtd_ez_2d.py:71-119, repeated): line_values (n_sources, n_steps)
+ * float32 amplitude * temporal(t + dt/2) per step (core/sources.py:221-223); phases: for every monitor in add
+ * order, (n_samples, nf) complex64 as float pairs for samples first_sample .. first_sample + n_samples - 1 (sample q
+ * is taken after engine step q * sample_interval; monitors.py:22-24,219-220).  Asynchronous on the handle's stream. */
+int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line_values, int64_t first_sample,
+                      int64_t n_samples, const float *phases);
+
+/* Engine steps taken since create / reset (FDTDEngine2D_Ez.n_step). */
+int os_fdtd2d_step_count(OsFdtd2D *h, int64_t *n_step);
+
+/* Spectra of a flux line: (nf, hi - lo) complex128 as double pairs, E then H (_LineSpectra.host, monitors.py:240). */
+int os_fdtd2d_read_flux_spectra(OsFdtd2D *h, int32_t monitor_id, double *e_spectra, double *h_spectra);
+
+/* Field copies (nx, ny) float32 (solution_state / restore_solution, fdtd_2d_base.py:419-456). */
+int os_fdtd2d_read_field(OsFdtd2D *h, int32_t component, float *out);
+int os_fdtd2d_write_field(OsFdtd2D *h, int32_t component, const float *in);
+
+/* Zero fields, psi slabs and spectra and the step count (Fields2D.reset, fields.py:32-36). */
+int os_fdtd2d_reset(OsFdtd2D *h);
+
+/* Waits for the handle's stream. */
+int os_fdtd2d_synchronize(OsFdtd2D *h);
+
+/* Launch on the caller's CUDA stream (a cudaStream_t; NULL = back to the handle's own stream).  Work already queued
+ * on the previous stream is waited for first.  No open_sol counterpart: the B200 hook for torch streams. */
+int os_fdtd2d_set_stream(OsFdtd2D *h, void *cuda_stream);
+
+/* Device milliseconds of the dominant field kernels over the last os_fdtd2d_advance (CUDA events on the handle's
+ * stream around its launches; 0 before the first advance). */
+int os_fdtd2d_last_advance_ms(OsFdtd2D *h, float *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OPENSOL_FDTD_H */

@@ -1,0 +1,209 @@
+// Device kernels of the 2D E_z engine.  Compiled with -fmad=false: every multiply and add below is rounded on its own,
+// in the order open_sol's CPU twins evaluate it, so the results are bit-identical to the reference CPU backend.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define OS_MAX_LINES_2D 16
+#define EZ2D_BLOCK_X 128
+#define EZ2D_BLOCK_Y 2
+
+struct LineSrcDev {
+    int32_t axis, position, lo, hi;
+    const float *profile;
+};
+
+// Everything one step of the E_z engine reads, passed by value (kernel parameter space).
+struct Ez2DParams {
+    int32_t nx, ny, periodic_x, periodic_y, npml, cpml_mask;
+    float *ez, *hx, *hy;
+    const float *ca, *cb, *da, *db;   // ca NULL: 1; da/db NULL: the uniform values
+    float da_uniform, db_uniform;
+    const float *inv_dx_e, *inv_dx_h, *inv_dy_e, *inv_dy_h;
+    const float *b_e[4], *a_e[4], *inv_e[4], *b_h[4], *a_h[4], *inv_h[4];
+    float *psi_e[4], *psi_h[4];
+    int32_t n_lines;
+    LineSrcDev lines[OS_MAX_LINES_2D];
+};
+
+// CPML side ids in open_sol FACES order.
+enum { SX_LO = 0, SX_HI = 1, SY_LO = 2, SY_HI = 3 };
+
+// H half step of cell (i, j): fdtd_ez_2d_kernels.py:37-48 (real-only engine: the periodic wrap reads
+// ez * 1 + ez * 0, as the reference's partner term with wrap cos 1, sin 0), then the H-row CPML of the y sides on H_x
+// and of the x sides on H_y (boundaries.py:27-37,752-755: psi = b psi + a (ez[r+1] - ez[r]) inv; hy += db psi,
+// hx += (-db) psi).
+__global__ void __launch_bounds__(EZ2D_BLOCK_X *EZ2D_BLOCK_Y) ez2d_h_kernel(const Ez2DParams p) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= p.nx || j >= p.ny) return;
+    const int nx = p.nx, ny = p.ny, npml = p.npml;
+    const size_t idx = (size_t)i * ny + j;
+    const float e = p.ez[idx];
+    const float da = p.da ? p.da[idx] : p.da_uniform;
+    const float db = p.db ? p.db[idx] : p.db_uniform;
+    const float one = 1.0f, zero = 0.0f;
+
+    // H_x (hi-y faces)
+    if (j < ny - 1 || p.periodic_y) {
+        const float e_up = j < ny - 1 ? p.ez[idx + 1] : p.ez[(size_t)i * ny] * one + p.ez[(size_t)i * ny] * zero;
+        float v = da * p.hx[idx] - db * (e_up - e) * p.inv_dy_h[j];
+        if ((p.cpml_mask & (1 << SY_LO)) && j < npml) {
+            const int k = j;
+            float *psi = p.psi_h[SY_LO] + (size_t)i * npml + k;
+            float q = *psi * p.b_h[SY_LO][k];
+            q += p.a_h[SY_LO][k] * (p.ez[idx + 1] - e) * p.inv_h[SY_LO][k];
+            *psi = q;
+            v += (-db) * q;
+        } else if ((p.cpml_mask & (1 << SY_HI)) && j >= ny - npml - 1 && j < ny - 1) {
+            const int k = j - (ny - npml - 1);
+            float *psi = p.psi_h[SY_HI] + (size_t)i * npml + k;
+            float q = *psi * p.b_h[SY_HI][k];
+            q += p.a_h[SY_HI][k] * (p.ez[idx + 1] - e) * p.inv_h[SY_HI][k];
+            *psi = q;
+            v += (-db) * q;
+        }
+        p.hx[idx] = v;
+    }
+    // H_y (hi-x faces)
+    if (i < nx - 1 || p.periodic_x) {
+        const float e_up = i < nx - 1 ? p.ez[idx + ny] : p.ez[j] * one + p.ez[j] * zero;
+        float v = da * p.hy[idx] + db * (e_up - e) * p.inv_dx_h[i];
+        if ((p.cpml_mask & (1 << SX_LO)) && i < npml) {
+            const int k = i;
+            float *psi = p.psi_h[SX_LO] + (size_t)k * ny + j;
+            float q = *psi * p.b_h[SX_LO][k];
+            q += p.a_h[SX_LO][k] * (p.ez[idx + ny] - e) * p.inv_h[SX_LO][k];
+            *psi = q;
+            v += db * q;
+        } else if ((p.cpml_mask & (1 << SX_HI)) && i >= nx - npml - 1 && i < nx - 1) {
+            const int k = i - (nx - npml - 1);
+            float *psi = p.psi_h[SX_HI] + (size_t)k * ny + j;
+            float q = *psi * p.b_h[SX_HI][k];
+            q += p.a_h[SX_HI][k] * (p.ez[idx + ny] - e) * p.inv_h[SX_HI][k];
+            *psi = q;
+            v += db * q;
+        }
+        p.hy[idx] = v;
+    }
+}
+
+// E half step of cell (i, j): fdtd_ez_2d_kernels.py:103-120, then the E-row CPML x sides (ez += cb psi) and y sides
+// (ez += (-cb) psi) (boundaries.py:757-760), then the soft line sources in add order (core/sources.py:221-229: skipped
+// when the step's float32 value is 0, else ez += value * profile).
+__global__ void __launch_bounds__(EZ2D_BLOCK_X *EZ2D_BLOCK_Y)
+    ez2d_e_kernel(const Ez2DParams p, const float *__restrict__ line_values, int64_t n_steps, int64_t k_step) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= p.nx || j >= p.ny) return;
+    const int nx = p.nx, ny = p.ny, npml = p.npml;
+    const size_t idx = (size_t)i * ny + j;
+    const float one = 1.0f, zero = 0.0f;
+    const float hy_c = p.hy[idx], hx_c = p.hx[idx];
+    float curl;
+    if (i >= 1) {
+        curl = (hy_c - p.hy[idx - ny]) * p.inv_dx_e[i];
+    } else if (p.periodic_x) {
+        const size_t w = (size_t)(nx - 1) * ny + j;
+        curl = (hy_c - (p.hy[w] * one - p.hy[w] * zero)) * p.inv_dx_e[i];
+    } else {
+        curl = hy_c * p.inv_dx_e[i];
+    }
+    if (j >= 1) {
+        curl -= (hx_c - p.hx[idx - 1]) * p.inv_dy_e[j];
+    } else if (p.periodic_y) {
+        const size_t w = idx + ny - 1;
+        curl -= (hx_c - (p.hx[w] * one - p.hx[w] * zero)) * p.inv_dy_e[j];
+    } else {
+        curl -= hx_c * p.inv_dy_e[j];
+    }
+    const float cb = p.cb[idx];
+    const float ez_old = p.ez[idx];
+    float v = (p.ca ? p.ca[idx] * ez_old : ez_old) + cb * curl;
+    if ((p.cpml_mask & (1 << SX_LO)) && i >= 1 && i <= npml) {
+        const int k = i - 1;
+        float *psi = p.psi_e[SX_LO] + (size_t)k * ny + j;
+        float q = *psi * p.b_e[SX_LO][k];
+        q += p.a_e[SX_LO][k] * (hy_c - p.hy[idx - ny]) * p.inv_e[SX_LO][k];
+        *psi = q;
+        v += cb * q;
+    } else if ((p.cpml_mask & (1 << SX_HI)) && i >= nx - npml - 1 && i <= nx - 2) {
+        const int k = i - (nx - npml - 1);
+        float *psi = p.psi_e[SX_HI] + (size_t)k * ny + j;
+        float q = *psi * p.b_e[SX_HI][k];
+        q += p.a_e[SX_HI][k] * (hy_c - p.hy[idx - ny]) * p.inv_e[SX_HI][k];
+        *psi = q;
+        v += cb * q;
+    }
+    if ((p.cpml_mask & (1 << SY_LO)) && j >= 1 && j <= npml) {
+        const int k = j - 1;
+        float *psi = p.psi_e[SY_LO] + (size_t)i * npml + k;
+        float q = *psi * p.b_e[SY_LO][k];
+        q += p.a_e[SY_LO][k] * (hx_c - p.hx[idx - 1]) * p.inv_e[SY_LO][k];
+        *psi = q;
+        v += (-cb) * q;
+    } else if ((p.cpml_mask & (1 << SY_HI)) && j >= ny - npml - 1 && j <= ny - 2) {
+        const int k = j - (ny - npml - 1);
+        float *psi = p.psi_e[SY_HI] + (size_t)i * npml + k;
+        float q = *psi * p.b_e[SY_HI][k];
+        q += p.a_e[SY_HI][k] * (hx_c - p.hx[idx - 1]) * p.inv_e[SY_HI][k];
+        *psi = q;
+        v += (-cb) * q;
+    }
+    for (int l = 0; l < p.n_lines; ++l) {
+        const LineSrcDev &s = p.lines[l];
+        const int along = s.axis == 0 ? i : j, across = s.axis == 0 ? j : i;
+        if (across == s.position && along >= s.lo && along < s.hi) {
+            const float value = line_values[(size_t)l * n_steps + k_step];
+            if (value != 0.0f) v += value * s.profile[along - s.lo];
+        }
+    }
+    p.ez[idx] = v;
+}
+
+// Line DFT of a flux monitor at one sample (physics/em/monitors.py:45-46,84-90): acc[f, c] += complex128(phase_f) *
+// (double)field, for E_z and the tangential H, one thread per (frequency, cell).  The products of a float phase and a
+// float sample are exact in double, so the float64 running sums equal the reference's complex128 ones.
+__global__ void ez2d_flux_kernel(const float *__restrict__ ez, const float *__restrict__ h_field, int ny,
+                                 int normal_axis, int position, int lo, int n, int nf, const float *__restrict__ phases,
+                                 double *__restrict__ e_acc, double *__restrict__ h_acc) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * nf) return;
+    const int f = t / n, c = t - f * n;
+    const size_t cell = normal_axis == 0 ? (size_t)position * ny + (size_t)(lo + c) : (size_t)(lo + c) * ny + position;
+    const double pr = (double)phases[2 * f], pi = (double)phases[2 * f + 1];
+    const double e = (double)ez[cell], hv = (double)h_field[cell];
+    const size_t a = ((size_t)f * n + c) * 2;
+    e_acc[a] += pr * e;
+    e_acc[a + 1] += pi * e;
+    h_acc[a] += pr * hv;
+    h_acc[a + 1] += pi * hv;
+}
+
+// ca / cb from float32 eps_r, sigma_e (fdtd_ez_2d_kernels.py:314-332, T = float); sigma NULL = lossless (ca not
+// written: it is 1).
+__global__ void ez2d_e_coefficients_kernel(const float *__restrict__ eps_r, const float *__restrict__ sigma, float dt,
+                                           float eps0, size_t n, float *__restrict__ ca, float *__restrict__ cb) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const float eps = eps_r[t] * eps0;
+    const float s = sigma ? sigma[t] : 0.0f;
+    const float k = s * dt / (2.0f * eps);
+    const float denom = 1.0f + k;
+    if (ca) ca[t] = (1.0f - k) / denom;
+    cb[t] = (dt / eps) / denom;
+}
+
+// da / db from float32 mu_r, sigma_m (fdtd_ez_2d_kernels.py:335-353); NULL arrays read 1 / 0.
+__global__ void ez2d_h_coefficients_kernel(const float *__restrict__ mu_r, const float *__restrict__ sigma_m, float dt,
+                                           float mu0, size_t n, float *__restrict__ da, float *__restrict__ db) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const float mu = (mu_r ? mu_r[t] : 1.0f) * mu0;
+    const float s = sigma_m ? sigma_m[t] : 0.0f;
+    const float k = s * dt / (2.0f * mu);
+    const float denom = 1.0f + k;
+    da[t] = (1.0f - k) / denom;
+    db[t] = (dt / mu) / denom;
+}

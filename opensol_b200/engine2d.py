@@ -1,0 +1,230 @@
+"""FDTDEngine2D_Ez on the B200: the 2D E_z-polarisation Yee engine of open_sol (open_sol/physics/em/solvers/
+fdtd_ez_2d.py:11) re-built as device-resident state behind the C ABI of libopensol_fdtd.so.
+
+The host keeps only the float64 clock, the step counter and the setup rows; fields, coefficients, CPML psi slabs,
+line-source profiles and monitor spectra stay in HBM.  ``advance(n)`` hands a whole chunk of n steps to the device:
+per-step source values and per-sample DFT phases are precomputed on the host into small tables, so no host work sits
+between steps.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native
+from .boundaries import build_yee_rows
+from .constants import DTYPE, EPS0, MU0
+from .monitors import dft_phase_table
+
+
+class FDTDEngine2D_Ez:
+    """Device engine of one 2D E_z simulation (real fields, CPML and periodic faces)."""
+
+    polarization = 'ez'
+    kernel_name = 'ez2d_h_kernel+ez2d_e_kernel'   # the field kernels of one step
+    kernels_per_step = 2
+    steps_per_launch = 1
+
+    def __init__(self, domain, boundary_config, device: int = 0):
+        boundary_config.require_supported('FDTDEngine2D_Ez')
+        self.domain = domain
+        self.grid = domain.grid
+        self.boundary_config = boundary_config
+        self.nx, self.ny = self.grid.nx, self.grid.ny
+        self.dt = self.grid.dt
+        self.device = int(device)
+        self.n_step = 0
+        self.time = 0.0
+        # curl spacings with kappa folded in, CPML rows per active side (float32)
+        self.rows = build_yee_rows(boundary_config, (self.nx, self.ny), float(self.grid.dx), float(self.grid.dx),
+                                   float(self.dt))
+        self._handle = None
+        self._lines = []          # LineSource objects in add order
+        self._line_ids = {}       # id(source) -> native id
+        self._profiles_sent = {}  # id(source) -> profile array last uploaded
+        self._monitors = []       # FluxMonitor objects in add order
+        self._monitor_ids = {}
+        self._materials_version = None
+        self.sample_interval = 1
+        self._sample_interval_sent = None
+        self.h2d_bytes = 0   # host-to-device bytes this engine has uploaded (setup, materials, chunk tables)
+
+    # ------------------------------------------------------------------------------------------- native handle
+    @property
+    def handle(self):
+        """The native engine, created on first device use with its spacings and CPML rows."""
+        if self._handle is None:
+            lib = _native.load()
+            sides = sum(_native.OS_SIDE_BITS[face] for face, on in self.boundary_config.cpml_sides.items() if on)
+            grid = _native.OsGrid2D(self.nx, self.ny, int(self.boundary_config.periodic_x),
+                                    int(self.boundary_config.periodic_y), int(self.boundary_config.cpml_npml),
+                                    sides, self.device)
+            h = ctypes.c_void_p()
+            _native.check(lib.os_fdtd2d_create(ctypes.byref(grid), ctypes.byref(h)), 'os_fdtd2d_create')
+            self._handle = h
+            c = self.rows.curl
+            _native.check(lib.os_fdtd2d_set_spacings(h, _native.fptr(c['inv_dx_e']), _native.fptr(c['inv_dx_h']),
+                                                     _native.fptr(c['inv_dy_e']), _native.fptr(c['inv_dy_h'])))
+            for side in self.rows.sides:
+                _native.check(lib.os_fdtd2d_set_cpml_side(
+                    h, _native.OS_SIDE_BITS[side.face], *(_native.fptr(np.ascontiguousarray(getattr(side, n)))
+                                                          for n in ('b_e', 'a_e', 'inv_e', 'b_h', 'a_h', 'inv_h'))))
+        return self._handle
+
+    def close(self):
+        if self._handle is not None:
+            _native.load().os_fdtd2d_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------------------------------- setup
+    def attach_line_source(self, source):
+        """Register a line source; its profile and the device copy follow at the next sync."""
+        self._lines.append(source)
+
+    def attach_flux_monitor(self, monitor):
+        self._monitors.append(monitor)
+        monitor._reader = lambda m=monitor: self.read_flux_spectra(m)
+
+    def set_sample_interval(self, m):
+        self.sample_interval = int(m)
+
+    def sync_device(self):
+        """Bring the device engine up to date with the host setup: coefficients (when the materials changed), new
+        sources and monitors, changed profiles, the sample interval."""
+        lib = _native.load()
+        h = self.handle
+        materials = self.domain.materials
+        if self._materials_version != materials.version:
+            arrays = [materials.get(name) for name in ('eps_r', 'sigma_e', 'mu_r', 'sigma_m')]
+            arrays = [None if a is None else np.ascontiguousarray(a, dtype=DTYPE) for a in arrays]
+            _native.check(lib.os_fdtd2d_set_materials(h, *(_native.fptr(a) for a in arrays), float(self.dt),
+                                                      float(DTYPE(EPS0)), float(DTYPE(MU0))))
+            self.h2d_bytes += sum(a.nbytes for a in arrays if a is not None)
+            self._materials_version = materials.version
+        for source in self._lines:
+            profile = np.ascontiguousarray(source.profile, dtype=DTYPE)
+            key = id(source)
+            if key not in self._line_ids:
+                lo, hi = source.span
+                sid = ctypes.c_int32()
+                _native.check(lib.os_fdtd2d_add_line_source(h, 0 if source.axis == 'x' else 1, source.position, lo,
+                                                            hi, _native.fptr(profile), ctypes.byref(sid)))
+                self._line_ids[key] = sid.value
+            elif self._profiles_sent.get(key) is not source.profile:
+                _native.check(lib.os_fdtd2d_set_line_profile(h, self._line_ids[key], _native.fptr(profile)))
+            self._profiles_sent[key] = source.profile
+        for monitor in self._monitors:
+            if id(monitor) not in self._monitor_ids:
+                mid = ctypes.c_int32()
+                normal = 0 if monitor.axis == 'x' else 1
+                _native.check(lib.os_fdtd2d_add_flux_line(h, normal, monitor.position, monitor.span[0],
+                                                          monitor.span[1], monitor.n_freqs, ctypes.byref(mid)))
+                self._monitor_ids[id(monitor)] = mid.value
+        if self._sample_interval_sent != self.sample_interval:
+            _native.check(lib.os_fdtd2d_set_sample_interval(h, self.sample_interval))
+            self._sample_interval_sent = self.sample_interval
+
+    # ------------------------------------------------------------------------------------------- stepping
+    def chunk_tables(self, n_steps):
+        """(line values (n_lines, n_steps), first sample, n_samples, phase table, clock after the chunk): the host
+        side of one device chunk.  Clock: t_half = t + dt/2, t_full = t + dt accumulated in float64
+        (fdtd_ez_2d.py:76-79)."""
+        dt = float(self.dt)
+        t = self.time
+        t_half = np.empty(n_steps)
+        t_full = np.empty(n_steps)
+        for k in range(n_steps):
+            t_half[k] = t + 0.5 * dt
+            t = t + dt
+            t_full[k] = t
+        values = (np.stack([src.values(t_half) for src in self._lines]) if self._lines
+                  else np.zeros((0, n_steps), dtype=np.float32))
+        m = self.sample_interval
+        first_q = self.n_step // m + 1
+        last_q = (self.n_step + n_steps) // m
+        n_q = max(0, last_q - first_q + 1)
+        tables = []
+        for monitor in self._monitors:
+            times = [t_full[q * m - self.n_step - 1] for q in range(first_q, first_q + n_q)]
+            tables.append(dft_phase_table(2.0 * np.pi * monitor.frequencies, times, monitor.dt * m))
+        phases = np.concatenate([tb.reshape(-1) for tb in tables]) if tables else np.zeros(0, np.float32)
+        return np.ascontiguousarray(values, dtype=np.float32), first_q, n_q, phases, t
+
+    def advance(self, n_steps, tables=None):
+        """Run n_steps full Yee steps on the device (asynchronous); `tables` = a chunk_tables(n_steps) result
+        prepared earlier for the same clock and step count (a repeated run from reset reuses it)."""
+        n_steps = int(n_steps)
+        if n_steps <= 0:
+            return
+        self.sync_device()
+        values, first_q, n_q, phases, t_end = tables if tables is not None else self.chunk_tables(n_steps)
+        self.h2d_bytes += values.nbytes + phases.nbytes
+        _native.check(_native.load().os_fdtd2d_advance(
+            self.handle, n_steps, _native.fptr(values) if values.size else None, first_q, n_q,
+            _native.fptr(phases) if phases.size else None))
+        self.n_step += n_steps
+        self.time = t_end
+
+    def set_stream(self, cuda_stream):
+        """Enqueue on the caller's CUDA stream (an int cudaStream_t, e.g. torch.cuda.current_stream().cuda_stream;
+        None = the engine's own stream)."""
+        _native.check(_native.load().os_fdtd2d_set_stream(self.handle, cuda_stream or None))
+
+    def synchronize(self):
+        _native.check(_native.load().os_fdtd2d_synchronize(self.handle))
+
+    def last_advance_ms(self):
+        ms = ctypes.c_float()
+        _native.check(_native.load().os_fdtd2d_last_advance_ms(self.handle, ctypes.byref(ms)))
+        return float(ms.value)
+
+    def reset(self):
+        """Zero fields, psi and spectra; clock and step count back to 0."""
+        _native.check(_native.load().os_fdtd2d_reset(self.handle))
+        self.n_step = 0
+        self.time = 0.0
+
+    # ------------------------------------------------------------------------------------------- readout
+    def read_field(self, name):
+        comp = {'ez': _native.OS_EZ, 'hx': _native.OS_HX, 'hy': _native.OS_HY}[name]
+        out = np.empty((self.nx, self.ny), dtype=DTYPE)
+        _native.check(_native.load().os_fdtd2d_read_field(self.handle, comp, _native.fptr(out)))
+        return out
+
+    def write_field(self, name, values):
+        comp = {'ez': _native.OS_EZ, 'hx': _native.OS_HX, 'hy': _native.OS_HY}[name]
+        arr = np.ascontiguousarray(values, dtype=DTYPE)
+        if arr.shape != (self.nx, self.ny):
+            raise ValueError(f'{name} must have shape {(self.nx, self.ny)}, got {arr.shape}')
+        _native.check(_native.load().os_fdtd2d_write_field(self.handle, comp, _native.fptr(arr)))
+
+    def read_cb(self):
+        out = np.empty((self.nx, self.ny), dtype=DTYPE)
+        self.sync_device()
+        _native.check(_native.load().os_fdtd2d_read_cb(self.handle, _native.fptr(out)))
+        return out
+
+    def read_flux_spectra(self, monitor):
+        if id(monitor) not in self._monitor_ids:
+            self.sync_device()
+        mid = self._monitor_ids[id(monitor)]
+        n = monitor.n_cells
+        e = np.empty((monitor.n_freqs, n, 2), dtype=np.float64)
+        h = np.empty((monitor.n_freqs, n, 2), dtype=np.float64)
+        _native.check(_native.load().os_fdtd2d_read_flux_spectra(self.handle, mid, _native.dptr(e),
+                                                                 _native.dptr(h)))
+        return e[..., 0] + 1j * e[..., 1], h[..., 0] + 1j * h[..., 1]
+
+    def state(self):
+        """Host copies of the public fields (FDTDEngine2D_Ez.state, fdtd_ez_2d.py:56-67)."""
+        materials = self.domain.materials
+        return {'ez': self.read_field('ez'), 'hx': self.read_field('hx'), 'hy': self.read_field('hy'),
+                'eps_r': materials.array('eps_r'), 'sigma_e': materials.array('sigma_e'), 'jz_total': None,
+                'q_accum': None, 'q_accum_time': 0.0}

@@ -1,0 +1,234 @@
+"""EMPhysics on the B200 engine: open_sol's 2D FDTD physics (open_sol/physics/em/__init__.py:63) with the same
+constructor, PhysicsSolver contract, material helpers, sources and monitors, stepping FDTDEngine2D_Ez on the device.
+
+Only the E_z polarisation with single-precision fields is built; 'hz' and precision='double' raise.  Setup follows
+the reference's finalize order (physics/em/__init__.py:181-203): coefficients, Courant check, source calibration,
+DFT sample interval.  ``advance_ticks`` lets MultiphysicsRunner hand whole chunks to the device
+(coupling/runner.py:97-101,183-186).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .boundaries import BoundaryConfig
+from .constants import C0, DTYPE
+from .engine2d import FDTDEngine2D_Ez
+from .monitors import FluxMonitor, dft_sample_interval, resolve_frequencies
+from .sources import (LineSource, calibrate_line_source, carrier_angular_frequency, make_temporal,
+                      resolve_frequency)
+
+
+class EMPhysics:
+    """2D FDTD physics of a Domain, polarisation 'ez' (E_z, H_x, H_y), on one B200."""
+
+    name = 'em'
+    coordinate_grids = ('cartesian',)
+
+    def __init__(self, domain, polarization: str = 'ez', boundary_config=None, precision: str = 'single',
+                 device: int = 0):
+        if polarization not in ('ez', 'hz'):
+            raise ValueError(f"polarization must be 'ez' (E_z, H_x, H_y) or 'hz' (H_z, E_x, E_y), got "
+                             f"{polarization!r}")
+        if precision not in ('single', 'double'):
+            raise ValueError(f"EMPhysics precision must be 'single' (float32 fields) or 'double' (float64), got "
+                             f"{precision!r}")
+        if polarization != 'ez':
+            raise NotImplementedError("the B200 2D engine steps the 'ez' polarisation")
+        if precision != 'single':
+            raise NotImplementedError('the B200 engine steps float32 fields (stepper precision single)')
+        self.domain = domain
+        self.polarization = polarization
+        self.precision = precision
+        bc = boundary_config if boundary_config is not None else domain.boundary_config
+        if bc is None:
+            bc = BoundaryConfig.all_pml(domain.npml_sides['x_lo'])
+        bc._validate()
+        if bc.npml_sides != domain.npml_sides:
+            raise ValueError(f"boundary_config PML cells {bc.npml_sides} do not match the domain padding "
+                             f"{domain.npml_sides}; build the Domain with the same boundary_config")
+        self.boundary_config = bc
+        self.engine = FDTDEngine2D_Ez(domain, bc, device=device)
+        self.sources = []
+        self.monitors = []
+        self._calibrations = []       # (source, omega, normal width)
+        self._calibration_dirty = False
+        self._finalized = False
+        self.finalize_warnings = []
+        self.runtime_warnings = []
+
+    @property
+    def permittivity_arrays(self):
+        return ('eps_r',)
+
+    # --- PhysicsSolver contract ------------------------------------------------------------------------
+    def prepare(self, domain):
+        return
+
+    def dt_limit(self) -> float:
+        return float(self.engine.dt)
+
+    def step(self, t: float = None, dt: float = None):
+        """One Yee step (dt is advisory: the engine keeps its Courant dt)."""
+        self._before_steps()
+        self.engine.advance(1)
+
+    def advance_ticks(self, n_ticks: int, t: float, dt: float, stop_time: float):
+        """Whole chunk of the runner's tick loop (coupling/runner.py:183-203): ticks while t < stop_time, t += dt
+        after each, at most n_ticks; returns (ticks run, new t)."""
+        n_done = 0
+        while n_done < n_ticks and t < stop_time:
+            t = t + dt
+            n_done += 1
+        if n_done:
+            self._before_steps()
+            self.engine.advance(n_done)
+        return n_done, t
+
+    def _before_steps(self):
+        if not self._finalized:
+            self.finalize()
+        if self._calibration_dirty:
+            self._calibrate_sources()
+
+    def state(self) -> dict:
+        return self.engine.state()
+
+    def finalize(self) -> None:
+        """Coefficients from the final materials, Courant check, source calibration, DFT sample interval
+        (physics/em/__init__.py:181-203), then the device engine brought up to date."""
+        self.finalize_host()
+        self.engine.sync_device()
+
+    def finalize_host(self) -> None:
+        """The host half of finalize: Courant check, calibrated source profiles, DFT sample interval."""
+        self.finalize_warnings = []
+        self._check_courant_stability()
+        self._calibrate_sources()
+        if self.engine.n_step == 0:
+            m = dft_sample_interval(float(self.engine.dt), self.sources, [mon.frequencies for mon in self.monitors])
+            for monitor in self.monitors:
+                monitor.sample_interval = m
+            self.engine.set_sample_interval(m)
+        self._finalized = True
+
+    def materials_changed(self, names) -> None:
+        """Materials were rewritten: the device coefficients follow at the next step (the engine tracks the
+        MaterialGrid version) and the sources recalibrate (physics/em/__init__.py:205-209)."""
+        if frozenset(names) & {'eps_r', 'sigma_e', 'mu_r', 'sigma_m'}:
+            self._calibration_dirty = True
+
+    def renderer(self):
+        raise NotImplementedError('rendering is outside the B200 FDTD engine')
+
+    # --- checks / calibration --------------------------------------------------------------------------
+    def _check_courant_stability(self):
+        """ValueError when eps_r mu_r < (C0 dt)^2 (1/dx^2 + 1/dy^2) in some cell (physics/em/__init__.py:242-281,
+        without poles)."""
+        dt = float(self.engine.dt)
+        dx_cells, dy_cells = self.domain.cell_widths()
+        light = (C0 * dt) ** 2
+        required_x = (light / dx_cells ** 2).astype(DTYPE)
+        required_y = (light / dy_cells ** 2).astype(DTYPE)
+        materials = self.domain.materials
+        eps = materials.array('eps_r')
+        mu = materials.get('mu_r')
+        # uniform grid: the requirement is one value; the worst cell is the smallest eps mu
+        requirement = required_x[0] + required_y[0]
+        product = eps if mu is None else eps * mu
+        worst = float(product.min() / requirement)
+        if worst >= 1.0 - 1e-6:
+            return
+        ix, iy = np.unravel_index(int(np.argmin(product)), product.shape)
+        x_centers, y_centers = self.domain.cell_centers()
+        required = light * (1.0 / dx_cells[ix] ** 2 + 1.0 / dy_cells[iy] ** 2)
+        stable = math.floor(float(self.domain.grid.courant) * math.sqrt(max(worst, 0.0)) * 1e3) / 1e3
+        raise ValueError(f'eps_r * mu_r = {float(product[ix, iy]):.4g} at ({x_centers[ix]:.4g}, {y_centers[iy]:.4g}) '
+                         f'm is below (C0 dt)^2 (1/dx^2 + 1/dy^2) = {required:.4g} there, so the time step is '
+                         f'unstable; lower courant_factor to <= {stable:.3f}, or raise eps_r / mu_r')
+
+    def _calibrate_sources(self):
+        for source, omega, width in self._calibrations:
+            source.profile = calibrate_line_source(source, self.domain.materials, omega, width,
+                                                   float(self.domain.grid.dt))
+        self._calibration_dirty = False
+
+    # --- material helpers --------------------------------------------------------------------------------
+    def add_dielectric_rectangle(self, x0, y0, x1, y1, eps_r, sigma_e=0.0):
+        self._set_dielectric(self.domain.rect_mask(x0, y0, x1, y1), eps_r, sigma_e)
+
+    def add_dielectric_circle(self, cx, cy, radius, eps_r, sigma_e=0.0):
+        self._set_dielectric(self.domain.circle_mask(cx, cy, radius), eps_r, sigma_e)
+
+    def _set_dielectric(self, mask, eps_r, sigma_e):
+        self.domain.materials.set_mask(mask, eps_r=eps_r, sigma_e=sigma_e)
+        self.materials_changed(('eps_r', 'sigma_e'))
+
+    # --- sources ----------------------------------------------------------------------------------------
+    def add_line_source(self, axis, position, wavelength=None, frequency=None, bandwidth=0.5, amplitude=1.0,
+                        waveform='gaussian', span=None):
+        """Sheet current radiating `amplitude` [V/m] to each side (physics/em/__init__.py:442-473); axis 'x' = line
+        along x at y = position; span = (start, end) [m] or None (whole grid line)."""
+        temporal = make_temporal(waveform, resolve_frequency(wavelength, frequency), bandwidth)
+        d = self.domain
+        if axis not in ('x', 'y'):
+            raise ValueError(f"Line source axis must be 'x' or 'y', got {axis!r}")
+        if axis == 'x':
+            d.validate_physical_pos(0.0, position, "Line source (y)")
+            line_cell, along_cell, n_along = d.pos_to_cell_y(position), d.pos_to_cell_x, d.grid.nx
+        else:
+            d.validate_physical_pos(position, 0.0, "Line source (x)")
+            line_cell, along_cell, n_along = d.pos_to_cell_x(position), d.pos_to_cell_y, d.grid.ny
+        along_axis = 0 if axis == 'x' else 1
+        normal_width = float(d.cell_widths()[1 - along_axis][line_cell])
+        if span is None:
+            lo, hi = 0, n_along
+        else:
+            start, end = sorted((float(span[0]), float(span[1])))
+            for coord in (start, end):
+                if axis == 'x':
+                    d.validate_physical_pos(coord, position, "Line source span")
+                else:
+                    d.validate_physical_pos(position, coord, "Line source span")
+            lo, hi = along_cell(start), along_cell(end) + 1
+            window = d.physical_window()[along_axis]
+            bc = self.boundary_config
+            if lo == window.start and getattr(bc, f'{axis}_lo').value == 'cpml':
+                lo = 0
+            if hi == window.stop and getattr(bc, f'{axis}_hi').value == 'cpml':
+                hi = n_along
+        source = LineSource(axis, line_cell, temporal, amplitude, span=(lo, hi),
+                            profile=np.zeros(hi - lo, dtype=DTYPE))
+        self.sources.append(source)
+        self._calibrations.append((source, carrier_angular_frequency(temporal), normal_width))
+        self._calibration_dirty = True
+        self.engine.attach_line_source(source)
+        return source
+
+    # --- monitors ---------------------------------------------------------------------------------------
+    def add_flux_monitor(self, axis, position, span, wavelengths=None, frequencies=None):
+        """Poynting flux through a line (axis 'x' = along x at y = position, flux > 0 toward +y)
+        (physics/em/__init__.py:511-518, placement.flux_line_cells)."""
+        d = self.domain
+        if span is None or len(span) != 2:
+            raise ValueError(f"Flux monitor needs span = (start, end) along the line [m], got {span!r}")
+        lo, hi = sorted((float(span[0]), float(span[1])))
+        dx_cells, dy_cells = d.cell_widths()
+        if axis == 'x':
+            d.validate_physical_pos(lo, position, "Flux monitor start")
+            d.validate_physical_pos(hi, position, "Flux monitor end")
+            normal, line_cell, cells, widths = 'y', d.pos_to_cell_y(position), (d.pos_to_cell_x(lo),
+                                                                               d.pos_to_cell_x(hi) + 1), dx_cells
+        elif axis == 'y':
+            d.validate_physical_pos(position, lo, "Flux monitor start")
+            d.validate_physical_pos(position, hi, "Flux monitor end")
+            normal, line_cell, cells, widths = 'x', d.pos_to_cell_x(position), (d.pos_to_cell_y(lo),
+                                                                               d.pos_to_cell_y(hi) + 1), dy_cells
+        else:
+            raise ValueError(f"Flux monitor axis (along the line) must be 'x' or 'y', got {axis!r}")
+        monitor = FluxMonitor(normal, line_cell, cells, resolve_frequencies(wavelengths, frequencies),
+                              float(d.grid.dt), widths)
+        self.monitors.append(monitor)
+        self.engine.attach_flux_monitor(monitor)
+        return monitor

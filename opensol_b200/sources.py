@@ -1,0 +1,173 @@
+"""Temporal waveforms and soft line sources of the B200 FDTD engines.
+
+Waveforms are evaluated on the host in float64 with Python's math functions for a Python float time, exactly as
+open_sol's per-step call does (open_sol/core/sources.py:13-100), and rounded once to float32: the device reads a
+per-step table of amplitude * temporal(t + dt/2) instead of a per-step host scalar, so a whole chunk of steps runs
+without the host.  The sheet-current calibration (profile = cb |sqrt(eps/mu) cos(kappa/2)| 2 / (eta0 w_perp)) is
+computed on the host from the line cells' materials (open_sol/physics/em/sources.py:383-392,430-436,582-602).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .constants import C0, DTYPE, EPS0, ETA0, MU0
+
+
+class GaussianPulse:
+    """exp(-((t - t0)/tau)^2) sin(2 pi f0 (t - t0)), tau = 1/(pi bandwidth f0), t0 = 4.5 tau (core/sources.py:23-53)."""
+
+    def __init__(self, f0: float, bandwidth: float = 0.5, t0_factor: float = 4.5):
+        self.f0 = f0
+        self.bandwidth = bandwidth
+        self.tau = 1.0 / (bandwidth * f0 * np.pi)
+        self.t0 = t0_factor * self.tau
+
+    def __call__(self, t):
+        if isinstance(t, (float, int)):
+            delay = t - self.t0
+            return math.exp(-(delay / self.tau) ** 2) * math.sin(2.0 * math.pi * self.f0 * delay)
+        delay = np.asarray(t, dtype=np.float64) - self.t0
+        return np.exp(-(delay / self.tau) ** 2) * np.sin(2.0 * np.pi * self.f0 * delay)
+
+    @property
+    def duration(self) -> float:
+        return 2.0 * self.t0
+
+    def spectral_limit(self) -> float:
+        return self.f0 * (1.0 + 3.72 * self.bandwidth)
+
+
+class ContinuousWave:
+    """(1 - exp(-t / tau_ramp)) sin(2 pi f0 t), tau_ramp = ramp_periods / f0 (core/sources.py:56-78)."""
+
+    def __init__(self, f0: float, ramp_periods: float = 3.0):
+        self.f0 = f0
+        self.tau_ramp = ramp_periods / f0
+
+    def __call__(self, t):
+        if isinstance(t, (float, int)):
+            return (1.0 - math.exp(-t / self.tau_ramp)) * math.sin(2.0 * math.pi * self.f0 * t)
+        times = np.asarray(t, dtype=np.float64)
+        return (1.0 - np.exp(-times / self.tau_ramp)) * np.sin(2.0 * np.pi * self.f0 * times)
+
+    def spectral_limit(self):
+        return None
+
+
+class RickerWavelet:
+    """(1 - 2 a^2) exp(-a^2), a = pi f_peak (t - t0), t0 = 4 / f_peak (core/sources.py:81-100)."""
+
+    def __init__(self, f_peak: float, t0_factor: float = 4.0):
+        self.f_peak = f_peak
+        self.t0 = t0_factor / f_peak
+
+    def __call__(self, t):
+        if isinstance(t, (float, int)):
+            arg = math.pi * self.f_peak * (t - self.t0)
+            return (1.0 - 2.0 * arg * arg) * math.exp(-arg * arg)
+        arg = np.pi * self.f_peak * (np.asarray(t, dtype=np.float64) - self.t0)
+        return (1.0 - 2.0 * arg ** 2) * np.exp(-arg ** 2)
+
+    @property
+    def duration(self) -> float:
+        return 2.0 * self.t0
+
+    def spectral_limit(self) -> float:
+        return 4.2 * self.f_peak
+
+
+def make_temporal(waveform, frequency, bandwidth):
+    if waveform == 'gaussian':
+        return GaussianPulse(frequency, bandwidth)
+    if waveform == 'cw':
+        return ContinuousWave(frequency)
+    if waveform == 'ricker':
+        return RickerWavelet(frequency)
+    raise ValueError(f"unknown waveform {waveform!r}; valid: 'gaussian', 'cw', 'ricker'")
+
+
+def carrier_angular_frequency(temporal) -> float:
+    frequency = temporal.f_peak if isinstance(temporal, RickerWavelet) else temporal.f0
+    return 2.0 * np.pi * float(frequency)
+
+
+def resolve_frequency(wavelength, frequency) -> float:
+    """Source frequency [Hz] from exactly one of wavelength [m] / frequency [Hz] (physics/em/__init__.py:560-568)."""
+    if (wavelength is None) == (frequency is None):
+        raise ValueError(f"pass exactly one of wavelength or frequency, got wavelength={wavelength}, "
+                         f"frequency={frequency}")
+    value = float(frequency if frequency is not None else wavelength)
+    if not (np.isfinite(value) and value > 0):
+        raise ValueError(f"source wavelength / frequency must be finite and > 0, got {value}")
+    return value if frequency is not None else C0 / value
+
+
+class LineSource:
+    """Soft E_z sheet current on a grid line: axis 'x' = along x at y-cell `position`, 'y' = along y at x-cell
+    `position`, over the half-open cell range `span` (core/sources.py:190-229).  `profile` is the calibrated float32
+    injection per cell (set at finalize)."""
+
+    def __init__(self, axis, position, temporal, amplitude=1.0, span=None, profile=None):
+        if axis not in ('x', 'y'):
+            raise ValueError(f"LineSource axis must be 'x' or 'y', got {axis!r}")
+        if span is not None:
+            span = (int(span[0]), int(span[1]))
+            if not 0 <= span[0] < span[1]:
+                raise ValueError(f"LineSource span must be a half-open cell range lo < hi, got {span}")
+        self.axis = axis
+        self.position = int(position)
+        self.temporal = temporal
+        self.amplitude = DTYPE(amplitude)
+        self.span = span
+        self.profile = profile
+
+    def values(self, t_half_list):
+        """float32 amplitude * temporal(t) per time (the per-step value of LineSource.inject)."""
+        out = np.empty(len(t_half_list), dtype=np.float32)
+        temporal, amplitude = self.temporal, self.amplitude
+        for k, t in enumerate(t_half_list):
+            out[k] = DTYPE(amplitude * temporal(float(t)))
+        return out
+
+
+def sheet_admittance(line_eps, mu_r, sigma_m, omega, normal_spacing, dt):
+    """float32 |sqrt(eps/mu) cos(kappa/2)| of the line cells at omega (physics/em/sources.py:430-436 with
+    yee_grid.sheet_launch_factor, yee_grid.py:58-65)."""
+    permeability = np.asarray(mu_r).astype(np.complex128) - 1j * np.asarray(sigma_m).astype(np.float64) / (omega * MU0)
+    vacuum_half_phase = float(normal_spacing) * math.sin(0.5 * float(omega) * float(dt)) / (C0 * float(dt))
+    launch = np.sqrt(1.0 - np.asarray(line_eps * permeability, dtype=np.complex128) * vacuum_half_phase ** 2)
+    return np.abs(np.sqrt(line_eps / permeability) * launch).astype(DTYPE)
+
+
+def e_coefficients_host(eps_r, sigma_e, dt):
+    """float32 (ca, cb) of cells (fdtd_ez_2d_kernels.py:314-319), used for the calibration line cells."""
+    dt = DTYPE(dt)
+    eps = np.asarray(eps_r, dtype=DTYPE) * DTYPE(EPS0)
+    k = np.asarray(sigma_e, dtype=DTYPE) * dt / (2.0 * eps)
+    denom = 1.0 + k
+    return (1.0 - k) / denom, (dt / eps) / denom
+
+
+def calibrate_line_source(source, materials, omega, normal_width, dt):
+    """float32 profile of an E_z sheet current (SheetCurrentCalibration.apply for a LineSource,
+    physics/em/sources.py:582-602): cb * admittance * 2 / (eta0 w_perp) on the line cells."""
+    lo, hi = source.span
+    if source.axis == 'x':
+        line = (slice(lo, hi), source.position)
+    else:
+        line = (source.position, slice(lo, hi))
+
+    def cells(name):
+        arr = materials.get(name)
+        if arr is None:
+            return np.full(hi - lo, DTYPE(materials.DEFAULTS[name]), dtype=DTYPE)
+        return np.ascontiguousarray(arr[line])
+
+    eps_line, sigma_line = cells('eps_r'), cells('sigma_e')
+    _, cb_line = e_coefficients_host(eps_line, sigma_line, dt)
+    line_eps = eps_line.astype(np.complex128) - 1j * sigma_line.astype(np.float64) / (omega * EPS0)
+    admittance = sheet_admittance(line_eps, cells('mu_r'), cells('sigma_m'), omega, normal_width, dt)
+    weight = np.asarray(2.0 * np.ones(hi - lo) / (float(ETA0) * normal_width), dtype=DTYPE)
+    return (cb_line * admittance * weight).astype(DTYPE)

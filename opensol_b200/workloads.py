@@ -1,0 +1,54 @@
+"""Seeded synthetic workloads of the FDTD benchmarks, applied through the public scripting API (any target with
+add_dielectric_circle / add_dielectric_rectangle / add_line_source / add_flux_monitor).
+
+roofline_2d: an 8192 x 8192 total grid (8152 x 8152 window + 20 CPML cells per side) at dx = 20 nm, 2000 dielectric
+cylinders (centres uniform in the window interior, radius U(50, 200) nm, eps_r U(2, 12), painted in draw order), a
+Gaussian line source at 1550 nm with relative bandwidth 0.5 along y near the lo-x edge, and four 16-frequency flux
+lines (x = 10 % / 90 % and y = 10 % / 90 % of the window, frequencies spread over the source band); 10,000 steps.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .constants import C0
+
+ROOFLINE_2D = {
+    'total_cells': 8192, 'dx': 20e-9, 'npml': 20, 'n_cylinders': 2000, 'radius': (50e-9, 200e-9),
+    'eps_r': (2.0, 12.0), 'wavelength': 1550e-9, 'bandwidth': 0.5, 'n_freqs': 16, 'steps': 10_000, 'seed': 2024,
+}
+
+
+def roofline_2d_sim_args(total_cells=8192, dx=20e-9, npml=20):
+    """Simulation(size_x, size_y, dx, npml, boundaries='pml') arguments of a total_cells^2 grid incl. the CPML."""
+    window = (total_cells - 2 * npml) * dx
+    return {'size_x': window, 'size_y': window, 'dx': dx, 'npml': npml, 'boundaries': 'pml'}
+
+
+def roofline_2d_ops(total_cells=8192, dx=20e-9, npml=20, n_cylinders=2000, seed=2024, amplitude=1.0):
+    """The method calls of the roofline workload, as (method, args, kwargs) in draw order."""
+    spec = ROOFLINE_2D
+    window = (total_cells - 2 * npml) * dx
+    rng = np.random.default_rng(seed)
+    radius = rng.uniform(*spec['radius'], n_cylinders)
+    centres = rng.uniform(0.15 * window, 0.85 * window, (n_cylinders, 2))
+    eps = rng.uniform(*spec['eps_r'], n_cylinders)
+    ops = [('add_dielectric_circle', (float(cx), float(cy), float(r)), {'eps_r': float(e)})
+           for (cx, cy), r, e in zip(centres, radius, eps)]
+    f0 = C0 / spec['wavelength']
+    bw = spec['bandwidth']
+    freqs = np.linspace(f0 * (1 - bw / 2), f0 * (1 + bw / 2), spec['n_freqs']).tolist()
+    ops.append(('add_line_source', ('y', 0.08 * window), {'wavelength': spec['wavelength'], 'bandwidth': bw,
+                                                          'amplitude': amplitude}))
+    for axis, frac in (('y', 0.10), ('y', 0.90), ('x', 0.10), ('x', 0.90)):
+        ops.append(('add_flux_monitor', (axis, frac * window, (0.0, window)), {'frequencies': freqs}))
+    return ops
+
+
+def apply(target, ops):
+    """Apply (method, args, kwargs) calls; returns the flux monitors in add order."""
+    monitors = []
+    for method, args, kwargs in ops:
+        out = getattr(target, method)(*args, **kwargs)
+        if method == 'add_flux_monitor':
+            monitors.append(out)
+    return monitors
