@@ -97,7 +97,8 @@ int os_fdtd2d_add_line_source(OsFdtd2D *h, int32_t axis, int32_t position, int32
 int os_fdtd2d_set_line_profile(OsFdtd2D *h, int32_t source_id, const float *profile);
 
 /* Flux line: E_z and the tangential H (H_y for normal_axis 0, H_x for 1) on cells [lo, hi) of x-cell (normal 0) or
- * y-cell (normal 1) `position`, nf frequencies, complex128 running DFTs: FluxMonitor (physics/em/monitors.py:325). */
+ * y-cell (normal 1) `position`, nf frequencies, complex128 running DFTs: FluxMonitor (physics/em/monitors.py:325).
+ * At most 8. */
 int os_fdtd2d_add_flux_line(OsFdtd2D *h, int32_t normal_axis, int32_t position, int32_t lo, int32_t hi, int32_t nf,
                             int32_t *monitor_id);
 
@@ -110,6 +111,25 @@ int os_fdtd2d_set_sample_interval(OsFdtd2D *h, int64_t sample_interval);
  * is taken after engine step q * sample_interval; monitors.py:22-24,219-220).  Asynchronous on the handle's stream. */
 int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line_values, int64_t first_sample,
                       int64_t n_samples, const float *phases);
+
+/* Kernel choice: variant 1 (default) advances steps_per_launch (1..4) Yee steps per launch with temporally blocked,
+ * double-buffered kernels, tile_rows rows per interior tile; variant 0 launches one H and one E kernel per step.
+ * Every choice gives bit-identical results.  No open_sol counterpart (open_sol launches per half step). */
+int os_fdtd2d_configure(OsFdtd2D *h, int32_t variant, int32_t steps_per_launch, int32_t tile_rows);
+
+/* Kernels the last os_fdtd2d_advance launched. */
+int os_fdtd2d_launch_count(OsFdtd2D *h, int64_t *launches);
+
+/* Profiling: with `on`, every kernel of the following advances is bracketed by CUDA events; kernel_times returns the
+ * summed device milliseconds and launch count of one kind over the last advance (0 interior blocked kernel, 1 general
+ * blocked kernel, 2 DFT kernel, 3 per-step kernel pair).  No open_sol counterpart. */
+int os_fdtd2d_set_profiling(OsFdtd2D *h, int32_t on);
+
+/* The blocked kernels' plan for steps_per_launch: cells of the interior rectangle and tiles (warps) of the interior
+ * and general kernels.  No open_sol counterpart. */
+int os_fdtd2d_plan_info(OsFdtd2D *h, int32_t steps_per_launch, int64_t *interior_cells, int64_t *interior_tiles,
+                        int64_t *general_tiles);
+int os_fdtd2d_kernel_times(OsFdtd2D *h, int32_t kind, double *total_ms, int64_t *launches);
 
 /* Engine steps taken since create / reset (FDTDEngine2D_Ez.n_step). */
 int os_fdtd2d_step_count(OsFdtd2D *h, int64_t *n_step);

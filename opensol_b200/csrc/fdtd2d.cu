@@ -1,15 +1,19 @@
-// 2D E_z-polarisation FDTD engine for sm_100a: device state, step kernels and the os_fdtd2d_* C ABI.
+// 2D E_z-polarisation FDTD engine for sm_100a: device state, launch planning and the os_fdtd2d_* C ABI.
 //
-// One Yee step = the H kernel (Yee H update with the H-row CPML psi recursion and correction fused in) followed by the
-// E kernel (Yee E update, E-row CPML, then the soft line sources), and every sample_interval steps the line-DFT kernel.
-// This is open_sol's step (open_sol/physics/em/solvers/fdtd_ez_2d.py:71-119) with its separate CPML and source
-// launches folded into the two field passes.  The arithmetic of every cell follows the reference's evaluation order
-// (fdtd_ez_2d_kernels.py:23-122, boundaries.py:27-37, core/sources.py:146-154) and the file is compiled with
+// The default path (fdtd2d_tb.cuh) advances T Yee steps per launch: an interior kernel (4 columns per thread, 128-bit
+// loads, no CPML) plus a general kernel for the CPML slabs and grid edges, both reading one field buffer set and
+// writing the other; then, when the launch crossed DFT sample steps, the staged-DFT kernel.  The per-half-step kernels
+// of fdtd2d_kernels.cuh (one thread per cell, fields updated in place) remain selectable as variant 0 and serve as
+// the plain reference of the same arithmetic.  The arithmetic of every cell follows open_sol's evaluation order
+// (fdtd_ez_2d_kernels.py:23-122, boundaries.py:27-37, core/sources.py:146-154) and the files are compiled with
 // -fmad=false, so each product and sum is rounded on its own as on the CPU: results are bit-identical to open_sol's
 // CPU backend.  The CPML corrections of a cell are applied in FACES order (x sides, then y sides), as open_sol's one
 // launch per side does.
 #include "common.cuh"
 #include "fdtd2d_kernels.cuh"
+#include "fdtd2d_tb.cuh"
+
+#include <algorithm>
 
 #include <vector>
 #include <memory>
@@ -24,6 +28,7 @@ struct LineSource2D {
 struct FluxLine2D {
     int32_t normal_axis, position, lo, hi, nf;
     DeviceArray<double> e_acc, h_acc;   // (nf, n) complex128 as double pairs
+    DeviceArray<float> stage;           // (TB_MAX_T, 2, n) samples of one launch
 };
 
 }  // namespace os
@@ -34,14 +39,25 @@ struct OsFdtd2D {
     cudaStream_t own_stream = nullptr;    // created with the handle, destroyed with it
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     bool timed = false;
-    os::DeviceArray<float> ez, hx, hy;
+    os::DeviceArray<float> ez[2], hx[2], hy[2];   // double-buffered fields; `cur` is the live set
+    int cur = 0;
     os::DeviceArray<float> ca, cb, da, db;
     float da_uniform = 1.0f, db_uniform = 0.0f;
     bool has_ca = false, has_dadb = false, has_cb = false, has_spacings = false;
     os::DeviceArray<float> inv_dx_e, inv_dx_h, inv_dy_e, inv_dy_h;
     os::DeviceArray<float> cpml_rows[4];   // per side: b_e, a_e, inv_e, b_h, a_h, inv_h (6 * npml)
-    os::DeviceArray<float> psi_e[4], psi_h[4];
+    os::DeviceArray<float> psi_e[2][4], psi_h[2][4];
     bool cpml_set[4] = {false, false, false, false};
+    std::vector<float> host_inv[4];       // inv_dx_e, inv_dx_h, inv_dy_e, inv_dy_h (host copies: interior check)
+    int32_t variant = 1;                  // 0: per-half-step kernels, 1: temporally blocked
+    int32_t steps_per_launch = 4;         // T of the blocked kernels
+    int32_t tile_rows = 128;              // rows per interior tile
+    int32_t gen_tile_rows = 64;           // rows per general tile
+    int64_t launches = 0;                 // kernels launched by the last advance
+    bool profiling = false;               // bracket every kernel with events (os_fdtd2d_kernel_times)
+    std::vector<cudaEvent_t> prof_events; // pool, grown on demand
+    std::vector<int> prof_kind;           // kind of each recorded pair: 0 interior, 1 general, 2 DFT, 3 per-step
+    size_t prof_used = 0;
     std::vector<std::unique_ptr<os::LineSource2D>> lines;
     std::vector<std::unique_ptr<os::FluxLine2D>> fluxes;
     int64_t sample_interval = 1;
@@ -62,12 +78,13 @@ static size_t cells(const OsFdtd2D *h) { return (size_t)h->grid.nx * (size_t)h->
 
 static int zero_state(OsFdtd2D *h) {
     const size_t n = cells(h);
-    OS_CUDA(cudaMemsetAsync(h->ez.ptr, 0, n * sizeof(float), h->stream));
-    OS_CUDA(cudaMemsetAsync(h->hx.ptr, 0, n * sizeof(float), h->stream));
-    OS_CUDA(cudaMemsetAsync(h->hy.ptr, 0, n * sizeof(float), h->stream));
+    const int c = h->cur;
+    OS_CUDA(cudaMemsetAsync(h->ez[c].ptr, 0, n * sizeof(float), h->stream));
+    OS_CUDA(cudaMemsetAsync(h->hx[c].ptr, 0, n * sizeof(float), h->stream));
+    OS_CUDA(cudaMemsetAsync(h->hy[c].ptr, 0, n * sizeof(float), h->stream));
     for (int s = 0; s < 4; ++s) {
-        if (h->psi_e[s].ptr) OS_CUDA(cudaMemsetAsync(h->psi_e[s].ptr, 0, h->psi_e[s].bytes(), h->stream));
-        if (h->psi_h[s].ptr) OS_CUDA(cudaMemsetAsync(h->psi_h[s].ptr, 0, h->psi_h[s].bytes(), h->stream));
+        if (h->psi_e[c][s].ptr) OS_CUDA(cudaMemsetAsync(h->psi_e[c][s].ptr, 0, h->psi_e[c][s].bytes(), h->stream));
+        if (h->psi_h[c][s].ptr) OS_CUDA(cudaMemsetAsync(h->psi_h[c][s].ptr, 0, h->psi_h[c][s].bytes(), h->stream));
     }
     for (auto &f : h->fluxes) {
         OS_CUDA(cudaMemsetAsync(f->e_acc.ptr, 0, f->e_acc.bytes(), h->stream));
@@ -84,9 +101,9 @@ static Ez2DParams make_params(const OsFdtd2D *h) {
     p.periodic_x = h->grid.periodic_x;
     p.periodic_y = h->grid.periodic_y;
     p.npml = h->grid.npml;
-    p.ez = h->ez.ptr;
-    p.hx = h->hx.ptr;
-    p.hy = h->hy.ptr;
+    p.ez = h->ez[h->cur].ptr;
+    p.hx = h->hx[h->cur].ptr;
+    p.hy = h->hy[h->cur].ptr;
     p.ca = h->has_ca ? h->ca.ptr : nullptr;
     p.cb = h->cb.ptr;
     p.da = h->has_dadb ? h->da.ptr : nullptr;
@@ -109,8 +126,8 @@ static Ez2DParams make_params(const OsFdtd2D *h) {
         p.b_h[s] = rows + 3 * npml;
         p.a_h[s] = rows + 4 * npml;
         p.inv_h[s] = rows + 5 * npml;
-        p.psi_e[s] = h->psi_e[s].ptr;
-        p.psi_h[s] = h->psi_h[s].ptr;
+        p.psi_e[s] = h->psi_e[h->cur][s].ptr;
+        p.psi_h[s] = h->psi_h[h->cur][s].ptr;
     }
     p.n_lines = (int32_t)h->lines.size();
     for (size_t l = 0; l < h->lines.size(); ++l) {
@@ -158,14 +175,18 @@ extern "C" int os_fdtd2d_create(const OsGrid2D *grid, OsFdtd2D **out) {
     OS_CUDA(cudaEventCreate(&h->ev_start));
     OS_CUDA(cudaEventCreate(&h->ev_stop));
     const size_t n = cells(h.get());
-    OS_TRY(h->ez.alloc(n));
-    OS_TRY(h->hx.alloc(n));
-    OS_TRY(h->hy.alloc(n));
+    for (int b = 0; b < 2; ++b) {
+        OS_TRY(h->ez[b].alloc(n));
+        OS_TRY(h->hx[b].alloc(n));
+        OS_TRY(h->hy[b].alloc(n));
+    }
     for (int s = 0; s < 4; ++s) {
         if (!(g.cpml_sides & (1 << s))) continue;
         const size_t slab = (s < 2 ? (size_t)g.ny : (size_t)g.nx) * (size_t)g.npml;
-        OS_TRY(h->psi_e[s].alloc(slab));
-        OS_TRY(h->psi_h[s].alloc(slab));
+        for (int b = 0; b < 2; ++b) {
+            OS_TRY(h->psi_e[b][s].alloc(slab));
+            OS_TRY(h->psi_h[b][s].alloc(slab));
+        }
         OS_TRY(h->cpml_rows[s].alloc(6 * (size_t)g.npml));
     }
     OS_TRY(zero_state(h.get()));
@@ -178,6 +199,7 @@ extern "C" int os_fdtd2d_destroy(OsFdtd2D *h) {
     if (!h) return OS_OK;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     if (h->ev_start) cudaEventDestroy(h->ev_start);
     if (h->ev_stop) cudaEventDestroy(h->ev_stop);
     if (h->own_stream) cudaStreamSynchronize(h->own_stream);
@@ -195,6 +217,10 @@ extern "C" int os_fdtd2d_set_spacings(OsFdtd2D *h, const float *inv_dx_e, const 
     OS_TRY(upload(h->inv_dx_h, inv_dx_h, h->grid.nx, h->stream));
     OS_TRY(upload(h->inv_dy_e, inv_dy_e, h->grid.ny, h->stream));
     OS_TRY(upload(h->inv_dy_h, inv_dy_h, h->grid.ny, h->stream));
+    h->host_inv[0].assign(inv_dx_e, inv_dx_e + h->grid.nx);
+    h->host_inv[1].assign(inv_dx_h, inv_dx_h + h->grid.nx);
+    h->host_inv[2].assign(inv_dy_e, inv_dy_e + h->grid.ny);
+    h->host_inv[3].assign(inv_dy_h, inv_dy_h + h->grid.ny);
     h->has_spacings = true;
     return OS_OK;
 }
@@ -335,6 +361,7 @@ extern "C" int os_fdtd2d_add_flux_line(OsFdtd2D *h, int32_t normal_axis, int32_t
     OS_CHECK(0 <= position && position < n_across, OS_ERR_INVALID, "FluxMonitor position %d outside the grid",
              position);
     OS_CHECK(nf >= 1, OS_ERR_INVALID, "monitor frequencies must be a non-empty list");
+    OS_CHECK(h->fluxes.size() < (size_t)TB_MAX_MONS, OS_ERR_INVALID, "at most %d flux lines per engine", TB_MAX_MONS);
     OS_TRY(bind_device(h));
     std::unique_ptr<FluxLine2D> m(new FluxLine2D());
     m->normal_axis = normal_axis;
@@ -345,6 +372,7 @@ extern "C" int os_fdtd2d_add_flux_line(OsFdtd2D *h, int32_t normal_axis, int32_t
     const size_t n = (size_t)nf * (size_t)(hi - lo) * 2;
     OS_TRY(m->e_acc.alloc(n));
     OS_TRY(m->h_acc.alloc(n));
+    OS_TRY(m->stage.alloc((size_t)TB_MAX_T * 2 * (size_t)(hi - lo)));
     OS_CUDA(cudaMemsetAsync(m->e_acc.ptr, 0, m->e_acc.bytes(), h->stream));
     OS_CUDA(cudaMemsetAsync(m->h_acc.ptr, 0, m->h_acc.bytes(), h->stream));
     if (monitor_id) *monitor_id = (int32_t)h->fluxes.size();
@@ -359,6 +387,261 @@ extern "C" int os_fdtd2d_set_sample_interval(OsFdtd2D *h, int64_t sample_interva
     return OS_OK;
 }
 
+namespace os {
+
+// Event pair around one kernel launch when profiling (kind: 0 interior, 1 general, 2 DFT, 3 per-step kernels).
+static int prof_begin(OsFdtd2D *h, int kind) {
+    if (!h->profiling) return OS_OK;
+    while (h->prof_events.size() < 2 * (h->prof_used + 1)) {
+        cudaEvent_t e;
+        OS_CUDA(cudaEventCreate(&e));
+        h->prof_events.push_back(e);
+    }
+    if (h->prof_kind.size() < h->prof_used + 1) h->prof_kind.resize(h->prof_used + 1);
+    h->prof_kind[h->prof_used] = kind;
+    OS_CUDA(cudaEventRecord(h->prof_events[2 * h->prof_used], h->stream));
+    return OS_OK;
+}
+
+static int prof_end(OsFdtd2D *h) {
+    if (!h->profiling) return OS_OK;
+    OS_CUDA(cudaEventRecord(h->prof_events[2 * h->prof_used + 1], h->stream));
+    h->prof_used += 1;
+    return OS_OK;
+}
+
+struct Rect {
+    int r0, r1, c0, c1;
+};
+
+static int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+// Tiles of one kernel: rectangles cut into tile_w x tile_rows output tiles (one warp each).
+static void set_tiles(TBParams &q, const std::vector<Rect> &rects, int tile_w, int tile_rows) {
+    q.n_rects = 0;
+    int first = 0;
+    for (const Rect &r : rects) {
+        if (r.r1 <= r.r0 || r.c1 <= r.c0) continue;
+        TBRect &t = q.rects[q.n_rects++];
+        t.r0 = r.r0;
+        t.r1 = r.r1;
+        t.c0 = r.c0;
+        t.c1 = r.c1;
+        t.tiles_c = (r.c1 - r.c0 + tile_w - 1) / tile_w;
+        t.first_tile = first;
+        first += t.tiles_c * ((r.r1 - r.r0 + tile_rows - 1) / tile_rows);
+    }
+    q.tile_w = tile_w;
+    q.tile_rows = tile_rows;
+    q.n_tiles = first;
+}
+
+static bool constant_over(const std::vector<float> &v, int a, int b, float *value) {
+    if (a < 0 || b > (int)v.size() || a >= b) return false;
+    for (int k = a; k < b; ++k)
+        if (v[k] != v[a]) return false;
+    *value = v[a];
+    return true;
+}
+
+// The interior rectangle (cells whose T-step dependency cone avoids the CPML slabs and the non-periodic edges) and the
+// border rectangles around it.  Interior rows need i0 - T >= npml + 1 and i1 - 1 + T <= nx - npml - 2 on a CPML x
+// axis; columns likewise with the 4-column left halo of the 128-bit loads.
+static void plan_tiles(const OsFdtd2D *h, int T, TBParams &interior, TBParams &general, bool &has_interior) {
+    const OsGrid2D &g = h->grid;
+    const int npml = g.npml;
+    const bool cx = (g.cpml_sides & 3) != 0, cy = (g.cpml_sides & 12) != 0;
+    Rect in{0, g.nx, 0, g.ny};
+    if (!g.periodic_x) {
+        in.r0 = cx ? npml + 1 + T : g.nx;
+        in.r1 = cx ? g.nx - npml - 1 - T : 0;
+    }
+    if (!g.periodic_y) {
+        in.c0 = cy ? round_up(npml + 1 + 4, 4) : g.ny;
+        in.c1 = cy ? g.ny - npml - 1 - T : 0;
+    }
+    has_interior = in.r1 > in.r0 && in.c1 > in.c0 && g.ny % 4 == 0 && !h->has_dadb && h->da_uniform == 1.0f;
+    // uniform curl spacings over the interior cone
+    if (has_interior) {
+        const int ra = g.periodic_x ? 0 : in.r0 - T, rb = g.periodic_x ? g.nx : in.r1 + T;
+        const int ca = g.periodic_y ? 0 : in.c0 - 4, cbnd = g.periodic_y ? g.ny : std::min(g.ny, in.c1 + 124);
+        has_interior = constant_over(h->host_inv[0], ra, rb, &interior.s_inv_dx_e) &&
+                       constant_over(h->host_inv[1], ra, rb, &interior.s_inv_dx_h) &&
+                       constant_over(h->host_inv[2], ca, cbnd, &interior.s_inv_dy_e) &&
+                       constant_over(h->host_inv[3], ca, cbnd, &interior.s_inv_dy_h);
+    }
+    std::vector<Rect> border;
+    if (!has_interior) {
+        border.push_back(Rect{0, g.nx, 0, g.ny});
+        set_tiles(interior, {}, 120, h->tile_rows);
+    } else {
+        border.push_back(Rect{0, in.r0, 0, g.ny});
+        border.push_back(Rect{in.r1, g.nx, 0, g.ny});
+        border.push_back(Rect{in.r0, in.r1, 0, in.c0});
+        border.push_back(Rect{in.r0, in.r1, in.c1, g.ny});
+        set_tiles(interior, {in}, 120, h->tile_rows);
+    }
+    set_tiles(general, border, 32 - 2 * T, h->gen_tile_rows);
+}
+
+static void fill_common(const OsFdtd2D *h, TBParams &q) {
+    const OsGrid2D &g = h->grid;
+    q.nx = g.nx;
+    q.ny = g.ny;
+    q.px = g.periodic_x;
+    q.py = g.periodic_y;
+    q.npml = g.npml;
+    q.cpml_mask = g.cpml_sides;
+    q.cb = h->cb.ptr;
+    q.ca = h->has_ca ? h->ca.ptr : nullptr;
+    q.da = h->has_dadb ? h->da.ptr : nullptr;
+    q.db = h->has_dadb ? h->db.ptr : nullptr;
+    q.da_u = h->da_uniform;
+    q.db_u = h->db_uniform;
+    q.inv_dx_e = h->inv_dx_e.ptr;
+    q.inv_dx_h = h->inv_dx_h.ptr;
+    q.inv_dy_e = h->inv_dy_e.ptr;
+    q.inv_dy_h = h->inv_dy_h.ptr;
+    for (int s = 0; s < 4; ++s) q.cpml_rows[s] = h->cpml_rows[s].ptr;
+    q.n_lines = (int32_t)h->lines.size();
+    for (size_t l = 0; l < h->lines.size(); ++l) {
+        q.lines[l].axis = h->lines[l]->axis;
+        q.lines[l].position = h->lines[l]->position;
+        q.lines[l].lo = h->lines[l]->lo;
+        q.lines[l].hi = h->lines[l]->hi;
+        q.lines[l].profile = h->lines[l]->profile.ptr;
+    }
+    q.line_values = h->line_values.ptr;
+    q.n_mons = (int32_t)h->fluxes.size();
+    for (size_t k = 0; k < h->fluxes.size(); ++k) {
+        q.mons[k].normal_axis = h->fluxes[k]->normal_axis;
+        q.mons[k].position = h->fluxes[k]->position;
+        q.mons[k].lo = h->fluxes[k]->lo;
+        q.mons[k].hi = h->fluxes[k]->hi;
+        q.mons[k].stage = h->fluxes[k]->stage.ptr;
+    }
+    q.m = h->sample_interval;
+}
+
+template <int T>
+static int launch_tb(OsFdtd2D *h, const TBParams &interior, const TBParams &general, bool has_interior) {
+    const dim3 threads(TB_WARPS * 32);
+    if (has_interior && interior.n_tiles) {
+        const dim3 blocks((unsigned)((interior.n_tiles + TB_WARPS - 1) / TB_WARPS));
+        OS_TRY(prof_begin(h, 0));
+        if (h->has_ca) ez2d_tb_kernel<T, 4, false, true><<<blocks, threads, 0, h->stream>>>(interior);
+        else ez2d_tb_kernel<T, 4, false, false><<<blocks, threads, 0, h->stream>>>(interior);
+        OS_TRY(prof_end(h));
+        h->launches += 1;
+    }
+    if (general.n_tiles) {
+        const dim3 blocks((unsigned)((general.n_tiles + TB_WARPS - 1) / TB_WARPS));
+        OS_TRY(prof_begin(h, 1));
+        if (h->has_ca) ez2d_tb_kernel<T, 1, true, true><<<blocks, threads, 0, h->stream>>>(general);
+        else ez2d_tb_kernel<T, 1, true, false><<<blocks, threads, 0, h->stream>>>(general);
+        OS_TRY(prof_end(h));
+        h->launches += 1;
+    }
+    OS_CUDA(cudaGetLastError());
+    return OS_OK;
+}
+
+// Temporally blocked chunk: launches of T steps (a shorter last one), buffers swapped after each.
+static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples) {
+    const int64_t m = h->sample_interval;
+    int64_t k = 0;
+    while (k < n_steps) {
+        const int T = (int)std::min<int64_t>(h->steps_per_launch, n_steps - k);
+        TBParams interior{}, general{};
+        bool has_interior = false;
+        plan_tiles(h, T, interior, general, has_interior);
+        fill_common(h, interior);
+        fill_common(h, general);
+        const int in = h->cur, out = h->cur ^ 1;
+        for (TBParams *q : {&interior, &general}) {
+            q->ez_in = h->ez[in].ptr;
+            q->hx_in = h->hx[in].ptr;
+            q->hy_in = h->hy[in].ptr;
+            q->ez_out = h->ez[out].ptr;
+            q->hx_out = h->hx[out].ptr;
+            q->hy_out = h->hy[out].ptr;
+            for (int s = 0; s < 4; ++s) {
+                q->psi_e_in[s] = h->psi_e[in][s].ptr;
+                q->psi_h_in[s] = h->psi_h[in][s].ptr;
+                q->psi_e_out[s] = h->psi_e[out][s].ptr;
+                q->psi_h_out[s] = h->psi_h[out][s].ptr;
+            }
+            q->values_stride = n_steps;
+            q->k0 = k;
+            q->n0 = h->n_step;
+            q->q_first = h->n_step / m + 1;
+        }
+        int rc = OS_OK;
+        switch (T) {
+            case 1: rc = launch_tb<1>(h, interior, general, has_interior); break;
+            case 2: rc = launch_tb<2>(h, interior, general, has_interior); break;
+            case 3: rc = launch_tb<3>(h, interior, general, has_interior); break;
+            default: rc = launch_tb<4>(h, interior, general, has_interior); break;
+        }
+        if (rc != OS_OK) return rc;
+        h->cur = out;
+        // DFT samples taken inside this launch, accumulated in sample order
+        const int64_t q_lo = h->n_step / m + 1, q_hi = (h->n_step + T) / m;
+        if (!h->fluxes.empty() && q_hi >= q_lo) {
+            size_t offset = 0;
+            for (auto &f : h->fluxes) {
+                const float *ph = h->phases.ptr + offset + (size_t)(q_lo - first_sample) * f->nf * 2;
+                const int n = f->hi - f->lo;
+                const int total = n * f->nf;
+                OS_TRY(prof_begin(h, 2));
+                ez2d_flux_staged_kernel<<<(total + 255) / 256, 256, 0, h->stream>>>(
+                    f->stage.ptr, n, f->nf, (int)(q_hi - q_lo + 1), ph, f->e_acc.ptr, f->h_acc.ptr);
+                OS_TRY(prof_end(h));
+                h->launches += 1;
+                offset += (size_t)n_samples * f->nf * 2;
+            }
+            OS_CUDA(cudaGetLastError());
+        }
+        h->n_step += T;
+        k += T;
+    }
+    return OS_OK;
+}
+
+// Per-half-step chunk (variant 0): H kernel, E kernel, DFT of sample steps; fields updated in place.
+static int advance_per_step(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples) {
+    const int64_t m = h->sample_interval;
+    Ez2DParams p = make_params(h);
+    const dim3 block(EZ2D_BLOCK_X, EZ2D_BLOCK_Y);
+    const dim3 grid((unsigned)((h->grid.ny + block.x - 1) / block.x), (unsigned)((h->grid.nx + block.y - 1) / block.y));
+    for (int64_t k = 0; k < n_steps; ++k) {
+        OS_TRY(prof_begin(h, 3));
+        ez2d_h_kernel<<<grid, block, 0, h->stream>>>(p);
+        ez2d_e_kernel<<<grid, block, 0, h->stream>>>(p, h->line_values.ptr, n_steps, k);
+        OS_TRY(prof_end(h));
+        h->launches += 2;
+        h->n_step += 1;
+        if (!h->fluxes.empty() && h->n_step % m == 0) {
+            const int64_t q = h->n_step / m;
+            size_t offset = 0;
+            for (auto &f : h->fluxes) {
+                const float *ph = h->phases.ptr + offset + (size_t)(q - first_sample) * f->nf * 2;
+                const int n = f->hi - f->lo;
+                const int total = n * f->nf;
+                ez2d_flux_kernel<<<(total + 255) / 256, 256, 0, h->stream>>>(
+                    p.ez, f->normal_axis == 0 ? p.hy : p.hx, h->grid.ny, f->normal_axis, f->position, f->lo, n,
+                    f->nf, ph, f->e_acc.ptr, f->h_acc.ptr);
+                h->launches += 1;
+                offset += (size_t)n_samples * f->nf * 2;
+            }
+        }
+    }
+    OS_CUDA(cudaGetLastError());
+    return OS_OK;
+}
+
+}  // namespace os
+
 extern "C" int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line_values, int64_t first_sample,
                                  int64_t n_samples, const float *phases) {
     OS_CHECK(h, OS_ERR_INVALID, "os_fdtd2d_advance: null handle");
@@ -367,6 +650,8 @@ extern "C" int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line
     for (int s = 0; s < 4; ++s)
         OS_CHECK(!(h->grid.cpml_sides & (1 << s)) || h->cpml_set[s], OS_ERR_STATE,
                  "os_fdtd2d_advance: CPML side %d has no recursion rows", 1 << s);
+    h->launches = 0;
+    h->prof_used = 0;
     if (n_steps == 0) return OS_OK;
     OS_CHECK(h->lines.empty() || line_values, OS_ERR_INVALID, "os_fdtd2d_advance: line_values is required");
     const int64_t m = h->sample_interval;
@@ -382,32 +667,75 @@ extern "C" int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line
     size_t phase_floats = 0;
     for (auto &f : h->fluxes) phase_floats += (size_t)n_samples * f->nf * 2;
     if (!h->fluxes.empty() && phase_floats && phases) OS_TRY(upload(h->phases, phases, phase_floats, h->stream));
-
-    Ez2DParams p = make_params(h);
-    const dim3 block(EZ2D_BLOCK_X, EZ2D_BLOCK_Y);
-    const dim3 grid((unsigned)((h->grid.ny + block.x - 1) / block.x), (unsigned)((h->grid.nx + block.y - 1) / block.y));
     OS_CUDA(cudaEventRecord(h->ev_start, h->stream));
-    for (int64_t k = 0; k < n_steps; ++k) {
-        ez2d_h_kernel<<<grid, block, 0, h->stream>>>(p);
-        ez2d_e_kernel<<<grid, block, 0, h->stream>>>(p, h->line_values.ptr, n_steps, k);
-        h->n_step += 1;
-        if (!h->fluxes.empty() && h->n_step % m == 0) {
-            const int64_t q = h->n_step / m;
-            size_t offset = 0;
-            for (auto &f : h->fluxes) {
-                const float *ph = h->phases.ptr + offset + (size_t)(q - first_sample) * f->nf * 2;
-                const int n = f->hi - f->lo;
-                const int total = n * f->nf;
-                ez2d_flux_kernel<<<(total + 255) / 256, 256, 0, h->stream>>>(
-                    h->ez.ptr, f->normal_axis == 0 ? h->hy.ptr : h->hx.ptr, h->grid.ny, f->normal_axis, f->position,
-                    f->lo, n, f->nf, ph, f->e_acc.ptr, f->h_acc.ptr);
-                offset += (size_t)n_samples * f->nf * 2;
-            }
-        }
-    }
+    const int rc = h->variant == 0 ? advance_per_step(h, n_steps, first_sample, n_samples)
+                                   : advance_blocked(h, n_steps, first_sample, n_samples);
+    if (rc != OS_OK) return rc;
     OS_CUDA(cudaEventRecord(h->ev_stop, h->stream));
-    OS_CUDA(cudaGetLastError());
     h->timed = true;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_configure(OsFdtd2D *h, int32_t variant, int32_t steps_per_launch, int32_t tile_rows) {
+    OS_CHECK(h, OS_ERR_INVALID, "os_fdtd2d_configure: null handle");
+    OS_CHECK(variant == 0 || variant == 1, OS_ERR_INVALID, "variant must be 0 (per half step) or 1 (blocked)");
+    OS_CHECK(steps_per_launch >= 1 && steps_per_launch <= TB_MAX_T, OS_ERR_INVALID,
+             "steps_per_launch must be in [1, %d], got %d", TB_MAX_T, steps_per_launch);
+    OS_CHECK(tile_rows >= 1, OS_ERR_INVALID, "tile_rows must be >= 1, got %d", tile_rows);
+    h->variant = variant;
+    h->steps_per_launch = steps_per_launch;
+    h->tile_rows = tile_rows;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_plan_info(OsFdtd2D *h, int32_t steps_per_launch, int64_t *interior_cells,
+                                   int64_t *interior_tiles, int64_t *general_tiles) {
+    OS_CHECK(h && interior_cells && interior_tiles && general_tiles, OS_ERR_INVALID,
+             "os_fdtd2d_plan_info: null argument");
+    OS_CHECK(steps_per_launch >= 1 && steps_per_launch <= TB_MAX_T, OS_ERR_INVALID,
+             "steps_per_launch must be in [1, %d]", TB_MAX_T);
+    OS_CHECK(h->has_spacings, OS_ERR_STATE, "os_fdtd2d_plan_info: spacings are not set");
+    TBParams interior{}, general{};
+    bool has_interior = false;
+    plan_tiles(h, steps_per_launch, interior, general, has_interior);
+    int64_t cells_in = 0;
+    if (has_interior)
+        for (int r = 0; r < interior.n_rects; ++r)
+            cells_in += (int64_t)(interior.rects[r].r1 - interior.rects[r].r0) *
+                        (int64_t)(interior.rects[r].c1 - interior.rects[r].c0);
+    *interior_cells = cells_in;
+    *interior_tiles = has_interior ? interior.n_tiles : 0;
+    *general_tiles = general.n_tiles;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_set_profiling(OsFdtd2D *h, int32_t on) {
+    OS_CHECK(h, OS_ERR_INVALID, "os_fdtd2d_set_profiling: null handle");
+    h->profiling = on != 0;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_kernel_times(OsFdtd2D *h, int32_t kind, double *total_ms, int64_t *launches) {
+    OS_CHECK(h && total_ms && launches, OS_ERR_INVALID, "os_fdtd2d_kernel_times: null argument");
+    OS_TRY(bind_device(h));
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    double total = 0.0;
+    int64_t count = 0;
+    for (size_t k = 0; k < h->prof_used; ++k) {
+        if (h->prof_kind[k] != kind) continue;
+        float ms = 0.0f;
+        OS_CUDA(cudaEventElapsedTime(&ms, h->prof_events[2 * k], h->prof_events[2 * k + 1]));
+        total += ms;
+        count += 1;
+    }
+    *total_ms = total;
+    *launches = count;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_launch_count(OsFdtd2D *h, int64_t *launches) {
+    OS_CHECK(h && launches, OS_ERR_INVALID, "os_fdtd2d_launch_count: null argument");
+    *launches = h->launches;
     return OS_OK;
 }
 
@@ -430,9 +758,9 @@ extern "C" int os_fdtd2d_read_flux_spectra(OsFdtd2D *h, int32_t monitor_id, doub
 
 static float *component_ptr(OsFdtd2D *h, int32_t component) {
     switch (component) {
-        case OS_EZ: return h->ez.ptr;
-        case OS_HX: return h->hx.ptr;
-        case OS_HY: return h->hy.ptr;
+        case OS_EZ: return h->ez[h->cur].ptr;
+        case OS_HX: return h->hx[h->cur].ptr;
+        case OS_HY: return h->hy[h->cur].ptr;
         default: return nullptr;
     }
 }

@@ -1,0 +1,492 @@
+// Temporally blocked 2D E_z step kernels: one launch advances the whole grid by T Yee steps.
+//
+// Layout.  Fields are double-buffered (read set "in", write set "out", swapped per launch), so a launch has no
+// read-after-write hazard between its warps and every warp works alone: no __syncthreads, no atomics.  The grid is
+// cut into tiles; one warp owns one tile's outputs (a rectangle of rows x columns) and streams its rows in increasing
+// i.  Thread `lane` holds C adjacent columns; neighbours across threads come by warp shuffle.
+//
+// Time skew.  While streaming, stage s (1..T) of the warp's pipeline computes step s of row r - s when row r is
+// loaded: H^s[i] needs E^(s-1) at rows i and i+1, E^s[i] needs H^s at rows i and i-1 (fdtd_ez_2d_kernels.py:23-122),
+// so every input of stage s is already in registers.  Each field is kept as two rows (this iteration's and the last
+// one's) per stage; the iteration parity PH selects which array plays which role, so no register moves are needed.
+// A tile loads T extra rows before and after its own rows and halo columns on both sides; the cells of that cone are
+// recomputed redundantly (bit-identical, every cell being a pure function of the inputs).
+//
+// Two variants share the code.  The interior variant (GEN = false, C = 4, 128-bit loads) covers the cells whose whole
+// dependency cone lies off the CPML slabs and grid edges: uniform curl spacings, da = 1, uniform db, cb (and ca for
+// lossy cells) per cell.  The general variant (GEN = true, C = 1) covers the rest: per-row / per-column kappa-folded
+// spacings, per-cell da/db, the non-periodic edge rules, and the CPML psi recursion (boundaries.py:27-37) whose state
+// flows through the stages like the fields.  Periodic wraps are modular indices; where open_sol evaluates the wrapped
+// neighbour as f * cos + f * sin with cos 1, sin 0 (a real-only engine) the same expression is evaluated, so even the
+// signs of zeros match.
+//
+// Sources and monitors.  Line sources are added after E and its CPML, per step, in add order, skipped when the step's
+// float32 value is 0 (core/sources.py:221-229).  On a DFT sample step the owning warp copies the flux line's E_z and
+// tangential H into a small staging buffer; a separate kernel accumulates the running DFTs in sample order
+// (monitors.py:45-46), so the complex128 sums are exactly the reference's.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define TB_MAX_LINES 16
+#define TB_MAX_MONS 8
+#define TB_MAX_RECTS 4
+#define TB_WARPS 4
+#define TB_MAX_T 4
+
+struct TBLine {
+    int32_t axis, position, lo, hi;   // axis 0: cells (i, position), i in [lo, hi); axis 1: cells (position, j)
+    const float *profile;
+};
+
+struct TBMon {
+    int32_t normal_axis, position, lo, hi;   // normal 0: cells (position, j); normal 1: cells (i, position)
+    float *stage;                            // (samples of the launch, 2, hi - lo): E_z then the tangential H
+};
+
+struct TBRect {
+    int32_t r0, r1, c0, c1;   // output rows [r0, r1), columns [c0, c1)
+    int32_t tiles_c, first_tile;
+};
+
+struct TBParams {
+    int32_t nx, ny, px, py, npml, cpml_mask;
+    const float *ez_in, *hx_in, *hy_in;
+    float *ez_out, *hx_out, *hy_out;
+    const float *cb, *ca, *da, *db;   // ca NULL: 1; da/db NULL: da_u / db_u
+    float da_u, db_u;
+    const float *inv_dx_e, *inv_dx_h, *inv_dy_e, *inv_dy_h;
+    float s_inv_dx_e, s_inv_dx_h, s_inv_dy_e, s_inv_dy_h;   // the bulk values (interior variant)
+    const float *cpml_rows[4];                              // b_e, a_e, inv_e, b_h, a_h, inv_h (npml each)
+    const float *psi_e_in[4], *psi_h_in[4];
+    float *psi_e_out[4], *psi_h_out[4];
+    int32_t n_lines;
+    TBLine lines[TB_MAX_LINES];
+    const float *line_values;   // (n_lines, values_stride)
+    int64_t values_stride;
+    int64_t k0;                 // column of this launch's first step in line_values
+    int32_t n_mons;
+    TBMon mons[TB_MAX_MONS];
+    int64_t n0;                 // engine steps taken before this launch
+    int64_t m;                  // DFT sample interval
+    int64_t q_first;            // sample number of staging slot 0
+    int32_t n_rects;
+    TBRect rects[TB_MAX_RECTS];
+    int32_t tile_w, tile_rows, n_tiles;
+};
+
+__device__ __forceinline__ int tb_wrap(int a, int n) {
+    int r = a % n;
+    return r < 0 ? r + n : r;
+}
+
+// open_sol's wrapped lo-side neighbour of a real-only engine: f * wrap_cos - f_partner * wrap_sin with cos 1, sin 0
+// and partner = f (fdtd_ez_2d_kernels.py:109-118).
+__device__ __forceinline__ float tb_lo_wrap(float f) {
+    const float one = 1.0f, zero = 0.0f;
+    return f * one - f * zero;
+}
+
+template <int T, int C, bool GEN>
+struct TBState {
+    float E[2][T + 1][C];
+    float Hx[2][T + 1][C];
+    float Hy[2][T + 1][C];
+    // CPML psi (general variant): x-side psi of H_y / E_z rows, y-side psi of H_x / E_z columns
+    float pxh[2][T + 1][GEN ? C : 1];
+    float pxe[2][T + 1][GEN ? C : 1];
+    float pyh[2][T + 1][GEN ? C : 1];
+    float pye[2][T + 1][GEN ? C : 1];
+};
+
+// Per-thread column facts.
+template <int C>
+struct TBCols {
+    int jp[C];          // physical column
+    bool in_grid[C];    // a real cell (false: outside a non-periodic grid)
+    bool own[C];        // inside this tile's output columns
+    float inv_y_h[C], inv_y_e[C];
+    // y-side CPML: side (2 / 3) and slab index of the H and E column, -1 when none
+    int yh_side[C], yh_k[C], ye_side[C], ye_k[C];
+};
+
+// Which x-side (rows) or y-side (columns) CPML slab holds H row / E row `g` along an axis of n cells, and its index.
+__device__ __forceinline__ void tb_cpml_slot(int g, int n, int npml, bool lo_on, bool hi_on, int lo_side, int hi_side,
+                                             int &h_side, int &h_k, int &e_side, int &e_k) {
+    h_side = e_side = -1;
+    h_k = e_k = 0;
+    if (lo_on && g >= 0 && g < npml) { h_side = lo_side; h_k = g; }
+    else if (hi_on && g >= n - npml - 1 && g <= n - 2) { h_side = hi_side; h_k = g - (n - npml - 1); }
+    if (lo_on && g >= 1 && g <= npml) { e_side = lo_side; e_k = g - 1; }
+    else if (hi_on && g >= n - npml - 1 && g <= n - 2) { e_side = hi_side; e_k = g - (n - npml - 1); }
+}
+
+template <int C>
+__device__ __forceinline__ void tb_load_row(const float *__restrict__ src, size_t row_base, const TBCols<C> &cols,
+                                            bool vec, float (&out)[C]) {
+    if (C == 4 && vec) {
+        if (cols.in_grid[0]) {
+            const float4 v = __ldg(reinterpret_cast<const float4 *>(src + row_base + cols.jp[0]));
+            out[0] = v.x;
+            out[1] = v.y;
+            out[2] = v.z;
+            out[3] = v.w;
+        } else {
+#pragma unroll
+            for (int c = 0; c < C; ++c) out[c] = 0.0f;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < C; ++c) out[c] = cols.in_grid[c] ? __ldg(src + row_base + cols.jp[c]) : 0.0f;
+    }
+}
+
+template <int T, int C, bool GEN, bool CA>
+struct TBWarp {
+    const TBParams &p;
+    TBCols<C> cols;
+    TBState<T, C, GEN> st;
+    int i0, i1, r_begin, r_end;
+    bool vec;
+
+    __device__ __forceinline__ TBWarp(const TBParams &params) : p(params) {}
+
+    __device__ __forceinline__ int phys_row(int i) const { return p.px ? tb_wrap(i, p.nx) : i; }
+
+    // Stage 0 of stream row r: fields (and psi^0 of CPML cells) from the input buffers.
+    template <int PH>
+    __device__ __forceinline__ void load_row(int r) {
+        const int rp = phys_row(r);
+        const size_t base = (size_t)rp * (size_t)p.ny;
+        tb_load_row<C>(p.ez_in, base, cols, vec, st.E[PH][0]);
+        tb_load_row<C>(p.hx_in, base, cols, vec, st.Hx[PH][0]);
+        tb_load_row<C>(p.hy_in, base, cols, vec, st.Hy[PH][0]);
+        if constexpr (GEN) {
+            int xh_side, xh_k, xe_side, xe_k;
+            tb_cpml_slot(rp, p.nx, p.npml, p.cpml_mask & 1, p.cpml_mask & 2, 0, 1, xh_side, xh_k, xe_side, xe_k);
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const bool g = cols.in_grid[c];
+                const int j = cols.jp[c];
+                st.pxh[PH][0][c] = (g && xh_side >= 0) ? p.psi_h_in[xh_side][(size_t)xh_k * p.ny + j] : 0.0f;
+                st.pxe[PH][0][c] = (g && xe_side >= 0) ? p.psi_e_in[xe_side][(size_t)xe_k * p.ny + j] : 0.0f;
+                st.pyh[PH][0][c] = (g && cols.yh_side[c] >= 0)
+                                       ? p.psi_h_in[cols.yh_side[c]][(size_t)rp * p.npml + cols.yh_k[c]] : 0.0f;
+                st.pye[PH][0][c] = (g && cols.ye_side[c] >= 0)
+                                       ? p.psi_e_in[cols.ye_side[c]][(size_t)rp * p.npml + cols.ye_k[c]] : 0.0f;
+            }
+        }
+    }
+
+    // Stage S of the iteration of stream row r: step S of row i = r - S.
+    template <int PH, int S>
+    __device__ __forceinline__ void stage(int r) {
+        constexpr int Q = PH ^ 1;   // last iteration's arrays
+        const int i = r - S;
+        if (i < r_begin || i > r_end) return;
+        const int ip = phys_row(i);
+        const int nx = p.nx, ny = p.ny;
+        const size_t base = (size_t)ip * (size_t)ny;
+
+        float cb[C], ca[C], da[C], db[C];
+        tb_load_row<C>(p.cb, base, cols, vec, cb);
+        if constexpr (CA) {
+            tb_load_row<C>(p.ca, base, cols, vec, ca);
+        }
+        if constexpr (GEN) {
+            if (p.da) {
+                tb_load_row<C>(p.da, base, cols, vec, da);
+                tb_load_row<C>(p.db, base, cols, vec, db);
+            } else {
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    da[c] = p.da_u;
+                    db[c] = p.db_u;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < C; ++c) db[c] = p.db_u;
+        }
+        float inv_x_h, inv_x_e;
+        int xh_side = -1, xh_k = 0, xe_side = -1, xe_k = 0;
+        if constexpr (GEN) {
+            inv_x_h = __ldg(p.inv_dx_h + ip);
+            inv_x_e = __ldg(p.inv_dx_e + ip);
+            tb_cpml_slot(ip, nx, p.npml, p.cpml_mask & 1, p.cpml_mask & 2, 0, 1, xh_side, xh_k, xe_side, xe_k);
+        } else {
+            inv_x_h = p.s_inv_dx_h;
+            inv_x_e = p.s_inv_dx_e;
+        }
+
+        // ---- H^S of row i (fdtd_ez_2d_kernels.py:41-47, then the H-row CPML, boundaries.py:752-755)
+        float hxn[C], hyn[C];
+        const float e_right_last = __shfl_down_sync(0xffffffffu, st.E[Q][S - 1][0], 1);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const float e = st.E[Q][S - 1][c];
+            const float e_right = c < C - 1 ? st.E[Q][S - 1][c + 1] : e_right_last;
+            const float e_up = st.E[PH][S - 1][c];
+            const float hx_old = st.Hx[Q][S - 1][c];
+            const float hy_old = st.Hy[Q][S - 1][c];
+            const int j = cols.jp[c];
+            // H_x: every column but the last of a non-periodic y axis (whose face is never updated)
+            if (GEN && !p.py && j == ny - 1) {
+                hxn[c] = hx_old;
+            } else {
+                float v;
+                if constexpr (GEN) {
+                    v = da[c] * hx_old - db[c] * (e_right - e) * cols.inv_y_h[c];
+                    if (cols.yh_side[c] >= 0) {
+                        const int sd = cols.yh_side[c], k = cols.yh_k[c];
+                        const float *rows = p.cpml_rows[sd];
+                        float q = st.pyh[Q][S - 1][c] * rows[3 * p.npml + k];
+                        q += rows[4 * p.npml + k] * (e_right - e) * rows[5 * p.npml + k];
+                        st.pyh[PH][S][c] = q;
+                        v += (-db[c]) * q;
+                    }
+                } else {
+                    v = hx_old - db[c] * (e_right - e) * p.s_inv_dy_h;
+                }
+                hxn[c] = v;
+            }
+            // H_y: every row but the last of a non-periodic x axis
+            if (GEN && !p.px && ip == nx - 1) {
+                hyn[c] = hy_old;
+            } else {
+                float v;
+                if constexpr (GEN) {
+                    v = da[c] * hy_old + db[c] * (e_up - e) * inv_x_h;
+                    if (xh_side >= 0) {
+                        const float *rows = p.cpml_rows[xh_side];
+                        float q = st.pxh[Q][S - 1][c] * rows[3 * p.npml + xh_k];
+                        q += rows[4 * p.npml + xh_k] * (e_up - e) * rows[5 * p.npml + xh_k];
+                        st.pxh[PH][S][c] = q;
+                        v += db[c] * q;
+                    }
+                } else {
+                    v = hy_old + db[c] * (e_up - e) * inv_x_h;
+                }
+                hyn[c] = v;
+            }
+        }
+
+        // ---- E^S of row i (fdtd_ez_2d_kernels.py:107-120), E-row CPML x then y sides, line sources
+        const float hx_left_first = __shfl_up_sync(0xffffffffu, hxn[C - 1], 1);
+        const int64_t step = p.n0 + S;   // engine step number after this stage
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const int j = cols.jp[c];
+            float hx_left = c > 0 ? hxn[c - 1] : hx_left_first;
+            float hy_down = st.Hy[Q][S][c];   // H_y^S of row i - 1
+            float curl;
+            if (GEN && !p.px && ip == 0) {
+                curl = hyn[c] * inv_x_e;
+            } else {
+                if (p.px && ip == 0) hy_down = tb_lo_wrap(hy_down);
+                curl = (hyn[c] - hy_down) * inv_x_e;
+            }
+            const float inv_y_e = GEN ? cols.inv_y_e[c] : p.s_inv_dy_e;
+            if (GEN && !p.py && j == 0) {
+                curl -= hxn[c] * inv_y_e;
+            } else {
+                if (p.py && j == 0) hx_left = tb_lo_wrap(hx_left);
+                curl -= (hxn[c] - hx_left) * inv_y_e;
+            }
+            const float e_old = st.E[Q][S - 1][c];
+            float v = (CA ? ca[c] * e_old : e_old) + cb[c] * curl;
+            if constexpr (GEN) {
+                if (xe_side >= 0) {
+                    const float *rows = p.cpml_rows[xe_side];
+                    float q = st.pxe[Q][S - 1][c] * rows[xe_k];
+                    q += rows[p.npml + xe_k] * (hyn[c] - hy_down) * rows[2 * p.npml + xe_k];
+                    st.pxe[PH][S][c] = q;
+                    v += cb[c] * q;
+                }
+                if (cols.ye_side[c] >= 0) {
+                    const int sd = cols.ye_side[c], k = cols.ye_k[c];
+                    const float *rows = p.cpml_rows[sd];
+                    float q = st.pye[Q][S - 1][c] * rows[k];
+                    q += rows[p.npml + k] * (hxn[c] - hx_left) * rows[2 * p.npml + k];
+                    st.pye[PH][S][c] = q;
+                    v += (-cb[c]) * q;
+                }
+            }
+            for (int l = 0; l < p.n_lines; ++l) {
+                const TBLine &L = p.lines[l];
+                const int along = L.axis == 0 ? ip : j, across = L.axis == 0 ? j : ip;
+                if (across == L.position && along >= L.lo && along < L.hi && cols.in_grid[c]) {
+                    const float value = p.line_values[(size_t)l * p.values_stride + p.k0 + (S - 1)];
+                    if (value != 0.0f) v += value * L.profile[along - L.lo];
+                }
+            }
+            st.E[PH][S][c] = v;
+            st.Hx[PH][S][c] = hxn[c];
+            st.Hy[PH][S][c] = hyn[c];
+        }
+
+        // ---- DFT sample: the owner copies the flux lines' E_z and tangential H of this step
+        if (p.n_mons && step % p.m == 0 && i >= i0 && i < i1) {
+            const int64_t slot = step / p.m - p.q_first;
+            for (int mi = 0; mi < p.n_mons; ++mi) {
+                const TBMon &M = p.mons[mi];
+                const int n = M.hi - M.lo;
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    if (!cols.own[c]) continue;
+                    const int j = cols.jp[c];
+                    if (M.normal_axis == 0) {
+                        if (ip == M.position && j >= M.lo && j < M.hi) {
+                            M.stage[(slot * 2) * n + (j - M.lo)] = st.E[PH][S][c];
+                            M.stage[(slot * 2 + 1) * n + (j - M.lo)] = hyn[c];
+                        }
+                    } else if (j == M.position && ip >= M.lo && ip < M.hi) {
+                        M.stage[(slot * 2) * n + (ip - M.lo)] = st.E[PH][S][c];
+                        M.stage[(slot * 2 + 1) * n + (ip - M.lo)] = hxn[c];
+                    }
+                }
+            }
+        }
+    }
+
+    // Outputs of stage T (row r - T) into the output buffers.
+    template <int PH>
+    __device__ __forceinline__ void store(int r) {
+        const int i = r - T;
+        if (i < i0 || i >= i1) return;
+        const int ip = phys_row(i);
+        const size_t base = (size_t)ip * (size_t)p.ny;
+        bool all_own = true;
+#pragma unroll
+        for (int c = 0; c < C; ++c) all_own = all_own && cols.own[c];
+        if (C == 4 && vec && all_own) {
+            *reinterpret_cast<float4 *>(p.ez_out + base + cols.jp[0]) =
+                make_float4(st.E[PH][T][0], st.E[PH][T][1], st.E[PH][T][2], st.E[PH][T][3]);
+            *reinterpret_cast<float4 *>(p.hx_out + base + cols.jp[0]) =
+                make_float4(st.Hx[PH][T][0], st.Hx[PH][T][1], st.Hx[PH][T][2], st.Hx[PH][T][3]);
+            *reinterpret_cast<float4 *>(p.hy_out + base + cols.jp[0]) =
+                make_float4(st.Hy[PH][T][0], st.Hy[PH][T][1], st.Hy[PH][T][2], st.Hy[PH][T][3]);
+        } else {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                if (!cols.own[c]) continue;
+                p.ez_out[base + cols.jp[c]] = st.E[PH][T][c];
+                p.hx_out[base + cols.jp[c]] = st.Hx[PH][T][c];
+                p.hy_out[base + cols.jp[c]] = st.Hy[PH][T][c];
+            }
+        }
+        if constexpr (GEN) {
+            int xh_side, xh_k, xe_side, xe_k;
+            tb_cpml_slot(ip, p.nx, p.npml, p.cpml_mask & 1, p.cpml_mask & 2, 0, 1, xh_side, xh_k, xe_side, xe_k);
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                if (!cols.own[c]) continue;
+                const int j = cols.jp[c];
+                if (xh_side >= 0) p.psi_h_out[xh_side][(size_t)xh_k * p.ny + j] = st.pxh[PH][T][c];
+                if (xe_side >= 0) p.psi_e_out[xe_side][(size_t)xe_k * p.ny + j] = st.pxe[PH][T][c];
+                if (cols.yh_side[c] >= 0)
+                    p.psi_h_out[cols.yh_side[c]][(size_t)ip * p.npml + cols.yh_k[c]] = st.pyh[PH][T][c];
+                if (cols.ye_side[c] >= 0)
+                    p.psi_e_out[cols.ye_side[c]][(size_t)ip * p.npml + cols.ye_k[c]] = st.pye[PH][T][c];
+            }
+        }
+    }
+
+    template <int PH, int S>
+    __device__ __forceinline__ void stages_from(int r) {
+        if constexpr (S <= T) {
+            stage<PH, S>(r);
+            if constexpr (S == 1) {
+                // stage 1 was the last reader of last iteration's stage-0 row: prefetch row r + 1 into it
+                if (r + 1 <= r_end) load_row<PH ^ 1>(r + 1);
+            }
+            stages_from<PH, S + 1>(r);
+        }
+    }
+
+    template <int PH>
+    __device__ __forceinline__ void iteration(int r) {
+        stages_from<PH, 1>(r);
+        store<PH>(r);
+    }
+};
+
+template <int T, int C, bool GEN, bool CA>
+__global__ void __launch_bounds__(TB_WARPS * 32) ez2d_tb_kernel(const TBParams p) {
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x * TB_WARPS + (threadIdx.x >> 5);
+    if (w >= p.n_tiles) return;   // whole warps leave together (the shuffles below need all 32 lanes)
+    int rect = 0;
+    for (int q = 1; q < p.n_rects; ++q)
+        if (w >= p.rects[q].first_tile) rect = q;
+    const TBRect R = p.rects[rect];
+    const int t = w - R.first_tile;
+    const int tc = t % R.tiles_c, tr = t / R.tiles_c;
+    const int j0 = R.c0 + tc * p.tile_w, j1 = min(j0 + p.tile_w, R.c1);
+
+    TBWarp<T, C, GEN, CA> W(p);
+    W.i0 = R.r0 + tr * p.tile_rows;
+    W.i1 = min(W.i0 + p.tile_rows, R.r1);
+    W.r_begin = p.px ? W.i0 - T : max(0, W.i0 - T);
+    W.r_end = p.px ? W.i1 - 1 + T : min(p.nx - 1, W.i1 - 1 + T);
+    W.vec = (C == 4) && (p.ny % 4 == 0);
+    constexpr int HL = C == 1 ? T : 4;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        const int jl = j0 - HL + lane * C + c;
+        W.cols.in_grid[c] = p.py || (jl >= 0 && jl < p.ny);
+        W.cols.jp[c] = p.py ? tb_wrap(jl, p.ny) : jl;
+        W.cols.own[c] = jl >= j0 && jl < j1;
+        const int jc = W.cols.in_grid[c] ? W.cols.jp[c] : 0;
+        if (GEN) {
+            W.cols.inv_y_h[c] = __ldg(p.inv_dy_h + jc);
+            W.cols.inv_y_e[c] = __ldg(p.inv_dy_e + jc);
+            tb_cpml_slot(W.cols.in_grid[c] ? jc : -1, p.ny, p.npml, p.cpml_mask & 4, p.cpml_mask & 8, 2, 3,
+                         W.cols.yh_side[c], W.cols.yh_k[c], W.cols.ye_side[c], W.cols.ye_k[c]);
+        } else {
+            W.cols.inv_y_h[c] = W.cols.inv_y_e[c] = 0.0f;
+            W.cols.yh_side[c] = W.cols.ye_side[c] = -1;
+            W.cols.yh_k[c] = W.cols.ye_k[c] = 0;
+        }
+    }
+    // Pipeline registers start at 0 (a non-periodic first row reads no H_y below it; the rest is outside the cone).
+#pragma unroll
+    for (int ph = 0; ph < 2; ++ph)
+#pragma unroll
+        for (int s = 0; s <= T; ++s)
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                W.st.E[ph][s][c] = W.st.Hx[ph][s][c] = W.st.Hy[ph][s][c] = 0.0f;
+                if (GEN) W.st.pxh[ph][s][c] = W.st.pxe[ph][s][c] = W.st.pyh[ph][s][c] = W.st.pye[ph][s][c] = 0.0f;
+            }
+    W.template load_row<0>(W.r_begin);
+    const int r_last = W.r_end + T;
+    for (int r = W.r_begin; r <= r_last; r += 2) {
+        W.template iteration<0>(r);
+        if (r + 1 <= r_last) W.template iteration<1>(r + 1);
+    }
+}
+
+// Running DFTs of one flux line from the staged samples of one launch, in sample order (monitors.py:45-46,84-90).
+__global__ void ez2d_flux_staged_kernel(const float *__restrict__ stage, int n, int nf, int n_q,
+                                        const float *__restrict__ phases, double *__restrict__ e_acc,
+                                        double *__restrict__ h_acc) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * nf) return;
+    const int f = t / n, c = t - f * n;
+    const size_t a = ((size_t)f * n + c) * 2;
+    double er = e_acc[a], ei = e_acc[a + 1], hr = h_acc[a], hi = h_acc[a + 1];
+    for (int q = 0; q < n_q; ++q) {
+        const double pr = (double)phases[((size_t)q * nf + f) * 2], pi = (double)phases[((size_t)q * nf + f) * 2 + 1];
+        const double e = (double)stage[((size_t)q * 2) * n + c], hv = (double)stage[((size_t)q * 2 + 1) * n + c];
+        er += pr * e;
+        ei += pi * e;
+        hr += pr * hv;
+        hi += pi * hv;
+    }
+    e_acc[a] = er;
+    e_acc[a + 1] = ei;
+    h_acc[a] = hr;
+    h_acc[a + 1] = hi;
+}

@@ -22,9 +22,8 @@ class FDTDEngine2D_Ez:
     """Device engine of one 2D E_z simulation (real fields, CPML and periodic faces)."""
 
     polarization = 'ez'
-    kernel_name = 'ez2d_h_kernel+ez2d_e_kernel'   # the field kernels of one step
-    kernels_per_step = 2
-    steps_per_launch = 1
+    KERNEL_KINDS = {0: 'ez2d_tb_kernel (interior)', 1: 'ez2d_tb_kernel (general)', 2: 'ez2d_flux_staged_kernel',
+                    3: 'ez2d_h_kernel+ez2d_e_kernel'}
 
     def __init__(self, domain, boundary_config, device: int = 0):
         boundary_config.require_supported('FDTDEngine2D_Ez')
@@ -48,6 +47,8 @@ class FDTDEngine2D_Ez:
         self._materials_version = None
         self.sample_interval = 1
         self._sample_interval_sent = None
+        self.variant, self.steps_per_launch, self.tile_rows = 1, 4, 128
+        self._config_sent = None
         self.h2d_bytes = 0   # host-to-device bytes this engine has uploaded (setup, materials, chunk tables)
 
     # ------------------------------------------------------------------------------------------- native handle
@@ -130,6 +131,50 @@ class FDTDEngine2D_Ez:
         if self._sample_interval_sent != self.sample_interval:
             _native.check(lib.os_fdtd2d_set_sample_interval(h, self.sample_interval))
             self._sample_interval_sent = self.sample_interval
+        config = (self.variant, self.steps_per_launch, self.tile_rows)
+        if self._config_sent != config:
+            _native.check(lib.os_fdtd2d_configure(h, *config))
+            self._config_sent = config
+
+    def configure(self, variant=None, steps_per_launch=None, tile_rows=None):
+        """Kernel choice (results are bit-identical for every choice): variant 1 = temporally blocked kernels
+        advancing steps_per_launch (1..4) steps per launch with tile_rows rows per interior tile; variant 0 = one H
+        and one E kernel per step."""
+        if variant is not None:
+            self.variant = int(variant)
+        if steps_per_launch is not None:
+            self.steps_per_launch = int(steps_per_launch)
+        if tile_rows is not None:
+            self.tile_rows = int(tile_rows)
+        if self._handle is not None:
+            self.sync_device()
+
+    def launch_count(self):
+        """Kernels the last advance launched."""
+        n = ctypes.c_int64()
+        _native.check(_native.load().os_fdtd2d_launch_count(self.handle, ctypes.byref(n)))
+        return int(n.value)
+
+    def plan_info(self, steps_per_launch=None):
+        """(interior cells, interior tiles, general tiles) of the blocked kernels' plan."""
+        T = self.steps_per_launch if steps_per_launch is None else int(steps_per_launch)
+        a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _native.check(_native.load().os_fdtd2d_plan_info(self.handle, T, ctypes.byref(a), ctypes.byref(b),
+                                                         ctypes.byref(c)))
+        return int(a.value), int(b.value), int(c.value)
+
+    def set_profiling(self, on):
+        _native.check(_native.load().os_fdtd2d_set_profiling(self.handle, int(bool(on))))
+
+    def kernel_times(self):
+        """{kernel kind name: (total device ms, launches)} of the last advance (profiling on)."""
+        out = {}
+        for kind, name in self.KERNEL_KINDS.items():
+            ms, n = ctypes.c_double(), ctypes.c_int64()
+            _native.check(_native.load().os_fdtd2d_kernel_times(self.handle, kind, ctypes.byref(ms), ctypes.byref(n)))
+            if n.value:
+                out[name] = (float(ms.value), int(n.value))
+        return out
 
     # ------------------------------------------------------------------------------------------- stepping
     def chunk_tables(self, n_steps):

@@ -72,6 +72,48 @@ def test_cases_bit_exact_against_oracle(spec):
         np.testing.assert_array_equal(h, omon.h_acc)
 
 
+# (variant, steps per launch, interior tile rows): per-step kernels, and the blocked kernels at every T with tile
+# heights from a few rows (many ragged tiles, tiles shorter than T) to 128
+KERNEL_CONFIGS = [(0, 1, 128), (1, 1, 128), (1, 2, 32), (1, 3, 7), (1, 4, 128), (1, 4, 3)]
+
+
+@pytest.mark.parametrize('config', KERNEL_CONFIGS, ids=[f'v{v}_T{t}_rows{r}' for v, t, r in KERNEL_CONFIGS])
+@pytest.mark.parametrize('spec', CASES, ids=[c['name'] for c in CASES])
+def test_kernel_configs_bit_exact(spec, config):
+    """Every kernel variant and launch shape gives open_sol's fields and spectra bit for bit."""
+    g = np.load(os.path.join(GOLDEN, f"{spec['name']}.npz"))
+    sim = ob.Simulation(**spec['sim'], verbose=False)
+    sim.em.engine.configure(*config)
+    mons = apply_ops(sim, spec)
+    done = 0
+    for cp in spec['checkpoints']:
+        sim.run(n_steps=cp - done, verbose=False)
+        done = cp
+        for name, arr in _fields(sim).items():
+            assert _digest(arr) == str(g[f'sha_{name}_{cp}']), f'{name} differs from open_sol at step {cp}'
+        for k, mon in enumerate(mons):
+            e, h = mon.spectra()
+            np.testing.assert_array_equal(e, g[f'spec_e{k}_{cp}'])
+            np.testing.assert_array_equal(h, g[f'spec_h{k}_{cp}'])
+
+
+def test_interior_and_general_kernels_both_run():
+    """The headline grid uses both blocked kernels: the interior kernel holds nearly all cells."""
+    args = workloads.roofline_2d_sim_args()
+    sim = ob.Simulation(**args, verbose=False)
+    workloads.apply(sim, workloads.roofline_2d_ops())
+    sim.em.finalize()
+    cells, tiles_in, tiles_gen = sim.em.engine.plan_info(4)
+    assert tiles_in > 0 and tiles_gen > 0
+    assert cells > 0.98 * sim.grid.nx * sim.grid.ny
+    sim.em.engine.set_profiling(True)
+    sim.run(n_steps=52, verbose=False)
+    times = sim.em.engine.kernel_times()
+    assert times['ez2d_tb_kernel (interior)'][1] == 13 and times['ez2d_tb_kernel (general)'][1] == 13
+    assert times['ez2d_flux_staged_kernel'][1] == 2 * 4
+    sim.clear()
+
+
 def _random_spec(seed):
     rng = np.random.default_rng(seed)
     dx = float(rng.choice([15e-9, 20e-9, 25e-9]))
@@ -212,7 +254,10 @@ def test_roofline_workload_full_size_bit_exact():
 
 def test_roofline_workload_linearity():
     """Size-independent property at full size: the update is linear, so doubling the source amplitude doubles every
-    field value exactly (a power-of-two scale commutes with float rounding) and scales every flux by exactly 4."""
+    field and quadruples every flux.  Not bit for bit: a power-of-two scale commutes with rounding only for normal
+    numbers, and the leading edge of the pulse passes through subnormal values (~1e-38) whose rounding seeds ulp-level
+    differences; the bar is float32 rounding (LINEARITY_RTOL of the largest value)."""
+    LINEARITY_RTOL = 1e-5
     args = workloads.roofline_2d_sim_args()
     out = []
     for amplitude in (1.0, 2.0):
@@ -221,7 +266,25 @@ def test_roofline_workload_linearity():
         sim.run(n_steps=600, verbose=False)
         out.append((sim.em.engine.read_field('ez'), [m.flux() for m in mons]))
         sim.clear()
-    assert np.abs(out[0][0]).max() > 0
-    np.testing.assert_array_equal(out[1][0], 2.0 * out[0][0])
+    scale = np.abs(out[1][0]).max()
+    assert scale > 0
+    assert np.abs(out[1][0] - 2.0 * out[0][0]).max() <= LINEARITY_RTOL * scale
+    flux_scale = max(float(np.abs(f).max()) for f in out[1][1])
     for f1, f2 in zip(out[0][1], out[1][1]):
-        np.testing.assert_array_equal(f2, 4.0 * f1)
+        assert np.abs(f2 - 4.0 * f1).max() <= LINEARITY_RTOL * flux_scale
+
+
+def test_roofline_workload_deterministic():
+    """Two runs of the full-size workload give bit-identical fields and fluxes (no races, no atomics order)."""
+    args = workloads.roofline_2d_sim_args()
+    out = []
+    for _ in range(2):
+        sim = ob.Simulation(**args, verbose=False)
+        mons = workloads.apply(sim, workloads.roofline_2d_ops())
+        sim.run(n_steps=400, verbose=False)
+        out.append((sim.em.engine.read_field('ez'), sim.em.engine.read_field('hy'), [m.flux() for m in mons]))
+        sim.clear()
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    for f1, f2 in zip(out[0][2], out[1][2]):
+        np.testing.assert_array_equal(f1, f2)
