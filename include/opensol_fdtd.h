@@ -125,6 +125,13 @@ int os_fdtd2d_launch_count(OsFdtd2D *h, int64_t *launches);
  * blocked kernel, 2 DFT kernel, 3 per-step kernel pair).  No open_sol counterpart. */
 int os_fdtd2d_set_profiling(OsFdtd2D *h, int32_t on);
 
+/* Autotuner of the interior tile height: times `repeats` launches of steps_per_launch steps for every candidate
+ * rows-per-tile on the live fields (trial launches write the idle buffer set, which is not swapped in, so the
+ * simulation state is unchanged), keeps the fastest as the engine's tile_rows and returns it with its time per
+ * launch.  No open_sol counterpart. */
+int os_fdtd2d_autotune(OsFdtd2D *h, int32_t steps_per_launch, const int32_t *candidates, int32_t n_candidates,
+                       int32_t repeats, int32_t *best_rows, float *best_ms);
+
 /* The blocked kernels' plan for steps_per_launch: cells of the interior rectangle and tiles (warps) of the interior
  * and general kernels.  No open_sol counterpart. */
 int os_fdtd2d_plan_info(OsFdtd2D *h, int32_t steps_per_launch, int64_t *interior_cells, int64_t *interior_tiles,

@@ -56,6 +56,8 @@ SIGNATURES = {
     'os_fdtd2d_configure': [_P, _I32, _I32, _I32],
     'os_fdtd2d_launch_count': [_P, ctypes.POINTER(_I64)],
     'os_fdtd2d_set_profiling': [_P, _I32],
+    'os_fdtd2d_autotune': [_P, _I32, ctypes.POINTER(_I32), _I32, _I32, ctypes.POINTER(_I32),
+                           ctypes.POINTER(ctypes.c_float)],
     'os_fdtd2d_plan_info': [_P, _I32, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
     'os_fdtd2d_kernel_times': [_P, _I32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_I64)],
     'os_fdtd2d_read_flux_spectra': [_P, _I32, _D, _D],

@@ -37,6 +37,8 @@ struct OsFdtd2D {
     OsGrid2D grid{};
     cudaStream_t stream = nullptr;        // the stream every call enqueues on
     cudaStream_t own_stream = nullptr;    // created with the handle, destroyed with it
+    cudaStream_t side_stream = nullptr;   // the border kernel runs here, overlapping the interior kernel
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     bool timed = false;
     os::DeviceArray<float> ez[2], hx[2], hy[2];   // double-buffered fields; `cur` is the live set
@@ -52,7 +54,7 @@ struct OsFdtd2D {
     int32_t variant = 1;                  // 0: per-half-step kernels, 1: temporally blocked
     int32_t steps_per_launch = 4;         // T of the blocked kernels
     int32_t tile_rows = 128;              // rows per interior tile
-    int32_t gen_tile_rows = 64;           // rows per general tile
+    int32_t gen_tile_rows = 16;           // rows per general tile
     int64_t launches = 0;                 // kernels launched by the last advance
     bool profiling = false;               // bracket every kernel with events (os_fdtd2d_kernel_times)
     std::vector<cudaEvent_t> prof_events; // pool, grown on demand
@@ -171,6 +173,9 @@ extern "C" int os_fdtd2d_create(const OsGrid2D *grid, OsFdtd2D **out) {
     h->device = g.device;
     OS_TRY(bind_device(h.get()));
     OS_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    OS_CUDA(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
+    OS_CUDA(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+    OS_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
     h->stream = h->own_stream;
     OS_CUDA(cudaEventCreate(&h->ev_start));
     OS_CUDA(cudaEventCreate(&h->ev_stop));
@@ -203,9 +208,13 @@ extern "C" int os_fdtd2d_destroy(OsFdtd2D *h) {
     if (h->ev_start) cudaEventDestroy(h->ev_start);
     if (h->ev_stop) cudaEventDestroy(h->ev_stop);
     if (h->own_stream) cudaStreamSynchronize(h->own_stream);
-    cudaStream_t stream = h->own_stream;
+    if (h->side_stream) cudaStreamSynchronize(h->side_stream);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    cudaStream_t stream = h->own_stream, side = h->side_stream;
     delete h;   // frees the device arrays
     if (stream) cudaStreamDestroy(stream);
+    if (side) cudaStreamDestroy(side);
     return OS_OK;
 }
 
@@ -390,7 +399,7 @@ extern "C" int os_fdtd2d_set_sample_interval(OsFdtd2D *h, int64_t sample_interva
 namespace os {
 
 // Event pair around one kernel launch when profiling (kind: 0 interior, 1 general, 2 DFT, 3 per-step kernels).
-static int prof_begin(OsFdtd2D *h, int kind) {
+static int prof_begin(OsFdtd2D *h, int kind, cudaStream_t stream) {
     if (!h->profiling) return OS_OK;
     while (h->prof_events.size() < 2 * (h->prof_used + 1)) {
         cudaEvent_t e;
@@ -399,13 +408,13 @@ static int prof_begin(OsFdtd2D *h, int kind) {
     }
     if (h->prof_kind.size() < h->prof_used + 1) h->prof_kind.resize(h->prof_used + 1);
     h->prof_kind[h->prof_used] = kind;
-    OS_CUDA(cudaEventRecord(h->prof_events[2 * h->prof_used], h->stream));
+    OS_CUDA(cudaEventRecord(h->prof_events[2 * h->prof_used], stream));
     return OS_OK;
 }
 
-static int prof_end(OsFdtd2D *h) {
+static int prof_end(OsFdtd2D *h, cudaStream_t stream) {
     if (!h->profiling) return OS_OK;
-    OS_CUDA(cudaEventRecord(h->prof_events[2 * h->prof_used + 1], h->stream));
+    OS_CUDA(cudaEventRecord(h->prof_events[2 * h->prof_used + 1], stream));
     h->prof_used += 1;
     return OS_OK;
 }
@@ -461,10 +470,11 @@ static void plan_tiles(const OsFdtd2D *h, int T, TBParams &interior, TBParams &g
         in.c1 = cy ? g.ny - npml - 1 - T : 0;
     }
     has_interior = in.r1 > in.r0 && in.c1 > in.c0 && g.ny % 4 == 0 && !h->has_dadb && h->da_uniform == 1.0f;
-    // uniform curl spacings over the interior cone
+    // uniform curl spacings over the interior's dependency cone (rows [r0 - T, r1 + T), columns [c0 - 4, c1 + T));
+    // the columns a tile loads beyond its cone feed no output and may be anything
     if (has_interior) {
         const int ra = g.periodic_x ? 0 : in.r0 - T, rb = g.periodic_x ? g.nx : in.r1 + T;
-        const int ca = g.periodic_y ? 0 : in.c0 - 4, cbnd = g.periodic_y ? g.ny : std::min(g.ny, in.c1 + 124);
+        const int ca = g.periodic_y ? 0 : in.c0 - 4, cbnd = g.periodic_y ? g.ny : in.c1 + T;
         has_interior = constant_over(h->host_inv[0], ra, rb, &interior.s_inv_dx_e) &&
                        constant_over(h->host_inv[1], ra, rb, &interior.s_inv_dx_h) &&
                        constant_over(h->host_inv[2], ca, cbnd, &interior.s_inv_dy_e) &&
@@ -523,27 +533,65 @@ static void fill_common(const OsFdtd2D *h, TBParams &q) {
     q.m = h->sample_interval;
 }
 
+// One blocked launch: the border (general) kernel forks onto the side stream and overlaps the interior kernel; both
+// read the same input buffers and write disjoint cells of the output buffers, and the main stream waits for both.
 template <int T>
 static int launch_tb(OsFdtd2D *h, const TBParams &interior, const TBParams &general, bool has_interior) {
     const dim3 threads(TB_WARPS * 32);
-    if (has_interior && interior.n_tiles) {
-        const dim3 blocks((unsigned)((interior.n_tiles + TB_WARPS - 1) / TB_WARPS));
-        OS_TRY(prof_begin(h, 0));
-        if (h->has_ca) ez2d_tb_kernel<T, 4, false, true><<<blocks, threads, 0, h->stream>>>(interior);
-        else ez2d_tb_kernel<T, 4, false, false><<<blocks, threads, 0, h->stream>>>(interior);
-        OS_TRY(prof_end(h));
-        h->launches += 1;
+    const bool run_interior = has_interior && interior.n_tiles;
+    const bool fork = run_interior && general.n_tiles;
+    cudaStream_t gstream = fork ? h->side_stream : h->stream;
+    if (fork) {
+        OS_CUDA(cudaEventRecord(h->ev_fork, h->stream));
+        OS_CUDA(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
     }
     if (general.n_tiles) {
         const dim3 blocks((unsigned)((general.n_tiles + TB_WARPS - 1) / TB_WARPS));
-        OS_TRY(prof_begin(h, 1));
-        if (h->has_ca) ez2d_tb_kernel<T, 1, true, true><<<blocks, threads, 0, h->stream>>>(general);
-        else ez2d_tb_kernel<T, 1, true, false><<<blocks, threads, 0, h->stream>>>(general);
-        OS_TRY(prof_end(h));
+        OS_TRY(prof_begin(h, 1, gstream));
+        if (h->has_ca) ez2d_tb_kernel<T, 1, true, true><<<blocks, threads, 0, gstream>>>(general);
+        else ez2d_tb_kernel<T, 1, true, false><<<blocks, threads, 0, gstream>>>(general);
+        OS_TRY(prof_end(h, gstream));
         h->launches += 1;
+    }
+    if (run_interior) {
+        const dim3 blocks((unsigned)((interior.n_tiles + TB_WARPS - 1) / TB_WARPS));
+        OS_TRY(prof_begin(h, 0, h->stream));
+        if (h->has_ca) ez2d_tb_kernel<T, 4, false, true><<<blocks, threads, 0, h->stream>>>(interior);
+        else ez2d_tb_kernel<T, 4, false, false><<<blocks, threads, 0, h->stream>>>(interior);
+        OS_TRY(prof_end(h, h->stream));
+        h->launches += 1;
+    }
+    if (fork) {
+        OS_CUDA(cudaEventRecord(h->ev_join, h->side_stream));
+        OS_CUDA(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
     }
     OS_CUDA(cudaGetLastError());
     return OS_OK;
+}
+
+static int launch_tb_any(OsFdtd2D *h, int T, const TBParams &interior, const TBParams &general, bool has_interior) {
+    switch (T) {
+        case 1: return launch_tb<1>(h, interior, general, has_interior);
+        case 2: return launch_tb<2>(h, interior, general, has_interior);
+        case 3: return launch_tb<3>(h, interior, general, has_interior);
+        default: return launch_tb<4>(h, interior, general, has_interior);
+    }
+}
+
+// Input / output buffer sets of one launch from buffer `in` to buffer `out`.
+static void bind_buffers(OsFdtd2D *h, TBParams &q, int in, int out) {
+    q.ez_in = h->ez[in].ptr;
+    q.hx_in = h->hx[in].ptr;
+    q.hy_in = h->hy[in].ptr;
+    q.ez_out = h->ez[out].ptr;
+    q.hx_out = h->hx[out].ptr;
+    q.hy_out = h->hy[out].ptr;
+    for (int s = 0; s < 4; ++s) {
+        q.psi_e_in[s] = h->psi_e[in][s].ptr;
+        q.psi_h_in[s] = h->psi_h[in][s].ptr;
+        q.psi_e_out[s] = h->psi_e[out][s].ptr;
+        q.psi_h_out[s] = h->psi_h[out][s].ptr;
+    }
 }
 
 // Temporally blocked chunk: launches of T steps (a shorter last one), buffers swapped after each.
@@ -559,31 +607,17 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
         fill_common(h, general);
         const int in = h->cur, out = h->cur ^ 1;
         for (TBParams *q : {&interior, &general}) {
-            q->ez_in = h->ez[in].ptr;
-            q->hx_in = h->hx[in].ptr;
-            q->hy_in = h->hy[in].ptr;
-            q->ez_out = h->ez[out].ptr;
-            q->hx_out = h->hx[out].ptr;
-            q->hy_out = h->hy[out].ptr;
-            for (int s = 0; s < 4; ++s) {
-                q->psi_e_in[s] = h->psi_e[in][s].ptr;
-                q->psi_h_in[s] = h->psi_h[in][s].ptr;
-                q->psi_e_out[s] = h->psi_e[out][s].ptr;
-                q->psi_h_out[s] = h->psi_h[out][s].ptr;
-            }
+            bind_buffers(h, *q, in, out);
             q->values_stride = n_steps;
             q->k0 = k;
             q->n0 = h->n_step;
             q->q_first = h->n_step / m + 1;
+            q->sample_mask = 0;
+            for (int st = 1; st <= T; ++st)
+                if ((h->n_step + st) % m == 0) q->sample_mask |= 1u << (st - 1);
+            if (h->fluxes.empty()) q->sample_mask = 0;
         }
-        int rc = OS_OK;
-        switch (T) {
-            case 1: rc = launch_tb<1>(h, interior, general, has_interior); break;
-            case 2: rc = launch_tb<2>(h, interior, general, has_interior); break;
-            case 3: rc = launch_tb<3>(h, interior, general, has_interior); break;
-            default: rc = launch_tb<4>(h, interior, general, has_interior); break;
-        }
-        if (rc != OS_OK) return rc;
+        OS_TRY(launch_tb_any(h, T, interior, general, has_interior));
         h->cur = out;
         // DFT samples taken inside this launch, accumulated in sample order
         const int64_t q_lo = h->n_step / m + 1, q_hi = (h->n_step + T) / m;
@@ -593,10 +627,10 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
                 const float *ph = h->phases.ptr + offset + (size_t)(q_lo - first_sample) * f->nf * 2;
                 const int n = f->hi - f->lo;
                 const int total = n * f->nf;
-                OS_TRY(prof_begin(h, 2));
+                OS_TRY(prof_begin(h, 2, h->stream));
                 ez2d_flux_staged_kernel<<<(total + 255) / 256, 256, 0, h->stream>>>(
                     f->stage.ptr, n, f->nf, (int)(q_hi - q_lo + 1), ph, f->e_acc.ptr, f->h_acc.ptr);
-                OS_TRY(prof_end(h));
+                OS_TRY(prof_end(h, h->stream));
                 h->launches += 1;
                 offset += (size_t)n_samples * f->nf * 2;
             }
@@ -615,10 +649,10 @@ static int advance_per_step(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, 
     const dim3 block(EZ2D_BLOCK_X, EZ2D_BLOCK_Y);
     const dim3 grid((unsigned)((h->grid.ny + block.x - 1) / block.x), (unsigned)((h->grid.nx + block.y - 1) / block.y));
     for (int64_t k = 0; k < n_steps; ++k) {
-        OS_TRY(prof_begin(h, 3));
+        OS_TRY(prof_begin(h, 3, h->stream));
         ez2d_h_kernel<<<grid, block, 0, h->stream>>>(p);
         ez2d_e_kernel<<<grid, block, 0, h->stream>>>(p, h->line_values.ptr, n_steps, k);
-        OS_TRY(prof_end(h));
+        OS_TRY(prof_end(h, h->stream));
         h->launches += 2;
         h->n_step += 1;
         if (!h->fluxes.empty() && h->n_step % m == 0) {
@@ -688,6 +722,65 @@ extern "C" int os_fdtd2d_configure(OsFdtd2D *h, int32_t variant, int32_t steps_p
     return OS_OK;
 }
 
+extern "C" int os_fdtd2d_autotune(OsFdtd2D *h, int32_t steps_per_launch, const int32_t *candidates,
+                                  int32_t n_candidates, int32_t repeats, int32_t *best_rows, float *best_ms) {
+    OS_CHECK(h && candidates && n_candidates > 0 && best_rows && best_ms, OS_ERR_INVALID,
+             "os_fdtd2d_autotune: null argument or no candidates");
+    OS_CHECK(steps_per_launch >= 1 && steps_per_launch <= TB_MAX_T, OS_ERR_INVALID,
+             "steps_per_launch must be in [1, %d]", TB_MAX_T);
+    OS_CHECK(h->has_cb && h->has_spacings, OS_ERR_STATE, "os_fdtd2d_autotune: coefficients and spacings must be set");
+    OS_TRY(bind_device(h));
+    const int saved_rows = h->tile_rows;
+    const bool saved_prof = h->profiling;
+    h->profiling = false;
+    cudaEvent_t t0, t1;
+    OS_CUDA(cudaEventCreate(&t0));
+    OS_CUDA(cudaEventCreate(&t1));
+    float best = -1.0f;
+    int best_r = saved_rows;
+    int rc = OS_OK;
+    for (int c = 0; c < n_candidates && rc == OS_OK; ++c) {
+        if (candidates[c] < 1) continue;
+        h->tile_rows = candidates[c];
+        TBParams interior{}, general{};
+        bool has_interior = false;
+        plan_tiles(h, steps_per_launch, interior, general, has_interior);
+        for (TBParams *q : {&interior, &general}) {
+            fill_common(h, *q);
+            q->n_lines = 0;       // sources and monitors do not change the timing of a trial launch
+            q->n_mons = 0;
+            q->sample_mask = 0;
+            // trial launches read the live buffers and write the idle ones, which are never swapped in
+            bind_buffers(h, *q, h->cur, h->cur ^ 1);
+        }
+        for (int w = 0; w < 2 && rc == OS_OK; ++w) rc = launch_tb_any(h, steps_per_launch, interior, general, has_interior);
+        if (rc != OS_OK) break;
+        if (cudaEventRecord(t0, h->stream) != cudaSuccess) { rc = OS_ERR_CUDA; break; }
+        for (int k = 0; k < std::max(1, repeats) && rc == OS_OK; ++k)
+            rc = launch_tb_any(h, steps_per_launch, interior, general, has_interior);
+        if (rc != OS_OK) break;
+        float ms = 0.0f;
+        if (cudaEventRecord(t1, h->stream) != cudaSuccess || cudaEventSynchronize(t1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, t0, t1) != cudaSuccess) {
+            rc = os::cuda_status(cudaGetLastError(), "os_fdtd2d_autotune timing");
+            break;
+        }
+        ms /= std::max(1, repeats);
+        if (best < 0.0f || ms < best) {
+            best = ms;
+            best_r = candidates[c];
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    h->profiling = saved_prof;
+    h->tile_rows = rc == OS_OK ? best_r : saved_rows;
+    if (rc != OS_OK) return rc;
+    *best_rows = best_r;
+    *best_ms = best;
+    return OS_OK;
+}
+
 extern "C" int os_fdtd2d_plan_info(OsFdtd2D *h, int32_t steps_per_launch, int64_t *interior_cells,
                                    int64_t *interior_tiles, int64_t *general_tiles) {
     OS_CHECK(h && interior_cells && interior_tiles && general_tiles, OS_ERR_INVALID,
@@ -719,6 +812,7 @@ extern "C" int os_fdtd2d_kernel_times(OsFdtd2D *h, int32_t kind, double *total_m
     OS_CHECK(h && total_ms && launches, OS_ERR_INVALID, "os_fdtd2d_kernel_times: null argument");
     OS_TRY(bind_device(h));
     OS_CUDA(cudaStreamSynchronize(h->stream));
+    OS_CUDA(cudaStreamSynchronize(h->side_stream));
     double total = 0.0;
     int64_t count = 0;
     for (size_t k = 0; k < h->prof_used; ++k) {

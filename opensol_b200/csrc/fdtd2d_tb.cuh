@@ -71,6 +71,7 @@ struct TBParams {
     int64_t n0;                 // engine steps taken before this launch
     int64_t m;                  // DFT sample interval
     int64_t q_first;            // sample number of staging slot 0
+    uint32_t sample_mask;       // bit s - 1: step s of this launch is a DFT sample step
     int32_t n_rects;
     TBRect rects[TB_MAX_RECTS];
     int32_t tile_w, tile_rows, n_tiles;
@@ -144,37 +145,59 @@ __device__ __forceinline__ void tb_load_row(const float *__restrict__ src, size_
 
 template <int T, int C, bool GEN, bool CA>
 struct TBWarp {
-    const TBParams &p;
+    const TBParams &p;   // rare paths only (CPML rows, line and monitor records); hot values are copied below
     TBCols<C> cols;
     TBState<T, C, GEN> st;
     int i0, i1, r_begin, r_end;
     bool vec;
+    // hot parameters in registers: reading them through `p` after a global store would reload them
+    int nx, ny, npml, cpml_mask;
+    bool px, py;
+    const float *__restrict__ ez_in, *__restrict__ hx_in, *__restrict__ hy_in;
+    float *ez_out, *hx_out, *hy_out;
+    const float *__restrict__ cbp, *__restrict__ cap, *__restrict__ dap, *__restrict__ dbp;
+    float da_u, db_u, s_inv_dx_e, s_inv_dx_h, s_inv_dy_e, s_inv_dy_h;
+    const float *__restrict__ inv_dx_e, *__restrict__ inv_dx_h;
+    uint32_t sample_mask;
+    uint32_t line_mask;   // line sources whose cells can fall in this tile's cone
+    uint32_t mon_mask;    // flux lines with cells among this tile's outputs
 
-    __device__ __forceinline__ TBWarp(const TBParams &params) : p(params) {}
+    __device__ __forceinline__ TBWarp(const TBParams &params)
+        : p(params), nx(params.nx), ny(params.ny), npml(params.npml), cpml_mask(params.cpml_mask),
+          px(params.px != 0), py(params.py != 0), ez_in(params.ez_in), hx_in(params.hx_in), hy_in(params.hy_in),
+          ez_out(params.ez_out), hx_out(params.hx_out), hy_out(params.hy_out), cbp(params.cb), cap(params.ca),
+          dap(params.da), dbp(params.db), da_u(params.da_u), db_u(params.db_u), s_inv_dx_e(params.s_inv_dx_e),
+          s_inv_dx_h(params.s_inv_dx_h), s_inv_dy_e(params.s_inv_dy_e), s_inv_dy_h(params.s_inv_dy_h),
+          inv_dx_e(params.inv_dx_e), inv_dx_h(params.inv_dx_h), sample_mask(params.sample_mask) {}
 
-    __device__ __forceinline__ int phys_row(int i) const { return p.px ? tb_wrap(i, p.nx) : i; }
+    __device__ __forceinline__ int phys_row(int i) const { return px ? tb_wrap(i, nx) : i; }
 
     // Stage 0 of stream row r: fields (and psi^0 of CPML cells) from the input buffers.
     template <int PH>
     __device__ __forceinline__ void load_row(int r) {
         const int rp = phys_row(r);
-        const size_t base = (size_t)rp * (size_t)p.ny;
-        tb_load_row<C>(p.ez_in, base, cols, vec, st.E[PH][0]);
-        tb_load_row<C>(p.hx_in, base, cols, vec, st.Hx[PH][0]);
-        tb_load_row<C>(p.hy_in, base, cols, vec, st.Hy[PH][0]);
+        const size_t base = (size_t)rp * (size_t)ny;
+        tb_load_row<C>(ez_in, base, cols, vec, st.E[PH][0]);
+        tb_load_row<C>(hx_in, base, cols, vec, st.Hx[PH][0]);
+        tb_load_row<C>(hy_in, base, cols, vec, st.Hy[PH][0]);
+        // the coefficient rows of row r are first read by stage 1 of the next iteration: pull them into L1 now
+        if (cols.in_grid[0]) {
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(cbp + base + cols.jp[0]));
+            if (CA) asm volatile("prefetch.global.L1 [%0];" ::"l"(cap + base + cols.jp[0]));
+        }
         if constexpr (GEN) {
             int xh_side, xh_k, xe_side, xe_k;
-            tb_cpml_slot(rp, p.nx, p.npml, p.cpml_mask & 1, p.cpml_mask & 2, 0, 1, xh_side, xh_k, xe_side, xe_k);
+            tb_cpml_slot(rp, nx, npml, cpml_mask & 1, cpml_mask & 2, 0, 1, xh_side, xh_k, xe_side, xe_k);
 #pragma unroll
             for (int c = 0; c < C; ++c) {
                 const bool g = cols.in_grid[c];
                 const int j = cols.jp[c];
-                st.pxh[PH][0][c] = (g && xh_side >= 0) ? p.psi_h_in[xh_side][(size_t)xh_k * p.ny + j] : 0.0f;
-                st.pxe[PH][0][c] = (g && xe_side >= 0) ? p.psi_e_in[xe_side][(size_t)xe_k * p.ny + j] : 0.0f;
+                st.pxh[PH][0][c] = (g && xh_side >= 0) ? p.psi_h_in[xh_side][(size_t)xh_k * ny + j] : 0.0f;
+                st.pxe[PH][0][c] = (g && xe_side >= 0) ? p.psi_e_in[xe_side][(size_t)xe_k * ny + j] : 0.0f;
                 st.pyh[PH][0][c] = (g && cols.yh_side[c] >= 0)
-                                       ? p.psi_h_in[cols.yh_side[c]][(size_t)rp * p.npml + cols.yh_k[c]] : 0.0f;
+                                       ? p.psi_h_in[cols.yh_side[c]][(size_t)rp * npml + cols.yh_k[c]] : 0.0f;
                 st.pye[PH][0][c] = (g && cols.ye_side[c] >= 0)
-                                       ? p.psi_e_in[cols.ye_side[c]][(size_t)rp * p.npml + cols.ye_k[c]] : 0.0f;
+                                       ? p.psi_e_in[cols.ye_side[c]][(size_t)rp * npml + cols.ye_k[c]] : 0.0f;
             }
         }
     }
@@ -186,38 +209,37 @@ struct TBWarp {
         const int i = r - S;
         if (i < r_begin || i > r_end) return;
         const int ip = phys_row(i);
-        const int nx = p.nx, ny = p.ny;
         const size_t base = (size_t)ip * (size_t)ny;
 
         float cb[C], ca[C], da[C], db[C];
-        tb_load_row<C>(p.cb, base, cols, vec, cb);
+        tb_load_row<C>(cbp, base, cols, vec, cb);
         if constexpr (CA) {
-            tb_load_row<C>(p.ca, base, cols, vec, ca);
+            tb_load_row<C>(cap, base, cols, vec, ca);
         }
         if constexpr (GEN) {
-            if (p.da) {
-                tb_load_row<C>(p.da, base, cols, vec, da);
-                tb_load_row<C>(p.db, base, cols, vec, db);
+            if (dap) {
+                tb_load_row<C>(dap, base, cols, vec, da);
+                tb_load_row<C>(dbp, base, cols, vec, db);
             } else {
 #pragma unroll
                 for (int c = 0; c < C; ++c) {
-                    da[c] = p.da_u;
-                    db[c] = p.db_u;
+                    da[c] = da_u;
+                    db[c] = db_u;
                 }
             }
         } else {
 #pragma unroll
-            for (int c = 0; c < C; ++c) db[c] = p.db_u;
+            for (int c = 0; c < C; ++c) db[c] = db_u;
         }
         float inv_x_h, inv_x_e;
         int xh_side = -1, xh_k = 0, xe_side = -1, xe_k = 0;
         if constexpr (GEN) {
-            inv_x_h = __ldg(p.inv_dx_h + ip);
-            inv_x_e = __ldg(p.inv_dx_e + ip);
-            tb_cpml_slot(ip, nx, p.npml, p.cpml_mask & 1, p.cpml_mask & 2, 0, 1, xh_side, xh_k, xe_side, xe_k);
+            inv_x_h = __ldg(inv_dx_h + ip);
+            inv_x_e = __ldg(inv_dx_e + ip);
+            tb_cpml_slot(ip, nx, npml, cpml_mask & 1, cpml_mask & 2, 0, 1, xh_side, xh_k, xe_side, xe_k);
         } else {
-            inv_x_h = p.s_inv_dx_h;
-            inv_x_e = p.s_inv_dx_e;
+            inv_x_h = s_inv_dx_h;
+            inv_x_e = s_inv_dx_e;
         }
 
         // ---- H^S of row i (fdtd_ez_2d_kernels.py:41-47, then the H-row CPML, boundaries.py:752-755)
@@ -232,7 +254,7 @@ struct TBWarp {
             const float hy_old = st.Hy[Q][S - 1][c];
             const int j = cols.jp[c];
             // H_x: every column but the last of a non-periodic y axis (whose face is never updated)
-            if (GEN && !p.py && j == ny - 1) {
+            if (GEN && !py && j == ny - 1) {
                 hxn[c] = hx_old;
             } else {
                 float v;
@@ -241,18 +263,18 @@ struct TBWarp {
                     if (cols.yh_side[c] >= 0) {
                         const int sd = cols.yh_side[c], k = cols.yh_k[c];
                         const float *rows = p.cpml_rows[sd];
-                        float q = st.pyh[Q][S - 1][c] * rows[3 * p.npml + k];
-                        q += rows[4 * p.npml + k] * (e_right - e) * rows[5 * p.npml + k];
+                        float q = st.pyh[Q][S - 1][c] * rows[3 * npml + k];
+                        q += rows[4 * npml + k] * (e_right - e) * rows[5 * npml + k];
                         st.pyh[PH][S][c] = q;
                         v += (-db[c]) * q;
                     }
                 } else {
-                    v = hx_old - db[c] * (e_right - e) * p.s_inv_dy_h;
+                    v = hx_old - db[c] * (e_right - e) * s_inv_dy_h;
                 }
                 hxn[c] = v;
             }
             // H_y: every row but the last of a non-periodic x axis
-            if (GEN && !p.px && ip == nx - 1) {
+            if (GEN && !px && ip == nx - 1) {
                 hyn[c] = hy_old;
             } else {
                 float v;
@@ -260,8 +282,8 @@ struct TBWarp {
                     v = da[c] * hy_old + db[c] * (e_up - e) * inv_x_h;
                     if (xh_side >= 0) {
                         const float *rows = p.cpml_rows[xh_side];
-                        float q = st.pxh[Q][S - 1][c] * rows[3 * p.npml + xh_k];
-                        q += rows[4 * p.npml + xh_k] * (e_up - e) * rows[5 * p.npml + xh_k];
+                        float q = st.pxh[Q][S - 1][c] * rows[3 * npml + xh_k];
+                        q += rows[4 * npml + xh_k] * (e_up - e) * rows[5 * npml + xh_k];
                         st.pxh[PH][S][c] = q;
                         v += db[c] * q;
                     }
@@ -274,24 +296,23 @@ struct TBWarp {
 
         // ---- E^S of row i (fdtd_ez_2d_kernels.py:107-120), E-row CPML x then y sides, line sources
         const float hx_left_first = __shfl_up_sync(0xffffffffu, hxn[C - 1], 1);
-        const int64_t step = p.n0 + S;   // engine step number after this stage
 #pragma unroll
         for (int c = 0; c < C; ++c) {
             const int j = cols.jp[c];
             float hx_left = c > 0 ? hxn[c - 1] : hx_left_first;
             float hy_down = st.Hy[Q][S][c];   // H_y^S of row i - 1
             float curl;
-            if (GEN && !p.px && ip == 0) {
+            if (GEN && !px && ip == 0) {
                 curl = hyn[c] * inv_x_e;
             } else {
-                if (p.px && ip == 0) hy_down = tb_lo_wrap(hy_down);
+                if (px && ip == 0) hy_down = tb_lo_wrap(hy_down);
                 curl = (hyn[c] - hy_down) * inv_x_e;
             }
-            const float inv_y_e = GEN ? cols.inv_y_e[c] : p.s_inv_dy_e;
-            if (GEN && !p.py && j == 0) {
+            const float inv_y_e = GEN ? cols.inv_y_e[c] : s_inv_dy_e;
+            if (GEN && !py && j == 0) {
                 curl -= hxn[c] * inv_y_e;
             } else {
-                if (p.py && j == 0) hx_left = tb_lo_wrap(hx_left);
+                if (py && j == 0) hx_left = tb_lo_wrap(hx_left);
                 curl -= (hxn[c] - hx_left) * inv_y_e;
             }
             const float e_old = st.E[Q][S - 1][c];
@@ -300,7 +321,7 @@ struct TBWarp {
                 if (xe_side >= 0) {
                     const float *rows = p.cpml_rows[xe_side];
                     float q = st.pxe[Q][S - 1][c] * rows[xe_k];
-                    q += rows[p.npml + xe_k] * (hyn[c] - hy_down) * rows[2 * p.npml + xe_k];
+                    q += rows[npml + xe_k] * (hyn[c] - hy_down) * rows[2 * npml + xe_k];
                     st.pxe[PH][S][c] = q;
                     v += cb[c] * q;
                 }
@@ -308,12 +329,13 @@ struct TBWarp {
                     const int sd = cols.ye_side[c], k = cols.ye_k[c];
                     const float *rows = p.cpml_rows[sd];
                     float q = st.pye[Q][S - 1][c] * rows[k];
-                    q += rows[p.npml + k] * (hxn[c] - hx_left) * rows[2 * p.npml + k];
+                    q += rows[npml + k] * (hxn[c] - hx_left) * rows[2 * npml + k];
                     st.pye[PH][S][c] = q;
                     v += (-cb[c]) * q;
                 }
             }
-            for (int l = 0; l < p.n_lines; ++l) {
+            for (uint32_t lines = line_mask; lines; lines &= lines - 1) {
+                const int l = __ffs(lines) - 1;
                 const TBLine &L = p.lines[l];
                 const int along = L.axis == 0 ? ip : j, across = L.axis == 0 ? j : ip;
                 if (across == L.position && along >= L.lo && along < L.hi && cols.in_grid[c]) {
@@ -327,9 +349,10 @@ struct TBWarp {
         }
 
         // ---- DFT sample: the owner copies the flux lines' E_z and tangential H of this step
-        if (p.n_mons && step % p.m == 0 && i >= i0 && i < i1) {
-            const int64_t slot = step / p.m - p.q_first;
-            for (int mi = 0; mi < p.n_mons; ++mi) {
+        if (mon_mask && ((sample_mask >> (S - 1)) & 1u) && i >= i0 && i < i1) {
+            const int slot = __popc(sample_mask & ((1u << (S - 1)) - 1u));
+            for (uint32_t mons = mon_mask; mons; mons &= mons - 1) {
+                const int mi = __ffs(mons) - 1;
                 const TBMon &M = p.mons[mi];
                 const int n = M.hi - M.lo;
 #pragma unroll
@@ -356,39 +379,39 @@ struct TBWarp {
         const int i = r - T;
         if (i < i0 || i >= i1) return;
         const int ip = phys_row(i);
-        const size_t base = (size_t)ip * (size_t)p.ny;
+        const size_t base = (size_t)ip * (size_t)ny;
         bool all_own = true;
 #pragma unroll
         for (int c = 0; c < C; ++c) all_own = all_own && cols.own[c];
         if (C == 4 && vec && all_own) {
-            *reinterpret_cast<float4 *>(p.ez_out + base + cols.jp[0]) =
+            *reinterpret_cast<float4 *>(ez_out + base + cols.jp[0]) =
                 make_float4(st.E[PH][T][0], st.E[PH][T][1], st.E[PH][T][2], st.E[PH][T][3]);
-            *reinterpret_cast<float4 *>(p.hx_out + base + cols.jp[0]) =
+            *reinterpret_cast<float4 *>(hx_out + base + cols.jp[0]) =
                 make_float4(st.Hx[PH][T][0], st.Hx[PH][T][1], st.Hx[PH][T][2], st.Hx[PH][T][3]);
-            *reinterpret_cast<float4 *>(p.hy_out + base + cols.jp[0]) =
+            *reinterpret_cast<float4 *>(hy_out + base + cols.jp[0]) =
                 make_float4(st.Hy[PH][T][0], st.Hy[PH][T][1], st.Hy[PH][T][2], st.Hy[PH][T][3]);
         } else {
 #pragma unroll
             for (int c = 0; c < C; ++c) {
                 if (!cols.own[c]) continue;
-                p.ez_out[base + cols.jp[c]] = st.E[PH][T][c];
-                p.hx_out[base + cols.jp[c]] = st.Hx[PH][T][c];
-                p.hy_out[base + cols.jp[c]] = st.Hy[PH][T][c];
+                ez_out[base + cols.jp[c]] = st.E[PH][T][c];
+                hx_out[base + cols.jp[c]] = st.Hx[PH][T][c];
+                hy_out[base + cols.jp[c]] = st.Hy[PH][T][c];
             }
         }
         if constexpr (GEN) {
             int xh_side, xh_k, xe_side, xe_k;
-            tb_cpml_slot(ip, p.nx, p.npml, p.cpml_mask & 1, p.cpml_mask & 2, 0, 1, xh_side, xh_k, xe_side, xe_k);
+            tb_cpml_slot(ip, nx, npml, cpml_mask & 1, cpml_mask & 2, 0, 1, xh_side, xh_k, xe_side, xe_k);
 #pragma unroll
             for (int c = 0; c < C; ++c) {
                 if (!cols.own[c]) continue;
                 const int j = cols.jp[c];
-                if (xh_side >= 0) p.psi_h_out[xh_side][(size_t)xh_k * p.ny + j] = st.pxh[PH][T][c];
-                if (xe_side >= 0) p.psi_e_out[xe_side][(size_t)xe_k * p.ny + j] = st.pxe[PH][T][c];
+                if (xh_side >= 0) p.psi_h_out[xh_side][(size_t)xh_k * ny + j] = st.pxh[PH][T][c];
+                if (xe_side >= 0) p.psi_e_out[xe_side][(size_t)xe_k * ny + j] = st.pxe[PH][T][c];
                 if (cols.yh_side[c] >= 0)
-                    p.psi_h_out[cols.yh_side[c]][(size_t)ip * p.npml + cols.yh_k[c]] = st.pyh[PH][T][c];
+                    p.psi_h_out[cols.yh_side[c]][(size_t)ip * npml + cols.yh_k[c]] = st.pyh[PH][T][c];
                 if (cols.ye_side[c] >= 0)
-                    p.psi_e_out[cols.ye_side[c]][(size_t)ip * p.npml + cols.ye_k[c]] = st.pye[PH][T][c];
+                    p.psi_e_out[cols.ye_side[c]][(size_t)ip * npml + cols.ye_k[c]] = st.pye[PH][T][c];
             }
         }
     }
@@ -432,10 +455,36 @@ __global__ void __launch_bounds__(TB_WARPS * 32) ez2d_tb_kernel(const TBParams p
     W.r_end = p.px ? W.i1 - 1 + T : min(p.nx - 1, W.i1 - 1 + T);
     W.vec = (C == 4) && (p.ny % 4 == 0);
     constexpr int HL = C == 1 ? T : 4;
+    // Line sources that can reach this tile's cone, flux lines with cells among its outputs (usually none).
+    {
+        const int cone_c0 = j0 - HL, cone_c1 = j0 - HL + 32 * C;   // loaded columns (stream coordinates)
+        uint32_t lm = 0, mm = 0;
+        for (int l = 0; l < p.n_lines; ++l) {
+            const TBLine &L = p.lines[l];
+            bool hit;
+            if (p.px || p.py) {
+                hit = true;   // wrapped coordinates: keep the per-cell test
+            } else if (L.axis == 0) {   // cells (i, position), i in [lo, hi)
+                hit = L.position >= cone_c0 && L.position < cone_c1 && L.hi > W.r_begin && L.lo <= W.r_end;
+            } else {                    // cells (position, j)
+                hit = L.position >= W.r_begin && L.position <= W.r_end && L.hi > cone_c0 && L.lo < cone_c1;
+            }
+            if (hit) lm |= 1u << l;
+        }
+        for (int q = 0; q < p.n_mons; ++q) {
+            const TBMon &M = p.mons[q];
+            const bool hit = M.normal_axis == 0
+                                 ? (M.position >= W.i0 && M.position < W.i1 && M.hi > j0 && M.lo < j1)
+                                 : (M.position >= j0 && M.position < j1 && M.hi > W.i0 && M.lo < W.i1);
+            if (hit) mm |= 1u << q;
+        }
+        W.line_mask = lm;
+        W.mon_mask = p.sample_mask ? mm : 0u;
+    }
 #pragma unroll
     for (int c = 0; c < C; ++c) {
         const int jl = j0 - HL + lane * C + c;
-        W.cols.in_grid[c] = p.py || (jl >= 0 && jl < p.ny);
+        W.cols.in_grid[c] = p.py || (jl >= 0 && jl < p.ny);   // (p.py: wrapped)
         W.cols.jp[c] = p.py ? tb_wrap(jl, p.ny) : jl;
         W.cols.own[c] = jl >= j0 && jl < j1;
         const int jc = W.cols.in_grid[c] ? W.cols.jp[c] : 0;

@@ -149,6 +149,20 @@ class FDTDEngine2D_Ez:
         if self._handle is not None:
             self.sync_device()
 
+    AUTOTUNE_ROWS = (32, 48, 64, 96, 128, 192, 256)
+
+    def autotune(self, candidates=AUTOTUNE_ROWS, repeats=3):
+        """Time the interior tile heights on this engine's fields and keep the fastest (the simulation state is not
+        changed: trial launches write the idle buffer set).  Returns (rows, ms per launch)."""
+        self.sync_device()
+        arr = (ctypes.c_int32 * len(candidates))(*candidates)
+        rows, ms = ctypes.c_int32(), ctypes.c_float()
+        _native.check(_native.load().os_fdtd2d_autotune(self.handle, self.steps_per_launch, arr, len(candidates),
+                                                        int(repeats), ctypes.byref(rows), ctypes.byref(ms)))
+        self.tile_rows = int(rows.value)
+        self._config_sent = (self.variant, self.steps_per_launch, self.tile_rows)
+        return self.tile_rows, float(ms.value)
+
     def launch_count(self):
         """Kernels the last advance launched."""
         n = ctypes.c_int64()

@@ -97,6 +97,26 @@ def test_kernel_configs_bit_exact(spec, config):
             np.testing.assert_array_equal(h, g[f'spec_h{k}_{cp}'])
 
 
+def test_autotune_keeps_state_and_results():
+    """The tile-height autotuner times trial launches on the live fields without changing them; the run afterwards is
+    still open_sol's bit for bit."""
+    spec = CASES[0]
+    g = np.load(os.path.join(GOLDEN, 'c1.npz'))
+    sim = ob.Simulation(**spec['sim'], verbose=False)
+    mons = apply_ops(sim, spec)
+    sim.run(n_steps=150, verbose=False)
+    before = _fields(sim)
+    rows, ms = sim.em.engine.autotune(candidates=(3, 16, 64), repeats=2)
+    assert rows in (3, 16, 64) and ms > 0
+    for name, arr in _fields(sim).items():
+        np.testing.assert_array_equal(arr, before[name])
+    sim.run(n_steps=150, verbose=False)
+    for name, arr in _fields(sim).items():
+        assert _digest(arr) == str(g[f'sha_{name}_300'])
+    e, h = mons[0].spectra()
+    np.testing.assert_array_equal(e, g['spec_e0_300'])
+
+
 def test_interior_and_general_kernels_both_run():
     """The headline grid uses both blocked kernels: the interior kernel holds nearly all cells."""
     args = workloads.roofline_2d_sim_args()
