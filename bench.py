@@ -48,7 +48,7 @@ def parse_args():
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-e2e', action='store_true')
     p.add_argument('--variant', type=int, default=1, help='1: temporally blocked kernels (default), 0: per step')
-    p.add_argument('--steps-per-launch', type=int, default=4)
+    p.add_argument('--steps-per-launch', type=int, default=3)
     p.add_argument('--tile-rows', type=int, default=0, help='rows per interior tile (0: autotune)')
     return p.parse_args()
 

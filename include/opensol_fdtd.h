@@ -113,7 +113,8 @@ int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line_values, in
                       int64_t n_samples, const float *phases);
 
 /* Kernel choice: variant 1 (default) advances steps_per_launch (1..4) Yee steps per launch with temporally blocked,
- * double-buffered kernels, tile_rows rows per interior tile; variant 0 launches one H and one E kernel per step.
+ * double-buffered kernels, tile_rows rows per interior tile; variant 2 the same with the general kernel on every
+ * cell; variant 0 launches one H and one E kernel per step.
  * Every choice gives bit-identical results.  No open_sol counterpart (open_sol launches per half step). */
 int os_fdtd2d_configure(OsFdtd2D *h, int32_t variant, int32_t steps_per_launch, int32_t tile_rows);
 

@@ -12,6 +12,7 @@
 #include "common.cuh"
 #include "fdtd2d_kernels.cuh"
 #include "fdtd2d_tb.cuh"
+#include "fdtd2d_interior.cuh"
 
 #include <algorithm>
 
@@ -52,7 +53,7 @@ struct OsFdtd2D {
     bool cpml_set[4] = {false, false, false, false};
     std::vector<float> host_inv[4];       // inv_dx_e, inv_dx_h, inv_dy_e, inv_dy_h (host copies: interior check)
     int32_t variant = 1;                  // 0: per-half-step kernels, 1: temporally blocked
-    int32_t steps_per_launch = 4;         // T of the blocked kernels
+    int32_t steps_per_launch = 3;         // T of the blocked kernels
     int32_t tile_rows = 128;              // rows per interior tile
     int32_t gen_tile_rows = 16;           // rows per general tile
     int64_t launches = 0;                 // kernels launched by the last advance
@@ -64,6 +65,7 @@ struct OsFdtd2D {
     std::vector<std::unique_ptr<os::FluxLine2D>> fluxes;
     int64_t sample_interval = 1;
     int64_t n_step = 0;
+    os::DeviceArray<int32_t> err;         // set by a kernel whose bounded wait ran out
     os::DeviceArray<float> line_values;   // (n_lines, n_steps) of the current chunk
     os::DeviceArray<float> phases;        // per monitor (n_samples, nf, 2) of the current chunk
     int device = 0;
@@ -77,6 +79,19 @@ static int bind_device(OsFdtd2D *h) {
 }
 
 static size_t cells(const OsFdtd2D *h) { return (size_t)h->grid.nx * (size_t)h->grid.ny; }
+
+// Synchronise the handle's stream and report a kernel whose bounded wait ran out (the flag is cleared).
+static int sync_and_check(OsFdtd2D *h) {
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    int32_t flag = 0;
+    OS_CUDA(cudaMemcpy(&flag, h->err.ptr, sizeof(flag), cudaMemcpyDeviceToHost));
+    if (flag) {
+        OS_CUDA(cudaMemset(h->err.ptr, 0, sizeof(int32_t)));
+        set_error("a staged row did not arrive within the bounded wait: the fields of the last advance are invalid");
+        return OS_ERR_CUDA;
+    }
+    return OS_OK;
+}
 
 static int zero_state(OsFdtd2D *h) {
     const size_t n = cells(h);
@@ -194,6 +209,8 @@ extern "C" int os_fdtd2d_create(const OsGrid2D *grid, OsFdtd2D **out) {
         }
         OS_TRY(h->cpml_rows[s].alloc(6 * (size_t)g.npml));
     }
+    OS_TRY(h->err.alloc(1));
+    OS_CUDA(cudaMemsetAsync(h->err.ptr, 0, sizeof(int32_t), h->stream));
     OS_TRY(zero_state(h.get()));
     OS_CUDA(cudaStreamSynchronize(h->stream));
     *out = h.release();
@@ -469,7 +486,8 @@ static void plan_tiles(const OsFdtd2D *h, int T, TBParams &interior, TBParams &g
         in.c0 = cy ? round_up(npml + 1 + 4, 4) : g.ny;
         in.c1 = cy ? g.ny - npml - 1 - T : 0;
     }
-    has_interior = in.r1 > in.r0 && in.c1 > in.c0 && g.ny % 4 == 0 && !h->has_dadb && h->da_uniform == 1.0f;
+    has_interior = h->variant == 1 && in.r1 > in.r0 && in.c1 > in.c0 && g.ny % 4 == 0 && !h->has_dadb &&
+                   h->da_uniform == 1.0f;
     // uniform curl spacings over the interior's dependency cone (rows [r0 - T, r1 + T), columns [c0 - 4, c1 + T));
     // the columns a tile loads beyond its cone feed no output and may be anything
     if (has_interior) {
@@ -531,6 +549,35 @@ static void fill_common(const OsFdtd2D *h, TBParams &q) {
         q.mons[k].stage = h->fluxes[k]->stage.ptr;
     }
     q.m = h->sample_interval;
+    q.err = h->err.ptr;
+}
+
+template <int T, bool CA, bool PX, bool PY>
+static int launch_interior(OsFdtd2D *h, const TBParams &q) {
+    const size_t smem = (size_t)TB_WARPS * tb_warp_smem_bytes(T, CA);
+    static bool attr_set = false;   // one flag per instantiation
+    if (!attr_set) {
+        OS_CUDA(cudaFuncSetAttribute(ez2d_interior_kernel<T, CA, PX, PY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+        attr_set = true;
+    }
+    const dim3 blocks((unsigned)((q.n_tiles + TB_WARPS - 1) / TB_WARPS)), threads(TB_WARPS * 32);
+    ez2d_interior_kernel<T, CA, PX, PY><<<blocks, threads, smem, h->stream>>>(q);
+    return OS_OK;
+}
+
+template <int T, bool CA>
+static int launch_interior_ca(OsFdtd2D *h, const TBParams &q) {
+    const bool px = h->grid.periodic_x != 0, py = h->grid.periodic_y != 0;
+    if (px && py) return launch_interior<T, CA, true, true>(h, q);
+    if (px) return launch_interior<T, CA, true, false>(h, q);
+    if (py) return launch_interior<T, CA, false, true>(h, q);
+    return launch_interior<T, CA, false, false>(h, q);
+}
+
+template <int T>
+static int launch_interior_any(OsFdtd2D *h, const TBParams &q) {
+    return h->has_ca ? launch_interior_ca<T, true>(h, q) : launch_interior_ca<T, false>(h, q);
 }
 
 // One blocked launch: the border (general) kernel forks onto the side stream and overlaps the interior kernel; both
@@ -554,10 +601,8 @@ static int launch_tb(OsFdtd2D *h, const TBParams &interior, const TBParams &gene
         h->launches += 1;
     }
     if (run_interior) {
-        const dim3 blocks((unsigned)((interior.n_tiles + TB_WARPS - 1) / TB_WARPS));
         OS_TRY(prof_begin(h, 0, h->stream));
-        if (h->has_ca) ez2d_tb_kernel<T, 4, false, true><<<blocks, threads, 0, h->stream>>>(interior);
-        else ez2d_tb_kernel<T, 4, false, false><<<blocks, threads, 0, h->stream>>>(interior);
+        OS_TRY(launch_interior_any<T>(h, interior));
         OS_TRY(prof_end(h, h->stream));
         h->launches += 1;
     }
@@ -703,7 +748,7 @@ extern "C" int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line
     if (!h->fluxes.empty() && phase_floats && phases) OS_TRY(upload(h->phases, phases, phase_floats, h->stream));
     OS_CUDA(cudaEventRecord(h->ev_start, h->stream));
     const int rc = h->variant == 0 ? advance_per_step(h, n_steps, first_sample, n_samples)
-                                   : advance_blocked(h, n_steps, first_sample, n_samples);
+                                   : advance_blocked(h, n_steps, first_sample, n_samples);   // 1 and 2
     if (rc != OS_OK) return rc;
     OS_CUDA(cudaEventRecord(h->ev_stop, h->stream));
     h->timed = true;
@@ -712,7 +757,8 @@ extern "C" int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line
 
 extern "C" int os_fdtd2d_configure(OsFdtd2D *h, int32_t variant, int32_t steps_per_launch, int32_t tile_rows) {
     OS_CHECK(h, OS_ERR_INVALID, "os_fdtd2d_configure: null handle");
-    OS_CHECK(variant == 0 || variant == 1, OS_ERR_INVALID, "variant must be 0 (per half step) or 1 (blocked)");
+    OS_CHECK(variant >= 0 && variant <= 2, OS_ERR_INVALID,
+             "variant must be 0 (per half step), 1 (blocked) or 2 (blocked, general kernel only)");
     OS_CHECK(steps_per_launch >= 1 && steps_per_launch <= TB_MAX_T, OS_ERR_INVALID,
              "steps_per_launch must be in [1, %d], got %d", TB_MAX_T, steps_per_launch);
     OS_CHECK(tile_rows >= 1, OS_ERR_INVALID, "tile_rows must be >= 1, got %d", tile_rows);
@@ -846,7 +892,7 @@ extern "C" int os_fdtd2d_read_flux_spectra(OsFdtd2D *h, int32_t monitor_id, doub
     FluxLine2D &f = *h->fluxes[monitor_id];
     OS_CUDA(cudaMemcpyAsync(e_spectra, f.e_acc.ptr, f.e_acc.bytes(), cudaMemcpyDeviceToHost, h->stream));
     OS_CUDA(cudaMemcpyAsync(h_spectra, f.h_acc.ptr, f.h_acc.bytes(), cudaMemcpyDeviceToHost, h->stream));
-    OS_CUDA(cudaStreamSynchronize(h->stream));
+    OS_TRY(sync_and_check(h));
     return OS_OK;
 }
 
@@ -865,7 +911,7 @@ extern "C" int os_fdtd2d_read_field(OsFdtd2D *h, int32_t component, float *out) 
     OS_CHECK(src, OS_ERR_INVALID, "os_fdtd2d_read_field: unknown component %d", component);
     OS_TRY(bind_device(h));
     OS_CUDA(cudaMemcpyAsync(out, src, cells(h) * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-    OS_CUDA(cudaStreamSynchronize(h->stream));
+    OS_TRY(sync_and_check(h));
     return OS_OK;
 }
 
@@ -888,8 +934,7 @@ extern "C" int os_fdtd2d_reset(OsFdtd2D *h) {
 extern "C" int os_fdtd2d_synchronize(OsFdtd2D *h) {
     OS_CHECK(h, OS_ERR_INVALID, "os_fdtd2d_synchronize: null handle");
     OS_TRY(bind_device(h));
-    OS_CUDA(cudaStreamSynchronize(h->stream));
-    return OS_OK;
+    return sync_and_check(h);
 }
 
 extern "C" int os_fdtd2d_set_stream(OsFdtd2D *h, void *cuda_stream) {

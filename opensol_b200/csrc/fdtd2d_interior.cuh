@@ -1,0 +1,357 @@
+// Interior kernel of the temporally blocked 2D E_z step (the cells whose T-step dependency cone avoids the CPML slabs
+// and the non-periodic grid edges; fdtd2d_tb.cuh has the general kernel and the shared plumbing).
+//
+// One warp streams one tile of 120 output columns (128 loaded: 4 halo columns on each side, enough for T <= 4) and
+// tile_rows output rows, T steps per launch, with the time-skewed register pipeline described in fdtd2d_tb.cuh.  Rows
+// arrive in a per-warp shared-memory ring by 1D bulk copies (TMA) TB_AHEAD rows ahead.  A thread holds 4 adjacent
+// columns as two float2 pairs and does the arithmetic with the packed sm_100 operations __fadd2_rn / __fmul2_rn: each
+// lane of a packed operation is rounded on its own exactly like the scalar __fadd_rn / __fmul_rn, so the results are
+// the same bits as open_sol's float32 evaluation (x - y is evaluated as x + (-y), which IEEE defines identically).
+// One exception is kept out: the code generator merges a packed multiply into a following packed add (a packed fused
+// multiply-add, one rounding instead of two, even from explicit .rn PTX), so every add whose operand is a product is
+// done per lane with the scalar __fadd_rn, which is never merged.  Multiplies and the adds of plain differences stay
+// packed.  The periodic wraps are compile-time (PX, PY): a non-periodic axis costs nothing.
+#pragma once
+
+#include "fdtd2d_tb.cuh"
+
+// packed add / subtract: only for operands that are not products (see above)
+__device__ __forceinline__ float2 ip_sub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 ip_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+// per-lane add / subtract of a product: two separately rounded scalar operations, never merged with the multiply
+__device__ __forceinline__ float2 ip_add_p(float2 a, float2 b) {
+    return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
+}
+__device__ __forceinline__ float2 ip_sub_p(float2 a, float2 b) {
+    return make_float2(__fadd_rn(a.x, -b.x), __fadd_rn(a.y, -b.y));
+}
+
+template <int T, bool CA, bool PX, bool PY>
+struct IPWarp {
+    const TBParams &p;
+    // tile
+    int i0, i1, r_begin, r_end, j0, j1;
+    int lane, jl0, jp0;
+    uint32_t own;          // bit c: column jl0 + c is an output column
+    bool in_grid0;         // the 4 columns are real cells
+    bool wrap_lo0;         // PY: the first column is column 0 (its lo neighbour is the wrapped last column)
+    uint32_t line_mask, mon_mask, sample_mask;
+    int nx, ny;
+    float2 db2, ixh2, ixe2, iyh2, iye2;
+    float *ez_out, *hx_out, *hy_out;
+    const float *__restrict__ ez_in, *__restrict__ hx_in, *__restrict__ hy_in, *__restrict__ cbp, *__restrict__ cap;
+    // staging ring
+    float *sm_fields, *sm_cb, *sm_ca;
+    uint64_t *sm_bar;
+    uint32_t row_bytes;
+    bool failed = false;
+    // pipeline: [parity][stage][pair]
+    float2 E[2][T + 1][2], Hx[2][T + 1][2], Hy[2][T + 1][2];
+
+    __device__ __forceinline__ IPWarp(const TBParams &params) : p(params) {}
+
+    __device__ __forceinline__ int phys_row(int i) const { return PX ? tb_wrap(i, nx) : i; }
+
+    __device__ __forceinline__ uint32_t window(float *dst, const float *src_row, uint64_t *bar, bool issue) const {
+        uint32_t bytes = 0;
+        int remaining = 128, d = 0, col = PY ? tb_wrap(j0 - 4, ny) : j0 - 4;
+        while (remaining > 0 && col < ny) {
+            const int len = min(remaining, ny - col);
+            if (issue) tb_bulk_g2s(dst + d, src_row + col, (uint32_t)len * 4u, bar);
+            bytes += (uint32_t)len * 4u;
+            d += len;
+            remaining -= len;
+            if (!PY) break;
+            col = 0;
+        }
+        return bytes;
+    }
+
+    // lane 0: stage stream row R
+    __device__ __forceinline__ void issue_row(int R) {
+        const int k = R - r_begin;
+        const int fs = k % tb_field_slots(), cs = k % tb_coef_slots(T);
+        uint64_t *bar = sm_bar + fs;
+        const size_t base = (size_t)phys_row(R) * (size_t)ny;
+        tb_mbar_expect_tx(bar, row_bytes * (CA ? 5u : 4u));
+        float *f = sm_fields + fs * 384;
+        window(f, ez_in + base, bar, true);
+        window(f + 128, hx_in + base, bar, true);
+        window(f + 256, hy_in + base, bar, true);
+        window(sm_cb + cs * 128, cbp + base, bar, true);
+        if (CA) window(sm_ca + cs * 128, cap + base, bar, true);
+    }
+
+    template <int PH>
+    __device__ __forceinline__ bool take_row(int R) {
+        const int k = R - r_begin;
+        const int fs = k % tb_field_slots();
+        if (R <= r_end && !tb_mbar_wait(sm_bar + fs, (uint32_t)((k / tb_field_slots()) & 1))) return false;
+        const float *f = sm_fields + fs * 384 + lane * 4;
+        const float4 e = *reinterpret_cast<const float4 *>(f);
+        const float4 hx = *reinterpret_cast<const float4 *>(f + 128);
+        const float4 hy = *reinterpret_cast<const float4 *>(f + 256);
+        E[PH][0][0] = make_float2(e.x, e.y);
+        E[PH][0][1] = make_float2(e.z, e.w);
+        Hx[PH][0][0] = make_float2(hx.x, hx.y);
+        Hx[PH][0][1] = make_float2(hx.z, hx.w);
+        Hy[PH][0][0] = make_float2(hy.x, hy.y);
+        Hy[PH][0][1] = make_float2(hy.z, hy.w);
+        return true;
+    }
+
+    // Line sources of this tile's cone (rare): ez += value * profile on the line cells, per component.
+    template <int S>
+    __device__ __forceinline__ void inject(int ip, float2 (&ez)[2]) const {
+        for (uint32_t lines = line_mask; lines; lines &= lines - 1) {
+            const int l = __ffs(lines) - 1;
+            const TBLine &L = p.lines[l];
+            const float value = p.line_values[(size_t)l * p.values_stride + p.k0 + (S - 1)];
+            if (value == 0.0f || !in_grid0) continue;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int j = jp0 + c;
+                const int along = L.axis == 0 ? ip : j, across = L.axis == 0 ? j : ip;
+                if (across == L.position && along >= L.lo && along < L.hi) {
+                    float &v = (c & 1) ? ez[c >> 1].y : ez[c >> 1].x;
+                    v = __fadd_rn(v, __fmul_rn(value, L.profile[along - L.lo]));
+                }
+            }
+        }
+    }
+
+    template <int S>
+    __device__ __forceinline__ void sample(int i, int ip, const float2 (&ez)[2], const float2 (&hxn)[2],
+                                           const float2 (&hyn)[2]) const {
+        const int slot = __popc(sample_mask & ((1u << (S - 1)) - 1u));
+        for (uint32_t mons = mon_mask; mons; mons &= mons - 1) {
+            const TBMon &M = p.mons[__ffs(mons) - 1];
+            const int n = M.hi - M.lo;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                if (!((own >> c) & 1u)) continue;
+                const int j = jp0 + c;
+                const float e = (c & 1) ? ez[c >> 1].y : ez[c >> 1].x;
+                if (M.normal_axis == 0) {
+                    if (ip == M.position && j >= M.lo && j < M.hi) {
+                        M.stage[(slot * 2) * n + (j - M.lo)] = e;
+                        M.stage[(slot * 2 + 1) * n + (j - M.lo)] = (c & 1) ? hyn[c >> 1].y : hyn[c >> 1].x;
+                    }
+                } else if (j == M.position && ip >= M.lo && ip < M.hi) {
+                    M.stage[(slot * 2) * n + (ip - M.lo)] = e;
+                    M.stage[(slot * 2 + 1) * n + (ip - M.lo)] = (c & 1) ? hxn[c >> 1].y : hxn[c >> 1].x;
+                }
+            }
+        }
+    }
+
+    // Step S of row i = r - S (every row of the stream window, see fdtd2d_tb.cuh).
+    template <int PH, int S>
+    __device__ __forceinline__ void stage(int r) {
+        constexpr int Q = PH ^ 1;
+        const int i = r - S;
+        const int ip = phys_row(i);
+        const int cs = (i - r_begin + tb_coef_slots(T)) % tb_coef_slots(T);
+        const float4 cbv = *reinterpret_cast<const float4 *>(sm_cb + cs * 128 + lane * 4);
+        const float2 cb[2] = {make_float2(cbv.x, cbv.y), make_float2(cbv.z, cbv.w)};
+        float2 ca[2];
+        if constexpr (CA) {
+            const float4 cav = *reinterpret_cast<const float4 *>(sm_ca + cs * 128 + lane * 4);
+            ca[0] = make_float2(cav.x, cav.y);
+            ca[1] = make_float2(cav.z, cav.w);
+        }
+        const float2(&eq)[2] = E[Q][S - 1];    // E^(S-1) of row i
+        const float2(&eu)[2] = E[PH][S - 1];   // E^(S-1) of row i + 1
+        // ---- H^S (fdtd_ez_2d_kernels.py:41-47 with da = 1)
+        const float e_right_last = __shfl_down_sync(0xffffffffu, eq[0].x, 1);
+        const float2 eright[2] = {make_float2(eq[0].y, eq[1].x), make_float2(eq[1].y, e_right_last)};
+        float2 hxn[2], hyn[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            hxn[k] = ip_sub_p(Hx[Q][S - 1][k], ip_mul(ip_mul(db2, ip_sub(eright[k], eq[k])), iyh2));
+            hyn[k] = ip_add_p(Hy[Q][S - 1][k], ip_mul(ip_mul(db2, ip_sub(eu[k], eq[k])), ixh2));
+        }
+        // ---- E^S (fdtd_ez_2d_kernels.py:107-120)
+        float hx_left_first = __shfl_up_sync(0xffffffffu, hxn[1].y, 1);
+        if (PY && wrap_lo0) hx_left_first = tb_lo_wrap(hx_left_first);
+        const float2 hxl[2] = {make_float2(hx_left_first, hxn[0].x), make_float2(hxn[0].y, hxn[1].x)};
+        float2 hyd[2] = {Hy[Q][S][0], Hy[Q][S][1]};   // H_y^S of row i - 1
+        if (PX && ip == 0) {
+#pragma unroll
+            for (int k = 0; k < 2; ++k) hyd[k] = make_float2(tb_lo_wrap(hyd[k].x), tb_lo_wrap(hyd[k].y));
+        }
+        float2 ez[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const float2 curl = ip_sub_p(ip_mul(ip_sub(hyn[k], hyd[k]), ixe2), ip_mul(ip_sub(hxn[k], hxl[k]), iye2));
+            ez[k] = ip_add_p(CA ? ip_mul(ca[k], eq[k]) : eq[k], ip_mul(cb[k], curl));
+        }
+        if (line_mask) inject<S>(ip, ez);
+        if (mon_mask && ((sample_mask >> (S - 1)) & 1u) && i >= i0 && i < i1) sample<S>(i, ip, ez, hxn, hyn);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            E[PH][S][k] = ez[k];
+            Hx[PH][S][k] = hxn[k];
+            Hy[PH][S][k] = hyn[k];
+        }
+    }
+
+    template <int PH>
+    __device__ __forceinline__ void store(int r) {
+        const int i = r - T;
+        if (i < i0 || i >= i1) return;
+        const size_t base = (size_t)phys_row(i) * (size_t)ny + jp0;
+        if (own == 0xFu) {
+            *reinterpret_cast<float4 *>(ez_out + base) =
+                make_float4(E[PH][T][0].x, E[PH][T][0].y, E[PH][T][1].x, E[PH][T][1].y);
+            *reinterpret_cast<float4 *>(hx_out + base) =
+                make_float4(Hx[PH][T][0].x, Hx[PH][T][0].y, Hx[PH][T][1].x, Hx[PH][T][1].y);
+            *reinterpret_cast<float4 *>(hy_out + base) =
+                make_float4(Hy[PH][T][0].x, Hy[PH][T][0].y, Hy[PH][T][1].x, Hy[PH][T][1].y);
+        } else if (own) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                if (!((own >> c) & 1u)) continue;
+                ez_out[base + c] = (c & 1) ? E[PH][T][c >> 1].y : E[PH][T][c >> 1].x;
+                hx_out[base + c] = (c & 1) ? Hx[PH][T][c >> 1].y : Hx[PH][T][c >> 1].x;
+                hy_out[base + c] = (c & 1) ? Hy[PH][T][c >> 1].y : Hy[PH][T][c >> 1].x;
+            }
+        }
+    }
+
+    template <int PH, int S>
+    __device__ __forceinline__ void stages_from(int r) {
+        if constexpr (S <= T) {
+            stage<PH, S>(r);
+            stages_from<PH, S + 1>(r);
+        }
+    }
+
+    template <int PH>
+    __device__ __forceinline__ void iteration(int r) {
+        if (!take_row<PH>(r)) {
+            failed = true;
+            return;
+        }
+        stages_from<PH, 1>(r);
+        store<PH>(r);
+        __syncwarp();
+        if (lane == 0 && r + TB_AHEAD + 1 <= r_end) {
+            tb_fence_proxy_async();
+            issue_row(r + TB_AHEAD + 1);
+        }
+    }
+
+    __device__ __forceinline__ void drain(int r_from) {
+        for (int R = r_from; R <= min(r_end, r_from + TB_AHEAD); ++R) {
+            const int k = R - r_begin;
+            tb_mbar_wait(sm_bar + k % tb_field_slots(), (uint32_t)((k / tb_field_slots()) & 1));
+        }
+    }
+};
+
+template <int T, bool CA, bool PX, bool PY>
+__global__ void __launch_bounds__(TB_WARPS * 32) ez2d_interior_kernel(const TBParams p) {
+    extern __shared__ __align__(16) unsigned char tb_smem[];
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x * TB_WARPS + (threadIdx.x >> 5);
+    if (w >= p.n_tiles) return;   // whole warps leave together
+    int rect = 0;
+    for (int q = 1; q < p.n_rects; ++q)
+        if (w >= p.rects[q].first_tile) rect = q;
+    const TBRect R = p.rects[rect];
+    const int t = w - R.first_tile;
+    const int tc = t % R.tiles_c, tr = t / R.tiles_c;
+
+    IPWarp<T, CA, PX, PY> W(p);
+    W.lane = lane;
+    W.nx = p.nx;
+    W.ny = p.ny;
+    W.j0 = R.c0 + tc * p.tile_w;
+    W.j1 = min(W.j0 + p.tile_w, R.c1);
+    W.i0 = R.r0 + tr * p.tile_rows;
+    W.i1 = min(W.i0 + p.tile_rows, R.r1);
+    W.r_begin = W.i0 - T;
+    W.r_end = PX ? W.i1 - 1 + T : min(p.nx - 1, W.i1 - 1 + T);
+    W.jl0 = W.j0 - 4 + lane * 4;
+    W.jp0 = PY ? tb_wrap(W.jl0, p.ny) : W.jl0;
+    W.in_grid0 = PY || (W.jl0 >= 0 && W.jl0 < p.ny);
+    W.wrap_lo0 = PY && W.jp0 == 0;
+    W.own = 0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+        if (W.jl0 + c >= W.j0 && W.jl0 + c < W.j1) W.own |= 1u << c;
+    W.db2 = make_float2(p.db_u, p.db_u);
+    W.ixh2 = make_float2(p.s_inv_dx_h, p.s_inv_dx_h);
+    W.ixe2 = make_float2(p.s_inv_dx_e, p.s_inv_dx_e);
+    W.iyh2 = make_float2(p.s_inv_dy_h, p.s_inv_dy_h);
+    W.iye2 = make_float2(p.s_inv_dy_e, p.s_inv_dy_e);
+    W.ez_in = p.ez_in;
+    W.hx_in = p.hx_in;
+    W.hy_in = p.hy_in;
+    W.cbp = p.cb;
+    W.cap = p.ca;
+    W.ez_out = p.ez_out;
+    W.hx_out = p.hx_out;
+    W.hy_out = p.hy_out;
+    W.sample_mask = p.sample_mask;
+    // line sources that can reach the cone, flux lines among the outputs
+    {
+        const int c0 = W.j0 - 4, c1 = W.j0 + 124;
+        uint32_t lm = 0, mm = 0;
+        for (int l = 0; l < p.n_lines; ++l) {
+            const TBLine &L = p.lines[l];
+            bool hit;
+            if (PX || PY) hit = true;
+            else if (L.axis == 0) hit = L.position >= c0 && L.position < c1 && L.hi > W.r_begin && L.lo <= W.r_end;
+            else hit = L.position >= W.r_begin && L.position <= W.r_end && L.hi > c0 && L.lo < c1;
+            if (hit) lm |= 1u << l;
+        }
+        for (int q = 0; q < p.n_mons; ++q) {
+            const TBMon &M = p.mons[q];
+            const bool hit = M.normal_axis == 0
+                                 ? (M.position >= W.i0 && M.position < W.i1 && M.hi > W.j0 && M.lo < W.j1)
+                                 : (M.position >= W.j0 && M.position < W.j1 && M.hi > W.i0 && M.lo < W.i1);
+            if (hit) mm |= 1u << q;
+        }
+        W.line_mask = lm;
+        W.mon_mask = p.sample_mask ? mm : 0u;
+    }
+#pragma unroll
+    for (int ph = 0; ph < 2; ++ph)
+#pragma unroll
+        for (int s = 0; s <= T; ++s)
+#pragma unroll
+            for (int k = 0; k < 2; ++k) W.E[ph][s][k] = W.Hx[ph][s][k] = W.Hy[ph][s][k] = make_float2(0.0f, 0.0f);
+
+    unsigned char *mine = tb_smem + (threadIdx.x >> 5) * tb_warp_smem_bytes(T, CA);
+    W.sm_fields = reinterpret_cast<float *>(mine);
+    W.sm_cb = W.sm_fields + tb_field_slots() * 384;
+    W.sm_ca = W.sm_cb + tb_coef_slots(T) * 128;
+    W.sm_bar = reinterpret_cast<uint64_t *>(W.sm_cb + tb_coef_slots(T) * 128 * (CA ? 2 : 1));
+    W.row_bytes = W.window(nullptr, nullptr, nullptr, false);
+    if (lane == 0) {
+        for (int q = 0; q < tb_field_slots(); ++q) tb_mbar_init(W.sm_bar + q, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        tb_fence_proxy_async();
+        for (int Rr = W.r_begin; Rr <= min(W.r_end, W.r_begin + TB_AHEAD); ++Rr) W.issue_row(Rr);
+    }
+    __syncwarp();
+    const int r_last = W.r_end + T;
+    for (int r = W.r_begin; r <= r_last; r += 2) {
+        W.template iteration<0>(r);
+        if (W.failed) {
+            if (lane == 0) atomicExch(p.err, 1);
+            W.drain(r);
+            return;
+        }
+        if (r + 1 <= r_last) {
+            W.template iteration<1>(r + 1);
+            if (W.failed) {
+                if (lane == 0) atomicExch(p.err, 1);
+                W.drain(r + 1);
+                return;
+            }
+        }
+    }
+}

@@ -20,6 +20,14 @@
 // neighbour as f * cos + f * sin with cos 1, sin 0 (a real-only engine) the same expression is evaluated, so even the
 // signs of zeros match.
 //
+// Row staging (interior variant).  Rows are brought into a per-warp shared-memory ring by the copy engine: lane 0
+// issues one 1D bulk copy (cp.async.bulk, TMA) per array and row segment, TB_AHEAD rows ahead of the row being
+// consumed, completing on an mbarrier per ring slot; the fields of a row are read back once, the coefficient rows (cb,
+// ca) are read by stages 1..T from a ring deep enough to keep them until stage T has used them.  The copies occupy no
+// registers while in flight, so the loads of the next rows overlap T stages of arithmetic of several rows.  Before a
+// slot is refilled the warp synchronises and lane 0 orders the lanes' reads before the copy engine's writes with
+// fence.proxy.async.  Waits are bounded: a wait that runs out sets the engine's error flag and the warp stops.
+//
 // Sources and monitors.  Line sources are added after E and its CPML, per step, in add order, skipped when the step's
 // float32 value is 0 (core/sources.py:221-229).  On a DFT sample step the owning warp copies the flux line's E_z and
 // tangential H into a small staging buffer; a separate kernel accumulates the running DFTs in sample order
@@ -34,6 +42,8 @@
 #define TB_MAX_RECTS 4
 #define TB_WARPS 4
 #define TB_MAX_T 4
+#define TB_AHEAD 3                        // rows staged ahead of the row being consumed (interior variant)
+#define TB_WAIT_NS 2000000000ull          // bound of one mbarrier wait (2 s): then the error flag is set
 
 struct TBLine {
     int32_t axis, position, lo, hi;   // axis 0: cells (i, position), i in [lo, hi); axis 1: cells (position, j)
@@ -75,11 +85,77 @@ struct TBParams {
     int32_t n_rects;
     TBRect rects[TB_MAX_RECTS];
     int32_t tile_w, tile_rows, n_tiles;
+    int32_t *err;   // set to 1 when a bounded wait runs out (read by the host after the launch)
 };
 
+// Shared memory of one warp of the interior variant: field ring (TB_AHEAD + 1 slots x E, H_x, H_y rows), coefficient
+// rings (T + TB_AHEAD + 1 slots of cb, and of ca when per-cell), one mbarrier per field slot.
+__host__ __device__ constexpr int tb_field_slots() { return TB_AHEAD + 1; }
+__host__ __device__ constexpr int tb_coef_slots(int T) { return T + TB_AHEAD + 1; }
+__host__ __device__ constexpr int tb_warp_smem_bytes(int T, bool ca) {
+    return (tb_field_slots() * 3 + tb_coef_slots(T) * (ca ? 2 : 1)) * 128 * 4 + tb_field_slots() * 8;
+}
+
+__device__ __forceinline__ uint32_t tb_smem_addr(const void *ptr) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(ptr));
+}
+
+__device__ __forceinline__ void tb_mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tb_smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void tb_mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tb_smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool tb_mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(tb_smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ uint64_t tb_globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for the mbarrier phase of `parity`, at most TB_WAIT_NS; warp-uniform result.
+__device__ __forceinline__ bool tb_mbar_wait(uint64_t *bar, uint32_t parity) {
+    bool done = tb_mbar_try_wait(bar, parity);
+    if (!done) {
+        const uint64_t t0 = tb_globaltimer();
+        while (!(done = tb_mbar_try_wait(bar, parity)))
+            if (tb_globaltimer() - t0 > TB_WAIT_NS) break;
+    }
+    return __all_sync(0xffffffffu, done);
+}
+
+// One bulk copy global -> shared completing on `bar` (16-byte aligned addresses, bytes a multiple of 16).
+__device__ __forceinline__ void tb_bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     tb_smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(tb_smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tb_fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// a mod n for the few periods a stream index can be off (no integer division: the streams stay within a couple of
+// periods of [0, n)).
 __device__ __forceinline__ int tb_wrap(int a, int n) {
-    int r = a % n;
-    return r < 0 ? r + n : r;
+    while (a < 0) a += n;
+    while (a >= n) a -= n;
+    return a;
 }
 
 // open_sol's wrapped lo-side neighbour of a real-only engine: f * wrap_cos - f_partner * wrap_sin with cos 1, sin 0
@@ -101,15 +177,22 @@ struct TBState {
     float pye[2][T + 1][GEN ? C : 1];
 };
 
-// Per-thread column facts.
+// Per-thread column facts.  An interior thread's C columns are contiguous and aligned, so they share one base
+// column, one in-grid flag and one wrap flag (only the first can be column 0); a mask holds which are outputs.
 template <int C>
 struct TBCols {
-    int jp[C];          // physical column
-    bool in_grid[C];    // a real cell (false: outside a non-periodic grid)
-    bool own[C];        // inside this tile's output columns
+    int jp0;            // physical column of the first column (jp0 + c: the others, C > 1)
+    int jps[1];         // physical column (C = 1: the general variant)
+    bool in_grid0;      // the columns are real cells (false: outside a non-periodic grid)
+    uint32_t own;       // bit c: column c is one of this tile's output columns
+    bool wrap_lo0;      // the first column is column 0 of a periodic y axis
     float inv_y_h[C], inv_y_e[C];
-    // y-side CPML: side (2 / 3) and slab index of the H and E column, -1 when none
+    // y-side CPML (general variant): side (2 / 3) and slab index of the H and E column, -1 when none
     int yh_side[C], yh_k[C], ye_side[C], ye_k[C];
+    __device__ __forceinline__ int jp(int c) const { return C == 1 ? jps[0] : jp0 + c; }
+    __device__ __forceinline__ bool in_grid(int c) const { return in_grid0; }
+    __device__ __forceinline__ bool owns(int c) const { return (own >> c) & 1u; }
+    __device__ __forceinline__ bool wrap_lo(int c) const { return c == 0 && wrap_lo0; }
 };
 
 // Which x-side (rows) or y-side (columns) CPML slab holds H row / E row `g` along an axis of n cells, and its index.
@@ -127,8 +210,8 @@ template <int C>
 __device__ __forceinline__ void tb_load_row(const float *__restrict__ src, size_t row_base, const TBCols<C> &cols,
                                             bool vec, float (&out)[C]) {
     if (C == 4 && vec) {
-        if (cols.in_grid[0]) {
-            const float4 v = __ldg(reinterpret_cast<const float4 *>(src + row_base + cols.jp[0]));
+        if (cols.in_grid0) {
+            const float4 v = __ldg(reinterpret_cast<const float4 *>(src + row_base + cols.jp(0)));
             out[0] = v.x;
             out[1] = v.y;
             out[2] = v.z;
@@ -139,7 +222,7 @@ __device__ __forceinline__ void tb_load_row(const float *__restrict__ src, size_
         }
     } else {
 #pragma unroll
-        for (int c = 0; c < C; ++c) out[c] = cols.in_grid[c] ? __ldg(src + row_base + cols.jp[c]) : 0.0f;
+        for (int c = 0; c < C; ++c) out[c] = cols.in_grid(c) ? __ldg(src + row_base + cols.jp(c)) : 0.0f;
     }
 }
 
@@ -161,6 +244,14 @@ struct TBWarp {
     uint32_t sample_mask;
     uint32_t line_mask;   // line sources whose cells can fall in this tile's cone
     uint32_t mon_mask;    // flux lines with cells among this tile's outputs
+    // interior variant: this warp's staging ring
+    static constexpr bool BULK = !GEN;
+    float *sm_fields = nullptr, *sm_cb = nullptr, *sm_ca = nullptr;
+    uint64_t *sm_bar = nullptr;
+    int win0 = 0;          // first column of the 128-column window (stream coordinates)
+    uint32_t row_bytes = 0;  // bytes one array's row window brings in
+    int lane = 0;
+    bool failed = false;
 
     __device__ __forceinline__ TBWarp(const TBParams &params)
         : p(params), nx(params.nx), ny(params.ny), npml(params.npml), cpml_mask(params.cpml_mask),
@@ -172,6 +263,66 @@ struct TBWarp {
 
     __device__ __forceinline__ int phys_row(int i) const { return px ? tb_wrap(i, nx) : i; }
 
+    // Bulk copies of one array's 128-column window of physical row rp into `dst` (lane 0).  The window wraps on a
+    // periodic y axis (several segments when ny < 128); on a non-periodic axis the part beyond the grid is not copied
+    // (those columns lie outside every output's cone).
+    __device__ __forceinline__ void copy_window(float *dst, const float *src_row, uint64_t *bar) const {
+        int remaining = 128, d = 0, col = py ? tb_wrap(win0, ny) : win0;
+        while (remaining > 0 && col < ny) {
+            const int len = min(remaining, ny - col);
+            tb_bulk_g2s(dst + d, src_row + col, (uint32_t)len * 4u, bar);
+            d += len;
+            remaining -= len;
+            if (!py) break;
+            col = 0;
+        }
+    }
+
+    __device__ __forceinline__ uint32_t window_bytes() const {
+        uint32_t bytes = 0;
+        int remaining = 128, col = py ? tb_wrap(win0, ny) : win0;
+        while (remaining > 0 && col < ny) {
+            const int len = min(remaining, ny - col);
+            bytes += (uint32_t)len * 4u;
+            remaining -= len;
+            if (!py) break;
+            col = 0;
+        }
+        return bytes;
+    }
+
+    // Lane 0: stage stream row R (fields into field slot, coefficients into coefficient slots).
+    __device__ __forceinline__ void issue_row(int R) {
+        const int k = R - r_begin;
+        const int fs = k % tb_field_slots(), cs = k % tb_coef_slots(T);
+        uint64_t *bar = sm_bar + fs;
+        const size_t base = (size_t)phys_row(R) * (size_t)ny;
+        tb_mbar_expect_tx(bar, row_bytes * (CA ? 5u : 4u));
+        float *f = sm_fields + fs * 384;
+        copy_window(f, ez_in + base, bar);
+        copy_window(f + 128, hx_in + base, bar);
+        copy_window(f + 256, hy_in + base, bar);
+        copy_window(sm_cb + cs * 128, cbp + base, bar);
+        if (CA) copy_window(sm_ca + cs * 128, cap + base, bar);
+    }
+
+    // All lanes: wait until stream row R has landed (R <= r_end), then read its fields into the stage-0 registers
+    // (R > r_end: the slot's last row, long landed; the values feed no output).
+    template <int PH>
+    __device__ __forceinline__ bool take_row(int R) {
+        const int k = R - r_begin;
+        const int fs = k % tb_field_slots();
+        if (R <= r_end && !tb_mbar_wait(sm_bar + fs, (uint32_t)((k / tb_field_slots()) & 1))) return false;
+        const float *f = sm_fields + fs * 384 + lane * 4;
+        const float4 e = *reinterpret_cast<const float4 *>(f);
+        const float4 hx = *reinterpret_cast<const float4 *>(f + 128);
+        const float4 hy = *reinterpret_cast<const float4 *>(f + 256);
+        st.E[PH][0][0] = e.x; st.E[PH][0][1] = e.y; st.E[PH][0][2] = e.z; st.E[PH][0][3] = e.w;
+        st.Hx[PH][0][0] = hx.x; st.Hx[PH][0][1] = hx.y; st.Hx[PH][0][2] = hx.z; st.Hx[PH][0][3] = hx.w;
+        st.Hy[PH][0][0] = hy.x; st.Hy[PH][0][1] = hy.y; st.Hy[PH][0][2] = hy.z; st.Hy[PH][0][3] = hy.w;
+        return true;
+    }
+
     // Stage 0 of stream row r: fields (and psi^0 of CPML cells) from the input buffers.
     template <int PH>
     __device__ __forceinline__ void load_row(int r) {
@@ -181,17 +332,17 @@ struct TBWarp {
         tb_load_row<C>(hx_in, base, cols, vec, st.Hx[PH][0]);
         tb_load_row<C>(hy_in, base, cols, vec, st.Hy[PH][0]);
         // the coefficient rows of row r are first read by stage 1 of the next iteration: pull them into L1 now
-        if (cols.in_grid[0]) {
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(cbp + base + cols.jp[0]));
-            if (CA) asm volatile("prefetch.global.L1 [%0];" ::"l"(cap + base + cols.jp[0]));
+        if (cols.in_grid0) {
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(cbp + base + cols.jp(0)));
+            if (CA) asm volatile("prefetch.global.L1 [%0];" ::"l"(cap + base + cols.jp(0)));
         }
         if constexpr (GEN) {
             int xh_side, xh_k, xe_side, xe_k;
             tb_cpml_slot(rp, nx, npml, cpml_mask & 1, cpml_mask & 2, 0, 1, xh_side, xh_k, xe_side, xe_k);
 #pragma unroll
             for (int c = 0; c < C; ++c) {
-                const bool g = cols.in_grid[c];
-                const int j = cols.jp[c];
+                const bool g = cols.in_grid(c);
+                const int j = cols.jp(c);
                 st.pxh[PH][0][c] = (g && xh_side >= 0) ? p.psi_h_in[xh_side][(size_t)xh_k * ny + j] : 0.0f;
                 st.pxe[PH][0][c] = (g && xe_side >= 0) ? p.psi_e_in[xe_side][(size_t)xe_k * ny + j] : 0.0f;
                 st.pyh[PH][0][c] = (g && cols.yh_side[c] >= 0)
@@ -207,14 +358,27 @@ struct TBWarp {
     __device__ __forceinline__ void stage(int r) {
         constexpr int Q = PH ^ 1;   // last iteration's arrays
         const int i = r - S;
-        if (i < r_begin || i > r_end) return;
+        // The general variant skips rows outside the stream (its loads index global rows).  The interior variant
+        // always computes: out-of-stream rows only read in-bounds ring slots and produce values no output uses, and
+        // an unconditional pipeline keeps only one phase of the arrays alive across iterations.
+        if (GEN && (i < r_begin || i > r_end)) return;
         const int ip = phys_row(i);
         const size_t base = (size_t)ip * (size_t)ny;
 
         float cb[C], ca[C], da[C], db[C];
-        tb_load_row<C>(cbp, base, cols, vec, cb);
-        if constexpr (CA) {
-            tb_load_row<C>(cap, base, cols, vec, ca);
+        if constexpr (BULK) {
+            const int cs = (i - r_begin + tb_coef_slots(T)) % tb_coef_slots(T);   // i >= r_begin - T
+            const float4 v = *reinterpret_cast<const float4 *>(sm_cb + cs * 128 + lane * 4);
+            cb[0] = v.x; cb[1] = v.y; cb[2] = v.z; cb[3] = v.w;
+            if constexpr (CA) {
+                const float4 w = *reinterpret_cast<const float4 *>(sm_ca + cs * 128 + lane * 4);
+                ca[0] = w.x; ca[1] = w.y; ca[2] = w.z; ca[3] = w.w;
+            }
+        } else {
+            tb_load_row<C>(cbp, base, cols, vec, cb);
+            if constexpr (CA) {
+                tb_load_row<C>(cap, base, cols, vec, ca);
+            }
         }
         if constexpr (GEN) {
             if (dap) {
@@ -252,7 +416,7 @@ struct TBWarp {
             const float e_up = st.E[PH][S - 1][c];
             const float hx_old = st.Hx[Q][S - 1][c];
             const float hy_old = st.Hy[Q][S - 1][c];
-            const int j = cols.jp[c];
+            const int j = cols.jp(c);
             // H_x: every column but the last of a non-periodic y axis (whose face is never updated)
             if (GEN && !py && j == ny - 1) {
                 hxn[c] = hx_old;
@@ -296,23 +460,24 @@ struct TBWarp {
 
         // ---- E^S of row i (fdtd_ez_2d_kernels.py:107-120), E-row CPML x then y sides, line sources
         const float hx_left_first = __shfl_up_sync(0xffffffffu, hxn[C - 1], 1);
+        const bool wrap_row = px && ip == 0;   // row 0 of a periodic x axis: its lo neighbour is the last row
 #pragma unroll
         for (int c = 0; c < C; ++c) {
-            const int j = cols.jp[c];
+            const int j = cols.jp(c);
             float hx_left = c > 0 ? hxn[c - 1] : hx_left_first;
             float hy_down = st.Hy[Q][S][c];   // H_y^S of row i - 1
             float curl;
             if (GEN && !px && ip == 0) {
                 curl = hyn[c] * inv_x_e;
             } else {
-                if (px && ip == 0) hy_down = tb_lo_wrap(hy_down);
+                if (wrap_row) hy_down = tb_lo_wrap(hy_down);
                 curl = (hyn[c] - hy_down) * inv_x_e;
             }
             const float inv_y_e = GEN ? cols.inv_y_e[c] : s_inv_dy_e;
             if (GEN && !py && j == 0) {
                 curl -= hxn[c] * inv_y_e;
             } else {
-                if (py && j == 0) hx_left = tb_lo_wrap(hx_left);
+                if (cols.wrap_lo(c)) hx_left = tb_lo_wrap(hx_left);
                 curl -= (hxn[c] - hx_left) * inv_y_e;
             }
             const float e_old = st.E[Q][S - 1][c];
@@ -338,7 +503,7 @@ struct TBWarp {
                 const int l = __ffs(lines) - 1;
                 const TBLine &L = p.lines[l];
                 const int along = L.axis == 0 ? ip : j, across = L.axis == 0 ? j : ip;
-                if (across == L.position && along >= L.lo && along < L.hi && cols.in_grid[c]) {
+                if (across == L.position && along >= L.lo && along < L.hi && cols.in_grid(c)) {
                     const float value = p.line_values[(size_t)l * p.values_stride + p.k0 + (S - 1)];
                     if (value != 0.0f) v += value * L.profile[along - L.lo];
                 }
@@ -357,8 +522,8 @@ struct TBWarp {
                 const int n = M.hi - M.lo;
 #pragma unroll
                 for (int c = 0; c < C; ++c) {
-                    if (!cols.own[c]) continue;
-                    const int j = cols.jp[c];
+                    if (!cols.owns(c)) continue;
+                    const int j = cols.jp(c);
                     if (M.normal_axis == 0) {
                         if (ip == M.position && j >= M.lo && j < M.hi) {
                             M.stage[(slot * 2) * n + (j - M.lo)] = st.E[PH][S][c];
@@ -380,23 +545,20 @@ struct TBWarp {
         if (i < i0 || i >= i1) return;
         const int ip = phys_row(i);
         const size_t base = (size_t)ip * (size_t)ny;
-        bool all_own = true;
-#pragma unroll
-        for (int c = 0; c < C; ++c) all_own = all_own && cols.own[c];
-        if (C == 4 && vec && all_own) {
-            *reinterpret_cast<float4 *>(ez_out + base + cols.jp[0]) =
+        if (C == 4 && vec && cols.own == 0xFu) {
+            *reinterpret_cast<float4 *>(ez_out + base + cols.jp(0)) =
                 make_float4(st.E[PH][T][0], st.E[PH][T][1], st.E[PH][T][2], st.E[PH][T][3]);
-            *reinterpret_cast<float4 *>(hx_out + base + cols.jp[0]) =
+            *reinterpret_cast<float4 *>(hx_out + base + cols.jp(0)) =
                 make_float4(st.Hx[PH][T][0], st.Hx[PH][T][1], st.Hx[PH][T][2], st.Hx[PH][T][3]);
-            *reinterpret_cast<float4 *>(hy_out + base + cols.jp[0]) =
+            *reinterpret_cast<float4 *>(hy_out + base + cols.jp(0)) =
                 make_float4(st.Hy[PH][T][0], st.Hy[PH][T][1], st.Hy[PH][T][2], st.Hy[PH][T][3]);
-        } else {
+        } else if (cols.own) {
 #pragma unroll
             for (int c = 0; c < C; ++c) {
-                if (!cols.own[c]) continue;
-                ez_out[base + cols.jp[c]] = st.E[PH][T][c];
-                hx_out[base + cols.jp[c]] = st.Hx[PH][T][c];
-                hy_out[base + cols.jp[c]] = st.Hy[PH][T][c];
+                if (!cols.owns(c)) continue;
+                ez_out[base + cols.jp(c)] = st.E[PH][T][c];
+                hx_out[base + cols.jp(c)] = st.Hx[PH][T][c];
+                hy_out[base + cols.jp(c)] = st.Hy[PH][T][c];
             }
         }
         if constexpr (GEN) {
@@ -404,8 +566,8 @@ struct TBWarp {
             tb_cpml_slot(ip, nx, npml, cpml_mask & 1, cpml_mask & 2, 0, 1, xh_side, xh_k, xe_side, xe_k);
 #pragma unroll
             for (int c = 0; c < C; ++c) {
-                if (!cols.own[c]) continue;
-                const int j = cols.jp[c];
+                if (!cols.owns(c)) continue;
+                const int j = cols.jp(c);
                 if (xh_side >= 0) p.psi_h_out[xh_side][(size_t)xh_k * ny + j] = st.pxh[PH][T][c];
                 if (xe_side >= 0) p.psi_e_out[xe_side][(size_t)xe_k * ny + j] = st.pxe[PH][T][c];
                 if (cols.yh_side[c] >= 0)
@@ -420,7 +582,7 @@ struct TBWarp {
     __device__ __forceinline__ void stages_from(int r) {
         if constexpr (S <= T) {
             stage<PH, S>(r);
-            if constexpr (S == 1) {
+            if constexpr (S == 1 && !BULK) {
                 // stage 1 was the last reader of last iteration's stage-0 row: prefetch row r + 1 into it
                 if (r + 1 <= r_end) load_row<PH ^ 1>(r + 1);
             }
@@ -430,13 +592,36 @@ struct TBWarp {
 
     template <int PH>
     __device__ __forceinline__ void iteration(int r) {
+        if constexpr (BULK) {
+            if (!take_row<PH>(r)) {
+                failed = true;
+                return;
+            }
+        }
         stages_from<PH, 1>(r);
         store<PH>(r);
+        if constexpr (BULK) {
+            // the field slot of row r and the coefficient slot of row r - T are free: refill with row r + AHEAD + 1
+            __syncwarp();
+            if (lane == 0 && r + TB_AHEAD + 1 <= r_end) {
+                tb_fence_proxy_async();
+                issue_row(r + TB_AHEAD + 1);
+            }
+        }
+    }
+
+    // After a failed wait: wait (bounded) for the copies still in flight so none lands after the warp has left.
+    __device__ __forceinline__ void drain(int r_from) {
+        for (int R = r_from; R <= min(r_end, r_from + TB_AHEAD); ++R) {
+            const int k = R - r_begin;
+            tb_mbar_wait(sm_bar + k % tb_field_slots(), (uint32_t)((k / tb_field_slots()) & 1));
+        }
     }
 };
 
 template <int T, int C, bool GEN, bool CA>
 __global__ void __launch_bounds__(TB_WARPS * 32) ez2d_tb_kernel(const TBParams p) {
+    extern __shared__ __align__(16) unsigned char tb_smem[];
     const int lane = threadIdx.x & 31;
     const int w = blockIdx.x * TB_WARPS + (threadIdx.x >> 5);
     if (w >= p.n_tiles) return;   // whole warps leave together (the shuffles below need all 32 lanes)
@@ -481,22 +666,30 @@ __global__ void __launch_bounds__(TB_WARPS * 32) ez2d_tb_kernel(const TBParams p
         W.line_mask = lm;
         W.mon_mask = p.sample_mask ? mm : 0u;
     }
+    {
+        const int jl0 = j0 - HL + lane * C;   // first loaded column of this thread (stream coordinates)
+        W.cols.in_grid0 = p.py || (jl0 >= 0 && jl0 < p.ny);
+        W.cols.jp0 = p.py ? tb_wrap(jl0, p.ny) : jl0;
+        W.cols.wrap_lo0 = p.py && W.cols.jp0 == 0;
+        W.cols.own = 0;
 #pragma unroll
-    for (int c = 0; c < C; ++c) {
-        const int jl = j0 - HL + lane * C + c;
-        W.cols.in_grid[c] = p.py || (jl >= 0 && jl < p.ny);   // (p.py: wrapped)
-        W.cols.jp[c] = p.py ? tb_wrap(jl, p.ny) : jl;
-        W.cols.own[c] = jl >= j0 && jl < j1;
-        const int jc = W.cols.in_grid[c] ? W.cols.jp[c] : 0;
-        if (GEN) {
-            W.cols.inv_y_h[c] = __ldg(p.inv_dy_h + jc);
-            W.cols.inv_y_e[c] = __ldg(p.inv_dy_e + jc);
-            tb_cpml_slot(W.cols.in_grid[c] ? jc : -1, p.ny, p.npml, p.cpml_mask & 4, p.cpml_mask & 8, 2, 3,
-                         W.cols.yh_side[c], W.cols.yh_k[c], W.cols.ye_side[c], W.cols.ye_k[c]);
-        } else {
-            W.cols.inv_y_h[c] = W.cols.inv_y_e[c] = 0.0f;
-            W.cols.yh_side[c] = W.cols.ye_side[c] = -1;
-            W.cols.yh_k[c] = W.cols.ye_k[c] = 0;
+        for (int c = 0; c < C; ++c) {
+            const int jl = jl0 + c;
+            if (jl >= j0 && jl < j1) W.cols.own |= 1u << c;
+            const int jpc = p.py ? tb_wrap(jl, p.ny) : jl;
+            if (c == 0) W.cols.jps[0] = jpc;
+            const bool g = p.py || (jl >= 0 && jl < p.ny);
+            const int jc = g ? jpc : 0;
+            if (GEN) {
+                W.cols.inv_y_h[c] = __ldg(p.inv_dy_h + jc);
+                W.cols.inv_y_e[c] = __ldg(p.inv_dy_e + jc);
+                tb_cpml_slot(g ? jc : -1, p.ny, p.npml, p.cpml_mask & 4, p.cpml_mask & 8, 2, 3, W.cols.yh_side[c],
+                             W.cols.yh_k[c], W.cols.ye_side[c], W.cols.ye_k[c]);
+            } else {
+                W.cols.inv_y_h[c] = W.cols.inv_y_e[c] = 0.0f;
+                W.cols.yh_side[c] = W.cols.ye_side[c] = -1;
+                W.cols.yh_k[c] = W.cols.ye_k[c] = 0;
+            }
         }
     }
     // Pipeline registers start at 0 (a non-periodic first row reads no H_y below it; the rest is outside the cone).
@@ -509,11 +702,41 @@ __global__ void __launch_bounds__(TB_WARPS * 32) ez2d_tb_kernel(const TBParams p
                 W.st.E[ph][s][c] = W.st.Hx[ph][s][c] = W.st.Hy[ph][s][c] = 0.0f;
                 if (GEN) W.st.pxh[ph][s][c] = W.st.pxe[ph][s][c] = W.st.pyh[ph][s][c] = W.st.pye[ph][s][c] = 0.0f;
             }
-    W.template load_row<0>(W.r_begin);
+    W.lane = lane;
+    if constexpr (!GEN) {
+        unsigned char *mine = tb_smem + (threadIdx.x >> 5) * tb_warp_smem_bytes(T, CA);
+        W.sm_fields = reinterpret_cast<float *>(mine);
+        W.sm_cb = W.sm_fields + tb_field_slots() * 384;
+        W.sm_ca = W.sm_cb + tb_coef_slots(T) * 128;
+        W.sm_bar = reinterpret_cast<uint64_t *>(W.sm_cb + tb_coef_slots(T) * 128 * (CA ? 2 : 1));
+        W.win0 = j0 - 4;
+        W.row_bytes = W.window_bytes();
+        if (lane == 0) {
+            for (int q = 0; q < tb_field_slots(); ++q) tb_mbar_init(W.sm_bar + q, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            tb_fence_proxy_async();   // the copy engine sees the initialised barriers
+            for (int R = W.r_begin; R <= min(W.r_end, W.r_begin + TB_AHEAD); ++R) W.issue_row(R);
+        }
+        __syncwarp();
+    } else {
+        W.template load_row<0>(W.r_begin);
+    }
     const int r_last = W.r_end + T;
     for (int r = W.r_begin; r <= r_last; r += 2) {
         W.template iteration<0>(r);
-        if (r + 1 <= r_last) W.template iteration<1>(r + 1);
+        if (W.failed) {
+            if (lane == 0) atomicExch(p.err, 1);
+            W.drain(r);
+            return;
+        }
+        if (r + 1 <= r_last) {
+            W.template iteration<1>(r + 1);
+            if (W.failed) {
+                if (lane == 0) atomicExch(p.err, 1);
+                W.drain(r + 1);
+                return;
+            }
+        }
     }
 }
 

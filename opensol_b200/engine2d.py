@@ -22,7 +22,7 @@ class FDTDEngine2D_Ez:
     """Device engine of one 2D E_z simulation (real fields, CPML and periodic faces)."""
 
     polarization = 'ez'
-    KERNEL_KINDS = {0: 'ez2d_tb_kernel (interior)', 1: 'ez2d_tb_kernel (general)', 2: 'ez2d_flux_staged_kernel',
+    KERNEL_KINDS = {0: 'ez2d_interior_kernel', 1: 'ez2d_tb_kernel (general)', 2: 'ez2d_flux_staged_kernel',
                     3: 'ez2d_h_kernel+ez2d_e_kernel'}
 
     def __init__(self, domain, boundary_config, device: int = 0):
@@ -47,7 +47,7 @@ class FDTDEngine2D_Ez:
         self._materials_version = None
         self.sample_interval = 1
         self._sample_interval_sent = None
-        self.variant, self.steps_per_launch, self.tile_rows = 1, 4, 128
+        self.variant, self.steps_per_launch, self.tile_rows = 1, 3, 128
         self._config_sent = None
         self.h2d_bytes = 0   # host-to-device bytes this engine has uploaded (setup, materials, chunk tables)
 
@@ -138,8 +138,8 @@ class FDTDEngine2D_Ez:
 
     def configure(self, variant=None, steps_per_launch=None, tile_rows=None):
         """Kernel choice (results are bit-identical for every choice): variant 1 = temporally blocked kernels
-        advancing steps_per_launch (1..4) steps per launch with tile_rows rows per interior tile; variant 0 = one H
-        and one E kernel per step."""
+        advancing steps_per_launch (1..4, default 3) steps per launch with tile_rows rows per interior tile; variant
+        2 = the same with the general kernel on every cell; variant 0 = one H and one E kernel per step."""
         if variant is not None:
             self.variant = int(variant)
         if steps_per_launch is not None:

@@ -74,7 +74,8 @@ def test_cases_bit_exact_against_oracle(spec):
 
 # (variant, steps per launch, interior tile rows): per-step kernels, and the blocked kernels at every T with tile
 # heights from a few rows (many ragged tiles, tiles shorter than T) to 128
-KERNEL_CONFIGS = [(0, 1, 128), (1, 1, 128), (1, 2, 32), (1, 3, 7), (1, 4, 128), (1, 4, 3)]
+KERNEL_CONFIGS = [(0, 1, 128), (1, 1, 128), (1, 2, 32), (1, 3, 7), (1, 3, 128), (1, 4, 128), (1, 4, 3), (2, 3, 128),
+                  (2, 4, 16)]
 
 
 @pytest.mark.parametrize('config', KERNEL_CONFIGS, ids=[f'v{v}_T{t}_rows{r}' for v, t, r in KERNEL_CONFIGS])
@@ -123,13 +124,14 @@ def test_interior_and_general_kernels_both_run():
     sim = ob.Simulation(**args, verbose=False)
     workloads.apply(sim, workloads.roofline_2d_ops())
     sim.em.finalize()
+    sim.em.engine.configure(steps_per_launch=4)
     cells, tiles_in, tiles_gen = sim.em.engine.plan_info(4)
     assert tiles_in > 0 and tiles_gen > 0
     assert cells > 0.98 * sim.grid.nx * sim.grid.ny
     sim.em.engine.set_profiling(True)
     sim.run(n_steps=52, verbose=False)
     times = sim.em.engine.kernel_times()
-    assert times['ez2d_tb_kernel (interior)'][1] == 13 and times['ez2d_tb_kernel (general)'][1] == 13
+    assert times['ez2d_interior_kernel'][1] == 13 and times['ez2d_tb_kernel (general)'][1] == 13
     assert times['ez2d_flux_staged_kernel'][1] == 2 * 4
     sim.clear()
 
