@@ -127,9 +127,9 @@ int os_fdtd2d_launch_count(OsFdtd2D *h, int64_t *launches);
 int os_fdtd2d_set_profiling(OsFdtd2D *h, int32_t on);
 
 /* Autotuner of the interior tile height: times `repeats` launches of steps_per_launch steps for every candidate
- * rows-per-tile on the live fields (trial launches write the idle buffer set, which is not swapped in, so the
- * simulation state is unchanged), keeps the fastest as the engine's tile_rows and returns it with its time per
- * launch.  No open_sol counterpart. */
+ * rows-per-tile, in three interleaved rounds (each candidate keeps its fastest), on the live fields (trial launches
+ * write the idle buffer set, which is not swapped in, so the simulation state is unchanged), keeps the fastest as
+ * the engine's tile_rows and returns it with its time per launch.  No open_sol counterpart. */
 int os_fdtd2d_autotune(OsFdtd2D *h, int32_t steps_per_launch, const int32_t *candidates, int32_t n_candidates,
                        int32_t repeats, int32_t *best_rows, float *best_ms);
 

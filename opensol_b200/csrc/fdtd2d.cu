@@ -785,7 +785,11 @@ extern "C" int os_fdtd2d_autotune(OsFdtd2D *h, int32_t steps_per_launch, const i
     float best = -1.0f;
     int best_r = saved_rows;
     int rc = OS_OK;
-    for (int c = 0; c < n_candidates && rc == OS_OK; ++c) {
+    // candidates are timed in interleaved rounds and each keeps its fastest round, so that a slow spell of the
+    // device during one candidate's trial does not decide the choice
+    constexpr int kRounds = 3;
+    for (int c_all = 0; c_all < kRounds * n_candidates && rc == OS_OK; ++c_all) {
+        const int c = c_all % n_candidates;
         if (candidates[c] < 1) continue;
         h->tile_rows = candidates[c];
         TBParams interior{}, general{};
@@ -799,7 +803,8 @@ extern "C" int os_fdtd2d_autotune(OsFdtd2D *h, int32_t steps_per_launch, const i
             // trial launches read the live buffers and write the idle ones, which are never swapped in
             bind_buffers(h, *q, h->cur, h->cur ^ 1);
         }
-        for (int w = 0; w < 2 && rc == OS_OK; ++w) rc = launch_tb_any(h, steps_per_launch, interior, general, has_interior);
+        for (int w = 0; w < (c_all < n_candidates ? 2 : 1) && rc == OS_OK; ++w)
+            rc = launch_tb_any(h, steps_per_launch, interior, general, has_interior);
         if (rc != OS_OK) break;
         if (cudaEventRecord(t0, h->stream) != cudaSuccess) { rc = OS_ERR_CUDA; break; }
         for (int k = 0; k < std::max(1, repeats) && rc == OS_OK; ++k)

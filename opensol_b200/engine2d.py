@@ -151,7 +151,7 @@ class FDTDEngine2D_Ez:
 
     AUTOTUNE_ROWS = (32, 48, 64, 96, 128, 192, 256)
 
-    def autotune(self, candidates=AUTOTUNE_ROWS, repeats=3):
+    def autotune(self, candidates=AUTOTUNE_ROWS, repeats=4):
         """Time the interior tile heights on this engine's fields and keep the fastest (the simulation state is not
         changed: trial launches write the idle buffer set).  Returns (rows, ms per launch)."""
         self.sync_device()
