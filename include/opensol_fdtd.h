@@ -112,6 +112,21 @@ int os_fdtd2d_set_sample_interval(OsFdtd2D *h, int64_t sample_interval);
 int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line_values, int64_t first_sample,
                       int64_t n_samples, const float *phases);
 
+/* Floats in the fixed device scratch of os_fdtd2d_advance_noalloc (1 MiB), and the device ordinals it serves. */
+#define OS_FDTD_NOALLOC_MAX_FLOATS 262144
+#define OS_FDTD_MAX_DEVICES 64
+
+/* os_fdtd2d_advance without any device allocation; no open_sol counterpart.  Same arguments, checks and results as os_fdtd2d_advance, but the chunk's tables go
+ * to a fixed file-scope device array of OS_FDTD_NOALLOC_MAX_FLOATS floats instead of the handle's grow-only
+ * buffers: for callers that must not allocate mid-run (jobs sharing a GPU on several streams, where cudaFree's
+ * device-wide wait would stall the others; jobs held to a fixed memory budget).  Limits: n_sources * n_steps
+ * source values plus the phase floats (rounded to 64 after the values) must fit, else OS_ERR_INVALID and nothing
+ * runs; profiling must be off.  The first call per device looks the array up (it may load the module), so make it
+ * before any stream capture.  One array per device and process: calls whose device work may overlap (unordered
+ * streams) race on it. */
+int os_fdtd2d_advance_noalloc(OsFdtd2D *h, int64_t n_steps, const float *line_values, int64_t first_sample,
+                              int64_t n_samples, const float *phases);
+
 /* Kernel choice: variant 1 (default) advances steps_per_launch (1..4) Yee steps per launch with temporally blocked,
  * double-buffered kernels, tile_rows rows per interior tile; variant 2 the same with the general kernel on every
  * cell; variant 0 launches one H and one E kernel per step.

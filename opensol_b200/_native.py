@@ -52,6 +52,7 @@ SIGNATURES = {
     'os_fdtd2d_add_flux_line': [_P, _I32, _I32, _I32, _I32, _I32, ctypes.POINTER(_I32)],
     'os_fdtd2d_set_sample_interval': [_P, _I64],
     'os_fdtd2d_advance': [_P, _I64, _F, _I64, _I64, _F],
+    'os_fdtd2d_advance_noalloc': [_P, _I64, _F, _I64, _I64, _F],
     'os_fdtd2d_step_count': [_P, ctypes.POINTER(_I64)],
     'os_fdtd2d_configure': [_P, _I32, _I32, _I32],
     'os_fdtd2d_launch_count': [_P, ctypes.POINTER(_I64)],

@@ -18,6 +18,7 @@
 
 #include <vector>
 #include <memory>
+#include <mutex>
 
 namespace os {
 
@@ -639,8 +640,10 @@ static void bind_buffers(OsFdtd2D *h, TBParams &q, int in, int out) {
     }
 }
 
-// Temporally blocked chunk: launches of T steps (a shorter last one), buffers swapped after each.
-static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples) {
+// Temporally blocked chunk: launches of T steps (a shorter last one), buffers swapped after each.  `values` and
+// `phase_table` are the chunk's device tables (source values, DFT phases).
+static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples,
+                           const float *values, const float *phase_table) {
     const int64_t m = h->sample_interval;
     int64_t k = 0;
     while (k < n_steps) {
@@ -653,6 +656,7 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
         const int in = h->cur, out = h->cur ^ 1;
         for (TBParams *q : {&interior, &general}) {
             bind_buffers(h, *q, in, out);
+            q->line_values = values;
             q->values_stride = n_steps;
             q->k0 = k;
             q->n0 = h->n_step;
@@ -669,7 +673,7 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
         if (!h->fluxes.empty() && q_hi >= q_lo) {
             size_t offset = 0;
             for (auto &f : h->fluxes) {
-                const float *ph = h->phases.ptr + offset + (size_t)(q_lo - first_sample) * f->nf * 2;
+                const float *ph = phase_table + offset + (size_t)(q_lo - first_sample) * f->nf * 2;
                 const int n = f->hi - f->lo;
                 const int total = n * f->nf;
                 OS_TRY(prof_begin(h, 2, h->stream));
@@ -688,7 +692,8 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
 }
 
 // Per-half-step chunk (variant 0): H kernel, E kernel, DFT of sample steps; fields updated in place.
-static int advance_per_step(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples) {
+static int advance_per_step(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples,
+                            const float *values, const float *phase_table) {
     const int64_t m = h->sample_interval;
     Ez2DParams p = make_params(h);
     const dim3 block(EZ2D_BLOCK_X, EZ2D_BLOCK_Y);
@@ -696,7 +701,7 @@ static int advance_per_step(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, 
     for (int64_t k = 0; k < n_steps; ++k) {
         OS_TRY(prof_begin(h, 3, h->stream));
         ez2d_h_kernel<<<grid, block, 0, h->stream>>>(p);
-        ez2d_e_kernel<<<grid, block, 0, h->stream>>>(p, h->line_values.ptr, n_steps, k);
+        ez2d_e_kernel<<<grid, block, 0, h->stream>>>(p, values, n_steps, k);
         OS_TRY(prof_end(h, h->stream));
         h->launches += 2;
         h->n_step += 1;
@@ -704,7 +709,7 @@ static int advance_per_step(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, 
             const int64_t q = h->n_step / m;
             size_t offset = 0;
             for (auto &f : h->fluxes) {
-                const float *ph = h->phases.ptr + offset + (size_t)(q - first_sample) * f->nf * 2;
+                const float *ph = phase_table + offset + (size_t)(q - first_sample) * f->nf * 2;
                 const int n = f->hi - f->lo;
                 const int total = n * f->nf;
                 ez2d_flux_kernel<<<(total + 255) / 256, 256, 0, h->stream>>>(
@@ -719,40 +724,121 @@ static int advance_per_step(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, 
     return OS_OK;
 }
 
-}  // namespace os
-
-extern "C" int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line_values, int64_t first_sample,
-                                 int64_t n_samples, const float *phases) {
-    OS_CHECK(h, OS_ERR_INVALID, "os_fdtd2d_advance: null handle");
+// Argument and state checks shared by the advance entry points (`fn` names the caller in messages).
+static int check_advance(const OsFdtd2D *h, const char *fn, int64_t n_steps, const float *line_values,
+                         int64_t first_sample, int64_t n_samples, const float *phases) {
+    OS_CHECK(h, OS_ERR_INVALID, "%s: null handle", fn);
     OS_CHECK(n_steps >= 0, OS_ERR_INVALID, "n_steps must be >= 0, got %lld", (long long)n_steps);
-    OS_CHECK(h->has_cb && h->has_spacings, OS_ERR_STATE, "os_fdtd2d_advance: coefficients and spacings must be set");
+    OS_CHECK(h->has_cb && h->has_spacings, OS_ERR_STATE, "%s: coefficients and spacings must be set", fn);
     for (int s = 0; s < 4; ++s)
         OS_CHECK(!(h->grid.cpml_sides & (1 << s)) || h->cpml_set[s], OS_ERR_STATE,
-                 "os_fdtd2d_advance: CPML side %d has no recursion rows", 1 << s);
-    h->launches = 0;
-    h->prof_used = 0;
+                 "%s: CPML side %d has no recursion rows", fn, 1 << s);
     if (n_steps == 0) return OS_OK;
-    OS_CHECK(h->lines.empty() || line_values, OS_ERR_INVALID, "os_fdtd2d_advance: line_values is required");
+    OS_CHECK(h->lines.empty() || line_values, OS_ERR_INVALID, "%s: line_values is required", fn);
     const int64_t m = h->sample_interval;
     const int64_t q_first = h->n_step / m + 1, q_last = (h->n_step + n_steps) / m;
     if (!h->fluxes.empty() && q_last >= q_first) {
         OS_CHECK(phases && first_sample <= q_first && first_sample + n_samples - 1 >= q_last, OS_ERR_INVALID,
-                 "os_fdtd2d_advance: the phase table covers samples [%lld, %lld), the chunk needs [%lld, %lld]",
+                 "%s: the phase table covers samples [%lld, %lld), the chunk needs [%lld, %lld]", fn,
                  (long long)first_sample, (long long)(first_sample + n_samples), (long long)q_first,
                  (long long)q_last);
     }
+    return OS_OK;
+}
+
+// The chunk's kernels between the start/stop timing events, reading the given device tables.
+static int run_chunk(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples, const float *values,
+                     const float *phase_table) {
+    OS_CUDA(cudaEventRecord(h->ev_start, h->stream));
+    const int rc = h->variant == 0 ? advance_per_step(h, n_steps, first_sample, n_samples, values, phase_table)
+                                   : advance_blocked(h, n_steps, first_sample, n_samples, values, phase_table);
+    if (rc != OS_OK) return rc;
+    OS_CUDA(cudaEventRecord(h->ev_stop, h->stream));
+    h->timed = true;
+    return OS_OK;
+}
+
+}  // namespace os
+
+extern "C" int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line_values, int64_t first_sample,
+                                 int64_t n_samples, const float *phases) {
+    OS_TRY(check_advance(h, "os_fdtd2d_advance", n_steps, line_values, first_sample, n_samples, phases));
+    h->launches = 0;
+    h->prof_used = 0;
+    if (n_steps == 0) return OS_OK;
     OS_TRY(bind_device(h));
     if (!h->lines.empty()) OS_TRY(upload(h->line_values, line_values, h->lines.size() * (size_t)n_steps, h->stream));
     size_t phase_floats = 0;
     for (auto &f : h->fluxes) phase_floats += (size_t)n_samples * f->nf * 2;
     if (!h->fluxes.empty() && phase_floats && phases) OS_TRY(upload(h->phases, phases, phase_floats, h->stream));
-    OS_CUDA(cudaEventRecord(h->ev_start, h->stream));
-    const int rc = h->variant == 0 ? advance_per_step(h, n_steps, first_sample, n_samples)
-                                   : advance_blocked(h, n_steps, first_sample, n_samples);   // 1 and 2
-    if (rc != OS_OK) return rc;
-    OS_CUDA(cudaEventRecord(h->ev_stop, h->stream));
-    h->timed = true;
+    return run_chunk(h, n_steps, first_sample, n_samples, h->line_values.ptr, h->phases.ptr);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Allocation-free advance.  os_fdtd2d_advance stages a chunk's source-value and DFT-phase tables in grow-only
+// device buffers of the handle, which allocate on the first chunk and whenever a chunk outgrows them (cudaFree +
+// cudaMalloc; cudaFree waits for the whole device).  Callers that must not allocate at that point -- a serving loop
+// whose jobs share one GPU on several streams, where a device-wide wait in one job stalls the others, or a job
+// admitted under a fixed memory budget that must not grow after admission -- use os_fdtd2d_advance_noalloc, which
+// stages the same tables in this fixed file-scope array instead.  Nothing in it has to start at zero: every call
+// copies its tables in before its kernels read them and the kernels read no float beyond what was copied.  The array
+// is one per device and per process, so calls whose device work can overlap (different streams with no ordering
+// between them) race on it; calls on one stream, or ordered by events, are safe.
+static __device__ __align__(256) float g_noalloc_scratch[OS_FDTD_NOALLOC_MAX_FLOATS];
+
+namespace os {
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device (the first lookup may load
+// the module onto the device, so the first call for a device belongs before any stream capture).
+static int noalloc_scratch(int device, float **out) {
+    static std::mutex mu;
+    static float *addr[OS_FDTD_MAX_DEVICES] = {};
+    OS_CHECK(device >= 0 && device < OS_FDTD_MAX_DEVICES, OS_ERR_INVALID,
+             "os_fdtd2d_advance_noalloc: device %d is outside [0, %d)", device, OS_FDTD_MAX_DEVICES);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[device]) {
+        void *p = nullptr;
+        OS_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        OS_CHECK(p && ((uintptr_t)p & 255) == 0, OS_ERR_CUDA,
+                 "os_fdtd2d_advance_noalloc: the scratch array is not 256-byte aligned on device %d", device);
+        addr[device] = (float *)p;
+    }
+    *out = addr[device];
     return OS_OK;
+}
+
+}  // namespace os
+
+extern "C" int os_fdtd2d_advance_noalloc(OsFdtd2D *h, int64_t n_steps, const float *line_values,
+                                         int64_t first_sample, int64_t n_samples, const float *phases) {
+    using namespace os;
+    OS_TRY(check_advance(h, "os_fdtd2d_advance_noalloc", n_steps, line_values, first_sample, n_samples, phases));
+    OS_CHECK(!h->profiling, OS_ERR_STATE,
+             "os_fdtd2d_advance_noalloc: profiling is on (its event pool grows on demand); turn it off first");
+    // tables: line values at float 0, phases at the next 64-float (256-byte) boundary
+    const size_t value_floats = n_steps > 0 ? h->lines.size() * (size_t)n_steps : 0;
+    size_t phase_floats = 0;
+    if (n_steps > 0 && n_samples > 0)
+        for (auto &f : h->fluxes) phase_floats += (size_t)n_samples * f->nf * 2;
+    const size_t phase_offset = (value_floats + 63) / 64 * 64;
+    const size_t need = phase_floats ? phase_offset + phase_floats : value_floats;
+    OS_CHECK(need <= (size_t)OS_FDTD_NOALLOC_MAX_FLOATS, OS_ERR_INVALID,
+             "os_fdtd2d_advance_noalloc: the chunk's tables need %zu floats (%zu source values + %zu phase floats), "
+             "the fixed scratch holds %d; advance fewer steps per call",
+             need, value_floats, phase_floats, OS_FDTD_NOALLOC_MAX_FLOATS);
+    h->launches = 0;
+    h->prof_used = 0;
+    if (n_steps == 0) return OS_OK;
+    OS_TRY(bind_device(h));
+    float *scratch = nullptr;
+    OS_TRY(noalloc_scratch(h->device, &scratch));
+    if (value_floats)
+        OS_CUDA(cudaMemcpyAsync(scratch, line_values, value_floats * sizeof(float), cudaMemcpyHostToDevice,
+                                h->stream));
+    if (phase_floats && phases)
+        OS_CUDA(cudaMemcpyAsync(scratch + phase_offset, phases, phase_floats * sizeof(float),
+                                cudaMemcpyHostToDevice, h->stream));
+    return run_chunk(h, n_steps, first_sample, n_samples, scratch, scratch + phase_offset);
 }
 
 extern "C" int os_fdtd2d_configure(OsFdtd2D *h, int32_t variant, int32_t steps_per_launch, int32_t tile_rows) {
