@@ -178,6 +178,84 @@ int os_fdtd2d_set_stream(OsFdtd2D *h, void *cuda_stream);
  * stream around its launches; 0 before the first advance). */
 int os_fdtd2d_last_advance_ms(OsFdtd2D *h, float *ms);
 
+/* ----------------------------------------------------------------------------------------------------------------
+ * 3D engine (E_x..H_z): replaces FDTDEngine3D (open_sol/physics/em3d/engine3d.py:157) for a Cartesian grid, one real
+ * field set (no Bloch phase) and float32 fields.  Fields (nx, ny, nz) z contiguous, idx = (i * ny + j) * nz + k.
+ * ---------------------------------------------------------------------------------------------------------------- */
+typedef struct OsFdtd3D OsFdtd3D;
+
+/* Field components of os_fdtd3d_read_field / write_field. */
+enum { OS_EX = 0, OS_EY = 1, OS_EZ3 = 2, OS_HX3 = 3, OS_HY3 = 4, OS_HZ3 = 5 };
+
+typedef struct {
+    int32_t nx, ny, nz;          /* total grid incl. CPML cells (Domain3D.uniform pads them: core/domain3d.py:55-65) */
+    int32_t periodic[3];         /* periodic axes (BoundaryConfig3D.periodic, boundaries3d.py:97-98) */
+    int32_t device;              /* CUDA device ordinal */
+} OsGrid3D;
+
+/* Zeroed fields on `device`: FDTDEngine3D.__init__ (engine3d.py:162-263) and Fields3D. */
+int os_fdtd3d_create(const OsGrid3D *grid, OsFdtd3D **out);
+int os_fdtd3d_destroy(OsFdtd3D *h);
+
+/* Kappa-folded curl spacings inv_e (1 / cell width) and inv_h (1 / hi-face spacing, 0 on the last row of an open
+ * axis) per axis (engine3d.py:189-203), and the hi-face shares as one array wl_x, wu_x, wl_y, wu_y, wl_z, wu_z
+ * (face_shares, physics/em/yee_grid.py:119-125; engine3d.py:204-205). */
+int os_fdtd3d_set_rows(OsFdtd3D *h, const float *inv_e_x, const float *inv_e_y, const float *inv_e_z,
+                       const float *inv_h_x, const float *inv_h_y, const float *inv_h_z, const float *shares);
+
+/* uint16 material id per cell and the per-id float32 tables (eps per E component with the PEC id at eps -1, sigma_e,
+ * mu_r, sigma_m): FDTDEngine3D.rebuild_materials (engine3d.py:337-369, material_index3d.py:131).  The H coefficients
+ * da / db per id are derived on the device (edge_coefficients, physics/em3d/kernels3d.py:44-54). */
+int os_fdtd3d_set_materials(OsFdtd3D *h, const uint16_t *material_id, int32_t n_ids, const float *t_ex,
+                            const float *t_ey, const float *t_ez, const float *t_sig, const float *t_mu,
+                            const float *t_sm, float dt);
+
+/* CPML layers of one axis (0, 1, 2): row maps grid row -> psi row (-1 outside), recursion b and gain per psi row, for
+ * the E ('e' rows at cell centres) and H ('h' rows at hi faces) kinds: CPMLAxis3D (boundaries3d.py:192-243).  The psi
+ * slabs (n_rows x the other two axes, two components per kind) are allocated and zeroed. */
+int os_fdtd3d_set_cpml_axis(OsFdtd3D *h, int32_t axis, int32_t n_rows, const int32_t *row_map_e, const float *b_e,
+                            const float *gain_e, const int32_t *row_map_h, const float *b_h, const float *gain_h);
+
+/* cb of E component comp on the face of cell (i, j, k): box_face_cb_3d for one cell (kernels3d.py:745-779), the
+ * dipole calibration input (DipoleSource3D.calibrate, sources3d.py:56-61).  Synchronous. */
+int os_fdtd3d_face_cb(OsFdtd3D *h, int32_t comp, int32_t i, int32_t j, int32_t k, float *cb);
+
+/* Electric dipole on E component comp of cell (i, j, k): E += FP32(s(t + dt/2)) * weight after every E update
+ * (DipoleSource3D.inject, sources3d.py:69-75).  At most 16. */
+int os_fdtd3d_add_dipole(OsFdtd3D *h, int32_t comp, int32_t i, int32_t j, int32_t k, float weight,
+                         int32_t *dipole_id);
+int os_fdtd3d_set_dipole_weight(OsFdtd3D *h, int32_t dipole_id, float weight);
+
+/* A flux monitor of nf frequencies (PlaneFlux3D / FluxBox3D, physics/em3d/monitors3d.py:42-162) and its (E, H) pairs:
+ * E component e_comp averaged over the layers edge - 1 and edge along normal_axis, H component h_comp on layer
+ * edge - 1, over the box origin / extent of the two tangential axes (extent 1 along the normal); complex128 running
+ * DFTs (nf, cells) for E and H, cells in grid axis order. */
+int os_fdtd3d_add_flux_monitor(OsFdtd3D *h, int32_t nf, int32_t *monitor_id);
+int os_fdtd3d_add_flux_pair(OsFdtd3D *h, int32_t monitor_id, int32_t e_comp, int32_t h_comp, int32_t normal_axis,
+                            int32_t edge, const int32_t *origin, const int32_t *extent, int32_t *pair_id);
+int os_fdtd3d_set_sample_interval(OsFdtd3D *h, int64_t sample_interval);
+
+/* n_steps Yee steps (FDTDEngine3D.advance, engine3d.py:497-554, repeated): dipole_values (n_dipoles, n_steps) float32
+ * amplitude FP32(temporal(t + dt/2)) per step; phases: per sample, for every monitor in add order, nf complex64 as
+ * float pairs (sample q is taken after engine step q * sample_interval), samples first_sample .. first_sample +
+ * n_samples - 1.  Asynchronous on the handle's stream. */
+int os_fdtd3d_advance(OsFdtd3D *h, int64_t n_steps, const float *dipole_values, int64_t first_sample,
+                      int64_t n_samples, const float *phases);
+
+int os_fdtd3d_read_field(OsFdtd3D *h, int32_t component, float *out);
+int os_fdtd3d_write_field(OsFdtd3D *h, int32_t component, const float *in);
+
+/* Spectra of one pair: (nf, cells) complex128 as double pairs, E then H (PlaneFlux3D._pairs e_dft / h_dft). */
+int os_fdtd3d_read_flux_pair(OsFdtd3D *h, int32_t pair_id, double *e_spectra, double *h_spectra);
+
+/* Zero fields, psi and spectra; step count back to 0. */
+int os_fdtd3d_reset(OsFdtd3D *h);
+int os_fdtd3d_synchronize(OsFdtd3D *h);
+int os_fdtd3d_set_stream(OsFdtd3D *h, void *cuda_stream);
+int os_fdtd3d_last_advance_ms(OsFdtd3D *h, float *ms);
+int os_fdtd3d_launch_count(OsFdtd3D *h, int64_t *launches);
+int os_fdtd3d_step_count(OsFdtd3D *h, int64_t *n_step);
+
 #ifdef __cplusplus
 }
 #endif

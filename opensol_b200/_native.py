@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(_HERE, '_lib', 'libopensol_fdtd.so')
 OS_OK, OS_ERR_INVALID, OS_ERR_CUDA, OS_ERR_NO_MEMORY, OS_ERR_STATE = 0, 1, 2, 3, 4
 OS_SIDE_BITS = {'x_lo': 1, 'x_hi': 2, 'y_lo': 4, 'y_hi': 8, 'z_lo': 16, 'z_hi': 32}
 OS_EZ, OS_HX, OS_HY = 0, 1, 2
+FIELDS_3D = ('ex', 'ey', 'ez', 'hx', 'hy', 'hz')   # os_fdtd3d_read_field / write_field component order
 
 _lock = threading.Lock()
 _lib = None
@@ -26,6 +27,11 @@ class OsGrid2D(ctypes.Structure):
     _fields_ = [('nx', ctypes.c_int32), ('ny', ctypes.c_int32), ('periodic_x', ctypes.c_int32),
                 ('periodic_y', ctypes.c_int32), ('npml', ctypes.c_int32), ('cpml_sides', ctypes.c_int32),
                 ('device', ctypes.c_int32)]
+
+
+class OsGrid3D(ctypes.Structure):
+    _fields_ = [('nx', ctypes.c_int32), ('ny', ctypes.c_int32), ('nz', ctypes.c_int32),
+                ('periodic', ctypes.c_int32 * 3), ('device', ctypes.c_int32)]
 
 
 _F = ctypes.POINTER(ctypes.c_float)
@@ -68,6 +74,28 @@ SIGNATURES = {
     'os_fdtd2d_synchronize': [_P],
     'os_fdtd2d_set_stream': [_P, _P],
     'os_fdtd2d_last_advance_ms': [_P, ctypes.POINTER(ctypes.c_float)],
+    'os_fdtd3d_create': [ctypes.POINTER(OsGrid3D), ctypes.POINTER(_P)],
+    'os_fdtd3d_destroy': [_P],
+    'os_fdtd3d_set_rows': [_P, _F, _F, _F, _F, _F, _F, _F],
+    'os_fdtd3d_set_materials': [_P, ctypes.POINTER(ctypes.c_uint16), _I32, _F, _F, _F, _F, _F, _F, ctypes.c_float],
+    'os_fdtd3d_set_cpml_axis': [_P, _I32, _I32, ctypes.POINTER(_I32), _F, _F, ctypes.POINTER(_I32), _F, _F],
+    'os_fdtd3d_face_cb': [_P, _I32, _I32, _I32, _I32, _F],
+    'os_fdtd3d_add_dipole': [_P, _I32, _I32, _I32, _I32, ctypes.c_float, ctypes.POINTER(_I32)],
+    'os_fdtd3d_set_dipole_weight': [_P, _I32, ctypes.c_float],
+    'os_fdtd3d_add_flux_monitor': [_P, _I32, ctypes.POINTER(_I32)],
+    'os_fdtd3d_add_flux_pair': [_P, _I32, _I32, _I32, _I32, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32),
+                                ctypes.POINTER(_I32)],
+    'os_fdtd3d_set_sample_interval': [_P, _I64],
+    'os_fdtd3d_advance': [_P, _I64, _F, _I64, _I64, _F],
+    'os_fdtd3d_read_field': [_P, _I32, _F],
+    'os_fdtd3d_write_field': [_P, _I32, _F],
+    'os_fdtd3d_read_flux_pair': [_P, _I32, _D, _D],
+    'os_fdtd3d_reset': [_P],
+    'os_fdtd3d_synchronize': [_P],
+    'os_fdtd3d_set_stream': [_P, _P],
+    'os_fdtd3d_last_advance_ms': [_P, ctypes.POINTER(ctypes.c_float)],
+    'os_fdtd3d_launch_count': [_P, ctypes.POINTER(_I64)],
+    'os_fdtd3d_step_count': [_P, ctypes.POINTER(_I64)],
 }
 
 

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, 'csrc')
 LIB_DIR = os.path.join(HERE, '_lib')
 LIB_NAME = 'libopensol_fdtd.so'
-SOURCES = ['common.cu', 'fdtd2d.cu']
+SOURCES = ['common.cu', 'fdtd2d.cu', 'fdtd3d.cu']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 

@@ -1,0 +1,527 @@
+// 3D FDTD engine for sm_100a: device state, launches and the os_fdtd3d_* C ABI (replaces open_sol's FDTDEngine3D,
+// physics/em3d/engine3d.py:157-554, for a Cartesian grid with one real field set and float32 fields).
+//
+// One Yee step = em3d_h_kernel (H with its CPML) then em3d_e_kernel (E with its CPML and the dipole injection), the
+// reference's own step order (engine3d.py:497-554); on DFT sample steps em3d_flux_kernel accumulates every flux pair.
+// A chunk of n steps is enqueued with no host synchronisation: per-step dipole amplitudes and per-sample DFT phases
+// arrive as small tables computed on the host in float64 and rounded as open_sol rounds them.
+#include "common.cuh"
+#include "fdtd3d_kernels.cuh"
+
+#include <algorithm>
+#include <memory>
+#include <vector>
+
+struct OsFdtd3D {
+    OsGrid3D grid{};
+    int device = 0;
+    cudaStream_t stream = nullptr, own_stream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    bool timed = false;
+    os::DeviceArray<float> field[6];            // ex, ey, ez, hx, hy, hz
+    os::DeviceArray<uint16_t> mat;
+    os::DeviceArray<float> tables;              // t_ex, t_ey, t_ez, t_sig, t_da, t_db (6 * n_ids)
+    os::DeviceArray<float> same;                // same-id face ca, cb per component (6 * n_ids)
+    int32_t n_ids = 0;
+    bool same_ok = false;                       // every face share is 0.5
+    bool has_materials = false, has_spacings = false;
+    bool h_uniform = true, e_lossless = true;
+    float da_u = 1.0f, db_u = 0.0f, dt = 0.0f;
+    os::DeviceArray<float> rows;                // iex, iey, iez, ihx, ihy, ihz, wlx, wux, wly, wuy, wlz, wuz
+    struct Cpml {
+        int32_t nr = 0;
+        os::DeviceArray<int32_t> rm;            // rm_e (n), rm_h (n)
+        os::DeviceArray<float> coef;            // b_e, g_e, b_h, g_h (nr each)
+        os::DeviceArray<float> psi;             // pe_first, pe_second, ph_first, ph_second
+        size_t psi_count = 0;
+    } cpml[3];
+    struct Dipole {
+        int32_t comp, i, o;                     // component, x plane, in-plane offset j nz + k
+        float weight;
+    };
+    std::vector<Dipole> dipoles;
+    std::vector<int32_t> monitor_nf;            // frequencies per flux monitor
+    std::vector<Em3DFluxPair> pairs;            // host copy (pointers into acc)
+    std::vector<std::unique_ptr<os::DeviceArray<double>>> acc;   // per pair: e then h accumulators
+    os::DeviceArray<Em3DFluxPair> pairs_dev;
+    bool pairs_dirty = false;
+    int32_t max_pair_cells = 0;
+    int64_t sample_interval = 1;
+    int64_t n_step = 0;
+    int64_t launches = 0;
+    int32_t x_chunk = 64;
+    os::DeviceArray<float> values;              // (n_dipoles, n_steps) of the current chunk
+    os::DeviceArray<float> phases;              // (n_samples, sum nf, 2) of the current chunk
+    os::DeviceArray<float> scratch;             // one float (face cb read-back)
+};
+
+namespace os {
+
+static int bind3(OsFdtd3D *h) {
+    OS_CUDA(cudaSetDevice(h->device));
+    return OS_OK;
+}
+
+static size_t cells3(const OsFdtd3D *h) { return (size_t)h->grid.nx * h->grid.ny * h->grid.nz; }
+
+static Em3DParams make_params3(const OsFdtd3D *h) {
+    Em3DParams p{};
+    const OsGrid3D &g = h->grid;
+    p.nx = g.nx;
+    p.ny = g.ny;
+    p.nz = g.nz;
+    p.px = g.periodic[0];
+    p.py = g.periodic[1];
+    p.pz = g.periodic[2];
+    p.x_chunk = h->x_chunk;
+    p.ex = h->field[0].ptr;
+    p.ey = h->field[1].ptr;
+    p.ez = h->field[2].ptr;
+    p.hx = h->field[3].ptr;
+    p.hy = h->field[4].ptr;
+    p.hz = h->field[5].ptr;
+    p.mat = h->mat.ptr;
+    const int n = h->n_ids;
+    const float *t = h->tables.ptr;
+    p.t_ex = t;
+    p.t_ey = t + n;
+    p.t_ez = t + 2 * n;
+    p.t_sig = t + 3 * n;
+    p.t_da = t + 4 * n;
+    p.t_db = t + 5 * n;
+    p.h_uniform = h->h_uniform;
+    p.da_u = h->da_u;
+    p.db_u = h->db_u;
+    p.e_lossless = h->e_lossless;
+    p.n_ids = h->n_ids;
+    p.same_ok = h->same_ok && h->same.ptr;
+    p.t_same = h->same.ptr;
+    const float *r = h->rows.ptr;
+    const size_t nx = g.nx, ny = g.ny, nz = g.nz;
+    p.iex = r;
+    p.iey = r + nx;
+    p.iez = r + nx + ny;
+    p.ihx = r + nx + ny + nz;
+    p.ihy = p.ihx + nx;
+    p.ihz = p.ihy + ny;
+    p.wlx = p.ihz + nz;
+    p.wux = p.wlx + nx;
+    p.wly = p.wux + nx;
+    p.wuy = p.wly + ny;
+    p.wlz = p.wuy + ny;
+    p.wuz = p.wlz + nz;
+    p.dt = h->dt;
+    for (int a = 0; a < 3; ++a) {
+        const auto &c = h->cpml[a];
+        Em3DCpmlAxis &q = p.cpml[a];
+        q.nr = c.nr;
+        if (!c.nr) continue;
+        const size_t n_axis = a == 0 ? nx : (a == 1 ? ny : nz);
+        q.rm_e = c.rm.ptr;
+        q.rm_h = c.rm.ptr + n_axis;
+        q.b_e = c.coef.ptr;
+        q.g_e = c.coef.ptr + c.nr;
+        q.b_h = c.coef.ptr + 2 * c.nr;
+        q.g_h = c.coef.ptr + 3 * c.nr;
+        q.pe_first = c.psi.ptr;
+        q.pe_second = c.psi.ptr + c.psi_count;
+        q.ph_first = c.psi.ptr + 2 * c.psi_count;
+        q.ph_second = c.psi.ptr + 3 * c.psi_count;
+    }
+    p.n_dip = (int32_t)h->dipoles.size();
+    for (size_t d = 0; d < h->dipoles.size(); ++d) {
+        p.dip_comp[d] = h->dipoles[d].comp;
+        p.dip_i[d] = h->dipoles[d].i;
+        p.dip_o[d] = h->dipoles[d].o;
+        p.dip_weight[d] = h->dipoles[d].weight;
+    }
+    return p;
+}
+
+static int zero_state3(OsFdtd3D *h) {
+    for (auto &f : h->field) OS_CUDA(cudaMemsetAsync(f.ptr, 0, f.bytes(), h->stream));
+    for (auto &c : h->cpml)
+        if (c.psi.ptr) OS_CUDA(cudaMemsetAsync(c.psi.ptr, 0, c.psi.bytes(), h->stream));
+    for (auto &a : h->acc) OS_CUDA(cudaMemsetAsync(a->ptr, 0, a->bytes(), h->stream));
+    h->n_step = 0;
+    return OS_OK;
+}
+
+static dim3 grid3(const OsFdtd3D *h) {
+    return dim3((unsigned)((h->grid.nz + EM3D_BZ - 1) / EM3D_BZ), (unsigned)((h->grid.ny + EM3D_BY - 1) / EM3D_BY),
+                (unsigned)((h->grid.nx + h->x_chunk - 1) / h->x_chunk));
+}
+
+}  // namespace os
+
+using namespace os;
+
+extern "C" int os_fdtd3d_create(const OsGrid3D *grid, OsFdtd3D **out) {
+    OS_CHECK(grid && out, OS_ERR_INVALID, "os_fdtd3d_create: null argument");
+    *out = nullptr;
+    const OsGrid3D g = *grid;
+    OS_CHECK(g.nx >= 1 && g.ny >= 1 && g.nz >= 1, OS_ERR_INVALID, "os_fdtd3d_create: grid %d x %d x %d has no cells",
+             g.nx, g.ny, g.nz);
+    OS_CHECK(g.ny <= 65535 * EM3D_BY && (int64_t)g.ny * g.nz < ((int64_t)1 << 31) &&
+                 (int64_t)g.nx * g.ny * g.nz < ((int64_t)1 << 40), OS_ERR_INVALID,
+             "os_fdtd3d_create: grid %d x %d x %d too large", g.nx, g.ny, g.nz);
+    std::unique_ptr<OsFdtd3D> h(new OsFdtd3D());
+    h->grid = g;
+    h->device = g.device;
+    OS_TRY(bind3(h.get()));
+    OS_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    h->stream = h->own_stream;
+    OS_CUDA(cudaEventCreate(&h->ev_start));
+    OS_CUDA(cudaEventCreate(&h->ev_stop));
+    const size_t n = cells3(h.get());
+    for (auto &f : h->field) OS_TRY(f.alloc(n));
+    OS_TRY(h->mat.alloc(n));
+    OS_TRY(h->rows.alloc(4 * ((size_t)g.nx + g.ny + g.nz)));
+    OS_TRY(h->scratch.alloc(1));
+    // x chunk: enough blocks for ~8 per SM on the (y, z) tiling, never below 16 planes
+    const size_t tiles = ((size_t)(g.nz + EM3D_BZ - 1) / EM3D_BZ) * ((size_t)(g.ny + EM3D_BY - 1) / EM3D_BY);
+    const size_t want_chunks = std::max<size_t>(1, (148 * 8 + tiles - 1) / tiles);
+    h->x_chunk = (int32_t)std::max<size_t>(16, ((size_t)g.nx + want_chunks - 1) / want_chunks);
+    OS_TRY(zero_state3(h.get()));
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    *out = h.release();
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_destroy(OsFdtd3D *h) {
+    if (!h) return OS_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->ev_start) cudaEventDestroy(h->ev_start);
+    if (h->ev_stop) cudaEventDestroy(h->ev_stop);
+    cudaStream_t s = h->own_stream;
+    delete h;
+    if (s) cudaStreamDestroy(s);
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_set_rows(OsFdtd3D *h, const float *inv_e_x, const float *inv_e_y, const float *inv_e_z,
+                                  const float *inv_h_x, const float *inv_h_y, const float *inv_h_z,
+                                  const float *shares) {
+    OS_CHECK(h && inv_e_x && inv_e_y && inv_e_z && inv_h_x && inv_h_y && inv_h_z && shares, OS_ERR_INVALID,
+             "os_fdtd3d_set_rows: null argument");
+    OS_TRY(bind3(h));
+    const OsGrid3D &g = h->grid;
+    std::vector<float> all;
+    all.reserve(4 * ((size_t)g.nx + g.ny + g.nz));
+    all.insert(all.end(), inv_e_x, inv_e_x + g.nx);
+    all.insert(all.end(), inv_e_y, inv_e_y + g.ny);
+    all.insert(all.end(), inv_e_z, inv_e_z + g.nz);
+    all.insert(all.end(), inv_h_x, inv_h_x + g.nx);
+    all.insert(all.end(), inv_h_y, inv_h_y + g.ny);
+    all.insert(all.end(), inv_h_z, inv_h_z + g.nz);
+    all.insert(all.end(), shares, shares + 2 * ((size_t)g.nx + g.ny + g.nz));
+    OS_CUDA(cudaMemcpyAsync(h->rows.ptr, all.data(), all.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    h->same_ok = true;
+    for (size_t q = 0; q < 2 * ((size_t)g.nx + g.ny + g.nz); ++q)
+        if (shares[q] != 0.5f) h->same_ok = false;
+    h->has_spacings = true;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_set_materials(OsFdtd3D *h, const uint16_t *material_id, int32_t n_ids, const float *t_ex,
+                                       const float *t_ey, const float *t_ez, const float *t_sig, const float *t_mu,
+                                       const float *t_sm, float dt) {
+    OS_CHECK(h && material_id && t_ex && t_ey && t_ez && t_sig && t_mu && t_sm, OS_ERR_INVALID,
+             "os_fdtd3d_set_materials: null argument");
+    OS_CHECK(n_ids >= 1 && n_ids <= 65536, OS_ERR_INVALID, "os_fdtd3d_set_materials: %d material ids (1..65536)",
+             n_ids);
+    OS_CHECK(dt > 0.0f, OS_ERR_INVALID, "os_fdtd3d_set_materials: dt must be > 0");
+    OS_TRY(bind3(h));
+    const size_t n = cells3(h);
+    OS_CUDA(cudaMemcpyAsync(h->mat.ptr, material_id, n * sizeof(uint16_t), cudaMemcpyHostToDevice, h->stream));
+    OS_TRY(h->tables.alloc(6 * (size_t)n_ids));
+    h->n_ids = n_ids;
+    float *t = h->tables.ptr;
+    OS_CUDA(cudaMemcpyAsync(t, t_ex, n_ids * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    OS_CUDA(cudaMemcpyAsync(t + n_ids, t_ey, n_ids * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    OS_CUDA(cudaMemcpyAsync(t + 2 * n_ids, t_ez, n_ids * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    OS_CUDA(cudaMemcpyAsync(t + 3 * n_ids, t_sig, n_ids * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    DeviceArray<float> mu, sm;
+    OS_TRY(upload(mu, t_mu, (size_t)n_ids, h->stream));
+    OS_TRY(upload(sm, t_sm, (size_t)n_ids, h->stream));
+    em3d_h_tables_kernel<<<(n_ids + 255) / 256, 256, 0, h->stream>>>(mu.ptr, sm.ptr, n_ids, dt, t + 4 * n_ids,
+                                                                    t + 5 * n_ids);
+    OS_CUDA(cudaGetLastError());
+    std::vector<float> dadb(2 * (size_t)n_ids);
+    OS_CUDA(cudaMemcpyAsync(dadb.data(), t + 4 * n_ids, dadb.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                            h->stream));
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    h->dt = dt;
+    h->h_uniform = true;
+    h->da_u = dadb[0];
+    h->db_u = dadb[n_ids];
+    for (int32_t m = 1; m < n_ids; ++m)
+        if (dadb[m] != h->da_u || dadb[n_ids + m] != h->db_u) h->h_uniform = false;
+    h->e_lossless = true;
+    for (int32_t m = 0; m < n_ids; ++m)
+        if (t_sig[m] != 0.0f) h->e_lossless = false;
+    OS_TRY(h->same.alloc(6 * (size_t)n_ids));
+    Em3DParams q = make_params3(h);
+    em3d_same_tables_kernel<<<(n_ids + 255) / 256, 256, 0, h->stream>>>(q, h->same.ptr);
+    OS_CUDA(cudaGetLastError());
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    h->has_materials = true;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_set_cpml_axis(OsFdtd3D *h, int32_t axis, int32_t n_rows, const int32_t *row_map_e,
+                                       const float *b_e, const float *gain_e, const int32_t *row_map_h,
+                                       const float *b_h, const float *gain_h) {
+    OS_CHECK(h && axis >= 0 && axis < 3, OS_ERR_INVALID, "os_fdtd3d_set_cpml_axis: bad handle or axis %d", axis);
+    OS_CHECK(n_rows >= 1 && row_map_e && b_e && gain_e && row_map_h && b_h && gain_h, OS_ERR_INVALID,
+             "os_fdtd3d_set_cpml_axis: rows and row maps are required (n_rows %d)", n_rows);
+    OS_CHECK(!h->grid.periodic[axis], OS_ERR_INVALID, "os_fdtd3d_set_cpml_axis: axis %d is periodic", axis);
+    OS_TRY(bind3(h));
+    const OsGrid3D &g = h->grid;
+    const int n = axis == 0 ? g.nx : (axis == 1 ? g.ny : g.nz);
+    for (int r = 0; r < n; ++r) {
+        OS_CHECK(row_map_e[r] >= -1 && row_map_e[r] < n_rows && row_map_h[r] >= -1 && row_map_h[r] < n_rows,
+                 OS_ERR_INVALID, "os_fdtd3d_set_cpml_axis: row map entry %d out of [-1, %d)", r, n_rows);
+    }
+    auto &c = h->cpml[axis];
+    c.nr = n_rows;
+    OS_TRY(c.rm.alloc(2 * (size_t)n));
+    OS_CUDA(cudaMemcpyAsync(c.rm.ptr, row_map_e, n * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    OS_CUDA(cudaMemcpyAsync(c.rm.ptr + n, row_map_h, n * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
+    OS_TRY(c.coef.alloc(4 * (size_t)n_rows));
+    OS_CUDA(cudaMemcpyAsync(c.coef.ptr, b_e, n_rows * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    OS_CUDA(cudaMemcpyAsync(c.coef.ptr + n_rows, gain_e, n_rows * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    OS_CUDA(cudaMemcpyAsync(c.coef.ptr + 2 * n_rows, b_h, n_rows * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    OS_CUDA(cudaMemcpyAsync(c.coef.ptr + 3 * n_rows, gain_h, n_rows * sizeof(float), cudaMemcpyHostToDevice,
+                            h->stream));
+    const size_t other = axis == 0 ? (size_t)g.ny * g.nz : (axis == 1 ? (size_t)g.nx * g.nz : (size_t)g.nx * g.ny);
+    c.psi_count = other * (size_t)n_rows;
+    OS_TRY(c.psi.alloc(4 * c.psi_count));
+    OS_CUDA(cudaMemsetAsync(c.psi.ptr, 0, c.psi.bytes(), h->stream));
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_face_cb(OsFdtd3D *h, int32_t comp, int32_t i, int32_t j, int32_t k, float *cb) {
+    OS_CHECK(h && cb && comp >= 0 && comp < 3, OS_ERR_INVALID, "os_fdtd3d_face_cb: bad argument");
+    OS_CHECK(h->has_materials && h->has_spacings, OS_ERR_STATE, "os_fdtd3d_face_cb: materials and rows must be set");
+    const OsGrid3D &g = h->grid;
+    OS_CHECK(i >= 0 && i < g.nx && j >= 0 && j < g.ny && k >= 0 && k < g.nz, OS_ERR_INVALID,
+             "os_fdtd3d_face_cb: cell (%d, %d, %d) outside the grid", i, j, k);
+    OS_TRY(bind3(h));
+    em3d_face_cb_kernel<<<1, 1, 0, h->stream>>>(make_params3(h), comp, i, j, k, h->scratch.ptr);
+    OS_CUDA(cudaGetLastError());
+    OS_CUDA(cudaMemcpyAsync(cb, h->scratch.ptr, sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_add_dipole(OsFdtd3D *h, int32_t comp, int32_t i, int32_t j, int32_t k, float weight,
+                                    int32_t *dipole_id) {
+    OS_CHECK(h && comp >= 0 && comp < 3, OS_ERR_INVALID, "os_fdtd3d_add_dipole: bad handle or component %d", comp);
+    const OsGrid3D &g = h->grid;
+    OS_CHECK(i >= 0 && i < g.nx && j >= 0 && j < g.ny && k >= 0 && k < g.nz, OS_ERR_INVALID,
+             "os_fdtd3d_add_dipole: cell (%d, %d, %d) outside the grid", i, j, k);
+    OS_CHECK((int)h->dipoles.size() < EM3D_MAX_DIPOLES, OS_ERR_INVALID, "os_fdtd3d_add_dipole: at most %d dipoles",
+             EM3D_MAX_DIPOLES);
+    h->dipoles.push_back({comp, i, j * g.nz + k, weight});
+    if (dipole_id) *dipole_id = (int32_t)h->dipoles.size() - 1;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_set_dipole_weight(OsFdtd3D *h, int32_t dipole_id, float weight) {
+    OS_CHECK(h && dipole_id >= 0 && dipole_id < (int32_t)h->dipoles.size(), OS_ERR_INVALID,
+             "os_fdtd3d_set_dipole_weight: no dipole %d", dipole_id);
+    h->dipoles[dipole_id].weight = weight;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_add_flux_monitor(OsFdtd3D *h, int32_t nf, int32_t *monitor_id) {
+    OS_CHECK(h && nf >= 1 && monitor_id, OS_ERR_INVALID, "os_fdtd3d_add_flux_monitor: bad argument (nf %d)", nf);
+    h->monitor_nf.push_back(nf);
+    *monitor_id = (int32_t)h->monitor_nf.size() - 1;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_add_flux_pair(OsFdtd3D *h, int32_t monitor_id, int32_t e_comp, int32_t h_comp,
+                                       int32_t normal_axis, int32_t edge, const int32_t *origin,
+                                       const int32_t *extent, int32_t *pair_id) {
+    OS_CHECK(h && origin && extent && pair_id, OS_ERR_INVALID, "os_fdtd3d_add_flux_pair: null argument");
+    OS_CHECK(monitor_id >= 0 && monitor_id < (int32_t)h->monitor_nf.size(), OS_ERR_INVALID,
+             "os_fdtd3d_add_flux_pair: no monitor %d", monitor_id);
+    OS_CHECK(e_comp >= 0 && e_comp < 3 && h_comp >= 0 && h_comp < 3 && normal_axis >= 0 && normal_axis < 3,
+             OS_ERR_INVALID, "os_fdtd3d_add_flux_pair: components and axis must be 0, 1 or 2");
+    const OsGrid3D &g = h->grid;
+    const int dims[3] = {g.nx, g.ny, g.nz};
+    OS_CHECK(edge >= 1 && edge <= dims[normal_axis] - 1, OS_ERR_INVALID,
+             "os_fdtd3d_add_flux_pair: edge %d needs a cell on both sides (1..%d)", edge, dims[normal_axis] - 1);
+    OS_CHECK(extent[normal_axis] == 1, OS_ERR_INVALID, "os_fdtd3d_add_flux_pair: extent along the normal must be 1");
+    int64_t count = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (a == normal_axis) continue;
+        OS_CHECK(extent[a] >= 1 && origin[a] >= 0 && origin[a] + extent[a] <= dims[a], OS_ERR_INVALID,
+                 "os_fdtd3d_add_flux_pair: samples [%d, %d) outside axis %d of %d cells", origin[a],
+                 origin[a] + extent[a], a, dims[a]);
+        count *= extent[a];
+    }
+    OS_CHECK(count <= ((int64_t)1 << 30), OS_ERR_INVALID, "os_fdtd3d_add_flux_pair: too many samples");
+    OS_TRY(bind3(h));
+    Em3DFluxPair q{};
+    q.e_comp = e_comp;
+    q.h_comp = h_comp;
+    q.normal = normal_axis;
+    q.edge = edge;
+    for (int a = 0; a < 3; ++a) {
+        q.o[a] = a == normal_axis ? 0 : origin[a];
+        q.n[a] = extent[a];
+    }
+    q.nf = h->monitor_nf[monitor_id];
+    int32_t offset = 0;
+    for (int32_t m = 0; m < monitor_id; ++m) offset += 2 * h->monitor_nf[m];
+    q.phase_offset = offset;
+    auto acc = std::make_unique<DeviceArray<double>>();
+    OS_TRY(acc->alloc(4 * (size_t)q.nf * (size_t)count));
+    OS_CUDA(cudaMemsetAsync(acc->ptr, 0, acc->bytes(), h->stream));
+    q.e_acc = acc->ptr;
+    q.h_acc = acc->ptr + 2 * (size_t)q.nf * (size_t)count;
+    h->acc.push_back(std::move(acc));
+    h->pairs.push_back(q);
+    h->max_pair_cells = std::max<int32_t>(h->max_pair_cells, (int32_t)count);
+    h->pairs_dirty = true;
+    *pair_id = (int32_t)h->pairs.size() - 1;
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_set_sample_interval(OsFdtd3D *h, int64_t sample_interval) {
+    OS_CHECK(h && sample_interval >= 1, OS_ERR_INVALID, "sample interval must be >= 1");
+    h->sample_interval = sample_interval;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_advance(OsFdtd3D *h, int64_t n_steps, const float *dipole_values, int64_t first_sample,
+                                 int64_t n_samples, const float *phases) {
+    OS_CHECK(h, OS_ERR_INVALID, "os_fdtd3d_advance: null handle");
+    OS_CHECK(n_steps >= 0, OS_ERR_INVALID, "n_steps must be >= 0, got %lld", (long long)n_steps);
+    OS_CHECK(h->has_materials && h->has_spacings, OS_ERR_STATE, "os_fdtd3d_advance: materials and rows must be set");
+    h->launches = 0;
+    if (n_steps == 0) return OS_OK;
+    OS_CHECK(h->dipoles.empty() || dipole_values, OS_ERR_INVALID, "os_fdtd3d_advance: dipole_values is required");
+    const int64_t m = h->sample_interval;
+    const int64_t q_first = h->n_step / m + 1, q_last = (h->n_step + n_steps) / m;
+    int32_t row_floats = 0;
+    for (int32_t nf : h->monitor_nf) row_floats += 2 * nf;
+    const bool sampling = !h->pairs.empty() && q_last >= q_first;
+    if (sampling)
+        OS_CHECK(phases && first_sample <= q_first && first_sample + n_samples - 1 >= q_last, OS_ERR_INVALID,
+                 "os_fdtd3d_advance: the phase table covers samples [%lld, %lld), the chunk needs [%lld, %lld]",
+                 (long long)first_sample, (long long)(first_sample + n_samples), (long long)q_first,
+                 (long long)q_last);
+    OS_TRY(bind3(h));
+    if (!h->dipoles.empty()) OS_TRY(upload(h->values, dipole_values, h->dipoles.size() * (size_t)n_steps, h->stream));
+    if (sampling) OS_TRY(upload(h->phases, phases, (size_t)n_samples * row_floats, h->stream));
+    if (h->pairs_dirty) {
+        OS_TRY(upload(h->pairs_dev, h->pairs.data(), h->pairs.size(), h->stream));
+        h->pairs_dirty = false;
+    }
+    Em3DParams p = make_params3(h);
+    p.dip_values = h->values.ptr;
+    p.values_stride = n_steps;
+    const dim3 grid = grid3(h), block(EM3D_BZ, EM3D_BY);
+    OS_CUDA(cudaEventRecord(h->ev_start, h->stream));
+    for (int64_t k = 0; k < n_steps; ++k) {
+        p.k_step = k;
+        em3d_h_kernel<<<grid, block, 0, h->stream>>>(p);
+        em3d_e_kernel<<<grid, block, 0, h->stream>>>(p);
+        h->launches += 2;
+        h->n_step += 1;
+        if (!h->pairs.empty() && h->n_step % m == 0) {
+            const int64_t q = h->n_step / m;
+            const dim3 fgrid((unsigned)((h->max_pair_cells + 255) / 256), (unsigned)h->pairs.size());
+            em3d_flux_kernel<<<fgrid, 256, 0, h->stream>>>(h->pairs_dev.ptr, p.ex, p.ey, p.ez, p.hx, p.hy, p.hz,
+                                                            h->grid.ny, h->grid.nz,
+                                                            h->phases.ptr + (size_t)(q - first_sample) * row_floats);
+            h->launches += 1;
+        }
+    }
+    OS_CUDA(cudaGetLastError());
+    OS_CUDA(cudaEventRecord(h->ev_stop, h->stream));
+    h->timed = true;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_read_field(OsFdtd3D *h, int32_t component, float *out) {
+    OS_CHECK(h && out && component >= 0 && component < 6, OS_ERR_INVALID, "os_fdtd3d_read_field: bad argument");
+    OS_TRY(bind3(h));
+    OS_CUDA(cudaMemcpyAsync(out, h->field[component].ptr, h->field[component].bytes(), cudaMemcpyDeviceToHost,
+                            h->stream));
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_write_field(OsFdtd3D *h, int32_t component, const float *in) {
+    OS_CHECK(h && in && component >= 0 && component < 6, OS_ERR_INVALID, "os_fdtd3d_write_field: bad argument");
+    OS_TRY(bind3(h));
+    OS_CUDA(cudaMemcpyAsync(h->field[component].ptr, in, h->field[component].bytes(), cudaMemcpyHostToDevice,
+                            h->stream));
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_read_flux_pair(OsFdtd3D *h, int32_t pair_id, double *e_spectra, double *h_spectra) {
+    OS_CHECK(h && e_spectra && h_spectra && pair_id >= 0 && pair_id < (int32_t)h->pairs.size(), OS_ERR_INVALID,
+             "os_fdtd3d_read_flux_pair: bad argument");
+    OS_TRY(bind3(h));
+    const Em3DFluxPair &q = h->pairs[pair_id];
+    const size_t n = 2 * (size_t)q.nf * q.n[0] * q.n[1] * q.n[2];
+    OS_CUDA(cudaMemcpyAsync(e_spectra, q.e_acc, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    OS_CUDA(cudaMemcpyAsync(h_spectra, q.h_acc, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_reset(OsFdtd3D *h) {
+    OS_CHECK(h, OS_ERR_INVALID, "os_fdtd3d_reset: null handle");
+    OS_TRY(bind3(h));
+    OS_TRY(zero_state3(h));
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_synchronize(OsFdtd3D *h) {
+    OS_CHECK(h, OS_ERR_INVALID, "os_fdtd3d_synchronize: null handle");
+    OS_TRY(bind3(h));
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_set_stream(OsFdtd3D *h, void *cuda_stream) {
+    OS_CHECK(h, OS_ERR_INVALID, "os_fdtd3d_set_stream: null handle");
+    OS_TRY(bind3(h));
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    h->stream = cuda_stream ? (cudaStream_t)cuda_stream : h->own_stream;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_last_advance_ms(OsFdtd3D *h, float *ms) {
+    OS_CHECK(h && ms, OS_ERR_INVALID, "os_fdtd3d_last_advance_ms: null argument");
+    OS_CHECK(h->timed, OS_ERR_STATE, "os_fdtd3d_last_advance_ms: no advance recorded yet");
+    OS_TRY(bind3(h));
+    OS_CUDA(cudaEventSynchronize(h->ev_stop));
+    OS_CUDA(cudaEventElapsedTime(ms, h->ev_start, h->ev_stop));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_launch_count(OsFdtd3D *h, int64_t *launches) {
+    OS_CHECK(h && launches, OS_ERR_INVALID, "os_fdtd3d_launch_count: null argument");
+    *launches = h->launches;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_step_count(OsFdtd3D *h, int64_t *n_step) {
+    OS_CHECK(h && n_step, OS_ERR_INVALID, "os_fdtd3d_step_count: null argument");
+    *n_step = h->n_step;
+    return OS_OK;
+}

@@ -1,0 +1,452 @@
+// 3D Yee kernels for sm_100a: the H update and the E update of one step (CPML fused through per-axis row maps, the
+// dipole injection fused into the E update) and the running DFT of the flux planes.
+//
+// Layout as open_sol's em_fdtd_3d (engine3d.py:4-12): fields (nx, ny, nz) float32, z contiguous, idx = (i ny + j) nz
+// + k; E_x on the hi-x face, E_y on the hi-y face, E_z on the hi-z face of a cell; H on the edges; a uint16 material id
+// per cell and small per-id tables.  Each thread owns one (j, k) column and streams along x over a chunk of planes,
+// carrying the plane it loaded as the next (H) or previous (E) neighbour into the following iteration; a warp covers 32
+// consecutive k, so every field access of a warp is one contiguous 128-byte row.
+//
+// Arithmetic: the evaluation order of update_h_3d / update_e_3d (physics/em3d/kernels3d.py:335-392,538-609) and its
+// numpy twins (:451-463,640-661) for a Cartesian grid with one real field set (the radial factors are exactly 1 and
+// are left out), compiled with -fmad=false: results equal the reference's numpy twins bit for bit.  A sample read
+// across the hi edge of an axis is c F + s F with c = 1, s = 0, as the reference's wrap_load evaluates it; on a
+// non-periodic axis the last row's inverse spacing is 0.  The missing lo H below row 0 of a non-periodic axis is 0.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define EM3D_EPS0F 8.8541878128e-12f
+
+constexpr int EM3D_BZ = 32;            // threads along z (one warp)
+constexpr int EM3D_BY = 8;             // warps along y
+constexpr int EM3D_MAX_DIPOLES = 16;
+
+struct Em3DCpmlAxis {
+    const int32_t *rm_h, *rm_e;        // grid row -> psi row (-1 outside the layers)
+    const float *b_h, *g_h, *b_e, *g_e;
+    float *ph_first, *ph_second, *pe_first, *pe_second;
+    int32_t nr;                        // psi rows of the axis (0: no CPML on it)
+};
+
+struct Em3DParams {
+    int32_t nx, ny, nz, px, py, pz;
+    int32_t x_chunk;                   // x planes per block
+    float *ex, *ey, *ez, *hx, *hy, *hz;
+    const uint16_t *mat;
+    const float *t_ex, *t_ey, *t_ez, *t_sig;   // E tables per material id
+    const float *t_da, *t_db;                  // H coefficients per material id
+    int32_t h_uniform;                         // every id has da = da_u, db = db_u (mat is not read by H)
+    float da_u, db_u;
+    int32_t e_lossless;                        // every sigma_e is 0: ca = 1, cb = dt / eps
+    int32_t n_ids;
+    int32_t same_ok;                           // every face share is 0.5: t_same holds the same-id faces
+    const float *t_same;                       // per component: ca (n_ids) then cb (n_ids)
+    const float *iex, *iey, *iez, *ihx, *ihy, *ihz;
+    const float *wlx, *wux, *wly, *wuy, *wlz, *wuz;
+    float dt;
+    Em3DCpmlAxis cpml[3];
+    int32_t n_dip;
+    int32_t dip_comp[EM3D_MAX_DIPOLES];
+    int32_t dip_i[EM3D_MAX_DIPOLES];           // x plane of the dipole cell
+    int32_t dip_o[EM3D_MAX_DIPOLES];           // in-plane offset j nz + k
+    float dip_weight[EM3D_MAX_DIPOLES];
+    const float *dip_values;                   // (n_dip, values_stride) float32 amplitude per step
+    int64_t values_stride, k_step;
+};
+
+__device__ __forceinline__ float em3d_wrapped(float v) { return __fadd_rn(__fmul_rn(1.0f, v), __fmul_rn(0.0f, v)); }
+
+__device__ __forceinline__ float em3d_psi(float *psi, size_t p, float b, float g, float difference) {
+    const float value = b * psi[p] + g * difference;
+    psi[p] = value;
+    return value;
+}
+
+// ---------------------------------------------------------------------------------------------------- H update
+// Thread (j, k) streams x-planes i0 .. i1 - 1.  The loads of plane i + 1 (its next plane, its y / z neighbours, its
+// own H) are issued before plane i is computed, so every warp keeps two planes of loads in flight; fields the kernel
+// only reads go through the read-only path.  In-plane offsets are 32-bit (ny nz < 2^31 is checked at create).
+__global__ void __launch_bounds__(EM3D_BZ * EM3D_BY) em3d_h_kernel(const Em3DParams p) {
+    const int k = blockIdx.x * EM3D_BZ + threadIdx.x;
+    const int j = blockIdx.y * EM3D_BY + threadIdx.y;
+    if (j >= p.ny || k >= p.nz) return;
+    const int i0 = blockIdx.z * p.x_chunk;
+    const int i1 = min(p.nx, i0 + p.x_chunk);
+    const size_t sx = (size_t)p.ny * p.nz;
+    const float *__restrict__ ex = p.ex;
+    const float *__restrict__ ey = p.ey;
+    const float *__restrict__ ez = p.ez;
+    float *__restrict__ hx = p.hx;
+    float *__restrict__ hy = p.hy;
+    float *__restrict__ hz = p.hz;
+    const bool wy = j + 1 == p.ny, wz = k + 1 == p.nz;
+    const int o = j * p.nz + k;
+    const int oy = wy ? k : o + p.nz;             // hi y neighbour (row 0 across the edge)
+    const int oz = wz ? j * p.nz : o + 1;         // hi z neighbour
+    const float ihy = p.ihy[j], ihz = p.ihz[k];
+    const int32_t ry = p.cpml[1].nr ? p.cpml[1].rm_h[j] : -1;
+    const int32_t rz = p.cpml[2].nr ? p.cpml[2].rm_h[k] : -1;
+    size_t b = (size_t)i0 * sx;                                   // plane i
+    size_t bn = (size_t)(i0 + 1 < p.nx ? i0 + 1 : 0) * sx;        // plane i + 1 (plane 0 across the x edge)
+    float ex0 = __ldg(ex + b + o), ey0 = __ldg(ey + b + o), ez0 = __ldg(ez + b + o);
+    float exn = __ldg(ex + bn + o), eyn = __ldg(ey + bn + o), ezn = __ldg(ez + bn + o);
+    float exy = __ldg(ex + b + oy), ezy = __ldg(ez + b + oy);
+    float exz = __ldg(ex + b + oz), eyz = __ldg(ey + b + oz);
+    float hx0 = hx[b + o], hy0 = hy[b + o], hz0 = hz[b + o];
+    for (int i = i0; i < i1; ++i) {
+        const bool more = i + 1 < i1;
+        const size_t bnn = (size_t)(i + 2 < p.nx ? i + 2 : 0) * sx;   // plane i + 2
+        float exn2 = 0.0f, eyn2 = 0.0f, ezn2 = 0.0f, exy2 = 0.0f, ezy2 = 0.0f, exz2 = 0.0f, eyz2 = 0.0f;
+        float hx2 = 0.0f, hy2 = 0.0f, hz2 = 0.0f;
+        if (more) {
+            exn2 = __ldg(ex + bnn + o);
+            eyn2 = __ldg(ey + bnn + o);
+            ezn2 = __ldg(ez + bnn + o);
+            exy2 = __ldg(ex + bn + oy);
+            ezy2 = __ldg(ez + bn + oy);
+            exz2 = __ldg(ex + bn + oz);
+            eyz2 = __ldg(ey + bn + oz);
+            hx2 = hx[bn + o];
+            hy2 = hy[bn + o];
+            hz2 = hz[bn + o];
+        }
+        const bool wx = i + 1 == p.nx;
+        const float dez_y = (wy ? em3d_wrapped(ezy) : ezy) - ez0;
+        const float dey_z = (wz ? em3d_wrapped(eyz) : eyz) - ey0;
+        const float dex_z = (wz ? em3d_wrapped(exz) : exz) - ex0;
+        const float dez_x = (wx ? em3d_wrapped(ezn) : ezn) - ez0;
+        const float dey_x = (wx ? em3d_wrapped(eyn) : eyn) - ey0;
+        const float dex_y = (wy ? em3d_wrapped(exy) : exy) - ex0;
+        float da, db;
+        if (p.h_uniform) {
+            da = p.da_u;
+            db = p.db_u;
+        } else {
+            const uint16_t m = p.mat[b + o];
+            da = p.t_da[m];
+            db = p.t_db[m];
+        }
+        const float ihx = p.ihx[i];
+        float vx = da * hx0 - db * (dez_y * ihy - dey_z * ihz);
+        float vy = da * hy0 - db * (dex_z * ihz - dez_x * ihx);
+        float vz = da * hz0 - db * (dey_x * ihx - dex_y * ihy);
+        if (p.cpml[0].nr) {
+            const int32_t r = p.cpml[0].rm_h[i];
+            if (r >= 0) {   // x layers: H_y from E_z (+), H_z from E_y (-)
+                const Em3DCpmlAxis &c = p.cpml[0];
+                const size_t q = (size_t)r * sx + o;
+                vy += db * em3d_psi(c.ph_first, q, c.b_h[r], c.g_h[r], dez_x);
+                vz -= db * em3d_psi(c.ph_second, q, c.b_h[r], c.g_h[r], dey_x);
+            }
+        }
+        if (ry >= 0) {   // y layers: H_x from E_z (-), H_z from E_x (+)
+            const Em3DCpmlAxis &c = p.cpml[1];
+            const size_t q = ((size_t)i * c.nr + ry) * p.nz + k;
+            vx -= db * em3d_psi(c.ph_first, q, c.b_h[ry], c.g_h[ry], dez_y);
+            vz += db * em3d_psi(c.ph_second, q, c.b_h[ry], c.g_h[ry], dex_y);
+        }
+        if (rz >= 0) {   // z layers: H_x from E_y (+), H_y from E_x (-)
+            const Em3DCpmlAxis &c = p.cpml[2];
+            const size_t q = ((size_t)i * p.ny + j) * c.nr + rz;
+            vx += db * em3d_psi(c.ph_first, q, c.b_h[rz], c.g_h[rz], dey_z);
+            vy -= db * em3d_psi(c.ph_second, q, c.b_h[rz], c.g_h[rz], dex_z);
+        }
+        hx[b + o] = vx;
+        hy[b + o] = vy;
+        hz[b + o] = vz;
+        ex0 = exn;
+        ey0 = eyn;
+        ez0 = ezn;
+        exn = exn2;
+        eyn = eyn2;
+        ezn = ezn2;
+        exy = exy2;
+        ezy = ezy2;
+        exz = exz2;
+        eyz = eyz2;
+        hx0 = hx2;
+        hy0 = hy2;
+        hz0 = hz2;
+        b = bn;
+        bn = bnn;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------- E update
+// ca, cb of the face between cells a and b (face_coefficients, kernels3d.py:61-82; b = a on the last row of a
+// non-periodic axis).
+__device__ __forceinline__ void em3d_face(const Em3DParams &p, const float *t_eps, uint16_t ia, uint16_t ib, float wa,
+                                          float wb, float &ca, float &cb) {
+    float ea = t_eps[ia], eb = t_eps[ib];
+    if (ea < 0.0f && eb < 0.0f) {
+        ca = 0.0f;
+        cb = 0.0f;
+        return;
+    }
+    float sa = 0.0f, sb = 0.0f;
+    if (!p.e_lossless) {
+        sa = p.t_sig[ia];
+        sb = p.t_sig[ib];
+    }
+    if (ea < 0.0f) {
+        ea = eb;
+        sa = sb;
+    } else if (eb < 0.0f) {
+        eb = ea;
+        sb = sa;
+    }
+    const float eps = (wa * ea + wb * eb) * EM3D_EPS0F;
+    if (p.e_lossless) {   // sigma 0: loss 0, den 1, so ca = 1 and cb = dt / eps exactly
+        ca = 1.0f;
+        cb = p.dt / eps;
+        return;
+    }
+    const float sig = wa * sa + wb * sb;
+    const float loss = sig * p.dt / (2.0f * eps);
+    const float den = 1.0f + loss;
+    ca = (1.0f - loss) / den;
+    cb = (p.dt / eps) / den;
+}
+
+// The same with the table of faces between two cells of one material id (t_same: per component ca then cb per id,
+// computed by em3d_face with the grid's uniform shares 0.5 / 0.5, so the values are the formula's own).
+__device__ __forceinline__ void em3d_face_fast(const Em3DParams &p, int comp, const float *t_eps, uint16_t ia,
+                                               uint16_t ib, float wa, float wb, float &ca, float &cb) {
+    if (p.same_ok && ia == ib) {
+        ca = p.t_same[(2 * comp) * p.n_ids + ia];
+        cb = p.t_same[(2 * comp + 1) * p.n_ids + ia];
+        return;
+    }
+    em3d_face(p, t_eps, ia, ib, wa, wb, ca, cb);
+}
+
+// F0 - F[lo neighbour]: the wrapped sample on a periodic axis, F0 itself below row 0 of an open axis.
+__device__ __forceinline__ float em3d_lo_diff(float f0, float lo, bool first_row, int periodic) {
+    if (!first_row) return f0 - lo;
+    return periodic ? f0 - em3d_wrapped(lo) : f0;
+}
+
+__global__ void __launch_bounds__(EM3D_BZ * EM3D_BY) em3d_e_kernel(const Em3DParams p) {
+    const int k = blockIdx.x * EM3D_BZ + threadIdx.x;
+    const int j = blockIdx.y * EM3D_BY + threadIdx.y;
+    if (j >= p.ny || k >= p.nz) return;
+    const int i0 = blockIdx.z * p.x_chunk;
+    const int i1 = min(p.nx, i0 + p.x_chunk);
+    const size_t sx = (size_t)p.ny * p.nz;
+    const float *__restrict__ hx = p.hx;
+    const float *__restrict__ hy = p.hy;
+    const float *__restrict__ hz = p.hz;
+    float *__restrict__ ex = p.ex;
+    float *__restrict__ ey = p.ey;
+    float *__restrict__ ez = p.ez;
+    const uint16_t *__restrict__ mat = p.mat;
+    const bool fy = j == 0, fz = k == 0;
+    const int o = j * p.nz + k;
+    const int oym = fy ? (p.ny - 1) * p.nz + k : o - p.nz;   // lo y neighbour (last row across the edge)
+    const int ozm = fz ? j * p.nz + p.nz - 1 : o - 1;
+    // hi partners of the E_y / E_z faces (the cell itself on the last row of an open axis)
+    const int oyp = j + 1 < p.ny ? o + p.nz : (p.py ? k : o);
+    const int ozp = k + 1 < p.nz ? o + 1 : (p.pz ? j * p.nz : o);
+    const float iey = p.iey[j], iez = p.iez[k];
+    const float wly = p.wly[j], wuy = p.wuy[j], wlz = p.wlz[k], wuz = p.wuz[k];
+    const int32_t ry = p.cpml[1].nr ? p.cpml[1].rm_e[j] : -1;
+    const int32_t rz = p.cpml[2].nr ? p.cpml[2].rm_e[k] : -1;
+    auto partner_plane = [&](int i) -> size_t {   // plane of the hi-x partner of plane i
+        return (size_t)(i + 1 < p.nx ? i + 1 : (p.px ? 0 : i)) * sx;
+    };
+    size_t b = (size_t)i0 * sx;
+    const size_t bm = (size_t)(i0 > 0 ? i0 - 1 : p.nx - 1) * sx;   // plane i - 1 (wrapped for i = 0)
+    float hy_m = __ldg(hy + bm + o), hz_m = __ldg(hz + bm + o);
+    float hx0 = __ldg(hx + b + o), hy0 = __ldg(hy + b + o), hz0 = __ldg(hz + b + o);
+    float hx_y = __ldg(hx + b + oym), hz_y = __ldg(hz + b + oym);
+    float hx_z = __ldg(hx + b + ozm), hy_z = __ldg(hy + b + ozm);
+    float ex0 = ex[b + o], ey0 = ey[b + o], ez0 = ez[b + o];
+    uint16_t m0 = __ldg(mat + b + o), mx = __ldg(mat + partner_plane(i0) + o);
+    uint16_t my = __ldg(mat + b + oyp), mz = __ldg(mat + b + ozp);
+    for (int i = i0; i < i1; ++i) {
+        const bool more = i + 1 < i1;
+        const size_t bn = (size_t)(i + 1) * sx;   // plane i + 1 (only read when more)
+        float hx2 = 0.0f, hy2 = 0.0f, hz2 = 0.0f, hx_y2 = 0.0f, hz_y2 = 0.0f, hx_z2 = 0.0f, hy_z2 = 0.0f;
+        float ex2 = 0.0f, ey2 = 0.0f, ez2 = 0.0f;
+        uint16_t mx2 = 0, my2 = 0, mz2 = 0;
+        if (more) {
+            hx2 = __ldg(hx + bn + o);
+            hy2 = __ldg(hy + bn + o);
+            hz2 = __ldg(hz + bn + o);
+            hx_y2 = __ldg(hx + bn + oym);
+            hz_y2 = __ldg(hz + bn + oym);
+            hx_z2 = __ldg(hx + bn + ozm);
+            hy_z2 = __ldg(hy + bn + ozm);
+            ex2 = ex[bn + o];
+            ey2 = ey[bn + o];
+            ez2 = ez[bn + o];
+            mx2 = __ldg(mat + partner_plane(i + 1) + o);
+            my2 = __ldg(mat + bn + oyp);
+            mz2 = __ldg(mat + bn + ozp);
+        }
+        const bool fx = i == 0;
+        const float dhz_y = em3d_lo_diff(hz0, hz_y, fy, p.py);
+        const float dhy_z = em3d_lo_diff(hy0, hy_z, fz, p.pz);
+        const float dhx_z = em3d_lo_diff(hx0, hx_z, fz, p.pz);
+        const float dhz_x = em3d_lo_diff(hz0, hz_m, fx, p.px);
+        const float dhy_x = em3d_lo_diff(hy0, hy_m, fx, p.px);
+        const float dhx_y = em3d_lo_diff(hx0, hx_y, fy, p.py);
+        float ca, cbx, cby, cbz;
+        em3d_face_fast(p, 0, p.t_ex, m0, mx, p.wlx[i], p.wux[i], ca, cbx);
+        const float iex = p.iex[i];
+        float vx = ca * ex0 + cbx * (dhz_y * iey - dhy_z * iez);
+        em3d_face_fast(p, 1, p.t_ey, m0, my, wly, wuy, ca, cby);
+        float vy = ca * ey0 + cby * (dhx_z * iez - dhz_x * iex);
+        em3d_face_fast(p, 2, p.t_ez, m0, mz, wlz, wuz, ca, cbz);
+        float vz = ca * ez0 + cbz * (dhy_x * iex - dhx_y * iey);
+        if (p.cpml[0].nr) {
+            const int32_t r = p.cpml[0].rm_e[i];
+            if (r >= 0) {   // x layers: E_y from H_z (-), E_z from H_y (+)
+                const Em3DCpmlAxis &c = p.cpml[0];
+                const size_t q = (size_t)r * sx + o;
+                vy -= cby * em3d_psi(c.pe_first, q, c.b_e[r], c.g_e[r], dhz_x);
+                vz += cbz * em3d_psi(c.pe_second, q, c.b_e[r], c.g_e[r], dhy_x);
+            }
+        }
+        if (ry >= 0) {   // y layers: E_x from H_z (+), E_z from H_x (-)
+            const Em3DCpmlAxis &c = p.cpml[1];
+            const size_t q = ((size_t)i * c.nr + ry) * p.nz + k;
+            vx += cbx * em3d_psi(c.pe_first, q, c.b_e[ry], c.g_e[ry], dhz_y);
+            vz -= cbz * em3d_psi(c.pe_second, q, c.b_e[ry], c.g_e[ry], dhx_y);
+        }
+        if (rz >= 0) {   // z layers: E_x from H_y (-), E_y from H_x (+)
+            const Em3DCpmlAxis &c = p.cpml[2];
+            const size_t q = ((size_t)i * p.ny + j) * c.nr + rz;
+            vx -= cbx * em3d_psi(c.pe_first, q, c.b_e[rz], c.g_e[rz], dhy_z);
+            vy += cby * em3d_psi(c.pe_second, q, c.b_e[rz], c.g_e[rz], dhx_z);
+        }
+        // dipoles (DipoleSource3D.inject, sources3d.py:69-75): E += FP32(s(t + dt/2)) * weight after the update
+        for (int d = 0; d < p.n_dip; ++d) {
+            if (p.dip_o[d] != o || p.dip_i[d] != i) continue;
+            const float add = p.dip_values[d * p.values_stride + p.k_step] * p.dip_weight[d];
+            if (p.dip_comp[d] == 0) vx = vx + add;
+            else if (p.dip_comp[d] == 1) vy = vy + add;
+            else vz = vz + add;
+        }
+        ex[b + o] = vx;
+        ey[b + o] = vy;
+        ez[b + o] = vz;
+        hy_m = hy0;
+        hz_m = hz0;
+        hx0 = hx2;
+        hy0 = hy2;
+        hz0 = hz2;
+        hx_y = hx_y2;
+        hz_y = hz_y2;
+        hx_z = hx_z2;
+        hy_z = hy_z2;
+        ex0 = ex2;
+        ey0 = ey2;
+        ez0 = ez2;
+        m0 = (i + 1 < p.nx) ? mx : m0;   // the next plane's own id (mx is it whenever i + 1 < nx)
+        mx = mx2;
+        my = my2;
+        mz = mz2;
+        b = bn;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------- running DFT
+// One (E, H) pair of a flux plane (PlaneFlux3D, monitors3d.py:42-113): E = mean of the two layers across the plane,
+// H on the plane, complex128 sums acc += ph * sample (the line kernels of physics/em/monitors.py:84-96).
+struct Em3DFluxPair {
+    int32_t e_comp, h_comp, normal, edge;
+    int32_t o[3], n[3];                // box of the pair's samples (n[normal] = 1, o[normal] ignored)
+    int32_t nf;
+    int32_t phase_offset;              // offset of the pair's monitor in one sample's phase row (floats)
+    double *e_acc, *h_acc;             // (nf, n cells) complex128 as double pairs
+};
+
+__global__ void em3d_flux_kernel(const Em3DFluxPair *pairs, const float *ex, const float *ey, const float *ez,
+                                 const float *hx, const float *hy, const float *hz, int ny, int nz,
+                                 const float *phases) {
+    const Em3DFluxPair q = pairs[blockIdx.y];
+    const int cells = q.n[0] * q.n[1] * q.n[2];
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cells) return;
+    int ijk[3] = {c / (q.n[1] * q.n[2]), (c / q.n[2]) % q.n[1], c % q.n[2]};
+    for (int a = 0; a < 3; ++a) ijk[a] += q.o[a];
+    ijk[q.normal] = q.edge - 1;
+    const size_t lower = ((size_t)ijk[0] * ny + ijk[1]) * nz + ijk[2];
+    const size_t step = q.normal == 0 ? (size_t)ny * nz : (q.normal == 1 ? (size_t)nz : 1);
+    const float *e = q.e_comp == 0 ? ex : (q.e_comp == 1 ? ey : ez);
+    const float *h = q.h_comp == 0 ? hx : (q.h_comp == 1 ? hy : hz);
+    const double mean = 0.5 * ((double)e[lower] + (double)e[lower + step]);
+    const double hv = (double)h[lower];
+    const float *ph = phases + q.phase_offset;
+    for (int f = 0; f < q.nf; ++f) {
+        const double pr = (double)ph[2 * f], pi = (double)ph[2 * f + 1];
+        double2 *ea = reinterpret_cast<double2 *>(q.e_acc) + (size_t)f * cells + c;
+        double2 *ha = reinterpret_cast<double2 *>(q.h_acc) + (size_t)f * cells + c;
+        double2 v = *ea;
+        v.x = v.x + pr * mean;
+        v.y = v.y + pi * mean;
+        *ea = v;
+        double2 w = *ha;
+        w.x = w.x + pr * hv;
+        w.y = w.y + pi * hv;
+        *ha = w;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------- setup
+// da, db per material id (edge_coefficients, kernels3d.py:44-54): mu = mu_r mu0, loss = sigma_m dt / (2 mu).
+__global__ void em3d_h_tables_kernel(const float *t_mu, const float *t_sm, int n, float dt, float *t_da,
+                                     float *t_db) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    const float mu = t_mu[m] * 1.2566370614e-6f;
+    const float loss = t_sm[m] * dt / (2.0f * mu);
+    const float den = 1.0f + loss;
+    t_da[m] = (1.0f - loss) / den;
+    t_db[m] = (dt / mu) / den;
+}
+
+// cb of E component comp on the face of cell (i, j, k) (box_face_cb_3d for a one-cell box, kernels3d.py:745-779).
+__global__ void em3d_face_cb_kernel(const Em3DParams p, int comp, int i, int j, int k, float *out) {
+    const size_t sy = (size_t)p.nz, sx = (size_t)p.ny * p.nz;
+    const size_t idx = (size_t)i * sx + (size_t)j * sy + k;
+    size_t b;
+    float wa, wb;
+    const float *t;
+    if (comp == 0) {
+        b = i + 1 < p.nx ? idx + sx : (p.px ? idx - (size_t)(p.nx - 1) * sx : idx);
+        wa = p.wlx[i];
+        wb = p.wux[i];
+        t = p.t_ex;
+    } else if (comp == 1) {
+        b = j + 1 < p.ny ? idx + sy : (p.py ? idx - (size_t)(p.ny - 1) * sy : idx);
+        wa = p.wly[j];
+        wb = p.wuy[j];
+        t = p.t_ey;
+    } else {
+        b = k + 1 < p.nz ? idx + 1 : (p.pz ? idx - (size_t)(p.nz - 1) : idx);
+        wa = p.wlz[k];
+        wb = p.wuz[k];
+        t = p.t_ez;
+    }
+    float ca, cb;
+    em3d_face(p, t, p.mat[idx], p.mat[b], wa, wb, ca, cb);
+    *out = cb;
+}
+
+// ca, cb of the faces between two cells of the same material id, per E component, with the uniform shares 0.5 / 0.5
+// (the values em3d_face gives those faces; out: per component ca then cb, n_ids each).
+__global__ void em3d_same_tables_kernel(const Em3DParams p, float *out) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= p.n_ids) return;
+    const float *t[3] = {p.t_ex, p.t_ey, p.t_ez};
+    for (int comp = 0; comp < 3; ++comp) {
+        float ca, cb;
+        em3d_face(p, t[comp], (uint16_t)m, (uint16_t)m, 0.5f, 0.5f, ca, cb);
+        out[(2 * comp) * p.n_ids + m] = ca;
+        out[(2 * comp + 1) * p.n_ids + m] = cb;
+    }
+}

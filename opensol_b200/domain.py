@@ -70,6 +70,15 @@ class MaterialGrid:
     def property_names(self):
         return tuple(self.DEFAULTS)
 
+    def add_properties(self, schema: dict):
+        """Register properties with their fill values (core/material_grid.py:45-47): an array filled with a value
+        other than its default is allocated now, the others stay implicit."""
+        for name, value in schema.items():
+            if name not in self.DEFAULTS:
+                raise AttributeError(f"MaterialGrid has no property '{name}'; registered: {list(self.DEFAULTS)}")
+            if DTYPE(value) != DTYPE(self.DEFAULTS[name]) or name in self._arrays:
+                self.array(name).fill(DTYPE(value))
+
     def get(self, name):
         """The array of `name`, or None while it holds its default everywhere."""
         return self._arrays.get(name)

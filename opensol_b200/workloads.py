@@ -52,3 +52,38 @@ def apply(target, ops):
         if method == 'add_flux_monitor':
             monitors.append(out)
     return monitors
+
+
+# 3D: a 512^3 total grid (488^3 window + 12 CPML cells per face) at dx = 20 nm, 500 dielectric spheres (centres uniform
+# in the window interior, radius U(40, 160) nm, eps_r U(2, 12), painted in draw order), a z-polarised Gaussian dipole
+# at the centre at 1310 nm (relative bandwidth 0.5, moment 1e-12 A m) and a closed 8-frequency flux box (faces at 20 %
+# and 80 % of the window); 2,000 steps.
+ROOFLINE_3D = {
+    'total_cells': 512, 'dx': 20e-9, 'npml': 12, 'n_spheres': 500, 'radius': (40e-9, 160e-9), 'eps_r': (2.0, 12.0),
+    'wavelength': 1310e-9, 'bandwidth': 0.5, 'n_freqs': 8, 'steps': 2_000, 'seed': 2025,
+}
+
+
+def roofline_3d_physics(total_cells=512, npml=12, n_spheres=500, seed=2025, device=0):
+    """(EMPhysics3D, flux box) of the 3D workload on a total_cells^3 grid incl. the CPML, not yet finalized."""
+    from .domain3d import BoundaryConfig3D, Domain3D
+    from .physics3d import EMPhysics3D
+    spec = ROOFLINE_3D
+    dx = spec['dx']
+    window = (total_cells - 2 * npml) * dx
+    config = BoundaryConfig3D(npml=npml)
+    domain = Domain3D.uniform(window, window, window, dx, npml_sides=config.npml_sides, boundary_config=config)
+    physics = EMPhysics3D(domain, device=device)
+    rng = np.random.default_rng(seed)
+    radius = rng.uniform(*spec['radius'], n_spheres)
+    centres = rng.uniform(0.15 * window, 0.85 * window, (n_spheres, 3))
+    eps = rng.uniform(*spec['eps_r'], n_spheres)
+    for (cx, cy, cz), r, e in zip(centres, radius, eps):
+        physics.add_dielectric_sphere(float(cx), float(cy), float(cz), float(r), eps_r=float(e))
+    physics.add_dipole(0.5 * window, 0.5 * window, 0.5 * window, orientation='z', dipole_moment=1e-12,
+                       wavelength=spec['wavelength'], bandwidth=spec['bandwidth'])
+    f0 = C0 / spec['wavelength']
+    bw = spec['bandwidth']
+    freqs = np.linspace(f0 * (1 - bw / 2), f0 * (1 + bw / 2), spec['n_freqs']).tolist()
+    box = physics.add_flux_box((0.2 * window,) * 3, (0.8 * window,) * 3, frequencies=freqs)
+    return physics, box

@@ -9,7 +9,8 @@ Run in a container that holds the reference source tree (read-only):
 Each case writes <name>.npz with, per twin kind ('numba_' / 'numpy_' prefix): SHA-256 digests of the six fields at
 every checkpoint, the central x and z planes of every field, every monitor's flux and the SHA-256 of its complex128
 spectra; plus the setup rows (dt, DFT sample interval, material-id digest and eps table, dipole cell, weight and
-dual volume, CPML row maps / recursion / gain rows, kappa-folded curl spacings).
+dual volume, CPML row maps / recursion / gain rows, kappa-folded curl spacings).  material_index3d.npz holds open_sol's
+material index of arrays with more distinct values than the id limit (its re-quantisation path).
 """
 import hashlib
 import json
@@ -112,6 +113,39 @@ def setup_rows(physics, monitors):
     return out
 
 
+def binned_index_cases():
+    """(limit, arrays) of the re-quantisation cases: a continuous eps alone above the limit, and a continuous eps with
+    a four-level sigma whose joint count needs the level budgets halved."""
+    import numpy as np
+    rng = np.random.default_rng(21)
+    shape = (40, 30, 20)
+    eps = rng.uniform(1.0, 12.0, shape).astype(np.float32)
+    sigma = (rng.integers(0, 4, shape).astype(np.float32) * np.float32(2.5e3))
+    ones = np.ones(shape, np.float32)
+    zeros = np.zeros(shape, np.float32)
+    return [(300, {'eps_r': eps, 'sigma_e': zeros, 'mu_r': ones}),
+            (5000, {'eps_r': eps, 'sigma_e': sigma, 'mu_r': ones})]
+
+
+def binned_index_fixture():
+    """open_sol's material index on arrays with more distinct values than the id limit (re-quantised levels)."""
+    import numpy as np
+    from open_sol.physics.em3d.material_index3d import build_material_index
+    out = {}
+    for case, (limit, arrays) in enumerate(binned_index_cases()):
+        shape = arrays['eps_r'].shape
+        ids = np.zeros(shape, np.uint16)
+        chunks = [(slice(start, min(start + 7, shape[0])),) for start in range(0, shape[0], 7)]
+        tables, errors, deltas = build_material_index(arrays, chunks, ids, limit, {})
+        out[f'case{case}_ids'] = ids
+        for name, table in tables.items():
+            out[f'case{case}_table_{name}'] = np.asarray(table)
+        for name, error in errors.items():
+            out[f'case{case}_error_{name}'] = np.float64(error)
+            out[f'case{case}_delta_{name}'] = np.float64(deltas[name])
+    return out
+
+
 def main():
     reference = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('OPENSOL_REFERENCE')
     if not reference:
@@ -137,6 +171,9 @@ def main():
         index[spec['name']] = sorted(out)
         print(f"{spec['name']}: {len(out)} entries, shape {tuple(out['shape'])}, m {int(out['sample_interval'])}, "
               f"dt {float(out['dt']):.6g}")
+    binned = binned_index_fixture()
+    np.savez_compressed(os.path.join(HERE, 'material_index3d.npz'), **binned)
+    index['material_index3d'] = sorted(binned)
     with open(os.path.join(HERE, 'index3d.json'), 'w') as f:
         json.dump({'generated_by': 'tests/golden/make_golden3d.py (open_sol em_fdtd_3d, CPU backend, numba and numpy '
                                    'twins)', 'cases': index}, f, indent=1)
