@@ -178,6 +178,22 @@ int os_fdtd2d_set_stream(OsFdtd2D *h, void *cuda_stream);
  * stream around its launches; 0 before the first advance). */
 int os_fdtd2d_last_advance_ms(OsFdtd2D *h, float *ms);
 
+/* Batched advance of several 2D simulations on one device (the serving loop's step; no open_sol counterpart: open_sol
+ * steps one simulation at a time).  Every T steps, one border launch and one interior launch per template
+ * configuration cover the tiles of all jobs, and one launch folds all their DFT samples; each job's results equal
+ * those of os_fdtd2d_advance.  Jobs must use the blocked kernels with the same steps per launch and be on the batch's
+ * stream (os_fdtd2d_set_stream(job, stream of os_fdtd2d_batch_stream)).  line_values / first_samples / n_samples /
+ * phases: per job, as os_fdtd2d_advance takes them. */
+typedef struct OsFdtd2DBatch OsFdtd2DBatch;
+int os_fdtd2d_batch_create(int32_t device, OsFdtd2DBatch **out);
+int os_fdtd2d_batch_destroy(OsFdtd2DBatch *b);
+int os_fdtd2d_batch_stream(OsFdtd2DBatch *b, void **stream);
+int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handles, int32_t n_jobs, int64_t n_steps,
+                            const float *const *line_values, const int64_t *first_samples, const int64_t *n_samples,
+                            const float *const *phases);
+/* Device milliseconds and kernel launches of the last batched advance (waits for it). */
+int os_fdtd2d_batch_last_ms(OsFdtd2DBatch *b, float *ms, int64_t *launches);
+
 /* ----------------------------------------------------------------------------------------------------------------
  * 3D engine (E_x..H_z): replaces FDTDEngine3D (open_sol/physics/em3d/engine3d.py:157) for a Cartesian grid, one real
  * field set (no Bloch phase) and float32 fields.  Fields (nx, ny, nz) z contiguous, idx = (i * ny + j) * nz + k.

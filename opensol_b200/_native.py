@@ -74,6 +74,12 @@ SIGNATURES = {
     'os_fdtd2d_synchronize': [_P],
     'os_fdtd2d_set_stream': [_P, _P],
     'os_fdtd2d_last_advance_ms': [_P, ctypes.POINTER(ctypes.c_float)],
+    'os_fdtd2d_batch_create': [_I32, ctypes.POINTER(_P)],
+    'os_fdtd2d_batch_destroy': [_P],
+    'os_fdtd2d_batch_stream': [_P, ctypes.POINTER(_P)],
+    'os_fdtd2d_batch_advance': [_P, ctypes.POINTER(_P), _I32, _I64, ctypes.POINTER(_F), ctypes.POINTER(_I64),
+                                ctypes.POINTER(_I64), ctypes.POINTER(_F)],
+    'os_fdtd2d_batch_last_ms': [_P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_I64)],
     'os_fdtd3d_create': [ctypes.POINTER(OsGrid3D), ctypes.POINTER(_P)],
     'os_fdtd3d_destroy': [_P],
     'os_fdtd3d_set_rows': [_P, _F, _F, _F, _F, _F, _F, _F],

@@ -19,6 +19,7 @@
 #include <vector>
 #include <memory>
 #include <mutex>
+#include <cstring>
 
 namespace os {
 
@@ -1046,5 +1047,308 @@ extern "C" int os_fdtd2d_last_advance_ms(OsFdtd2D *h, float *ms) {
     OS_TRY(bind_device(h));
     OS_CUDA(cudaEventSynchronize(h->ev_stop));
     OS_CUDA(cudaEventElapsedTime(ms, h->ev_start, h->ev_stop));
+    return OS_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Batched advance of several simulations on one device: every T steps one border launch and one interior launch per
+// template configuration cover the tiles of all of them (a warp finds its simulation in a prefix table of tile
+// counts), and one launch folds the DFT samples of all their flux lines.  Each simulation's arithmetic is exactly
+// that of os_fdtd2d_advance, so its results are the same alone and in the batch.  The per-launch parameters of the
+// whole call are built on the host into one page-locked block and reach the device in one copy.
+struct OsFdtd2DBatch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_copied = nullptr, ev_start = nullptr, ev_stop = nullptr;
+    bool copy_pending = false, timed = false;
+    unsigned char *host = nullptr;     // page-locked staging of one call's launch parameters
+    size_t host_capacity = 0;
+    os::DeviceArray<unsigned char> dev;
+    int64_t launches = 0;
+};
+
+namespace os {
+
+struct BatchGroup {                    // one kernel launch of a batched step: jobs sharing a template configuration
+    int kind;                          // 0 interior, 1 general
+    bool ca, px, py;
+    std::vector<TBParams> params;
+    std::vector<int> tile_start{0};
+    size_t params_off = 0, tiles_off = 0;
+};
+
+struct BatchLaunch {
+    int T;
+    std::vector<BatchGroup> groups;
+    std::vector<FluxBatchItem> items;
+    int max_item_cells = 0;
+    size_t items_off = 0;
+};
+
+static BatchGroup &batch_group(BatchLaunch &L, int kind, bool ca, bool px, bool py) {
+    for (auto &g : L.groups)
+        if (g.kind == kind && g.ca == ca && g.px == px && g.py == py) return g;
+    L.groups.push_back(BatchGroup{kind, ca, px, py, {}, {0}, 0, 0});
+    return L.groups.back();
+}
+
+template <int T, bool CA, bool PX, bool PY>
+static int launch_interior_batch(cudaStream_t s, const TBParams *jobs, const int *tiles, int n_jobs, int total) {
+    const size_t smem = (size_t)TB_WARPS * tb_warp_smem_bytes(T, CA);
+    static bool attr_set = false;
+    if (!attr_set) {
+        OS_CUDA(cudaFuncSetAttribute(ez2d_interior_batch_kernel<T, CA, PX, PY>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    ez2d_interior_batch_kernel<T, CA, PX, PY>
+        <<<(unsigned)((total + TB_WARPS - 1) / TB_WARPS), TB_WARPS * 32, smem, s>>>(jobs, tiles, n_jobs);
+    return OS_OK;
+}
+
+template <int T>
+static int launch_group(cudaStream_t s, const BatchGroup &g, const unsigned char *dev) {
+    const TBParams *jobs = reinterpret_cast<const TBParams *>(dev + g.params_off);
+    const int *tiles = reinterpret_cast<const int *>(dev + g.tiles_off);
+    const int n = (int)g.params.size(), total = g.tile_start.back();
+    if (!total) return OS_OK;
+    if (g.kind == 1) {
+        const dim3 blocks((unsigned)((total + TB_WARPS - 1) / TB_WARPS));
+        if (g.ca) ez2d_tb_batch_kernel<T, 1, true, true><<<blocks, TB_WARPS * 32, 0, s>>>(jobs, tiles, n);
+        else ez2d_tb_batch_kernel<T, 1, true, false><<<blocks, TB_WARPS * 32, 0, s>>>(jobs, tiles, n);
+        return OS_OK;
+    }
+    if (g.ca) {
+        if (g.px && g.py) return launch_interior_batch<T, true, true, true>(s, jobs, tiles, n, total);
+        if (g.px) return launch_interior_batch<T, true, true, false>(s, jobs, tiles, n, total);
+        if (g.py) return launch_interior_batch<T, true, false, true>(s, jobs, tiles, n, total);
+        return launch_interior_batch<T, true, false, false>(s, jobs, tiles, n, total);
+    }
+    if (g.px && g.py) return launch_interior_batch<T, false, true, true>(s, jobs, tiles, n, total);
+    if (g.px) return launch_interior_batch<T, false, true, false>(s, jobs, tiles, n, total);
+    if (g.py) return launch_interior_batch<T, false, false, true>(s, jobs, tiles, n, total);
+    return launch_interior_batch<T, false, false, false>(s, jobs, tiles, n, total);
+}
+
+static int launch_group_any(int T, cudaStream_t s, const BatchGroup &g, const unsigned char *dev) {
+    switch (T) {
+        case 1: return launch_group<1>(s, g, dev);
+        case 2: return launch_group<2>(s, g, dev);
+        case 3: return launch_group<3>(s, g, dev);
+        default: return launch_group<4>(s, g, dev);
+    }
+}
+
+static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+}  // namespace os
+
+extern "C" int os_fdtd2d_batch_create(int32_t device, OsFdtd2DBatch **out) {
+    OS_CHECK(out, OS_ERR_INVALID, "os_fdtd2d_batch_create: null argument");
+    *out = nullptr;
+    std::unique_ptr<OsFdtd2DBatch> b(new OsFdtd2DBatch());
+    b->device = device;
+    OS_CUDA(cudaSetDevice(device));
+    OS_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    OS_CUDA(cudaEventCreateWithFlags(&b->ev_copied, cudaEventDisableTiming));
+    OS_CUDA(cudaEventCreate(&b->ev_start));
+    OS_CUDA(cudaEventCreate(&b->ev_stop));
+    *out = b.release();
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_batch_destroy(OsFdtd2DBatch *b) {
+    if (!b) return OS_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->host) cudaFreeHost(b->host);
+    if (b->ev_copied) cudaEventDestroy(b->ev_copied);
+    if (b->ev_start) cudaEventDestroy(b->ev_start);
+    if (b->ev_stop) cudaEventDestroy(b->ev_stop);
+    cudaStream_t s = b->stream;
+    delete b;
+    if (s) cudaStreamDestroy(s);
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_batch_stream(OsFdtd2DBatch *b, void **stream) {
+    OS_CHECK(b && stream, OS_ERR_INVALID, "os_fdtd2d_batch_stream: null argument");
+    *stream = (void *)b->stream;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handles, int32_t n_jobs, int64_t n_steps,
+                                       const float *const *line_values, const int64_t *first_samples,
+                                       const int64_t *n_samples, const float *const *phases) {
+    using namespace os;
+    OS_CHECK(b && (n_jobs == 0 || (handles && line_values && first_samples && n_samples && phases)), OS_ERR_INVALID,
+             "os_fdtd2d_batch_advance: null argument");
+    OS_CHECK(n_jobs >= 0 && n_steps >= 0, OS_ERR_INVALID, "os_fdtd2d_batch_advance: negative count");
+    b->launches = 0;
+    if (n_jobs == 0 || n_steps == 0) return OS_OK;
+    const int T = handles[0]->steps_per_launch;
+    for (int32_t q = 0; q < n_jobs; ++q) {
+        OsFdtd2D *h = handles[q];
+        OS_CHECK(h, OS_ERR_INVALID, "os_fdtd2d_batch_advance: job %d has no handle", q);
+        OS_TRY(check_advance(h, "os_fdtd2d_batch_advance", n_steps, line_values[q], first_samples[q], n_samples[q],
+                             phases[q]));
+        OS_CHECK(h->device == b->device, OS_ERR_INVALID, "os_fdtd2d_batch_advance: job %d is on device %d, the batch on "
+                 "%d", q, h->device, b->device);
+        OS_CHECK(h->variant != 0 && h->steps_per_launch == T, OS_ERR_INVALID,
+                 "os_fdtd2d_batch_advance: every job needs the blocked kernels with the same steps per launch (%d)", T);
+        OS_CHECK(h->stream == b->stream, OS_ERR_STATE,
+                 "os_fdtd2d_batch_advance: job %d is not on the batch stream (os_fdtd2d_set_stream with "
+                 "os_fdtd2d_batch_stream)", q);
+        OS_CHECK(!h->profiling, OS_ERR_STATE, "os_fdtd2d_batch_advance: job %d has profiling on", q);
+    }
+    OS_CUDA(cudaSetDevice(b->device));
+    // every job's own tables, in its own buffers, as os_fdtd2d_advance uploads them
+    for (int32_t q = 0; q < n_jobs; ++q) {
+        OsFdtd2D *h = handles[q];
+        h->launches = 0;
+        h->prof_used = 0;
+        if (!h->lines.empty()) OS_TRY(upload(h->line_values, line_values[q], h->lines.size() * (size_t)n_steps,
+                                             b->stream));
+        size_t phase_floats = 0;
+        for (auto &f : h->fluxes) phase_floats += (size_t)n_samples[q] * f->nf * 2;
+        if (!h->fluxes.empty() && phase_floats && phases[q])
+            OS_TRY(upload(h->phases, phases[q], phase_floats, b->stream));
+    }
+    // plans of the full-T launches and of the shorter last one, per job
+    const int64_t n_launch = (n_steps + T - 1) / T;
+    const int T_last = (int)(n_steps - (n_launch - 1) * T);
+    struct Plan {
+        TBParams interior{}, general{};
+        bool has_interior = false;
+    };
+    std::vector<Plan> plan_full(n_jobs), plan_last(n_jobs);
+    for (int32_t q = 0; q < n_jobs; ++q) {
+        plan_tiles(handles[q], T, plan_full[q].interior, plan_full[q].general, plan_full[q].has_interior);
+        plan_tiles(handles[q], T_last, plan_last[q].interior, plan_last[q].general, plan_last[q].has_interior);
+        for (Plan *pl : {&plan_full[q], &plan_last[q]}) {
+            fill_common(handles[q], pl->interior);
+            fill_common(handles[q], pl->general);
+        }
+    }
+    std::vector<BatchLaunch> launches((size_t)n_launch);
+    for (int64_t l = 0; l < n_launch; ++l) {
+        BatchLaunch &L = launches[(size_t)l];
+        L.T = l + 1 < n_launch ? T : T_last;
+        for (int32_t q = 0; q < n_jobs; ++q) {
+            OsFdtd2D *h = handles[q];
+            const Plan &pl = l + 1 < n_launch ? plan_full[q] : plan_last[q];
+            const int in = (h->cur + (int)(l & 1)) & 1, out = in ^ 1;
+            const int64_t m = h->sample_interval, n0 = h->n_step + l * T;
+            uint32_t mask = 0;
+            for (int st = 1; st <= L.T; ++st)
+                if ((n0 + st) % m == 0) mask |= 1u << (st - 1);
+            if (h->fluxes.empty()) mask = 0;
+            for (int kind = 1; kind >= 0; --kind) {
+                const TBParams &base = kind == 0 ? pl.interior : pl.general;
+                if (kind == 0 && !pl.has_interior) continue;
+                if (!base.n_tiles) continue;
+                BatchGroup &g = batch_group(L, kind, h->has_ca, kind == 0 && h->grid.periodic_x,
+                                            kind == 0 && h->grid.periodic_y);
+                g.params.push_back(base);
+                TBParams &p = g.params.back();
+                bind_buffers(h, p, in, out);
+                p.line_values = h->line_values.ptr;
+                p.values_stride = n_steps;
+                p.k0 = l * T;
+                p.n0 = n0;
+                p.q_first = n0 / m + 1;
+                p.sample_mask = mask;
+                g.tile_start.push_back(g.tile_start.back() + p.n_tiles);
+            }
+            const int64_t q_lo = n0 / m + 1, q_hi = (n0 + L.T) / m;
+            if (!h->fluxes.empty() && q_hi >= q_lo) {
+                size_t offset = 0;
+                for (auto &f : h->fluxes) {
+                    FluxBatchItem it{};
+                    it.stage = f->stage.ptr;
+                    it.phases = h->phases.ptr + offset + (size_t)(q_lo - first_samples[q]) * f->nf * 2;
+                    it.e_acc = f->e_acc.ptr;
+                    it.h_acc = f->h_acc.ptr;
+                    it.n = f->hi - f->lo;
+                    it.nf = f->nf;
+                    it.n_q = (int)(q_hi - q_lo + 1);
+                    L.items.push_back(it);
+                    L.max_item_cells = std::max(L.max_item_cells, it.n * it.nf);
+                    offset += (size_t)n_samples[q] * f->nf * 2;
+                }
+            }
+        }
+    }
+    // one page-locked block for the whole call, one copy to the device
+    size_t total = 0;
+    for (auto &L : launches) {
+        for (auto &g : L.groups) {
+            g.params_off = total = align_up(total, 16);
+            total += g.params.size() * sizeof(TBParams);
+            g.tiles_off = total = align_up(total, 16);
+            total += g.tile_start.size() * sizeof(int);
+        }
+        L.items_off = total = align_up(total, 16);
+        total += L.items.size() * sizeof(FluxBatchItem);
+    }
+    if (b->copy_pending) {   // the previous call's copy still reads the staging block
+        OS_CUDA(cudaEventSynchronize(b->ev_copied));
+        b->copy_pending = false;
+    }
+    if (total > b->host_capacity) {
+        if (b->host) OS_CUDA(cudaFreeHost(b->host));
+        b->host = nullptr;
+        b->host_capacity = 0;
+        OS_CUDA(cudaHostAlloc((void **)&b->host, total, cudaHostAllocPortable));
+        b->host_capacity = total;
+    }
+    for (auto &L : launches) {
+        for (auto &g : L.groups) {
+            memcpy(b->host + g.params_off, g.params.data(), g.params.size() * sizeof(TBParams));
+            memcpy(b->host + g.tiles_off, g.tile_start.data(), g.tile_start.size() * sizeof(int));
+        }
+        if (!L.items.empty()) memcpy(b->host + L.items_off, L.items.data(), L.items.size() * sizeof(FluxBatchItem));
+    }
+    OS_TRY(b->dev.alloc(total));
+    OS_CUDA(cudaMemcpyAsync(b->dev.ptr, b->host, total, cudaMemcpyHostToDevice, b->stream));
+    OS_CUDA(cudaEventRecord(b->ev_copied, b->stream));
+    b->copy_pending = true;
+    OS_CUDA(cudaEventRecord(b->ev_start, b->stream));
+    for (auto &L : launches) {
+        for (auto &g : L.groups) {
+            if (g.kind != 1) continue;
+            OS_TRY(launch_group_any(L.T, b->stream, g, b->dev.ptr));
+            b->launches += 1;
+        }
+        for (auto &g : L.groups) {
+            if (g.kind != 0) continue;
+            OS_TRY(launch_group_any(L.T, b->stream, g, b->dev.ptr));
+            b->launches += 1;
+        }
+        if (!L.items.empty()) {
+            const dim3 grid((unsigned)((L.max_item_cells + 255) / 256), (unsigned)L.items.size());
+            ez2d_flux_staged_batch_kernel<<<grid, 256, 0, b->stream>>>(
+                reinterpret_cast<const FluxBatchItem *>(b->dev.ptr + L.items_off));
+            b->launches += 1;
+        }
+    }
+    OS_CUDA(cudaGetLastError());
+    OS_CUDA(cudaEventRecord(b->ev_stop, b->stream));
+    b->timed = true;
+    for (int32_t q = 0; q < n_jobs; ++q) {
+        OsFdtd2D *h = handles[q];
+        h->cur = (h->cur + (int)(n_launch & 1)) & 1;
+        h->n_step += n_steps;
+    }
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_batch_last_ms(OsFdtd2DBatch *b, float *ms, int64_t *launches) {
+    OS_CHECK(b && ms && launches, OS_ERR_INVALID, "os_fdtd2d_batch_last_ms: null argument");
+    OS_CHECK(b->timed, OS_ERR_STATE, "os_fdtd2d_batch_last_ms: no batched advance yet");
+    OS_CUDA(cudaSetDevice(b->device));
+    OS_CUDA(cudaEventSynchronize(b->ev_stop));
+    OS_CUDA(cudaEventElapsedTime(ms, b->ev_start, b->ev_stop));
+    *launches = b->launches;
     return OS_OK;
 }

@@ -250,11 +250,10 @@ struct IPWarp {
     }
 };
 
+// One warp's tile w of the interior plan p (tb_smem: the block's dynamic shared memory).
 template <int T, bool CA, bool PX, bool PY>
-__global__ void __launch_bounds__(TB_WARPS * 32) ez2d_interior_kernel(const TBParams p) {
-    extern __shared__ __align__(16) unsigned char tb_smem[];
+__device__ __forceinline__ void ez2d_interior_tile(const TBParams &p, int w, unsigned char *tb_smem) {
     const int lane = threadIdx.x & 31;
-    const int w = blockIdx.x * TB_WARPS + (threadIdx.x >> 5);
     if (w >= p.n_tiles) return;   // whole warps leave together
     int rect = 0;
     for (int q = 1; q < p.n_rects; ++q)
@@ -354,4 +353,24 @@ __global__ void __launch_bounds__(TB_WARPS * 32) ez2d_interior_kernel(const TBPa
             }
         }
     }
+}
+
+template <int T, bool CA, bool PX, bool PY>
+__global__ void __launch_bounds__(TB_WARPS * 32) ez2d_interior_kernel(const TBParams p) {
+    extern __shared__ __align__(16) unsigned char tb_smem[];
+    ez2d_interior_tile<T, CA, PX, PY>(p, blockIdx.x * TB_WARPS + (threadIdx.x >> 5), tb_smem);
+}
+
+// Several simulations in one launch: warp g runs tile g - tile_start[job] of jobs[job], tile_start ascending with
+// tile_start[n_jobs] = the total (every job shares T and the template configuration).
+template <int T, bool CA, bool PX, bool PY>
+__global__ void __launch_bounds__(TB_WARPS * 32) ez2d_interior_batch_kernel(const TBParams *__restrict__ jobs,
+                                                                         const int *__restrict__ tile_start,
+                                                                         int n_jobs) {
+    extern __shared__ __align__(16) unsigned char tb_smem[];
+    const int g = blockIdx.x * TB_WARPS + (threadIdx.x >> 5);
+    if (g >= tile_start[n_jobs]) return;
+    int job = 0;
+    while (job + 1 < n_jobs && g >= tile_start[job + 1]) ++job;
+    ez2d_interior_tile<T, CA, PX, PY>(jobs[job], g - tile_start[job], tb_smem);
 }

@@ -620,10 +620,8 @@ struct TBWarp {
 };
 
 template <int T, int C, bool GEN, bool CA>
-__global__ void __launch_bounds__(TB_WARPS * 32) ez2d_tb_kernel(const TBParams p) {
-    extern __shared__ __align__(16) unsigned char tb_smem[];
+__device__ __forceinline__ void ez2d_tb_tile(const TBParams &p, int w, unsigned char *tb_smem) {
     const int lane = threadIdx.x & 31;
-    const int w = blockIdx.x * TB_WARPS + (threadIdx.x >> 5);
     if (w >= p.n_tiles) return;   // whole warps leave together (the shuffles below need all 32 lanes)
     int rect = 0;
     for (int q = 1; q < p.n_rects; ++q)
@@ -740,11 +738,28 @@ __global__ void __launch_bounds__(TB_WARPS * 32) ez2d_tb_kernel(const TBParams p
     }
 }
 
+template <int T, int C, bool GEN, bool CA>
+__global__ void __launch_bounds__(TB_WARPS * 32) ez2d_tb_kernel(const TBParams p) {
+    extern __shared__ __align__(16) unsigned char tb_smem[];
+    ez2d_tb_tile<T, C, GEN, CA>(p, blockIdx.x * TB_WARPS + (threadIdx.x >> 5), tb_smem);
+}
+
+// Several simulations in one launch (as ez2d_interior_batch_kernel).
+template <int T, int C, bool GEN, bool CA>
+__global__ void __launch_bounds__(TB_WARPS * 32) ez2d_tb_batch_kernel(const TBParams *__restrict__ jobs,
+                                                                   const int *__restrict__ tile_start, int n_jobs) {
+    extern __shared__ __align__(16) unsigned char tb_smem[];
+    const int g = blockIdx.x * TB_WARPS + (threadIdx.x >> 5);
+    if (g >= tile_start[n_jobs]) return;
+    int job = 0;
+    while (job + 1 < n_jobs && g >= tile_start[job + 1]) ++job;
+    ez2d_tb_tile<T, C, GEN, CA>(jobs[job], g - tile_start[job], tb_smem);
+}
+
 // Running DFTs of one flux line from the staged samples of one launch, in sample order (monitors.py:45-46,84-90).
-__global__ void ez2d_flux_staged_kernel(const float *__restrict__ stage, int n, int nf, int n_q,
-                                        const float *__restrict__ phases, double *__restrict__ e_acc,
-                                        double *__restrict__ h_acc) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void ez2d_flux_staged(int t, const float *__restrict__ stage, int n, int nf, int n_q,
+                                                 const float *__restrict__ phases, double *__restrict__ e_acc,
+                                                 double *__restrict__ h_acc) {
     if (t >= n * nf) return;
     const int f = t / n, c = t - f * n;
     const size_t a = ((size_t)f * n + c) * 2;
@@ -761,4 +776,24 @@ __global__ void ez2d_flux_staged_kernel(const float *__restrict__ stage, int n, 
     e_acc[a + 1] = ei;
     h_acc[a] = hr;
     h_acc[a + 1] = hi;
+}
+
+__global__ void ez2d_flux_staged_kernel(const float *__restrict__ stage, int n, int nf, int n_q,
+                                        const float *__restrict__ phases, double *__restrict__ e_acc,
+                                        double *__restrict__ h_acc) {
+    ez2d_flux_staged(blockIdx.x * blockDim.x + threadIdx.x, stage, n, nf, n_q, phases, e_acc, h_acc);
+}
+
+// One flux line of one simulation in a batched launch.
+struct FluxBatchItem {
+    const float *stage;
+    const float *phases;
+    double *e_acc, *h_acc;
+    int32_t n, nf, n_q, pad;
+};
+
+__global__ void ez2d_flux_staged_batch_kernel(const FluxBatchItem *__restrict__ items) {
+    const FluxBatchItem it = items[blockIdx.y];
+    ez2d_flux_staged(blockIdx.x * blockDim.x + threadIdx.x, it.stage, it.n, it.nf, it.n_q, it.phases, it.e_acc,
+                     it.h_acc);
 }
