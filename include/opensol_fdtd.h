@@ -194,6 +194,26 @@ int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handles, int32_t 
 /* Device milliseconds and kernel launches of the last batched advance (waits for it). */
 int os_fdtd2d_batch_last_ms(OsFdtd2DBatch *b, float *ms, int64_t *launches);
 
+/* Discrete adjoint of a 2D simulation for d(objective)/d(eps_r) on a design box (no open_sol counterpart: open_sol has
+ * no FDTD adjoint).  Checkpoint slots of the full state (fields and psi of the live buffers) are filled by
+ * os_fdtd2d_adjoint_save during the forward run; os_fdtd2d_adjoint_segment restores a slot, recomputes n_steps from
+ * it with the per-step kernels while recording E over the box, then runs the transposed steps backward through the
+ * segment: at the steps source_steps (increasing, indices within the segment) the adjoint sources dJ/de and dJ/dh
+ * of DFT samples of flux line monitor_id enter (n_sources x line cells each), and the box accumulates
+ * sum lambda_E (E^{n+1} - E^n) in float64 (os_fdtd2d_adjoint_gradient; dJ/deps_r = -that / eps_r where
+ * cb = dt / (eps_r eps0)).  Segments run last to first after os_fdtd2d_adjoint_reset; the live fields hold the
+ * recomputed state afterwards (reset the simulation before another forward run). */
+typedef struct OsAdjoint2D OsAdjoint2D;
+int os_fdtd2d_adjoint_create(OsFdtd2D *h, int32_t box_i0, int32_t box_i1, int32_t box_j0, int32_t box_j1,
+                             int32_t n_slots, int32_t segment_steps, OsAdjoint2D **out);
+int os_fdtd2d_adjoint_destroy(OsAdjoint2D *a);
+int os_fdtd2d_adjoint_save(OsAdjoint2D *a, int32_t slot);
+int os_fdtd2d_adjoint_reset(OsAdjoint2D *a);
+int os_fdtd2d_adjoint_segment(OsAdjoint2D *a, int32_t slot, int64_t step0, int32_t n_steps, const float *line_values,
+                              int32_t monitor_id, int32_t n_sources, const int32_t *source_steps,
+                              const float *source_e, const float *source_h);
+int os_fdtd2d_adjoint_gradient(OsAdjoint2D *a, double *out);
+
 /* ----------------------------------------------------------------------------------------------------------------
  * 3D engine (E_x..H_z): replaces FDTDEngine3D (open_sol/physics/em3d/engine3d.py:157) for a Cartesian grid, one real
  * field set (no Bloch phase) and float32 fields.  Fields (nx, ny, nz) z contiguous, idx = (i * ny + j) * nz + k.

@@ -80,6 +80,12 @@ SIGNATURES = {
     'os_fdtd2d_batch_advance': [_P, ctypes.POINTER(_P), _I32, _I64, ctypes.POINTER(_F), ctypes.POINTER(_I64),
                                 ctypes.POINTER(_I64), ctypes.POINTER(_F)],
     'os_fdtd2d_batch_last_ms': [_P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_I64)],
+    'os_fdtd2d_adjoint_create': [_P, _I32, _I32, _I32, _I32, _I32, _I32, ctypes.POINTER(_P)],
+    'os_fdtd2d_adjoint_destroy': [_P],
+    'os_fdtd2d_adjoint_save': [_P, _I32],
+    'os_fdtd2d_adjoint_reset': [_P],
+    'os_fdtd2d_adjoint_segment': [_P, _I32, _I64, _I32, _F, _I32, _I32, ctypes.POINTER(_I32), _F, _F],
+    'os_fdtd2d_adjoint_gradient': [_P, _D],
     'os_fdtd3d_create': [ctypes.POINTER(OsGrid3D), ctypes.POINTER(_P)],
     'os_fdtd3d_destroy': [_P],
     'os_fdtd3d_set_rows': [_P, _F, _F, _F, _F, _F, _F, _F],

@@ -1352,3 +1352,259 @@ extern "C" int os_fdtd2d_batch_last_ms(OsFdtd2DBatch *b, float *ms, int64_t *lau
     *launches = b->launches;
     return OS_OK;
 }
+
+// ---------------------------------------------------------------------------------------------------------------
+// Discrete adjoint of a 2D E_z simulation (fdtd2d_adjoint.cuh): checkpoints of the forward state, recomputation of a
+// segment from its checkpoint with the per-step kernels (bit-identical to every other kernel choice) while the E of
+// the design box is recorded, then the transposed steps backward through the segment.
+#include "fdtd2d_adjoint.cuh"
+
+struct OsAdjoint2D {
+    OsFdtd2D *h = nullptr;
+    int32_t bi0 = 0, bi1 = 0, bj0 = 0, bj1 = 0;
+    int32_t n_slots = 0, seg_steps = 0;
+    size_t slot_floats = 0;
+    os::DeviceArray<float> ckpt;                       // n_slots x (ez, hx, hy, psi_e sides, psi_h sides)
+    os::DeviceArray<float> le[2], lhx[2], lhy[2];
+    os::DeviceArray<float> lpe[2][4], lph[2][4];
+    int e_par = 0;                                     // live parity of lambda_E and the psi adjoints
+    os::DeviceArray<float> rec;                        // (seg_steps + 1) x box
+    os::DeviceArray<double> grad;                      // box
+    os::DeviceArray<float> values, src_e, src_h;
+};
+
+namespace os {
+
+static size_t adj_box(const OsAdjoint2D *a) { return (size_t)(a->bi1 - a->bi0) * (size_t)(a->bj1 - a->bj0); }
+
+// (device pointer, floats) of every piece of one checkpoint in slot order
+static void adj_pieces(OsAdjoint2D *a, std::vector<std::pair<float *, size_t>> &out) {
+    OsFdtd2D *h = a->h;
+    const size_t n = cells(h);
+    const int c = h->cur;
+    out.clear();
+    out.push_back({h->ez[c].ptr, n});
+    out.push_back({h->hx[c].ptr, n});
+    out.push_back({h->hy[c].ptr, n});
+    for (int s = 0; s < 4; ++s) {
+        if (h->psi_e[c][s].ptr) out.push_back({h->psi_e[c][s].ptr, h->psi_e[c][s].count});
+        if (h->psi_h[c][s].ptr) out.push_back({h->psi_h[c][s].ptr, h->psi_h[c][s].count});
+    }
+}
+
+static Ez2DAdjParams adj_params(OsAdjoint2D *a) {
+    OsFdtd2D *h = a->h;
+    Ez2DAdjParams p{};
+    p.nx = h->grid.nx;
+    p.ny = h->grid.ny;
+    p.px = h->grid.periodic_x;
+    p.py = h->grid.periodic_y;
+    p.npml = h->grid.npml;
+    p.cpml_mask = h->grid.cpml_sides;
+    p.ca = h->has_ca ? h->ca.ptr : nullptr;
+    p.cb = h->cb.ptr;
+    p.da = h->has_dadb ? h->da.ptr : nullptr;
+    p.db = h->has_dadb ? h->db.ptr : nullptr;
+    p.da_u = h->da_uniform;
+    p.db_u = h->db_uniform;
+    p.ixe = h->inv_dx_e.ptr;
+    p.ixh = h->inv_dx_h.ptr;
+    p.iye = h->inv_dy_e.ptr;
+    p.iyh = h->inv_dy_h.ptr;
+    const int npml = h->grid.npml;
+    for (int s = 0; s < 4; ++s) {
+        if (!(h->grid.cpml_sides & (1 << s))) continue;
+        const float *rows = h->cpml_rows[s].ptr;
+        p.b_e[s] = rows;
+        p.a_e[s] = rows + npml;
+        p.inv_e[s] = rows + 2 * npml;
+        p.b_h[s] = rows + 3 * npml;
+        p.a_h[s] = rows + 4 * npml;
+        p.inv_h[s] = rows + 5 * npml;
+    }
+    p.bi0 = a->bi0;
+    p.bi1 = a->bi1;
+    p.bj0 = a->bj0;
+    p.bj1 = a->bj1;
+    p.grad = a->grad.ptr;
+    return p;
+}
+
+}  // namespace os
+
+extern "C" int os_fdtd2d_adjoint_create(OsFdtd2D *h, int32_t box_i0, int32_t box_i1, int32_t box_j0, int32_t box_j1,
+                                        int32_t n_slots, int32_t segment_steps, OsAdjoint2D **out) {
+    using namespace os;
+    OS_CHECK(h && out, OS_ERR_INVALID, "os_fdtd2d_adjoint_create: null argument");
+    *out = nullptr;
+    OS_CHECK(h->has_cb && h->has_spacings, OS_ERR_STATE, "os_fdtd2d_adjoint_create: coefficients and spacings first");
+    OS_CHECK(0 <= box_i0 && box_i0 < box_i1 && box_i1 <= h->grid.nx && 0 <= box_j0 && box_j0 < box_j1 &&
+                 box_j1 <= h->grid.ny, OS_ERR_INVALID, "os_fdtd2d_adjoint_create: design box outside the grid");
+    OS_CHECK(n_slots >= 1 && segment_steps >= 1, OS_ERR_INVALID, "os_fdtd2d_adjoint_create: bad checkpoint layout");
+    std::unique_ptr<OsAdjoint2D> a(new OsAdjoint2D());
+    a->h = h;
+    a->bi0 = box_i0;
+    a->bi1 = box_i1;
+    a->bj0 = box_j0;
+    a->bj1 = box_j1;
+    a->n_slots = n_slots;
+    a->seg_steps = segment_steps;
+    OS_TRY(bind_device(h));
+    std::vector<std::pair<float *, size_t>> pieces;
+    adj_pieces(a.get(), pieces);
+    for (auto &pc : pieces) a->slot_floats += pc.second;
+    OS_TRY(a->ckpt.alloc(a->slot_floats * (size_t)n_slots));
+    const size_t n = cells(h);
+    for (int b = 0; b < 2; ++b) {
+        OS_TRY(a->le[b].alloc(n));
+        OS_TRY(a->lhx[b].alloc(n));
+        OS_TRY(a->lhy[b].alloc(n));
+        for (int s = 0; s < 4; ++s) {
+            if (!(h->grid.cpml_sides & (1 << s))) continue;
+            OS_TRY(a->lpe[b][s].alloc(h->psi_e[0][s].count));
+            OS_TRY(a->lph[b][s].alloc(h->psi_h[0][s].count));
+        }
+    }
+    OS_TRY(a->rec.alloc((size_t)(segment_steps + 1) * adj_box(a.get())));
+    OS_TRY(a->grad.alloc(adj_box(a.get())));
+    *out = a.release();
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_adjoint_destroy(OsAdjoint2D *a) {
+    if (!a) return OS_OK;
+    cudaSetDevice(a->h->device);
+    cudaStreamSynchronize(a->h->stream);
+    delete a;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_adjoint_save(OsAdjoint2D *a, int32_t slot) {
+    using namespace os;
+    OS_CHECK(a && slot >= 0 && slot < a->n_slots, OS_ERR_INVALID, "os_fdtd2d_adjoint_save: no slot %d", slot);
+    OS_TRY(bind_device(a->h));
+    std::vector<std::pair<float *, size_t>> pieces;
+    adj_pieces(a, pieces);
+    float *dst = a->ckpt.ptr + (size_t)slot * a->slot_floats;
+    for (auto &pc : pieces) {
+        OS_CUDA(cudaMemcpyAsync(dst, pc.first, pc.second * sizeof(float), cudaMemcpyDeviceToDevice, a->h->stream));
+        dst += pc.second;
+    }
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_adjoint_reset(OsAdjoint2D *a) {
+    using namespace os;
+    OS_CHECK(a, OS_ERR_INVALID, "os_fdtd2d_adjoint_reset: null handle");
+    OS_TRY(bind_device(a->h));
+    cudaStream_t s = a->h->stream;
+    for (int b = 0; b < 2; ++b) {
+        for (DeviceArray<float> *d : {&a->le[b], &a->lhx[b], &a->lhy[b]})
+            OS_CUDA(cudaMemsetAsync(d->ptr, 0, d->bytes(), s));
+        for (int q = 0; q < 4; ++q) {
+            if (a->lpe[b][q].ptr) OS_CUDA(cudaMemsetAsync(a->lpe[b][q].ptr, 0, a->lpe[b][q].bytes(), s));
+            if (a->lph[b][q].ptr) OS_CUDA(cudaMemsetAsync(a->lph[b][q].ptr, 0, a->lph[b][q].bytes(), s));
+        }
+    }
+    OS_CUDA(cudaMemsetAsync(a->grad.ptr, 0, a->grad.bytes(), s));
+    a->e_par = 0;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_adjoint_segment(OsAdjoint2D *a, int32_t slot, int64_t step0, int32_t n_steps,
+                                         const float *line_values, int32_t monitor_id, int32_t n_sources,
+                                         const int32_t *source_steps, const float *source_e, const float *source_h) {
+    using namespace os;
+    OS_CHECK(a && slot >= 0 && slot < a->n_slots, OS_ERR_INVALID, "os_fdtd2d_adjoint_segment: no slot %d", slot);
+    OsFdtd2D *h = a->h;
+    OS_CHECK(n_steps >= 1 && n_steps <= a->seg_steps, OS_ERR_INVALID,
+             "os_fdtd2d_adjoint_segment: %d steps, the segment holds at most %d", n_steps, a->seg_steps);
+    OS_CHECK(h->lines.empty() || line_values, OS_ERR_INVALID, "os_fdtd2d_adjoint_segment: line_values is required");
+    OS_CHECK(monitor_id >= 0 && monitor_id < (int32_t)h->fluxes.size(), OS_ERR_INVALID,
+             "os_fdtd2d_adjoint_segment: no monitor %d", monitor_id);
+    OS_CHECK(n_sources == 0 || (source_steps && source_e && source_h), OS_ERR_INVALID,
+             "os_fdtd2d_adjoint_segment: adjoint sources are required");
+    for (int32_t q = 0; q < n_sources; ++q)
+        OS_CHECK(source_steps[q] >= 0 && source_steps[q] < n_steps && (q == 0 || source_steps[q] > source_steps[q - 1]),
+                 OS_ERR_INVALID, "os_fdtd2d_adjoint_segment: source steps must be increasing within the segment");
+    OS_TRY(bind_device(h));
+    cudaStream_t s = h->stream;
+    // restore the checkpoint into the live buffers
+    {
+        std::vector<std::pair<float *, size_t>> pieces;
+        adj_pieces(a, pieces);
+        const float *src = a->ckpt.ptr + (size_t)slot * a->slot_floats;
+        for (auto &pc : pieces) {
+            OS_CUDA(cudaMemcpyAsync(pc.first, src, pc.second * sizeof(float), cudaMemcpyDeviceToDevice, s));
+            src += pc.second;
+        }
+    }
+    if (!h->lines.empty()) OS_TRY(upload(a->values, line_values, h->lines.size() * (size_t)n_steps, s));
+    const FluxLine2D &mon = *h->fluxes[monitor_id];
+    const int n_line = mon.hi - mon.lo;
+    if (n_sources) {
+        OS_TRY(upload(a->src_e, source_e, (size_t)n_sources * n_line, s));
+        OS_TRY(upload(a->src_h, source_h, (size_t)n_sources * n_line, s));
+    }
+    // recompute the segment, recording E over the box after every step
+    const size_t box = adj_box(a);
+    const int box_blocks = (int)((box + 255) / 256);
+    Ez2DParams p = make_params(h);
+    const dim3 block(EZ2D_BLOCK_X, EZ2D_BLOCK_Y);
+    const dim3 grid((unsigned)((h->grid.ny + block.x - 1) / block.x), (unsigned)((h->grid.nx + block.y - 1) / block.y));
+    ez2d_record_box_kernel<<<box_blocks, 256, 0, s>>>(p.ez, h->grid.ny, a->bi0, a->bi1, a->bj0, a->bj1, a->rec.ptr);
+    for (int32_t k = 0; k < n_steps; ++k) {
+        ez2d_h_kernel<<<grid, block, 0, s>>>(p);
+        ez2d_e_kernel<<<grid, block, 0, s>>>(p, a->values.ptr, n_steps, k);
+        ez2d_record_box_kernel<<<box_blocks, 256, 0, s>>>(p.ez, h->grid.ny, a->bi0, a->bi1, a->bj0, a->bj1,
+                                                          a->rec.ptr + (size_t)(k + 1) * box);
+    }
+    // transposed steps backward through the segment
+    Ez2DAdjParams q = adj_params(a);
+    const dim3 ablock(32, 8);
+    const dim3 agrid((unsigned)((h->grid.ny + 31) / 32), (unsigned)((h->grid.nx + 7) / 8));
+    int src_index = n_sources - 1;
+    for (int32_t k = n_steps - 1; k >= 0; --k) {
+        const int e = a->e_par;
+        if (src_index >= 0 && source_steps[src_index] == k) {
+            float *lh = mon.normal_axis == 0 ? a->lhy[0].ptr : a->lhx[0].ptr;
+            ez2d_adj_source_kernel<<<(n_line + 127) / 128, 128, 0, s>>>(
+                a->le[e].ptr, lh, h->grid.ny, mon.normal_axis, mon.position, mon.lo, n_line,
+                a->src_e.ptr + (size_t)src_index * n_line, a->src_h.ptr + (size_t)src_index * n_line);
+            --src_index;
+        }
+        q.le_in = a->le[e].ptr;
+        q.lhx_in = a->lhx[0].ptr;
+        q.lhy_in = a->lhy[0].ptr;
+        q.lhx_out = a->lhx[1].ptr;
+        q.lhy_out = a->lhy[1].ptr;
+        for (int sd = 0; sd < 4; ++sd) {
+            q.lpe_in[sd] = a->lpe[e][sd].ptr;
+            q.lpe_out[sd] = a->lpe[e ^ 1][sd].ptr;
+            q.lph_in[sd] = a->lph[e][sd].ptr;
+            q.lph_out[sd] = a->lph[e ^ 1][sd].ptr;
+        }
+        q.e_next = a->rec.ptr + (size_t)(k + 1) * box;
+        q.e_prev = a->rec.ptr + (size_t)k * box;
+        ez2d_adj_e_kernel<<<agrid, ablock, 0, s>>>(q);
+        q.lhx_in = a->lhx[1].ptr;
+        q.lhy_in = a->lhy[1].ptr;
+        q.lhx_out = a->lhx[0].ptr;
+        q.lhy_out = a->lhy[0].ptr;
+        q.le_out = a->le[e ^ 1].ptr;
+        ez2d_adj_h_kernel<<<agrid, ablock, 0, s>>>(q);
+        a->e_par = e ^ 1;
+    }
+    OS_CUDA(cudaGetLastError());
+    h->n_step = step0 + n_steps;   // the live buffers hold the recomputed state at the segment's end
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_adjoint_gradient(OsAdjoint2D *a, double *out) {
+    using namespace os;
+    OS_CHECK(a && out, OS_ERR_INVALID, "os_fdtd2d_adjoint_gradient: null argument");
+    OS_TRY(bind_device(a->h));
+    OS_CUDA(cudaMemcpyAsync(out, a->grad.ptr, a->grad.bytes(), cudaMemcpyDeviceToHost, a->h->stream));
+    OS_CUDA(cudaStreamSynchronize(a->h->stream));
+    return OS_OK;
+}

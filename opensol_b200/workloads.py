@@ -87,3 +87,29 @@ def roofline_3d_physics(total_cells=512, npml=12, n_spheres=500, seed=2025, devi
     freqs = np.linspace(f0 * (1 - bw / 2), f0 * (1 + bw / 2), spec['n_freqs']).tolist()
     box = physics.add_flux_box((0.2 * window,) * 3, (0.8 * window,) * 3, frequencies=freqs)
     return physics, box
+
+
+# Adjoint: a 1024 x 1024 total grid (984 x 984 window + 20 CPML cells per side) at dx = 20 nm, a 200 x 200-cell design
+# region at the window centre with eps_r U(1, 12.1) (seeded), a Gaussian line source at 1550 nm (bandwidth 0.5) along y
+# at 15 % of the window, and the objective: the DFT flux at 1550 nm through a line along y at 85 % of the window after
+# 8,000 steps, with checkpoints every 256 steps.
+ADJOINT_2D = {'total_cells': 1024, 'dx': 20e-9, 'npml': 20, 'design': 200, 'eps_r': (1.0, 12.1),
+              'wavelength': 1550e-9, 'bandwidth': 0.5, 'steps': 8000, 'checkpoint_every': 256, 'seed': 2026}
+
+
+def adjoint_2d_problem(total_cells=1024, design=200, steps=8000, checkpoint_every=256, seed=2026, device=0):
+    """(Simulation, flux monitor, design box (i0, i1, j0, j1), design eps_r (design, design) float32) of the adjoint
+    workload, finalized."""
+    from .simulation import Simulation
+    spec = ADJOINT_2D
+    dx, npml = spec['dx'], spec['npml']
+    window = (total_cells - 2 * npml) * dx
+    sim = Simulation(window, window, dx, npml=npml, boundaries='pml', verbose=False, device=device)
+    i0 = j0 = (total_cells - design) // 2
+    box = (i0, i0 + design, j0, j0 + design)
+    eps = np.random.default_rng(seed).uniform(*spec['eps_r'], (design, design)).astype(np.float32)
+    sim.domain.materials.array('eps_r')[box[0]:box[1], box[2]:box[3]] = eps
+    sim.add_line_source('y', 0.15 * window, wavelength=spec['wavelength'], bandwidth=spec['bandwidth'])
+    monitor = sim.add_flux_monitor('y', 0.85 * window, (0.0, window), wavelengths=[spec['wavelength']])
+    sim.em.finalize()
+    return sim, monitor, box, eps
