@@ -50,6 +50,10 @@ def parse_args():
     p.add_argument('--variant', type=int, default=1, help='1: temporally blocked kernels (default), 0: per step')
     p.add_argument('--steps-per-launch', type=int, default=3)
     p.add_argument('--tile-rows', type=int, default=0, help='rows per interior tile (0: autotune)')
+    p.add_argument('--workload', default='roofline_2d', choices=['roofline_2d', 'em3d', 'serving', 'adjoint'],
+                   help='roofline_2d: the headline 8192^2 2D run; em3d: the 512^3 3D run; serving: the batched job '
+                        'stream against one-at-a-time runs; adjoint: gradient cost against one forward run')
+    p.add_argument('--jobs', type=int, default=64, help='serving: jobs of the request stream')
     return p.parse_args()
 
 
@@ -336,12 +340,146 @@ def run_e2e(args, device, world, barrier, reduce_max):
             'timing': 'host wall clock around Simulation.run + flux(), synchronized, max over ranks'}
 
 
+def run_em3d(args):
+    """The 512^3 3D workload (opensol_b200/workloads.py roofline_3d_physics): cell-updates/s over the total grid, one
+    bench step = args.sim_steps Yee steps from rest (2000 when left at the 2D default)."""
+    import torch
+    from opensol_b200 import workloads
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    steps = args.sim_steps if args.sim_steps != SIM_STEPS else workloads.ROOFLINE_3D['steps']
+    physics, box = workloads.roofline_3d_physics(device=local)
+    physics.finalize()
+    engine = physics.engine
+    stream = torch.cuda.current_stream()
+    engine.set_stream(stream.cuda_stream)
+    tables = engine.chunk_tables(steps)
+    for _ in range(args.warmup):
+        engine.reset()
+        engine.advance(steps, tables)
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            engine.reset()
+            engine.advance(steps, tables)
+            launches += engine.launch_count()
+        stop.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(stop)
+    cells = engine.nx * engine.ny * engine.nz
+    value = cells * steps * args.steps / (ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    achieved = 52.0 * value
+    line = {'metric': 'FDTD Gcell-updates/s (3D)', 'value': value, 'unit': 'Gcell-updates/s', 'n_gpus': 1,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms / args.steps, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': f'em3d: {engine.nx}^3 total grid incl. 12 CPML cells/face, dx 20 nm, 500 seeded '
+                                   'spheres eps_r U(2,12), z dipole 1310 nm at the centre, 8-frequency flux box, '
+                                   f'{steps} Yee steps per bench step', 'l2': 'fields 6 x 537 MB, no flush'},
+            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
+                         'traffic': None, 'peak_source': f'{peak_kind} hbm_gbs', 'bytes_per_cell_update': 52,
+                         'kernel': 'em3d_h_kernel + em3d_e_kernel (whole step)'},
+            'gpu_launches': launches, 'clocks': clocks.summary(),
+            'flux_box_first': float(box.flux()[0])}
+    print(json.dumps(line), flush=True)
+
+
+def run_serving(args):
+    """The serving stream (opensol_b200/serving.py make_job_specs): sims/s of the batched loop with every job queued
+    at once, against one-at-a-time runs of the same jobs; p50 / p99 latency with Poisson arrivals at 20 jobs/s."""
+    import numpy as np
+    import torch
+    from opensol_b200 import serving
+    torch.cuda.set_device(0)
+    specs = serving.make_job_specs(n_jobs=args.jobs, rate=20.0, seed=7)
+    work = sum(s.cells() * s.steps for s in specs)
+    warm = serving.make_job_specs(n_jobs=3, rate=0.0, seed=1, side_range=(64, 128), steps_range=(100, 300))
+    loop = serving.ServingLoop(max_active=48, chunk_steps=512, tile_rows=32)
+    loop.run(warm, realtime=False)
+    loop.close()
+    serving.run_alone(warm[0])
+    loop = serving.ServingLoop(max_active=48, chunk_steps=512, tile_rows=32)
+    t0 = time.perf_counter()
+    batched = {r.job_id: r for r in loop.run(specs, realtime=False)}
+    t_batch = time.perf_counter() - t0
+    loop.close()
+    t0 = time.perf_counter()
+    alone = {s.job_id: serving.run_alone(s, tile_rows=128)[0] for s in specs}
+    t_alone = time.perf_counter() - t0
+    same = all(np.array_equal(a, b) for j, r in batched.items() for a, b in zip(r.fluxes, alone[j]))
+    loop = serving.ServingLoop(max_active=48, chunk_steps=512, tile_rows=32)
+    t0 = time.perf_counter()
+    realtime = loop.run(specs, realtime=True)
+    t_rt = time.perf_counter() - t0
+    loop.close()
+    p50, p99 = serving.latency_percentiles(realtime)
+    line = {'metric': 'batched sims/s', 'value': len(specs) / t_batch, 'unit': 'sims/s', 'n_gpus': 1,
+            'steps': 1, 'warmup': 1, 'ms_per_step': t_batch * 1e3, 'higher_is_better': True, 'scaling': 'strong',
+            'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': f'serving: {len(specs)} jobs, square windows U{{256..2048}} + 15 CPML cells/side, '
+                                   '1-40 rectangles eps_r U(1,12), line source U(1000,1600) nm, U(2000,20000) steps, '
+                                   'two 4-frequency flux lines; Poisson 20 jobs/s for the latency run',
+                       'max_active': 48, 'chunk_steps': 512, 'memory_budget_gb': 120},
+            'one_at_a_time_sims_per_s': len(specs) / t_alone, 'speedup_vs_one_at_a_time': t_alone / t_batch,
+            'cell_updates_per_s_batched': work / t_batch, 'fluxes_equal_alone_and_batched': bool(same),
+            'latency_p50_s': p50, 'latency_p99_s': p99, 'realtime_makespan_s': t_rt,
+            'timing': 'host wall clock (synchronised), one process, one B200'}
+    print(json.dumps(line), flush=True)
+
+
+def run_adjoint(args):
+    """The adjoint workload (opensol_b200/workloads.py adjoint_2d_problem): wall(forward + gradient) / wall(forward)."""
+    import numpy as np
+    import torch
+    from opensol_b200 import workloads
+    from opensol_b200.adjoint import FluxAdjoint2D
+    torch.cuda.set_device(0)
+    spec = workloads.ADJOINT_2D
+    sim, monitor, box, eps = workloads.adjoint_2d_problem()
+    sim.em.engine.configure(tile_rows=32)
+    adj = FluxAdjoint2D(sim, monitor, 0, box, spec['steps'], checkpoint_every=spec['checkpoint_every'])
+    adj.forward()
+    adj.backward()
+    fw, bw = [], []
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        J = adj.forward()
+        sim.em.engine.synchronize()
+        t1 = time.perf_counter()
+        grad = adj.backward()
+        t2 = time.perf_counter()
+        fw.append(t1 - t0)
+        bw.append(t2 - t1)
+    f, b = min(fw), min(bw)
+    line = {'metric': 'adjoint gradient cost / forward cost', 'value': (f + b) / f, 'unit': 'x',
+            'n_gpus': 1, 'steps': len(fw), 'warmup': 1, 'ms_per_step': (f + b) * 1e3, 'higher_is_better': False,
+            'scaling': 'strong', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': f'adjoint: {sim.em.engine.nx}^2 total grid incl. 20 CPML cells/side, dx 20 nm, '
+                                   f'{box[1] - box[0]}x{box[3] - box[2]} design box eps_r U(1,12.1), 1550 nm line '
+                                   f'source, flux objective at 1550 nm after {spec["steps"]} steps, checkpoints '
+                                   f'every {spec["checkpoint_every"]}'},
+            'forward_s': f, 'backward_s': b, 'objective': J, 'grad_abs_max': float(np.abs(grad).max()),
+            'forward_gcell_updates_per_s': sim.em.engine.nx * sim.em.engine.ny * spec['steps'] / f / 1e9,
+            'timing': 'host wall clock (synchronised), best of the timed repeats'}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == 'reference':
         run_reference(args)
         return
-    run_b200(args)
+    if args.workload == 'em3d':
+        run_em3d(args)
+    elif args.workload == 'serving':
+        run_serving(args)
+    elif args.workload == 'adjoint':
+        run_adjoint(args)
+    else:
+        run_b200(args)
 
 
 if __name__ == '__main__':

@@ -1371,6 +1371,10 @@ struct OsAdjoint2D {
     os::DeviceArray<float> rec;                        // (seg_steps + 1) x box
     os::DeviceArray<double> grad;                      // box
     os::DeviceArray<float> values, src_e, src_h;
+    os::DeviceArray<int32_t> src_row;                  // per step of the segment: row of its adjoint source, or -1
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};     // full-segment body, per starting parity
+    int graph_monitor[2] = {-1, -1};
+    int64_t graph_launches = 0;
 };
 
 namespace os {
@@ -1475,6 +1479,8 @@ extern "C" int os_fdtd2d_adjoint_destroy(OsAdjoint2D *a) {
     if (!a) return OS_OK;
     cudaSetDevice(a->h->device);
     cudaStreamSynchronize(a->h->stream);
+    for (cudaGraphExec_t g : a->graph)
+        if (g) cudaGraphExecDestroy(g);
     delete a;
     return OS_OK;
 }
@@ -1539,62 +1545,103 @@ extern "C" int os_fdtd2d_adjoint_segment(OsAdjoint2D *a, int32_t slot, int64_t s
             src += pc.second;
         }
     }
-    if (!h->lines.empty()) OS_TRY(upload(a->values, line_values, h->lines.size() * (size_t)n_steps, s));
+    if (!h->lines.empty()) {   // the values of the whole segment length, so a captured body reads them in place
+        OS_TRY(a->values.alloc(h->lines.size() * (size_t)a->seg_steps));
+        OS_CUDA(cudaMemcpyAsync(a->values.ptr, line_values, h->lines.size() * (size_t)n_steps * sizeof(float),
+                                cudaMemcpyHostToDevice, s));
+    }
     const FluxLine2D &mon = *h->fluxes[monitor_id];
     const int n_line = mon.hi - mon.lo;
-    if (n_sources) {
-        OS_TRY(upload(a->src_e, source_e, (size_t)n_sources * n_line, s));
-        OS_TRY(upload(a->src_h, source_h, (size_t)n_sources * n_line, s));
+    {   // source rows and the per-step row table
+        std::vector<int32_t> rows((size_t)a->seg_steps, -1);
+        for (int32_t q = 0; q < n_sources; ++q) rows[(size_t)source_steps[q]] = q;
+        OS_TRY(a->src_row.alloc((size_t)a->seg_steps));
+        OS_CUDA(cudaMemcpyAsync(a->src_row.ptr, rows.data(), rows.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                s));
+        OS_TRY(a->src_e.alloc((size_t)a->seg_steps * n_line));
+        OS_TRY(a->src_h.alloc((size_t)a->seg_steps * n_line));
+        if (n_sources) {
+            OS_CUDA(cudaMemcpyAsync(a->src_e.ptr, source_e, (size_t)n_sources * n_line * sizeof(float),
+                                    cudaMemcpyHostToDevice, s));
+            OS_CUDA(cudaMemcpyAsync(a->src_h.ptr, source_h, (size_t)n_sources * n_line * sizeof(float),
+                                    cudaMemcpyHostToDevice, s));
+        }
     }
-    // recompute the segment, recording E over the box after every step
-    const size_t box = adj_box(a);
-    const int box_blocks = (int)((box + 255) / 256);
-    Ez2DParams p = make_params(h);
-    const dim3 block(EZ2D_BLOCK_X, EZ2D_BLOCK_Y);
-    const dim3 grid((unsigned)((h->grid.ny + block.x - 1) / block.x), (unsigned)((h->grid.nx + block.y - 1) / block.y));
-    ez2d_record_box_kernel<<<box_blocks, 256, 0, s>>>(p.ez, h->grid.ny, a->bi0, a->bi1, a->bj0, a->bj1, a->rec.ptr);
-    for (int32_t k = 0; k < n_steps; ++k) {
-        ez2d_h_kernel<<<grid, block, 0, s>>>(p);
-        ez2d_e_kernel<<<grid, block, 0, s>>>(p, a->values.ptr, n_steps, k);
+    // the body: recompute the segment recording E over the box, then the transposed steps backward; a full-length
+    // segment replays one captured graph (its arguments are the same for every segment of that parity)
+    auto body = [&](int32_t steps) -> int {
+        const size_t box = adj_box(a);
+        const int box_blocks = (int)((box + 255) / 256);
+        Ez2DParams p = make_params(h);
+        const dim3 block(EZ2D_BLOCK_X, EZ2D_BLOCK_Y);
+        const dim3 grid((unsigned)((h->grid.ny + block.x - 1) / block.x),
+                        (unsigned)((h->grid.nx + block.y - 1) / block.y));
         ez2d_record_box_kernel<<<box_blocks, 256, 0, s>>>(p.ez, h->grid.ny, a->bi0, a->bi1, a->bj0, a->bj1,
-                                                          a->rec.ptr + (size_t)(k + 1) * box);
-    }
-    // transposed steps backward through the segment
-    Ez2DAdjParams q = adj_params(a);
-    const dim3 ablock(32, 8);
-    const dim3 agrid((unsigned)((h->grid.ny + 31) / 32), (unsigned)((h->grid.nx + 7) / 8));
-    int src_index = n_sources - 1;
-    for (int32_t k = n_steps - 1; k >= 0; --k) {
-        const int e = a->e_par;
-        if (src_index >= 0 && source_steps[src_index] == k) {
+                                                          a->rec.ptr);
+        for (int32_t k = 0; k < steps; ++k) {
+            ez2d_h_kernel<<<grid, block, 0, s>>>(p);
+            ez2d_e_kernel<<<grid, block, 0, s>>>(p, a->values.ptr, steps, k);
+            ez2d_record_box_kernel<<<box_blocks, 256, 0, s>>>(p.ez, h->grid.ny, a->bi0, a->bi1, a->bj0, a->bj1,
+                                                              a->rec.ptr + (size_t)(k + 1) * box);
+        }
+        Ez2DAdjParams q = adj_params(a);
+        const dim3 ablock(32, 8);
+        const dim3 agrid((unsigned)((h->grid.ny + 31) / 32), (unsigned)((h->grid.nx + 7) / 8));
+        int e = a->e_par;
+        for (int32_t k = steps - 1; k >= 0; --k) {
             float *lh = mon.normal_axis == 0 ? a->lhy[0].ptr : a->lhx[0].ptr;
             ez2d_adj_source_kernel<<<(n_line + 127) / 128, 128, 0, s>>>(
-                a->le[e].ptr, lh, h->grid.ny, mon.normal_axis, mon.position, mon.lo, n_line,
-                a->src_e.ptr + (size_t)src_index * n_line, a->src_h.ptr + (size_t)src_index * n_line);
-            --src_index;
+                a->le[e].ptr, lh, h->grid.ny, mon.normal_axis, mon.position, mon.lo, n_line, a->src_row.ptr, k,
+                a->src_e.ptr, a->src_h.ptr);
+            q.le_in = a->le[e].ptr;
+            q.lhx_in = a->lhx[0].ptr;
+            q.lhy_in = a->lhy[0].ptr;
+            q.lhx_out = a->lhx[1].ptr;
+            q.lhy_out = a->lhy[1].ptr;
+            for (int sd = 0; sd < 4; ++sd) {
+                q.lpe_in[sd] = a->lpe[e][sd].ptr;
+                q.lpe_out[sd] = a->lpe[e ^ 1][sd].ptr;
+                q.lph_in[sd] = a->lph[e][sd].ptr;
+                q.lph_out[sd] = a->lph[e ^ 1][sd].ptr;
+            }
+            q.e_next = a->rec.ptr + (size_t)(k + 1) * box;
+            q.e_prev = a->rec.ptr + (size_t)k * box;
+            ez2d_adj_e_kernel<<<agrid, ablock, 0, s>>>(q);
+            q.lhx_in = a->lhx[1].ptr;
+            q.lhy_in = a->lhy[1].ptr;
+            q.lhx_out = a->lhx[0].ptr;
+            q.lhy_out = a->lhy[0].ptr;
+            q.le_out = a->le[e ^ 1].ptr;
+            ez2d_adj_h_kernel<<<agrid, ablock, 0, s>>>(q);
+            e ^= 1;
         }
-        q.le_in = a->le[e].ptr;
-        q.lhx_in = a->lhx[0].ptr;
-        q.lhy_in = a->lhy[0].ptr;
-        q.lhx_out = a->lhx[1].ptr;
-        q.lhy_out = a->lhy[1].ptr;
-        for (int sd = 0; sd < 4; ++sd) {
-            q.lpe_in[sd] = a->lpe[e][sd].ptr;
-            q.lpe_out[sd] = a->lpe[e ^ 1][sd].ptr;
-            q.lph_in[sd] = a->lph[e][sd].ptr;
-            q.lph_out[sd] = a->lph[e ^ 1][sd].ptr;
+        return OS_OK;
+    };
+    const int par = a->e_par;
+    if (n_steps == a->seg_steps) {
+        if (!a->graph[par] || a->graph_monitor[par] != monitor_id) {
+            if (a->graph[par]) OS_CUDA(cudaGraphExecDestroy(a->graph[par]));
+            a->graph[par] = nullptr;
+            cudaGraph_t g = nullptr;
+            OS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            const int rc = body(n_steps);
+            const cudaError_t end = cudaStreamEndCapture(s, &g);
+            if (rc != OS_OK) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            OS_CUDA(end);
+            const cudaError_t inst = cudaGraphInstantiate(&a->graph[par], g, 0);
+            cudaGraphDestroy(g);
+            OS_CUDA(inst);
+            a->graph_monitor[par] = monitor_id;
         }
-        q.e_next = a->rec.ptr + (size_t)(k + 1) * box;
-        q.e_prev = a->rec.ptr + (size_t)k * box;
-        ez2d_adj_e_kernel<<<agrid, ablock, 0, s>>>(q);
-        q.lhx_in = a->lhx[1].ptr;
-        q.lhy_in = a->lhy[1].ptr;
-        q.lhx_out = a->lhx[0].ptr;
-        q.lhy_out = a->lhy[0].ptr;
-        q.le_out = a->le[e ^ 1].ptr;
-        ez2d_adj_h_kernel<<<agrid, ablock, 0, s>>>(q);
-        a->e_par = e ^ 1;
+        OS_CUDA(cudaGraphLaunch(a->graph[par], s));
+        a->graph_launches += 1;
+    } else {
+        OS_TRY(body(n_steps));
     }
+    a->e_par = (par + (int)(n_steps & 1)) & 1;
     OS_CUDA(cudaGetLastError());
     h->n_step = step0 + n_steps;   // the live buffers hold the recomputed state at the segment's end
     return OS_OK;

@@ -168,12 +168,16 @@ __global__ void __launch_bounds__(256) ez2d_adj_h_kernel(const Ez2DAdjParams p) 
     p.lhy_out[idx] = hy_updated ? da * p.lhy_in[idx] : p.lhy_in[idx];
 }
 
-// dJ/de and dJ/dh of one DFT sample added to lambda_E and lambda_H on a flux line (normal 0: x-cell `position`, H_y;
-// normal 1: y-cell `position`, H_x).
+// dJ/de and dJ/dh of the DFT sample of step k (row row_of_step[k] of de / dh, none when -1) added to lambda_E and
+// lambda_H on a flux line (normal 0: x-cell `position`, H_y; normal 1: y-cell `position`, H_x).
 __global__ void ez2d_adj_source_kernel(float *le, float *lh, int ny, int normal_axis, int position, int lo, int n,
-                                       const float *__restrict__ de, const float *__restrict__ dh) {
+                                       const int32_t *__restrict__ row_of_step, int k, const float *__restrict__ de_rows,
+                                       const float *__restrict__ dh_rows) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
+    const int row = row_of_step[k];
+    if (row < 0) return;
+    const float *de = de_rows + (size_t)row * n, *dh = dh_rows + (size_t)row * n;
     const size_t cell = normal_axis == 0 ? (size_t)position * ny + (lo + c) : (size_t)(lo + c) * ny + position;
     le[cell] += de[c];
     lh[cell] += dh[c];
