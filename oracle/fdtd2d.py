@@ -296,11 +296,12 @@ class FluxMonitor:
     e_acc: np.ndarray = None
     h_acc: np.ndarray = None
     sample_interval: int = 1
+    flux_sign: float = None   # None: the E_z sign (S_x = -E_z H_y, S_y = +E_z H_x)
 
     def flux(self):
         e = self.e_acc
         h = self.h_acc * np.exp(1j * np.pi * self.frequencies * self.dt)[:, None]
-        sign = -1.0 if self.normal_axis == 'x' else 1.0
+        sign = self.flux_sign if self.flux_sign is not None else (-1.0 if self.normal_axis == 'x' else 1.0)
         e_time_average = np.cos(np.pi * self.frequencies * self.dt)
         integrand = sign * e_time_average[:, None] * np.real(e * np.conj(h))
         return integrand @ self.widths
@@ -532,13 +533,10 @@ class OracleEz2D:
             times_full[k] = t
         return values, times_full
 
-    def advance(self, n_steps):
-        lib, State, Line, Flux = load_library(self.real)
-        d, real = self.domain, self.real
-        R = ctypes.c_float if real == np.float32 else ctypes.c_double
+    def _chunk_phase_tables(self, n_steps, times_full):
+        """(first sample, sample count, per-monitor float32 (n_q, nf, 2) phase tables) of the DFT samples the next
+        n_steps steps take (monitors.py:22-24,219-220)."""
         m = self.sample_interval
-        values, times_full = self.source_values(n_steps)
-        # phase table of the samples in this chunk
         first_q = self.n_step // m + 1
         last_q = (self.n_step + n_steps) // m
         n_q = max(0, last_q - first_q + 1)
@@ -550,7 +548,58 @@ class OracleEz2D:
                 step = (first_q + qi) * m
                 table[qi] = dft_phases(omega, times_full[step - self.n_step - 1], mon.dt * m)
             phase_tables.append(table)
+        return first_q, n_q, phase_tables
 
+    def _cpml_state(self, st, R):
+        """Fill the CPML members of a ctypes state; returns the arrays the pointers refer to."""
+        st.npml = self.domain.npml
+        keep = []
+        for side in self.cpml_sides:
+            k = FACES.index(side.name)
+            st.cpml_active[k] = 1
+            for attr in ('b_e', 'a_e', 'inv_e', 'b_h', 'a_h', 'inv_h'):
+                arr = np.ascontiguousarray(getattr(side, attr), dtype=self.real)
+                keep.append(arr)
+                getattr(st, attr)[k] = _ptr(arr, R)
+            st.psi_e[k] = _ptr(self.psi_e[side.name], R)
+            st.psi_h[k] = _ptr(self.psi_h[side.name], R)
+        return keep
+
+    def _line_structs(self, Line, values):
+        lines = (Line * max(1, len(self.sources)))()
+        for i, (src, v) in enumerate(zip(self.sources, values)):
+            lines[i].axis, lines[i].position = (0 if src.axis == 'x' else 1), src.position
+            lines[i].lo, lines[i].hi = src.lo, src.hi
+            lines[i].profile = _ptr(src.profile, ctypes.c_float)
+            lines[i].values = _ptr(v, ctypes.c_float)
+        return lines
+
+    def _flux_structs(self, Flux, phase_tables, first_q, n_q):
+        fluxes = (Flux * max(1, len(self.monitors)))()
+        for i, (mon, table) in enumerate(zip(self.monitors, phase_tables)):
+            fluxes[i].normal_axis = 0 if mon.normal_axis == 'x' else 1
+            fluxes[i].position, fluxes[i].lo, fluxes[i].hi = mon.position, mon.lo, mon.hi
+            fluxes[i].nf = mon.frequencies.size
+            fluxes[i].e_acc = mon.e_acc.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            fluxes[i].h_acc = mon.h_acc.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            fluxes[i].phases = _ptr(table, ctypes.c_float)
+            fluxes[i].first_sample, fluxes[i].n_samples = first_q, n_q
+        return fluxes
+
+    def _clock_after(self, n_steps, times_full):
+        self.n_step += n_steps
+        if n_steps:
+            self.time = float(times_full[-1])
+        dt = float(self.domain.dt)
+        for _ in range(n_steps):
+            self.runner_t = self.runner_t + dt
+
+    def advance(self, n_steps):
+        lib, State, Line, Flux = load_library(self.real)
+        d, real = self.domain, self.real
+        R = ctypes.c_float if real == np.float32 else ctypes.c_double
+        values, times_full = self.source_values(n_steps)
+        first_q, n_q, phase_tables = self._chunk_phase_tables(n_steps, times_full)
         st = State()
         st.nx, st.ny, st.periodic_x, st.periodic_y = d.nx, d.ny, int(d.periodic_x), int(d.periodic_y)
         st.ez, st.hx, st.hy = _ptr(self.ez, R), _ptr(self.hx, R), _ptr(self.hy, R)
@@ -561,39 +610,12 @@ class OracleEz2D:
         st.da_uniform, st.db_uniform = 1.0, 0.0
         for name in ('inv_dx_e', 'inv_dx_h', 'inv_dy_e', 'inv_dy_h'):
             setattr(st, name, _ptr(self.curl[name], R))
-        st.npml = d.npml
-        keep = []
-        for side in self.cpml_sides:
-            k = FACES.index(side.name)
-            st.cpml_active[k] = 1
-            for attr in ('b_e', 'a_e', 'inv_e', 'b_h', 'a_h', 'inv_h'):
-                arr = np.ascontiguousarray(getattr(side, attr), dtype=real)
-                keep.append(arr)
-                getattr(st, attr)[k] = _ptr(arr, R)
-            st.psi_e[k] = _ptr(self.psi_e[side.name], R)
-            st.psi_h[k] = _ptr(self.psi_h[side.name], R)
-        lines = (Line * max(1, len(self.sources)))()
-        for i, (src, v) in enumerate(zip(self.sources, values)):
-            lines[i].axis, lines[i].position = (0 if src.axis == 'x' else 1), src.position
-            lines[i].lo, lines[i].hi = src.lo, src.hi
-            lines[i].profile = _ptr(src.profile, ctypes.c_float)
-            lines[i].values = _ptr(v, ctypes.c_float)
-        fluxes = (Flux * max(1, len(self.monitors)))()
-        for i, (mon, table) in enumerate(zip(self.monitors, phase_tables)):
-            fluxes[i].normal_axis = 0 if mon.normal_axis == 'x' else 1
-            fluxes[i].position, fluxes[i].lo, fluxes[i].hi = mon.position, mon.lo, mon.hi
-            fluxes[i].nf = mon.frequencies.size
-            fluxes[i].e_acc = mon.e_acc.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-            fluxes[i].h_acc = mon.h_acc.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-            fluxes[i].phases = _ptr(table, ctypes.c_float)
-            fluxes[i].first_sample, fluxes[i].n_samples = first_q, n_q
+        keep = self._cpml_state(st, R)
+        lines = self._line_structs(Line, values)
+        fluxes = self._flux_structs(Flux, phase_tables, first_q, n_q)
         rc = lib.oracle_ez2d_advance(ctypes.byref(st), self.n_step, n_steps, len(self.sources), lines,
-                                     len(self.monitors), fluxes, m)
+                                     len(self.monitors), fluxes, self.sample_interval)
+        del keep
         if rc != 0:
             raise RuntimeError('oracle phase table does not cover a sample')
-        self.n_step += n_steps
-        if n_steps:
-            self.time = float(times_full[-1])
-        dt = float(d.dt)
-        for _ in range(n_steps):
-            self.runner_t = self.runner_t + dt
+        self._clock_after(n_steps, times_full)

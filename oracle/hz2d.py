@@ -1,0 +1,207 @@
+"""ORACLE -- TEST INFRASTRUCTURE ONLY.
+
+Nothing in the product (``opensol_b200``) imports this module.  Only ``tests/`` use it, as the checker the CUDA H_z
+engine is compared with.
+
+A CPU restatement of open_sol's 2D H_z-polarisation FDTD path (``Simulation(polarization='hz').run`` ->
+``EMPhysics.step`` -> ``FDTDEngine2D_Hz.advance``): setup in numpy, the time step in C (``oracle/hz2d.c``).  The grid,
+Courant step, CPML rows, Gaussian pulse, DFT sample interval / phases and the clocks are those of the E_z oracle
+(oracle/fdtd2d.py); what differs:
+
+* materials: the dielectric helpers write eps_xx and eps_yy (physics/em/__init__.py:154-156,317-327);
+* E face coefficients: width-weighted hi-face means of eps_xx (E_x, along y) and eps_yy (E_y, along x) and sigma_e,
+  the partner cell wrapping on a periodic axis and the cell itself on the last face of an open one (face_shares /
+  face_partner, physics/em/yee_grid.py:76-84,119-125), then ca / cb as fdtd_hz_2d_kernels.py:254-274;
+* H_z coefficients da / db at the cell centres: the E_z engine's (fdtd_2d_base.py:294-);
+* the sheet source sits on the hi faces of its line cells (TangentialSheetCurrentSource, physics/em/sources.py:469-480)
+  with w_perp = the dual spacing across that face (placement.py:254-265; a line on the last cell of an open axis is
+  refused), line eps = width-weighted mean of the line row and the next row of eps_xx (axis 'x') / eps_yy (axis 'y'),
+  sigma_e included, cb = cb_x / cb_y (sources.py:582-602);
+* flux: E_y (normal x) / E_x (normal y) with H_z, S_x = +E_y H_z, S_y = -E_x H_z (monitors.py:350-362).
+
+Pinned against fixtures generated from the reference itself (``tests/golden/make_golden_hz.py``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from oracle.fdtd2d import (DTYPE, EPS0, ETA0, LIB_DIR, OracleEz2D, _make_structs, _ptr, build_cpml,
+                           dft_sample_interval, h_coefficients, paint_circle, paint_rect, sheet_admittance,
+                           yee_inverse_spacings)
+
+
+def face_shares(widths, periodic, real):
+    """(lower, upper) hi-face weights w_k / (w_k + w_k+1), w_k+1 / (w_k + w_k+1) (yee_grid.py:119-125)."""
+    widths = np.asarray(widths, dtype=np.float64)
+    partner = np.roll(widths, -1) if periodic else np.concatenate((widths[1:], widths[-1:]))
+    return (widths / (widths + partner)).astype(real), (partner / (widths + partner)).astype(real)
+
+
+def partner_index(n, periodic):
+    """Upper partner cell of each hi face of an axis of n cells (yee_grid.face_partner of the indices)."""
+    idx = np.arange(int(n))
+    return np.roll(idx, -1) if periodic else np.concatenate((idx[1:], idx[-1:]))
+
+
+def face_coefficient_pair(eps_rel, sigma, dt, real):
+    """ca, cb of one face set from face eps_r / sigma (fdtd_hz_2d_kernels.py:254-260), T = real."""
+    dt = real(dt)
+    eps = eps_rel * real(EPS0)
+    k = sigma * dt / (2.0 * eps)
+    denom = 1.0 + k
+    return ((1.0 - k) / denom).astype(real), ((dt / eps) / denom).astype(real)
+
+
+def e_face_coefficients(eps_xx, eps_yy, sigma_e, kernel_widths, periodic_x, periodic_y, dt, real):
+    """(ca_x, cb_x, ca_y, cb_y) of the E_x (hi-y) and E_y (hi-x) faces (fdtd_hz_2d_kernels.py:263-274)."""
+    nx, ny = eps_xx.shape
+    lo_y, up_y = face_shares(kernel_widths[1], periodic_y, real)
+    lo_x, up_x = face_shares(kernel_widths[0], periodic_x, real)
+    pj, pi = partner_index(ny, periodic_y), partner_index(nx, periodic_x)
+    exx, eyy, sig = (a.astype(real, copy=False) for a in (eps_xx, eps_yy, sigma_e))
+    ca_x, cb_x = face_coefficient_pair(exx * lo_y + exx[:, pj] * up_y, sig * lo_y + sig[:, pj] * up_y, dt, real)
+    lx, ux = lo_x[:, None], up_x[:, None]
+    ca_y, cb_y = face_coefficient_pair(eyy * lx + eyy[pi] * ux, sig * lx + sig[pi] * ux, dt, real)
+    return ca_x, cb_x, ca_y, cb_y
+
+
+def _make_hz_state(real):
+    R = ctypes.c_float if real == np.float32 else ctypes.c_double
+    P = ctypes.POINTER(R)
+
+    class StateHz(ctypes.Structure):
+        _fields_ = [('nx', ctypes.c_int32), ('ny', ctypes.c_int32), ('periodic_x', ctypes.c_int32),
+                    ('periodic_y', ctypes.c_int32), ('hz', P), ('ex', P), ('ey', P), ('ca_x', P), ('cb_x', P),
+                    ('ca_y', P), ('cb_y', P), ('da', P), ('db', P), ('inv_dx_e', P), ('inv_dx_h', P),
+                    ('inv_dy_e', P), ('inv_dy_h', P), ('npml', ctypes.c_int32), ('cpml_active', ctypes.c_int32 * 4),
+                    ('b_e', P * 4), ('a_e', P * 4), ('inv_e', P * 4), ('b_h', P * 4), ('a_h', P * 4),
+                    ('inv_h', P * 4), ('psi_e', P * 4), ('psi_h', P * 4)]
+    return StateHz
+
+
+_LIBS = {}
+
+
+def load_library(real=np.float32):
+    """The float32 / float64 build of oracle/hz2d.c (oracle/Makefile, into oracle/_build)."""
+    key = np.dtype(real).name
+    if key not in _LIBS:
+        name = 'libhz2d_oracle_f32.so' if real == np.float32 else 'libhz2d_oracle_f64.so'
+        path = os.path.join(LIB_DIR, name)
+        if not os.path.exists(path):
+            raise RuntimeError(f'oracle library {path} is not built (run: make -C oracle)')
+        lib = ctypes.CDLL(path)
+        _, Line, Flux = _make_structs(real)
+        State = _make_hz_state(real)
+        lib.oracle_hz2d_advance.restype = ctypes.c_int
+        lib.oracle_hz2d_advance.argtypes = [ctypes.POINTER(State), ctypes.c_int64, ctypes.c_int64, ctypes.c_int32,
+                                            ctypes.POINTER(Line), ctypes.c_int32, ctypes.POINTER(Flux),
+                                            ctypes.c_int64]
+        _LIBS[key] = (lib, State, Line, Flux)
+    return _LIBS[key]
+
+
+class OracleHz2D(OracleEz2D):
+    """The whole 2D H_z path of one simulation on the CPU (same construction calls as OracleEz2D)."""
+
+    def __init__(self, size_x, size_y, dx, npml=15, boundaries=None, courant=None, precision='single'):
+        super().__init__(size_x, size_y, dx, npml, boundaries, courant, precision)
+        shape = (self.domain.nx, self.domain.ny)
+        self.eps_xx = self.eps_r
+        self.eps_yy = np.full(shape, DTYPE(1.0), dtype=DTYPE)
+        self.hz = np.zeros(shape, dtype=self.real)
+        self.ex = np.zeros(shape, dtype=self.real)
+        self.ey = np.zeros(shape, dtype=self.real)
+        del self.ez, self.hx, self.hy
+
+    def add_dielectric_rectangle(self, x0, y0, x1, y1, eps_r, sigma_e=0.0):
+        for array in (self.eps_xx, self.eps_yy):
+            paint_rect(self.domain, array, x0, y0, x1, y1, eps_r)
+        if sigma_e is not None:
+            paint_rect(self.domain, self.sigma_e, x0, y0, x1, y1, sigma_e)
+
+    def add_dielectric_circle(self, cx, cy, radius, eps_r, sigma_e=0.0):
+        for array in (self.eps_xx, self.eps_yy):
+            paint_circle(self.domain, array, cx, cy, radius, eps_r)
+        if sigma_e is not None:
+            paint_circle(self.domain, self.sigma_e, cx, cy, radius, sigma_e)
+
+    def add_line_source(self, axis, position, wavelength=None, frequency=None, bandwidth=0.5, amplitude=1.0,
+                        span=None):
+        """As the E_z line source, on the hi faces of the line cells: w_perp = 1 / inv_d*_h[line cell] of the kernel
+        widths (placement.py:254-265)."""
+        src = super().add_line_source(axis, position, wavelength, frequency, bandwidth, amplitude, span)
+        d = self.domain
+        normal = 1 if axis == 'x' else 0
+        n_cells = d.ny if axis == 'x' else d.nx
+        periodic = d.periodic_y if axis == 'x' else d.periodic_x
+        if src.position == n_cells - 1 and not periodic:
+            self.sources.pop()
+            raise ValueError('the H_z sheet would sit on the outer grid wall')
+        _, inv_face = yee_inverse_spacings(d.kernel_widths[normal])
+        src.normal_width = 1.0 / float(inv_face[src.position])
+        return src
+
+    def add_flux_monitor(self, axis, position, span, wavelengths=None, frequencies=None):
+        mon = super().add_flux_monitor(axis, position, span, wavelengths, frequencies)
+        mon.flux_sign = 1.0 if mon.normal_axis == 'x' else -1.0
+        return mon
+
+    def finalize(self):
+        d, real = self.domain, self.real
+        self.ca_x, self.cb_x, self.ca_y, self.cb_y = e_face_coefficients(
+            self.eps_xx, self.eps_yy, self.sigma_e, d.kernel_widths, d.periodic_x, d.periodic_y, d.dt, real)
+        self.da, self.db = h_coefficients(self.sigma_m, self.mu_r, d.dt, real)
+        self.cpml_sides, self.curl = build_cpml(d, real)
+        for src in self.sources:
+            normal = 1 if src.axis == 'x' else 0
+            widths = d.kernel_widths[normal]
+            lower_row, upper_row = src.position, (src.position + 1) % widths.size
+            w_lo, w_hi = float(widths[lower_row]), float(widths[upper_row])
+            cell_eps, cb_face = (self.eps_xx, self.cb_x) if src.axis == 'x' else (self.eps_yy, self.cb_y)
+            omega = 2.0 * np.pi * float(src.temporal.f0)
+
+            def row(array, r, src=src):
+                return array[src.lo:src.hi, r] if src.axis == 'x' else array[r, src.lo:src.hi]
+
+            def row_eps(r):
+                return (np.asarray(row(cell_eps, r), dtype=np.complex128)
+                        - 1j * np.asarray(row(self.sigma_e, r), dtype=np.float64) / (omega * EPS0))
+
+            line_eps = (row_eps(lower_row) * w_lo + row_eps(upper_row) * w_hi) / (w_lo + w_hi)
+            admittance = sheet_admittance(line_eps, row(self.mu_r, src.position), row(self.sigma_m, src.position),
+                                          omega, src.normal_width, float(d.dt))
+            weight = np.asarray(2.0 * np.ones(src.hi - src.lo) / (float(ETA0) * src.normal_width), dtype=DTYPE)
+            src.profile = (row(cb_face, src.position) * admittance * weight).astype(DTYPE)
+        self.sample_interval = dft_sample_interval(float(d.dt), self.sources, [m.frequencies for m in self.monitors])
+        for m in self.monitors:
+            m.sample_interval = self.sample_interval
+        self.psi_e = {s.name: np.zeros(self._psi_shape(s.name), dtype=real) for s in self.cpml_sides}
+        self.psi_h = {s.name: np.zeros(self._psi_shape(s.name), dtype=real) for s in self.cpml_sides}
+        self._finalized = True
+
+    def advance(self, n_steps):
+        lib, State, Line, Flux = load_library(self.real)
+        d, real = self.domain, self.real
+        R = ctypes.c_float if real == np.float32 else ctypes.c_double
+        values, times_full = self.source_values(n_steps)
+        first_q, n_q, phase_tables = self._chunk_phase_tables(n_steps, times_full)
+        st = State()
+        st.nx, st.ny, st.periodic_x, st.periodic_y = d.nx, d.ny, int(d.periodic_x), int(d.periodic_y)
+        st.hz, st.ex, st.ey = _ptr(self.hz, R), _ptr(self.ex, R), _ptr(self.ey, R)
+        for name in ('ca_x', 'cb_x', 'ca_y', 'cb_y', 'da', 'db'):
+            setattr(st, name, _ptr(getattr(self, name), R))
+        for name in ('inv_dx_e', 'inv_dx_h', 'inv_dy_e', 'inv_dy_h'):
+            setattr(st, name, _ptr(self.curl[name], R))
+        keep = self._cpml_state(st, R)
+        lines = self._line_structs(Line, values)
+        fluxes = self._flux_structs(Flux, phase_tables, first_q, n_q)
+        rc = lib.oracle_hz2d_advance(ctypes.byref(st), self.n_step, n_steps, len(self.sources), lines,
+                                     len(self.monitors), fluxes, self.sample_interval)
+        del keep
+        if rc != 0:
+            raise RuntimeError('oracle phase table does not cover a sample')
+        self._clock_after(n_steps, times_full)
