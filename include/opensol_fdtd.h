@@ -85,6 +85,41 @@ int os_fdtd2d_set_coefficients(OsFdtd2D *h, const float *ca, const float *cb, co
  * (physics/em/sources.py:582-602). */
 int os_fdtd2d_read_cb(OsFdtd2D *h, float *cb);
 
+/* ----------------------------------------------------------------------------------------------------------------
+ * 2D H_z polarisation (H_z at the cell centres, E_x on the hi-y faces, E_y on the hi-x faces): replaces
+ * FDTDEngine2D_Hz (open_sol/physics/em/solvers/fdtd_hz_2d.py:12).  An OsFdtd2D made by os_fdtd2d_hz_create takes
+ * the same spacing, CPML, line-source, flux-line, sample-interval, advance, read/write, reset and stream calls as an
+ * E_z engine, with these meanings: a line source adds to E_x (axis 0, the hi-y faces of y-cell `position`) or E_y
+ * (axis 1, the hi-x faces of x-cell `position`) after the E update (TangentialSheetCurrentSource,
+ * physics/em/sources.py:469-480); a flux line samples E_y (normal 0) or E_x (normal 1) with H_z
+ * (FluxMonitor 'hz', physics/em/monitors.py:350-362); field components are OS_HZ_HZ / OS_HZ_EX / OS_HZ_EY.
+ * os_fdtd2d_configure takes variant 1 (default: one fused kernel per step, tile_rows rows per CTA, 0 = chosen per
+ * grid) or 0 (one H_z and one E kernel per step) with steps_per_launch 1.  The E_z-only calls (set_materials,
+ * set_coefficients, read_cb, autotune, plan_info, batch, adjoint) return OS_ERR_STATE on an H_z handle and the
+ * H_z-only calls below on an E_z handle.
+ * ---------------------------------------------------------------------------------------------------------------- */
+enum { OS_HZ_HZ = 0, OS_HZ_EX = 1, OS_HZ_EY = 2 };
+
+/* Zeroed H_z engine: FDTDEngine2D_Hz.__init__ (fdtd_hz_2d.py:24-92) with the same grid checks as os_fdtd2d_create. */
+int os_fdtd2d_hz_create(const OsGrid2D *grid, OsFdtd2D **out);
+
+/* E face coefficients ca_x, cb_x (E_x faces) and ca_y, cb_y (E_y faces) from the float32 cell arrays (nx, ny) and
+ * the float32 face shares lower_x, upper_x (nx,) and lower_y, upper_y (ny,): e_face_coefficients
+ * (fdtd_hz_2d_kernels.py:196-277, face_shares yee_grid.py:119-125); da / db as os_fdtd2d_set_materials.  sigma_e
+ * NULL = lossless; mu_r, sigma_m NULL = vacuum permeability.  A lossless grid with eps_xx = eps_yy, every eps > 0,
+ * and vacuum permeability keeps one eps_r word per cell and the step kernel evaluates cb = dt / (face eps eps0)
+ * itself (the same bits as the stored form). */
+int os_fdtd2d_hz_set_materials(OsFdtd2D *h, const float *eps_xx, const float *eps_yy, const float *sigma_e,
+                               const float *mu_r, const float *sigma_m, const float *lower_x, const float *upper_x,
+                               const float *lower_y, const float *upper_y, float dt, float eps0, float mu0);
+
+/* Copies cb_x and cb_y (nx, ny) to the host (the face coefficients SheetCurrentCalibration.apply reads for a
+ * TangentialSheetCurrentSource, physics/em/sources.py:586-590). */
+int os_fdtd2d_hz_read_cb(OsFdtd2D *h, float *cb_x, float *cb_y);
+
+/* 1 when the lossless one-word-per-cell form is active, else 0.  No open_sol counterpart. */
+int os_fdtd2d_hz_form(OsFdtd2D *h, int32_t *lossless_form);
+
 /* One CPML side (a single OS_SIDE_* bit): psi recursion rows b, a and bulk curl spacing of its cell-centre (_e) and
  * hi-face (_h) rows, npml each (_cpml_row_set, boundaries.py:671-686; rows from cpml_side_rows, :570-576). */
 int os_fdtd2d_set_cpml_side(OsFdtd2D *h, int32_t side, const float *b_e, const float *a_e, const float *inv_e,

@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(_HERE, '_lib', 'libopensol_fdtd.so')
 OS_OK, OS_ERR_INVALID, OS_ERR_CUDA, OS_ERR_NO_MEMORY, OS_ERR_STATE = 0, 1, 2, 3, 4
 OS_SIDE_BITS = {'x_lo': 1, 'x_hi': 2, 'y_lo': 4, 'y_hi': 8, 'z_lo': 16, 'z_hi': 32}
 OS_EZ, OS_HX, OS_HY = 0, 1, 2
+OS_HZ_HZ, OS_HZ_EX, OS_HZ_EY = 0, 1, 2   # field buffers of an H_z engine
 FIELDS_3D = ('ex', 'ey', 'ez', 'hx', 'hy', 'hz')   # os_fdtd3d_read_field / write_field component order
 
 _lock = threading.Lock()
@@ -52,6 +53,11 @@ SIGNATURES = {
     'os_fdtd2d_set_materials': [_P, _F, _F, _F, _F, ctypes.c_float, ctypes.c_float, ctypes.c_float],
     'os_fdtd2d_set_coefficients': [_P, _F, _F, _F, _F, ctypes.c_float, ctypes.c_float],
     'os_fdtd2d_read_cb': [_P, _F],
+    'os_fdtd2d_hz_create': [ctypes.POINTER(OsGrid2D), ctypes.POINTER(_P)],
+    'os_fdtd2d_hz_set_materials': [_P, _F, _F, _F, _F, _F, _F, _F, _F, _F, ctypes.c_float, ctypes.c_float,
+                                   ctypes.c_float],
+    'os_fdtd2d_hz_read_cb': [_P, _F, _F],
+    'os_fdtd2d_hz_form': [_P, ctypes.POINTER(_I32)],
     'os_fdtd2d_set_cpml_side': [_P, _I32, _F, _F, _F, _F, _F, _F],
     'os_fdtd2d_add_line_source': [_P, _I32, _I32, _I32, _I32, _F, ctypes.POINTER(_I32)],
     'os_fdtd2d_set_line_profile': [_P, _I32, _F],

@@ -13,7 +13,7 @@ from enum import Enum
 
 import numpy as np
 
-from .constants import EPS0, FACES, FACES_3D
+from .constants import DTYPE, EPS0, FACES, FACES_3D
 
 
 class BCType(Enum):
@@ -262,6 +262,14 @@ def inverse_spacings(widths):
         raise ValueError(f"cell widths must be a non-empty 1D array, got shape {widths.shape}")
     face_spacing = 0.5 * (widths + np.roll(widths, -1))
     return 1.0 / widths, 1.0 / face_spacing
+
+
+def face_shares(widths, periodic):
+    """float32 (lower, upper) hi-face weights w_k / (w_k + w_k+1), w_k+1 / (w_k + w_k+1); the last partner is the
+    first cell (periodic) or the cell itself (yee_grid.py:76-84,119-125)."""
+    widths = np.asarray(widths, dtype=np.float64)
+    partner = np.roll(widths, -1) if periodic else np.concatenate((widths[1:], widths[-1:]))
+    return (widths / (widths + partner)).astype(DTYPE), (partner / (widths + partner)).astype(DTYPE)
 
 
 @dataclass(frozen=True)

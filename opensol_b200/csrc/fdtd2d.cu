@@ -13,6 +13,7 @@
 #include "fdtd2d_kernels.cuh"
 #include "fdtd2d_tb.cuh"
 #include "fdtd2d_interior.cuh"
+#include "fdtd2d_hz.cuh"
 
 #include <algorithm>
 
@@ -71,6 +72,15 @@ struct OsFdtd2D {
     os::DeviceArray<float> line_values;   // (n_lines, n_steps) of the current chunk
     os::DeviceArray<float> phases;        // per monitor (n_samples, nf, 2) of the current chunk
     int device = 0;
+    // H_z polarisation (os_fdtd2d_hz_create): ez / hx / hy hold H_z / E_x / E_y, ca / cb the E_x face coefficients
+    int32_t polarization = 0;             // 0 E_z, 1 H_z
+    os::DeviceArray<float> ca_y, cb_y;    // E_y face coefficients (coefficient form)
+    os::DeviceArray<float> eps_cell;      // eps_r per cell (lossless form: face coefficients evaluated in the kernel)
+    os::DeviceArray<float> shares;        // lower_x, upper_x (nx each), lower_y, upper_y (ny each)
+    bool hz_eps = false;                  // lossless form active
+    float dt_hz = 0.0f, eps0_hz = 0.0f;   // dt and eps0 of the lossless form
+    int32_t hz_rows = 0;                  // rows per CTA of the fused step kernel (0: chosen per grid)
+    int sm_count = 148;                   // multiprocessors of the device (launch sizing)
 };
 
 namespace os {
@@ -159,6 +169,18 @@ static Ez2DParams make_params(const OsFdtd2D *h) {
     return p;
 }
 
+// Entry points of one polarisation refuse a handle of the other.
+static int require_hz(const OsFdtd2D *h, const char *fn) {
+    OS_CHECK(h, OS_ERR_INVALID, "%s: null handle", fn);
+    OS_CHECK(h->polarization == 1, OS_ERR_STATE, "%s: the handle is an E_z engine (os_fdtd2d_create)", fn);
+    return OS_OK;
+}
+static int require_ez(const OsFdtd2D *h, const char *fn) {
+    OS_CHECK(h, OS_ERR_INVALID, "%s: null handle", fn);
+    OS_CHECK(h->polarization == 0, OS_ERR_STATE, "%s: the handle is an H_z engine (os_fdtd2d_hz_create)", fn);
+    return OS_OK;
+}
+
 }  // namespace os
 
 using namespace os;
@@ -194,6 +216,7 @@ extern "C" int os_fdtd2d_create(const OsGrid2D *grid, OsFdtd2D **out) {
     OS_CUDA(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     OS_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
     h->stream = h->own_stream;
+    OS_CUDA(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device));
     OS_CUDA(cudaEventCreate(&h->ev_start));
     OS_CUDA(cudaEventCreate(&h->ev_stop));
     const size_t n = cells(h.get());
@@ -255,7 +278,8 @@ extern "C" int os_fdtd2d_set_spacings(OsFdtd2D *h, const float *inv_dx_e, const 
 
 extern "C" int os_fdtd2d_set_materials(OsFdtd2D *h, const float *eps_r, const float *sigma_e, const float *mu_r,
                                        const float *sigma_m, float dt, float eps0, float mu0) {
-    OS_CHECK(h && eps_r, OS_ERR_INVALID, "os_fdtd2d_set_materials: eps_r is required");
+    OS_TRY(require_ez(h, "os_fdtd2d_set_materials"));
+    OS_CHECK(eps_r, OS_ERR_INVALID, "os_fdtd2d_set_materials: eps_r is required");
     OS_TRY(bind_device(h));
     const size_t n = cells(h);
     OS_TRY(h->cb.alloc(n));
@@ -300,7 +324,8 @@ extern "C" int os_fdtd2d_set_materials(OsFdtd2D *h, const float *eps_r, const fl
 
 extern "C" int os_fdtd2d_set_coefficients(OsFdtd2D *h, const float *ca, const float *cb, const float *da,
                                           const float *db, float da_uniform, float db_uniform) {
-    OS_CHECK(h && cb, OS_ERR_INVALID, "os_fdtd2d_set_coefficients: cb is required");
+    OS_TRY(require_ez(h, "os_fdtd2d_set_coefficients"));
+    OS_CHECK(cb, OS_ERR_INVALID, "os_fdtd2d_set_coefficients: cb is required");
     OS_CHECK((da == nullptr) == (db == nullptr), OS_ERR_INVALID, "os_fdtd2d_set_coefficients: pass both da and db or neither");
     OS_TRY(bind_device(h));
     const size_t n = cells(h);
@@ -319,11 +344,113 @@ extern "C" int os_fdtd2d_set_coefficients(OsFdtd2D *h, const float *ca, const fl
 }
 
 extern "C" int os_fdtd2d_read_cb(OsFdtd2D *h, float *cb) {
-    OS_CHECK(h && cb, OS_ERR_INVALID, "os_fdtd2d_read_cb: null argument");
+    OS_TRY(require_ez(h, "os_fdtd2d_read_cb"));
+    OS_CHECK(cb, OS_ERR_INVALID, "os_fdtd2d_read_cb: null argument");
     OS_CHECK(h->has_cb, OS_ERR_STATE, "os_fdtd2d_read_cb: coefficients are not set");
     OS_TRY(bind_device(h));
     OS_CUDA(cudaMemcpyAsync(cb, h->cb.ptr, cells(h) * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
     OS_CUDA(cudaStreamSynchronize(h->stream));
+    return OS_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// H_z polarisation: the same handle with H_z / E_x / E_y in the three field buffer sets.
+
+extern "C" int os_fdtd2d_hz_create(const OsGrid2D *grid, OsFdtd2D **out) {
+    OS_TRY(os_fdtd2d_create(grid, out));
+    (*out)->polarization = 1;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_hz_set_materials(OsFdtd2D *h, const float *eps_xx, const float *eps_yy,
+                                          const float *sigma_e, const float *mu_r, const float *sigma_m,
+                                          const float *lower_x, const float *upper_x, const float *lower_y,
+                                          const float *upper_y, float dt, float eps0, float mu0) {
+    OS_TRY(require_hz(h, "os_fdtd2d_hz_set_materials"));
+    OS_CHECK(eps_xx && eps_yy && lower_x && upper_x && lower_y && upper_y, OS_ERR_INVALID,
+             "os_fdtd2d_hz_set_materials: eps_xx, eps_yy and the face shares are required");
+    OS_TRY(bind_device(h));
+    const size_t n = cells(h);
+    const int nx = h->grid.nx, ny = h->grid.ny;
+    // Lossless form: no sigma_e (or all zero), eps_xx = eps_yy with every eps_r > 0 and finite, vacuum permeability;
+    // then k = 0 and the denominators are exactly 1, so cb = dt / (face eps_r * eps0) is evaluated in the step kernel.
+    bool lossless = true;
+    if (sigma_e)
+        for (size_t c = 0; c < n && lossless; ++c) lossless = sigma_e[c] == 0.0f;
+    bool eps_form = lossless && !mu_r && !sigma_m && std::memcmp(eps_xx, eps_yy, n * sizeof(float)) == 0;
+    for (size_t c = 0; c < n && eps_form; ++c) eps_form = eps_xx[c] > 0.0f && eps_xx[c] <= 3.0e38f;
+    std::vector<float> shares(2 * (size_t)nx + 2 * (size_t)ny);
+    std::memcpy(shares.data(), lower_x, nx * sizeof(float));
+    std::memcpy(shares.data() + nx, upper_x, nx * sizeof(float));
+    std::memcpy(shares.data() + 2 * nx, lower_y, ny * sizeof(float));
+    std::memcpy(shares.data() + 2 * nx + ny, upper_y, ny * sizeof(float));
+    OS_TRY(upload(h->shares, shares.data(), shares.size(), h->stream));
+    DeviceArray<float> exx, eyy, sig;
+    OS_TRY(upload(exx, eps_xx, n, h->stream));
+    OS_TRY(upload(eyy, eps_yy, n, h->stream));
+    if (sigma_e && !lossless) OS_TRY(upload(sig, sigma_e, n, h->stream));
+    OS_TRY(h->cb.alloc(n));
+    OS_TRY(h->cb_y.alloc(n));
+    if (!lossless) {
+        OS_TRY(h->ca.alloc(n));
+        OS_TRY(h->ca_y.alloc(n));
+    }
+    const float *sh = h->shares.ptr;
+    const dim3 block(EZ2D_BLOCK_X, EZ2D_BLOCK_Y);
+    const dim3 grid_dim((unsigned)((ny + block.x - 1) / block.x), (unsigned)((nx + block.y - 1) / block.y));
+    hz2d_face_coefficients_kernel<<<grid_dim, block, 0, h->stream>>>(
+        exx.ptr, eyy.ptr, sig.ptr, sh, sh + nx, sh + 2 * nx, sh + 2 * nx + ny, nx, ny, h->grid.periodic_x,
+        h->grid.periodic_y, dt, eps0, lossless ? nullptr : h->ca.ptr, h->cb.ptr, lossless ? nullptr : h->ca_y.ptr,
+        h->cb_y.ptr);
+    OS_CUDA(cudaGetLastError());
+    h->has_ca = !lossless;
+    h->has_cb = true;
+    h->hz_eps = eps_form;
+    h->dt_hz = dt;
+    h->eps0_hz = eps0;
+    if (eps_form) {
+        OS_TRY(h->eps_cell.alloc(n));
+        OS_CUDA(cudaMemcpyAsync(h->eps_cell.ptr, exx.ptr, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+    }
+    if (mu_r || sigma_m) {
+        DeviceArray<float> mu_dev, sm_dev;
+        if (mu_r) OS_TRY(upload(mu_dev, mu_r, n, h->stream));
+        if (sigma_m) OS_TRY(upload(sm_dev, sigma_m, n, h->stream));
+        OS_TRY(h->da.alloc(n));
+        OS_TRY(h->db.alloc(n));
+        const unsigned blocks = (unsigned)((n + 255) / 256);
+        ez2d_h_coefficients_kernel<<<blocks, 256, 0, h->stream>>>(mu_dev.ptr, sm_dev.ptr, dt, mu0, n, h->da.ptr,
+                                                                  h->db.ptr);
+        OS_CUDA(cudaGetLastError());
+        h->has_dadb = true;
+    } else {
+        // vacuum permeability: da = (1 - 0) / 1, db = (dt / mu0) / 1 (fdtd_ez_2d_kernels.py:335-340)
+        const float mu = 1.0f * mu0;
+        const float k = (0.0f * dt) / (2.0f * mu);
+        const float denom = 1.0f + k;
+        h->da_uniform = (1.0f - k) / denom;
+        h->db_uniform = (dt / mu) / denom;
+        h->has_dadb = false;
+    }
+    OS_CUDA(cudaStreamSynchronize(h->stream));   // the staging arrays are freed on return
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_hz_read_cb(OsFdtd2D *h, float *cb_x, float *cb_y) {
+    OS_TRY(require_hz(h, "os_fdtd2d_hz_read_cb"));
+    OS_CHECK(cb_x && cb_y, OS_ERR_INVALID, "os_fdtd2d_hz_read_cb: null argument");
+    OS_CHECK(h->has_cb, OS_ERR_STATE, "os_fdtd2d_hz_read_cb: materials are not set");
+    OS_TRY(bind_device(h));
+    OS_CUDA(cudaMemcpyAsync(cb_x, h->cb.ptr, cells(h) * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    OS_CUDA(cudaMemcpyAsync(cb_y, h->cb_y.ptr, cells(h) * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_hz_form(OsFdtd2D *h, int32_t *lossless_form) {
+    OS_TRY(require_hz(h, "os_fdtd2d_hz_form"));
+    OS_CHECK(lossless_form, OS_ERR_INVALID, "os_fdtd2d_hz_form: null argument");
+    *lossless_form = h->hz_eps ? 1 : 0;
     return OS_OK;
 }
 
@@ -725,6 +852,131 @@ static int advance_per_step(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, 
     return OS_OK;
 }
 
+// Parameters of the H_z kernels: inputs from buffer set `in`, outputs to `out` (the same set for the in-place
+// per-half-step kernels).
+static Hz2DParams make_hz_params(const OsFdtd2D *h, int in, int out) {
+    Hz2DParams p{};
+    p.nx = h->grid.nx;
+    p.ny = h->grid.ny;
+    p.px = h->grid.periodic_x;
+    p.py = h->grid.periodic_y;
+    p.npml = h->grid.npml;
+    p.hz_in = h->ez[in].ptr;
+    p.ex_in = h->hx[in].ptr;
+    p.ey_in = h->hy[in].ptr;
+    p.hz_out = h->ez[out].ptr;
+    p.ex_out = h->hx[out].ptr;
+    p.ey_out = h->hy[out].ptr;
+    p.ca_x = h->has_ca ? h->ca.ptr : nullptr;
+    p.cb_x = h->cb.ptr;
+    p.ca_y = h->has_ca ? h->ca_y.ptr : nullptr;
+    p.cb_y = h->cb_y.ptr;
+    p.da = h->has_dadb ? h->da.ptr : nullptr;
+    p.db = h->has_dadb ? h->db.ptr : nullptr;
+    p.da_u = h->da_uniform;
+    p.db_u = h->db_uniform;
+    p.eps = h->eps_cell.ptr;
+    p.dt = h->dt_hz;
+    p.eps0 = h->eps0_hz;
+    const int nx = h->grid.nx, ny = h->grid.ny;
+    p.lo_x = h->shares.ptr;
+    p.up_x = h->shares.ptr ? h->shares.ptr + nx : nullptr;
+    p.lo_y = h->shares.ptr ? h->shares.ptr + 2 * nx : nullptr;
+    p.up_y = h->shares.ptr ? h->shares.ptr + 2 * nx + ny : nullptr;
+    p.ixe = h->inv_dx_e.ptr;
+    p.ixh = h->inv_dx_h.ptr;
+    p.iye = h->inv_dy_e.ptr;
+    p.iyh = h->inv_dy_h.ptr;
+    const int npml = h->grid.npml;
+    for (int s = 0; s < 4; ++s) {
+        if (!(h->grid.cpml_sides & (1 << s))) continue;
+        p.cpml_mask |= 1 << s;
+        const float *rows = h->cpml_rows[s].ptr;
+        p.b_e[s] = rows;
+        p.a_e[s] = rows + npml;
+        p.inv_e[s] = rows + 2 * npml;
+        p.b_h[s] = rows + 3 * npml;
+        p.a_h[s] = rows + 4 * npml;
+        p.inv_h[s] = rows + 5 * npml;
+        p.psi_e_in[s] = h->psi_e[in][s].ptr;
+        p.psi_h_in[s] = h->psi_h[in][s].ptr;
+        p.psi_e_out[s] = h->psi_e[out][s].ptr;
+        p.psi_h_out[s] = h->psi_h[out][s].ptr;
+    }
+    p.n_lines = (int32_t)h->lines.size();
+    for (size_t l = 0; l < h->lines.size(); ++l) {
+        p.lines[l].axis = h->lines[l]->axis;
+        p.lines[l].position = h->lines[l]->position;
+        p.lines[l].lo = h->lines[l]->lo;
+        p.lines[l].hi = h->lines[l]->hi;
+        p.lines[l].profile = h->lines[l]->profile.ptr;
+    }
+    return p;
+}
+
+// Rows per CTA of the fused H_z step: enough CTAs for several waves on the device's SMs, 16..256 rows.
+static int hz_rows_per_cta(const OsFdtd2D *h) {
+    if (h->hz_rows > 0) return h->hz_rows;
+    const int64_t strips = (h->grid.ny + HZ_STRIP - 1) / HZ_STRIP;
+    const int64_t want_ctas = (int64_t)h->sm_count * 8;
+    int64_t rows = (int64_t)h->grid.nx * strips / want_ctas;
+    rows = std::max<int64_t>(16, std::min<int64_t>(256, rows));
+    return (int)rows;
+}
+
+// H_z chunk: variant 0 launches the in-place H and E kernels per step, otherwise one fused step kernel per step
+// (buffers swapped after each); the flux lines are sampled after every step that is a sample step.
+static int advance_hz(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples, const float *values,
+                      const float *phase_table) {
+    const int64_t m = h->sample_interval;
+    const int nx = h->grid.nx, ny = h->grid.ny;
+    const dim3 cell_block(EZ2D_BLOCK_X, EZ2D_BLOCK_Y);
+    const dim3 cell_grid((unsigned)((ny + cell_block.x - 1) / cell_block.x),
+                         (unsigned)((nx + cell_block.y - 1) / cell_block.y));
+    const int rows = hz_rows_per_cta(h);
+    const dim3 step_grid((unsigned)((ny + HZ_STRIP - 1) / HZ_STRIP), (unsigned)((nx + rows - 1) / rows));
+    for (int64_t k = 0; k < n_steps; ++k) {
+        const int in = h->cur, out = h->variant == 0 ? h->cur : h->cur ^ 1;
+        Hz2DParams p = make_hz_params(h, in, out);
+        p.line_values = values;
+        p.values_stride = n_steps;
+        p.k_step = k;
+        p.rows_per_cta = rows;
+        OS_TRY(prof_begin(h, 3, h->stream));
+        if (h->variant == 0) {
+            hz2d_h_kernel<<<cell_grid, cell_block, 0, h->stream>>>(p);
+            hz2d_e_kernel<<<cell_grid, cell_block, 0, h->stream>>>(p);
+            h->launches += 2;
+        } else {
+            if (h->hz_eps) hz2d_step_kernel<true><<<step_grid, HZ_STRIP, 0, h->stream>>>(p);
+            else hz2d_step_kernel<false><<<step_grid, HZ_STRIP, 0, h->stream>>>(p);
+            h->launches += 1;
+        }
+        OS_TRY(prof_end(h, h->stream));
+        h->cur = out;
+        h->n_step += 1;
+        if (!h->fluxes.empty() && h->n_step % m == 0) {
+            const int64_t q = h->n_step / m;
+            size_t offset = 0;
+            for (auto &f : h->fluxes) {
+                const float *ph = phase_table + offset + (size_t)(q - first_sample) * f->nf * 2;
+                const int n = f->hi - f->lo;
+                const int total = n * f->nf;
+                // E_y on the hi-x faces for a line normal to x, E_x on the hi-y faces for one normal to y; H_z
+                OS_TRY(prof_begin(h, 2, h->stream));
+                ez2d_flux_kernel<<<(total + 255) / 256, 256, 0, h->stream>>>(
+                    f->normal_axis == 0 ? h->hy[h->cur].ptr : h->hx[h->cur].ptr, h->ez[h->cur].ptr, ny,
+                    f->normal_axis, f->position, f->lo, n, f->nf, ph, f->e_acc.ptr, f->h_acc.ptr);
+                OS_TRY(prof_end(h, h->stream));
+                h->launches += 1;
+                offset += (size_t)n_samples * f->nf * 2;
+            }
+        }
+    }
+    OS_CUDA(cudaGetLastError());
+    return OS_OK;
+}
+
 // Argument and state checks shared by the advance entry points (`fn` names the caller in messages).
 static int check_advance(const OsFdtd2D *h, const char *fn, int64_t n_steps, const float *line_values,
                          int64_t first_sample, int64_t n_samples, const float *phases) {
@@ -751,8 +1003,9 @@ static int check_advance(const OsFdtd2D *h, const char *fn, int64_t n_steps, con
 static int run_chunk(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples, const float *values,
                      const float *phase_table) {
     OS_CUDA(cudaEventRecord(h->ev_start, h->stream));
-    const int rc = h->variant == 0 ? advance_per_step(h, n_steps, first_sample, n_samples, values, phase_table)
-                                   : advance_blocked(h, n_steps, first_sample, n_samples, values, phase_table);
+    const int rc = h->polarization == 1 ? advance_hz(h, n_steps, first_sample, n_samples, values, phase_table)
+                   : h->variant == 0    ? advance_per_step(h, n_steps, first_sample, n_samples, values, phase_table)
+                                        : advance_blocked(h, n_steps, first_sample, n_samples, values, phase_table);
     if (rc != OS_OK) return rc;
     OS_CUDA(cudaEventRecord(h->ev_stop, h->stream));
     h->timed = true;
@@ -848,6 +1101,15 @@ extern "C" int os_fdtd2d_configure(OsFdtd2D *h, int32_t variant, int32_t steps_p
              "variant must be 0 (per half step), 1 (blocked) or 2 (blocked, general kernel only)");
     OS_CHECK(steps_per_launch >= 1 && steps_per_launch <= TB_MAX_T, OS_ERR_INVALID,
              "steps_per_launch must be in [1, %d], got %d", TB_MAX_T, steps_per_launch);
+    if (h->polarization == 1) {
+        // H_z: variant 0 per-half-step kernels, 1 the fused step kernel with tile_rows rows per CTA (0: per grid)
+        OS_CHECK(variant <= 1 && steps_per_launch == 1 && tile_rows >= 0, OS_ERR_INVALID,
+                 "an H_z engine takes variant 0 or 1, steps_per_launch 1 and tile_rows >= 0, got %d, %d, %d", variant,
+                 steps_per_launch, tile_rows);
+        h->variant = variant;
+        h->hz_rows = tile_rows;
+        return OS_OK;
+    }
     OS_CHECK(tile_rows >= 1, OS_ERR_INVALID, "tile_rows must be >= 1, got %d", tile_rows);
     h->variant = variant;
     h->steps_per_launch = steps_per_launch;
@@ -857,7 +1119,8 @@ extern "C" int os_fdtd2d_configure(OsFdtd2D *h, int32_t variant, int32_t steps_p
 
 extern "C" int os_fdtd2d_autotune(OsFdtd2D *h, int32_t steps_per_launch, const int32_t *candidates,
                                   int32_t n_candidates, int32_t repeats, int32_t *best_rows, float *best_ms) {
-    OS_CHECK(h && candidates && n_candidates > 0 && best_rows && best_ms, OS_ERR_INVALID,
+    OS_TRY(require_ez(h, "os_fdtd2d_autotune"));
+    OS_CHECK(candidates && n_candidates > 0 && best_rows && best_ms, OS_ERR_INVALID,
              "os_fdtd2d_autotune: null argument or no candidates");
     OS_CHECK(steps_per_launch >= 1 && steps_per_launch <= TB_MAX_T, OS_ERR_INVALID,
              "steps_per_launch must be in [1, %d]", TB_MAX_T);
@@ -921,8 +1184,8 @@ extern "C" int os_fdtd2d_autotune(OsFdtd2D *h, int32_t steps_per_launch, const i
 
 extern "C" int os_fdtd2d_plan_info(OsFdtd2D *h, int32_t steps_per_launch, int64_t *interior_cells,
                                    int64_t *interior_tiles, int64_t *general_tiles) {
-    OS_CHECK(h && interior_cells && interior_tiles && general_tiles, OS_ERR_INVALID,
-             "os_fdtd2d_plan_info: null argument");
+    OS_TRY(require_ez(h, "os_fdtd2d_plan_info"));
+    OS_CHECK(interior_cells && interior_tiles && general_tiles, OS_ERR_INVALID, "os_fdtd2d_plan_info: null argument");
     OS_CHECK(steps_per_launch >= 1 && steps_per_launch <= TB_MAX_T, OS_ERR_INVALID,
              "steps_per_launch must be in [1, %d]", TB_MAX_T);
     OS_CHECK(h->has_spacings, OS_ERR_STATE, "os_fdtd2d_plan_info: spacings are not set");
@@ -1190,6 +1453,7 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
     for (int32_t q = 0; q < n_jobs; ++q) {
         OsFdtd2D *h = handles[q];
         OS_CHECK(h, OS_ERR_INVALID, "os_fdtd2d_batch_advance: job %d has no handle", q);
+        OS_TRY(require_ez(h, "os_fdtd2d_batch_advance"));
         OS_TRY(check_advance(h, "os_fdtd2d_batch_advance", n_steps, line_values[q], first_samples[q], n_samples[q],
                              phases[q]));
         OS_CHECK(h->device == b->device, OS_ERR_INVALID, "os_fdtd2d_batch_advance: job %d is on device %d, the batch on "
@@ -1440,6 +1704,7 @@ extern "C" int os_fdtd2d_adjoint_create(OsFdtd2D *h, int32_t box_i0, int32_t box
                                         int32_t n_slots, int32_t segment_steps, OsAdjoint2D **out) {
     using namespace os;
     OS_CHECK(h && out, OS_ERR_INVALID, "os_fdtd2d_adjoint_create: null argument");
+    OS_TRY(require_ez(h, "os_fdtd2d_adjoint_create"));
     *out = nullptr;
     OS_CHECK(h->has_cb && h->has_spacings, OS_ERR_STATE, "os_fdtd2d_adjoint_create: coefficients and spacings first");
     OS_CHECK(0 <= box_i0 && box_i0 < box_i1 && box_i1 <= h->grid.nx && 0 <= box_j0 && box_j0 < box_j1 &&

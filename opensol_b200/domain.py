@@ -48,10 +48,11 @@ def _window_slice(centres, lo, hi):
 
 
 class MaterialGrid:
-    """Host float32 (nx, ny[, nz]) material arrays eps_r, sigma_e, mu_r, sigma_m (core/material_grid.py:7-91).  An
-    array still at its default is not allocated (None): a lossless, non-magnetic grid uploads eps_r alone."""
+    """Host float32 (nx, ny[, nz]) material arrays eps_r, sigma_e, mu_r, sigma_m and the H_z polarisation's eps_xx,
+    eps_yy (core/material_grid.py:7-91).  An array still at its default is not allocated (None): a lossless,
+    non-magnetic E_z grid uploads eps_r alone."""
 
-    DEFAULTS = {'eps_r': 1.0, 'sigma_e': 0.0, 'mu_r': 1.0, 'sigma_m': 0.0}
+    DEFAULTS = {'eps_r': 1.0, 'sigma_e': 0.0, 'mu_r': 1.0, 'sigma_m': 0.0, 'eps_xx': 1.0, 'eps_yy': 1.0}
 
     def __init__(self, shape, pinned=False):
         self.shape = tuple(shape)

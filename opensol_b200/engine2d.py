@@ -13,7 +13,7 @@ import ctypes
 import numpy as np
 
 from . import _native
-from .boundaries import build_yee_rows
+from .boundaries import build_yee_rows, face_shares
 from .constants import DTYPE, EPS0, MU0
 from .monitors import dft_phase_table
 
@@ -22,6 +22,8 @@ class FDTDEngine2D_Ez:
     """Device engine of one 2D E_z simulation (real fields, CPML and periodic faces)."""
 
     polarization = 'ez'
+    FIELDS = {'ez': _native.OS_EZ, 'hx': _native.OS_HX, 'hy': _native.OS_HY}
+    _CREATE = 'os_fdtd2d_create'
     KERNEL_KINDS = {0: 'ez2d_interior_kernel', 1: 'ez2d_tb_kernel (general)', 2: 'ez2d_flux_staged_kernel',
                     3: 'ez2d_h_kernel+ez2d_e_kernel'}
 
@@ -62,7 +64,8 @@ class FDTDEngine2D_Ez:
                                     int(self.boundary_config.periodic_y), int(self.boundary_config.cpml_npml),
                                     sides, self.device)
             h = ctypes.c_void_p()
-            _native.check(lib.os_fdtd2d_create(ctypes.byref(grid), ctypes.byref(h)), 'os_fdtd2d_create')
+            create = getattr(lib, self._CREATE)
+            _native.check(create(ctypes.byref(grid), ctypes.byref(h)), self._CREATE)
             self._handle = h
             c = self.rows.curl
             _native.check(lib.os_fdtd2d_set_spacings(h, _native.fptr(c['inv_dx_e']), _native.fptr(c['inv_dx_h']),
@@ -103,11 +106,7 @@ class FDTDEngine2D_Ez:
         h = self.handle
         materials = self.domain.materials
         if self._materials_version != materials.version:
-            arrays = [materials.get(name) for name in ('eps_r', 'sigma_e', 'mu_r', 'sigma_m')]
-            arrays = [None if a is None else np.ascontiguousarray(a, dtype=DTYPE) for a in arrays]
-            _native.check(lib.os_fdtd2d_set_materials(h, *(_native.fptr(a) for a in arrays), float(self.dt),
-                                                      float(DTYPE(EPS0)), float(DTYPE(MU0))))
-            self.h2d_bytes += sum(a.nbytes for a in arrays if a is not None)
+            self._upload_materials(lib, h, materials)
             self._materials_version = materials.version
         for source in self._lines:
             profile = np.ascontiguousarray(source.profile, dtype=DTYPE)
@@ -135,6 +134,13 @@ class FDTDEngine2D_Ez:
         if self._config_sent != config:
             _native.check(lib.os_fdtd2d_configure(h, *config))
             self._config_sent = config
+
+    def _upload_materials(self, lib, h, materials):
+        arrays = [materials.get(name) for name in ('eps_r', 'sigma_e', 'mu_r', 'sigma_m')]
+        arrays = [None if a is None else np.ascontiguousarray(a, dtype=DTYPE) for a in arrays]
+        _native.check(lib.os_fdtd2d_set_materials(h, *(_native.fptr(a) for a in arrays), float(self.dt),
+                                                  float(DTYPE(EPS0)), float(DTYPE(MU0))))
+        self.h2d_bytes += sum(a.nbytes for a in arrays if a is not None)
 
     def configure(self, variant=None, steps_per_launch=None, tile_rows=None):
         """Kernel choice (results are bit-identical for every choice): variant 1 = temporally blocked kernels
@@ -252,13 +258,13 @@ class FDTDEngine2D_Ez:
 
     # ------------------------------------------------------------------------------------------- readout
     def read_field(self, name):
-        comp = {'ez': _native.OS_EZ, 'hx': _native.OS_HX, 'hy': _native.OS_HY}[name]
+        comp = self.FIELDS[name]
         out = np.empty((self.nx, self.ny), dtype=DTYPE)
         _native.check(_native.load().os_fdtd2d_read_field(self.handle, comp, _native.fptr(out)))
         return out
 
     def write_field(self, name, values):
-        comp = {'ez': _native.OS_EZ, 'hx': _native.OS_HX, 'hy': _native.OS_HY}[name]
+        comp = self.FIELDS[name]
         arr = np.ascontiguousarray(values, dtype=DTYPE)
         if arr.shape != (self.nx, self.ny):
             raise ValueError(f'{name} must have shape {(self.nx, self.ny)}, got {arr.shape}')
@@ -287,3 +293,68 @@ class FDTDEngine2D_Ez:
         return {'ez': self.read_field('ez'), 'hx': self.read_field('hx'), 'hy': self.read_field('hy'),
                 'eps_r': materials.array('eps_r'), 'sigma_e': materials.array('sigma_e'), 'jz_total': None,
                 'q_accum': None, 'q_accum_time': 0.0}
+
+
+class FDTDEngine2D_Hz(FDTDEngine2D_Ez):
+    """Device engine of one 2D H_z simulation (FDTDEngine2D_Hz, open_sol/physics/em/solvers/fdtd_hz_2d.py:12): H_z at
+    the cell centres, E_x / E_y on the hi-y / hi-x faces, face-averaged eps_xx / eps_yy / sigma_e.  One fused kernel
+    per Yee step (variant 1, tile_rows rows per CTA, 0 = chosen per grid) or the in-place per-half-step kernels
+    (variant 0); both give bit-identical fields."""
+
+    polarization = 'hz'
+    FIELDS = {'hz': _native.OS_HZ_HZ, 'ex': _native.OS_HZ_EX, 'ey': _native.OS_HZ_EY}
+    _CREATE = 'os_fdtd2d_hz_create'
+    KERNEL_KINDS = {2: 'ez2d_flux_kernel (E_x|E_y, H_z)', 3: 'hz2d_step_kernel | hz2d_h_kernel+hz2d_e_kernel'}
+
+    def __init__(self, domain, boundary_config, device: int = 0):
+        super().__init__(domain, boundary_config, device)
+        self.variant, self.steps_per_launch, self.tile_rows = 1, 1, 0
+        bc = boundary_config
+        widths_x, widths_y = domain.kernel_widths()
+        self.shares_x = face_shares(widths_x, bc.periodic_x)
+        self.shares_y = face_shares(widths_y, bc.periodic_y)
+
+    def _upload_materials(self, lib, h, materials):
+        arrays = [materials.get(name) for name in ('eps_xx', 'eps_yy', 'sigma_e', 'mu_r', 'sigma_m')]
+        for k in (0, 1):
+            if arrays[k] is None:
+                arrays[k] = materials.array('eps_xx' if k == 0 else 'eps_yy')
+        arrays = [None if a is None else np.ascontiguousarray(a, dtype=DTYPE) for a in arrays]
+        shares = [np.ascontiguousarray(a) for a in (*self.shares_x, *self.shares_y)]
+        _native.check(lib.os_fdtd2d_hz_set_materials(h, *(_native.fptr(a) for a in arrays),
+                                                     *(_native.fptr(a) for a in shares), float(self.dt),
+                                                     float(DTYPE(EPS0)), float(DTYPE(MU0))))
+        self.h2d_bytes += sum(a.nbytes for a in arrays if a is not None)
+
+    def configure(self, variant=None, steps_per_launch=None, tile_rows=None):
+        """variant 1 (default): one fused kernel per step with tile_rows rows per CTA (0 = chosen per grid); variant
+        0: one H_z and one E kernel per step.  steps_per_launch is 1."""
+        super().configure(variant, steps_per_launch, tile_rows)
+
+    def autotune(self, candidates=None, repeats=4):
+        raise NotImplementedError('the H_z engine chooses its rows per CTA from the grid (configure(tile_rows=...))')
+
+    def plan_info(self, steps_per_launch=None):
+        raise NotImplementedError('the H_z engine has no blocked-kernel plan')
+
+    def lossless_form(self):
+        """True when the step kernel evaluates the face cb from eps_r (no coefficient arrays stored)."""
+        self.sync_device()
+        out = ctypes.c_int32()
+        _native.check(_native.load().os_fdtd2d_hz_form(self.handle, ctypes.byref(out)))
+        return bool(out.value)
+
+    def read_cb(self):
+        """(cb_x, cb_y) of the E_x / E_y faces (nx, ny) from the device."""
+        self.sync_device()
+        cb_x = np.empty((self.nx, self.ny), dtype=DTYPE)
+        cb_y = np.empty((self.nx, self.ny), dtype=DTYPE)
+        _native.check(_native.load().os_fdtd2d_hz_read_cb(self.handle, _native.fptr(cb_x), _native.fptr(cb_y)))
+        return cb_x, cb_y
+
+    def state(self):
+        """Host copies of the public fields (FDTDEngine2D_Hz.state, fdtd_hz_2d.py:94-104)."""
+        materials = self.domain.materials
+        return {'hz': self.read_field('hz'), 'eps_xx': materials.array('eps_xx'),
+                'eps_yy': materials.array('eps_yy'), 'sigma_e': materials.array('sigma_e'), 'q_accum': None,
+                'q_accum_time': 0.0}

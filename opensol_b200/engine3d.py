@@ -15,7 +15,7 @@ import ctypes
 import numpy as np
 
 from . import _native
-from .boundaries import cpml_axis_profiles, cpml_recursion, cpml_side_rows
+from .boundaries import cpml_axis_profiles, cpml_recursion, cpml_side_rows, face_shares  # noqa: F401
 from .constants import DTYPE
 from .domain3d import AXES
 from .material_index3d import build_material_index
@@ -24,14 +24,6 @@ from .monitors import dft_phase_table
 MAX_MATERIAL_IDS = 65535
 REQUIRED_ARRAYS = ('eps_r', 'sigma_e', 'mu_r')
 OPTIONAL_ARRAYS = ('eps_xx', 'eps_yy', 'sigma_m')
-
-
-def face_shares(widths, periodic):
-    """float32 (lower, upper) hi-face weights w_k / (w_k + w_k+1), w_k+1 / (w_k + w_k+1); the last partner is the
-    first cell (periodic) or the cell itself (yee_grid.py:76-84,119-125)."""
-    widths = np.asarray(widths, dtype=np.float64)
-    partner = np.roll(widths, -1) if periodic else np.concatenate((widths[1:], widths[-1:]))
-    return (widths / (widths + partner)).astype(DTYPE), (partner / (widths + partner)).astype(DTYPE)
 
 
 class CPMLLayers3D:

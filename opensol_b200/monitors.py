@@ -55,11 +55,14 @@ def dft_phase_table(omega, times, dt_m):
 
 
 class FluxMonitor:
-    """Spectral Poynting flux through the hi face of a line of cells (physics/em/monitors.py:325-379, polarisation
-    'ez'): axis = the monitor's normal ('x': a line of constant x-cell `position`, E_z and H_y; 'y': E_z and H_x), > 0
-    toward +axis.  The spectra are read from the engine's device sums when flux() is called."""
+    """Spectral Poynting flux through the hi face of a line of cells (physics/em/monitors.py:325-379): axis = the
+    monitor's normal ('x': a line of constant x-cell `position`; 'y': of constant y-cell), > 0 toward +axis.  E_z with
+    H_y / H_x for polarisation 'ez'; E_y / E_x on the hi faces with H_z for 'hz'.  The spectra are read from the
+    engine's device sums when flux() is called."""
 
-    def __init__(self, axis, position, span, frequencies, dt, cell_widths):
+    def __init__(self, axis, position, span, frequencies, dt, cell_widths, polarization='ez'):
+        if polarization not in ('ez', 'hz'):
+            raise ValueError(f"FluxMonitor polarization must be 'ez' or 'hz', got {polarization!r}")
         if axis not in ('x', 'y'):
             raise ValueError(f"FluxMonitor axis must be 'x' or 'y', got {axis!r}")
         span = (int(span[0]), int(span[1]))
@@ -74,7 +77,9 @@ class FluxMonitor:
         self.frequencies = check_frequencies(frequencies)
         self.dt = float(dt)
         self.n_freqs = len(self.frequencies)
-        self._flux_sign = -1.0 if axis == 'x' else 1.0
+        self.polarization = polarization
+        # ez: S_x = -E_z H_y, S_y = +E_z H_x; hz: S_x = +E_y H_z, S_y = -E_x H_z (monitors.py:350-362)
+        self._flux_sign = (-1.0 if axis == 'x' else 1.0) if polarization == 'ez' else (1.0 if axis == 'x' else -1.0)
         self._cell_widths = cell_widths[span[0]:span[1]].copy()
         self.sample_interval = 1
         self._reader = None   # () -> (e_spectra, h_spectra) complex128 (nf, n), set by the engine

@@ -1,7 +1,8 @@
 """EMPhysics on the B200 engine: open_sol's 2D FDTD physics (open_sol/physics/em/__init__.py:63) with the same
-constructor, PhysicsSolver contract, material helpers, sources and monitors, stepping FDTDEngine2D_Ez on the device.
+constructor, PhysicsSolver contract, material helpers, sources and monitors, stepping its engine on the device.
 
-Only the E_z polarisation with single-precision fields is built; 'hz' and precision='double' raise.  Setup follows
+Both polarisations step float32 fields: 'ez' (E_z, H_x, H_y on FDTDEngine2D_Ez) and 'hz' (H_z, E_x, E_y on
+FDTDEngine2D_Hz, face-averaged eps_xx / eps_yy); precision='double' raises.  Setup follows
 the reference's finalize order (physics/em/__init__.py:181-203): coefficients, Courant check, source calibration,
 DFT sample interval.  ``advance_ticks`` lets MultiphysicsRunner hand whole chunks to the device
 (coupling/runner.py:97-101,183-186).
@@ -12,16 +13,16 @@ import math
 
 import numpy as np
 
-from .boundaries import BoundaryConfig
+from .boundaries import BoundaryConfig, inverse_spacings
 from .constants import C0, DTYPE
-from .engine2d import FDTDEngine2D_Ez
+from .engine2d import FDTDEngine2D_Ez, FDTDEngine2D_Hz
 from .monitors import FluxMonitor, dft_sample_interval, resolve_frequencies
-from .sources import (LineSource, calibrate_line_source, carrier_angular_frequency, make_temporal,
-                      resolve_frequency)
+from .sources import (LineSource, calibrate_line_source, calibrate_tangential_sheet, carrier_angular_frequency,
+                      make_temporal, resolve_frequency)
 
 
 class EMPhysics:
-    """2D FDTD physics of a Domain, polarisation 'ez' (E_z, H_x, H_y), on one B200."""
+    """2D FDTD physics of a Domain, polarisation 'ez' (E_z, H_x, H_y) or 'hz' (H_z, E_x, E_y), on one B200."""
 
     name = 'em'
     coordinate_grids = ('cartesian',)
@@ -34,8 +35,6 @@ class EMPhysics:
         if precision not in ('single', 'double'):
             raise ValueError(f"EMPhysics precision must be 'single' (float32 fields) or 'double' (float64), got "
                              f"{precision!r}")
-        if polarization != 'ez':
-            raise NotImplementedError("the B200 2D engine steps the 'ez' polarisation")
         if precision != 'single':
             raise NotImplementedError('the B200 engine steps float32 fields (stepper precision single)')
         self.domain = domain
@@ -49,7 +48,15 @@ class EMPhysics:
             raise ValueError(f"boundary_config PML cells {bc.npml_sides} do not match the domain padding "
                              f"{domain.npml_sides}; build the Domain with the same boundary_config")
         self.boundary_config = bc
-        self.engine = FDTDEngine2D_Ez(domain, bc, device=device)
+        if polarization == 'hz':
+            # eps_xx / eps_yy start from eps_r (register_em_arrays, physics/em/materials.py:27-35)
+            materials = domain.materials
+            for name in ('eps_xx', 'eps_yy'):
+                if materials.get(name) is None:
+                    np.copyto(materials.array(name), materials.array('eps_r'))
+            self.engine = FDTDEngine2D_Hz(domain, bc, device=device)
+        else:
+            self.engine = FDTDEngine2D_Ez(domain, bc, device=device)
         self.sources = []
         self.monitors = []
         self._calibrations = []       # (source, omega, normal width)
@@ -60,7 +67,8 @@ class EMPhysics:
 
     @property
     def permittivity_arrays(self):
-        return ('eps_r',)
+        """MaterialGrid permittivity arrays the engine reads (physics/em/__init__.py:154-156)."""
+        return ('eps_r',) if self.polarization == 'ez' else ('eps_xx', 'eps_yy')
 
     # --- PhysicsSolver contract ------------------------------------------------------------------------
     def prepare(self, domain):
@@ -116,7 +124,7 @@ class EMPhysics:
     def materials_changed(self, names) -> None:
         """Materials were rewritten: the device coefficients follow at the next step (the engine tracks the
         MaterialGrid version) and the sources recalibrate (physics/em/__init__.py:205-209)."""
-        if frozenset(names) & {'eps_r', 'sigma_e', 'mu_r', 'sigma_m'}:
+        if frozenset(names) & {'eps_r', 'eps_xx', 'eps_yy', 'sigma_e', 'mu_r', 'sigma_m'}:
             self._calibration_dirty = True
 
     def renderer(self):
@@ -132,7 +140,10 @@ class EMPhysics:
         required_x = (light / dx_cells ** 2).astype(DTYPE)
         required_y = (light / dy_cells ** 2).astype(DTYPE)
         materials = self.domain.materials
-        eps = materials.array('eps_r')
+        if self.polarization == 'ez':
+            eps = materials.array('eps_r')
+        else:
+            eps = np.minimum(materials.array('eps_xx'), materials.array('eps_yy'))
         mu = materials.get('mu_r')
         # uniform grid: the requirement is one value; the worst cell is the smallest eps mu
         requirement = required_x[0] + required_y[0]
@@ -149,9 +160,16 @@ class EMPhysics:
                          f'unstable; lower courant_factor to <= {stable:.3f}, or raise eps_r / mu_r')
 
     def _calibrate_sources(self):
+        dt = float(self.domain.grid.dt)
         for source, omega, width in self._calibrations:
-            source.profile = calibrate_line_source(source, self.domain.materials, omega, width,
-                                                   float(self.domain.grid.dt))
+            if self.polarization == 'ez':
+                source.profile = calibrate_line_source(source, self.domain.materials, omega, width, dt)
+            else:
+                normal = 1 if source.axis == 'x' else 0
+                source.profile = calibrate_tangential_sheet(
+                    source, self.domain.materials, omega, width, dt,
+                    self.engine.shares_y if normal == 1 else self.engine.shares_x,
+                    self.domain.kernel_widths()[normal])
         self._calibration_dirty = False
 
     # --- material helpers --------------------------------------------------------------------------------
@@ -162,8 +180,11 @@ class EMPhysics:
         self._set_dielectric(self.domain.circle_mask(cx, cy, radius), eps_r, sigma_e)
 
     def _set_dielectric(self, mask, eps_r, sigma_e):
-        self.domain.materials.set_mask(mask, eps_r=eps_r, sigma_e=sigma_e)
-        self.materials_changed(('eps_r', 'sigma_e'))
+        """Isotropic eps_r into every permittivity array of this polarisation, plus sigma_e
+        (physics/em/__init__.py:323-327)."""
+        permittivity = {name: eps_r for name in self.permittivity_arrays}
+        self.domain.materials.set_mask(mask, sigma_e=sigma_e, **permittivity)
+        self.materials_changed(self.permittivity_arrays + ('sigma_e',))
 
     # --- sources ----------------------------------------------------------------------------------------
     def add_line_source(self, axis, position, wavelength=None, frequency=None, bandwidth=0.5, amplitude=1.0,
@@ -182,6 +203,15 @@ class EMPhysics:
             line_cell, along_cell, n_along = d.pos_to_cell_x(position), d.pos_to_cell_y, d.grid.ny
         along_axis = 0 if axis == 'x' else 1
         normal_width = float(d.cell_widths()[1 - along_axis][line_cell])
+        if self.polarization == 'hz':
+            # on the hi face of the line cell: w_perp = the dual spacing there (placement.py:254-265)
+            periodic = self.boundary_config.periodic_y if axis == 'x' else self.boundary_config.periodic_x
+            n_cells = d.grid.ny if axis == 'x' else d.grid.nx
+            if line_cell == n_cells - 1 and not periodic:
+                raise ValueError(f"Line source: the H_z sheet sits on the hi face of cell {line_cell}, the outer grid "
+                                 f"wall; move the line at least one cell inside")
+            _, inv_face = inverse_spacings(d.kernel_widths()[1 - along_axis])
+            normal_width = 1.0 / float(inv_face[line_cell])
         if span is None:
             lo, hi = 0, n_along
         else:
@@ -228,7 +258,7 @@ class EMPhysics:
         else:
             raise ValueError(f"Flux monitor axis (along the line) must be 'x' or 'y', got {axis!r}")
         monitor = FluxMonitor(normal, line_cell, cells, resolve_frequencies(wavelengths, frequencies),
-                              float(d.grid.dt), widths)
+                              float(d.grid.dt), widths, polarization=self.polarization)
         self.monitors.append(monitor)
         self.engine.attach_flux_monitor(monitor)
         return monitor

@@ -171,3 +171,37 @@ def calibrate_line_source(source, materials, omega, normal_width, dt):
     admittance = sheet_admittance(line_eps, cells('mu_r'), cells('sigma_m'), omega, normal_width, dt)
     weight = np.asarray(2.0 * np.ones(hi - lo) / (float(ETA0) * normal_width), dtype=DTYPE)
     return (cb_line * admittance * weight).astype(DTYPE)
+
+
+def calibrate_tangential_sheet(source, materials, omega, normal_spacing, dt, shares, normal_widths):
+    """float32 profile of an H_z in-plane sheet current on the hi faces of its line cells (SheetCurrentCalibration.apply
+    for a TangentialSheetCurrentSource, physics/em/sources.py:582-602): cb of the E_x (axis 'x') / E_y (axis 'y') faces
+    * admittance of the width-weighted face permittivity * 2 / (eta0 w_perp).  `shares` = the (lower, upper) face
+    weights and `normal_widths` the kernel cell widths of the axis across the line."""
+    lo, hi = source.span
+    n = len(normal_widths)
+    lower_row, upper_row = source.position, (source.position + 1) % n
+    eps_name = 'eps_xx' if source.axis == 'x' else 'eps_yy'
+
+    def row(name, r):
+        arr = materials.get(name)
+        if arr is None:
+            return np.full(hi - lo, DTYPE(materials.DEFAULTS[name]), dtype=DTYPE)
+        return np.ascontiguousarray(arr[lo:hi, r] if source.axis == 'x' else arr[r, lo:hi])
+
+    # the faces' ca / cb (fdtd_hz_2d_kernels.py:254-274): face value = lower cell * lower share + upper cell * upper
+    lower, upper = shares[0][source.position], shares[1][source.position]
+    eps_face = row(eps_name, lower_row) * lower + row(eps_name, upper_row) * upper
+    sigma_face = row('sigma_e', lower_row) * lower + row('sigma_e', upper_row) * upper
+    _, cb_line = e_coefficients_host(eps_face, sigma_face, dt)
+
+    def row_permittivity(r):
+        return (row(eps_name, r).astype(np.complex128)
+                - 1j * row('sigma_e', r).astype(np.float64) / (omega * EPS0))
+
+    w_lo, w_hi = float(normal_widths[lower_row]), float(normal_widths[upper_row])
+    line_eps = (row_permittivity(lower_row) * w_lo + row_permittivity(upper_row) * w_hi) / (w_lo + w_hi)
+    admittance = sheet_admittance(line_eps, row('mu_r', source.position), row('sigma_m', source.position), omega,
+                                  normal_spacing, dt)
+    weight = np.asarray(2.0 * np.ones(hi - lo) / (float(ETA0) * normal_spacing), dtype=DTYPE)
+    return (cb_line * admittance * weight).astype(DTYPE)

@@ -1,0 +1,197 @@
+"""GPU parity of the 2D H_z engine (the CUDA path through the C ABI) against open_sol's own outputs and the oracle.
+
+The engine evaluates every cell in the reference's order without fused multiply-add, so these tests assert
+bit-identical H_z / E_x / E_y (array_equal, and the SHA-256 digests of open_sol's own fields in tests/golden),
+bit-identical complex128 spectra and fluxes, for both kernel sets (the fused step kernel, variant 1, in its lossless
+one-word-per-cell form and in its coefficient-array form; the per-half-step kernels, variant 0) and for row runs
+per CTA from 1 row up.
+"""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from cases import apply_ops
+from cases_hz import HZ_CASES
+from oracle.hz2d import OracleHz2D
+
+import opensol_b200 as ob
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), 'golden')
+
+
+def _digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def _fields(sim):
+    return {n: sim.em.engine.read_field(n) for n in ('hz', 'ex', 'ey')}
+
+
+def _oracle_kwargs(spec):
+    return {k: v for k, v in spec['sim'].items() if k != 'polarization'}
+
+
+# (variant, rows per CTA): the per-half-step kernels, and the fused kernel with the per-grid choice and with runs of
+# 1, 2, 7 and 64 rows (ragged last runs, halo rows on every run)
+HZ_CONFIGS = [(0, 0), (1, 0), (1, 1), (1, 2), (1, 7), (1, 64)]
+
+
+@pytest.mark.parametrize('config', HZ_CONFIGS, ids=[f'v{v}_rows{r}' for v, r in HZ_CONFIGS])
+@pytest.mark.parametrize('spec', HZ_CASES, ids=[c['name'] for c in HZ_CASES])
+def test_hz_cases_bit_exact_against_reference_fixtures(spec, config):
+    g = np.load(os.path.join(GOLDEN, f"{spec['name']}.npz"))
+    sim = ob.Simulation(**spec['sim'], verbose=False)
+    mons = apply_ops(sim, spec)
+    sim.em.engine.configure(variant=config[0], steps_per_launch=1, tile_rows=config[1])
+    done = 0
+    for cp in spec['checkpoints']:
+        sim.run(n_steps=cp - done, verbose=False)
+        done = cp
+        for name, arr in _fields(sim).items():
+            assert _digest(arr) == str(g[f'sha_{name}_{cp}']), f'{name} differs from open_sol at step {cp}'
+        for k, mon in enumerate(mons):
+            e, h = mon.spectra()
+            np.testing.assert_array_equal(e, g[f'spec_e{k}_{cp}'])
+            np.testing.assert_array_equal(h, g[f'spec_h{k}_{cp}'])
+            np.testing.assert_array_equal(mon.flux(), g[f'flux{k}_{cp}'])
+
+
+def test_hz_forms_and_face_coefficients():
+    """The lossy case runs the coefficient form, the lossless ones the one-word form; the device face coefficients
+    equal open_sol's ca_x / cb_x / ca_y / cb_y bit for bit."""
+    for spec in HZ_CASES:
+        g = np.load(os.path.join(GOLDEN, f"{spec['name']}.npz"))
+        sim = ob.Simulation(**spec['sim'], verbose=False)
+        apply_ops(sim, spec)
+        sim.em.finalize()
+        eng = sim.em.engine
+        lossy = any(op[2].get('sigma_e') for op in spec['ops'] if op[0].startswith('add_dielectric'))
+        assert eng.lossless_form() == (not lossy)
+        cb_x, cb_y = eng.read_cb()
+        np.testing.assert_array_equal(cb_x, g['cb_x'])
+        np.testing.assert_array_equal(cb_y, g['cb_y'])
+
+
+def _random_spec(seed):
+    rng = np.random.default_rng(1000 + seed)
+    dx = float(rng.choice([15e-9, 20e-9, 25e-9]))
+    boundaries = str(rng.choice(['pml', 'periodic_x', 'periodic_y', 'periodic']))
+    npml = int(rng.integers(4, 13))
+    # up to 300 cells a side: several 128-column strips, ragged last strips and exact multiples of 128
+    nx_win = int(rng.choice([int(rng.integers(6, 97)), int(rng.integers(100, 301)), 256 - 2 * npml, 256]))
+    ny_win = int(rng.choice([int(rng.integers(6, 97)), int(rng.integers(100, 301)), 128 - 2 * npml, 256]))
+    size_x, size_y = nx_win * dx, ny_win * dx
+    lossy = rng.random() < 0.4
+    ops = []
+    for _ in range(int(rng.integers(0, 6))):
+        sigma = float(rng.choice([0.0, 2e4])) if lossy else 0.0
+        if rng.random() < 0.5:
+            ops.append(['add_dielectric_circle', [float(rng.uniform(0, size_x)), float(rng.uniform(0, size_y)),
+                                                  float(rng.uniform(0, 0.4 * max(size_x, size_y)))],
+                        {'eps_r': float(rng.uniform(1, 12)), 'sigma_e': sigma}])
+        else:
+            xs, ys = sorted(rng.uniform(0, size_x, 2).tolist()), sorted(rng.uniform(0, size_y, 2).tolist())
+            ops.append(['add_dielectric_rectangle', [xs[0], ys[0], xs[1], ys[1]],
+                        {'eps_r': float(rng.uniform(1, 12)), 'sigma_e': sigma}])
+    for _ in range(int(rng.integers(1, 4))):
+        axis = str(rng.choice(['x', 'y']))
+        pos = float(rng.uniform(0, size_y if axis == 'x' else size_x))
+        length = size_x if axis == 'x' else size_y
+        span = None if rng.random() < 0.4 else sorted(rng.uniform(0, length, 2).tolist())
+        ops.append(['add_line_source', [axis, pos], {'wavelength': float(rng.uniform(400e-9, 1600e-9)),
+                                                     'bandwidth': float(rng.uniform(0.3, 0.9)),
+                                                     'amplitude': float(rng.uniform(0.5, 3.0)), 'span': span}])
+    for _ in range(int(rng.integers(0, 3))):
+        axis = str(rng.choice(['x', 'y']))
+        pos = float(rng.uniform(0, size_y if axis == 'x' else size_x))
+        length = size_x if axis == 'x' else size_y
+        span = sorted(rng.uniform(0, length, 2).tolist())
+        ops.append(['add_flux_monitor', [axis, pos, span],
+                    {'wavelengths': rng.uniform(400e-9, 1600e-9, int(rng.integers(1, 5))).tolist()}])
+    rows = int(rng.choice([0, 1, 3, 16, 100]))
+    return {'sim': {'size_x': size_x, 'size_y': size_y, 'dx': dx, 'npml': npml, 'boundaries': boundaries},
+            'ops': ops, 'steps': int(rng.integers(1, 200)), 'rows': rows, 'variant': int(rng.random() < 0.8)}
+
+
+@pytest.mark.parametrize('seed', range(24))
+def test_hz_random_geometries_bit_exact(seed):
+    """Every boundary preset, grids from the 2 npml + 2 minimum to 300+ cells (several column strips, ragged and
+    exact multiples of the strip), lossless and lossy, 1-3 sheets (spans cut to the CPML), 0-2 flux lines, 1-199
+    steps in two chunks, variant 0 or the fused kernel with various row runs."""
+    spec = _random_spec(seed)
+    sim = ob.Simulation(**spec['sim'], polarization='hz', verbose=False)
+    mons = apply_ops(sim, spec)
+    sim.em.engine.configure(variant=spec['variant'], steps_per_launch=1, tile_rows=spec['rows'])
+    o = OracleHz2D(**spec['sim'])
+    omons = apply_ops(o, spec)
+    first = spec['steps'] // 3
+    for n in (first, spec['steps'] - first):
+        sim.run(n_steps=n, verbose=False)
+        o.run(n_steps=n)
+    for name, arr in _fields(sim).items():
+        np.testing.assert_array_equal(arr, getattr(o, name), err_msg=name)
+    for mon, omon in zip(mons, omons):
+        e, h = mon.spectra()
+        np.testing.assert_array_equal(e, omon.e_acc)
+        np.testing.assert_array_equal(h, omon.h_acc)
+        np.testing.assert_array_equal(mon.flux(), omon.flux())
+
+
+def test_hz_magnetic_cells_take_the_coefficient_form():
+    """mu_r != 1 on a box: per-cell da / db (coefficient form), against the oracle."""
+    args = {'size_x': 2.0e-6, 'size_y': 3.5e-6, 'dx': 25e-9, 'npml': 10, 'boundaries': 'pml'}
+    spec = {'ops': [['add_dielectric_circle', [1.0e-6, 1.5e-6, 0.4e-6], {'eps_r': 5.0}],
+                    ['add_line_source', ['y', 0.4e-6], {'wavelength': 800e-9}],
+                    ['add_flux_monitor', ['y', 1.6e-6, [0.2e-6, 3.3e-6]], {'wavelengths': [700e-9, 900e-9]}]]}
+    sim = ob.Simulation(**args, polarization='hz', verbose=False)
+    mons = apply_ops(sim, spec)
+    o = OracleHz2D(**args)
+    omons = apply_ops(o, spec)
+    box = (slice(50, 70), slice(60, 120))
+    sim.domain.materials.array('mu_r')[box] = np.float32(2.5)
+    sim.domain.materials.version += 1
+    sim.em.materials_changed(('mu_r',))
+    o.mu_r[box] = np.float32(2.5)
+    sim.run(n_steps=300, verbose=False)
+    o.run(n_steps=300)
+    assert not sim.em.engine.lossless_form()
+    for name, arr in _fields(sim).items():
+        np.testing.assert_array_equal(arr, getattr(o, name), err_msg=name)
+    np.testing.assert_array_equal(mons[0].flux(), omons[0].flux())
+
+
+def test_hz_variants_agree_and_reset():
+    spec = HZ_CASES[0]
+    results = []
+    for variant in (0, 1):
+        sim = ob.Simulation(**spec['sim'], verbose=False)
+        mons = apply_ops(sim, spec)
+        sim.em.engine.configure(variant=variant, steps_per_launch=1, tile_rows=0)
+        for n in (1, 9, 90):
+            sim.run(n_steps=n, verbose=False)
+        results.append((_fields(sim), mons[0].spectra()))
+        sim.em.engine.reset()
+        sim.em.engine.advance(100)
+        again = _fields(sim)
+        for name in again:
+            np.testing.assert_array_equal(again[name], results[-1][0][name])
+    for name in results[0][0]:
+        np.testing.assert_array_equal(results[0][0][name], results[1][0][name])
+    np.testing.assert_array_equal(results[0][1][0], results[1][1][0])
+
+
+def test_hz_field_write_read_roundtrip_and_launch_count():
+    sim = ob.Simulation(1e-6, 0.5e-6, 25e-9, npml=8, polarization='hz', verbose=False)
+    sim.add_flux_monitor('y', 0.5e-6, (0.1e-6, 0.4e-6), wavelengths=[700e-9])
+    sim.add_line_source('x', 0.2e-6, wavelength=700e-9)
+    sim.em.finalize()
+    rng = np.random.default_rng(3)
+    values = rng.standard_normal((sim.grid.nx, sim.grid.ny)).astype(np.float32)
+    sim.em.engine.write_field('ex', values)
+    np.testing.assert_array_equal(sim.em.engine.read_field('ex'), values)
+    sim.em.engine.advance(12)
+    m = sim.em.engine.sample_interval
+    assert sim.em.engine.launch_count() == 12 + 12 // m
