@@ -50,9 +50,11 @@ def parse_args():
     p.add_argument('--variant', type=int, default=1, help='1: temporally blocked kernels (default), 0: per step')
     p.add_argument('--steps-per-launch', type=int, default=3)
     p.add_argument('--tile-rows', type=int, default=0, help='rows per interior tile (0: autotune)')
-    p.add_argument('--workload', default='roofline_2d', choices=['roofline_2d', 'em3d', 'serving', 'adjoint'],
-                   help='roofline_2d: the headline 8192^2 2D run; em3d: the 512^3 3D run; serving: the batched job '
-                        'stream against one-at-a-time runs; adjoint: gradient cost against one forward run')
+    p.add_argument('--workload', default='roofline_2d',
+                   choices=['roofline_2d', 'hz2d', 'em3d', 'serving', 'adjoint'],
+                   help='roofline_2d: the headline 8192^2 2D run; hz2d: the same grid in the H_z polarisation; '
+                        'em3d: the 512^3 3D run; serving: the batched job stream against one-at-a-time runs; '
+                        'adjoint: gradient cost against one forward run')
     p.add_argument('--jobs', type=int, default=64, help='serving: jobs of the request stream')
     return p.parse_args()
 
@@ -340,6 +342,101 @@ def run_e2e(args, device, world, barrier, reduce_max):
             'timing': 'host wall clock around Simulation.run + flux(), synchronized, max over ranks'}
 
 
+def run_hz2d(args):
+    """The roofline_2d geometry in the H_z polarisation (H_z, E_x, E_y; the same 2000 cylinders, line source and
+    four flux lines): cell-updates/s over the total grid, one bench step = one whole simulation of args.sim_steps Yee
+    steps from rest, device time with CUDA events on the engine's stream.  Roofline: the 28 algorithmic bytes per
+    cell-update (3 fields read + written, one eps word) over the fused step kernel's mean launch time."""
+    import torch
+    import opensol_b200 as ob
+    from opensol_b200 import workloads
+    torch.cuda.set_device(0)
+    sim = ob.Simulation(**workloads.roofline_2d_sim_args(total_cells=args.grid), polarization='hz', verbose=False)
+    monitors = workloads.apply(sim, workloads.roofline_2d_ops(total_cells=args.grid))
+    variant = args.variant if args.variant in (0, 1) else 1
+    sim.em.engine.configure(variant=variant, steps_per_launch=1, tile_rows=args.tile_rows)
+    sim.em.finalize()
+    engine = sim.em.engine
+    stream = torch.cuda.current_stream()
+    engine.set_stream(stream.cuda_stream)
+    tables = engine.chunk_tables(args.sim_steps)
+    for _ in range(args.warmup):
+        engine.reset()
+        engine.advance(args.sim_steps, tables)
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    with ClockSampler(0) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            engine.reset()
+            engine.advance(args.sim_steps, tables)
+            launches += engine.launch_count()
+        stop.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(stop)
+    cells = engine.nx * engine.ny
+    value = cells * args.sim_steps * args.steps / (ms / 1e3) / 1e9
+    flux = [m.flux() for m in monitors]
+    if args.sim_steps >= 2000:
+        assert any(float(abs(f).max()) > 0 for f in flux), 'every flux is zero: the run did no work'
+    engine.set_profiling(True)
+    engine.reset()
+    engine.advance(args.sim_steps, tables)
+    times = engine.kernel_times()
+    engine.set_profiling(False)
+    name = engine.KERNEL_KINDS[3]
+    total_ms, n_launch = times[name]
+    launch_ms = total_ms / n_launch
+    peak, peak_kind = measured_peak_hbm()
+    achieved = BYTES_PER_CELL_UPDATE * cells / (launch_ms / 1e3) / 1e9
+    roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
+                'traffic': None, 'peak_source': f'{peak_kind} hbm_gbs (copy bandwidth)', 'kernel': name,
+                'bytes_per_cell_update': BYTES_PER_CELL_UPDATE, 'cell_updates_per_launch': cells,
+                'launch_ms': launch_ms, 'lossless_form': engine.lossless_form(),
+                'kernel_share': {k: v[0] / sum(t[0] for t in times.values()) for k, v in times.items()}}
+    traffic_path = os.path.join(ROOT, 'profiles', 'traffic.json')
+    if os.path.exists(traffic_path):
+        with open(traffic_path) as f:
+            t = json.load(f).get('hz2d_step_kernel')
+        if t:
+            roofline['traffic'] = t['dram_bytes_per_cell_update'] * cells
+            roofline['traffic_note'] = t['note']
+    line = {'metric': 'FDTD Gcell-updates/s (2D H_z)', 'value': value, 'unit': 'Gcell-updates/s', 'n_gpus': 1,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms / args.steps, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': f'hz2d: 2D H_z FDTD, {args.grid}x{args.grid} total grid incl. 20 CPML cells/side, '
+                                   'dx 20 nm, 2000 seeded cylinders eps_r U(2,12), 1550 nm E_y sheet source, '
+                                   f'4 x 16-frequency flux lines, {args.sim_steps} Yee steps per bench step',
+                       'grid': [args.grid, args.grid], 'sim_steps': args.sim_steps,
+                       'kernel': {'variant': engine.variant, 'rows_per_cta': engine.tile_rows},
+                       'l2': 'inputs larger than L2 (fields 3 x 268 MB), no flush'},
+            'roofline': roofline, 'gpu_launches': launches, 'clocks': clocks.summary()}
+    sim.clear()
+    if not args.no_cpu_baseline and args.grid == 8192:
+        line['cpu_baseline'] = cpu_baseline_hz()
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_hz(sample_steps=CPU_SAMPLE_STEPS):
+    """The H_z oracle (C + OpenMP restatement of open_sol's H_z step) on the same 8192^2 grid: a bounded sample of
+    sample_steps Yee steps after a 2-step warm-up."""
+    from oracle.hz2d import OracleHz2D
+    from opensol_b200 import workloads
+    subprocess.run(['make', '-s', '-C', os.path.join(ROOT, 'oracle')], check=True)
+    o = OracleHz2D(**workloads.roofline_2d_sim_args())
+    workloads.apply(o, workloads.roofline_2d_ops())
+    o.finalize()
+    o.run(n_steps=2)
+    t0 = time.perf_counter()
+    o.run(n_steps=sample_steps)
+    wall = time.perf_counter() - t0
+    cells = o.domain.nx * o.domain.ny
+    return {'value': cells * sample_steps / wall / 1e9, 'unit': 'Gcell-updates/s', 'cores': os.cpu_count(),
+            'kind': 'port', 'sample': f'{sample_steps} H_z Yee steps of the 8192x8192 grid after 2 warm-up steps, '
+                                      f'C restatement with OpenMP on {os.cpu_count()} threads', 'wall_s': wall}
+
+
 def run_em3d(args):
     """The 512^3 3D workload (opensol_b200/workloads.py roofline_3d_physics): cell-updates/s over the total grid, one
     bench step = args.sim_steps Yee steps from rest (2000 when left at the 2D default)."""
@@ -474,6 +571,8 @@ def main():
         return
     if args.workload == 'em3d':
         run_em3d(args)
+    elif args.workload == 'hz2d':
+        run_hz2d(args)
     elif args.workload == 'serving':
         run_serving(args)
     elif args.workload == 'adjoint':

@@ -93,8 +93,9 @@ int os_fdtd2d_read_cb(OsFdtd2D *h, float *cb);
  * (axis 1, the hi-x faces of x-cell `position`) after the E update (TangentialSheetCurrentSource,
  * physics/em/sources.py:469-480); a flux line samples E_y (normal 0) or E_x (normal 1) with H_z
  * (FluxMonitor 'hz', physics/em/monitors.py:350-362); field components are OS_HZ_HZ / OS_HZ_EX / OS_HZ_EY.
- * os_fdtd2d_configure takes variant 1 (default: one fused kernel per step, tile_rows rows per CTA, 0 = chosen per
- * grid) or 0 (one H_z and one E kernel per step) with steps_per_launch 1.  The E_z-only calls (set_materials,
+ * os_fdtd2d_configure takes variant 1 (default: per step an interior kernel over the box of plain cells, tile_rows
+ * rows per CTA, 0 = chosen per grid, and a border kernel over the rest) or 0 (one H_z and one E kernel per step) with
+ * steps_per_launch 1.  The E_z-only calls (set_materials,
  * set_coefficients, read_cb, autotune, plan_info, batch, adjoint) return OS_ERR_STATE on an H_z handle and the
  * H_z-only calls below on an E_z handle.
  * ---------------------------------------------------------------------------------------------------------------- */

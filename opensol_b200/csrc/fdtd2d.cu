@@ -914,14 +914,89 @@ static Hz2DParams make_hz_params(const OsFdtd2D *h, int in, int out) {
     return p;
 }
 
-// Rows per CTA of the fused H_z step: enough CTAs for several waves on the device's SMs, 16..256 rows.
-static int hz_rows_per_cta(const OsFdtd2D *h) {
+// The fused H_z step's split: the interior box (every H_z / E_x / E_y update plain, columns in groups of 4) and the
+// border rectangles around it.
+struct HzPlan {
+    bool interior = false;
+    int ia = 0, ib = 0, jc0 = 0, jc1 = 0;
+    HzBorderRects rects{};
+};
+
+static HzPlan hz_plan(const OsFdtd2D *h) {
+    HzPlan q;
+    const int nx = h->grid.nx, ny = h->grid.ny, npml = h->grid.npml, sides = h->grid.cpml_sides;
+    // rows [ia, ib) own, row ib the halo: no CPML row among H_z rows ia..ib and E_y rows ia..ib-1, no grid edge
+    q.ia = (sides & 1) ? npml + 1 : 1;
+    q.ib = (sides & 2) ? nx - npml - 2 : nx - 2;
+    int c0 = (sides & 4) ? npml + 1 : 1;
+    c0 = (c0 + 3) / 4 * 4;
+    const int cmax = (sides & 8) ? ny - npml - 2 : ny - 2;   // the halo column jc1 <= cmax
+    q.jc0 = c0;
+    q.jc1 = cmax > c0 ? c0 + (cmax - c0) / 4 * 4 : c0;
+    q.interior = q.ib > q.ia && q.jc1 > q.jc0;
+    int n = 0;
+    auto add = [&](int r0, int r1, int cc0, int cc1) {
+        if (r1 <= r0 || cc1 <= cc0) return;
+        q.rects.r0[n] = r0, q.rects.r1[n] = r1, q.rects.c0[n] = cc0, q.rects.c1[n] = cc1;
+        ++n;
+    };
+    if (q.interior) {
+        add(0, q.ia, 0, ny);
+        add(q.ib, nx, 0, ny);
+        add(q.ia, q.ib, 0, q.jc0);
+        add(q.ia, q.ib, q.jc1, ny);
+    } else {
+        add(0, nx, 0, ny);
+    }
+    q.rects.n = n;
+    q.rects.first[0] = 0;
+    for (int k = 0; k < n; ++k)
+        q.rects.first[k + 1] =
+            q.rects.first[k] + (int64_t)(q.rects.r1[k] - q.rects.r0[k]) * (q.rects.c1[k] - q.rects.c0[k]);
+    return q;
+}
+
+// Rows per CTA of the interior kernel: about four waves of CTAs over the device's resident slots, 8..64 rows.
+static int hz_rows_per_cta(const OsFdtd2D *h, const HzPlan &q) {
     if (h->hz_rows > 0) return h->hz_rows;
-    const int64_t strips = (h->grid.ny + HZ_STRIP - 1) / HZ_STRIP;
-    const int64_t want_ctas = (int64_t)h->sm_count * 8;
-    int64_t rows = (int64_t)h->grid.nx * strips / want_ctas;
-    rows = std::max<int64_t>(16, std::min<int64_t>(256, rows));
+    const int64_t warps = (q.jc1 - q.jc0 + 127) / 128;
+    const int64_t ctas_x = (warps + HZ_THREADS / 32 - 1) / (HZ_THREADS / 32);
+    const int64_t want_ctas = (int64_t)h->sm_count * 6 * 4;
+    int64_t rows = ((int64_t)(q.ib - q.ia) * ctas_x + want_ctas - 1) / want_ctas;
+    rows = std::max<int64_t>(8, std::min<int64_t>(64, rows));
     return (int)rows;
+}
+
+// One fused H_z step: the interior kernel (TMA-staged rows for the lossless form on a row length that keeps the
+// copies 16-byte aligned, direct loads otherwise), then the border kernel.
+static void launch_hz_step(OsFdtd2D *h, const HzPlan &q, Hz2DParams p) {
+    const bool vec = h->grid.ny % 4 == 0;
+    if (q.interior) {
+        p.ia = q.ia, p.ib = q.ib, p.jc0 = q.jc0, p.jc1 = q.jc1;
+        p.rows_per_cta = hz_rows_per_cta(h, q);
+        const int warps = (q.jc1 - q.jc0 + 127) / 128;
+        const dim3 grid((unsigned)((warps + HZ_THREADS / 32 - 1) / (HZ_THREADS / 32)),
+                        (unsigned)((q.ib - q.ia + p.rows_per_cta - 1) / p.rows_per_cta));
+        int32_t *err = h->err.ptr;
+        if (h->hz_eps && vec) {
+            hz2d_interior_kernel<true, true, true>
+                <<<grid, HZ_THREADS, (HZ_THREADS / 32) * hz_warp_smem_bytes(), h->stream>>>(p, err);
+        } else if (h->hz_eps) {
+            hz2d_interior_kernel<true, false, false><<<grid, HZ_THREADS, 0, h->stream>>>(p, err);
+        } else if (vec) {
+            hz2d_interior_kernel<false, true, false><<<grid, HZ_THREADS, 0, h->stream>>>(p, err);
+        } else {
+            hz2d_interior_kernel<false, false, false><<<grid, HZ_THREADS, 0, h->stream>>>(p, err);
+        }
+        h->launches += 1;
+    }
+    const int64_t cells = q.rects.first[q.rects.n];
+    if (cells > 0) {
+        const unsigned blocks = (unsigned)((cells + 255) / 256);
+        if (h->hz_eps) hz2d_border_kernel<true><<<blocks, 256, 0, h->stream>>>(p, q.rects);
+        else hz2d_border_kernel<false><<<blocks, 256, 0, h->stream>>>(p, q.rects);
+        h->launches += 1;
+    }
 }
 
 // H_z chunk: variant 0 launches the in-place H and E kernels per step, otherwise one fused step kernel per step
@@ -933,24 +1008,20 @@ static int advance_hz(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_
     const dim3 cell_block(EZ2D_BLOCK_X, EZ2D_BLOCK_Y);
     const dim3 cell_grid((unsigned)((ny + cell_block.x - 1) / cell_block.x),
                          (unsigned)((nx + cell_block.y - 1) / cell_block.y));
-    const int rows = hz_rows_per_cta(h);
-    const dim3 step_grid((unsigned)((ny + HZ_STRIP - 1) / HZ_STRIP), (unsigned)((nx + rows - 1) / rows));
+    const HzPlan plan = hz_plan(h);
     for (int64_t k = 0; k < n_steps; ++k) {
         const int in = h->cur, out = h->variant == 0 ? h->cur : h->cur ^ 1;
         Hz2DParams p = make_hz_params(h, in, out);
         p.line_values = values;
         p.values_stride = n_steps;
         p.k_step = k;
-        p.rows_per_cta = rows;
         OS_TRY(prof_begin(h, 3, h->stream));
         if (h->variant == 0) {
             hz2d_h_kernel<<<cell_grid, cell_block, 0, h->stream>>>(p);
             hz2d_e_kernel<<<cell_grid, cell_block, 0, h->stream>>>(p);
             h->launches += 2;
         } else {
-            if (h->hz_eps) hz2d_step_kernel<true><<<step_grid, HZ_STRIP, 0, h->stream>>>(p);
-            else hz2d_step_kernel<false><<<step_grid, HZ_STRIP, 0, h->stream>>>(p);
-            h->launches += 1;
+            launch_hz_step(h, plan, p);
         }
         OS_TRY(prof_end(h, h->stream));
         h->cur = out;

@@ -14,22 +14,24 @@
 // Two kernel sets:
 //   hz2d_h_kernel + hz2d_e_kernel: one thread per cell, one launch per half step, fields updated in place (the plain
 //        form of the arithmetic, variant 0);
-//   hz2d_step_kernel: one launch per Yee step reading one field / psi buffer set and writing the other.  A CTA owns a
-//        strip of 128 columns and a run of rows; it streams down the rows computing H_z of row i (own columns plus
-//        the one column right of the strip, from the old E only), then E_x of row i and E_y of row i - 1 from the new
-//        H_z held in shared memory and registers, so each field is read and written once per step.  The CTA also
-//        computes H_z of the row after its run (not stored) for the E_y of its last row.  With EPS (lossless, eps_xx
-//        = eps_yy, uniform permeability) the face coefficients are not stored: cb = dt / (eps_face eps0) is evaluated
-//        from one eps_r word per cell exactly as the coefficient kernel does (denominator 1 + 0 = 1), trading two
-//        divisions for 8 bytes per cell.
+//   hz2d_interior_kernel + hz2d_border_kernel (variant 1): per Yee step, both read one field / psi buffer set and
+//        write the other.  The interior kernel covers the box where every update is the plain Yee one (no CPML row,
+//        edge or wrap in reach): each warp streams a strip of 128 columns down its rows, 4 columns per lane, H_z of a
+//        row then E_x of the row and E_y of the row below from registers and warp shuffles, so each field is read
+//        and written once per step; in the lossless form (eps_xx = eps_yy, no sigma, vacuum permeability) the rows
+//        arrive by TMA bulk copies into a per-warp ring and the face cb = dt / (face eps eps0) is evaluated from one
+//        eps_r word per cell, exactly as the coefficient kernel evaluates it (denominator 1 + 0 = 1).  The border
+//        kernel updates the frame around the box one thread per cell with the per-cell functions, evaluating the
+//        two neighbouring new H_z its E_x / E_y read again from the old E.
 #pragma once
 
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "fdtd2d_kernels.cuh"
+#include "fdtd2d_tb.cuh"
 
-#define HZ_STRIP 128
+#define HZ_THREADS 128   // threads per CTA of the fused step; 4 columns each
 
 struct Hz2DParams {
     int32_t nx, ny, px, py, npml, cpml_mask;
@@ -50,6 +52,7 @@ struct Hz2DParams {
     const float *line_values;
     int64_t values_stride, k_step;
     int32_t rows_per_cta;
+    int32_t ia, ib, jc0, jc1;                 // interior box of the fused step: rows [ia, ib), columns [jc0, jc1)
 };
 
 __device__ __forceinline__ float hz_wrap_lo(float w) { return w * 1.0f - w * 0.0f; }
@@ -198,90 +201,358 @@ __device__ __forceinline__ float hz_cb_lossless(float eps_self, float eps_partne
     return dt / (face * eps0);
 }
 
-template <bool EPS>
-__global__ void __launch_bounds__(HZ_STRIP) hz2d_step_kernel(const Hz2DParams p) {
-    __shared__ float s_hz[2][HZ_STRIP + 1];
-    __shared__ float s_eps[2][HZ_STRIP + 1];
-    const int t = threadIdx.x;
-    const int j0 = blockIdx.x * HZ_STRIP;
-    const int j = j0 + t;
-    const int nx = p.nx, ny = p.ny;
-    const int r0 = blockIdx.y * p.rows_per_cta;
-    if (r0 >= nx) return;   // whole CTA
-    const int r1 = min(nx, r0 + p.rows_per_cta);
-    const bool active = j < ny;
-    const int last_t = min(HZ_STRIP - 1, ny - 1 - j0);
-    const int jh = (j0 + HZ_STRIP < ny) ? j0 + HZ_STRIP : (p.py ? 0 : -1);   // H_z column right of the strip
-    const bool halo_thread = t == last_t && jh >= 0;
-    const bool halo_row = p.px || r1 < nx;
-    const int i_end = halo_row ? r1 : r1 - 1;
-    const float lo_y = EPS && active ? p.lo_y[j] : 0.0f, up_y = EPS && active ? p.up_y[j] : 0.0f;
-    const float iyh = active ? p.iyh[j] : 0.0f;
-    (void)iyh;
+// four consecutive floats of a row (16-byte aligned when VEC)
+template <bool VEC>
+__device__ __forceinline__ void hz_ld4(const float *base, size_t idx, float (&v)[4]) {
+    if (VEC) {
+        const float4 q = __ldg(reinterpret_cast<const float4 *>(base + idx));
+        v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+    } else {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) v[c] = __ldg(base + idx + c);
+    }
+}
 
-    float hz_prev = 0.0f, ey_prev = 0.0f, eps_prev = 0.0f, ca_y_prev = 1.0f, cb_y_prev = 0.0f;
-    for (int i = r0; i <= i_end; ++i) {
-        const int r = i == nx ? 0 : i;   // physical row (i == nx only on a periodic x)
-        const bool own_row = i < r1;
-        const int b = i & 1;
-        float h_new = 0.0f, ex_c = 0.0f, ey_c = 0.0f, eps_c = 0.0f;
-        if (active) {
-            h_new = hz2d_hz_at(p, r, j, own_row, ex_c, ey_c);
-            const size_t idx = (size_t)r * ny + j;
-            if (own_row) p.hz_out[idx] = h_new;
-            if (EPS) eps_c = p.eps[idx];
-            s_hz[b][t] = h_new;
-            if (EPS) s_eps[b][t] = eps_c;
-        }
-        if (halo_thread) {
-            float ex_h, ey_h;
-            s_hz[b][t + 1] = hz2d_hz_at(p, r, jh, false, ex_h, ey_h);
-            if (EPS) s_eps[b][t + 1] = p.eps[(size_t)r * ny + jh];
-        }
-        __syncthreads();
-        if (active) {
-            const size_t idx = (size_t)r * ny + j;
-            float ca_x = 1.0f, cb_x = 0.0f, ca_y = 1.0f, cb_y = 0.0f;
-            if (own_row) {
-                // E_x of (r, j)
-                if (j < ny - 1 || p.py) {
-                    const float right = s_hz[b][t + 1];
-                    const float up = j < ny - 1 ? right : hz_wrap_hi(right);
-                    if (EPS) {
-                        cb_x = hz_cb_lossless(eps_c, s_eps[b][t + 1], lo_y, up_y, p.dt, p.eps0);
-                    } else {
-                        ca_x = p.ca_x ? p.ca_x[idx] : 1.0f;
-                        cb_x = p.cb_x[idx];
-                    }
-                    p.ex_out[idx] = hz2d_ex_at(p, r, j, ex_c, ca_x, cb_x, h_new, up);
-                } else {
-                    p.ex_out[idx] = ex_c;   // the last face of an open y is never updated
+template <bool VEC>
+__device__ __forceinline__ void hz_st4(float *base, size_t idx, const float (&v)[4]) {
+    if (VEC) {
+        *reinterpret_cast<float4 *>(base + idx) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) base[idx + c] = v[c];
+    }
+}
+
+// ---- the fused step: an interior kernel and a border kernel per Yee step, both reading one field / psi buffer set
+// and writing the other, over disjoint cells.
+//
+// The interior box (rows [ia, ib), columns [jc0, jc1), chosen by the host) holds the cells whose H_z, E_x and E_y
+// updates, and those of the H_z one row below and one column right of the box, touch no CPML row, grid edge or wrap:
+// there every cell takes the same plain expressions.  The border kernel covers the rest of the grid with the per-cell
+// functions above.
+
+// H_z of four plain cells from their old values (ex_left: E_x of the column left of the first).
+__device__ __forceinline__ void hz_plain_h(const float (&hzo)[4], const float (&exo)[4], const float (&eyo)[4],
+                                           const float (&eyp)[4], float ex_left, const float (&iye)[4], float ixe,
+                                           const float (&da)[4], const float (&db)[4], float (&hn)[4]) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float dex = exo[c] - (c == 0 ? ex_left : exo[c - 1]);
+        const float dey = eyo[c] - eyp[c];
+        float curl = dex * iye[c];
+        curl -= dey * ixe;
+        hn[c] = da[c] * hzo[c] + db[c] * curl;
+    }
+}
+
+// E_x of four plain faces and E_y of the four faces of the row below (lossless form: cb from eps; else coefficient
+// arrays), then the sheet sources crossing them (added after E in add order, skipped for a 0 value).
+template <bool EPS>
+__device__ __forceinline__ void hz_plain_e(const Hz2DParams &p, float (&vx)[4], float (&vy)[4], int r, int re, int jt,
+                                           bool do_x, bool do_y, const float (&hn)[4], const float (&exo)[4],
+                                           const float (&ep)[4], float h_next, float e_next, const float (&lo_y)[4],
+                                           const float (&up_y)[4], const float (&iyh)[4], const float (&hzp)[4],
+                                           const float (&eyp)[4], const float (&epp)[4], const float (&cax)[4],
+                                           const float (&cbx)[4], const float (&cay)[4], const float (&cby)[4]) {
+    const float ixh = do_y ? __ldg(p.ixh + re) : 0.0f;
+    const float lo_x = EPS && do_y ? __ldg(p.lo_x + re) : 0.0f, up_x = EPS && do_y ? __ldg(p.up_x + re) : 0.0f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float bx = EPS ? hz_cb_lossless(ep[c], c < 3 ? ep[c + 1] : e_next, lo_y[c], up_y[c], p.dt, p.eps0)
+                             : cbx[c];
+        const float dx = (c < 3 ? hn[c + 1] : h_next) - hn[c];
+        vx[c] = (EPS ? 1.0f : cax[c]) * exo[c] + bx * dx * iyh[c];
+        const float by = EPS ? hz_cb_lossless(epp[c], ep[c], lo_x, up_x, p.dt, p.eps0) : cby[c];
+        const float dy = hn[c] - hzp[c];
+        vy[c] = (EPS ? 1.0f : cay[c]) * eyp[c] - by * dy * ixh;
+    }
+    for (int l = 0; l < p.n_lines; ++l) {
+        const LineSrcDev &L = p.lines[l];
+        if (L.axis == 0) {   // E_x faces (i, position), i in [lo, hi)
+            if (do_x && L.position >= jt && L.position < jt + 4 && r >= L.lo && r < L.hi) {
+                const float value = p.line_values[(size_t)l * p.values_stride + p.k_step];
+                if (value != 0.0f) {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        if (jt + c == L.position) vx[c] += value * L.profile[r - L.lo];
                 }
             }
-            // E_y of (i - 1, j)
-            if (i > r0) {
-                const int re = i - 1;
-                const size_t ide = (size_t)re * ny + j;
-                if (re < nx - 1 || p.px) {
-                    const float up = re < nx - 1 ? h_new : hz_wrap_hi(h_new);
-                    if (EPS) cb_y_prev = hz_cb_lossless(eps_prev, eps_c, p.lo_x[re], p.up_x[re], p.dt, p.eps0);
-                    p.ey_out[ide] = hz2d_ey_at(p, re, j, ey_prev, ca_y_prev, cb_y_prev, hz_prev, up);
-                } else {
-                    p.ey_out[ide] = ey_prev;
-                }
+        } else if (do_y && L.position == re && jt + 3 >= L.lo && jt < L.hi) {   // E_y faces (position, j)
+            const float value = p.line_values[(size_t)l * p.values_stride + p.k_step];
+            if (value != 0.0f) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    if (jt + c >= L.lo && jt + c < L.hi) vy[c] += value * L.profile[jt + c - L.lo];
             }
-            if (!EPS && own_row) {
-                ca_y = p.ca_y ? p.ca_y[idx] : 1.0f;
-                cb_y = p.cb_y[idx];
-            }
-            hz_prev = h_new;
-            ey_prev = ey_c;
-            eps_prev = eps_c;
-            ca_y_prev = ca_y;
-            cb_y_prev = cb_y;
         }
     }
-    if (!halo_row && active) p.ey_out[(size_t)(r1 - 1) * ny + j] = ey_prev;   // the last face of an open x
+}
+
+// Row staging of the interior kernel (lossless form): lane 0 of each warp copies row windows of H_z, E_x, E_y and
+// eps_r (the strip's 128 columns plus 4 on each side, clipped to the grid) into a per-warp ring of HZ_SLOTS slots by
+// 1D bulk copies (cp.async.bulk, no multicast), HZ_AHEAD rows ahead of the row being consumed, each slot completing
+// on its own mbarrier.  The lanes read their old values, the E_x left of their first column and (the strip's last
+// lane) the halo column from shared memory.  A slot is refilled after the warp has read it (__syncwarp, then lane 0
+// orders the reads before the copy engine's writes with fence.proxy.async).  Waits are bounded (tb_mbar_wait): one
+// that runs out sets the engine's error flag, waits (bounded) for the copies still in flight and ends the warp.
+#define HZ_AHEAD 3
+#define HZ_SLOTS (HZ_AHEAD + 1)
+#define HZ_WIN 136   // floats of one staged row window: 4 + 128 + 4 columns
+__host__ __device__ constexpr int hz_warp_smem_bytes() { return HZ_SLOTS * 4 * HZ_WIN * 4 + HZ_SLOTS * 8; }
+
+struct HzStage {
+    float *ring;          // [slot][array: hz, ex, ey, eps][HZ_WIN]
+    uint64_t *bar;        // [slot]
+    int jw, c_lo, c_hi;   // window columns [c_lo, c_hi) of the grid at slot offset c_lo - (jw - 4)
+
+    __device__ __forceinline__ float *slot(int s, int a) const { return ring + (s * 4 + a) * HZ_WIN; }
+
+    // lane 0: copy row r into slot s
+    __device__ __forceinline__ void issue(const Hz2DParams &p, int r, int s) const {
+        const uint32_t bytes = (uint32_t)(c_hi - c_lo) * 4u;
+        tb_mbar_expect_tx(bar + s, 4u * bytes);
+        const size_t src = (size_t)r * p.ny + c_lo;
+        const int off = c_lo - (jw - 4);
+        tb_bulk_g2s(slot(s, 0) + off, p.hz_in + src, bytes, bar + s);
+        tb_bulk_g2s(slot(s, 1) + off, p.ex_in + src, bytes, bar + s);
+        tb_bulk_g2s(slot(s, 2) + off, p.ey_in + src, bytes, bar + s);
+        tb_bulk_g2s(slot(s, 3) + off, p.eps + src, bytes, bar + s);
+    }
+};
+
+// Interior kernel.  Each warp owns a strip of up to 128 columns of the box (lane l: columns jt .. jt + 3,
+// jt = jw + 4 l) and walks the CTA's rows r0 .. r1 - 1 plus the halo row r1, with no barrier: row i gives H_z of
+// row i from the old E (the strip's last lane also the halo column right of the strip), the next lane's first H_z /
+// eps by warp shuffle, then E_x of row i and E_y of row i - 1.  STAGED (lossless form): rows through the TMA ring;
+// otherwise 16-byte (VEC) or scalar loads from global memory.
+template <bool EPS, bool VEC, bool STAGED>
+__global__ void __launch_bounds__(HZ_THREADS, 6) hz2d_interior_kernel(const Hz2DParams p, int32_t *err) {
+    extern __shared__ __align__(16) unsigned char hz_smem[];
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int jw = p.jc0 + (blockIdx.x * (HZ_THREADS / 32) + warp) * 128;
+    if (jw >= p.jc1) return;   // whole warp (its barriers are never used)
+    const int jt = jw + 4 * lane;
+    const int ny = p.ny;
+    const int r0 = p.ia + blockIdx.y * p.rows_per_cta;
+    if (r0 >= p.ib) return;
+    const int r1 = min(p.ib, r0 + p.rows_per_cta);
+    const int j_end = min(jw + 128, p.jc1);             // the strip's columns [jw, j_end); halo column j_end
+    const bool active = jt < j_end;
+    const int last_lane = (j_end - 1 - jw) / 4;
+    const bool halo_lane = lane == last_lane;
+
+    HzStage st;
+    if constexpr (STAGED) {
+        unsigned char *mine = hz_smem + warp * hz_warp_smem_bytes();
+        st.ring = reinterpret_cast<float *>(mine);
+        st.bar = reinterpret_cast<uint64_t *>(mine + HZ_SLOTS * 4 * HZ_WIN * 4);
+        st.jw = jw;
+        st.c_lo = max(jw - 4, 0);
+        st.c_hi = min(jw + 132, ny);
+        if (lane == 0) {
+            for (int s = 0; s < HZ_SLOTS; ++s) tb_mbar_init(st.bar + s, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            tb_fence_proxy_async();
+            for (int i = r0; i <= min(r1, r0 + HZ_AHEAD); ++i) st.issue(p, i, (i - r0) % HZ_SLOTS);
+        }
+        __syncwarp();
+    }
+
+    float iye[4], iyh[4], lo_y[4], up_y[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int jc = active ? jt + c : jw;
+        iye[c] = __ldg(p.iye + jc);
+        iyh[c] = __ldg(p.iyh + jc);
+        lo_y[c] = EPS ? __ldg(p.lo_y + jc) : 0.0f;
+        up_y[c] = EPS ? __ldg(p.up_y + jc) : 0.0f;
+    }
+    const float iye_h = __ldg(p.iye + j_end);
+    float hzp[4] = {0.0f, 0.0f, 0.0f, 0.0f}, eyp[4] = {0.0f, 0.0f, 0.0f, 0.0f}, epp[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    float ey_halo_prev = 0.0f;   // old E_y of the halo column, row below
+    if (active) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) eyp[c] = __ldg(p.ey_in + (size_t)(r0 - 1) * ny + jt + c);
+    }
+    if (halo_lane) ey_halo_prev = __ldg(p.ey_in + (size_t)(r0 - 1) * ny + j_end);
+
+    for (int i = r0; i <= r1; ++i) {
+        const bool own_row = i < r1;
+        const size_t row = (size_t)i * ny;
+        float hzo[4] = {0.0f, 0.0f, 0.0f, 0.0f}, exo[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        float eyo[4] = {0.0f, 0.0f, 0.0f, 0.0f}, ep[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        float ex_left = 0.0f, hz_h = 0.0f, ex_h = 0.0f, ey_h = 0.0f, ep_h = 0.0f;
+        if constexpr (STAGED) {
+            const int k = i - r0, s = k % HZ_SLOTS;
+            if (!tb_mbar_wait(st.bar + s, (uint32_t)((k / HZ_SLOTS) & 1))) {
+                if (lane == 0) atomicExch(err, 1);
+                for (int q = i; q <= min(r1, i + HZ_AHEAD); ++q) {   // copies still in flight, this row's included
+                    const int kq = q - r0;
+                    tb_mbar_wait(st.bar + kq % HZ_SLOTS, (uint32_t)((kq / HZ_SLOTS) & 1));
+                }
+                return;
+            }
+            if (active) {
+                const int o = 4 + 4 * lane;
+                const float4 a = *reinterpret_cast<const float4 *>(st.slot(s, 0) + o);
+                const float4 bx = *reinterpret_cast<const float4 *>(st.slot(s, 1) + o);
+                const float4 by = *reinterpret_cast<const float4 *>(st.slot(s, 2) + o);
+                const float4 be = *reinterpret_cast<const float4 *>(st.slot(s, 3) + o);
+                hzo[0] = a.x, hzo[1] = a.y, hzo[2] = a.z, hzo[3] = a.w;
+                exo[0] = bx.x, exo[1] = bx.y, exo[2] = bx.z, exo[3] = bx.w;
+                eyo[0] = by.x, eyo[1] = by.y, eyo[2] = by.z, eyo[3] = by.w;
+                ep[0] = be.x, ep[1] = be.y, ep[2] = be.z, ep[3] = be.w;
+                ex_left = st.slot(s, 1)[o - 1];
+                if (halo_lane) {
+                    hz_h = st.slot(s, 0)[o + 4];
+                    ex_h = st.slot(s, 1)[o + 4];
+                    ey_h = st.slot(s, 2)[o + 4];
+                    ep_h = st.slot(s, 3)[o + 4];
+                }
+            }
+            __syncwarp();
+            if (lane == 0 && i + HZ_AHEAD + 1 <= r1) {
+                tb_fence_proxy_async();
+                st.issue(p, i + HZ_AHEAD + 1, s);
+            }
+        } else {
+            if (active) {
+                hz_ld4<VEC>(p.hz_in, row + jt, hzo);
+                hz_ld4<VEC>(p.ex_in, row + jt, exo);
+                hz_ld4<VEC>(p.ey_in, row + jt, eyo);
+                if (EPS) hz_ld4<VEC>(p.eps, row + jt, ep);
+                if (lane == 0) ex_left = __ldg(p.ex_in + row + jt - 1);
+                if (halo_lane) {
+                    hz_h = __ldg(p.hz_in + row + j_end);
+                    ex_h = __ldg(p.ex_in + row + j_end);
+                    ey_h = __ldg(p.ey_in + row + j_end);
+                    if (EPS) ep_h = __ldg(p.eps + row + j_end);
+                }
+            }
+            const float left = __shfl_up_sync(FULL, exo[3], 1);
+            if (lane != 0) ex_left = left;
+        }
+
+        // H_z of the row and of the halo column
+        const float ixe = __ldg(p.ixe + i);
+        float da[4], db[4];
+        float da_h = p.da_u, db_h = p.db_u;
+        if (!EPS && p.da) {
+            if (active) {
+                hz_ld4<VEC>(p.da, row + jt, da);
+                hz_ld4<VEC>(p.db, row + jt, db);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) da[c] = db[c] = 0.0f;
+            }
+            if (halo_lane) da_h = __ldg(p.da + row + j_end), db_h = __ldg(p.db + row + j_end);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) da[c] = p.da_u, db[c] = p.db_u;
+        }
+        float hn[4];
+        hz_plain_h(hzo, exo, eyo, eyp, ex_left, iye, ixe, da, db, hn);
+        if (own_row && active) hz_st4<VEC>(p.hz_out, row + jt, hn);
+        float h_halo = 0.0f;
+        if (halo_lane) {
+            const float dex = ex_h - exo[3];
+            const float dey = ey_h - ey_halo_prev;
+            float curl = dex * iye_h;
+            curl -= dey * ixe;
+            h_halo = da_h * hz_h + db_h * curl;
+        }
+        ey_halo_prev = ey_h;
+        float h_next = __shfl_down_sync(FULL, hn[0], 1), e_next = EPS ? __shfl_down_sync(FULL, ep[0], 1) : 0.0f;
+        if (halo_lane) h_next = h_halo, e_next = ep_h;
+
+        // E_x of row i, E_y of row i - 1
+        if (active) {
+            float cax[4], cbx[4], cay[4], cby[4];
+            const int re = i - 1;
+            const bool do_y = i > r0;
+            if (!EPS) {
+                hz_ld4<VEC>(p.cb_x, row + jt, cbx);
+                hz_ld4<VEC>(p.cb_y, (size_t)re * ny + jt, cby);
+                if (p.ca_x) {
+                    hz_ld4<VEC>(p.ca_x, row + jt, cax);
+                    hz_ld4<VEC>(p.ca_y, (size_t)re * ny + jt, cay);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) cax[c] = cay[c] = 1.0f;
+                }
+            }
+            float vx[4], vy[4];
+            hz_plain_e<EPS>(p, vx, vy, i, re, jt, own_row, do_y, hn, exo, ep, h_next, e_next, lo_y, up_y, iyh, hzp,
+                            eyp, epp, cax, cbx, cay, cby);
+            if (own_row) hz_st4<VEC>(p.ex_out, row + jt, vx);
+            if (do_y) hz_st4<VEC>(p.ey_out, (size_t)re * ny + jt, vy);
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            hzp[c] = hn[c];
+            eyp[c] = eyo[c];
+            epp[c] = ep[c];
+        }
+    }
+}
+
+// Border kernel: one thread per cell of the grid outside the interior box (up to four rectangles, rects[k] = rows
+// [r0, r1) x columns [c0, c1), cell offsets in first[k]).  A thread updates its H_z, E_x and E_y; the new H_z of the
+// cell right of it and of the cell above it, which its E_x / E_y read, it evaluates again from the old E (not stored).
+struct HzBorderRects {
+    int32_t n;
+    int32_t r0[4], r1[4], c0[4], c1[4];
+    int64_t first[5];
+};
+
+template <bool EPS>
+__global__ void __launch_bounds__(256) hz2d_border_kernel(const Hz2DParams p, const HzBorderRects rects) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= rects.first[rects.n]) return;
+    int k = 0;
+    while (k + 1 < rects.n && t >= rects.first[k + 1]) ++k;
+    const int64_t local = t - rects.first[k];
+    const int w = rects.c1[k] - rects.c0[k];
+    const int i = rects.r0[k] + (int)(local / w), j = rects.c0[k] + (int)(local % w);
+    const int nx = p.nx, ny = p.ny;
+    const size_t idx = (size_t)i * ny + j;
+    float exo, eyo, scratch_x, scratch_y;
+    const float h = hz2d_hz_at(p, i, j, true, exo, eyo);
+    p.hz_out[idx] = h;
+    if (j < ny - 1 || p.py) {
+        const int jn = j < ny - 1 ? j + 1 : 0;
+        const float hn = hz2d_hz_at(p, i, jn, false, scratch_x, scratch_y);
+        const float up = j < ny - 1 ? hn : hz_wrap_hi(hn);
+        float ca = 1.0f, cb;
+        if (EPS) {
+            cb = hz_cb_lossless(__ldg(p.eps + idx), __ldg(p.eps + (size_t)i * ny + jn), __ldg(p.lo_y + j),
+                                __ldg(p.up_y + j), p.dt, p.eps0);
+        } else {
+            ca = p.ca_x ? __ldg(p.ca_x + idx) : 1.0f;
+            cb = __ldg(p.cb_x + idx);
+        }
+        p.ex_out[idx] = hz2d_ex_at(p, i, j, exo, ca, cb, h, up);
+    } else {
+        p.ex_out[idx] = exo;   // the last face of an open y is never updated
+    }
+    if (i < nx - 1 || p.px) {
+        const int in = i < nx - 1 ? i + 1 : 0;
+        const float hn = hz2d_hz_at(p, in, j, false, scratch_x, scratch_y);
+        const float up = i < nx - 1 ? hn : hz_wrap_hi(hn);
+        float ca = 1.0f, cb;
+        if (EPS) {
+            cb = hz_cb_lossless(__ldg(p.eps + idx), __ldg(p.eps + (size_t)in * ny + j), __ldg(p.lo_x + i),
+                                __ldg(p.up_x + i), p.dt, p.eps0);
+        } else {
+            ca = p.ca_y ? __ldg(p.ca_y + idx) : 1.0f;
+            cb = __ldg(p.cb_y + idx);
+        }
+        p.ey_out[idx] = hz2d_ey_at(p, i, j, eyo, ca, cb, h, up);
+    } else {
+        p.ey_out[idx] = eyo;   // the last face of an open x is never updated
+    }
 }
 
 // ---------------------------------------------------------------------------------------------- coefficients

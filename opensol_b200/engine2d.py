@@ -297,14 +297,15 @@ class FDTDEngine2D_Ez:
 
 class FDTDEngine2D_Hz(FDTDEngine2D_Ez):
     """Device engine of one 2D H_z simulation (FDTDEngine2D_Hz, open_sol/physics/em/solvers/fdtd_hz_2d.py:12): H_z at
-    the cell centres, E_x / E_y on the hi-y / hi-x faces, face-averaged eps_xx / eps_yy / sigma_e.  One fused kernel
-    per Yee step (variant 1, tile_rows rows per CTA, 0 = chosen per grid) or the in-place per-half-step kernels
-    (variant 0); both give bit-identical fields."""
+    the cell centres, E_x / E_y on the hi-y / hi-x faces, face-averaged eps_xx / eps_yy / sigma_e.  Per Yee step an
+    interior kernel over the box of plain cells (tile_rows rows per CTA, 0 = chosen per grid) and a border kernel over
+    the rest (variant 1), or the in-place per-half-step kernels (variant 0); both give bit-identical fields."""
 
     polarization = 'hz'
     FIELDS = {'hz': _native.OS_HZ_HZ, 'ex': _native.OS_HZ_EX, 'ey': _native.OS_HZ_EY}
     _CREATE = 'os_fdtd2d_hz_create'
-    KERNEL_KINDS = {2: 'ez2d_flux_kernel (E_x|E_y, H_z)', 3: 'hz2d_step_kernel | hz2d_h_kernel+hz2d_e_kernel'}
+    KERNEL_KINDS = {2: 'ez2d_flux_kernel (E_x|E_y, H_z)',
+                    3: 'hz2d_interior_kernel+hz2d_border_kernel | hz2d_h_kernel+hz2d_e_kernel'}
 
     def __init__(self, domain, boundary_config, device: int = 0):
         super().__init__(domain, boundary_config, device)
@@ -327,8 +328,8 @@ class FDTDEngine2D_Hz(FDTDEngine2D_Ez):
         self.h2d_bytes += sum(a.nbytes for a in arrays if a is not None)
 
     def configure(self, variant=None, steps_per_launch=None, tile_rows=None):
-        """variant 1 (default): one fused kernel per step with tile_rows rows per CTA (0 = chosen per grid); variant
-        0: one H_z and one E kernel per step.  steps_per_launch is 1."""
+        """variant 1 (default): interior + border kernel per step, tile_rows interior rows per CTA (0 = chosen per
+        grid); variant 0: one H_z and one E kernel per step.  steps_per_launch is 1."""
         super().configure(variant, steps_per_launch, tile_rows)
 
     def autotune(self, candidates=None, repeats=4):

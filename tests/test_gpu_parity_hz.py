@@ -2,9 +2,9 @@
 
 The engine evaluates every cell in the reference's order without fused multiply-add, so these tests assert
 bit-identical H_z / E_x / E_y (array_equal, and the SHA-256 digests of open_sol's own fields in tests/golden),
-bit-identical complex128 spectra and fluxes, for both kernel sets (the fused step kernel, variant 1, in its lossless
-one-word-per-cell form and in its coefficient-array form; the per-half-step kernels, variant 0) and for row runs
-per CTA from 1 row up.
+bit-identical complex128 spectra and fluxes, for both kernel sets (variant 1: the interior kernel, TMA-staged in the
+lossless one-word-per-cell form or with direct loads in the coefficient form, plus the border kernel; variant 0: the
+per-half-step kernels) and for interior row runs per CTA from 1 row up.
 """
 import hashlib
 import os
@@ -34,8 +34,8 @@ def _oracle_kwargs(spec):
     return {k: v for k, v in spec['sim'].items() if k != 'polarization'}
 
 
-# (variant, rows per CTA): the per-half-step kernels, and the fused kernel with the per-grid choice and with runs of
-# 1, 2, 7 and 64 rows (ragged last runs, halo rows on every run)
+# (variant, rows per CTA): the per-half-step kernels, and the interior + border kernels with the per-grid choice and
+# with interior runs of 1, 2, 7 and 64 rows (ragged last runs, halo rows on every run)
 HZ_CONFIGS = [(0, 0), (1, 0), (1, 1), (1, 2), (1, 7), (1, 64)]
 
 
@@ -194,4 +194,5 @@ def test_hz_field_write_read_roundtrip_and_launch_count():
     np.testing.assert_array_equal(sim.em.engine.read_field('ex'), values)
     sim.em.engine.advance(12)
     m = sim.em.engine.sample_interval
-    assert sim.em.engine.launch_count() == 12 + 12 // m
+    # per step the interior kernel and the border kernel, plus one DFT launch per sample step
+    assert sim.em.engine.launch_count() == 12 * 2 + 12 // m
