@@ -385,22 +385,28 @@ def run_hz2d(args):
     engine.advance(args.sim_steps, tables)
     times = engine.kernel_times()
     engine.set_profiling(False)
-    name = engine.KERNEL_KINDS[3]
+    peak, peak_kind = measured_peak_hbm()
+    interior_cells, border_cells = engine.hz_plan()
+    if engine.variant == 1 and interior_cells:
+        name = engine.KERNEL_KINDS[0]
+        units = interior_cells
+    else:
+        name = engine.KERNEL_KINDS[3 if engine.variant == 0 else 1]
+        units = cells
     total_ms, n_launch = times[name]
     launch_ms = total_ms / n_launch
-    peak, peak_kind = measured_peak_hbm()
-    achieved = BYTES_PER_CELL_UPDATE * cells / (launch_ms / 1e3) / 1e9
+    achieved = BYTES_PER_CELL_UPDATE * units / (launch_ms / 1e3) / 1e9
     roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
                 'traffic': None, 'peak_source': f'{peak_kind} hbm_gbs (copy bandwidth)', 'kernel': name,
-                'bytes_per_cell_update': BYTES_PER_CELL_UPDATE, 'cell_updates_per_launch': cells,
-                'launch_ms': launch_ms, 'lossless_form': engine.lossless_form(),
+                'bytes_per_cell_update': BYTES_PER_CELL_UPDATE, 'cell_updates_per_launch': units,
+                'border_cells': border_cells, 'launch_ms': launch_ms, 'lossless_form': engine.lossless_form(),
                 'kernel_share': {k: v[0] / sum(t[0] for t in times.values()) for k, v in times.items()}}
     traffic_path = os.path.join(ROOT, 'profiles', 'traffic.json')
     if os.path.exists(traffic_path):
         with open(traffic_path) as f:
-            t = json.load(f).get('hz2d_step_kernel')
+            t = json.load(f).get('hz2d_interior_kernel')
         if t:
-            roofline['traffic'] = t['dram_bytes_per_cell_update'] * cells
+            roofline['traffic'] = t['dram_bytes_per_cell_update'] * units
             roofline['traffic_note'] = t['note']
     line = {'metric': 'FDTD Gcell-updates/s (2D H_z)', 'value': value, 'unit': 'Gcell-updates/s', 'n_gpus': 1,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms / args.steps, 'higher_is_better': True,

@@ -121,6 +121,9 @@ int os_fdtd2d_hz_read_cb(OsFdtd2D *h, float *cb_x, float *cb_y);
 /* 1 when the lossless one-word-per-cell form is active, else 0.  No open_sol counterpart. */
 int os_fdtd2d_hz_form(OsFdtd2D *h, int32_t *lossless_form);
 
+/* Cells the variant-1 step gives the interior kernel and the border kernel.  No open_sol counterpart. */
+int os_fdtd2d_hz_plan(OsFdtd2D *h, int64_t *interior_cells, int64_t *border_cells);
+
 /* One CPML side (a single OS_SIDE_* bit): psi recursion rows b, a and bulk curl spacing of its cell-centre (_e) and
  * hi-face (_h) rows, npml each (_cpml_row_set, boundaries.py:671-686; rows from cpml_side_rows, :570-576). */
 int os_fdtd2d_set_cpml_side(OsFdtd2D *h, int32_t side, const float *b_e, const float *a_e, const float *inv_e,

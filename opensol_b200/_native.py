@@ -58,6 +58,7 @@ SIGNATURES = {
                                    ctypes.c_float],
     'os_fdtd2d_hz_read_cb': [_P, _F, _F],
     'os_fdtd2d_hz_form': [_P, ctypes.POINTER(_I32)],
+    'os_fdtd2d_hz_plan': [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
     'os_fdtd2d_set_cpml_side': [_P, _I32, _F, _F, _F, _F, _F, _F],
     'os_fdtd2d_add_line_source': [_P, _I32, _I32, _I32, _I32, _F, ctypes.POINTER(_I32)],
     'os_fdtd2d_set_line_profile': [_P, _I32, _F],

@@ -967,10 +967,26 @@ static int hz_rows_per_cta(const OsFdtd2D *h, const HzPlan &q) {
     return (int)rows;
 }
 
-// One fused H_z step: the interior kernel (TMA-staged rows for the lossless form on a row length that keeps the
-// copies 16-byte aligned, direct loads otherwise), then the border kernel.
-static void launch_hz_step(OsFdtd2D *h, const HzPlan &q, Hz2DParams p) {
+// One fused H_z step: the border kernel forks onto the side stream and overlaps the interior kernel (TMA-staged rows
+// for the lossless form on a row length that keeps the copies 16-byte aligned, direct loads otherwise); both read the
+// same input buffers and write disjoint cells of the output buffers, and the main stream waits for both.
+static int launch_hz_step(OsFdtd2D *h, const HzPlan &q, Hz2DParams p) {
     const bool vec = h->grid.ny % 4 == 0;
+    const int64_t border_cells = q.rects.first[q.rects.n];
+    const bool fork = q.interior && border_cells > 0;
+    cudaStream_t bstream = fork ? h->side_stream : h->stream;
+    if (fork) {
+        OS_CUDA(cudaEventRecord(h->ev_fork, h->stream));
+        OS_CUDA(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
+    }
+    if (border_cells > 0) {
+        const unsigned blocks = (unsigned)((border_cells + 255) / 256);
+        OS_TRY(prof_begin(h, 1, bstream));
+        if (h->hz_eps) hz2d_border_kernel<true><<<blocks, 256, 0, bstream>>>(p, q.rects);
+        else hz2d_border_kernel<false><<<blocks, 256, 0, bstream>>>(p, q.rects);
+        OS_TRY(prof_end(h, bstream));
+        h->launches += 1;
+    }
     if (q.interior) {
         p.ia = q.ia, p.ib = q.ib, p.jc0 = q.jc0, p.jc1 = q.jc1;
         p.rows_per_cta = hz_rows_per_cta(h, q);
@@ -978,6 +994,7 @@ static void launch_hz_step(OsFdtd2D *h, const HzPlan &q, Hz2DParams p) {
         const dim3 grid((unsigned)((warps + HZ_THREADS / 32 - 1) / (HZ_THREADS / 32)),
                         (unsigned)((q.ib - q.ia + p.rows_per_cta - 1) / p.rows_per_cta));
         int32_t *err = h->err.ptr;
+        OS_TRY(prof_begin(h, 0, h->stream));
         if (h->hz_eps && vec) {
             hz2d_interior_kernel<true, true, true>
                 <<<grid, HZ_THREADS, (HZ_THREADS / 32) * hz_warp_smem_bytes(), h->stream>>>(p, err);
@@ -988,15 +1005,14 @@ static void launch_hz_step(OsFdtd2D *h, const HzPlan &q, Hz2DParams p) {
         } else {
             hz2d_interior_kernel<false, false, false><<<grid, HZ_THREADS, 0, h->stream>>>(p, err);
         }
+        OS_TRY(prof_end(h, h->stream));
         h->launches += 1;
     }
-    const int64_t cells = q.rects.first[q.rects.n];
-    if (cells > 0) {
-        const unsigned blocks = (unsigned)((cells + 255) / 256);
-        if (h->hz_eps) hz2d_border_kernel<true><<<blocks, 256, 0, h->stream>>>(p, q.rects);
-        else hz2d_border_kernel<false><<<blocks, 256, 0, h->stream>>>(p, q.rects);
-        h->launches += 1;
+    if (fork) {
+        OS_CUDA(cudaEventRecord(h->ev_join, h->side_stream));
+        OS_CUDA(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
     }
+    return OS_OK;
 }
 
 // H_z chunk: variant 0 launches the in-place H and E kernels per step, otherwise one fused step kernel per step
@@ -1015,15 +1031,15 @@ static int advance_hz(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_
         p.line_values = values;
         p.values_stride = n_steps;
         p.k_step = k;
-        OS_TRY(prof_begin(h, 3, h->stream));
         if (h->variant == 0) {
+            OS_TRY(prof_begin(h, 3, h->stream));
             hz2d_h_kernel<<<cell_grid, cell_block, 0, h->stream>>>(p);
             hz2d_e_kernel<<<cell_grid, cell_block, 0, h->stream>>>(p);
+            OS_TRY(prof_end(h, h->stream));
             h->launches += 2;
         } else {
-            launch_hz_step(h, plan, p);
+            OS_TRY(launch_hz_step(h, plan, p));
         }
-        OS_TRY(prof_end(h, h->stream));
         h->cur = out;
         h->n_step += 1;
         if (!h->fluxes.empty() && h->n_step % m == 0) {
@@ -1084,6 +1100,15 @@ static int run_chunk(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t
 }
 
 }  // namespace os
+
+extern "C" int os_fdtd2d_hz_plan(OsFdtd2D *h, int64_t *interior_cells, int64_t *border_cells) {
+    OS_TRY(require_hz(h, "os_fdtd2d_hz_plan"));
+    OS_CHECK(interior_cells && border_cells, OS_ERR_INVALID, "os_fdtd2d_hz_plan: null argument");
+    const HzPlan q = hz_plan(h);
+    *interior_cells = q.interior ? (int64_t)(q.ib - q.ia) * (q.jc1 - q.jc0) : 0;
+    *border_cells = q.rects.first[q.rects.n];
+    return OS_OK;
+}
 
 extern "C" int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line_values, int64_t first_sample,
                                  int64_t n_samples, const float *phases) {

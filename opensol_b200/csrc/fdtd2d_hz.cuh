@@ -510,12 +510,21 @@ struct HzBorderRects {
 template <bool EPS>
 __global__ void __launch_bounds__(256) hz2d_border_kernel(const Hz2DParams p, const HzBorderRects rects) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= rects.first[rects.n]) return;
+    const int64_t total = rects.n == 1 ? rects.first[1] : rects.n == 2 ? rects.first[2]
+                          : rects.n == 3 ? rects.first[3] : rects.first[4];
+    if (t >= total) return;
+    // the rectangle of this cell, selected without indexing the parameter arrays by a runtime value
     int k = 0;
-    while (k + 1 < rects.n && t >= rects.first[k + 1]) ++k;
-    const int64_t local = t - rects.first[k];
-    const int w = rects.c1[k] - rects.c0[k];
-    const int i = rects.r0[k] + (int)(local / w), j = rects.c0[k] + (int)(local % w);
+    if (rects.n > 1 && t >= rects.first[1]) k = 1;
+    if (rects.n > 2 && t >= rects.first[2]) k = 2;
+    if (rects.n > 3 && t >= rects.first[3]) k = 3;
+    const int64_t first = k == 0 ? 0 : k == 1 ? rects.first[1] : k == 2 ? rects.first[2] : rects.first[3];
+    const int rr0 = k == 0 ? rects.r0[0] : k == 1 ? rects.r0[1] : k == 2 ? rects.r0[2] : rects.r0[3];
+    const int cc0 = k == 0 ? rects.c0[0] : k == 1 ? rects.c0[1] : k == 2 ? rects.c0[2] : rects.c0[3];
+    const int cc1 = k == 0 ? rects.c1[0] : k == 1 ? rects.c1[1] : k == 2 ? rects.c1[2] : rects.c1[3];
+    const int64_t local = t - first;
+    const int w = cc1 - cc0;
+    const int i = rr0 + (int)(local / w), j = cc0 + (int)(local % w);
     const int nx = p.nx, ny = p.ny;
     const size_t idx = (size_t)i * ny + j;
     float exo, eyo, scratch_x, scratch_y;

@@ -304,8 +304,8 @@ class FDTDEngine2D_Hz(FDTDEngine2D_Ez):
     polarization = 'hz'
     FIELDS = {'hz': _native.OS_HZ_HZ, 'ex': _native.OS_HZ_EX, 'ey': _native.OS_HZ_EY}
     _CREATE = 'os_fdtd2d_hz_create'
-    KERNEL_KINDS = {2: 'ez2d_flux_kernel (E_x|E_y, H_z)',
-                    3: 'hz2d_interior_kernel+hz2d_border_kernel | hz2d_h_kernel+hz2d_e_kernel'}
+    KERNEL_KINDS = {0: 'hz2d_interior_kernel', 1: 'hz2d_border_kernel', 2: 'ez2d_flux_kernel (E_x|E_y, H_z)',
+                    3: 'hz2d_h_kernel+hz2d_e_kernel'}
 
     def __init__(self, domain, boundary_config, device: int = 0):
         super().__init__(domain, boundary_config, device)
@@ -336,7 +336,14 @@ class FDTDEngine2D_Hz(FDTDEngine2D_Ez):
         raise NotImplementedError('the H_z engine chooses its rows per CTA from the grid (configure(tile_rows=...))')
 
     def plan_info(self, steps_per_launch=None):
-        raise NotImplementedError('the H_z engine has no blocked-kernel plan')
+        raise NotImplementedError('the H_z engine has no blocked-kernel plan (hz_plan gives its split)')
+
+    def hz_plan(self):
+        """(interior cells, border cells) of the variant-1 step."""
+        self.sync_device()
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        _native.check(_native.load().os_fdtd2d_hz_plan(self.handle, ctypes.byref(a), ctypes.byref(b)))
+        return int(a.value), int(b.value)
 
     def lossless_form(self):
         """True when the step kernel evaluates the face cb from eps_r (no coefficient arrays stored)."""
