@@ -210,7 +210,9 @@ int os_fdtd2d_reset(OsFdtd2D *h);
 int os_fdtd2d_synchronize(OsFdtd2D *h);
 
 /* Launch on the caller's CUDA stream (a cudaStream_t; NULL = back to the handle's own stream).  Work already queued
- * on the previous stream is waited for first.  No open_sol counterpart: the B200 hook for torch streams. */
+ * on the previous stream is waited for first.  The caller keeps that stream alive while the handle uses it: set the
+ * handle back (NULL) before destroying the stream; os_fdtd2d_destroy itself never touches a caller's stream.  No
+ * open_sol counterpart: the B200 hook for torch streams. */
 int os_fdtd2d_set_stream(OsFdtd2D *h, void *cuda_stream);
 
 /* Device milliseconds of the dominant field kernels over the last os_fdtd2d_advance (CUDA events on the handle's

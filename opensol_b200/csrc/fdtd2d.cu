@@ -14,6 +14,7 @@
 #include "fdtd2d_tb.cuh"
 #include "fdtd2d_interior.cuh"
 #include "fdtd2d_hz.cuh"
+#include "fdtd2d_frame.cuh"
 
 #include <algorithm>
 
@@ -53,6 +54,8 @@ struct OsFdtd2D {
     os::DeviceArray<float> inv_dx_e, inv_dx_h, inv_dy_e, inv_dy_h;
     os::DeviceArray<float> cpml_rows[4];   // per side: b_e, a_e, inv_e, b_h, a_h, inv_h (6 * npml)
     os::DeviceArray<float> psi_e[2][4], psi_h[2][4];
+    // scratch states of the frame's intermediate steps in a blocked launch (E_z engines; allocated at creation)
+    os::DeviceArray<float> sez[2], shx[2], shy[2], spsi_e[2][4], spsi_h[2][4];
     bool cpml_set[4] = {false, false, false, false};
     std::vector<float> host_inv[4];       // inv_dx_e, inv_dx_h, inv_dy_e, inv_dy_h (host copies: interior check)
     int32_t variant = 1;                  // 0: per-half-step kernels, 1: temporally blocked
@@ -185,7 +188,7 @@ static int require_ez(const OsFdtd2D *h, const char *fn) {
 
 using namespace os;
 
-extern "C" int os_fdtd2d_create(const OsGrid2D *grid, OsFdtd2D **out) {
+static int create_2d(const OsGrid2D *grid, int32_t polarization, OsFdtd2D **out) {
     OS_CHECK(grid && out, OS_ERR_INVALID, "os_fdtd2d_create: null argument");
     *out = nullptr;
     const OsGrid2D g = *grid;
@@ -220,10 +223,16 @@ extern "C" int os_fdtd2d_create(const OsGrid2D *grid, OsFdtd2D **out) {
     OS_CUDA(cudaEventCreate(&h->ev_start));
     OS_CUDA(cudaEventCreate(&h->ev_stop));
     const size_t n = cells(h.get());
+    h->polarization = polarization;
     for (int b = 0; b < 2; ++b) {
         OS_TRY(h->ez[b].alloc(n));
         OS_TRY(h->hx[b].alloc(n));
         OS_TRY(h->hy[b].alloc(n));
+        if (polarization == 0) {
+            OS_TRY(h->sez[b].alloc(n));
+            OS_TRY(h->shx[b].alloc(n));
+            OS_TRY(h->shy[b].alloc(n));
+        }
     }
     for (int s = 0; s < 4; ++s) {
         if (!(g.cpml_sides & (1 << s))) continue;
@@ -231,6 +240,10 @@ extern "C" int os_fdtd2d_create(const OsGrid2D *grid, OsFdtd2D **out) {
         for (int b = 0; b < 2; ++b) {
             OS_TRY(h->psi_e[b][s].alloc(slab));
             OS_TRY(h->psi_h[b][s].alloc(slab));
+            if (polarization == 0) {
+                OS_TRY(h->spsi_e[b][s].alloc(slab));
+                OS_TRY(h->spsi_h[b][s].alloc(slab));
+            }
         }
         OS_TRY(h->cpml_rows[s].alloc(6 * (size_t)g.npml));
     }
@@ -242,10 +255,13 @@ extern "C" int os_fdtd2d_create(const OsGrid2D *grid, OsFdtd2D **out) {
     return OS_OK;
 }
 
+extern "C" int os_fdtd2d_create(const OsGrid2D *grid, OsFdtd2D **out) { return create_2d(grid, 0, out); }
+
 extern "C" int os_fdtd2d_destroy(OsFdtd2D *h) {
     if (!h) return OS_OK;
     cudaSetDevice(h->device);
-    if (h->stream) cudaStreamSynchronize(h->stream);
+    // only the streams the handle owns: a caller's stream (os_fdtd2d_set_stream) may already be destroyed; freeing
+    // the device arrays below waits for the device anyway
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     if (h->ev_start) cudaEventDestroy(h->ev_start);
     if (h->ev_stop) cudaEventDestroy(h->ev_stop);
@@ -356,11 +372,7 @@ extern "C" int os_fdtd2d_read_cb(OsFdtd2D *h, float *cb) {
 // ---------------------------------------------------------------------------------------------------------------
 // H_z polarisation: the same handle with H_z / E_x / E_y in the three field buffer sets.
 
-extern "C" int os_fdtd2d_hz_create(const OsGrid2D *grid, OsFdtd2D **out) {
-    OS_TRY(os_fdtd2d_create(grid, out));
-    (*out)->polarization = 1;
-    return OS_OK;
-}
+extern "C" int os_fdtd2d_hz_create(const OsGrid2D *grid, OsFdtd2D **out) { return create_2d(grid, 1, out); }
 
 extern "C" int os_fdtd2d_hz_set_materials(OsFdtd2D *h, const float *eps_xx, const float *eps_yy,
                                           const float *sigma_e, const float *mu_r, const float *sigma_m,
@@ -709,6 +721,77 @@ static int launch_interior_any(OsFdtd2D *h, const TBParams &q) {
     return h->has_ca ? launch_interior_ca<T, true>(h, q) : launch_interior_ca<T, false>(h, q);
 }
 
+// The frame of one blocked launch of T steps: T single-step launches of ez2d_frame_step_kernel on stream `s`, step k
+// over the grid minus the interior rectangle shrunk by T - k cells on each non-periodic side, from the state of step
+// k - 1 (the input buffer set for k = 1, else a scratch set) to that of step k (a scratch set, the output buffer set
+// for k = T).  `q` carries the launch's sources, monitors and sample mask.
+static int launch_frame_chain(OsFdtd2D *h, int T, const TBParams &q, const Rect *in, cudaStream_t s) {
+    const OsGrid2D &g = h->grid;
+    const int in_set = h->cur, out_set = h->cur ^ 1;
+    for (int k = 1; k <= T; ++k) {
+        EzFrameParams f{};
+        f.nx = g.nx, f.ny = g.ny, f.px = g.periodic_x, f.py = g.periodic_y, f.npml = g.npml;
+        f.cpml_mask = g.cpml_sides;
+        f.ca = q.ca, f.cb = q.cb, f.da = q.da, f.db = q.db, f.da_u = q.da_u, f.db_u = q.db_u;
+        f.inv_dx_e = q.inv_dx_e, f.inv_dx_h = q.inv_dx_h, f.inv_dy_e = q.inv_dy_e, f.inv_dy_h = q.inv_dy_h;
+        const bool from_io = k == 1, to_io = k == T;
+        const int src = (k - 2) % 2, dst = (k - 1) % 2;
+        f.ez_in = from_io ? h->ez[in_set].ptr : h->sez[src].ptr;
+        f.hx_in = from_io ? h->hx[in_set].ptr : h->shx[src].ptr;
+        f.hy_in = from_io ? h->hy[in_set].ptr : h->shy[src].ptr;
+        f.ez_out = to_io ? h->ez[out_set].ptr : h->sez[dst].ptr;
+        f.hx_out = to_io ? h->hx[out_set].ptr : h->shx[dst].ptr;
+        f.hy_out = to_io ? h->hy[out_set].ptr : h->shy[dst].ptr;
+        for (int sd = 0; sd < 4; ++sd) {
+            f.cpml_rows[sd] = q.cpml_rows[sd];
+            f.psi_e_in[sd] = from_io ? h->psi_e[in_set][sd].ptr : h->spsi_e[src][sd].ptr;
+            f.psi_h_in[sd] = from_io ? h->psi_h[in_set][sd].ptr : h->spsi_h[src][sd].ptr;
+            f.psi_e_out[sd] = to_io ? h->psi_e[out_set][sd].ptr : h->spsi_e[dst][sd].ptr;
+            f.psi_h_out[sd] = to_io ? h->psi_h[out_set][sd].ptr : h->spsi_h[dst][sd].ptr;
+        }
+        f.n_lines = q.n_lines;
+        for (int l = 0; l < q.n_lines; ++l) f.lines[l] = q.lines[l];
+        f.line_values = q.line_values;
+        f.values_stride = q.values_stride;
+        f.k_col = q.k0 + (k - 1);
+        f.n_mons = q.n_mons;
+        for (int m = 0; m < q.n_mons; ++m) f.mons[m] = q.mons[m];
+        f.sample_slot = ((q.sample_mask >> (k - 1)) & 1u) ? __builtin_popcount(q.sample_mask & ((1u << (k - 1)) - 1u))
+                                                         : -1;
+        // the interior (its cells are the interior kernel's) and this step's region around it shrunk by T - k
+        Rect sh{0, 0, 0, 0};
+        if (in) {
+            f.in_r0 = in->r0, f.in_r1 = in->r1, f.in_c0 = in->c0, f.in_c1 = in->c1;
+            const int w = T - k;
+            sh = *in;
+            if (!g.periodic_x) sh.r0 += w, sh.r1 -= w;
+            if (!g.periodic_y) sh.c0 += w, sh.c1 -= w;
+        }
+        std::vector<Rect> region;
+        if (sh.r1 > sh.r0 && sh.c1 > sh.c0) {
+            region = {Rect{0, sh.r0, 0, g.ny}, Rect{sh.r1, g.nx, 0, g.ny}, Rect{sh.r0, sh.r1, 0, sh.c0},
+                      Rect{sh.r0, sh.r1, sh.c1, g.ny}};
+        } else {
+            region = {Rect{0, g.nx, 0, g.ny}};
+        }
+        f.n_rects = 0;
+        f.first[0] = 0;
+        for (const Rect &r : region) {
+            if (r.r1 <= r.r0 || r.c1 <= r.c0) continue;
+            const int n = f.n_rects++;
+            f.r0[n] = r.r0, f.r1[n] = r.r1, f.c0[n] = r.c0, f.c1[n] = r.c1;
+            f.first[n + 1] = f.first[n] + (int64_t)(r.r1 - r.r0) * (r.c1 - r.c0);
+        }
+        const int64_t cells_k = f.first[f.n_rects];
+        if (cells_k == 0) continue;
+        OS_TRY(prof_begin(h, 1, s));
+        ez2d_frame_step_kernel<<<(unsigned)((cells_k + 255) / 256), 256, 0, s>>>(f);
+        OS_TRY(prof_end(h, s));
+        h->launches += 1;
+    }
+    return OS_OK;
+}
+
 // One blocked launch: the border (general) kernel forks onto the side stream and overlaps the interior kernel; both
 // read the same input buffers and write disjoint cells of the output buffers, and the main stream waits for both.
 template <int T>
@@ -721,7 +804,13 @@ static int launch_tb(OsFdtd2D *h, const TBParams &interior, const TBParams &gene
         OS_CUDA(cudaEventRecord(h->ev_fork, h->stream));
         OS_CUDA(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
     }
-    if (general.n_tiles) {
+    if (general.n_tiles && h->variant == 1) {
+        // the frame: one single-step launch per step over the shrinking band around the interior
+        Rect in{};
+        if (run_interior) in = Rect{interior.rects[0].r0, interior.rects[0].r1, interior.rects[0].c0,
+                                    interior.rects[0].c1};
+        OS_TRY(launch_frame_chain(h, T, general, run_interior ? &in : nullptr, gstream));
+    } else if (general.n_tiles) {
         const dim3 blocks((unsigned)((general.n_tiles + TB_WARPS - 1) / TB_WARPS));
         OS_TRY(prof_begin(h, 1, gstream));
         if (h->has_ca) ez2d_tb_kernel<T, 1, true, true><<<blocks, threads, 0, gstream>>>(general);

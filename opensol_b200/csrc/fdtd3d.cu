@@ -191,7 +191,8 @@ extern "C" int os_fdtd3d_create(const OsGrid3D *grid, OsFdtd3D **out) {
 extern "C" int os_fdtd3d_destroy(OsFdtd3D *h) {
     if (!h) return OS_OK;
     cudaSetDevice(h->device);
-    if (h->stream) cudaStreamSynchronize(h->stream);
+    // only the handle's own stream: a caller's stream (os_fdtd3d_set_stream) may already be destroyed
+    if (h->own_stream) cudaStreamSynchronize(h->own_stream);
     if (h->ev_start) cudaEventDestroy(h->ev_start);
     if (h->ev_stop) cudaEventDestroy(h->ev_stop);
     cudaStream_t s = h->own_stream;

@@ -24,7 +24,8 @@ class FDTDEngine2D_Ez:
     polarization = 'ez'
     FIELDS = {'ez': _native.OS_EZ, 'hx': _native.OS_HX, 'hy': _native.OS_HY}
     _CREATE = 'os_fdtd2d_create'
-    KERNEL_KINDS = {0: 'ez2d_interior_kernel', 1: 'ez2d_tb_kernel (general)', 2: 'ez2d_flux_staged_kernel',
+    KERNEL_KINDS = {0: 'ez2d_interior_kernel', 1: 'ez2d_frame_step_kernel | ez2d_tb_kernel (general)',
+                    2: 'ez2d_flux_staged_kernel',
                     3: 'ez2d_h_kernel+ez2d_e_kernel'}
 
     def __init__(self, domain, boundary_config, device: int = 0):

@@ -17,6 +17,7 @@ from __future__ import annotations
 import ctypes
 import math
 import time
+import weakref
 from collections import deque
 from dataclasses import dataclass, field
 
@@ -37,10 +38,12 @@ class BatchAdvancer:
         stream = ctypes.c_void_p()
         _native.check(_native.load().os_fdtd2d_batch_stream(self._handle, ctypes.byref(stream)))
         self.stream = stream.value
+        self._adopted = []   # weak references to the engines on the batch stream
 
     def adopt(self, engine):
-        """Put an engine on the batch stream (the batch launches on it)."""
+        """Put an engine on the batch stream (the batch launches on it); close() hands it back to its own stream."""
         engine.set_stream(self.stream)
+        self._adopted.append(weakref.ref(engine))
 
     def advance(self, engines, n_steps):
         n_steps = int(n_steps)
@@ -68,6 +71,12 @@ class BatchAdvancer:
 
     def close(self):
         if self._handle is not None:
+            # engines still open go back to their own streams before the batch stream is destroyed
+            for ref in self._adopted:
+                engine = ref()
+                if engine is not None and engine._handle is not None:
+                    engine.set_stream(None)
+            self._adopted = []
             _native.load().os_fdtd2d_batch_destroy(self._handle)
             self._handle = None
 
