@@ -500,20 +500,20 @@ def run_serving(args):
     specs = serving.make_job_specs(n_jobs=args.jobs, rate=20.0, seed=7)
     work = sum(s.cells() * s.steps for s in specs)
     warm = serving.make_job_specs(n_jobs=3, rate=0.0, seed=1, side_range=(64, 128), steps_range=(100, 300))
-    loop = serving.ServingLoop(max_active=48, chunk_steps=512, tile_rows=32)
+    loop = serving.ServingLoop(max_active=48, chunk_steps=512)
     loop.run(warm, realtime=False)
     loop.close()
     serving.run_alone(warm[0])
-    loop = serving.ServingLoop(max_active=48, chunk_steps=512, tile_rows=32)
+    loop = serving.ServingLoop(max_active=48, chunk_steps=512)
     t0 = time.perf_counter()
     batched = {r.job_id: r for r in loop.run(specs, realtime=False)}
     t_batch = time.perf_counter() - t0
     loop.close()
     t0 = time.perf_counter()
-    alone = {s.job_id: serving.run_alone(s, tile_rows=128)[0] for s in specs}
+    alone = {s.job_id: serving.run_alone(s)[0] for s in specs}
     t_alone = time.perf_counter() - t0
     same = all(np.array_equal(a, b) for j, r in batched.items() for a, b in zip(r.fluxes, alone[j]))
-    loop = serving.ServingLoop(max_active=48, chunk_steps=512, tile_rows=32)
+    loop = serving.ServingLoop(max_active=48, chunk_steps=512)
     t0 = time.perf_counter()
     realtime = loop.run(specs, realtime=True)
     t_rt = time.perf_counter() - t0
@@ -525,7 +525,8 @@ def run_serving(args):
             'config': {'workload': f'serving: {len(specs)} jobs, square windows U{{256..2048}} + 15 CPML cells/side, '
                                    '1-40 rectangles eps_r U(1,12), line source U(1000,1600) nm, U(2000,20000) steps, '
                                    'two 4-frequency flux lines; Poisson 20 jobs/s for the latency run',
-                       'max_active': 48, 'chunk_steps': 512, 'memory_budget_gb': 120},
+                       'max_active': 48, 'chunk_steps': 512, 'memory_budget_gb': 120,
+                       'tile_rows': 'chosen per call from the active jobs (batched) / per grid (one at a time)'},
             'one_at_a_time_sims_per_s': len(specs) / t_alone, 'speedup_vs_one_at_a_time': t_alone / t_batch,
             'cell_updates_per_s_batched': work / t_batch, 'fluxes_equal_alone_and_batched': bool(same),
             'latency_p50_s': p50, 'latency_p99_s': p99, 'realtime_makespan_s': t_rt,

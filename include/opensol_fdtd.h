@@ -42,6 +42,12 @@ int os_fdtd_last_error(char *buf, size_t n);
 /* Library version (major * 10000 + minor * 100 + patch). */
 int os_fdtd_version(void);
 
+/* Device memory of destroyed 2D engines is kept in a process-wide pool and handed to new engines of the same array
+ * sizes (after the old engine's queued work has finished), so engines created and destroyed while others run call
+ * neither cudaMalloc nor cudaFree, which waits for the whole device.  At most 16 GiB is kept; os_fdtd_pool_trim frees
+ * the pooled memory.  No open_sol counterpart (open_sol relies on cupy's memory pool). */
+int os_fdtd_pool_trim(void);
+
 /* Page-locked host memory for material arrays and read-back buffers (cudaHostAlloc), so host<->device copies run at
  * full PCIe / C2C rate.  No open_sol counterpart (open_sol's cupy pool allocates device memory only). */
 int os_fdtd_host_alloc(size_t bytes, void **out);
@@ -167,8 +173,10 @@ int os_fdtd2d_advance_noalloc(OsFdtd2D *h, int64_t n_steps, const float *line_va
                               int64_t n_samples, const float *phases);
 
 /* Kernel choice: variant 1 (default) advances steps_per_launch (1..4) Yee steps per launch with temporally blocked,
- * double-buffered kernels, tile_rows rows per interior tile; variant 2 the same with the general kernel on every
- * cell; variant 0 launches one H and one E kernel per step.
+ * double-buffered kernels, tile_rows rows per interior tile (0, the default: chosen from the grid so that the tiles
+ * fill the device's warp slots once, 8..128 rows) and the frame around the interior advanced one step per launch;
+ * variant 2 the same with the blocked general kernel on the frame; variant 0 launches one H and one E kernel per
+ * step.
  * Every choice gives bit-identical results.  No open_sol counterpart (open_sol launches per half step). */
 int os_fdtd2d_configure(OsFdtd2D *h, int32_t variant, int32_t steps_per_launch, int32_t tile_rows);
 

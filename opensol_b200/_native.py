@@ -45,6 +45,7 @@ _P = ctypes.c_void_p
 SIGNATURES = {
     'os_fdtd_last_error': [ctypes.c_char_p, ctypes.c_size_t],
     'os_fdtd_version': [],
+    'os_fdtd_pool_trim': [],
     'os_fdtd_host_alloc': [ctypes.c_size_t, ctypes.POINTER(_P)],
     'os_fdtd_host_free': [_P],
     'os_fdtd2d_create': [ctypes.POINTER(OsGrid2D), ctypes.POINTER(_P)],

@@ -60,7 +60,7 @@ struct OsFdtd2D {
     std::vector<float> host_inv[4];       // inv_dx_e, inv_dx_h, inv_dy_e, inv_dy_h (host copies: interior check)
     int32_t variant = 1;                  // 0: per-half-step kernels, 1: temporally blocked
     int32_t steps_per_launch = 3;         // T of the blocked kernels
-    int32_t tile_rows = 128;              // rows per interior tile
+    int32_t tile_rows = 0;                // rows per interior tile (0: chosen from the grid, interior_rows)
     int32_t gen_tile_rows = 16;           // rows per general tile
     int64_t launches = 0;                 // kernels launched by the last advance
     bool profiling = false;               // bracket every kernel with events (os_fdtd2d_kernel_times)
@@ -260,8 +260,31 @@ extern "C" int os_fdtd2d_create(const OsGrid2D *grid, OsFdtd2D **out) { return c
 extern "C" int os_fdtd2d_destroy(OsFdtd2D *h) {
     if (!h) return OS_OK;
     cudaSetDevice(h->device);
-    // only the streams the handle owns: a caller's stream (os_fdtd2d_set_stream) may already be destroyed; freeing
-    // the device arrays below waits for the device anyway
+    // The device arrays go to the pool, to be handed out again once the work queued so far on the handle's streams
+    // (its own, the side stream, and a caller's stream it is set to, which the caller keeps alive while the handle
+    // uses it) has finished; no cudaFree, which would wait for the whole device.
+    {
+        cudaStream_t streams[3] = {h->own_stream, h->side_stream, h->stream};
+        const int n_streams = (h->stream && h->stream != h->own_stream) ? 3 : 2;
+        PoolEvents *ev = pool_events(streams, n_streams);
+        auto give = [&](auto &a) { a.give_to_pool(ev); };
+        for (int b = 0; b < 2; ++b) {
+            give(h->ez[b]), give(h->hx[b]), give(h->hy[b]);
+            give(h->sez[b]), give(h->shx[b]), give(h->shy[b]);
+            for (int sd = 0; sd < 4; ++sd) {
+                give(h->psi_e[b][sd]), give(h->psi_h[b][sd]);
+                give(h->spsi_e[b][sd]), give(h->spsi_h[b][sd]);
+            }
+        }
+        give(h->ca), give(h->cb), give(h->da), give(h->db), give(h->ca_y), give(h->cb_y);
+        give(h->eps_cell), give(h->shares);
+        give(h->inv_dx_e), give(h->inv_dx_h), give(h->inv_dy_e), give(h->inv_dy_h);
+        for (int sd = 0; sd < 4; ++sd) give(h->cpml_rows[sd]);
+        for (auto &l : h->lines) give(l->profile);
+        for (auto &f : h->fluxes) give(f->e_acc), give(f->h_acc), give(f->stage);
+        give(h->err), give(h->line_values), give(h->phases);
+        pool_events_done(ev);
+    }
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     if (h->ev_start) cudaEventDestroy(h->ev_start);
     if (h->ev_stop) cudaEventDestroy(h->ev_stop);
@@ -614,7 +637,24 @@ static bool constant_over(const std::vector<float> &v, int a, int b, float *valu
 // The interior rectangle (cells whose T-step dependency cone avoids the CPML slabs and the non-periodic edges) and the
 // border rectangles around it.  Interior rows need i0 - T >= npml + 1 and i1 - 1 + T <= nx - npml - 2 on a CPML x
 // axis; columns likewise with the 4-column left halo of the 128-bit loads.
-static void plan_tiles(const OsFdtd2D *h, int T, TBParams &interior, TBParams &general, bool &has_interior) {
+// Rows per interior tile when the handle leaves the choice to the plan (tile_rows 0): one wave of warps over the
+// device's resident warp slots (4 blocks of 4 warps per SM), 8..128 rows.  Each warp streams its tile's rows one
+// after the other, so a grid with fewer tiles than slots runs in the time of one tile; shorter tiles cut that time
+// until the tiles fill the slots.
+static int interior_rows(const OsFdtd2D *h, int rows, int cols, int rows_override = 0) {
+    if (rows_override > 0) return rows_override;
+    if (h->tile_rows > 0) return h->tile_rows;
+    const int64_t tiles_c = (cols + 119) / 120;
+    const int64_t slots = (int64_t)h->sm_count * 4 * TB_WARPS;
+    const int64_t r = (int64_t)rows * tiles_c / std::max<int64_t>(1, slots);
+    return (int)std::max<int64_t>(8, std::min<int64_t>(128, r));
+}
+
+// The interior rectangle of the blocked kernels (rows [r0, r1), columns [c0, c1)), or false when there is none.
+static bool interior_rect(const OsFdtd2D *h, int T, Rect &in);
+
+static void plan_tiles(const OsFdtd2D *h, int T, TBParams &interior, TBParams &general, bool &has_interior,
+                       int rows_override = 0) {
     const OsGrid2D &g = h->grid;
     const int npml = g.npml;
     const bool cx = (g.cpml_sides & 3) != 0, cy = (g.cpml_sides & 12) != 0;
@@ -627,8 +667,11 @@ static void plan_tiles(const OsFdtd2D *h, int T, TBParams &interior, TBParams &g
         in.c0 = cy ? round_up(npml + 1 + 4, 4) : g.ny;
         in.c1 = cy ? g.ny - npml - 1 - T : 0;
     }
-    has_interior = h->variant == 1 && in.r1 > in.r0 && in.c1 > in.c0 && g.ny % 4 == 0 && !h->has_dadb &&
-                   h->da_uniform == 1.0f;
+    // a row length that is not a multiple of 4 staggers the rows' 16-byte alignment: the interior kernel copies
+    // each row window from the boundary before it, which a periodic y (a window wrapping into two copies) does not
+    // allow
+    has_interior = h->variant == 1 && in.r1 > in.r0 && in.c1 > in.c0 && (g.ny % 4 == 0 || !g.periodic_y) &&
+                   !h->has_dadb && h->da_uniform == 1.0f;
     // uniform curl spacings over the interior's dependency cone (rows [r0 - T, r1 + T), columns [c0 - 4, c1 + T));
     // the columns a tile loads beyond its cone feed no output and may be anything
     if (has_interior) {
@@ -642,15 +685,24 @@ static void plan_tiles(const OsFdtd2D *h, int T, TBParams &interior, TBParams &g
     std::vector<Rect> border;
     if (!has_interior) {
         border.push_back(Rect{0, g.nx, 0, g.ny});
-        set_tiles(interior, {}, 120, h->tile_rows);
+        set_tiles(interior, {}, 120, interior_rows(h, 0, 0, rows_override));
     } else {
         border.push_back(Rect{0, in.r0, 0, g.ny});
         border.push_back(Rect{in.r1, g.nx, 0, g.ny});
         border.push_back(Rect{in.r0, in.r1, 0, in.c0});
         border.push_back(Rect{in.r0, in.r1, in.c1, g.ny});
-        set_tiles(interior, {in}, 120, h->tile_rows);
+        set_tiles(interior, {in}, 120, interior_rows(h, in.r1 - in.r0, in.c1 - in.c0, rows_override));
     }
     set_tiles(general, border, 32 - 2 * T, h->gen_tile_rows);
+}
+
+static bool interior_rect(const OsFdtd2D *h, int T, Rect &in) {
+    TBParams a{}, b{};
+    bool has = false;
+    plan_tiles(h, T, a, b, has, 128);
+    if (!has || !a.n_tiles) return false;
+    in = Rect{a.rects[0].r0, a.rects[0].r1, a.rects[0].c0, a.rects[0].c1};
+    return true;
 }
 
 static void fill_common(const OsFdtd2D *h, TBParams &q) {
@@ -695,7 +747,7 @@ static void fill_common(const OsFdtd2D *h, TBParams &q) {
 
 template <int T, bool CA, bool PX, bool PY>
 static int launch_interior(OsFdtd2D *h, const TBParams &q) {
-    const size_t smem = (size_t)TB_WARPS * tb_warp_smem_bytes(T, CA);
+    const size_t smem = (size_t)TB_WARPS * ip_warp_smem_bytes(T, CA);
     static bool attr_set = false;   // one flag per instantiation
     if (!attr_set) {
         OS_CUDA(cudaFuncSetAttribute(ez2d_interior_kernel<T, CA, PX, PY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -721,67 +773,83 @@ static int launch_interior_any(OsFdtd2D *h, const TBParams &q) {
     return h->has_ca ? launch_interior_ca<T, true>(h, q) : launch_interior_ca<T, false>(h, q);
 }
 
-// The frame of one blocked launch of T steps: T single-step launches of ez2d_frame_step_kernel on stream `s`, step k
-// over the grid minus the interior rectangle shrunk by T - k cells on each non-periodic side, from the state of step
-// k - 1 (the input buffer set for k = 1, else a scratch set) to that of step k (a scratch set, the output buffer set
-// for k = T).  `q` carries the launch's sources, monitors and sample mask.
-static int launch_frame_chain(OsFdtd2D *h, int T, const TBParams &q, const Rect *in, cudaStream_t s) {
+// Parameters of frame step k (1..T) of one blocked launch of T steps from buffer set in_set to out_set: the region
+// is the grid minus the interior rectangle `in` (NULL: none) shrunk by T - k cells on each non-periodic side; it
+// reads the state of step k - 1 (the input set for k = 1, else a scratch set) and writes that of step k (a scratch
+// set, the output set for k = T).  `q` carries the launch's sources, monitors, sample mask and first value column.
+static EzFrameParams make_frame_params(const OsFdtd2D *h, int T, int k, const TBParams &q, const Rect *in, int in_set,
+                                       int out_set) {
     const OsGrid2D &g = h->grid;
-    const int in_set = h->cur, out_set = h->cur ^ 1;
+    EzFrameParams f{};
+    f.nx = g.nx, f.ny = g.ny, f.px = g.periodic_x, f.py = g.periodic_y, f.npml = g.npml;
+    f.cpml_mask = g.cpml_sides;
+    f.ca = q.ca, f.cb = q.cb, f.da = q.da, f.db = q.db, f.da_u = q.da_u, f.db_u = q.db_u;
+    f.inv_dx_e = q.inv_dx_e, f.inv_dx_h = q.inv_dx_h, f.inv_dy_e = q.inv_dy_e, f.inv_dy_h = q.inv_dy_h;
+    const bool from_io = k == 1, to_io = k == T;
+    const int src = (k - 2) % 2, dst = (k - 1) % 2;
+    f.ez_in = from_io ? h->ez[in_set].ptr : h->sez[src].ptr;
+    f.hx_in = from_io ? h->hx[in_set].ptr : h->shx[src].ptr;
+    f.hy_in = from_io ? h->hy[in_set].ptr : h->shy[src].ptr;
+    f.ez_out = to_io ? h->ez[out_set].ptr : h->sez[dst].ptr;
+    f.hx_out = to_io ? h->hx[out_set].ptr : h->shx[dst].ptr;
+    f.hy_out = to_io ? h->hy[out_set].ptr : h->shy[dst].ptr;
+    for (int sd = 0; sd < 4; ++sd) {
+        f.cpml_rows[sd] = q.cpml_rows[sd];
+        f.psi_e_in[sd] = from_io ? h->psi_e[in_set][sd].ptr : h->spsi_e[src][sd].ptr;
+        f.psi_h_in[sd] = from_io ? h->psi_h[in_set][sd].ptr : h->spsi_h[src][sd].ptr;
+        f.psi_e_out[sd] = to_io ? h->psi_e[out_set][sd].ptr : h->spsi_e[dst][sd].ptr;
+        f.psi_h_out[sd] = to_io ? h->psi_h[out_set][sd].ptr : h->spsi_h[dst][sd].ptr;
+    }
+    f.n_lines = q.n_lines;
+    for (int l = 0; l < q.n_lines; ++l) f.lines[l] = q.lines[l];
+    f.line_values = q.line_values;
+    f.values_stride = q.values_stride;
+    f.k_col = q.k0 + (k - 1);
+    f.n_mons = q.n_mons;
+    for (int m = 0; m < q.n_mons; ++m) f.mons[m] = q.mons[m];
+    f.sample_slot = ((q.sample_mask >> (k - 1)) & 1u) ? __builtin_popcount(q.sample_mask & ((1u << (k - 1)) - 1u)) : -1;
+    Rect sh{0, 0, 0, 0};
+    if (in) {
+        f.in_r0 = in->r0, f.in_r1 = in->r1, f.in_c0 = in->c0, f.in_c1 = in->c1;
+        const int w = T - k;
+        sh = *in;
+        if (!g.periodic_x) sh.r0 += w, sh.r1 -= w;
+        if (!g.periodic_y) sh.c0 += w, sh.c1 -= w;
+    }
+    Rect region[4];
+    int n_region = 0;
+    if (sh.r1 > sh.r0 && sh.c1 > sh.c0) {
+        region[n_region++] = Rect{0, sh.r0, 0, g.ny};
+        region[n_region++] = Rect{sh.r1, g.nx, 0, g.ny};
+        region[n_region++] = Rect{sh.r0, sh.r1, 0, sh.c0};
+        region[n_region++] = Rect{sh.r0, sh.r1, sh.c1, g.ny};
+    } else {
+        region[n_region++] = Rect{0, g.nx, 0, g.ny};
+    }
+    f.n_rects = 0;
+    f.first[0] = 0;
+    for (int r = 0; r < n_region; ++r) {
+        const Rect &rc = region[r];
+        if (rc.r1 <= rc.r0 || rc.c1 <= rc.c0) continue;
+        const int n = f.n_rects++;
+        f.r0[n] = rc.r0, f.r1[n] = rc.r1, f.c0[n] = rc.c0, f.c1[n] = rc.c1;
+        f.first[n + 1] = f.first[n] + (int64_t)(rc.r1 - rc.r0) * (rc.c1 - rc.c0);
+    }
+    return f;
+}
+
+// The frame of one blocked launch of T steps: T single-step launches of ez2d_frame_step_kernel on stream `s`.
+// `tmpl` (NULL: built here) holds the launch's T step parameters for its buffer parity, made by make_frame_params
+// from the same plan; only the value column and the sample slot of each step are set here from `q`.
+static int launch_frame_chain(OsFdtd2D *h, int T, const TBParams &q, const Rect *in, cudaStream_t s,
+                              const EzFrameParams *tmpl) {
     for (int k = 1; k <= T; ++k) {
-        EzFrameParams f{};
-        f.nx = g.nx, f.ny = g.ny, f.px = g.periodic_x, f.py = g.periodic_y, f.npml = g.npml;
-        f.cpml_mask = g.cpml_sides;
-        f.ca = q.ca, f.cb = q.cb, f.da = q.da, f.db = q.db, f.da_u = q.da_u, f.db_u = q.db_u;
-        f.inv_dx_e = q.inv_dx_e, f.inv_dx_h = q.inv_dx_h, f.inv_dy_e = q.inv_dy_e, f.inv_dy_h = q.inv_dy_h;
-        const bool from_io = k == 1, to_io = k == T;
-        const int src = (k - 2) % 2, dst = (k - 1) % 2;
-        f.ez_in = from_io ? h->ez[in_set].ptr : h->sez[src].ptr;
-        f.hx_in = from_io ? h->hx[in_set].ptr : h->shx[src].ptr;
-        f.hy_in = from_io ? h->hy[in_set].ptr : h->shy[src].ptr;
-        f.ez_out = to_io ? h->ez[out_set].ptr : h->sez[dst].ptr;
-        f.hx_out = to_io ? h->hx[out_set].ptr : h->shx[dst].ptr;
-        f.hy_out = to_io ? h->hy[out_set].ptr : h->shy[dst].ptr;
-        for (int sd = 0; sd < 4; ++sd) {
-            f.cpml_rows[sd] = q.cpml_rows[sd];
-            f.psi_e_in[sd] = from_io ? h->psi_e[in_set][sd].ptr : h->spsi_e[src][sd].ptr;
-            f.psi_h_in[sd] = from_io ? h->psi_h[in_set][sd].ptr : h->spsi_h[src][sd].ptr;
-            f.psi_e_out[sd] = to_io ? h->psi_e[out_set][sd].ptr : h->spsi_e[dst][sd].ptr;
-            f.psi_h_out[sd] = to_io ? h->psi_h[out_set][sd].ptr : h->spsi_h[dst][sd].ptr;
-        }
-        f.n_lines = q.n_lines;
-        for (int l = 0; l < q.n_lines; ++l) f.lines[l] = q.lines[l];
+        EzFrameParams f = tmpl ? tmpl[k - 1] : make_frame_params(h, T, k, q, in, h->cur, h->cur ^ 1);
         f.line_values = q.line_values;
         f.values_stride = q.values_stride;
         f.k_col = q.k0 + (k - 1);
-        f.n_mons = q.n_mons;
-        for (int m = 0; m < q.n_mons; ++m) f.mons[m] = q.mons[m];
         f.sample_slot = ((q.sample_mask >> (k - 1)) & 1u) ? __builtin_popcount(q.sample_mask & ((1u << (k - 1)) - 1u))
                                                          : -1;
-        // the interior (its cells are the interior kernel's) and this step's region around it shrunk by T - k
-        Rect sh{0, 0, 0, 0};
-        if (in) {
-            f.in_r0 = in->r0, f.in_r1 = in->r1, f.in_c0 = in->c0, f.in_c1 = in->c1;
-            const int w = T - k;
-            sh = *in;
-            if (!g.periodic_x) sh.r0 += w, sh.r1 -= w;
-            if (!g.periodic_y) sh.c0 += w, sh.c1 -= w;
-        }
-        std::vector<Rect> region;
-        if (sh.r1 > sh.r0 && sh.c1 > sh.c0) {
-            region = {Rect{0, sh.r0, 0, g.ny}, Rect{sh.r1, g.nx, 0, g.ny}, Rect{sh.r0, sh.r1, 0, sh.c0},
-                      Rect{sh.r0, sh.r1, sh.c1, g.ny}};
-        } else {
-            region = {Rect{0, g.nx, 0, g.ny}};
-        }
-        f.n_rects = 0;
-        f.first[0] = 0;
-        for (const Rect &r : region) {
-            if (r.r1 <= r.r0 || r.c1 <= r.c0) continue;
-            const int n = f.n_rects++;
-            f.r0[n] = r.r0, f.r1[n] = r.r1, f.c0[n] = r.c0, f.c1[n] = r.c1;
-            f.first[n + 1] = f.first[n] + (int64_t)(r.r1 - r.r0) * (r.c1 - r.c0);
-        }
         const int64_t cells_k = f.first[f.n_rects];
         if (cells_k == 0) continue;
         OS_TRY(prof_begin(h, 1, s));
@@ -795,7 +863,8 @@ static int launch_frame_chain(OsFdtd2D *h, int T, const TBParams &q, const Rect 
 // One blocked launch: the border (general) kernel forks onto the side stream and overlaps the interior kernel; both
 // read the same input buffers and write disjoint cells of the output buffers, and the main stream waits for both.
 template <int T>
-static int launch_tb(OsFdtd2D *h, const TBParams &interior, const TBParams &general, bool has_interior) {
+static int launch_tb(OsFdtd2D *h, const TBParams &interior, const TBParams &general, bool has_interior,
+                     const EzFrameParams *frame_tmpl = nullptr) {
     const dim3 threads(TB_WARPS * 32);
     const bool run_interior = has_interior && interior.n_tiles;
     const bool fork = run_interior && general.n_tiles;
@@ -809,7 +878,7 @@ static int launch_tb(OsFdtd2D *h, const TBParams &interior, const TBParams &gene
         Rect in{};
         if (run_interior) in = Rect{interior.rects[0].r0, interior.rects[0].r1, interior.rects[0].c0,
                                     interior.rects[0].c1};
-        OS_TRY(launch_frame_chain(h, T, general, run_interior ? &in : nullptr, gstream));
+        OS_TRY(launch_frame_chain(h, T, general, run_interior ? &in : nullptr, gstream, frame_tmpl));
     } else if (general.n_tiles) {
         const dim3 blocks((unsigned)((general.n_tiles + TB_WARPS - 1) / TB_WARPS));
         OS_TRY(prof_begin(h, 1, gstream));
@@ -832,12 +901,13 @@ static int launch_tb(OsFdtd2D *h, const TBParams &interior, const TBParams &gene
     return OS_OK;
 }
 
-static int launch_tb_any(OsFdtd2D *h, int T, const TBParams &interior, const TBParams &general, bool has_interior) {
+static int launch_tb_any(OsFdtd2D *h, int T, const TBParams &interior, const TBParams &general, bool has_interior,
+                         const EzFrameParams *frame_tmpl = nullptr) {
     switch (T) {
-        case 1: return launch_tb<1>(h, interior, general, has_interior);
-        case 2: return launch_tb<2>(h, interior, general, has_interior);
-        case 3: return launch_tb<3>(h, interior, general, has_interior);
-        default: return launch_tb<4>(h, interior, general, has_interior);
+        case 1: return launch_tb<1>(h, interior, general, has_interior, frame_tmpl);
+        case 2: return launch_tb<2>(h, interior, general, has_interior, frame_tmpl);
+        case 3: return launch_tb<3>(h, interior, general, has_interior, frame_tmpl);
+        default: return launch_tb<4>(h, interior, general, has_interior, frame_tmpl);
     }
 }
 
@@ -862,14 +932,42 @@ static void bind_buffers(OsFdtd2D *h, TBParams &q, int in, int out) {
 static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples,
                            const float *values, const float *phase_table) {
     const int64_t m = h->sample_interval;
+    // The plan of a launch depends only on its length T (the full steps_per_launch, or a shorter last one): tiles,
+    // coefficients, sources, monitors, and the frame steps' regions for both buffer parities.  Each launch then only
+    // sets its buffers, first step and sample mask.
+    struct LaunchPlan {
+        int T = 0;
+        TBParams interior{}, general{};
+        bool has_interior = false;
+        std::vector<EzFrameParams> frame[2];   // [input buffer set][step - 1]
+    };
+    LaunchPlan plans[2];
+    auto plan_for = [&](int T) -> LaunchPlan & {
+        for (LaunchPlan &pl : plans)
+            if (pl.T == T) return pl;
+        LaunchPlan &pl = plans[plans[0].T ? 1 : 0];
+        pl = LaunchPlan{};
+        pl.T = T;
+        plan_tiles(h, T, pl.interior, pl.general, pl.has_interior);
+        fill_common(h, pl.interior);
+        fill_common(h, pl.general);
+        if (h->variant == 1 && pl.general.n_tiles) {
+            const bool run_interior = pl.has_interior && pl.interior.n_tiles;
+            const Rect box = run_interior ? Rect{pl.interior.rects[0].r0, pl.interior.rects[0].r1,
+                                                 pl.interior.rects[0].c0, pl.interior.rects[0].c1}
+                                          : Rect{0, 0, 0, 0};
+            for (int par = 0; par < 2; ++par)
+                for (int k = 1; k <= T; ++k)
+                    pl.frame[par].push_back(
+                        make_frame_params(h, T, k, pl.general, run_interior ? &box : nullptr, par, par ^ 1));
+        }
+        return pl;
+    };
     int64_t k = 0;
     while (k < n_steps) {
         const int T = (int)std::min<int64_t>(h->steps_per_launch, n_steps - k);
-        TBParams interior{}, general{};
-        bool has_interior = false;
-        plan_tiles(h, T, interior, general, has_interior);
-        fill_common(h, interior);
-        fill_common(h, general);
+        LaunchPlan &pl = plan_for(T);
+        TBParams interior = pl.interior, general = pl.general;
         const int in = h->cur, out = h->cur ^ 1;
         for (TBParams *q : {&interior, &general}) {
             bind_buffers(h, *q, in, out);
@@ -883,7 +981,8 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
                 if ((h->n_step + st) % m == 0) q->sample_mask |= 1u << (st - 1);
             if (h->fluxes.empty()) q->sample_mask = 0;
         }
-        OS_TRY(launch_tb_any(h, T, interior, general, has_interior));
+        OS_TRY(launch_tb_any(h, T, interior, general, pl.has_interior,
+                             pl.frame[in].empty() ? nullptr : pl.frame[in].data()));
         h->cur = out;
         // DFT samples taken inside this launch, accumulated in sample order
         const int64_t q_lo = h->n_step / m + 1, q_hi = (h->n_step + T) / m;
@@ -1295,7 +1394,7 @@ extern "C" int os_fdtd2d_configure(OsFdtd2D *h, int32_t variant, int32_t steps_p
         h->hz_rows = tile_rows;
         return OS_OK;
     }
-    OS_CHECK(tile_rows >= 1, OS_ERR_INVALID, "tile_rows must be >= 1, got %d", tile_rows);
+    OS_CHECK(tile_rows >= 0, OS_ERR_INVALID, "tile_rows must be >= 0 (0: chosen from the grid), got %d", tile_rows);
     h->variant = variant;
     h->steps_per_launch = steps_per_launch;
     h->tile_rows = tile_rows;
@@ -1525,8 +1624,15 @@ struct BatchGroup {                    // one kernel launch of a batched step: j
     size_t params_off = 0, tiles_off = 0;
 };
 
+struct FrameStep {                     // one frame step of a batched blocked launch: the jobs' regions
+    std::vector<EzFrameParams> params;
+    std::vector<int32_t> block_start{0};   // 256-thread blocks per job, cumulative
+    size_t params_off = 0, starts_off = 0;
+};
+
 struct BatchLaunch {
     int T;
+    std::vector<FrameStep> frames;     // steps 1..T
     std::vector<BatchGroup> groups;
     std::vector<FluxBatchItem> items;
     int max_item_cells = 0;
@@ -1542,7 +1648,7 @@ static BatchGroup &batch_group(BatchLaunch &L, int kind, bool ca, bool px, bool 
 
 template <int T, bool CA, bool PX, bool PY>
 static int launch_interior_batch(cudaStream_t s, const TBParams *jobs, const int *tiles, int n_jobs, int total) {
-    const size_t smem = (size_t)TB_WARPS * tb_warp_smem_bytes(T, CA);
+    const size_t smem = (size_t)TB_WARPS * ip_warp_smem_bytes(T, CA);
     static bool attr_set = false;
     if (!attr_set) {
         OS_CUDA(cudaFuncSetAttribute(ez2d_interior_batch_kernel<T, CA, PX, PY>,
@@ -1670,10 +1776,24 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
         TBParams interior{}, general{};
         bool has_interior = false;
     };
+    // one tile height for the jobs that leave it to the plan: the jobs' interior tiles together fill the device's
+    // warp slots once (8..128 rows), so a large batch gets tall tiles and the last few jobs short ones
+    int batch_rows = 0;
+    {
+        int64_t tile_rows_total = 0;
+        for (int32_t q = 0; q < n_jobs; ++q) {
+            Rect in{};
+            if (interior_rect(handles[q], T, in))
+                tile_rows_total += (int64_t)(in.r1 - in.r0) * ((in.c1 - in.c0 + 119) / 120);
+        }
+        const int64_t slots = (int64_t)handles[0]->sm_count * 4 * TB_WARPS;
+        batch_rows = (int)std::max<int64_t>(8, std::min<int64_t>(128, tile_rows_total / std::max<int64_t>(1, slots)));
+    }
     std::vector<Plan> plan_full(n_jobs), plan_last(n_jobs);
     for (int32_t q = 0; q < n_jobs; ++q) {
-        plan_tiles(handles[q], T, plan_full[q].interior, plan_full[q].general, plan_full[q].has_interior);
-        plan_tiles(handles[q], T_last, plan_last[q].interior, plan_last[q].general, plan_last[q].has_interior);
+        const int rows = handles[q]->tile_rows > 0 ? 0 : batch_rows;
+        plan_tiles(handles[q], T, plan_full[q].interior, plan_full[q].general, plan_full[q].has_interior, rows);
+        plan_tiles(handles[q], T_last, plan_last[q].interior, plan_last[q].general, plan_last[q].has_interior, rows);
         for (Plan *pl : {&plan_full[q], &plan_last[q]}) {
             fill_common(handles[q], pl->interior);
             fill_common(handles[q], pl->general);
@@ -1683,6 +1803,7 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
     for (int64_t l = 0; l < n_launch; ++l) {
         BatchLaunch &L = launches[(size_t)l];
         L.T = l + 1 < n_launch ? T : T_last;
+        L.frames.resize((size_t)L.T);
         for (int32_t q = 0; q < n_jobs; ++q) {
             OsFdtd2D *h = handles[q];
             const Plan &pl = l + 1 < n_launch ? plan_full[q] : plan_last[q];
@@ -1692,9 +1813,31 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
             for (int st = 1; st <= L.T; ++st)
                 if ((n0 + st) % m == 0) mask |= 1u << (st - 1);
             if (h->fluxes.empty()) mask = 0;
+            if (h->variant == 1 && pl.general.n_tiles) {
+                // the frame: one batched single-step launch per step over the jobs' shrinking bands
+                TBParams base = pl.general;
+                bind_buffers(h, base, in, out);
+                base.line_values = h->line_values.ptr;
+                base.values_stride = n_steps;
+                base.k0 = l * T;
+                base.sample_mask = mask;
+                const bool run_interior = pl.has_interior && pl.interior.n_tiles;
+                const Rect box = run_interior ? Rect{pl.interior.rects[0].r0, pl.interior.rects[0].r1,
+                                                     pl.interior.rects[0].c0, pl.interior.rects[0].c1}
+                                              : Rect{0, 0, 0, 0};
+                for (int k = 1; k <= L.T; ++k) {
+                    const EzFrameParams f = make_frame_params(h, L.T, k, base, run_interior ? &box : nullptr, in, out);
+                    const int64_t cells_k = f.first[f.n_rects];
+                    if (!cells_k) continue;
+                    FrameStep &fs = L.frames[(size_t)(k - 1)];
+                    fs.params.push_back(f);
+                    fs.block_start.push_back(fs.block_start.back() + (int32_t)((cells_k + 255) / 256));
+                }
+            }
             for (int kind = 1; kind >= 0; --kind) {
                 const TBParams &base = kind == 0 ? pl.interior : pl.general;
                 if (kind == 0 && !pl.has_interior) continue;
+                if (kind == 1 && h->variant == 1) continue;   // advanced by the frame steps above
                 if (!base.n_tiles) continue;
                 BatchGroup &g = batch_group(L, kind, h->has_ca, kind == 0 && h->grid.periodic_x,
                                             kind == 0 && h->grid.periodic_y);
@@ -1731,6 +1874,13 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
     // one page-locked block for the whole call, one copy to the device
     size_t total = 0;
     for (auto &L : launches) {
+        for (auto &fs : L.frames) {
+            if (fs.params.empty()) continue;
+            fs.params_off = total = align_up(total, 16);
+            total += fs.params.size() * sizeof(EzFrameParams);
+            fs.starts_off = total = align_up(total, 16);
+            total += fs.block_start.size() * sizeof(int32_t);
+        }
         for (auto &g : L.groups) {
             g.params_off = total = align_up(total, 16);
             total += g.params.size() * sizeof(TBParams);
@@ -1752,6 +1902,11 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
         b->host_capacity = total;
     }
     for (auto &L : launches) {
+        for (auto &fs : L.frames) {
+            if (fs.params.empty()) continue;
+            memcpy(b->host + fs.params_off, fs.params.data(), fs.params.size() * sizeof(EzFrameParams));
+            memcpy(b->host + fs.starts_off, fs.block_start.data(), fs.block_start.size() * sizeof(int32_t));
+        }
         for (auto &g : L.groups) {
             memcpy(b->host + g.params_off, g.params.data(), g.params.size() * sizeof(TBParams));
             memcpy(b->host + g.tiles_off, g.tile_start.data(), g.tile_start.size() * sizeof(int));
@@ -1764,6 +1919,13 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
     b->copy_pending = true;
     OS_CUDA(cudaEventRecord(b->ev_start, b->stream));
     for (auto &L : launches) {
+        for (auto &fs : L.frames) {
+            if (fs.params.empty()) continue;
+            ez2d_frame_step_batch_kernel<<<(unsigned)fs.block_start.back(), 256, 0, b->stream>>>(
+                reinterpret_cast<const EzFrameParams *>(b->dev.ptr + fs.params_off),
+                reinterpret_cast<const int32_t *>(b->dev.ptr + fs.starts_off), (int)fs.params.size());
+            b->launches += 1;
+        }
         for (auto &g : L.groups) {
             if (g.kind != 1) continue;
             OS_TRY(launch_group_any(L.T, b->stream, g, b->dev.ptr));

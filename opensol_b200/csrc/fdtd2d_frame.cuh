@@ -40,6 +40,7 @@ struct EzFrameParams {
     int32_t r0[4], r1[4], c0[4], c1[4];
     int64_t first[5];                 // cell offsets of the rectangles
 };
+static_assert(sizeof(EzFrameParams) % 4 == 0, "EzFrameParams is copied as 32-bit words");
 
 __device__ __forceinline__ float ezf_wrap_hi(float w) { return w * 1.0f + w * 0.0f; }
 
@@ -106,11 +107,13 @@ __device__ __forceinline__ float ezf_hy_at(const EzFrameParams &p, int i, int j,
     return v;
 }
 
-__global__ void __launch_bounds__(256) ez2d_frame_step_kernel(const EzFrameParams p) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t total = p.n_rects == 1 ? p.first[1] : p.n_rects == 2 ? p.first[2]
-                          : p.n_rects == 3 ? p.first[3] : p.first[4];
-    if (t >= total) return;
+// Cells of a step's region.
+__device__ __forceinline__ int64_t ezf_cells(const EzFrameParams &p) {
+    return p.n_rects == 1 ? p.first[1] : p.n_rects == 2 ? p.first[2] : p.n_rects == 3 ? p.first[3] : p.first[4];
+}
+
+// The step of the region's t-th cell (t < ezf_cells(p)).
+__device__ __forceinline__ void ezf_cell(const EzFrameParams &p, int64_t t) {
     // the rectangle of this cell, selected without indexing the parameter arrays by a runtime value
     int k = 0;
     if (p.n_rects > 1 && t >= p.first[1]) k = 1;
@@ -188,4 +191,32 @@ __global__ void __launch_bounds__(256) ez2d_frame_step_kernel(const EzFrameParam
             }
         }
     }
+}
+
+__global__ void __launch_bounds__(256) ez2d_frame_step_kernel(const EzFrameParams p) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < ezf_cells(p)) ezf_cell(p, t);
+}
+
+// One frame step of several simulations in one launch.  Each block serves one job: job q owns blocks
+// [block_start[q], block_start[q + 1]) and its cells in order; the block copies the job's parameters into shared
+// memory once, so the per-cell code reads them from there.
+__global__ void __launch_bounds__(256) ez2d_frame_step_batch_kernel(const EzFrameParams *__restrict__ jobs,
+                                                                    const int32_t *__restrict__ block_start,
+                                                                    int n_jobs) {
+    __shared__ __align__(16) unsigned char smem[sizeof(EzFrameParams)];
+    const int b = blockIdx.x;
+    int lo = 0, hi = n_jobs - 1;   // the job q with block_start[q] <= b < block_start[q + 1]
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (block_start[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(jobs + lo);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(smem);
+    for (int w = threadIdx.x; w < (int)(sizeof(EzFrameParams) / 4); w += blockDim.x) dst[w] = src[w];
+    __syncthreads();
+    const EzFrameParams &p = *reinterpret_cast<const EzFrameParams *>(smem);
+    const int64_t t = (int64_t)(b - block_start[lo]) * blockDim.x + threadIdx.x;
+    if (t < ezf_cells(p)) ezf_cell(p, t);
 }

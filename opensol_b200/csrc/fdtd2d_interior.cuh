@@ -15,6 +15,17 @@
 
 #include "fdtd2d_tb.cuh"
 
+// Floats of one staged row window in shared memory: the 128 columns plus room for a copy that starts up to 3 floats
+// before them (rounded down to a 16-byte boundary when the row length is not a multiple of 4) and is rounded up to
+// 16 bytes.
+#define IP_ROW 136
+
+// Shared memory of one warp of the interior kernel: field ring (TB_AHEAD + 1 slots x E, H_x, H_y windows),
+// coefficient rings (T + TB_AHEAD + 1 slots of cb, and of ca when per-cell), one mbarrier per field slot.
+__host__ __device__ constexpr int ip_warp_smem_bytes(int T, bool ca) {
+    return (tb_field_slots() * 3 + tb_coef_slots(T) * (ca ? 2 : 1)) * IP_ROW * 4 + tb_field_slots() * 8;
+}
+
 // packed add / subtract: only for operands that are not products (see above)
 __device__ __forceinline__ float2 ip_sub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
 __device__ __forceinline__ float2 ip_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
@@ -37,6 +48,7 @@ struct IPWarp {
     bool wrap_lo0;         // PY: the first column is column 0 (its lo neighbour is the wrapped last column)
     uint32_t line_mask, mon_mask, sample_mask;
     int nx, ny;
+    bool vec;              // ny % 4 == 0: every row window starts 16-byte aligned (float4 reads and stores)
     float2 db2, ixh2, ixe2, iyh2, iye2;
     float *ez_out, *hx_out, *hy_out;
     const float *__restrict__ ez_in, *__restrict__ hx_in, *__restrict__ hy_in, *__restrict__ cbp, *__restrict__ cap;
@@ -52,7 +64,24 @@ struct IPWarp {
 
     __device__ __forceinline__ int phys_row(int i) const { return PX ? tb_wrap(i, nx) : i; }
 
+    // Offset (0..3 floats) of row R's first window column behind the 16-byte boundary its copy starts on (0 when
+    // ny % 4 == 0; the host plans an interior on a row length that is not a multiple of 4 only for a non-periodic y).
+    __device__ __forceinline__ int row_off(int R) const {
+        return vec ? 0 : (int)(((size_t)phys_row(R) * (size_t)ny + (size_t)(j0 - 4)) & 3u);
+    }
+
+    // Bulk copies of one row window (columns j0 - 4 .., 128 of them, clipped to the grid) into dst; returns the
+    // bytes.  A row that does not start 16-byte aligned is copied from the boundary before it, rounded up to 16
+    // bytes (the data then starts at dst + row_off).
     __device__ __forceinline__ uint32_t window(float *dst, const float *src_row, uint64_t *bar, bool issue) const {
+        if (!vec) {
+            const int col = j0 - 4;
+            const int len = min(128, ny - col);
+            const int off = (int)(((uintptr_t)(src_row + col) >> 2) & 3u);
+            const uint32_t bytes = (uint32_t)((len + off + 3) & ~3) * 4u;
+            if (issue) tb_bulk_g2s(dst, src_row + col - off, bytes, bar);
+            return bytes;
+        }
         uint32_t bytes = 0;
         int remaining = 128, d = 0, col = PY ? tb_wrap(j0 - 4, ny) : j0 - 4;
         while (remaining > 0 && col < ny) {
@@ -73,13 +102,21 @@ struct IPWarp {
         const int fs = k % tb_field_slots(), cs = k % tb_coef_slots(T);
         uint64_t *bar = sm_bar + fs;
         const size_t base = (size_t)phys_row(R) * (size_t)ny;
-        tb_mbar_expect_tx(bar, row_bytes * (CA ? 5u : 4u));
-        float *f = sm_fields + fs * 384;
+        // every array of the row has the same alignment (the arrays start 256-byte aligned), so the same byte count
+        const uint32_t bytes = vec ? row_bytes : window(nullptr, ez_in + base, nullptr, false);
+        tb_mbar_expect_tx(bar, bytes * (CA ? 5u : 4u));
+        float *f = sm_fields + fs * (3 * IP_ROW);
         window(f, ez_in + base, bar, true);
-        window(f + 128, hx_in + base, bar, true);
-        window(f + 256, hy_in + base, bar, true);
-        window(sm_cb + cs * 128, cbp + base, bar, true);
-        if (CA) window(sm_ca + cs * 128, cap + base, bar, true);
+        window(f + IP_ROW, hx_in + base, bar, true);
+        window(f + 2 * IP_ROW, hy_in + base, bar, true);
+        window(sm_cb + cs * IP_ROW, cbp + base, bar, true);
+        if (CA) window(sm_ca + cs * IP_ROW, cap + base, bar, true);
+    }
+
+    // four consecutive floats of a staged window (16-byte aligned when vec)
+    __device__ __forceinline__ float4 ld_win(const float *q) const {
+        if (vec) return *reinterpret_cast<const float4 *>(q);
+        return make_float4(q[0], q[1], q[2], q[3]);
     }
 
     template <int PH>
@@ -87,10 +124,10 @@ struct IPWarp {
         const int k = R - r_begin;
         const int fs = k % tb_field_slots();
         if (R <= r_end && !tb_mbar_wait(sm_bar + fs, (uint32_t)((k / tb_field_slots()) & 1))) return false;
-        const float *f = sm_fields + fs * 384 + lane * 4;
-        const float4 e = *reinterpret_cast<const float4 *>(f);
-        const float4 hx = *reinterpret_cast<const float4 *>(f + 128);
-        const float4 hy = *reinterpret_cast<const float4 *>(f + 256);
+        const float *f = sm_fields + fs * (3 * IP_ROW) + row_off(R) + lane * 4;
+        const float4 e = ld_win(f);
+        const float4 hx = ld_win(f + IP_ROW);
+        const float4 hy = ld_win(f + 2 * IP_ROW);
         E[PH][0][0] = make_float2(e.x, e.y);
         E[PH][0][1] = make_float2(e.z, e.w);
         Hx[PH][0][0] = make_float2(hx.x, hx.y);
@@ -152,11 +189,12 @@ struct IPWarp {
         const int i = r - S;
         const int ip = phys_row(i);
         const int cs = (i - r_begin + tb_coef_slots(T)) % tb_coef_slots(T);
-        const float4 cbv = *reinterpret_cast<const float4 *>(sm_cb + cs * 128 + lane * 4);
+        const int co = row_off(i) + lane * 4;
+        const float4 cbv = ld_win(sm_cb + cs * IP_ROW + co);
         const float2 cb[2] = {make_float2(cbv.x, cbv.y), make_float2(cbv.z, cbv.w)};
         float2 ca[2];
         if constexpr (CA) {
-            const float4 cav = *reinterpret_cast<const float4 *>(sm_ca + cs * 128 + lane * 4);
+            const float4 cav = ld_win(sm_ca + cs * IP_ROW + co);
             ca[0] = make_float2(cav.x, cav.y);
             ca[1] = make_float2(cav.z, cav.w);
         }
@@ -201,7 +239,7 @@ struct IPWarp {
         const int i = r - T;
         if (i < i0 || i >= i1) return;
         const size_t base = (size_t)phys_row(i) * (size_t)ny + jp0;
-        if (own == 0xFu) {
+        if (own == 0xFu && vec) {
             *reinterpret_cast<float4 *>(ez_out + base) =
                 make_float4(E[PH][T][0].x, E[PH][T][0].y, E[PH][T][1].x, E[PH][T][1].y);
             *reinterpret_cast<float4 *>(hx_out + base) =
@@ -266,6 +304,7 @@ __device__ __forceinline__ void ez2d_interior_tile(const TBParams &p, int w, uns
     W.lane = lane;
     W.nx = p.nx;
     W.ny = p.ny;
+    W.vec = p.ny % 4 == 0;
     W.j0 = R.c0 + tc * p.tile_w;
     W.j1 = min(W.j0 + p.tile_w, R.c1);
     W.i0 = R.r0 + tr * p.tile_rows;
@@ -323,12 +362,12 @@ __device__ __forceinline__ void ez2d_interior_tile(const TBParams &p, int w, uns
 #pragma unroll
             for (int k = 0; k < 2; ++k) W.E[ph][s][k] = W.Hx[ph][s][k] = W.Hy[ph][s][k] = make_float2(0.0f, 0.0f);
 
-    unsigned char *mine = tb_smem + (threadIdx.x >> 5) * tb_warp_smem_bytes(T, CA);
+    unsigned char *mine = tb_smem + (threadIdx.x >> 5) * ip_warp_smem_bytes(T, CA);
     W.sm_fields = reinterpret_cast<float *>(mine);
-    W.sm_cb = W.sm_fields + tb_field_slots() * 384;
-    W.sm_ca = W.sm_cb + tb_coef_slots(T) * 128;
-    W.sm_bar = reinterpret_cast<uint64_t *>(W.sm_cb + tb_coef_slots(T) * 128 * (CA ? 2 : 1));
-    W.row_bytes = W.window(nullptr, nullptr, nullptr, false);
+    W.sm_cb = W.sm_fields + tb_field_slots() * 3 * IP_ROW;
+    W.sm_ca = W.sm_cb + tb_coef_slots(T) * IP_ROW;
+    W.sm_bar = reinterpret_cast<uint64_t *>(W.sm_cb + tb_coef_slots(T) * IP_ROW * (CA ? 2 : 1));
+    W.row_bytes = W.vec ? W.window(nullptr, nullptr, nullptr, false) : 0u;
     if (lane == 0) {
         for (int q = 0; q < tb_field_slots(); ++q) tb_mbar_init(W.sm_bar + q, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -356,7 +395,7 @@ __device__ __forceinline__ void ez2d_interior_tile(const TBParams &p, int w, uns
 }
 
 template <int T, bool CA, bool PX, bool PY>
-__global__ void __launch_bounds__(TB_WARPS * 32) ez2d_interior_kernel(const TBParams p) {
+__global__ void __launch_bounds__(TB_WARPS * 32, 4) ez2d_interior_kernel(const TBParams p) {
     extern __shared__ __align__(16) unsigned char tb_smem[];
     ez2d_interior_tile<T, CA, PX, PY>(p, blockIdx.x * TB_WARPS + (threadIdx.x >> 5), tb_smem);
 }
@@ -364,7 +403,7 @@ __global__ void __launch_bounds__(TB_WARPS * 32) ez2d_interior_kernel(const TBPa
 // Several simulations in one launch: warp g runs tile g - tile_start[job] of jobs[job], tile_start ascending with
 // tile_start[n_jobs] = the total (every job shares T and the template configuration).
 template <int T, bool CA, bool PX, bool PY>
-__global__ void __launch_bounds__(TB_WARPS * 32) ez2d_interior_batch_kernel(const TBParams *__restrict__ jobs,
+__global__ void __launch_bounds__(TB_WARPS * 32, 4) ez2d_interior_batch_kernel(const TBParams *__restrict__ jobs,
                                                                          const int *__restrict__ tile_start,
                                                                          int n_jobs) {
     extern __shared__ __align__(16) unsigned char tb_smem[];

@@ -50,7 +50,7 @@ class FDTDEngine2D_Ez:
         self._materials_version = None
         self.sample_interval = 1
         self._sample_interval_sent = None
-        self.variant, self.steps_per_launch, self.tile_rows = 1, 3, 128
+        self.variant, self.steps_per_launch, self.tile_rows = 1, 3, 0
         self._config_sent = None
         self.h2d_bytes = 0   # host-to-device bytes this engine has uploaded (setup, materials, chunk tables)
 
@@ -145,8 +145,9 @@ class FDTDEngine2D_Ez:
 
     def configure(self, variant=None, steps_per_launch=None, tile_rows=None):
         """Kernel choice (results are bit-identical for every choice): variant 1 = temporally blocked kernels
-        advancing steps_per_launch (1..4, default 3) steps per launch with tile_rows rows per interior tile; variant
-        2 = the same with the general kernel on every cell; variant 0 = one H and one E kernel per step."""
+        advancing steps_per_launch (1..4, default 3) steps per launch with tile_rows rows per interior tile (0, the
+        default: chosen from the grid), the frame one step per launch; variant 2 = the same with the blocked general
+        kernel on the frame; variant 0 = one H and one E kernel per step."""
         if variant is not None:
             self.variant = int(variant)
         if steps_per_launch is not None:

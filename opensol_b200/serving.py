@@ -129,7 +129,7 @@ def make_job_specs(n_jobs=256, rate=20.0, seed=7, side_range=(256, 2048), steps_
     return specs
 
 
-def build_job(spec, device=0, steps_per_launch=3, tile_rows=32):
+def build_job(spec, device=0, steps_per_launch=3, tile_rows=0):
     """(Simulation, flux monitors) of a request, finalized and on the device."""
     from .simulation import Simulation
     window = spec.side * spec.dx
@@ -175,7 +175,7 @@ class ServingLoop:
     """Admission by memory budget and slots, all active jobs stepped together in batched launches."""
 
     def __init__(self, device=0, memory_budget=120e9, max_active=48, chunk_steps=512, steps_per_launch=3,
-                 tile_rows=32):
+                 tile_rows=0):
         self.device = int(device)
         self.memory_budget = float(memory_budget)
         self.max_active = int(max_active)
@@ -236,13 +236,16 @@ class ServingLoop:
         return results
 
     def close(self):
+        """Release the batch and the device memory the finished jobs left in the engines' pool."""
         self.advancer.close()
+        _native.check(_native.load().os_fdtd_pool_trim())
 
 
-def run_alone(spec, device=0, steps_per_launch=3, tile_rows=None):
-    """One job on its own (the plain one-at-a-time run): (fluxes, wall seconds); tile_rows None = autotuned."""
+def run_alone(spec, device=0, steps_per_launch=3, tile_rows=0):
+    """One job on its own (the plain one-at-a-time run): (fluxes, wall seconds); tile_rows 0 = the engine's choice
+    from the grid, None = autotuned."""
     t0 = time.perf_counter()
-    sim, monitors = build_job(spec, device, steps_per_launch, tile_rows or 128)
+    sim, monitors = build_job(spec, device, steps_per_launch, tile_rows or 0)
     if tile_rows is None:
         sim.em.engine.autotune()
     sim.em.engine.advance(spec.steps)
