@@ -526,6 +526,7 @@ def run_serving(args):
                                    '1-40 rectangles eps_r U(1,12), line source U(1000,1600) nm, U(2000,20000) steps, '
                                    'two 4-frequency flux lines; Poisson 20 jobs/s for the latency run',
                        'max_active': 48, 'chunk_steps': 512, 'memory_budget_gb': 120,
+                       'steps_per_launch': {'batched': 2, 'one_at_a_time': 3},
                        'tile_rows': 'chosen per call from the active jobs (batched) / per grid (one at a time)'},
             'one_at_a_time_sims_per_s': len(specs) / t_alone, 'speedup_vs_one_at_a_time': t_alone / t_batch,
             'cell_updates_per_s_batched': work / t_batch, 'fluxes_equal_alone_and_batched': bool(same),

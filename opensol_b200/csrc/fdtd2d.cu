@@ -637,17 +637,33 @@ static bool constant_over(const std::vector<float> &v, int a, int b, float *valu
 // The interior rectangle (cells whose T-step dependency cone avoids the CPML slabs and the non-periodic edges) and the
 // border rectangles around it.  Interior rows need i0 - T >= npml + 1 and i1 - 1 + T <= nx - npml - 2 on a CPML x
 // axis; columns likewise with the 4-column left halo of the 128-bit loads.
-// Rows per interior tile when the handle leaves the choice to the plan (tile_rows 0): one wave of warps over the
-// device's resident warp slots (4 blocks of 4 warps per SM), 8..128 rows.  Each warp streams its tile's rows one
-// after the other, so a grid with fewer tiles than slots runs in the time of one tile; shorter tiles cut that time
-// until the tiles fill the slots.
-static int interior_rows(const OsFdtd2D *h, int rows, int cols, int rows_override = 0) {
+// Rows per interior tile when the choice is left to the plan (tile_rows 0), for one or several interior rectangles
+// (rows x columns) sharing a launch: each warp streams its tile's rows one after the other and blocks of 4 warps
+// run in waves of 4 per SM, so the launch takes about (whole waves) x (tile rows + the 2 T cone rows + 4 rows of
+// pipeline start).  The height in 8..128 that minimises that (the taller one on a tie).
+static int wave_rows(int sm_count, int T, const std::vector<std::pair<int, int>> &rects) {
+    const int64_t slots = (int64_t)sm_count * 4;
+    int best = 128;
+    int64_t best_cost = -1;
+    for (int R = 128; R >= 8; R -= 4) {
+        int64_t tiles = 0;
+        for (const auto &rc : rects) tiles += (int64_t)((rc.first + R - 1) / R) * ((rc.second + 119) / 120);
+        const int64_t blocks = (tiles + TB_WARPS - 1) / TB_WARPS;
+        const int64_t waves = (blocks + slots - 1) / slots;
+        const int64_t cost = waves * (R + 2 * T + 4);
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = R;
+        }
+    }
+    return best;
+}
+
+static int interior_rows(const OsFdtd2D *h, int T, int rows, int cols, int rows_override = 0) {
     if (rows_override > 0) return rows_override;
     if (h->tile_rows > 0) return h->tile_rows;
-    const int64_t tiles_c = (cols + 119) / 120;
-    const int64_t slots = (int64_t)h->sm_count * 4 * TB_WARPS;
-    const int64_t r = (int64_t)rows * tiles_c / std::max<int64_t>(1, slots);
-    return (int)std::max<int64_t>(8, std::min<int64_t>(128, r));
+    if (rows <= 0 || cols <= 0) return 128;
+    return wave_rows(h->sm_count, T, {{rows, cols}});
 }
 
 // The interior rectangle of the blocked kernels (rows [r0, r1), columns [c0, c1)), or false when there is none.
@@ -685,13 +701,13 @@ static void plan_tiles(const OsFdtd2D *h, int T, TBParams &interior, TBParams &g
     std::vector<Rect> border;
     if (!has_interior) {
         border.push_back(Rect{0, g.nx, 0, g.ny});
-        set_tiles(interior, {}, 120, interior_rows(h, 0, 0, rows_override));
+        set_tiles(interior, {}, 120, interior_rows(h, T, 0, 0, rows_override));
     } else {
         border.push_back(Rect{0, in.r0, 0, g.ny});
         border.push_back(Rect{in.r1, g.nx, 0, g.ny});
         border.push_back(Rect{in.r0, in.r1, 0, in.c0});
         border.push_back(Rect{in.r0, in.r1, in.c1, g.ny});
-        set_tiles(interior, {in}, 120, interior_rows(h, in.r1 - in.r0, in.c1 - in.c0, rows_override));
+        set_tiles(interior, {in}, 120, interior_rows(h, T, in.r1 - in.r0, in.c1 - in.c0, rows_override));
     }
     set_tiles(general, border, 32 - 2 * T, h->gen_tile_rows);
 }
@@ -1606,6 +1622,8 @@ extern "C" int os_fdtd2d_last_advance_ms(OsFdtd2D *h, float *ms) {
 struct OsFdtd2DBatch {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;          // the frame steps run here, overlapping the interior launches
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev_copied = nullptr, ev_start = nullptr, ev_stop = nullptr;
     bool copy_pending = false, timed = false;
     unsigned char *host = nullptr;     // page-locked staging of one call's launch parameters
@@ -1648,7 +1666,7 @@ static BatchGroup &batch_group(BatchLaunch &L, int kind, bool ca, bool px, bool 
 
 template <int T, bool CA, bool PX, bool PY>
 static int launch_interior_batch(cudaStream_t s, const TBParams *jobs, const int *tiles, int n_jobs, int total) {
-    const size_t smem = (size_t)TB_WARPS * ip_warp_smem_bytes(T, CA);
+    const size_t smem = (size_t)TB_WARPS * ip_warp_smem_bytes(T, CA) + (size_t)TB_WARPS * sizeof(TBParams);
     static bool attr_set = false;
     if (!attr_set) {
         OS_CUDA(cudaFuncSetAttribute(ez2d_interior_batch_kernel<T, CA, PX, PY>,
@@ -1704,6 +1722,9 @@ extern "C" int os_fdtd2d_batch_create(int32_t device, OsFdtd2DBatch **out) {
     b->device = device;
     OS_CUDA(cudaSetDevice(device));
     OS_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    OS_CUDA(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
+    OS_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+    OS_CUDA(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
     OS_CUDA(cudaEventCreateWithFlags(&b->ev_copied, cudaEventDisableTiming));
     OS_CUDA(cudaEventCreate(&b->ev_start));
     OS_CUDA(cudaEventCreate(&b->ev_stop));
@@ -1715,13 +1736,17 @@ extern "C" int os_fdtd2d_batch_destroy(OsFdtd2DBatch *b) {
     if (!b) return OS_OK;
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->side) cudaStreamSynchronize(b->side);
     if (b->host) cudaFreeHost(b->host);
     if (b->ev_copied) cudaEventDestroy(b->ev_copied);
     if (b->ev_start) cudaEventDestroy(b->ev_start);
     if (b->ev_stop) cudaEventDestroy(b->ev_stop);
-    cudaStream_t s = b->stream;
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    cudaStream_t s = b->stream, side = b->side;
     delete b;
     if (s) cudaStreamDestroy(s);
+    if (side) cudaStreamDestroy(side);
     return OS_OK;
 }
 
@@ -1776,18 +1801,17 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
         TBParams interior{}, general{};
         bool has_interior = false;
     };
-    // one tile height for the jobs that leave it to the plan: the jobs' interior tiles together fill the device's
-    // warp slots once (8..128 rows), so a large batch gets tall tiles and the last few jobs short ones
+    // one tile height for the jobs that leave it to the plan, chosen for all their interior tiles together (a large
+    // batch gets tall tiles, the last few jobs short ones)
     int batch_rows = 0;
     {
-        int64_t tile_rows_total = 0;
+        std::vector<std::pair<int, int>> rects;
         for (int32_t q = 0; q < n_jobs; ++q) {
             Rect in{};
-            if (interior_rect(handles[q], T, in))
-                tile_rows_total += (int64_t)(in.r1 - in.r0) * ((in.c1 - in.c0 + 119) / 120);
+            if (handles[q]->tile_rows == 0 && interior_rect(handles[q], T, in))
+                rects.push_back({in.r1 - in.r0, in.c1 - in.c0});
         }
-        const int64_t slots = (int64_t)handles[0]->sm_count * 4 * TB_WARPS;
-        batch_rows = (int)std::max<int64_t>(8, std::min<int64_t>(128, tile_rows_total / std::max<int64_t>(1, slots)));
+        if (!rects.empty()) batch_rows = wave_rows(handles[0]->sm_count, T, rects);
     }
     std::vector<Plan> plan_full(n_jobs), plan_last(n_jobs);
     for (int32_t q = 0; q < n_jobs; ++q) {
@@ -1919,9 +1943,17 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
     b->copy_pending = true;
     OS_CUDA(cudaEventRecord(b->ev_start, b->stream));
     for (auto &L : launches) {
+        // the frame steps fork onto the side stream and overlap the interior launches (disjoint cells; both read
+        // only the launch's input state), the stream waits for them before the DFT fold
+        bool fork = false;
+        for (auto &fs : L.frames) fork = fork || !fs.params.empty();
+        if (fork) {
+            OS_CUDA(cudaEventRecord(b->ev_fork, b->stream));
+            OS_CUDA(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
+        }
         for (auto &fs : L.frames) {
             if (fs.params.empty()) continue;
-            ez2d_frame_step_batch_kernel<<<(unsigned)fs.block_start.back(), 256, 0, b->stream>>>(
+            ez2d_frame_step_batch_kernel<<<(unsigned)fs.block_start.back(), 256, 0, b->side>>>(
                 reinterpret_cast<const EzFrameParams *>(b->dev.ptr + fs.params_off),
                 reinterpret_cast<const int32_t *>(b->dev.ptr + fs.starts_off), (int)fs.params.size());
             b->launches += 1;
@@ -1935,6 +1967,10 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
             if (g.kind != 0) continue;
             OS_TRY(launch_group_any(L.T, b->stream, g, b->dev.ptr));
             b->launches += 1;
+        }
+        if (fork) {
+            OS_CUDA(cudaEventRecord(b->ev_join, b->side));
+            OS_CUDA(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
         }
         if (!L.items.empty()) {
             const dim3 grid((unsigned)((L.max_item_cells + 255) / 256), (unsigned)L.items.size());

@@ -44,16 +44,31 @@ static_assert(sizeof(EzFrameParams) % 4 == 0, "EzFrameParams is copied as 32-bit
 
 __device__ __forceinline__ float ezf_wrap_hi(float w) { return w * 1.0f + w * 0.0f; }
 
-// CPML psi row of H row r on side s (lo: rows 0..npml-1, hi: n-npml-1..n-2), -1 outside.
-__device__ __forceinline__ int ezf_h_row(int s, int r, int n, int npml) {
-    const int k = (s == SX_LO || s == SY_LO) ? r : r - (n - npml - 1);
-    return (k >= 0 && k < npml) ? k : -1;
+// The CPML side of an axis (lo_side: SX_LO or SY_LO; lo_side + 1 the hi side) whose H rows (lo: rows 0..npml-1,
+// hi: n-npml-1..n-2) hold row r, with its slab row k; -1 when none.
+__device__ __forceinline__ int ezf_h_side(int lo_side, int mask, int r, int n, int npml, int &k) {
+    if (((mask >> lo_side) & 1) && r < npml) {
+        k = r;
+        return lo_side;
+    }
+    if (((mask >> (lo_side + 1)) & 1) && r >= n - npml - 1 && r <= n - 2) {
+        k = r - (n - npml - 1);
+        return lo_side + 1;
+    }
+    return -1;
 }
 
-// CPML psi row of E row r on side s (lo: rows 1..npml, hi: n-npml-1..n-2), -1 outside.
-__device__ __forceinline__ int ezf_e_row(int s, int r, int n, int npml) {
-    const int k = (s == SX_LO || s == SY_LO) ? r - 1 : r - (n - npml - 1);
-    return (k >= 0 && k < npml) ? k : -1;
+// The same for the E rows (lo: rows 1..npml, hi: n-npml-1..n-2).
+__device__ __forceinline__ int ezf_e_side(int lo_side, int mask, int r, int n, int npml, int &k) {
+    if (((mask >> lo_side) & 1) && r >= 1 && r <= npml) {
+        k = r - 1;
+        return lo_side;
+    }
+    if (((mask >> (lo_side + 1)) & 1) && r >= n - npml - 1 && r <= n - 2) {
+        k = r - (n - npml - 1);
+        return lo_side + 1;
+    }
+    return -1;
 }
 
 // New H_x of face (i, j) (fdtd_ez_2d_kernels.py:41-44, y-side H-row CPML); the last face of an open y keeps its
@@ -68,13 +83,12 @@ __device__ __forceinline__ float ezf_hx_at(const EzFrameParams &p, int i, int j,
     const float db = p.db ? __ldg(p.db + idx) : p.db_u;
     const float e_up = j < ny - 1 ? __ldg(p.ez_in + idx + 1) : ezf_wrap_hi(__ldg(p.ez_in + (size_t)i * ny));
     float v = da * hx_old - db * (e_up - e) * __ldg(p.inv_dy_h + j);
-    for (int s = SY_LO; s <= SY_HI; ++s) {
-        if (!(p.cpml_mask & (1 << s))) continue;
-        const int k = ezf_h_row(s, j, ny, npml);
-        if (k < 0) continue;
+    int k;
+    const int s = ezf_h_side(SY_LO, p.cpml_mask, j, ny, npml, k);
+    if (s >= 0) {
         const float *rows = p.cpml_rows[s];
         const size_t q_at = (size_t)i * npml + k;
-        float q = p.psi_h_in[s][q_at] * rows[3 * npml + k];
+        float q = __ldg(p.psi_h_in[s] + q_at) * rows[3 * npml + k];
         q += rows[4 * npml + k] * (__ldg(p.ez_in + idx + 1) - e) * rows[5 * npml + k];
         if (own) p.psi_h_out[s][q_at] = q;
         v += (-db) * q;
@@ -93,13 +107,12 @@ __device__ __forceinline__ float ezf_hy_at(const EzFrameParams &p, int i, int j,
     const float db = p.db ? __ldg(p.db + idx) : p.db_u;
     const float e_up = i < nx - 1 ? __ldg(p.ez_in + idx + ny) : ezf_wrap_hi(__ldg(p.ez_in + j));
     float v = da * hy_old + db * (e_up - e) * __ldg(p.inv_dx_h + i);
-    for (int s = SX_LO; s <= SX_HI; ++s) {
-        if (!(p.cpml_mask & (1 << s))) continue;
-        const int k = ezf_h_row(s, i, nx, npml);
-        if (k < 0) continue;
+    int k;
+    const int s = ezf_h_side(SX_LO, p.cpml_mask, i, nx, npml, k);
+    if (s >= 0) {
         const float *rows = p.cpml_rows[s];
         const size_t q_at = (size_t)k * ny + j;
-        float q = p.psi_h_in[s][q_at] * rows[3 * npml + k];
+        float q = __ldg(p.psi_h_in[s] + q_at) * rows[3 * npml + k];
         q += rows[4 * npml + k] * (__ldg(p.ez_in + idx + ny) - e) * rows[5 * npml + k];
         if (own) p.psi_h_out[s][q_at] = q;
         v += db * q;
@@ -125,7 +138,12 @@ __device__ __forceinline__ void ezf_cell(const EzFrameParams &p, int64_t t) {
     const int cc1 = k == 0 ? p.c1[0] : k == 1 ? p.c1[1] : k == 2 ? p.c1[2] : p.c1[3];
     const int64_t local = t - first;
     const int w = cc1 - cc0;
-    const int i = rr0 + (int)(local / w), j = cc0 + (int)(local % w);
+    int i, j;
+    if (local < 0x7fffffff) {   // 32-bit division for every cell but those of a rectangle past 2^31 cells
+        i = rr0 + (int)local / w, j = cc0 + (int)local % w;
+    } else {
+        i = rr0 + (int)(local / w), j = cc0 + (int)(local % w);
+    }
     const int nx = p.nx, ny = p.ny, npml = p.npml;
     const size_t idx = (size_t)i * ny + j;
 
@@ -152,17 +170,26 @@ __device__ __forceinline__ void ezf_cell(const EzFrameParams &p, int64_t t) {
     const float cb = __ldg(p.cb + idx);
     const float ez_old = __ldg(p.ez_in + idx);
     float v = (p.ca ? __ldg(p.ca + idx) * ez_old : ez_old) + cb * curl;
-    for (int s = SX_LO; s <= SY_HI; ++s) {
-        if (!(p.cpml_mask & (1 << s))) continue;
-        const bool xs = s < 2;
-        const int kr = ezf_e_row(s, xs ? i : j, xs ? nx : ny, npml);
-        if (kr < 0) continue;
-        const float *rows = p.cpml_rows[s];
-        const size_t q_at = xs ? (size_t)kr * ny + j : (size_t)i * npml + kr;
-        float q = p.psi_e_in[s][q_at] * rows[kr];
-        q += rows[npml + kr] * (xs ? hy_c - hy_dn : hx_c - hx_left) * rows[2 * npml + kr];
-        p.psi_e_out[s][q_at] = q;
-        v += (xs ? cb : -cb) * q;
+    if (p.cpml_mask) {   // the E-row CPML of the x side holding row i, then of the y side holding column j
+        int kr;
+        const int sx = ezf_e_side(SX_LO, p.cpml_mask, i, nx, npml, kr);
+        if (sx >= 0) {
+            const float *rows = p.cpml_rows[sx];
+            const size_t q_at = (size_t)kr * ny + j;
+            float q = __ldg(p.psi_e_in[sx] + q_at) * rows[kr];
+            q += rows[npml + kr] * (hy_c - hy_dn) * rows[2 * npml + kr];
+            p.psi_e_out[sx][q_at] = q;
+            v += cb * q;
+        }
+        const int sy = ezf_e_side(SY_LO, p.cpml_mask, j, ny, npml, kr);
+        if (sy >= 0) {
+            const float *rows = p.cpml_rows[sy];
+            const size_t q_at = (size_t)i * npml + kr;
+            float q = __ldg(p.psi_e_in[sy] + q_at) * rows[kr];
+            q += rows[npml + kr] * (hx_c - hx_left) * rows[2 * npml + kr];
+            p.psi_e_out[sy][q_at] = q;
+            v += (-cb) * q;
+        }
     }
     for (int l = 0; l < p.n_lines; ++l) {
         const TBLine &L = p.lines[l];

@@ -143,8 +143,18 @@ struct IPWarp {
         for (uint32_t lines = line_mask; lines; lines &= lines - 1) {
             const int l = __ffs(lines) - 1;
             const TBLine &L = p.lines[l];
+            if (!in_grid0) continue;
+            // the step's value is read only where this row holds a cell of the line
+            bool hit = false;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int j = jp0 + c;
+                const int along = L.axis == 0 ? ip : j, across = L.axis == 0 ? j : ip;
+                hit = hit || (across == L.position && along >= L.lo && along < L.hi);
+            }
+            if (!hit) continue;
             const float value = p.line_values[(size_t)l * p.values_stride + p.k0 + (S - 1)];
-            if (value == 0.0f || !in_grid0) continue;
+            if (value == 0.0f) continue;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const int j = jp0 + c;
@@ -402,6 +412,8 @@ __global__ void __launch_bounds__(TB_WARPS * 32, 4) ez2d_interior_kernel(const T
 
 // Several simulations in one launch: warp g runs tile g - tile_start[job] of jobs[job], tile_start ascending with
 // tile_start[n_jobs] = the total (every job shares T and the template configuration).
+static_assert(sizeof(TBParams) % 16 == 0, "TBParams is staged per warp in shared memory as 32-bit words");
+
 template <int T, bool CA, bool PX, bool PY>
 __global__ void __launch_bounds__(TB_WARPS * 32, 4) ez2d_interior_batch_kernel(const TBParams *__restrict__ jobs,
                                                                          const int *__restrict__ tile_start,
@@ -411,5 +423,12 @@ __global__ void __launch_bounds__(TB_WARPS * 32, 4) ez2d_interior_batch_kernel(c
     if (g >= tile_start[n_jobs]) return;
     int job = 0;
     while (job + 1 < n_jobs && g >= tile_start[job + 1]) ++job;
-    ez2d_interior_tile<T, CA, PX, PY>(jobs[job], g - tile_start[job], tb_smem);
+    // the warp's job parameters into shared memory (after the block's staging rings): the tile code reads them
+    // there, not from global memory
+    TBParams *mine = reinterpret_cast<TBParams *>(tb_smem + TB_WARPS * ip_warp_smem_bytes(T, CA)) + (threadIdx.x >> 5);
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(jobs + job);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(mine);
+    for (int w = threadIdx.x & 31; w < (int)(sizeof(TBParams) / 4); w += 32) dst[w] = src[w];
+    __syncwarp();
+    ez2d_interior_tile<T, CA, PX, PY>(*mine, g - tile_start[job], tb_smem);
 }

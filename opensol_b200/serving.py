@@ -45,12 +45,15 @@ class BatchAdvancer:
         engine.set_stream(self.stream)
         self._adopted.append(weakref.ref(engine))
 
-    def advance(self, engines, n_steps):
+    def advance(self, engines, n_steps, tables=None):
+        """Enqueue n_steps steps of every engine (asynchronous).  tables: the engines' chunk_tables(n_steps) made
+        beforehand for their present clocks (None: made here)."""
         n_steps = int(n_steps)
         n = len(engines)
         if n == 0 or n_steps <= 0:
             return
-        tables = [e.chunk_tables(n_steps) for e in engines]
+        if tables is None:
+            tables = [e.chunk_tables(n_steps) for e in engines]
         handles = (ctypes.c_void_p * n)(*[e.handle.value for e in engines])
         fp = ctypes.POINTER(ctypes.c_float)
         values = (fp * n)(*[_native.fptr(t[0]) if t[0].size else None for t in tables])
@@ -172,9 +175,11 @@ class _Active:
 
 
 class ServingLoop:
-    """Admission by memory budget and slots, all active jobs stepped together in batched launches."""
+    """Admission by memory budget and slots, all active jobs stepped together in batched launches.  Two steps per
+    blocked launch by default: with many jobs sharing the device the per-row latency of the interior tiles, not their
+    DRAM traffic, bounds a launch, and 2 steps measured faster than 3 or 4 (one job alone is fastest at 3)."""
 
-    def __init__(self, device=0, memory_budget=120e9, max_active=48, chunk_steps=512, steps_per_launch=3,
+    def __init__(self, device=0, memory_budget=120e9, max_active=48, chunk_steps=512, steps_per_launch=2,
                  tile_rows=0):
         self.device = int(device)
         self.memory_budget = float(memory_budget)
@@ -188,51 +193,70 @@ class ServingLoop:
         self.launches = 0
         self.peak_active = 0
         self.peak_bytes = 0
+        self.tick_log = []   # with time_ticks: (jobs, cell-updates, device ms) per tick
 
     def run(self, specs, realtime=True, time_ticks=False):
         """Serve `specs` (arrival times honoured on the wall clock when realtime, else all queued at once); returns
         the JobResults in completion order.  time_ticks: wait for every tick and add up its device time (device_ms,
-        launches), at the price of a host wait per tick."""
+        launches), at the price of a host wait per tick.
+
+        Each tick is enqueued first; while the device runs it the host admits arrivals (they join the next tick),
+        makes the next tick's source and phase tables, and only then reads the fluxes of the jobs the tick finished
+        (which waits for it) and releases them."""
         pending = deque(sorted(specs, key=lambda s: (s.arrival if realtime else 0.0, s.job_id)))
         active, results = [], []
         used = 0
         t0 = time.perf_counter()
-        while pending or active:
+
+        def admit(into, held):
             now = time.perf_counter() - t0
-            while (pending and (not realtime or pending[0].arrival <= now) and len(active) < self.max_active
-                   and used + pending[0].device_bytes() <= self.memory_budget):
+            while (pending and (not realtime or pending[0].arrival <= now) and len(into) < self.max_active
+                   and held + pending[0].device_bytes() <= self.memory_budget):
                 spec = pending.popleft()
                 sim, monitors = build_job(spec, self.device, self.steps_per_launch, self.tile_rows)
                 self.advancer.adopt(sim.em.engine)
-                active.append(_Active(spec, sim, monitors, spec.steps, time.perf_counter() - t0,
-                                      spec.device_bytes()))
-                used += spec.device_bytes()
+                into.append(_Active(spec, sim, monitors, spec.steps, time.perf_counter() - t0, spec.device_bytes()))
+                held += spec.device_bytes()
+            return held
+
+        tables = None
+        while pending or active:
+            if not active:
+                used = admit(active, used)
+                tables = None
+                if not active:
+                    if pending:
+                        time.sleep(max(0.0, min(0.005, pending[0].arrival - (time.perf_counter() - t0))))
+                    continue
             self.peak_active = max(self.peak_active, len(active))
             self.peak_bytes = max(self.peak_bytes, used)
-            if not active:
-                if pending:
-                    time.sleep(max(0.0, min(0.005, pending[0].arrival - (time.perf_counter() - t0))))
-                continue
             chunk = min(self.chunk_steps, min(a.remaining for a in active))
-            self.advancer.advance([a.sim.em.engine for a in active], chunk)
+            self.advancer.advance([a.sim.em.engine for a in active], chunk, tables)
             self.ticks += 1
             for a in active:
                 a.remaining -= chunk
             done = [a for a in active if a.remaining == 0]
+            survivors = [a for a in active if a.remaining > 0]
+            # while the device runs the tick: arrivals join the next one, whose tables are made now
+            used = admit(survivors, used)
+            tables = None
+            if survivors:
+                next_chunk = min(self.chunk_steps, min(a.remaining for a in survivors))
+                tables = [a.sim.em.engine.chunk_tables(next_chunk) for a in survivors]
             if time_ticks:
                 ms, launches = self.advancer.last_ms()
                 self.device_ms += ms
                 self.launches += launches
-            if done:
-                for a in done:
-                    fluxes = [m.flux() for m in a.monitors]
-                    finished = time.perf_counter() - t0
-                    arrival = a.spec.arrival if realtime else 0.0
-                    results.append(JobResult(a.spec.job_id, fluxes, arrival, a.admitted, finished, a.spec.steps,
-                                             a.spec.cells()))
-                    a.sim.em.engine.close()
-                    used -= a.bytes
-                active = [a for a in active if a.remaining > 0]
+                self.tick_log.append((len(active), sum(a.spec.cells() for a in active) * chunk, ms))
+            for a in done:
+                fluxes = [m.flux() for m in a.monitors]
+                finished = time.perf_counter() - t0
+                arrival = a.spec.arrival if realtime else 0.0
+                results.append(JobResult(a.spec.job_id, fluxes, arrival, a.admitted, finished, a.spec.steps,
+                                         a.spec.cells()))
+                a.sim.em.engine.close()
+                used -= a.bytes
+            active = survivors
         return results
 
     def close(self):
