@@ -761,27 +761,30 @@ static void fill_common(const OsFdtd2D *h, TBParams &q) {
     q.err = h->err.ptr;
 }
 
-template <int T, bool CA, bool PX, bool PY>
+template <int T, bool CA, bool PX, bool PY, bool VEC>
 static int launch_interior(OsFdtd2D *h, const TBParams &q) {
     const size_t smem = (size_t)TB_WARPS * ip_warp_smem_bytes(T, CA);
     static bool attr_set = false;   // one flag per instantiation
     if (!attr_set) {
-        OS_CUDA(cudaFuncSetAttribute(ez2d_interior_kernel<T, CA, PX, PY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
+        OS_CUDA(cudaFuncSetAttribute(ez2d_interior_kernel<T, CA, PX, PY, VEC>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set = true;
     }
     const dim3 blocks((unsigned)((q.n_tiles + TB_WARPS - 1) / TB_WARPS)), threads(TB_WARPS * 32);
-    ez2d_interior_kernel<T, CA, PX, PY><<<blocks, threads, smem, h->stream>>>(q);
+    ez2d_interior_kernel<T, CA, PX, PY, VEC><<<blocks, threads, smem, h->stream>>>(q);
     return OS_OK;
 }
 
+// ny % 4 == 0 selects the aligned kernels; a row length that is not a multiple of 4 only ever has an interior with a
+// non-periodic y (plan_tiles)
 template <int T, bool CA>
 static int launch_interior_ca(OsFdtd2D *h, const TBParams &q) {
-    const bool px = h->grid.periodic_x != 0, py = h->grid.periodic_y != 0;
-    if (px && py) return launch_interior<T, CA, true, true>(h, q);
-    if (px) return launch_interior<T, CA, true, false>(h, q);
-    if (py) return launch_interior<T, CA, false, true>(h, q);
-    return launch_interior<T, CA, false, false>(h, q);
+    const bool px = h->grid.periodic_x != 0, py = h->grid.periodic_y != 0, vec = h->grid.ny % 4 == 0;
+    if (!vec) return px ? launch_interior<T, CA, true, false, false>(h, q) : launch_interior<T, CA, false, false, false>(h, q);
+    if (px && py) return launch_interior<T, CA, true, true, true>(h, q);
+    if (px) return launch_interior<T, CA, true, false, true>(h, q);
+    if (py) return launch_interior<T, CA, false, true, true>(h, q);
+    return launch_interior<T, CA, false, false, true>(h, q);
 }
 
 template <int T>
@@ -1636,7 +1639,7 @@ namespace os {
 
 struct BatchGroup {                    // one kernel launch of a batched step: jobs sharing a template configuration
     int kind;                          // 0 interior, 1 general
-    bool ca, px, py;
+    bool ca, px, py, vec;              // vec: ny % 4 == 0 (interior groups)
     std::vector<TBParams> params;
     std::vector<int> tile_start{0};
     size_t params_off = 0, tiles_off = 0;
@@ -1657,25 +1660,38 @@ struct BatchLaunch {
     size_t items_off = 0;
 };
 
-static BatchGroup &batch_group(BatchLaunch &L, int kind, bool ca, bool px, bool py) {
+static BatchGroup &batch_group(BatchLaunch &L, int kind, bool ca, bool px, bool py, bool vec) {
     for (auto &g : L.groups)
-        if (g.kind == kind && g.ca == ca && g.px == px && g.py == py) return g;
-    L.groups.push_back(BatchGroup{kind, ca, px, py, {}, {0}, 0, 0});
+        if (g.kind == kind && g.ca == ca && g.px == px && g.py == py && g.vec == vec) return g;
+    L.groups.push_back(BatchGroup{kind, ca, px, py, vec, {}, {0}, 0, 0});
     return L.groups.back();
 }
 
-template <int T, bool CA, bool PX, bool PY>
+template <int T, bool CA, bool PX, bool PY, bool VEC>
 static int launch_interior_batch(cudaStream_t s, const TBParams *jobs, const int *tiles, int n_jobs, int total) {
     const size_t smem = (size_t)TB_WARPS * ip_warp_smem_bytes(T, CA) + (size_t)TB_WARPS * sizeof(TBParams);
     static bool attr_set = false;
     if (!attr_set) {
-        OS_CUDA(cudaFuncSetAttribute(ez2d_interior_batch_kernel<T, CA, PX, PY>,
+        OS_CUDA(cudaFuncSetAttribute(ez2d_interior_batch_kernel<T, CA, PX, PY, VEC>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set = true;
     }
-    ez2d_interior_batch_kernel<T, CA, PX, PY>
+    ez2d_interior_batch_kernel<T, CA, PX, PY, VEC>
         <<<(unsigned)((total + TB_WARPS - 1) / TB_WARPS), TB_WARPS * 32, smem, s>>>(jobs, tiles, n_jobs);
     return OS_OK;
+}
+
+template <int T, bool CA>
+static int launch_interior_batch_ca(cudaStream_t s, const BatchGroup &g, const TBParams *jobs, const int *tiles,
+                                    int n, int total) {
+    if (!g.vec) {
+        return g.px ? launch_interior_batch<T, CA, true, false, false>(s, jobs, tiles, n, total)
+                    : launch_interior_batch<T, CA, false, false, false>(s, jobs, tiles, n, total);
+    }
+    if (g.px && g.py) return launch_interior_batch<T, CA, true, true, true>(s, jobs, tiles, n, total);
+    if (g.px) return launch_interior_batch<T, CA, true, false, true>(s, jobs, tiles, n, total);
+    if (g.py) return launch_interior_batch<T, CA, false, true, true>(s, jobs, tiles, n, total);
+    return launch_interior_batch<T, CA, false, false, true>(s, jobs, tiles, n, total);
 }
 
 template <int T>
@@ -1690,16 +1706,8 @@ static int launch_group(cudaStream_t s, const BatchGroup &g, const unsigned char
         else ez2d_tb_batch_kernel<T, 1, true, false><<<blocks, TB_WARPS * 32, 0, s>>>(jobs, tiles, n);
         return OS_OK;
     }
-    if (g.ca) {
-        if (g.px && g.py) return launch_interior_batch<T, true, true, true>(s, jobs, tiles, n, total);
-        if (g.px) return launch_interior_batch<T, true, true, false>(s, jobs, tiles, n, total);
-        if (g.py) return launch_interior_batch<T, true, false, true>(s, jobs, tiles, n, total);
-        return launch_interior_batch<T, true, false, false>(s, jobs, tiles, n, total);
-    }
-    if (g.px && g.py) return launch_interior_batch<T, false, true, true>(s, jobs, tiles, n, total);
-    if (g.px) return launch_interior_batch<T, false, true, false>(s, jobs, tiles, n, total);
-    if (g.py) return launch_interior_batch<T, false, false, true>(s, jobs, tiles, n, total);
-    return launch_interior_batch<T, false, false, false>(s, jobs, tiles, n, total);
+    return g.ca ? launch_interior_batch_ca<T, true>(s, g, jobs, tiles, n, total)
+                : launch_interior_batch_ca<T, false>(s, g, jobs, tiles, n, total);
 }
 
 static int launch_group_any(int T, cudaStream_t s, const BatchGroup &g, const unsigned char *dev) {
@@ -1864,7 +1872,7 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
                 if (kind == 1 && h->variant == 1) continue;   // advanced by the frame steps above
                 if (!base.n_tiles) continue;
                 BatchGroup &g = batch_group(L, kind, h->has_ca, kind == 0 && h->grid.periodic_x,
-                                            kind == 0 && h->grid.periodic_y);
+                                            kind == 0 && h->grid.periodic_y, kind == 0 && h->grid.ny % 4 == 0);
                 g.params.push_back(base);
                 TBParams &p = g.params.back();
                 bind_buffers(h, p, in, out);

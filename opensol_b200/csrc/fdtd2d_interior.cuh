@@ -37,7 +37,7 @@ __device__ __forceinline__ float2 ip_sub_p(float2 a, float2 b) {
     return make_float2(__fadd_rn(a.x, -b.x), __fadd_rn(a.y, -b.y));
 }
 
-template <int T, bool CA, bool PX, bool PY>
+template <int T, bool CA, bool PX, bool PY, bool VEC>
 struct IPWarp {
     const TBParams &p;
     // tile
@@ -48,7 +48,7 @@ struct IPWarp {
     bool wrap_lo0;         // PY: the first column is column 0 (its lo neighbour is the wrapped last column)
     uint32_t line_mask, mon_mask, sample_mask;
     int nx, ny;
-    bool vec;              // ny % 4 == 0: every row window starts 16-byte aligned (float4 reads and stores)
+    static constexpr bool vec = VEC;   // ny % 4 == 0: every row window starts 16-byte aligned (float4 reads, stores)
     float2 db2, ixh2, ixe2, iyh2, iye2;
     float *ez_out, *hx_out, *hy_out;
     const float *__restrict__ ez_in, *__restrict__ hx_in, *__restrict__ hy_in, *__restrict__ cbp, *__restrict__ cap;
@@ -74,7 +74,7 @@ struct IPWarp {
     // bytes.  A row that does not start 16-byte aligned is copied from the boundary before it, rounded up to 16
     // bytes (the data then starts at dst + row_off).
     __device__ __forceinline__ uint32_t window(float *dst, const float *src_row, uint64_t *bar, bool issue) const {
-        if (!vec) {
+        if constexpr (!VEC) {
             const int col = j0 - 4;
             const int len = min(128, ny - col);
             const int off = (int)(((uintptr_t)(src_row + col) >> 2) & 3u);
@@ -115,8 +115,8 @@ struct IPWarp {
 
     // four consecutive floats of a staged window (16-byte aligned when vec)
     __device__ __forceinline__ float4 ld_win(const float *q) const {
-        if (vec) return *reinterpret_cast<const float4 *>(q);
-        return make_float4(q[0], q[1], q[2], q[3]);
+        if constexpr (VEC) return *reinterpret_cast<const float4 *>(q);
+        else return make_float4(q[0], q[1], q[2], q[3]);
     }
 
     template <int PH>
@@ -299,7 +299,7 @@ struct IPWarp {
 };
 
 // One warp's tile w of the interior plan p (tb_smem: the block's dynamic shared memory).
-template <int T, bool CA, bool PX, bool PY>
+template <int T, bool CA, bool PX, bool PY, bool VEC>
 __device__ __forceinline__ void ez2d_interior_tile(const TBParams &p, int w, unsigned char *tb_smem) {
     const int lane = threadIdx.x & 31;
     if (w >= p.n_tiles) return;   // whole warps leave together
@@ -310,11 +310,10 @@ __device__ __forceinline__ void ez2d_interior_tile(const TBParams &p, int w, uns
     const int t = w - R.first_tile;
     const int tc = t % R.tiles_c, tr = t / R.tiles_c;
 
-    IPWarp<T, CA, PX, PY> W(p);
+    IPWarp<T, CA, PX, PY, VEC> W(p);
     W.lane = lane;
     W.nx = p.nx;
     W.ny = p.ny;
-    W.vec = p.ny % 4 == 0;
     W.j0 = R.c0 + tc * p.tile_w;
     W.j1 = min(W.j0 + p.tile_w, R.c1);
     W.i0 = R.r0 + tr * p.tile_rows;
@@ -404,17 +403,17 @@ __device__ __forceinline__ void ez2d_interior_tile(const TBParams &p, int w, uns
     }
 }
 
-template <int T, bool CA, bool PX, bool PY>
+template <int T, bool CA, bool PX, bool PY, bool VEC>
 __global__ void __launch_bounds__(TB_WARPS * 32, 4) ez2d_interior_kernel(const TBParams p) {
     extern __shared__ __align__(16) unsigned char tb_smem[];
-    ez2d_interior_tile<T, CA, PX, PY>(p, blockIdx.x * TB_WARPS + (threadIdx.x >> 5), tb_smem);
+    ez2d_interior_tile<T, CA, PX, PY, VEC>(p, blockIdx.x * TB_WARPS + (threadIdx.x >> 5), tb_smem);
 }
 
 // Several simulations in one launch: warp g runs tile g - tile_start[job] of jobs[job], tile_start ascending with
 // tile_start[n_jobs] = the total (every job shares T and the template configuration).
 static_assert(sizeof(TBParams) % 16 == 0, "TBParams is staged per warp in shared memory as 32-bit words");
 
-template <int T, bool CA, bool PX, bool PY>
+template <int T, bool CA, bool PX, bool PY, bool VEC>
 __global__ void __launch_bounds__(TB_WARPS * 32, 4) ez2d_interior_batch_kernel(const TBParams *__restrict__ jobs,
                                                                          const int *__restrict__ tile_start,
                                                                          int n_jobs) {
@@ -425,10 +424,11 @@ __global__ void __launch_bounds__(TB_WARPS * 32, 4) ez2d_interior_batch_kernel(c
     while (job + 1 < n_jobs && g >= tile_start[job + 1]) ++job;
     // the warp's job parameters into shared memory (after the block's staging rings): the tile code reads them
     // there, not from global memory
-    TBParams *mine = reinterpret_cast<TBParams *>(tb_smem + TB_WARPS * ip_warp_smem_bytes(T, CA)) + (threadIdx.x >> 5);
+    TBParams *mine = reinterpret_cast<TBParams *>(tb_smem + TB_WARPS * ip_warp_smem_bytes(T, CA)) +
+                     (threadIdx.x >> 5);
     const uint32_t *src = reinterpret_cast<const uint32_t *>(jobs + job);
     uint32_t *dst = reinterpret_cast<uint32_t *>(mine);
     for (int w = threadIdx.x & 31; w < (int)(sizeof(TBParams) / 4); w += 32) dst[w] = src[w];
     __syncwarp();
-    ez2d_interior_tile<T, CA, PX, PY>(*mine, g - tile_start[job], tb_smem);
+    ez2d_interior_tile<T, CA, PX, PY, VEC>(*mine, g - tile_start[job], tb_smem);
 }
