@@ -222,7 +222,9 @@ def run_b200(args):
     if args.variant == 1 and not args.tile_rows:
         autotuned = engine.autotune()
         args.tile_rows = engine.tile_rows
-    stream = torch.cuda.current_stream()
+    # a stream of its own (torch's default stream is handle 0, which os_fdtd*_set_stream reads as "the engine's own
+    # stream"): the engine launches on it and the timing events are recorded on it
+    stream = torch.cuda.Stream()
     engine.set_stream(stream.cuda_stream)
     cells = engine.nx * engine.ny
     engine.reset()
@@ -357,7 +359,9 @@ def run_hz2d(args):
     sim.em.engine.configure(variant=variant, steps_per_launch=1, tile_rows=args.tile_rows)
     sim.em.finalize()
     engine = sim.em.engine
-    stream = torch.cuda.current_stream()
+    # a stream of its own (torch's default stream is handle 0, which os_fdtd*_set_stream reads as "the engine's own
+    # stream"): the engine launches on it and the timing events are recorded on it
+    stream = torch.cuda.Stream()
     engine.set_stream(stream.cuda_stream)
     tables = engine.chunk_tables(args.sim_steps)
     for _ in range(args.warmup):
@@ -454,7 +458,9 @@ def run_em3d(args):
     physics, box = workloads.roofline_3d_physics(device=local)
     physics.finalize()
     engine = physics.engine
-    stream = torch.cuda.current_stream()
+    # a stream of its own (torch's default stream is handle 0, which os_fdtd*_set_stream reads as "the engine's own
+    # stream"): the engine launches on it and the timing events are recorded on it
+    stream = torch.cuda.Stream()
     engine.set_stream(stream.cuda_stream)
     tables = engine.chunk_tables(steps)
     for _ in range(args.warmup):
@@ -499,16 +505,17 @@ def run_serving(args):
     torch.cuda.set_device(0)
     specs = serving.make_job_specs(n_jobs=args.jobs, rate=20.0, seed=7)
     work = sum(s.cells() * s.steps for s in specs)
-    warm = serving.make_job_specs(n_jobs=3, rate=0.0, seed=1, side_range=(64, 128), steps_range=(100, 300))
+    # warm-up: one untimed pass of the same stream, as a serving process that has run for a while: the kernels are
+    # loaded and the engines' device-memory pool holds blocks of every size the stream needs (both arms take their
+    # arrays from it)
     loop = serving.ServingLoop(max_active=48, chunk_steps=512)
-    loop.run(warm, realtime=False)
-    loop.close()
-    serving.run_alone(warm[0])
+    loop.run(specs, realtime=False)
+    loop.close(trim=False)
     loop = serving.ServingLoop(max_active=48, chunk_steps=512)
     t0 = time.perf_counter()
     batched = {r.job_id: r for r in loop.run(specs, realtime=False)}
     t_batch = time.perf_counter() - t0
-    loop.close()
+    loop.close(trim=False)
     t0 = time.perf_counter()
     alone = {s.job_id: serving.run_alone(s)[0] for s in specs}
     t_alone = time.perf_counter() - t0
@@ -526,7 +533,11 @@ def run_serving(args):
                                    '1-40 rectangles eps_r U(1,12), line source U(1000,1600) nm, U(2000,20000) steps, '
                                    'two 4-frequency flux lines; Poisson 20 jobs/s for the latency run',
                        'max_active': 48, 'chunk_steps': 512, 'memory_budget_gb': 120,
-                       'steps_per_launch': {'batched': 2, 'one_at_a_time': 3},
+                       'steps_per_launch': {'batched': 3, 'one_at_a_time': 3},
+                       'admission': 'all jobs queued at once: largest (cells x steps) first, at most 16 set up per '
+                                    'tick; latency run: arrival order',
+                       'warm_up': 'one untimed pass of the same stream (kernels loaded, device-memory pool warm for '
+                                  'both arms)',
                        'tile_rows': 'chosen per call from the active jobs (batched) / per grid (one at a time)'},
             'one_at_a_time_sims_per_s': len(specs) / t_alone, 'speedup_vs_one_at_a_time': t_alone / t_batch,
             'cell_updates_per_s_batched': work / t_batch, 'fluxes_equal_alone_and_batched': bool(same),

@@ -217,8 +217,8 @@ int os_fdtd2d_reset(OsFdtd2D *h);
 /* Waits for the handle's stream. */
 int os_fdtd2d_synchronize(OsFdtd2D *h);
 
-/* Launch on the caller's CUDA stream (a cudaStream_t; NULL = back to the handle's own stream).  Work already queued
- * on the previous stream is waited for first.  The caller keeps that stream alive while the handle uses it: set the
+/* Launch on the caller's CUDA stream (a cudaStream_t; NULL = back to the handle's own stream).  The new stream waits
+ * on the device for the work already queued on the previous one (an event; the host does not wait).  The caller keeps that stream alive while the handle uses it: set the
  * handle back (NULL) before destroying the stream; os_fdtd2d_destroy itself never touches a caller's stream.  No
  * open_sol counterpart: the B200 hook for torch streams. */
 int os_fdtd2d_set_stream(OsFdtd2D *h, void *cuda_stream);

@@ -83,12 +83,30 @@ struct DeviceArray {
         capacity = 0;
         cls = 0;
     }
+    // Room for n elements; a block that is too small is freed first (cudaFree, which waits for the whole device).
     int alloc(size_t n) {
         if (ptr && n <= capacity) {
             count = n;
             return OS_OK;
         }
         release();
+        return take(n);
+    }
+    // The same for an array whose uses are all ordered on `stream`: a block that is too small goes to the pool, to be
+    // handed out again once the work queued so far on `stream` has finished, so growing waits for nothing.
+    int alloc(size_t n, cudaStream_t stream) {
+        if (ptr && n <= capacity) {
+            count = n;
+            return OS_OK;
+        }
+        if (ptr) {
+            PoolEvents *ev = pool_events(&stream, 1);
+            give_to_pool(ev);
+            pool_events_done(ev);
+        }
+        return take(n);
+    }
+    int take(size_t n) {   // ptr is null here
         if (n == 0) return OS_OK;
         // 256 bytes of slack past the last element: a 16-byte-rounded bulk copy of a row window that ends at the last
         // element of the array stays inside the allocation
@@ -112,10 +130,18 @@ struct DeviceArray {
     size_t bytes() const { return count * sizeof(T); }
 };
 
+// Staging arrays whose last uses are queued on `stream` go to the pool (no host wait, no cudaFree).
+template <typename... A>
+void give_after(cudaStream_t stream, A &...arrays) {
+    PoolEvents *ev = pool_events(&stream, 1);
+    (arrays.give_to_pool(ev), ...);
+    pool_events_done(ev);
+}
+
 // Host-to-device copy of `n` elements on `stream` (the host buffer may be reused on return).
 template <typename T>
 int upload(DeviceArray<T> &dst, const T *src, size_t n, cudaStream_t stream) {
-    OS_TRY(dst.alloc(n));
+    OS_TRY(dst.alloc(n, stream));
     if (n) OS_CUDA(cudaMemcpyAsync(dst.ptr, src, n * sizeof(T), cudaMemcpyHostToDevice, stream));
     return OS_OK;
 }

@@ -45,6 +45,7 @@ struct OsFdtd2D {
     cudaStream_t side_stream = nullptr;   // the border kernel runs here, overlapping the interior kernel
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    cudaEvent_t ev_handoff = nullptr;     // orders the next stream after the previous one (os_fdtd2d_set_stream)
     bool timed = false;
     os::DeviceArray<float> ez[2], hx[2], hy[2];   // double-buffered fields; `cur` is the live set
     int cur = 0;
@@ -218,6 +219,7 @@ static int create_2d(const OsGrid2D *grid, int32_t polarization, OsFdtd2D **out)
     OS_CUDA(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
     OS_CUDA(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     OS_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+    OS_CUDA(cudaEventCreateWithFlags(&h->ev_handoff, cudaEventDisableTiming));
     h->stream = h->own_stream;
     OS_CUDA(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device));
     OS_CUDA(cudaEventCreate(&h->ev_start));
@@ -249,8 +251,7 @@ static int create_2d(const OsGrid2D *grid, int32_t polarization, OsFdtd2D **out)
     }
     OS_TRY(h->err.alloc(1));
     OS_CUDA(cudaMemsetAsync(h->err.ptr, 0, sizeof(int32_t), h->stream));
-    OS_TRY(zero_state(h.get()));
-    OS_CUDA(cudaStreamSynchronize(h->stream));
+    OS_TRY(zero_state(h.get()));   // queued on the handle's stream; every later use is ordered behind it
     *out = h.release();
     return OS_OK;
 }
@@ -292,6 +293,7 @@ extern "C" int os_fdtd2d_destroy(OsFdtd2D *h) {
     if (h->side_stream) cudaStreamSynchronize(h->side_stream);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->ev_handoff) cudaEventDestroy(h->ev_handoff);
     cudaStream_t stream = h->own_stream, side = h->side_stream;
     delete h;   // frees the device arrays
     if (stream) cudaStreamDestroy(stream);
@@ -322,9 +324,9 @@ extern "C" int os_fdtd2d_set_materials(OsFdtd2D *h, const float *eps_r, const fl
     OS_TRY(bind_device(h));
     const size_t n = cells(h);
     OS_TRY(h->cb.alloc(n));
-    // eps_r / sigma_e are staged in temporary device arrays (freed after the coefficient kernel has run); ca is only
-    // kept for a lossy grid.
-    DeviceArray<float> eps_dev, sigma_dev;
+    // eps_r / sigma_e (and mu_r / sigma_m) are staged in temporary device arrays that go to the pool behind the
+    // coefficient kernels (no host wait: jobs are set up while others run); ca is only kept for a lossy grid.
+    DeviceArray<float> eps_dev, sigma_dev, mu_dev, sm_dev;
     OS_TRY(upload(eps_dev, eps_r, n, h->stream));
     if (sigma_e) {
         OS_TRY(upload(sigma_dev, sigma_e, n, h->stream));
@@ -338,7 +340,6 @@ extern "C" int os_fdtd2d_set_materials(OsFdtd2D *h, const float *eps_r, const fl
     h->has_ca = sigma_e != nullptr;
     h->has_cb = true;
     if (mu_r || sigma_m) {
-        DeviceArray<float> mu_dev, sm_dev;
         if (mu_r) OS_TRY(upload(mu_dev, mu_r, n, h->stream));
         if (sigma_m) OS_TRY(upload(sm_dev, sigma_m, n, h->stream));
         OS_TRY(h->da.alloc(n));
@@ -347,7 +348,6 @@ extern "C" int os_fdtd2d_set_materials(OsFdtd2D *h, const float *eps_r, const fl
                                                                       h->db.ptr);
         OS_CUDA(cudaGetLastError());
         h->has_dadb = true;
-        OS_CUDA(cudaStreamSynchronize(h->stream));   // the staging arrays are freed on return
     } else {
         // vacuum permeability: da = (1 - 0) / 1, db = (dt / mu0) / 1 (fdtd_ez_2d_kernels.py:335-340)
         const float mu = 1.0f * mu0;
@@ -356,8 +356,8 @@ extern "C" int os_fdtd2d_set_materials(OsFdtd2D *h, const float *eps_r, const fl
         h->da_uniform = (1.0f - k) / denom;
         h->db_uniform = (dt / mu) / denom;
         h->has_dadb = false;
-        OS_CUDA(cudaStreamSynchronize(h->stream));
     }
+    give_after(h->stream, eps_dev, sigma_dev, mu_dev, sm_dev);
     return OS_OK;
 }
 
@@ -420,7 +420,7 @@ extern "C" int os_fdtd2d_hz_set_materials(OsFdtd2D *h, const float *eps_xx, cons
     std::memcpy(shares.data() + 2 * nx, lower_y, ny * sizeof(float));
     std::memcpy(shares.data() + 2 * nx + ny, upper_y, ny * sizeof(float));
     OS_TRY(upload(h->shares, shares.data(), shares.size(), h->stream));
-    DeviceArray<float> exx, eyy, sig;
+    DeviceArray<float> exx, eyy, sig, mu_dev, sm_dev;   // staging, to the pool behind the kernels that read them
     OS_TRY(upload(exx, eps_xx, n, h->stream));
     OS_TRY(upload(eyy, eps_yy, n, h->stream));
     if (sigma_e && !lossless) OS_TRY(upload(sig, sigma_e, n, h->stream));
@@ -448,7 +448,6 @@ extern "C" int os_fdtd2d_hz_set_materials(OsFdtd2D *h, const float *eps_xx, cons
         OS_CUDA(cudaMemcpyAsync(h->eps_cell.ptr, exx.ptr, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
     }
     if (mu_r || sigma_m) {
-        DeviceArray<float> mu_dev, sm_dev;
         if (mu_r) OS_TRY(upload(mu_dev, mu_r, n, h->stream));
         if (sigma_m) OS_TRY(upload(sm_dev, sigma_m, n, h->stream));
         OS_TRY(h->da.alloc(n));
@@ -467,7 +466,7 @@ extern "C" int os_fdtd2d_hz_set_materials(OsFdtd2D *h, const float *eps_xx, cons
         h->db_uniform = (dt / mu) / denom;
         h->has_dadb = false;
     }
-    OS_CUDA(cudaStreamSynchronize(h->stream));   // the staging arrays are freed on return
+    give_after(h->stream, exx, eyy, sig, mu_dev, sm_dev);
     return OS_OK;
 }
 
@@ -857,6 +856,9 @@ static EzFrameParams make_frame_params(const OsFdtd2D *h, int T, int k, const TB
     return f;
 }
 
+// Blocks of 256 threads (one per cell) of a frame step launch.
+static int64_t frame_blocks(const EzFrameParams &f) { return (f.first[f.n_rects] + 255) / 256; }
+
 // The frame of one blocked launch of T steps: T single-step launches of ez2d_frame_step_kernel on stream `s`.
 // `tmpl` (NULL: built here) holds the launch's T step parameters for its buffer parity, made by make_frame_params
 // from the same plan; only the value column and the sample slot of each step are set here from `q`.
@@ -869,10 +871,9 @@ static int launch_frame_chain(OsFdtd2D *h, int T, const TBParams &q, const Rect 
         f.k_col = q.k0 + (k - 1);
         f.sample_slot = ((q.sample_mask >> (k - 1)) & 1u) ? __builtin_popcount(q.sample_mask & ((1u << (k - 1)) - 1u))
                                                          : -1;
-        const int64_t cells_k = f.first[f.n_rects];
-        if (cells_k == 0) continue;
+        if (f.first[f.n_rects] == 0) continue;
         OS_TRY(prof_begin(h, 1, s));
-        ez2d_frame_step_kernel<<<(unsigned)((cells_k + 255) / 256), 256, 0, s>>>(f);
+        ez2d_frame_step_kernel<<<(unsigned)frame_blocks(f), 256, 0, s>>>(f);
         OS_TRY(prof_end(h, s));
         h->launches += 1;
     }
@@ -1600,7 +1601,9 @@ extern "C" int os_fdtd2d_set_stream(OsFdtd2D *h, void *cuda_stream) {
     OS_TRY(bind_device(h));
     cudaStream_t next = cuda_stream ? (cudaStream_t)cuda_stream : h->own_stream;
     if (next != h->stream) {
-        OS_CUDA(cudaStreamSynchronize(h->stream));
+        // the new stream waits on the device for the work queued so far on the old one (no host wait)
+        OS_CUDA(cudaEventRecord(h->ev_handoff, h->stream));
+        OS_CUDA(cudaStreamWaitEvent(next, h->ev_handoff, 0));
         h->stream = next;
     }
     return OS_OK;
@@ -1627,10 +1630,17 @@ struct OsFdtd2DBatch {
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;          // the frame steps run here, overlapping the interior launches
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    cudaEvent_t ev_copied = nullptr, ev_start = nullptr, ev_stop = nullptr;
-    bool copy_pending = false, timed = false;
-    unsigned char *host = nullptr;     // page-locked staging of one call's launch parameters
-    size_t host_capacity = 0;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    bool timed = false;
+    struct Staging {                   // page-locked staging of one call's launch parameters
+        unsigned char *host = nullptr;
+        size_t capacity = 0;
+        cudaEvent_t copied = nullptr;  // its copy to the device has run
+        bool pending = false;
+    };
+    static constexpr int kStaging = 4; // calls in flight before one waits for an earlier call's copy
+    Staging staging[kStaging];
+    int next_staging = 0;
     os::DeviceArray<unsigned char> dev;
     int64_t launches = 0;
 };
@@ -1733,7 +1743,7 @@ extern "C" int os_fdtd2d_batch_create(int32_t device, OsFdtd2DBatch **out) {
     OS_CUDA(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
     OS_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
     OS_CUDA(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
-    OS_CUDA(cudaEventCreateWithFlags(&b->ev_copied, cudaEventDisableTiming));
+    for (auto &st : b->staging) OS_CUDA(cudaEventCreateWithFlags(&st.copied, cudaEventDisableTiming));
     OS_CUDA(cudaEventCreate(&b->ev_start));
     OS_CUDA(cudaEventCreate(&b->ev_stop));
     *out = b.release();
@@ -1745,8 +1755,10 @@ extern "C" int os_fdtd2d_batch_destroy(OsFdtd2DBatch *b) {
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->side) cudaStreamSynchronize(b->side);
-    if (b->host) cudaFreeHost(b->host);
-    if (b->ev_copied) cudaEventDestroy(b->ev_copied);
+    for (auto &st : b->staging) {
+        if (st.host) cudaFreeHost(st.host);
+        if (st.copied) cudaEventDestroy(st.copied);
+    }
     if (b->ev_start) cudaEventDestroy(b->ev_start);
     if (b->ev_stop) cudaEventDestroy(b->ev_stop);
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
@@ -1859,11 +1871,10 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
                                               : Rect{0, 0, 0, 0};
                 for (int k = 1; k <= L.T; ++k) {
                     const EzFrameParams f = make_frame_params(h, L.T, k, base, run_interior ? &box : nullptr, in, out);
-                    const int64_t cells_k = f.first[f.n_rects];
-                    if (!cells_k) continue;
+                    if (!f.first[f.n_rects]) continue;
                     FrameStep &fs = L.frames[(size_t)(k - 1)];
                     fs.params.push_back(f);
-                    fs.block_start.push_back(fs.block_start.back() + (int32_t)((cells_k + 255) / 256));
+                    fs.block_start.push_back(fs.block_start.back() + (int32_t)frame_blocks(f));
                 }
             }
             for (int kind = 1; kind >= 0; --kind) {
@@ -1922,33 +1933,39 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
         L.items_off = total = align_up(total, 16);
         total += L.items.size() * sizeof(FluxBatchItem);
     }
-    if (b->copy_pending) {   // the previous call's copy still reads the staging block
-        OS_CUDA(cudaEventSynchronize(b->ev_copied));
-        b->copy_pending = false;
+    // a ring of staging blocks: a call waits only for the copy of the call kStaging calls back
+    OsFdtd2DBatch::Staging &st = b->staging[b->next_staging];
+    b->next_staging = (b->next_staging + 1) % OsFdtd2DBatch::kStaging;
+    if (st.pending) {
+        OS_CUDA(cudaEventSynchronize(st.copied));
+        st.pending = false;
     }
-    if (total > b->host_capacity) {
-        if (b->host) OS_CUDA(cudaFreeHost(b->host));
-        b->host = nullptr;
-        b->host_capacity = 0;
-        OS_CUDA(cudaHostAlloc((void **)&b->host, total, cudaHostAllocPortable));
-        b->host_capacity = total;
+    if (total > st.capacity) {   // grown by doubling: cudaFreeHost waits for the device
+        if (st.host) OS_CUDA(cudaFreeHost(st.host));
+        st.host = nullptr;
+        st.capacity = 0;
+        const size_t want = std::max(total, (size_t)2 * b->dev.capacity + ((size_t)1 << 20));
+        OS_CUDA(cudaHostAlloc((void **)&st.host, want, cudaHostAllocPortable));
+        st.capacity = want;
     }
+    unsigned char *const host = st.host;
     for (auto &L : launches) {
         for (auto &fs : L.frames) {
             if (fs.params.empty()) continue;
-            memcpy(b->host + fs.params_off, fs.params.data(), fs.params.size() * sizeof(EzFrameParams));
-            memcpy(b->host + fs.starts_off, fs.block_start.data(), fs.block_start.size() * sizeof(int32_t));
+            memcpy(host + fs.params_off, fs.params.data(), fs.params.size() * sizeof(EzFrameParams));
+            memcpy(host + fs.starts_off, fs.block_start.data(), fs.block_start.size() * sizeof(int32_t));
         }
         for (auto &g : L.groups) {
-            memcpy(b->host + g.params_off, g.params.data(), g.params.size() * sizeof(TBParams));
-            memcpy(b->host + g.tiles_off, g.tile_start.data(), g.tile_start.size() * sizeof(int));
+            memcpy(host + g.params_off, g.params.data(), g.params.size() * sizeof(TBParams));
+            memcpy(host + g.tiles_off, g.tile_start.data(), g.tile_start.size() * sizeof(int));
         }
-        if (!L.items.empty()) memcpy(b->host + L.items_off, L.items.data(), L.items.size() * sizeof(FluxBatchItem));
+        if (!L.items.empty()) memcpy(host + L.items_off, L.items.data(), L.items.size() * sizeof(FluxBatchItem));
     }
-    OS_TRY(b->dev.alloc(total));
-    OS_CUDA(cudaMemcpyAsync(b->dev.ptr, b->host, total, cudaMemcpyHostToDevice, b->stream));
-    OS_CUDA(cudaEventRecord(b->ev_copied, b->stream));
-    b->copy_pending = true;
+    // one device block, rewritten by each call's copy behind the previous call's launches on the stream
+    OS_TRY(b->dev.alloc(total > b->dev.capacity ? std::max(total, 2 * b->dev.capacity) : total, b->stream));
+    OS_CUDA(cudaMemcpyAsync(b->dev.ptr, host, total, cudaMemcpyHostToDevice, b->stream));
+    OS_CUDA(cudaEventRecord(st.copied, b->stream));
+    st.pending = true;
     OS_CUDA(cudaEventRecord(b->ev_start, b->stream));
     for (auto &L : launches) {
         // the frame steps fork onto the side stream and overlap the interior launches (disjoint cells; both read

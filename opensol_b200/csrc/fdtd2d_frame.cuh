@@ -5,9 +5,10 @@
 // launches over shrinking regions: step k (1..T) updates R_k = the grid minus `in` shrunk by T - k cells on each
 // non-periodic side, reading the state of step k - 1 (R_{k-1} contains every cell R_k reads) and writing that of
 // step k.  Step T writes exactly F, into the output buffer set, beside the interior kernel's cells; steps 1..T-1 write
-// scratch buffer sets.  Every cell of R_k is one thread: it updates its own H_x, H_y (with their CPML psi), evaluates
-// again the H_x left of it and the H_y below it (their psi not stored), then updates E_z with its CPML psi, the line
-// sources and, on a DFT sample step, stages the flux-line samples of the frame's own cells.  The arithmetic is that
+// scratch buffer sets.  Every cell of R_k is one thread: it updates its own H_x, H_y (with their CPML psi), takes the
+// H_x left of it from the lane before (the thread of that cell) or, at a warp's first lane and a rectangle's first
+// column, evaluates it again, evaluates again the H_y below it (their psi not stored), then updates E_z with its CPML
+// psi, the line sources and, on a DFT sample step, stages the flux-line samples of the frame's own cells.  The arithmetic is that
 // of ez2d_h_kernel / ez2d_e_kernel, in open_sol's order (fdtd_ez_2d_kernels.py:23-122, boundaries.py:27-37,
 // 752-760, core/sources.py:221-229), so the results are the same bits as every other path.
 #pragma once
@@ -125,8 +126,11 @@ __device__ __forceinline__ int64_t ezf_cells(const EzFrameParams &p) {
     return p.n_rects == 1 ? p.first[1] : p.n_rects == 2 ? p.first[2] : p.n_rects == 3 ? p.first[3] : p.first[4];
 }
 
-// The step of the region's t-th cell (t < ezf_cells(p)).
+// The step of the region's t-th cell.  Every lane of the warp calls it (the H_x hand-over is a warp shuffle); lanes
+// with t >= ezf_cells(p) compute nothing.
 __device__ __forceinline__ void ezf_cell(const EzFrameParams &p, int64_t t) {
+    const bool valid = t < ezf_cells(p);
+    if (!valid) t = 0;
     // the rectangle of this cell, selected without indexing the parameter arrays by a runtime value
     int k = 0;
     if (p.n_rects > 1 && t >= p.first[1]) k = 1;
@@ -147,16 +151,23 @@ __device__ __forceinline__ void ezf_cell(const EzFrameParams &p, int64_t t) {
     const int nx = p.nx, ny = p.ny, npml = p.npml;
     const size_t idx = (size_t)i * ny + j;
 
-    // ---- H half step: this cell's faces (stored), the H_x left of it and the H_y below it (evaluated again)
-    const float hx_c = ezf_hx_at(p, i, j, true);
-    const float hy_c = ezf_hy_at(p, i, j, true);
-    p.hx_out[idx] = hx_c;
-    p.hy_out[idx] = hy_c;
+    // ---- H half step: this cell's faces (stored), the H_x left of it (the lane before's when that lane holds
+    // cell (i, j - 1) of the same rectangle, else evaluated again) and the H_y below it (evaluated again)
+    float hx_c = 0.0f, hy_c = 0.0f;
+    if (valid) {
+        hx_c = ezf_hx_at(p, i, j, true);
+        hy_c = ezf_hy_at(p, i, j, true);
+        p.hx_out[idx] = hx_c;
+        p.hy_out[idx] = hy_c;
+    }
+    const float hx_lane_before = __shfl_up_sync(0xffffffffu, hx_c, 1);
+    if (!valid) return;
     const float one = 1.0f, zero = 0.0f;
     float hy_dn = 0.0f, hx_left = 0.0f;
     if (i >= 1) hy_dn = ezf_hy_at(p, i - 1, j, false);
     else if (p.px) hy_dn = ezf_hy_at(p, nx - 1, j, false);
-    if (j >= 1) hx_left = ezf_hx_at(p, i, j - 1, false);
+    if ((threadIdx.x & 31) != 0 && j > cc0) hx_left = hx_lane_before;   // thread t - 1: cell (i, j - 1)
+    else if (j >= 1) hx_left = ezf_hx_at(p, i, j - 1, false);
     else if (p.py) hx_left = ezf_hx_at(p, i, ny - 1, false);
 
     // ---- E half step (fdtd_ez_2d_kernels.py:103-120), E-row CPML x then y sides, line sources
@@ -221,8 +232,7 @@ __device__ __forceinline__ void ezf_cell(const EzFrameParams &p, int64_t t) {
 }
 
 __global__ void __launch_bounds__(256) ez2d_frame_step_kernel(const EzFrameParams p) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < ezf_cells(p)) ezf_cell(p, t);
+    ezf_cell(p, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // One frame step of several simulations in one launch.  Each block serves one job: job q owns blocks
@@ -244,6 +254,5 @@ __global__ void __launch_bounds__(256) ez2d_frame_step_batch_kernel(const EzFram
     for (int w = threadIdx.x; w < (int)(sizeof(EzFrameParams) / 4); w += blockDim.x) dst[w] = src[w];
     __syncthreads();
     const EzFrameParams &p = *reinterpret_cast<const EzFrameParams *>(smem);
-    const int64_t t = (int64_t)(b - block_start[lo]) * blockDim.x + threadIdx.x;
-    if (t < ezf_cells(p)) ezf_cell(p, t);
+    ezf_cell(p, (int64_t)(b - block_start[lo]) * blockDim.x + threadIdx.x);
 }

@@ -37,7 +37,7 @@ __device__ __forceinline__ float2 ip_sub_p(float2 a, float2 b) {
     return make_float2(__fadd_rn(a.x, -b.x), __fadd_rn(a.y, -b.y));
 }
 
-template <int T, bool CA, bool PX, bool PY, bool VEC>
+template <int T, bool CA, bool PX, bool PY, bool VEC, bool HELD>
 struct IPWarp {
     const TBParams &p;
     // tile
@@ -52,6 +52,20 @@ struct IPWarp {
     float2 db2, ixh2, ixe2, iyh2, iye2;
     float *ez_out, *hx_out, *hy_out;
     const float *__restrict__ ez_in, *__restrict__ hx_in, *__restrict__ hy_in, *__restrict__ cbp, *__restrict__ cap;
+    // HELD: the grid sizes, array pointers and bulk coefficients above are copied into registers once per tile (the
+    // one-grid kernel, whose p is its kernel parameter); otherwise they are read from p where they are used (the
+    // batched kernel, whose p is the warp's copy in shared memory), which keeps fewer registers live in the row loop
+    __device__ __forceinline__ int gnx() const { if constexpr (HELD) return nx; else return p.nx; }
+    __device__ __forceinline__ int gny() const { if constexpr (HELD) return ny; else return p.ny; }
+    __device__ __forceinline__ float2 pair(float2 held, float v) const {
+        if constexpr (HELD) return held;
+        else return make_float2(v, v);
+    }
+    template <typename P>
+    __device__ __forceinline__ P ptr(P held, P v) const {
+        if constexpr (HELD) return held;
+        else return v;
+    }
     // staging ring
     float *sm_fields, *sm_cb, *sm_ca;
     uint64_t *sm_bar;
@@ -62,12 +76,13 @@ struct IPWarp {
 
     __device__ __forceinline__ IPWarp(const TBParams &params) : p(params) {}
 
-    __device__ __forceinline__ int phys_row(int i) const { return PX ? tb_wrap(i, nx) : i; }
+    __device__ __forceinline__ int phys_row(int i) const { return PX ? tb_wrap(i, gnx()) : i; }
 
     // Offset (0..3 floats) of row R's first window column behind the 16-byte boundary its copy starts on (0 when
     // ny % 4 == 0; the host plans an interior on a row length that is not a multiple of 4 only for a non-periodic y).
     __device__ __forceinline__ int row_off(int R) const {
-        return vec ? 0 : (int)(((size_t)phys_row(R) * (size_t)ny + (size_t)(j0 - 4)) & 3u);
+        // (row * ny + j0 - 4) mod 4 in 32-bit arithmetic: a wrapped product keeps its value mod 4
+        return vec ? 0 : (int)(((uint32_t)phys_row(R) * (uint32_t)gny() + (uint32_t)j0) & 3u);
     }
 
     // Bulk copies of one row window (columns j0 - 4 .., 128 of them, clipped to the grid) into dst; returns the
@@ -76,13 +91,14 @@ struct IPWarp {
     __device__ __forceinline__ uint32_t window(float *dst, const float *src_row, uint64_t *bar, bool issue) const {
         if constexpr (!VEC) {
             const int col = j0 - 4;
-            const int len = min(128, ny - col);
+            const int len = min(128, gny() - col);
             const int off = (int)(((uintptr_t)(src_row + col) >> 2) & 3u);
             const uint32_t bytes = (uint32_t)((len + off + 3) & ~3) * 4u;
             if (issue) tb_bulk_g2s(dst, src_row + col - off, bytes, bar);
             return bytes;
         }
         uint32_t bytes = 0;
+        const int ny = gny();
         int remaining = 128, d = 0, col = PY ? tb_wrap(j0 - 4, ny) : j0 - 4;
         while (remaining > 0 && col < ny) {
             const int len = min(remaining, ny - col);
@@ -101,22 +117,36 @@ struct IPWarp {
         const int k = R - r_begin;
         const int fs = k % tb_field_slots(), cs = k % tb_coef_slots(T);
         uint64_t *bar = sm_bar + fs;
-        const size_t base = (size_t)phys_row(R) * (size_t)ny;
+        const size_t base = (size_t)phys_row(R) * (size_t)gny();
+        const float *e_in = ptr(ez_in, p.ez_in);
         // every array of the row has the same alignment (the arrays start 256-byte aligned), so the same byte count
-        const uint32_t bytes = vec ? row_bytes : window(nullptr, ez_in + base, nullptr, false);
+        const uint32_t bytes = vec ? row_bytes : window(nullptr, e_in + base, nullptr, false);
         tb_mbar_expect_tx(bar, bytes * (CA ? 5u : 4u));
         float *f = sm_fields + fs * (3 * IP_ROW);
-        window(f, ez_in + base, bar, true);
-        window(f + IP_ROW, hx_in + base, bar, true);
-        window(f + 2 * IP_ROW, hy_in + base, bar, true);
-        window(sm_cb + cs * IP_ROW, cbp + base, bar, true);
-        if (CA) window(sm_ca + cs * IP_ROW, cap + base, bar, true);
+        window(f, e_in + base, bar, true);
+        window(f + IP_ROW, ptr(hx_in, p.hx_in) + base, bar, true);
+        window(f + 2 * IP_ROW, ptr(hy_in, p.hy_in) + base, bar, true);
+        window(sm_cb + cs * IP_ROW, ptr(cbp, p.cb) + base, bar, true);
+        if (CA) window(sm_ca + cs * IP_ROW, ptr(cap, p.ca) + base, bar, true);
     }
 
-    // four consecutive floats of a staged window (16-byte aligned when vec)
-    __device__ __forceinline__ float4 ld_win(const float *q) const {
-        if constexpr (VEC) return *reinterpret_cast<const float4 *>(q);
-        else return make_float4(q[0], q[1], q[2], q[3]);
+    // The lane's four floats of a staged window: q = window + 4 lane (16-byte aligned), off = the row's offset
+    // (row_off).  An aligned row is one 16-byte read; otherwise two aligned 16-byte reads (conflict-free, where four
+    // scalar reads at a 16-byte lane stride would hit each bank four times) and a shift by the offset, which is the
+    // same for the whole warp.
+    __device__ __forceinline__ float4 ld_win(const float *q, int off) const {
+        const float4 a = *reinterpret_cast<const float4 *>(q);
+        if constexpr (VEC) {
+            return a;
+        } else {
+            const float4 b = *reinterpret_cast<const float4 *>(q + 4);
+            switch (off) {
+                case 0: return a;
+                case 1: return make_float4(a.y, a.z, a.w, b.x);
+                case 2: return make_float4(a.z, a.w, b.x, b.y);
+                default: return make_float4(a.w, b.x, b.y, b.z);
+            }
+        }
     }
 
     template <int PH>
@@ -124,10 +154,34 @@ struct IPWarp {
         const int k = R - r_begin;
         const int fs = k % tb_field_slots();
         if (R <= r_end && !tb_mbar_wait(sm_bar + fs, (uint32_t)((k / tb_field_slots()) & 1))) return false;
-        const float *f = sm_fields + fs * (3 * IP_ROW) + row_off(R) + lane * 4;
-        const float4 e = ld_win(f);
-        const float4 hx = ld_win(f + IP_ROW);
-        const float4 hy = ld_win(f + 2 * IP_ROW);
+        const float *f = sm_fields + fs * (3 * IP_ROW) + lane * 4;
+        float4 e, hx, hy;
+        if constexpr (VEC) {
+            e = ld_win(f, 0);
+            hx = ld_win(f + IP_ROW, 0);
+            hy = ld_win(f + 2 * IP_ROW, 0);
+        } else {   // the three windows of a row share its offset: one shift for all
+            const float4 a0 = *reinterpret_cast<const float4 *>(f), b0 = *reinterpret_cast<const float4 *>(f + 4);
+            const float4 a1 = *reinterpret_cast<const float4 *>(f + IP_ROW);
+            const float4 b1 = *reinterpret_cast<const float4 *>(f + IP_ROW + 4);
+            const float4 a2 = *reinterpret_cast<const float4 *>(f + 2 * IP_ROW);
+            const float4 b2 = *reinterpret_cast<const float4 *>(f + 2 * IP_ROW + 4);
+            switch (row_off(R)) {
+                case 0: e = a0, hx = a1, hy = a2; break;
+                case 1:
+                    e = make_float4(a0.y, a0.z, a0.w, b0.x), hx = make_float4(a1.y, a1.z, a1.w, b1.x);
+                    hy = make_float4(a2.y, a2.z, a2.w, b2.x);
+                    break;
+                case 2:
+                    e = make_float4(a0.z, a0.w, b0.x, b0.y), hx = make_float4(a1.z, a1.w, b1.x, b1.y);
+                    hy = make_float4(a2.z, a2.w, b2.x, b2.y);
+                    break;
+                default:
+                    e = make_float4(a0.w, b0.x, b0.y, b0.z), hx = make_float4(a1.w, b1.x, b1.y, b1.z);
+                    hy = make_float4(a2.w, b2.x, b2.y, b2.z);
+                    break;
+            }
+        }
         E[PH][0][0] = make_float2(e.x, e.y);
         E[PH][0][1] = make_float2(e.z, e.w);
         Hx[PH][0][0] = make_float2(hx.x, hx.y);
@@ -199,15 +253,18 @@ struct IPWarp {
         const int i = r - S;
         const int ip = phys_row(i);
         const int cs = (i - r_begin + tb_coef_slots(T)) % tb_coef_slots(T);
-        const int co = row_off(i) + lane * 4;
-        const float4 cbv = ld_win(sm_cb + cs * IP_ROW + co);
+        const int co = lane * 4, off = row_off(i);
+        const float4 cbv = ld_win(sm_cb + cs * IP_ROW + co, off);
         const float2 cb[2] = {make_float2(cbv.x, cbv.y), make_float2(cbv.z, cbv.w)};
         float2 ca[2];
         if constexpr (CA) {
-            const float4 cav = ld_win(sm_ca + cs * IP_ROW + co);
+            const float4 cav = ld_win(sm_ca + cs * IP_ROW + co, off);
             ca[0] = make_float2(cav.x, cav.y);
             ca[1] = make_float2(cav.z, cav.w);
         }
+        const float2 db2 = pair(this->db2, p.db_u), ixh2 = pair(this->ixh2, p.s_inv_dx_h);
+        const float2 iyh2 = pair(this->iyh2, p.s_inv_dy_h), ixe2 = pair(this->ixe2, p.s_inv_dx_e);
+        const float2 iye2 = pair(this->iye2, p.s_inv_dy_e);
         const float2(&eq)[2] = E[Q][S - 1];    // E^(S-1) of row i
         const float2(&eu)[2] = E[PH][S - 1];   // E^(S-1) of row i + 1
         // ---- H^S (fdtd_ez_2d_kernels.py:41-47 with da = 1)
@@ -248,7 +305,9 @@ struct IPWarp {
     __device__ __forceinline__ void store(int r) {
         const int i = r - T;
         if (i < i0 || i >= i1) return;
-        const size_t base = (size_t)phys_row(i) * (size_t)ny + jp0;
+        const size_t base = (size_t)phys_row(i) * (size_t)gny() + jp0;
+        float *ez_out = ptr(this->ez_out, p.ez_out), *hx_out = ptr(this->hx_out, p.hx_out);
+        float *hy_out = ptr(this->hy_out, p.hy_out);
         if (own == 0xFu && vec) {
             *reinterpret_cast<float4 *>(ez_out + base) =
                 make_float4(E[PH][T][0].x, E[PH][T][0].y, E[PH][T][1].x, E[PH][T][1].y);
@@ -256,6 +315,13 @@ struct IPWarp {
                 make_float4(Hx[PH][T][0].x, Hx[PH][T][0].y, Hx[PH][T][1].x, Hx[PH][T][1].y);
             *reinterpret_cast<float4 *>(hy_out + base) =
                 make_float4(Hy[PH][T][0].x, Hy[PH][T][0].y, Hy[PH][T][1].x, Hy[PH][T][1].y);
+        } else if (own == 0xFu) {   // a misaligned row: four scalar stores per field, no per-column tests
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                ez_out[base + 2 * k] = E[PH][T][k].x, ez_out[base + 2 * k + 1] = E[PH][T][k].y;
+                hx_out[base + 2 * k] = Hx[PH][T][k].x, hx_out[base + 2 * k + 1] = Hx[PH][T][k].y;
+                hy_out[base + 2 * k] = Hy[PH][T][k].x, hy_out[base + 2 * k + 1] = Hy[PH][T][k].y;
+            }
         } else if (own) {
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
@@ -299,7 +365,7 @@ struct IPWarp {
 };
 
 // One warp's tile w of the interior plan p (tb_smem: the block's dynamic shared memory).
-template <int T, bool CA, bool PX, bool PY, bool VEC>
+template <int T, bool CA, bool PX, bool PY, bool VEC, bool HELD>
 __device__ __forceinline__ void ez2d_interior_tile(const TBParams &p, int w, unsigned char *tb_smem) {
     const int lane = threadIdx.x & 31;
     if (w >= p.n_tiles) return;   // whole warps leave together
@@ -310,7 +376,7 @@ __device__ __forceinline__ void ez2d_interior_tile(const TBParams &p, int w, uns
     const int t = w - R.first_tile;
     const int tc = t % R.tiles_c, tr = t / R.tiles_c;
 
-    IPWarp<T, CA, PX, PY, VEC> W(p);
+    IPWarp<T, CA, PX, PY, VEC, HELD> W(p);
     W.lane = lane;
     W.nx = p.nx;
     W.ny = p.ny;
@@ -406,7 +472,7 @@ __device__ __forceinline__ void ez2d_interior_tile(const TBParams &p, int w, uns
 template <int T, bool CA, bool PX, bool PY, bool VEC>
 __global__ void __launch_bounds__(TB_WARPS * 32, 4) ez2d_interior_kernel(const TBParams p) {
     extern __shared__ __align__(16) unsigned char tb_smem[];
-    ez2d_interior_tile<T, CA, PX, PY, VEC>(p, blockIdx.x * TB_WARPS + (threadIdx.x >> 5), tb_smem);
+    ez2d_interior_tile<T, CA, PX, PY, VEC, true>(p, blockIdx.x * TB_WARPS + (threadIdx.x >> 5), tb_smem);
 }
 
 // Several simulations in one launch: warp g runs tile g - tile_start[job] of jobs[job], tile_start ascending with
@@ -430,5 +496,5 @@ __global__ void __launch_bounds__(TB_WARPS * 32, 4) ez2d_interior_batch_kernel(c
     uint32_t *dst = reinterpret_cast<uint32_t *>(mine);
     for (int w = threadIdx.x & 31; w < (int)(sizeof(TBParams) / 4); w += 32) dst[w] = src[w];
     __syncwarp();
-    ez2d_interior_tile<T, CA, PX, PY, VEC>(*mine, g - tile_start[job], tb_smem);
+    ez2d_interior_tile<T, CA, PX, PY, VEC, false>(*mine, g - tile_start[job], tb_smem);
 }

@@ -47,13 +47,14 @@ class BatchAdvancer:
 
     def advance(self, engines, n_steps, tables=None):
         """Enqueue n_steps steps of every engine (asynchronous).  tables: the engines' chunk_tables(n_steps) made
-        beforehand for their present clocks (None: made here)."""
+        beforehand for their present clocks (None, or a None entry: made here)."""
         n_steps = int(n_steps)
         n = len(engines)
         if n == 0 or n_steps <= 0:
             return
         if tables is None:
-            tables = [e.chunk_tables(n_steps) for e in engines]
+            tables = [None] * n
+        tables = [t if t is not None else e.chunk_tables(n_steps) for e, t in zip(engines, tables)]
         handles = (ctypes.c_void_p * n)(*[e.handle.value for e in engines])
         fp = ctypes.POINTER(ctypes.c_float)
         values = (fp * n)(*[_native.fptr(t[0]) if t[0].size else None for t in tables])
@@ -175,15 +176,21 @@ class _Active:
 
 
 class ServingLoop:
-    """Admission by memory budget and slots, all active jobs stepped together in batched launches.  Two steps per
-    blocked launch by default: with many jobs sharing the device the per-row latency of the interior tiles, not their
-    DRAM traffic, bounds a launch, and 2 steps measured faster than 3 or 4 (one job alone is fastest at 3)."""
+    """Admission by memory budget and slots, all active jobs stepped together in batched launches (three steps per
+    blocked launch, as for one job alone).
 
-    def __init__(self, device=0, memory_budget=120e9, max_active=48, chunk_steps=512, steps_per_launch=2,
-                 tile_rows=0):
+    A tick advances every active job by chunk_steps, or by what it has left when that is less: the jobs with a full
+    chunk left go together in one batched call, and the few that finish inside the tick in one call per remaining
+    step count, so a job near its end never shortens everyone's tick.  Order of admission: arrival order when
+    arrivals are honoured in real time; with every job queued at once, the largest (cells x steps) first, so that the
+    small jobs fill the slots at the end instead of one large job running alone."""
+
+    def __init__(self, device=0, memory_budget=120e9, max_active=48, chunk_steps=512, steps_per_launch=3,
+                 tile_rows=0, admit_per_tick=16):
         self.device = int(device)
         self.memory_budget = float(memory_budget)
         self.max_active = int(max_active)
+        self.admit_per_tick = max(1, int(admit_per_tick))
         self.chunk_steps = int(chunk_steps)
         self.steps_per_launch = int(steps_per_launch)
         self.tile_rows = int(tile_rows)
@@ -202,16 +209,22 @@ class ServingLoop:
 
         Each tick is enqueued first; while the device runs it the host admits arrivals (they join the next tick),
         makes the next tick's source and phase tables, and only then reads the fluxes of the jobs the tick finished
-        (which waits for it) and releases them."""
-        pending = deque(sorted(specs, key=lambda s: (s.arrival if realtime else 0.0, s.job_id)))
+        (which waits for it) and releases them.  At most admit_per_tick jobs are set up per tick, so a burst of
+        arrivals starts on the device while the rest of it is still being set up on the host."""
+        if realtime:
+            pending = deque(sorted(specs, key=lambda s: (s.arrival, s.job_id)))
+        else:
+            pending = deque(sorted(specs, key=lambda s: (-s.cells() * s.steps, s.job_id)))
         active, results = [], []
         used = 0
         t0 = time.perf_counter()
 
         def admit(into, held):
             now = time.perf_counter() - t0
-            while (pending and (not realtime or pending[0].arrival <= now) and len(into) < self.max_active
-                   and held + pending[0].device_bytes() <= self.memory_budget):
+            budget = self.admit_per_tick
+            while (pending and budget > 0 and (not realtime or pending[0].arrival <= now)
+                   and len(into) < self.max_active and held + pending[0].device_bytes() <= self.memory_budget):
+                budget -= 1
                 spec = pending.popleft()
                 sim, monitors = build_job(spec, self.device, self.steps_per_launch, self.tile_rows)
                 self.advancer.adopt(sim.em.engine)
@@ -219,35 +232,39 @@ class ServingLoop:
                 held += spec.device_bytes()
             return held
 
-        tables = None
+        def calls(jobs):
+            # (steps, jobs) of one tick: the jobs with a full chunk left together, the finishing ones by steps left
+            groups = {}
+            for a in jobs:
+                groups.setdefault(min(self.chunk_steps, a.remaining), []).append(a)
+            return sorted(groups.items(), key=lambda kv: -kv[0])
+
+        tables = {}   # id(job) -> its chunk tables for the next tick, made while the device runs the current one
         while pending or active:
             if not active:
                 used = admit(active, used)
-                tables = None
+                tables = {}
                 if not active:
                     if pending:
                         time.sleep(max(0.0, min(0.005, pending[0].arrival - (time.perf_counter() - t0))))
                     continue
             self.peak_active = max(self.peak_active, len(active))
             self.peak_bytes = max(self.peak_bytes, used)
-            chunk = min(self.chunk_steps, min(a.remaining for a in active))
-            self.advancer.advance([a.sim.em.engine for a in active], chunk, tables)
+            for n, group in calls(active):
+                self.advancer.advance([a.sim.em.engine for a in group], n, [tables.get(id(a)) for a in group])
+                for a in group:
+                    a.remaining -= n
+                if time_ticks:
+                    ms, launches = self.advancer.last_ms()
+                    self.device_ms += ms
+                    self.launches += launches
+                    self.tick_log.append((len(group), sum(a.spec.cells() for a in group) * n, ms))
             self.ticks += 1
-            for a in active:
-                a.remaining -= chunk
             done = [a for a in active if a.remaining == 0]
             survivors = [a for a in active if a.remaining > 0]
             # while the device runs the tick: arrivals join the next one, whose tables are made now
             used = admit(survivors, used)
-            tables = None
-            if survivors:
-                next_chunk = min(self.chunk_steps, min(a.remaining for a in survivors))
-                tables = [a.sim.em.engine.chunk_tables(next_chunk) for a in survivors]
-            if time_ticks:
-                ms, launches = self.advancer.last_ms()
-                self.device_ms += ms
-                self.launches += launches
-                self.tick_log.append((len(active), sum(a.spec.cells() for a in active) * chunk, ms))
+            tables = {id(a): a.sim.em.engine.chunk_tables(min(self.chunk_steps, a.remaining)) for a in survivors}
             for a in done:
                 fluxes = [m.flux() for m in a.monitors]
                 finished = time.perf_counter() - t0
@@ -259,10 +276,12 @@ class ServingLoop:
             active = survivors
         return results
 
-    def close(self):
-        """Release the batch and the device memory the finished jobs left in the engines' pool."""
+    def close(self, trim=True):
+        """Release the batch and (trim) the device memory the finished jobs left in the engines' pool; trim=False
+        keeps it for the next loop, whose jobs then take their arrays from the pool instead of cudaMalloc."""
         self.advancer.close()
-        _native.check(_native.load().os_fdtd_pool_trim())
+        if trim:
+            _native.check(_native.load().os_fdtd_pool_trim())
 
 
 def run_alone(spec, device=0, steps_per_launch=3, tile_rows=0):
