@@ -147,6 +147,18 @@ int os_fdtd2d_set_line_profile(OsFdtd2D *h, int32_t source_id, const float *prof
 int os_fdtd2d_add_flux_line(OsFdtd2D *h, int32_t normal_axis, int32_t position, int32_t lo, int32_t hi, int32_t nf,
                             int32_t *monitor_id);
 
+/* Field-map running DFT of E_z over the cell box [x_start, x_stop) x [y_start, y_stop): DFTMonitor (physics/em/
+ * monitors.py:248-311, polarization 'ez').  downsample s >= 1 samples every s-th cell along x and y from the middle of
+ * the first s-cell block (dft_sample_slice, monitors.py:152-155); nf frequencies; complex64 sums (nf, mx, my) updated
+ * at every DFT sample step with the chunk's phase table (whose rows follow the flux lines' rows, per map in add
+ * order).  A blocked advance ends a launch on every sample step when a map exists.  E_z engines only; not in batched
+ * advances. */
+int os_fdtd2d_add_dft_map(OsFdtd2D *h, int32_t x_start, int32_t x_stop, int32_t y_start, int32_t y_stop,
+                          int32_t downsample, int32_t nf, int32_t *map_id);
+
+/* Spectra of a field map: (nf, mx, my) complex64 as float pairs (DFTMonitor.ez_dft). */
+int os_fdtd2d_read_dft_map(OsFdtd2D *h, int32_t map_id, float *spectra);
+
 /* Steps between DFT samples (dft_sample_interval, physics/em/monitors.py:177-191). */
 int os_fdtd2d_set_sample_interval(OsFdtd2D *h, int64_t sample_interval);
 

@@ -8,13 +8,13 @@ from .boundaries import BCType, BoundaryConfig
 from .domain import Domain
 from .domain3d import BoundaryConfig3D, Domain3D
 from .grid import Grid2D, courant_time_step
-from .monitors import FluxMonitor, dft_sample_interval
+from .monitors import DFTMonitor, FluxMonitor, dft_sample_interval
 from .physics import EMPhysics
 from .physics3d import EMPhysics3D
 from .simulation import MultiphysicsRunner, Simulation
 from .sources import ContinuousWave, GaussianPulse, LineSource, RickerWavelet
 
-__all__ = ['BCType', 'BoundaryConfig', 'BoundaryConfig3D', 'Domain', 'Domain3D', 'EMPhysics3D', 'Grid2D', 'courant_time_step', 'FluxMonitor',
+__all__ = ['BCType', 'BoundaryConfig', 'BoundaryConfig3D', 'Domain', 'Domain3D', 'EMPhysics3D', 'Grid2D', 'courant_time_step', 'DFTMonitor', 'FluxMonitor',
            'dft_sample_interval', 'EMPhysics', 'MultiphysicsRunner', 'Simulation', 'ContinuousWave',
            'GaussianPulse', 'LineSource', 'RickerWavelet']
 __version__ = '0.1.0'

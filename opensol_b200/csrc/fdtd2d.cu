@@ -36,6 +36,11 @@ struct FluxLine2D {
     DeviceArray<float> stage;           // (TB_MAX_T, 2, n) samples of one launch
 };
 
+struct DftMap2D {                       // field-map running DFT of E_z (DFTMonitor)
+    int32_t x0, y0, ds, mx, my, nf;     // first sampled cell, stride, samples per axis, frequencies
+    DeviceArray<float> acc;             // (nf, mx, my) complex64 as float pairs
+};
+
 }  // namespace os
 
 struct OsFdtd2D {
@@ -70,6 +75,8 @@ struct OsFdtd2D {
     size_t prof_used = 0;
     std::vector<std::unique_ptr<os::LineSource2D>> lines;
     std::vector<std::unique_ptr<os::FluxLine2D>> fluxes;
+    std::vector<std::unique_ptr<os::DftMap2D>> maps;   // field-map DFTs (E_z engines), after the flux lines in a
+                                                       // chunk's phase table
     int64_t sample_interval = 1;
     int64_t n_step = 0;
     os::DeviceArray<int32_t> err;         // set by a kernel whose bounded wait ran out
@@ -123,6 +130,7 @@ static int zero_state(OsFdtd2D *h) {
         OS_CUDA(cudaMemsetAsync(f->e_acc.ptr, 0, f->e_acc.bytes(), h->stream));
         OS_CUDA(cudaMemsetAsync(f->h_acc.ptr, 0, f->h_acc.bytes(), h->stream));
     }
+    for (auto &d : h->maps) OS_CUDA(cudaMemsetAsync(d->acc.ptr, 0, d->acc.bytes(), h->stream));
     h->n_step = 0;
     return OS_OK;
 }
@@ -283,6 +291,7 @@ extern "C" int os_fdtd2d_destroy(OsFdtd2D *h) {
         for (int sd = 0; sd < 4; ++sd) give(h->cpml_rows[sd]);
         for (auto &l : h->lines) give(l->profile);
         for (auto &f : h->fluxes) give(f->e_acc), give(f->h_acc), give(f->stage);
+        for (auto &d : h->maps) give(d->acc);
         give(h->err), give(h->line_values), give(h->phases);
         pool_events_done(ev);
     }
@@ -949,6 +958,33 @@ static void bind_buffers(OsFdtd2D *h, TBParams &q, int in, int out) {
 
 // Temporally blocked chunk: launches of T steps (a shorter last one), buffers swapped after each.  `values` and
 // `phase_table` are the chunk's device tables (source values, DFT phases).
+// Floats of a chunk's phase table: per flux line, then per field map, (n_samples, nf) complex64 phases.
+static size_t phase_floats_of(const OsFdtd2D *h, int64_t n_samples) {
+    size_t n = 0;
+    for (auto &f : h->fluxes) n += (size_t)n_samples * f->nf * 2;
+    for (auto &d : h->maps) n += (size_t)n_samples * d->nf * 2;
+    return n;
+}
+
+// The field maps' DFT of sample q, from the E_z of buffer set `set` (the state right after the sample step).
+static int fold_maps(OsFdtd2D *h, const float *ez, int64_t q, int64_t first_sample, int64_t n_samples,
+                     const float *phase_table) {
+    size_t offset = 0;
+    for (auto &f : h->fluxes) offset += (size_t)n_samples * f->nf * 2;
+    for (auto &d : h->maps) {
+        const float *ph = phase_table + offset + (size_t)(q - first_sample) * d->nf * 2;
+        const int64_t total = (int64_t)d->nf * d->mx * d->my;
+        OS_TRY(prof_begin(h, 2, h->stream));
+        ez2d_dft_map_kernel<<<(unsigned)((total + 255) / 256), 256, 0, h->stream>>>(
+            ez, h->grid.ny, d->x0, d->y0, d->ds, d->mx, d->my, d->nf, ph, d->acc.ptr);
+        OS_TRY(prof_end(h, h->stream));
+        h->launches += 1;
+        offset += (size_t)n_samples * d->nf * 2;
+    }
+    OS_CUDA(cudaGetLastError());
+    return OS_OK;
+}
+
 static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples,
                            const float *values, const float *phase_table) {
     const int64_t m = h->sample_interval;
@@ -961,11 +997,10 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
         bool has_interior = false;
         std::vector<EzFrameParams> frame[2];   // [input buffer set][step - 1]
     };
-    LaunchPlan plans[2];
+    LaunchPlan plans[TB_MAX_T + 1];   // by T
     auto plan_for = [&](int T) -> LaunchPlan & {
-        for (LaunchPlan &pl : plans)
-            if (pl.T == T) return pl;
-        LaunchPlan &pl = plans[plans[0].T ? 1 : 0];
+        LaunchPlan &pl = plans[T];
+        if (pl.T == T) return pl;
         pl = LaunchPlan{};
         pl.T = T;
         plan_tiles(h, T, pl.interior, pl.general, pl.has_interior);
@@ -985,7 +1020,9 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
     };
     int64_t k = 0;
     while (k < n_steps) {
-        const int T = (int)std::min<int64_t>(h->steps_per_launch, n_steps - k);
+        int T = (int)std::min<int64_t>(h->steps_per_launch, n_steps - k);
+        // field maps read E_z between launches: a launch ends on every sample step
+        if (!h->maps.empty()) T = (int)std::min<int64_t>(T, m - h->n_step % m);
         LaunchPlan &pl = plan_for(T);
         TBParams interior = pl.interior, general = pl.general;
         const int in = h->cur, out = h->cur ^ 1;
@@ -1023,6 +1060,8 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
         }
         h->n_step += T;
         k += T;
+        if (!h->maps.empty() && h->n_step % m == 0)
+            OS_TRY(fold_maps(h, h->ez[h->cur].ptr, h->n_step / m, first_sample, n_samples, phase_table));
     }
     return OS_OK;
 }
@@ -1055,6 +1094,8 @@ static int advance_per_step(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, 
                 offset += (size_t)n_samples * f->nf * 2;
             }
         }
+        if (!h->maps.empty() && h->n_step % m == 0)
+            OS_TRY(fold_maps(h, p.ez, h->n_step / m, first_sample, n_samples, phase_table));
     }
     OS_CUDA(cudaGetLastError());
     return OS_OK;
@@ -1285,7 +1326,7 @@ static int check_advance(const OsFdtd2D *h, const char *fn, int64_t n_steps, con
     OS_CHECK(h->lines.empty() || line_values, OS_ERR_INVALID, "%s: line_values is required", fn);
     const int64_t m = h->sample_interval;
     const int64_t q_first = h->n_step / m + 1, q_last = (h->n_step + n_steps) / m;
-    if (!h->fluxes.empty() && q_last >= q_first) {
+    if ((!h->fluxes.empty() || !h->maps.empty()) && q_last >= q_first) {
         OS_CHECK(phases && first_sample <= q_first && first_sample + n_samples - 1 >= q_last, OS_ERR_INVALID,
                  "%s: the phase table covers samples [%lld, %lld), the chunk needs [%lld, %lld]", fn,
                  (long long)first_sample, (long long)(first_sample + n_samples), (long long)q_first,
@@ -1326,9 +1367,8 @@ extern "C" int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line
     if (n_steps == 0) return OS_OK;
     OS_TRY(bind_device(h));
     if (!h->lines.empty()) OS_TRY(upload(h->line_values, line_values, h->lines.size() * (size_t)n_steps, h->stream));
-    size_t phase_floats = 0;
-    for (auto &f : h->fluxes) phase_floats += (size_t)n_samples * f->nf * 2;
-    if (!h->fluxes.empty() && phase_floats && phases) OS_TRY(upload(h->phases, phases, phase_floats, h->stream));
+    const size_t phase_floats = phase_floats_of(h, n_samples);
+    if (phase_floats && phases) OS_TRY(upload(h->phases, phases, phase_floats, h->stream));
     return run_chunk(h, n_steps, first_sample, n_samples, h->line_values.ptr, h->phases.ptr);
 }
 
@@ -1375,9 +1415,7 @@ extern "C" int os_fdtd2d_advance_noalloc(OsFdtd2D *h, int64_t n_steps, const flo
              "os_fdtd2d_advance_noalloc: profiling is on (its event pool grows on demand); turn it off first");
     // tables: line values at float 0, phases at the next 64-float (256-byte) boundary
     const size_t value_floats = n_steps > 0 ? h->lines.size() * (size_t)n_steps : 0;
-    size_t phase_floats = 0;
-    if (n_steps > 0 && n_samples > 0)
-        for (auto &f : h->fluxes) phase_floats += (size_t)n_samples * f->nf * 2;
+    const size_t phase_floats = n_steps > 0 && n_samples > 0 ? phase_floats_of(h, n_samples) : 0;
     const size_t phase_offset = (value_floats + 63) / 64 * 64;
     const size_t need = phase_floats ? phase_offset + phase_floats : value_floats;
     OS_CHECK(need <= (size_t)OS_FDTD_NOALLOC_MAX_FLOATS, OS_ERR_INVALID,
@@ -1551,6 +1589,41 @@ extern "C" int os_fdtd2d_read_flux_spectra(OsFdtd2D *h, int32_t monitor_id, doub
     FluxLine2D &f = *h->fluxes[monitor_id];
     OS_CUDA(cudaMemcpyAsync(e_spectra, f.e_acc.ptr, f.e_acc.bytes(), cudaMemcpyDeviceToHost, h->stream));
     OS_CUDA(cudaMemcpyAsync(h_spectra, f.h_acc.ptr, f.h_acc.bytes(), cudaMemcpyDeviceToHost, h->stream));
+    OS_TRY(sync_and_check(h));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_add_dft_map(OsFdtd2D *h, int32_t x_start, int32_t x_stop, int32_t y_start, int32_t y_stop,
+                                     int32_t downsample, int32_t nf, int32_t *map_id) {
+    OS_TRY(require_ez(h, "os_fdtd2d_add_dft_map"));
+    OS_CHECK(0 <= x_start && x_start < x_stop && x_stop <= h->grid.nx && 0 <= y_start && y_start < y_stop &&
+                 y_stop <= h->grid.ny,
+             OS_ERR_INVALID, "DFTMonitor box [%d, %d) x [%d, %d) must be a non-empty box inside the %d x %d grid",
+             x_start, x_stop, y_start, y_stop, h->grid.nx, h->grid.ny);
+    OS_CHECK(downsample >= 1, OS_ERR_INVALID, "DFTMonitor downsample must be an int >= 1, got %d", downsample);
+    OS_CHECK(nf >= 1, OS_ERR_INVALID, "monitor frequencies must be a non-empty list");
+    OS_TRY(bind_device(h));
+    std::unique_ptr<DftMap2D> d(new DftMap2D());
+    // dft_sample_slice (monitors.py:152-155): every ds-th cell from the middle of the first ds-cell block
+    d->ds = downsample;
+    d->x0 = x_start + std::min(downsample, x_stop - x_start) / 2;
+    d->y0 = y_start + std::min(downsample, y_stop - y_start) / 2;
+    d->mx = (x_stop - d->x0 + downsample - 1) / downsample;
+    d->my = (y_stop - d->y0 + downsample - 1) / downsample;
+    d->nf = nf;
+    OS_TRY(d->acc.alloc((size_t)nf * d->mx * d->my * 2));
+    OS_CUDA(cudaMemsetAsync(d->acc.ptr, 0, d->acc.bytes(), h->stream));
+    if (map_id) *map_id = (int32_t)h->maps.size();
+    h->maps.push_back(std::move(d));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_read_dft_map(OsFdtd2D *h, int32_t map_id, float *spectra) {
+    OS_CHECK(h && spectra, OS_ERR_INVALID, "os_fdtd2d_read_dft_map: null argument");
+    OS_CHECK(map_id >= 0 && (size_t)map_id < h->maps.size(), OS_ERR_INVALID, "no field-map monitor %d", map_id);
+    OS_TRY(bind_device(h));
+    DftMap2D &d = *h->maps[map_id];
+    OS_CUDA(cudaMemcpyAsync(spectra, d.acc.ptr, d.acc.bytes(), cudaMemcpyDeviceToHost, h->stream));
     OS_TRY(sync_and_check(h));
     return OS_OK;
 }
@@ -1800,6 +1873,8 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
                  "os_fdtd2d_batch_advance: job %d is not on the batch stream (os_fdtd2d_set_stream with "
                  "os_fdtd2d_batch_stream)", q);
         OS_CHECK(!h->profiling, OS_ERR_STATE, "os_fdtd2d_batch_advance: job %d has profiling on", q);
+        OS_CHECK(h->maps.empty(), OS_ERR_STATE,
+                 "os_fdtd2d_batch_advance: job %d has field-map monitors (advance it with os_fdtd2d_advance)", q);
     }
     OS_CUDA(cudaSetDevice(b->device));
     // every job's own tables, in its own buffers, as os_fdtd2d_advance uploads them

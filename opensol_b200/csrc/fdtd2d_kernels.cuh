@@ -181,6 +181,25 @@ __global__ void ez2d_flux_kernel(const float *__restrict__ ez, const float *__re
     h_acc[a + 1] += pi * hv;
 }
 
+// Field-map DFT of E_z at one sample (DFTMonitor.update with _dft_accum_host, physics/em/monitors.py:36-37,281-311):
+// acc[f, a, b] += phase_f * E_z[x0 + a ds, y0 + b ds] in complex64 arithmetic: the float sample taken as a complex
+// number with imaginary part 0, the product's parts pr v - pi 0 and pr 0 + pi v, then the sum, each rounded to float.
+// One thread per (frequency, sample).
+__global__ void ez2d_dft_map_kernel(const float *__restrict__ ez, int ny, int x0, int y0, int ds, int mx, int my,
+                                    int nf, const float *__restrict__ phases, float *__restrict__ acc) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t per_f = (int64_t)mx * my;
+    if (t >= per_f * nf) return;
+    const int f = (int)(t / per_f);
+    const int64_t c = t - (int64_t)f * per_f;
+    const int a = (int)(c / my), b = (int)(c - (int64_t)a * my);
+    const float v = ez[(size_t)(x0 + a * ds) * ny + (size_t)(y0 + b * ds)];
+    const float pr = phases[2 * f], pi = phases[2 * f + 1], zero = 0.0f;
+    const float re = pr * v - pi * zero, im = pr * zero + pi * v;
+    acc[2 * t] = acc[2 * t] + re;
+    acc[2 * t + 1] = acc[2 * t + 1] + im;
+}
+
 // ca / cb from float32 eps_r, sigma_e (fdtd_ez_2d_kernels.py:314-332, T = float); sigma NULL = lossless (ca not
 // written: it is 1).
 __global__ void ez2d_e_coefficients_kernel(const float *__restrict__ eps_r, const float *__restrict__ sigma, float dt,

@@ -46,6 +46,7 @@ class FDTDEngine2D_Ez:
         self._line_ids = {}       # id(source) -> native id
         self._profiles_sent = {}  # id(source) -> profile array last uploaded
         self._monitors = []       # FluxMonitor objects in add order
+        self._maps = []           # DFTMonitor objects in add order
         self._monitor_ids = {}
         self._materials_version = None
         self.sample_interval = 1
@@ -97,6 +98,13 @@ class FDTDEngine2D_Ez:
         self._monitors.append(monitor)
         monitor._reader = lambda m=monitor: self.read_flux_spectra(m)
 
+    def attach_dft_monitor(self, monitor):
+        """Register a field-map DFTMonitor (E_z engines); its device sums are created at the next sync."""
+        if self.polarization != 'ez':
+            raise NotImplementedError('field-map DFT monitors are built for the E_z engine only')
+        self._maps.append(monitor)
+        monitor._reader = lambda m=monitor: self.read_dft_map(m)
+
     def set_sample_interval(self, m):
         self.sample_interval = int(m)
 
@@ -127,6 +135,13 @@ class FDTDEngine2D_Ez:
                 normal = 0 if monitor.axis == 'x' else 1
                 _native.check(lib.os_fdtd2d_add_flux_line(h, normal, monitor.position, monitor.span[0],
                                                           monitor.span[1], monitor.n_freqs, ctypes.byref(mid)))
+                self._monitor_ids[id(monitor)] = mid.value
+        for monitor in self._maps:
+            if id(monitor) not in self._monitor_ids:
+                mid = ctypes.c_int32()
+                xs, ys = monitor.x_slice, monitor.y_slice
+                _native.check(lib.os_fdtd2d_add_dft_map(h, xs.start or 0, xs.stop, ys.start or 0, ys.stop,
+                                                        monitor.downsample, monitor.n_freqs, ctypes.byref(mid)))
                 self._monitor_ids[id(monitor)] = mid.value
         if self._sample_interval_sent != self.sample_interval:
             _native.check(lib.os_fdtd2d_set_sample_interval(h, self.sample_interval))
@@ -218,7 +233,7 @@ class FDTDEngine2D_Ez:
         last_q = (self.n_step + n_steps) // m
         n_q = max(0, last_q - first_q + 1)
         tables = []
-        for monitor in self._monitors:
+        for monitor in self._monitors + self._maps:   # flux lines, then field maps (the device's table order)
             times = [t_full[q * m - self.n_step - 1] for q in range(first_q, first_q + n_q)]
             tables.append(dft_phase_table(2.0 * np.pi * monitor.frequencies, times, monitor.dt * m))
         phases = np.concatenate([tb.reshape(-1) for tb in tables]) if tables else np.zeros(0, np.float32)
@@ -288,6 +303,15 @@ class FDTDEngine2D_Ez:
         _native.check(_native.load().os_fdtd2d_read_flux_spectra(self.handle, mid, _native.dptr(e),
                                                                  _native.dptr(h)))
         return e[..., 0] + 1j * e[..., 1], h[..., 0] + 1j * h[..., 1]
+
+    def read_dft_map(self, monitor):
+        """(nf, mx, my) complex64 running DFT of a field-map monitor."""
+        if id(monitor) not in self._monitor_ids:
+            self.sync_device()
+        out = np.empty((monitor.n_freqs, monitor.mx, monitor.my, 2), dtype=np.float32)
+        _native.check(_native.load().os_fdtd2d_read_dft_map(self.handle, self._monitor_ids[id(monitor)],
+                                                            _native.fptr(out)))
+        return out.view(np.complex64)[..., 0]
 
     def state(self):
         """Host copies of the public fields (FDTDEngine2D_Ez.state, fdtd_ez_2d.py:56-67)."""

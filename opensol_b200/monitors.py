@@ -1,4 +1,4 @@
-"""Flux monitors and the DFT sampling rule of the B200 engines.
+"""Flux monitors, field-map DFT monitors and the DFT sampling rule of the B200 engines.
 
 The running DFTs live on the device as float64 (complex128) sums, exactly like open_sol's line spectra
 (open_sol/physics/em/monitors.py:84-96): each term is a float32 phase times a float32 field sample, which is exact in
@@ -103,3 +103,44 @@ class FluxMonitor:
         e_time_average = np.cos(np.pi * self.frequencies * self.dt)
         integrand = self._flux_sign * e_time_average[:, None] * np.real(e_spectra * np.conj(h_spectra))
         return integrand @ self._cell_widths
+
+
+def dft_sample_slice(start: int, stop: int, stride: int) -> slice:
+    """Cells a DFTMonitor samples along one axis of the box [start, stop): every stride-th cell from the middle of the
+    first stride-cell block (monitors.py:152-155)."""
+    return slice(start + min(stride, stop - start) // 2, stop, stride)
+
+
+class DFTMonitor:
+    """Running DFT of E_z over the cell box (x_slice, y_slice) at each frequency (physics/em/monitors.py:248-311,
+    polarization 'ez'): ez_dft[f, a, b] += phase_f * E_z at every DFT sample step, complex64 sums on the device;
+    downsample s > 1 records every s-th cell along x and y (x_samples / y_samples)."""
+
+    def __init__(self, x_slice, y_slice, frequencies, dt, polarization='ez', downsample=1):
+        for label, cells in (('x_slice', x_slice), ('y_slice', y_slice)):
+            if cells.step not in (None, 1) or cells.stop is None or not (cells.start or 0) < cells.stop:
+                raise ValueError(f"DFTMonitor {label} must be a non-empty unit-step slice, got {cells}")
+        if isinstance(downsample, bool) or int(downsample) != downsample or downsample < 1:
+            raise ValueError(f"DFTMonitor downsample must be an int >= 1, got {downsample!r}")
+        if polarization != 'ez':
+            raise NotImplementedError("field-map DFT monitors are built for polarization 'ez' only")
+        self.polarization = polarization
+        self.x_slice = x_slice
+        self.y_slice = y_slice
+        self.downsample = int(downsample)
+        self.x_samples = dft_sample_slice(x_slice.start or 0, x_slice.stop, self.downsample)
+        self.y_samples = dft_sample_slice(y_slice.start or 0, y_slice.stop, self.downsample)
+        self.frequencies = check_frequencies(frequencies)
+        self.dt = float(dt)
+        self.n_freqs = len(self.frequencies)
+        self.mx = len(range(self.x_samples.start, self.x_samples.stop, self.downsample))
+        self.my = len(range(self.y_samples.start, self.y_samples.stop, self.downsample))
+        self.sample_interval = 1
+        self._reader = None   # () -> complex64 (nf, mx, my), set by the engine
+
+    @property
+    def ez_dft(self):
+        """(n_freqs, mx, my) complex64 running DFT of E_z (read from the device)."""
+        if self._reader is None:
+            return np.zeros((self.n_freqs, self.mx, self.my), np.complex64)
+        return self._reader()

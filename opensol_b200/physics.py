@@ -16,7 +16,7 @@ import numpy as np
 from .boundaries import BoundaryConfig, inverse_spacings
 from .constants import C0, DTYPE
 from .engine2d import FDTDEngine2D_Ez, FDTDEngine2D_Hz
-from .monitors import FluxMonitor, dft_sample_interval, resolve_frequencies
+from .monitors import DFTMonitor, FluxMonitor, dft_sample_interval, resolve_frequencies
 from .sources import (LineSource, calibrate_line_source, calibrate_tangential_sheet, carrier_angular_frequency,
                       make_temporal, resolve_frequency)
 
@@ -237,6 +237,22 @@ class EMPhysics:
         return source
 
     # --- monitors ---------------------------------------------------------------------------------------
+    def add_dft_monitor(self, x0, y0, x1, y1, wavelengths=None, frequencies=None, downsample=1):
+        """Running DFT of E_z over the cell box of the physical box (x0, y0)-(x1, y1); downsample s > 1 records every
+        s-th cell along x and y (physics/em/__init__.py:500-509, placement.box_cells)."""
+        d = self.domain
+        d.validate_physical_pos(x0, y0, "DFT monitor corner 0")
+        d.validate_physical_pos(x1, y1, "DFT monitor corner 1")
+        x_lo, x_hi = sorted((x0, x1))
+        y_lo, y_hi = sorted((y0, y1))
+        cells = (d.pos_to_cell_x(x_lo), d.pos_to_cell_x(x_hi) + 1, d.pos_to_cell_y(y_lo), d.pos_to_cell_y(y_hi) + 1)
+        monitor = DFTMonitor(slice(cells[0], cells[1]), slice(cells[2], cells[3]),
+                             resolve_frequencies(wavelengths, frequencies), float(d.grid.dt),
+                             polarization=self.polarization, downsample=downsample)
+        self.monitors.append(monitor)
+        self.engine.attach_dft_monitor(monitor)
+        return monitor
+
     def add_flux_monitor(self, axis, position, span, wavelengths=None, frequencies=None):
         """Poynting flux through a line (axis 'x' = along x at y = position, flux > 0 toward +y)
         (physics/em/__init__.py:511-518, placement.flux_line_cells)."""

@@ -408,6 +408,7 @@ class OracleEz2D:
         self.hx = np.zeros(shape, dtype=self.real)
         self.hy = np.zeros(shape, dtype=self.real)
         self.sources, self.monitors = [], []
+        self.maps = []           # field-map DFT monitors (add_dft_monitor)
         self.n_step = 0
         self.time = 0.0          # engine clock (host float64 accumulation)
         self.runner_t = 0.0      # runner clock
@@ -470,6 +471,37 @@ class OracleEz2D:
         self.monitors.append(mon)
         return mon
 
+    def add_dft_monitor(self, x0, y0, x1, y1, wavelengths=None, frequencies=None, downsample=1):
+        """physics/em/__init__.py:500-509 with placement.box_cells (placement.py:97-105) and DFTMonitor
+        (monitors.py:248-289, polarization 'ez'): the cell box of the physical box, sampled every `downsample`-th cell
+        from the middle of the first block (dft_sample_slice, monitors.py:152-155); complex64 sums (nf, mx, my)."""
+        d = self.domain
+        freqs = (np.atleast_1d(np.array(frequencies, dtype=np.float64)) if frequencies is not None
+                 else C0 / np.atleast_1d(np.array(wavelengths, dtype=np.float64)))
+        x_lo, x_hi = sorted((x0, x1))
+        y_lo, y_hi = sorted((y0, y1))
+        ix0, ix1 = d.pos_to_cell_x(x_lo), d.pos_to_cell_x(x_hi) + 1
+        iy0, iy1 = d.pos_to_cell_y(y_lo), d.pos_to_cell_y(y_hi) + 1
+        ds = int(downsample)
+        xs = slice(ix0 + min(ds, ix1 - ix0) // 2, ix1, ds)
+        ys = slice(iy0 + min(ds, iy1 - iy0) // 2, iy1, ds)
+        mon = FluxMonitor.__new__(FluxMonitor)   # a plain record: frequencies, dt, sample boxes, sums
+        mon.frequencies, mon.dt, mon.x_samples, mon.y_samples, mon.downsample = freqs, float(d.dt), xs, ys, ds
+        mon.ez_dft = np.zeros((freqs.size, len(range(xs.start, xs.stop, ds)), len(range(ys.start, ys.stop, ds))),
+                              dtype=np.complex64)
+        self.maps.append(mon)
+        return mon
+
+    def _fold_maps(self):
+        """DFTMonitor.update at a sample step (monitors.py:281-311) with _dft_accum_host (:36-37): the complex64
+        phase exp(-j omega t) m dt at the engine clock, then acc += phase * E_z[box] in numpy complex64."""
+        m = self.sample_interval
+        for mon in self.maps:
+            table = dft_phases(2.0 * np.pi * mon.frequencies, self.time, mon.dt * m)
+            ph = (table[:, 0] + 1j * table[:, 1]).astype(np.complex64)
+            f = np.asarray(self.ez[mon.x_samples, mon.y_samples], dtype=np.float32)
+            mon.ez_dft += ph[:, None, None] * f[None, :, :]
+
     # -- finalize: coefficients, CPML, calibration, sample interval
     def finalize(self):
         d, real = self.domain, self.real
@@ -488,8 +520,9 @@ class OracleEz2D:
                                           float(d.dt))
             weight = np.asarray(2.0 * np.ones(src.hi - src.lo) / (float(ETA0) * src.normal_width), dtype=DTYPE)
             src.profile = (self.cb[line] * admittance * weight).astype(DTYPE)
-        self.sample_interval = dft_sample_interval(float(d.dt), self.sources, [m.frequencies for m in self.monitors])
-        for m in self.monitors:
+        self.sample_interval = dft_sample_interval(float(d.dt), self.sources,
+                                                   [m.frequencies for m in self.monitors + self.maps])
+        for m in self.monitors + self.maps:
             m.sample_interval = self.sample_interval
         self.psi_e = {s.name: np.zeros(self._psi_shape(s.name), dtype=real) for s in self.cpml_sides}
         self.psi_h = {s.name: np.zeros(self._psi_shape(s.name), dtype=real) for s in self.cpml_sides}
@@ -595,6 +628,20 @@ class OracleEz2D:
             self.runner_t = self.runner_t + dt
 
     def advance(self, n_steps):
+        """n_steps steps; with field maps, in pieces that end on the DFT sample steps, each followed by the maps'
+        update (the reference updates its monitors after every sampled step)."""
+        if not self.maps:
+            self._advance_chunk(n_steps)
+            return
+        m = self.sample_interval
+        while n_steps > 0:
+            piece = min(n_steps, m - self.n_step % m)
+            self._advance_chunk(piece)
+            n_steps -= piece
+            if self.n_step % m == 0:
+                self._fold_maps()
+
+    def _advance_chunk(self, n_steps):
         lib, State, Line, Flux = load_library(self.real)
         d, real = self.domain, self.real
         R = ctypes.c_float if real == np.float32 else ctypes.c_double

@@ -1,0 +1,42 @@
+"""Cases with field-map (running DFT) monitors, shared by the golden-fixture generator (run on open_sol itself),
+the oracle pinning tests and the GPU parity tests.  Same form as cases.py; 'dft' lists the field-map monitors added
+through the E_z physics (x0, y0, x1, y1 [m], frequencies [Hz], downsample)."""
+
+CASES_DFT = [
+    {   # all-CPML box: cylinder, lossy rectangle, spanned line source, flux line, a full-resolution map and a
+        # 3x-downsampled map whose box is not a multiple of 3 cells
+        'name': 'dft_pml',
+        'sim': {'size_x': 1.5e-6, 'size_y': 1.2e-6, 'dx': 25e-9, 'npml': 10, 'boundaries': 'pml'},
+        'ops': [
+            ['add_dielectric_circle', [0.75e-6, 0.7e-6, 0.2e-6], {'eps_r': 4.0}],
+            ['add_dielectric_rectangle', [0.2e-6, 0.9e-6, 0.6e-6, 1.1e-6], {'eps_r': 2.0, 'sigma_e': 5e4}],
+            ['add_line_source', ['x', 0.35e-6], {'wavelength': 700e-9, 'bandwidth': 0.6, 'span': [0.3e-6, 1.2e-6]}],
+            ['add_flux_monitor', ['x', 1.0e-6, [0.2e-6, 1.3e-6]], {'wavelengths': [600e-9, 700e-9]}],
+        ],
+        'dft': [
+            [0.3e-6, 0.2e-6, 1.2e-6, 1.0e-6, [4.2e14, 5.0e14], 1],
+            [0.1e-6, 0.05e-6, 1.4e-6, 1.15e-6, [4.6e14], 3],
+        ],
+        'checkpoints': [250, 500],
+    },
+    {   # periodic y, CPML in x: a map crossing the slab and one touching the y edge of the grid
+        'name': 'dft_periodic_y',
+        'sim': {'size_x': 2.0e-6, 'size_y': 1.0e-6, 'dx': 25e-9, 'npml': 12, 'boundaries': 'periodic_y'},
+        'ops': [
+            ['add_dielectric_rectangle', [1.0e-6, 0.0, 1.3e-6, 1.0e-6], {'eps_r': 2.25}],
+            ['add_line_source', ['y', 0.5e-6], {'wavelength': 650e-9, 'bandwidth': 0.7}],
+            ['add_flux_monitor', ['y', 1.6e-6, [0.0, 1.0e-6]], {'wavelengths': [650e-9]}],
+        ],
+        'dft': [
+            [0.7e-6, 0.0, 1.8e-6, 0.99e-6, [4.0e14, 4.6e14, 5.2e14], 2],
+        ],
+        'checkpoints': [300, 600],
+    },
+]
+
+
+def case(name):
+    for c in CASES_DFT:
+        if c['name'] == name:
+            return c
+    raise KeyError(name)

@@ -1,0 +1,112 @@
+"""GPU parity of the field-map (running DFT) monitors of the 2D E_z engine, through the C ABI, against open_sol's own
+maps (tests/golden/dft_*.npz) and the oracle.  Bar: bit-identical complex64 maps (array_equal), for every kernel
+variant and for chunk boundaries that do and do not fall on sample steps."""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from cases import apply_ops
+from cases_dft import CASES_DFT
+from oracle.fdtd2d import OracleEz2D
+from test_oracle_golden_dft import run_oracle_dft
+
+import opensol_b200 as ob
+from opensol_b200 import serving
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), 'golden')
+CONFIGS = [(1, 3, 0), (1, 2, 8), (1, 4, 16), (2, 3, 0), (0, 1, 0)]   # (variant, steps per launch, tile rows)
+
+
+def _digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def _build(spec, config):
+    sim = ob.Simulation(**spec['sim'], verbose=False)
+    fluxes = apply_ops(sim, spec)
+    maps = [sim.em.add_dft_monitor(x0, y0, x1, y1, frequencies=f, downsample=ds)
+            for x0, y0, x1, y1, f, ds in spec['dft']]
+    sim.em.engine.configure(variant=config[0], steps_per_launch=config[1], tile_rows=config[2])
+    return sim, fluxes, maps
+
+
+@pytest.mark.parametrize('config', CONFIGS, ids=[f'v{c[0]}_T{c[1]}_r{c[2]}' for c in CONFIGS])
+@pytest.mark.parametrize('spec', CASES_DFT, ids=[c['name'] for c in CASES_DFT])
+def test_maps_bit_exact_against_reference(spec, config):
+    g = np.load(os.path.join(GOLDEN, f"{spec['name']}.npz"))
+    sim, fluxes, maps = _build(spec, config)
+    done = 0
+    for cp in spec['checkpoints']:
+        sim.run(n_steps=cp - done, verbose=False, print_every=0)
+        done = cp
+        for name in ('ez', 'hx', 'hy'):
+            assert _digest(sim.em.engine.read_field(name)) == str(g[f'sha_{name}_{cp}']), f'{name} at {cp}'
+        for k, mon in enumerate(maps):
+            got = mon.ez_dft
+            assert got.dtype == np.complex64
+            np.testing.assert_array_equal(got, g[f'map{k}_{cp}'])
+        for k, mon in enumerate(fluxes):
+            np.testing.assert_array_equal(mon.spectra()[0], g[f'spec_e{k}_{cp}'])
+    sim.em.engine.close()
+
+
+@pytest.mark.parametrize('seed', [0, 1, 2])
+def test_random_maps_and_chunks_match_oracle(seed):
+    """Seeded boxes and downsample factors; the run advances in chunks of random length, so chunk ends fall both on
+    and between DFT sample steps."""
+    rng = np.random.default_rng(100 + seed)
+    spec = {'sim': {'size_x': 1.4e-6, 'size_y': 1.1e-6, 'dx': 25e-9, 'npml': 8,
+                    'boundaries': ['pml', 'periodic_x', 'periodic_y'][seed]},
+            'ops': [['add_dielectric_circle', [0.7e-6, 0.55e-6, 0.25e-6], {'eps_r': 3.0}],
+                    ['add_line_source', ['y' if seed != 2 else 'x', 0.3e-6], {'wavelength': 700e-9,
+                                                                              'bandwidth': 0.6}],
+                    ['add_flux_monitor', ['y', 1.0e-6, [0.1e-6, 1.0e-6]], {'wavelengths': [650e-9, 750e-9]}]],
+            'dft': []}
+    for _ in range(3):
+        x0, x1 = sorted(rng.uniform(0.0, 1.4e-6, 2))
+        y0, y1 = sorted(rng.uniform(0.0, 1.1e-6, 2))
+        spec['dft'].append([x0, y0, x1 - 1e-12, y1 - 1e-12, list(rng.uniform(3.5e14, 5.5e14, int(rng.integers(1, 4)))),
+                            int(rng.integers(1, 5))])
+    chunks = [int(c) for c in rng.integers(1, 60, 12)]
+    spec['checkpoints'] = list(np.cumsum(chunks))
+    _, o_maps, snaps = run_oracle_dft(spec)
+    sim, _, maps = _build(spec, CONFIGS[seed % 2])
+    sim.em.finalize()
+    done = 0
+    for cp in spec['checkpoints']:
+        sim.em.engine.advance(int(cp - done))
+        done = cp
+        for k, mon in enumerate(maps):
+            np.testing.assert_array_equal(mon.ez_dft, snaps[cp][0][k])
+    sim.em.engine.close()
+
+
+def test_reset_zeroes_maps_and_reruns_identically():
+    spec = CASES_DFT[0]
+    sim, _, maps = _build(spec, CONFIGS[0])
+    sim.run(n_steps=200, verbose=False, print_every=0)
+    first = [m.ez_dft.copy() for m in maps]
+    sim.em.engine.reset()
+    for m in maps:
+        assert not np.any(m.ez_dft)
+    sim.em.engine.advance(200)
+    for a, m in zip(first, maps):
+        np.testing.assert_array_equal(m.ez_dft, a)
+    sim.em.engine.close()
+
+
+def test_batched_advance_refuses_maps():
+    spec = CASES_DFT[0]
+    sim, _, _ = _build(spec, CONFIGS[0])
+    sim.em.finalize()
+    advancer = serving.BatchAdvancer(0)
+    try:
+        advancer.adopt(sim.em.engine)
+        with pytest.raises(RuntimeError, match='field-map'):
+            advancer.advance([sim.em.engine], 30)
+    finally:
+        advancer.close()
+        sim.em.engine.close()
