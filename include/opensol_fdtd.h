@@ -159,6 +159,16 @@ int os_fdtd2d_add_dft_map(OsFdtd2D *h, int32_t x_start, int32_t x_stop, int32_t 
 /* Spectra of a field map: (nf, mx, my) complex64 as float pairs (DFTMonitor.ez_dft). */
 int os_fdtd2d_read_dft_map(OsFdtd2D *h, int32_t map_id, float *spectra);
 
+/* Field probe: one component (OS_EZ / OS_HX / OS_HY, or OS_HZ_* on an H_z handle) of cell (ix, iy) recorded after
+ * every step from the current one on: FieldProbe.record at t_full (core/monitors.py:194-243, fdtd_2d_base.py:481-487).
+ * At most 8.  An advance with probes runs one step per launch.  Not in batched advances; os_fdtd2d_advance_noalloc
+ * refuses a chunk for which the probes' rows would have to grow. */
+int os_fdtd2d_add_probe(OsFdtd2D *h, int32_t ix, int32_t iy, int32_t component, int32_t *probe_id);
+
+/* The probe's values since it was added (or since the last reset), one per step, float32; *n_values = their count
+ * (values may be NULL to ask for it). */
+int os_fdtd2d_read_probe(OsFdtd2D *h, int32_t probe_id, float *values, int64_t max_values, int64_t *n_values);
+
 /* Steps between DFT samples (dft_sample_interval, physics/em/monitors.py:177-191). */
 int os_fdtd2d_set_sample_interval(OsFdtd2D *h, int64_t sample_interval);
 

@@ -36,6 +36,15 @@ struct FluxLine2D {
     DeviceArray<float> stage;           // (TB_MAX_T, 2, n) samples of one launch
 };
 
+// Field probes: one component of one cell recorded after every step.  rows holds, per probe, `capacity` floats
+// indexed by the step (n_step after the step - 1); a probe added at step s has rows from s on.
+constexpr int OS_MAX_PROBES = 8;
+struct ProbeSet {
+    int32_t n;
+    int32_t ix[OS_MAX_PROBES], iy[OS_MAX_PROBES], comp[OS_MAX_PROBES];
+    int64_t start[OS_MAX_PROBES];
+};
+
 struct DftMap2D {                       // field-map running DFT of E_z (DFTMonitor)
     int32_t x0, y0, ds, mx, my, nf;     // first sampled cell, stride, samples per axis, frequencies
     DeviceArray<float> acc;             // (nf, mx, my) complex64 as float pairs
@@ -77,6 +86,9 @@ struct OsFdtd2D {
     std::vector<std::unique_ptr<os::FluxLine2D>> fluxes;
     std::vector<std::unique_ptr<os::DftMap2D>> maps;   // field-map DFTs (E_z engines), after the flux lines in a
                                                        // chunk's phase table
+    os::ProbeSet probes{};                // field probes (recorded after every step)
+    os::DeviceArray<float> probe_rows;    // (OS_MAX_PROBES, probe_capacity) values by step
+    int64_t probe_capacity = 0;           // rows per probe
     int64_t sample_interval = 1;
     int64_t n_step = 0;
     os::DeviceArray<int32_t> err;         // set by a kernel whose bounded wait ran out
@@ -131,6 +143,7 @@ static int zero_state(OsFdtd2D *h) {
         OS_CUDA(cudaMemsetAsync(f->h_acc.ptr, 0, f->h_acc.bytes(), h->stream));
     }
     for (auto &d : h->maps) OS_CUDA(cudaMemsetAsync(d->acc.ptr, 0, d->acc.bytes(), h->stream));
+    for (int k = 0; k < h->probes.n; ++k) h->probes.start[k] = 0;   // rows recorded again from step 0
     h->n_step = 0;
     return OS_OK;
 }
@@ -292,6 +305,7 @@ extern "C" int os_fdtd2d_destroy(OsFdtd2D *h) {
         for (auto &l : h->lines) give(l->profile);
         for (auto &f : h->fluxes) give(f->e_acc), give(f->h_acc), give(f->stage);
         for (auto &d : h->maps) give(d->acc);
+        give(h->probe_rows);
         give(h->err), give(h->line_values), give(h->phases);
         pool_events_done(ev);
     }
@@ -985,6 +999,49 @@ static int fold_maps(OsFdtd2D *h, const float *ez, int64_t q, int64_t first_samp
     return OS_OK;
 }
 
+// The probes' values after step `row` + 1 from the buffer set `set` (FieldProbe.record at t_full,
+// fdtd_2d_base.py:481-487).  One warp.
+__global__ void ez2d_probe_kernel(ProbeSet ps, const float *f0, const float *f1, const float *f2, int ny, float *rows,
+                                  int64_t capacity, int64_t row) {
+    const int k = threadIdx.x;
+    if (k >= ps.n || row < ps.start[k]) return;
+    const float *f = ps.comp[k] == 0 ? f0 : ps.comp[k] == 1 ? f1 : f2;
+    rows[(size_t)k * capacity + row] = f[(size_t)ps.ix[k] * ny + ps.iy[k]];
+}
+
+static int record_probes(OsFdtd2D *h) {
+    const int c = h->cur;
+    OS_TRY(prof_begin(h, 2, h->stream));
+    ez2d_probe_kernel<<<1, 32, 0, h->stream>>>(h->probes, h->ez[c].ptr, h->hx[c].ptr, h->hy[c].ptr, h->grid.ny,
+                                                h->probe_rows.ptr, h->probe_capacity, h->n_step - 1);
+    OS_TRY(prof_end(h, h->stream));
+    h->launches += 1;
+    OS_CUDA(cudaGetLastError());
+    return OS_OK;
+}
+
+// Room for the probes' rows of the next n_steps steps: the rows grow by doubling, the recorded ones copied over on
+// the handle's stream and the old block given to the pool behind that copy.
+static int reserve_probe_rows(OsFdtd2D *h, int64_t n_steps) {
+    if (h->probes.n == 0) return OS_OK;
+    const int64_t need = h->n_step + n_steps;
+    if (need <= h->probe_capacity) return OS_OK;
+    const int64_t cap = std::max<int64_t>(need, std::max<int64_t>(1024, 2 * h->probe_capacity));
+    DeviceArray<float> grown;
+    OS_TRY(grown.alloc((size_t)OS_MAX_PROBES * (size_t)cap));
+    if (h->probe_capacity > 0 && h->n_step > 0)
+        OS_CUDA(cudaMemcpy2DAsync(grown.ptr, (size_t)cap * sizeof(float), h->probe_rows.ptr,
+                                  (size_t)h->probe_capacity * sizeof(float), (size_t)h->n_step * sizeof(float),
+                                  OS_MAX_PROBES, cudaMemcpyDeviceToDevice, h->stream));
+    give_after(h->stream, h->probe_rows);
+    std::swap(h->probe_rows.ptr, grown.ptr);
+    std::swap(h->probe_rows.count, grown.count);
+    std::swap(h->probe_rows.capacity, grown.capacity);
+    std::swap(h->probe_rows.cls, grown.cls);
+    h->probe_capacity = cap;
+    return OS_OK;
+}
+
 static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples,
                            const float *values, const float *phase_table) {
     const int64_t m = h->sample_interval;
@@ -1021,8 +1078,9 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
     int64_t k = 0;
     while (k < n_steps) {
         int T = (int)std::min<int64_t>(h->steps_per_launch, n_steps - k);
-        // field maps read E_z between launches: a launch ends on every sample step
+        // field maps read E_z between launches: a launch ends on every sample step; probes record every step
         if (!h->maps.empty()) T = (int)std::min<int64_t>(T, m - h->n_step % m);
+        if (h->probes.n) T = 1;
         LaunchPlan &pl = plan_for(T);
         TBParams interior = pl.interior, general = pl.general;
         const int in = h->cur, out = h->cur ^ 1;
@@ -1062,6 +1120,7 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
         k += T;
         if (!h->maps.empty() && h->n_step % m == 0)
             OS_TRY(fold_maps(h, h->ez[h->cur].ptr, h->n_step / m, first_sample, n_samples, phase_table));
+        if (h->probes.n) OS_TRY(record_probes(h));
     }
     return OS_OK;
 }
@@ -1096,6 +1155,7 @@ static int advance_per_step(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, 
         }
         if (!h->maps.empty() && h->n_step % m == 0)
             OS_TRY(fold_maps(h, p.ez, h->n_step / m, first_sample, n_samples, phase_table));
+        if (h->probes.n) OS_TRY(record_probes(h));
     }
     OS_CUDA(cudaGetLastError());
     return OS_OK;
@@ -1291,6 +1351,7 @@ static int advance_hz(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_
         }
         h->cur = out;
         h->n_step += 1;
+        if (h->probes.n) OS_TRY(record_probes(h));
         if (!h->fluxes.empty() && h->n_step % m == 0) {
             const int64_t q = h->n_step / m;
             size_t offset = 0;
@@ -1369,6 +1430,7 @@ extern "C" int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line
     if (!h->lines.empty()) OS_TRY(upload(h->line_values, line_values, h->lines.size() * (size_t)n_steps, h->stream));
     const size_t phase_floats = phase_floats_of(h, n_samples);
     if (phase_floats && phases) OS_TRY(upload(h->phases, phases, phase_floats, h->stream));
+    OS_TRY(reserve_probe_rows(h, n_steps));
     return run_chunk(h, n_steps, first_sample, n_samples, h->line_values.ptr, h->phases.ptr);
 }
 
@@ -1413,6 +1475,8 @@ extern "C" int os_fdtd2d_advance_noalloc(OsFdtd2D *h, int64_t n_steps, const flo
     OS_TRY(check_advance(h, "os_fdtd2d_advance_noalloc", n_steps, line_values, first_sample, n_samples, phases));
     OS_CHECK(!h->profiling, OS_ERR_STATE,
              "os_fdtd2d_advance_noalloc: profiling is on (its event pool grows on demand); turn it off first");
+    OS_CHECK(h->probes.n == 0 || h->n_step + n_steps <= h->probe_capacity, OS_ERR_STATE,
+             "os_fdtd2d_advance_noalloc: the field probes' rows would have to grow; advance with os_fdtd2d_advance");
     // tables: line values at float 0, phases at the next 64-float (256-byte) boundary
     const size_t value_floats = n_steps > 0 ? h->lines.size() * (size_t)n_steps : 0;
     const size_t phase_floats = n_steps > 0 && n_samples > 0 ? phase_floats_of(h, n_samples) : 0;
@@ -1615,6 +1679,36 @@ extern "C" int os_fdtd2d_add_dft_map(OsFdtd2D *h, int32_t x_start, int32_t x_sto
     OS_CUDA(cudaMemsetAsync(d->acc.ptr, 0, d->acc.bytes(), h->stream));
     if (map_id) *map_id = (int32_t)h->maps.size();
     h->maps.push_back(std::move(d));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_add_probe(OsFdtd2D *h, int32_t ix, int32_t iy, int32_t component, int32_t *probe_id) {
+    OS_CHECK(h, OS_ERR_INVALID, "os_fdtd2d_add_probe: null handle");
+    OS_CHECK(0 <= ix && ix < h->grid.nx && 0 <= iy && iy < h->grid.ny, OS_ERR_INVALID,
+             "field probe cell (%d, %d) outside the %d x %d grid", ix, iy, h->grid.nx, h->grid.ny);
+    OS_CHECK(component >= 0 && component <= 2, OS_ERR_INVALID, "unknown field component %d", component);
+    OS_CHECK(h->probes.n < OS_MAX_PROBES, OS_ERR_INVALID, "at most %d field probes per engine", OS_MAX_PROBES);
+    const int k = h->probes.n++;
+    h->probes.ix[k] = ix, h->probes.iy[k] = iy, h->probes.comp[k] = component;
+    h->probes.start[k] = h->n_step;
+    if (probe_id) *probe_id = k;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_read_probe(OsFdtd2D *h, int32_t probe_id, float *values, int64_t max_values,
+                                    int64_t *n_values) {
+    OS_CHECK(h && n_values, OS_ERR_INVALID, "os_fdtd2d_read_probe: null argument");
+    OS_CHECK(probe_id >= 0 && probe_id < h->probes.n, OS_ERR_INVALID, "no field probe %d", probe_id);
+    const int64_t start = h->probes.start[probe_id];
+    const int64_t n = std::max<int64_t>(0, h->n_step - start);
+    *n_values = n;
+    if (n == 0 || !values) return OS_OK;   // values NULL: the count only
+    OS_CHECK(max_values >= n, OS_ERR_INVALID, "os_fdtd2d_read_probe: room for %lld values, %lld recorded",
+             (long long)max_values, (long long)n);
+    OS_TRY(bind_device(h));
+    OS_CUDA(cudaMemcpyAsync(values, h->probe_rows.ptr + (size_t)probe_id * h->probe_capacity + start,
+                            (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    OS_TRY(sync_and_check(h));
     return OS_OK;
 }
 
@@ -1873,8 +1967,9 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
                  "os_fdtd2d_batch_advance: job %d is not on the batch stream (os_fdtd2d_set_stream with "
                  "os_fdtd2d_batch_stream)", q);
         OS_CHECK(!h->profiling, OS_ERR_STATE, "os_fdtd2d_batch_advance: job %d has profiling on", q);
-        OS_CHECK(h->maps.empty(), OS_ERR_STATE,
-                 "os_fdtd2d_batch_advance: job %d has field-map monitors (advance it with os_fdtd2d_advance)", q);
+        OS_CHECK(h->maps.empty() && h->probes.n == 0, OS_ERR_STATE,
+                 "os_fdtd2d_batch_advance: job %d has field-map monitors or field probes (advance it with "
+                 "os_fdtd2d_advance)", q);
     }
     OS_CUDA(cudaSetDevice(b->device));
     // every job's own tables, in its own buffers, as os_fdtd2d_advance uploads them

@@ -47,6 +47,8 @@ class FDTDEngine2D_Ez:
         self._profiles_sent = {}  # id(source) -> profile array last uploaded
         self._monitors = []       # FluxMonitor objects in add order
         self._maps = []           # DFTMonitor objects in add order
+        self._probes = []         # FieldProbe objects in add order
+        self._step_times = []     # engine clock after each step since reset (the probes' times)
         self._monitor_ids = {}
         self._materials_version = None
         self.sample_interval = 1
@@ -98,6 +100,13 @@ class FDTDEngine2D_Ez:
         self._monitors.append(monitor)
         monitor._reader = lambda m=monitor: self.read_flux_spectra(m)
 
+    def attach_probe(self, probe):
+        """Register a FieldProbe; it is created on the device at the next sync and records from the step then."""
+        if probe.field_component not in self.FIELDS:
+            raise ValueError(f"field probe component must be one of {tuple(self.FIELDS)}, got {probe.field_component!r}")
+        self._probes.append(probe)
+        probe._reader = lambda p=probe: self.read_probe(p)
+
     def attach_dft_monitor(self, monitor):
         """Register a field-map DFTMonitor (E_z engines); its device sums are created at the next sync."""
         if self.polarization != 'ez':
@@ -136,6 +145,13 @@ class FDTDEngine2D_Ez:
                 _native.check(lib.os_fdtd2d_add_flux_line(h, normal, monitor.position, monitor.span[0],
                                                           monitor.span[1], monitor.n_freqs, ctypes.byref(mid)))
                 self._monitor_ids[id(monitor)] = mid.value
+        for probe in self._probes:
+            if id(probe) not in self._monitor_ids:
+                pid = ctypes.c_int32()
+                _native.check(lib.os_fdtd2d_add_probe(h, probe.ix, probe.iy, self.FIELDS[probe.field_component],
+                                                      ctypes.byref(pid)))
+                self._monitor_ids[id(probe)] = pid.value
+                probe._first_step = self.n_step
         for monitor in self._maps:
             if id(monitor) not in self._monitor_ids:
                 mid = ctypes.c_int32()
@@ -251,8 +267,20 @@ class FDTDEngine2D_Ez:
         _native.check(_native.load().os_fdtd2d_advance(
             self.handle, n_steps, _native.fptr(values) if values.size else None, first_q, n_q,
             _native.fptr(phases) if phases.size else None))
+        self._append_step_times(n_steps)
         self.n_step += n_steps
         self.time = t_end
+
+    def _append_step_times(self, n_steps):
+        """The clock after each of the next n_steps steps (t_full, accumulated as chunk_tables does): the field
+        probes' sample times."""
+        if not self._probes:
+            self._step_times.extend([float('nan')] * n_steps)   # no probe reads these steps
+            return
+        dt, t = float(self.dt), self.time
+        for _ in range(n_steps):
+            t = t + dt
+            self._step_times.append(t)
 
     def set_stream(self, cuda_stream):
         """Enqueue on the caller's CUDA stream (an int cudaStream_t, e.g. torch.cuda.current_stream().cuda_stream;
@@ -272,6 +300,7 @@ class FDTDEngine2D_Ez:
         _native.check(_native.load().os_fdtd2d_reset(self.handle))
         self.n_step = 0
         self.time = 0.0
+        self._step_times = []
 
     # ------------------------------------------------------------------------------------------- readout
     def read_field(self, name):
@@ -303,6 +332,20 @@ class FDTDEngine2D_Ez:
         _native.check(_native.load().os_fdtd2d_read_flux_spectra(self.handle, mid, _native.dptr(e),
                                                                  _native.dptr(h)))
         return e[..., 0] + 1j * e[..., 1], h[..., 0] + 1j * h[..., 1]
+
+    def read_probe(self, probe):
+        """(times float64, values float32) of a FieldProbe since it was added or the last reset."""
+        if id(probe) not in self._monitor_ids:
+            self.sync_device()
+        lib, pid = _native.load(), self._monitor_ids[id(probe)]
+        n = ctypes.c_int64()
+        _native.check(lib.os_fdtd2d_read_probe(self.handle, pid, None, 0, ctypes.byref(n)))
+        values = np.empty(n.value, dtype=np.float32)
+        if n.value:
+            _native.check(lib.os_fdtd2d_read_probe(self.handle, pid, _native.fptr(values), n.value,
+                                                   ctypes.byref(n)))
+        first = self.n_step - n.value
+        return np.array(self._step_times[first:self.n_step], dtype=np.float64), values
 
     def read_dft_map(self, monitor):
         """(nf, mx, my) complex64 running DFT of a field-map monitor."""

@@ -144,3 +144,23 @@ class DFTMonitor:
         if self._reader is None:
             return np.zeros((self.n_freqs, self.mx, self.my), np.complex64)
         return self._reader()
+
+
+PROBE_COMPONENTS = {'ez': ('ez', 'hx', 'hy'), 'hz': ('hz', 'ex', 'ey')}
+
+
+class FieldProbe:
+    """One field component at cell (ix, iy), recorded after every step (core/monitors.py:194-243): get_data() gives
+    (times float64, values float32) since the probe was added or the engine was last reset; the values are recorded
+    on the device and read in one transfer."""
+
+    def __init__(self, ix, iy, field_component='ez'):
+        self.ix = int(ix)
+        self.iy = int(iy)
+        self.field_component = field_component
+        self._reader = None   # () -> (times, values), set by the engine
+
+    def get_data(self):
+        if self._reader is None:
+            return np.empty(0, np.float64), np.empty(0, np.float32)
+        return self._reader()

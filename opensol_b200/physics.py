@@ -16,7 +16,7 @@ import numpy as np
 from .boundaries import BoundaryConfig, inverse_spacings
 from .constants import C0, DTYPE
 from .engine2d import FDTDEngine2D_Ez, FDTDEngine2D_Hz
-from .monitors import DFTMonitor, FluxMonitor, dft_sample_interval, resolve_frequencies
+from .monitors import PROBE_COMPONENTS, DFTMonitor, FieldProbe, FluxMonitor, dft_sample_interval, resolve_frequencies
 from .sources import (LineSource, calibrate_line_source, calibrate_tangential_sheet, carrier_angular_frequency,
                       make_temporal, resolve_frequency)
 
@@ -115,8 +115,9 @@ class EMPhysics:
         self._check_courant_stability()
         self._calibrate_sources()
         if self.engine.n_step == 0:
-            m = dft_sample_interval(float(self.engine.dt), self.sources, [mon.frequencies for mon in self.monitors])
-            for monitor in self.monitors:
+            dft_monitors = [mon for mon in self.monitors if hasattr(mon, 'frequencies')]   # not the probes
+            m = dft_sample_interval(float(self.engine.dt), self.sources, [mon.frequencies for mon in dft_monitors])
+            for monitor in dft_monitors:
                 monitor.sample_interval = m
             self.engine.set_sample_interval(m)
         self._finalized = True
@@ -237,6 +238,22 @@ class EMPhysics:
         return source
 
     # --- monitors ---------------------------------------------------------------------------------------
+    def add_field_probe(self, x, y, field_component=None):
+        """Raw Yee samples of one field component at the cell containing (x, y) after every step; None = the
+        out-of-plane field (physics/em/__init__.py:492-498, placement.probe_cell)."""
+        components = PROBE_COMPONENTS[self.polarization]
+        if field_component is None:
+            field_component = components[0]
+        if field_component not in components:
+            raise ValueError(f"field probe component of an {self.polarization!r} physics must be one of "
+                             f"{components}, got {field_component!r}")
+        d = self.domain
+        d.validate_physical_pos(x, y, "Field probe")
+        probe = FieldProbe(d.pos_to_cell_x(x), d.pos_to_cell_y(y), field_component)
+        self.monitors.append(probe)
+        self.engine.attach_probe(probe)
+        return probe
+
     def add_dft_monitor(self, x0, y0, x1, y1, wavelengths=None, frequencies=None, downsample=1):
         """Running DFT of E_z over the cell box of the physical box (x0, y0)-(x1, y1); downsample s > 1 records every
         s-th cell along x and y (physics/em/__init__.py:500-509, placement.box_cells)."""

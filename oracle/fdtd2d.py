@@ -409,6 +409,7 @@ class OracleEz2D:
         self.hy = np.zeros(shape, dtype=self.real)
         self.sources, self.monitors = [], []
         self.maps = []           # field-map DFT monitors (add_dft_monitor)
+        self.probes = []         # field probes (add_field_probe): [ix, iy, component, times, values]
         self.n_step = 0
         self.time = 0.0          # engine clock (host float64 accumulation)
         self.runner_t = 0.0      # runner clock
@@ -491,6 +492,20 @@ class OracleEz2D:
                               dtype=np.complex64)
         self.maps.append(mon)
         return mon
+
+    def add_field_probe(self, x, y, field_component=None):
+        """physics/em/__init__.py:492-498 with placement.probe_cell (placement.py:29-45) and FieldProbe.record at
+        t_full after every step (core/monitors.py:226-236, fdtd_2d_base.py:481-487): (times, values) lists."""
+        d = self.domain
+        component = field_component or 'ez'
+        probe = [d.pos_to_cell_x(x), d.pos_to_cell_y(y), component, [], []]
+        self.probes.append(probe)
+        return probe
+
+    def _record_probes(self):
+        for ix, iy, component, times, values in self.probes:
+            times.append(self.time)
+            values.append(np.float32(getattr(self, component)[ix, iy]))
 
     def _fold_maps(self):
         """DFTMonitor.update at a sample step (monitors.py:281-311) with _dft_accum_host (:36-37): the complex64
@@ -630,16 +645,17 @@ class OracleEz2D:
     def advance(self, n_steps):
         """n_steps steps; with field maps, in pieces that end on the DFT sample steps, each followed by the maps'
         update (the reference updates its monitors after every sampled step)."""
-        if not self.maps:
+        if not self.maps and not self.probes:
             self._advance_chunk(n_steps)
             return
         m = self.sample_interval
         while n_steps > 0:
-            piece = min(n_steps, m - self.n_step % m)
+            piece = 1 if self.probes else min(n_steps, m - self.n_step % m)
             self._advance_chunk(piece)
             n_steps -= piece
-            if self.n_step % m == 0:
+            if self.maps and self.n_step % m == 0:
                 self._fold_maps()
+            self._record_probes()
 
     def _advance_chunk(self, n_steps):
         lib, State, Line, Flux = load_library(self.real)

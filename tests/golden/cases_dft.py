@@ -1,6 +1,7 @@
 """Cases with field-map (running DFT) monitors, shared by the golden-fixture generator (run on open_sol itself),
 the oracle pinning tests and the GPU parity tests.  Same form as cases.py; 'dft' lists the field-map monitors added
-through the E_z physics (x0, y0, x1, y1 [m], frequencies [Hz], downsample)."""
+through the E_z physics (x0, y0, x1, y1 [m], frequencies [Hz], downsample); 'probes' the field probes (x, y [m],
+component)."""
 
 CASES_DFT = [
     {   # all-CPML box: cylinder, lossy rectangle, spanned line source, flux line, a full-resolution map and a
@@ -17,6 +18,7 @@ CASES_DFT = [
             [0.3e-6, 0.2e-6, 1.2e-6, 1.0e-6, [4.2e14, 5.0e14], 1],
             [0.1e-6, 0.05e-6, 1.4e-6, 1.15e-6, [4.6e14], 3],
         ],
+        'probes': [[0.75e-6, 0.5e-6, 'ez'], [0.12e-6, 0.6e-6, 'hx'], [1.1e-6, 1.15e-6, 'hy']],
         'checkpoints': [250, 500],
     },
     {   # periodic y, CPML in x: a map crossing the slab and one touching the y edge of the grid
@@ -30,6 +32,7 @@ CASES_DFT = [
         'dft': [
             [0.7e-6, 0.0, 1.8e-6, 0.99e-6, [4.0e14, 4.6e14, 5.2e14], 2],
         ],
+        'probes': [[1.2e-6, 0.0, 'ez']],
         'checkpoints': [300, 600],
     },
 ]

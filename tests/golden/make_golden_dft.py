@@ -6,8 +6,8 @@ Run in a container that holds the reference source tree (read-only):
     python tests/golden/make_golden_dft.py /path/to/reference
 
 Each case writes <name>.npz: per field-map monitor its sample boxes (x / y sample slice starts, strides, counts) and
-its complex64 E_z spectra at every checkpoint, the flux monitor's complex128 spectra, the DFT sample interval and
-SHA-256 digests of the fields at every checkpoint.
+its complex64 E_z spectra at every checkpoint, the flux monitor's complex128 spectra, the DFT sample interval,
+SHA-256 digests of the fields at every checkpoint, and per field probe its times and float32 values at the end.
 """
 import hashlib
 import json
@@ -31,6 +31,7 @@ def run_case(spec):
     fluxes = apply_ops(sim, spec)
     maps = [sim.em.add_dft_monitor(x0, y0, x1, y1, frequencies=freqs, downsample=ds)
             for x0, y0, x1, y1, freqs, ds in spec['dft']]
+    probes = [sim.em.add_field_probe(x, y, comp) for x, y, comp in spec.get('probes', [])]
     out = {}
     done = 0
     for cp in spec['checkpoints']:
@@ -46,6 +47,10 @@ def run_case(spec):
     for k, mon in enumerate(maps):
         xs, ys = mon.x_samples, mon.y_samples
         out[f'map{k}_box'] = np.array([xs.start, xs.stop, mon.downsample, mon.mx, ys.start, ys.stop, mon.my])
+    for k, probe in enumerate(probes):
+        times, values = probe.get_data()
+        out[f'probe{k}_t'], out[f'probe{k}_v'] = np.asarray(times), np.asarray(values)
+        out[f'probe{k}_cell'] = np.array([probe.ix, probe.iy])
     out['sample_interval'] = np.int64(maps[0].sample_interval)
     out['n_step'] = np.int64(sim.em.engine.n_step)
     return out

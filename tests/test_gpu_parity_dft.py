@@ -1,6 +1,6 @@
-"""GPU parity of the field-map (running DFT) monitors of the 2D E_z engine, through the C ABI, against open_sol's own
-maps (tests/golden/dft_*.npz) and the oracle.  Bar: bit-identical complex64 maps (array_equal), for every kernel
-variant and for chunk boundaries that do and do not fall on sample steps."""
+"""GPU parity of the field-map (running DFT) monitors and field probes of the 2D engines, through the C ABI, against
+open_sol's own outputs (tests/golden/dft_*.npz) and the oracle.  Bar: bit-identical complex64 maps and float32 probe
+values (array_equal), for every kernel variant and for chunk boundaries that do and do not fall on sample steps."""
 import hashlib
 import os
 
@@ -29,6 +29,7 @@ def _build(spec, config):
     fluxes = apply_ops(sim, spec)
     maps = [sim.em.add_dft_monitor(x0, y0, x1, y1, frequencies=f, downsample=ds)
             for x0, y0, x1, y1, f, ds in spec['dft']]
+    sim.probes = [sim.em.add_field_probe(x, y, comp) for x, y, comp in spec.get('probes', [])]
     sim.em.engine.configure(variant=config[0], steps_per_launch=config[1], tile_rows=config[2])
     return sim, fluxes, maps
 
@@ -50,7 +51,38 @@ def test_maps_bit_exact_against_reference(spec, config):
             np.testing.assert_array_equal(got, g[f'map{k}_{cp}'])
         for k, mon in enumerate(fluxes):
             np.testing.assert_array_equal(mon.spectra()[0], g[f'spec_e{k}_{cp}'])
+    for k, probe in enumerate(sim.probes):
+        times, values = probe.get_data()
+        assert [probe.ix, probe.iy] == g[f'probe{k}_cell'].tolist()
+        np.testing.assert_array_equal(times, g[f'probe{k}_t'])
+        np.testing.assert_array_equal(values, g[f'probe{k}_v'])
     sim.em.engine.close()
+
+
+def test_hz_probes_record_every_step():
+    """H_z engine: the probes' values equal the fields read back after each single step."""
+    from cases_hz import HZ_CASES
+    spec = HZ_CASES[0]
+    sim = ob.Simulation(**spec['sim'], verbose=False)
+    apply_ops(sim, spec)
+    eng = sim.em.engine
+    cells = [(0.4e-6, 0.5e-6, 'hz'), (0.6e-6, 0.3e-6, 'ex'), (0.5e-6, 0.7e-6, 'ey')]
+    probes = [sim.em.add_field_probe(x, y, c) for x, y, c in cells]
+    sim.em.finalize()
+    expected = [[] for _ in probes]
+    for _ in range(40):
+        eng.advance(1)
+        for k, p in enumerate(probes):
+            expected[k].append(eng.read_field(p.field_component)[p.ix, p.iy])
+    eng.advance(25)   # and a longer chunk
+    for k, p in enumerate(probes):
+        times, values = p.get_data()
+        assert values.shape == (65,) and times.shape == (65,)
+        np.testing.assert_array_equal(values[:40], np.array(expected[k], dtype=np.float32))
+        np.testing.assert_array_equal(times[-1], eng.time)
+    final = [eng.read_field(p.field_component)[p.ix, p.iy] for p in probes]
+    assert [p.get_data()[1][-1] for p in probes] == final
+    eng.close()
 
 
 @pytest.mark.parametrize('seed', [0, 1, 2])

@@ -1,6 +1,7 @@
-"""Pin the oracle's field-map (running DFT) monitors to open_sol itself: the fixtures of tests/golden/dft_*.npz
-(generated by running the reference's CPU backend, see tests/golden/make_golden_dft.py) must be reproduced bit for
-bit -- the complex64 maps at every checkpoint, the sample boxes, the flux line spectra and the fields' digests."""
+"""Pin the oracle's field-map (running DFT) monitors and field probes to open_sol itself: the fixtures of
+tests/golden/dft_*.npz (generated by running the reference's CPU backend, see tests/golden/make_golden_dft.py) must be
+reproduced bit for bit -- the complex64 maps at every checkpoint, the sample boxes, the flux line spectra, the fields'
+digests and the probes' times and values."""
 import hashlib
 import os
 
@@ -23,6 +24,7 @@ def run_oracle_dft(spec):
     o = OracleEz2D(**spec['sim'])
     fluxes = apply_ops(o, spec)
     maps = [o.add_dft_monitor(x0, y0, x1, y1, frequencies=f, downsample=ds) for x0, y0, x1, y1, f, ds in spec['dft']]
+    o.probe_records = [o.add_field_probe(x, y, comp) for x, y, comp in spec.get('probes', [])]
     snaps = {}
     done = 0
     for cp in spec['checkpoints']:
@@ -52,3 +54,14 @@ def test_oracle_maps_match_reference(spec):
             assert np.abs(ref).max() > 0   # the map saw the pulse
         for k, e in enumerate(flux_e):
             np.testing.assert_array_equal(e, g[f'spec_e{k}_{cp}'])
+
+
+@pytest.mark.parametrize('spec', CASES_DFT, ids=[c['name'] for c in CASES_DFT])
+def test_oracle_probes_match_reference(spec):
+    g = np.load(os.path.join(GOLDEN, f"{spec['name']}.npz"))
+    o, _, _ = run_oracle_dft(spec)
+    for k, (ix, iy, _, times, values) in enumerate(o.probe_records):
+        assert [ix, iy] == g[f'probe{k}_cell'].tolist()
+        np.testing.assert_array_equal(np.array(times), g[f'probe{k}_t'])
+        np.testing.assert_array_equal(np.array(values, dtype=np.float32), g[f'probe{k}_v'])
+        assert np.abs(g[f'probe{k}_v']).max() > 0
