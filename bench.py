@@ -45,6 +45,8 @@ def parse_args():
     p.add_argument('--sim-steps', type=int, default=SIM_STEPS)
     p.add_argument('--grid', type=int, default=8192, help='total cells per side (8192 = the benchmark workload; '
                    'smaller grids are profiling cases of the same kernels)')
+    p.add_argument('--grid3d', type=int, default=512, help='em3d: total cells per side (512 = the benchmark '
+                   'workload; smaller grids scale the sphere count with the volume, for profiling)')
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-e2e', action='store_true')
     p.add_argument('--variant', type=int, default=1, help='1: temporally blocked kernels (default), 0: per step')
@@ -455,7 +457,9 @@ def run_em3d(args):
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     steps = args.sim_steps if args.sim_steps != SIM_STEPS else workloads.ROOFLINE_3D['steps']
-    physics, box = workloads.roofline_3d_physics(device=local)
+    physics, box = workloads.roofline_3d_physics(total_cells=args.grid3d,
+                                                 n_spheres=max(1, int(round(500 * (args.grid3d / 512) ** 3))),
+                                                 device=local)
     physics.finalize()
     engine = physics.engine
     # a stream of its own (torch's default stream is handle 0, which os_fdtd*_set_stream reads as "the engine's own

@@ -228,7 +228,7 @@ __device__ __forceinline__ float em3d_lo_diff(float f0, float lo, bool first_row
     return periodic ? f0 - em3d_wrapped(lo) : f0;
 }
 
-__global__ void __launch_bounds__(EM3D_BZ * EM3D_BY) em3d_e_kernel(const Em3DParams p) {
+__global__ void __launch_bounds__(EM3D_BZ * EM3D_BY, 4) em3d_e_kernel(const Em3DParams p) {
     const int k = blockIdx.x * EM3D_BZ + threadIdx.x;
     const int j = blockIdx.y * EM3D_BY + threadIdx.y;
     if (j >= p.ny || k >= p.nz) return;
