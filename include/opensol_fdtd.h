@@ -147,16 +147,18 @@ int os_fdtd2d_set_line_profile(OsFdtd2D *h, int32_t source_id, const float *prof
 int os_fdtd2d_add_flux_line(OsFdtd2D *h, int32_t normal_axis, int32_t position, int32_t lo, int32_t hi, int32_t nf,
                             int32_t *monitor_id);
 
-/* Field-map running DFT of E_z over the cell box [x_start, x_stop) x [y_start, y_stop): DFTMonitor (physics/em/
- * monitors.py:248-311, polarization 'ez').  downsample s >= 1 samples every s-th cell along x and y from the middle of
- * the first s-cell block (dft_sample_slice, monitors.py:152-155); nf frequencies; complex64 sums (nf, mx, my) updated
- * at every DFT sample step with the chunk's phase table (whose rows follow the flux lines' rows, per map in add
- * order).  A blocked advance ends a launch on every sample step when a map exists.  E_z engines only; not in batched
- * advances. */
+/* Field-map running DFT over the cell box [x_start, x_stop) x [y_start, y_stop): DFTMonitor (physics/em/
+ * monitors.py:248-322).  downsample s >= 1 samples every s-th cell along x and y from the middle of the first s-cell
+ * block (dft_sample_slice, monitors.py:152-155); nf frequencies; complex64 sums updated at every DFT sample step with
+ * the chunk's phase table, whose rows follow the flux lines' rows, per map in add order.  E_z handle: E_z, (nf, mx,
+ * my), one phase table per map.  H_z handle: H_z, E_x and E_y collocated to the cell centres ((3, nf, mx, my)), two
+ * phase tables per map (at t, then at t - dt/2 for H_z).  A blocked advance ends a launch on every sample step when
+ * a map exists.  Not in batched advances. */
 int os_fdtd2d_add_dft_map(OsFdtd2D *h, int32_t x_start, int32_t x_stop, int32_t y_start, int32_t y_stop,
                           int32_t downsample, int32_t nf, int32_t *map_id);
 
-/* Spectra of a field map: (nf, mx, my) complex64 as float pairs (DFTMonitor.ez_dft). */
+/* Spectra of a field map as float pairs: (nf, mx, my) complex64 (DFTMonitor.ez_dft), or (3, nf, mx, my) on an H_z
+ * handle (hz_dft, ex_dft, ey_dft). */
 int os_fdtd2d_read_dft_map(OsFdtd2D *h, int32_t map_id, float *spectra);
 
 /* Field probe: one component (OS_EZ / OS_HX / OS_HY, or OS_HZ_* on an H_z handle) of cell (ix, iy) recorded after

@@ -45,9 +45,10 @@ struct ProbeSet {
     int64_t start[OS_MAX_PROBES];
 };
 
-struct DftMap2D {                       // field-map running DFT of E_z (DFTMonitor)
+struct DftMap2D {                       // field-map running DFT (DFTMonitor)
     int32_t x0, y0, ds, mx, my, nf;     // first sampled cell, stride, samples per axis, frequencies
-    DeviceArray<float> acc;             // (nf, mx, my) complex64 as float pairs
+    bool hz;                            // H_z engine: H_z, E_x, E_y maps (E at the cell centres), two phase tables
+    DeviceArray<float> acc;             // E_z: (nf, mx, my); H_z: (3, nf, mx, my); complex64 as float pairs
 };
 
 }  // namespace os
@@ -976,7 +977,7 @@ static void bind_buffers(OsFdtd2D *h, TBParams &q, int in, int out) {
 static size_t phase_floats_of(const OsFdtd2D *h, int64_t n_samples) {
     size_t n = 0;
     for (auto &f : h->fluxes) n += (size_t)n_samples * f->nf * 2;
-    for (auto &d : h->maps) n += (size_t)n_samples * d->nf * 2;
+    for (auto &d : h->maps) n += (size_t)n_samples * d->nf * 2 * (d->hz ? 2 : 1);
     return n;
 }
 
@@ -989,11 +990,19 @@ static int fold_maps(OsFdtd2D *h, const float *ez, int64_t q, int64_t first_samp
         const float *ph = phase_table + offset + (size_t)(q - first_sample) * d->nf * 2;
         const int64_t total = (int64_t)d->nf * d->mx * d->my;
         OS_TRY(prof_begin(h, 2, h->stream));
-        ez2d_dft_map_kernel<<<(unsigned)((total + 255) / 256), 256, 0, h->stream>>>(
-            ez, h->grid.ny, d->x0, d->y0, d->ds, d->mx, d->my, d->nf, ph, d->acc.ptr);
+        if (d->hz) {   // E-time phases, then the H_z phases at t - dt/2
+            const float *ph_h = ph + (size_t)n_samples * d->nf * 2;
+            const int c = h->cur;
+            hz2d_dft_map_kernel<<<(unsigned)((total + 255) / 256), 256, 0, h->stream>>>(
+                h->ez[c].ptr, h->hx[c].ptr, h->hy[c].ptr, h->grid.nx, h->grid.ny, h->grid.periodic_x,
+                h->grid.periodic_y, d->x0, d->y0, d->ds, d->mx, d->my, d->nf, ph, ph_h, d->acc.ptr);
+        } else {
+            ez2d_dft_map_kernel<<<(unsigned)((total + 255) / 256), 256, 0, h->stream>>>(
+                ez, h->grid.ny, d->x0, d->y0, d->ds, d->mx, d->my, d->nf, ph, d->acc.ptr);
+        }
         OS_TRY(prof_end(h, h->stream));
         h->launches += 1;
-        offset += (size_t)n_samples * d->nf * 2;
+        offset += (size_t)n_samples * d->nf * 2 * (d->hz ? 2 : 1);
     }
     OS_CUDA(cudaGetLastError());
     return OS_OK;
@@ -1351,6 +1360,8 @@ static int advance_hz(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_
         }
         h->cur = out;
         h->n_step += 1;
+        if (!h->maps.empty() && h->n_step % m == 0)
+            OS_TRY(fold_maps(h, nullptr, h->n_step / m, first_sample, n_samples, phase_table));
         if (h->probes.n) OS_TRY(record_probes(h));
         if (!h->fluxes.empty() && h->n_step % m == 0) {
             const int64_t q = h->n_step / m;
@@ -1659,7 +1670,7 @@ extern "C" int os_fdtd2d_read_flux_spectra(OsFdtd2D *h, int32_t monitor_id, doub
 
 extern "C" int os_fdtd2d_add_dft_map(OsFdtd2D *h, int32_t x_start, int32_t x_stop, int32_t y_start, int32_t y_stop,
                                      int32_t downsample, int32_t nf, int32_t *map_id) {
-    OS_TRY(require_ez(h, "os_fdtd2d_add_dft_map"));
+    OS_CHECK(h, OS_ERR_INVALID, "os_fdtd2d_add_dft_map: null handle");
     OS_CHECK(0 <= x_start && x_start < x_stop && x_stop <= h->grid.nx && 0 <= y_start && y_start < y_stop &&
                  y_stop <= h->grid.ny,
              OS_ERR_INVALID, "DFTMonitor box [%d, %d) x [%d, %d) must be a non-empty box inside the %d x %d grid",
@@ -1675,7 +1686,8 @@ extern "C" int os_fdtd2d_add_dft_map(OsFdtd2D *h, int32_t x_start, int32_t x_sto
     d->mx = (x_stop - d->x0 + downsample - 1) / downsample;
     d->my = (y_stop - d->y0 + downsample - 1) / downsample;
     d->nf = nf;
-    OS_TRY(d->acc.alloc((size_t)nf * d->mx * d->my * 2));
+    d->hz = h->polarization == 1;
+    OS_TRY(d->acc.alloc((size_t)nf * d->mx * d->my * 2 * (d->hz ? 3 : 1)));
     OS_CUDA(cudaMemsetAsync(d->acc.ptr, 0, d->acc.bytes(), h->stream));
     if (map_id) *map_id = (int32_t)h->maps.size();
     h->maps.push_back(std::move(d));

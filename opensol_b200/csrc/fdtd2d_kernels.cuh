@@ -200,6 +200,37 @@ __global__ void ez2d_dft_map_kernel(const float *__restrict__ ez, int ny, int x0
     acc[2 * t + 1] = acc[2 * t + 1] + im;
 }
 
+// Field-map DFT of the H_z engine at one sample (DFTMonitor.update for 'hz', physics/em/monitors.py:296-322, with
+// _dft_accum_host and _dft_accum_pair_host :36-41): H_z at the cell with the phases of t - dt/2; E_x collocated to
+// the cell centre as float(0.5) (E_x[x, y] + E_x[x, y - 1]) and E_y as float(0.5) (E_y[x, y] + E_y[x - 1, y]) with
+// the E phases, the lo partner of row / column 0 the wrapped last face on a periodic axis, else the face itself
+// (_centre_pairs, :156-167).  acc: (3, nf, mx, my) complex64 (H_z, E_x, E_y).  One thread per (frequency, sample).
+__global__ void hz2d_dft_map_kernel(const float *__restrict__ hz, const float *__restrict__ ex,
+                                    const float *__restrict__ ey, int nx, int ny, int px, int py, int x0, int y0,
+                                    int ds, int mx, int my, int nf, const float *__restrict__ ph_e,
+                                    const float *__restrict__ ph_h, float *__restrict__ acc) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t per_f = (int64_t)mx * my, total = per_f * nf;
+    if (t >= total) return;
+    const int f = (int)(t / per_f);
+    const int64_t c = t - (int64_t)f * per_f;
+    const int a = (int)(c / my), b = (int)(c - (int64_t)a * my);
+    const int x = x0 + a * ds, y = y0 + b * ds;
+    const int y_lo = y >= 1 ? y - 1 : (py ? ny - 1 : 0), x_lo = x >= 1 ? x - 1 : (px ? nx - 1 : 0);
+    const float half = 0.5f, zero = 0.0f;
+    const float v[3] = {hz[(size_t)x * ny + y], half * (ex[(size_t)x * ny + y] + ex[(size_t)x * ny + y_lo]),
+                        half * (ey[(size_t)x * ny + y] + ey[(size_t)x_lo * ny + y])};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const float *ph = q == 0 ? ph_h : ph_e;
+        const float pr = ph[2 * f], pi = ph[2 * f + 1];
+        const float re = pr * v[q] - pi * zero, im = pr * zero + pi * v[q];
+        const int64_t o = 2 * ((int64_t)q * total + t);
+        acc[o] = acc[o] + re;
+        acc[o + 1] = acc[o + 1] + im;
+    }
+}
+
 // ca / cb from float32 eps_r, sigma_e (fdtd_ez_2d_kernels.py:314-332, T = float); sigma NULL = lossless (ca not
 // written: it is 1).
 __global__ void ez2d_e_coefficients_kernel(const float *__restrict__ eps_r, const float *__restrict__ sigma, float dt,

@@ -108,9 +108,7 @@ class FDTDEngine2D_Ez:
         probe._reader = lambda p=probe: self.read_probe(p)
 
     def attach_dft_monitor(self, monitor):
-        """Register a field-map DFTMonitor (E_z engines); its device sums are created at the next sync."""
-        if self.polarization != 'ez':
-            raise NotImplementedError('field-map DFT monitors are built for the E_z engine only')
+        """Register a field-map DFTMonitor; its device sums are created at the next sync."""
         self._maps.append(monitor)
         monitor._reader = lambda m=monitor: self.read_dft_map(m)
 
@@ -252,6 +250,9 @@ class FDTDEngine2D_Ez:
         for monitor in self._monitors + self._maps:   # flux lines, then field maps (the device's table order)
             times = [t_full[q * m - self.n_step - 1] for q in range(first_q, first_q + n_q)]
             tables.append(dft_phase_table(2.0 * np.pi * monitor.frequencies, times, monitor.dt * m))
+            if monitor in self._maps and self.polarization == 'hz':   # H_z holds t - dt/2 (monitors.py:283-284)
+                tables.append(dft_phase_table(2.0 * np.pi * monitor.frequencies,
+                                              [t - 0.5 * monitor.dt for t in times], monitor.dt * m))
         phases = np.concatenate([tb.reshape(-1) for tb in tables]) if tables else np.zeros(0, np.float32)
         return np.ascontiguousarray(values, dtype=np.float32), first_q, n_q, phases, t
 
@@ -348,13 +349,16 @@ class FDTDEngine2D_Ez:
         return np.array(self._step_times[first:self.n_step], dtype=np.float64), values
 
     def read_dft_map(self, monitor):
-        """(nf, mx, my) complex64 running DFT of a field-map monitor."""
+        """(nf, mx, my) complex64 running DFT of a field-map monitor (E_z); (3, nf, mx, my) = H_z, E_x, E_y on the
+        H_z engine."""
         if id(monitor) not in self._monitor_ids:
             self.sync_device()
-        out = np.empty((monitor.n_freqs, monitor.mx, monitor.my, 2), dtype=np.float32)
+        parts = 3 if self.polarization == 'hz' else 1
+        out = np.empty((parts, monitor.n_freqs, monitor.mx, monitor.my, 2), dtype=np.float32)
         _native.check(_native.load().os_fdtd2d_read_dft_map(self.handle, self._monitor_ids[id(monitor)],
                                                             _native.fptr(out)))
-        return out.view(np.complex64)[..., 0]
+        maps = out.view(np.complex64)[..., 0]
+        return maps if parts == 3 else maps[0]
 
     def state(self):
         """Host copies of the public fields (FDTDEngine2D_Ez.state, fdtd_ez_2d.py:56-67)."""

@@ -112,9 +112,10 @@ def dft_sample_slice(start: int, stop: int, stride: int) -> slice:
 
 
 class DFTMonitor:
-    """Running DFT of E_z over the cell box (x_slice, y_slice) at each frequency (physics/em/monitors.py:248-311,
-    polarization 'ez'): ez_dft[f, a, b] += phase_f * E_z at every DFT sample step, complex64 sums on the device;
-    downsample s > 1 records every s-th cell along x and y (x_samples / y_samples)."""
+    """Running DFT over the cell box (x_slice, y_slice) at each frequency (physics/em/monitors.py:248-322): E_z
+    ('ez', ez_dft), or H_z plus E_x / E_y collocated to the cell centres ('hz', hz_dft / ex_dft / ey_dft; the partner
+    face of cell 0 wraps on a periodic axis), += phase_f * sample at every DFT sample step, complex64 sums on the
+    device; downsample s > 1 records every s-th cell along x and y (x_samples / y_samples)."""
 
     def __init__(self, x_slice, y_slice, frequencies, dt, polarization='ez', downsample=1):
         for label, cells in (('x_slice', x_slice), ('y_slice', y_slice)):
@@ -122,8 +123,8 @@ class DFTMonitor:
                 raise ValueError(f"DFTMonitor {label} must be a non-empty unit-step slice, got {cells}")
         if isinstance(downsample, bool) or int(downsample) != downsample or downsample < 1:
             raise ValueError(f"DFTMonitor downsample must be an int >= 1, got {downsample!r}")
-        if polarization != 'ez':
-            raise NotImplementedError("field-map DFT monitors are built for polarization 'ez' only")
+        if polarization not in ('ez', 'hz'):
+            raise ValueError(f"DFTMonitor polarization must be 'ez' or 'hz', got {polarization!r}")
         self.polarization = polarization
         self.x_slice = x_slice
         self.y_slice = y_slice
@@ -138,12 +139,37 @@ class DFTMonitor:
         self.sample_interval = 1
         self._reader = None   # () -> complex64 (nf, mx, my), set by the engine
 
+    def _maps(self):
+        parts = 1 if self.polarization == 'ez' else 3
+        if self._reader is None:
+            maps = np.zeros((parts, self.n_freqs, self.mx, self.my), np.complex64)
+            return maps[0] if parts == 1 else maps
+        return self._reader()
+
     @property
     def ez_dft(self):
         """(n_freqs, mx, my) complex64 running DFT of E_z (read from the device)."""
-        if self._reader is None:
-            return np.zeros((self.n_freqs, self.mx, self.my), np.complex64)
-        return self._reader()
+        if self.polarization != 'ez':
+            raise AttributeError("an 'hz' DFTMonitor has hz_dft, ex_dft and ey_dft")
+        return self._maps()
+
+    @property
+    def hz_dft(self):
+        if self.polarization != 'hz':
+            raise AttributeError("an 'ez' DFTMonitor has ez_dft")
+        return self._maps()[0]
+
+    @property
+    def ex_dft(self):
+        if self.polarization != 'hz':
+            raise AttributeError("an 'ez' DFTMonitor has ez_dft")
+        return self._maps()[1]
+
+    @property
+    def ey_dft(self):
+        if self.polarization != 'hz':
+            raise AttributeError("an 'ez' DFTMonitor has ez_dft")
+        return self._maps()[2]
 
 
 PROBE_COMPONENTS = {'ez': ('ez', 'hx', 'hy'), 'hz': ('hz', 'ex', 'ey')}

@@ -29,7 +29,7 @@ import os
 import numpy as np
 
 from oracle.fdtd2d import (DTYPE, EPS0, ETA0, LIB_DIR, OracleEz2D, _make_structs, _ptr, build_cpml,
-                           dft_sample_interval, h_coefficients, paint_circle, paint_rect, sheet_admittance,
+                           dft_phases, dft_sample_interval, h_coefficients, paint_circle, paint_rect, sheet_admittance,
                            yee_inverse_spacings)
 
 
@@ -104,6 +104,20 @@ def load_library(real=np.float32):
     return _LIBS[key]
 
 
+def centre_pairs(samples, periodic, stride):
+    """(face cells, partner face cells, box cells) slice triples pairing the hi faces of the sampled cells with their
+    lo faces (cell - 1); cell 0 pairs with the wrapped last face on a periodic axis, else with its own face
+    (monitors.py:156-167 with yee_grid.lower_face, :91-94).  samples: the dft_sample_slice of the box."""
+    hi = samples.stop
+    if samples.start >= 1:
+        return ((samples, slice(samples.start - 1, hi - 1, stride), slice(None)),)
+    partner = -1 if periodic else 0
+    first = (slice(0, 1), slice(partner, partner + 1 or None), slice(0, 1))
+    if hi == 1:
+        return (first,)
+    return (first, (slice(1, hi), slice(0, hi - 1), slice(1, hi)))
+
+
 class OracleHz2D(OracleEz2D):
     """The whole 2D H_z path of one simulation on the CPU (same construction calls as OracleEz2D)."""
 
@@ -176,14 +190,47 @@ class OracleHz2D(OracleEz2D):
                                           omega, src.normal_width, float(d.dt))
             weight = np.asarray(2.0 * np.ones(src.hi - src.lo) / (float(ETA0) * src.normal_width), dtype=DTYPE)
             src.profile = (row(cb_face, src.position) * admittance * weight).astype(DTYPE)
-        self.sample_interval = dft_sample_interval(float(d.dt), self.sources, [m.frequencies for m in self.monitors])
-        for m in self.monitors:
+        self.sample_interval = dft_sample_interval(float(d.dt), self.sources,
+                                                   [m.frequencies for m in self.monitors + self.maps])
+        for m in self.monitors + self.maps:
             m.sample_interval = self.sample_interval
         self.psi_e = {s.name: np.zeros(self._psi_shape(s.name), dtype=real) for s in self.cpml_sides}
         self.psi_h = {s.name: np.zeros(self._psi_shape(s.name), dtype=real) for s in self.cpml_sides}
         self._finalized = True
 
-    def advance(self, n_steps):
+    def add_dft_monitor(self, x0, y0, x1, y1, wavelengths=None, frequencies=None, downsample=1):
+        """DFTMonitor for 'hz' (physics/em/monitors.py:276-284): H_z, E_x and E_y maps of the sampled cells."""
+        mon = super().add_dft_monitor(x0, y0, x1, y1, wavelengths, frequencies, downsample)
+        shape = mon.ez_dft.shape
+        del mon.ez_dft
+        mon.hz_dft, mon.ex_dft, mon.ey_dft = (np.zeros(shape, dtype=np.complex64) for _ in range(3))
+        return mon
+
+    def add_field_probe(self, x, y, field_component=None):
+        return super().add_field_probe(x, y, field_component or 'hz')
+
+    def _fold_maps(self):
+        """DFTMonitor.update for 'hz' (monitors.py:281-322): H_z with the phases of t - dt/2, E_x / E_y as the
+        float32 mean of a cell's hi face and its lo partner (_centre_pairs) with the phases of t, each added in numpy
+        complex64 (_dft_accum_host / _dft_accum_pair_host, :36-41)."""
+        d = self.domain
+        m = self.sample_interval
+        for mon in self.maps:
+            omega = 2.0 * np.pi * mon.frequencies
+            table_e = dft_phases(omega, self.time, mon.dt * m)
+            table_h = dft_phases(omega, self.time - 0.5 * mon.dt, mon.dt * m)
+            ph_e = (table_e[:, 0] + 1j * table_e[:, 1]).astype(np.complex64)[:, None, None]
+            ph_h = (table_h[:, 0] + 1j * table_h[:, 1]).astype(np.complex64)[:, None, None]
+            xs, ys = mon.x_samples, mon.y_samples
+            mon.hz_dft += ph_h * np.asarray(self.hz[xs, ys], dtype=np.float32)[None, :, :]
+            for faces, partners, box in centre_pairs(ys, d.periodic_y, mon.downsample):
+                mean = np.float32(0.5) * (self.ex[xs, faces] + self.ex[xs, partners])
+                mon.ex_dft[:, :, box] += ph_e * mean[None, :, :]
+            for faces, partners, box in centre_pairs(xs, d.periodic_x, mon.downsample):
+                mean = np.float32(0.5) * (self.ey[faces, ys] + self.ey[partners, ys])
+                mon.ey_dft[:, box, :] += ph_e * mean[None, :, :]
+
+    def _advance_chunk(self, n_steps):
         lib, State, Line, Flux = load_library(self.real)
         d, real = self.domain, self.real
         R = ctypes.c_float if real == np.float32 else ctypes.c_double

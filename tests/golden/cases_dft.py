@@ -38,8 +38,47 @@ CASES_DFT = [
 ]
 
 
+# H_z polarisation: maps of H_z and of E_x / E_y collocated to the cell centres; one box starts on the periodic
+# axis's cell 0 at full resolution (its E partner face wraps to the last face)
+CASES_DFT_HZ = [
+    {   # all-CPML box: circle, lossy rectangle, E_x sheet, flux line; a full-resolution and a 2x-downsampled map
+        'name': 'dft_hz_pml',
+        'sim': {'size_x': 1.5e-6, 'size_y': 1.2e-6, 'dx': 25e-9, 'npml': 10, 'boundaries': 'pml',
+                'polarization': 'hz'},
+        'ops': [
+            ['add_dielectric_circle', [0.75e-6, 0.7e-6, 0.2e-6], {'eps_r': 4.0}],
+            ['add_dielectric_rectangle', [0.2e-6, 0.9e-6, 0.6e-6, 1.1e-6], {'eps_r': 2.0, 'sigma_e': 5e4}],
+            ['add_line_source', ['x', 0.35e-6], {'wavelength': 700e-9, 'bandwidth': 0.6, 'span': [0.3e-6, 1.2e-6]}],
+            ['add_flux_monitor', ['x', 1.0e-6, [0.2e-6, 1.3e-6]], {'wavelengths': [600e-9, 700e-9]}],
+        ],
+        'dft': [
+            [0.3e-6, 0.2e-6, 1.2e-6, 1.0e-6, [4.2e14, 5.0e14], 1],
+            [0.1e-6, 0.05e-6, 1.4e-6, 1.15e-6, [4.6e14], 2],
+        ],
+        'probes': [[0.75e-6, 0.5e-6, 'hz'], [0.5e-6, 0.6e-6, 'ex']],
+        'checkpoints': [250, 500],
+    },
+    {   # periodic y: a full-resolution map from y = 0 (wrapped partner faces) and a 3x-downsampled one
+        'name': 'dft_hz_periodic_y',
+        'sim': {'size_x': 2.0e-6, 'size_y': 1.0e-6, 'dx': 25e-9, 'npml': 12, 'boundaries': 'periodic_y',
+                'polarization': 'hz'},
+        'ops': [
+            ['add_dielectric_rectangle', [1.0e-6, 0.0, 1.3e-6, 1.0e-6], {'eps_r': 2.25}],
+            ['add_line_source', ['y', 0.5e-6], {'wavelength': 650e-9, 'bandwidth': 0.7}],
+            ['add_flux_monitor', ['y', 1.6e-6, [0.0, 1.0e-6]], {'wavelengths': [650e-9]}],
+        ],
+        'dft': [
+            [0.7e-6, 0.0, 1.8e-6, 0.6e-6, [4.0e14, 5.2e14], 1],
+            [0.4e-6, 0.1e-6, 1.5e-6, 0.99e-6, [4.6e14], 3],
+        ],
+        'probes': [[1.2e-6, 0.0, 'ey']],
+        'checkpoints': [300, 600],
+    },
+]
+
+
 def case(name):
-    for c in CASES_DFT:
+    for c in CASES_DFT + CASES_DFT_HZ:
         if c['name'] == name:
             return c
     raise KeyError(name)

@@ -6,7 +6,7 @@ Run in a container that holds the reference source tree (read-only):
     python tests/golden/make_golden_dft.py /path/to/reference
 
 Each case writes <name>.npz: per field-map monitor its sample boxes (x / y sample slice starts, strides, counts) and
-its complex64 E_z spectra at every checkpoint, the flux monitor's complex128 spectra, the DFT sample interval,
+its complex64 spectra at every checkpoint (E_z; or H_z, E_x, E_y for the H_z cases), the flux monitor's complex128 spectra, the DFT sample interval,
 SHA-256 digests of the fields at every checkpoint, and per field probe its times and float32 values at the end.
 """
 import hashlib
@@ -38,10 +38,15 @@ def run_case(spec):
         sim.run(n_steps=cp - done, print_every=0)
         done = cp
         fields = sim.em.fields
-        for name in ('ez', 'hx', 'hy'):
+        names = ('ez', 'hx', 'hy') if spec['sim'].get('polarization', 'ez') == 'ez' else ('hz', 'ex', 'ey')
+        for name in names:
             out[f'sha_{name}_{cp}'] = digest(np.array(getattr(fields, name)))
         for k, mon in enumerate(maps):
-            out[f'map{k}_{cp}'] = np.array(mon.ez_dft)
+            if mon.polarization == 'ez':
+                out[f'map{k}_{cp}'] = np.array(mon.ez_dft)
+            else:
+                for part in ('hz', 'ex', 'ey'):
+                    out[f'map{k}_{part}_{cp}'] = np.array(getattr(mon, f'{part}_dft'))
         for k, mon in enumerate(fluxes):
             out[f'spec_e{k}_{cp}'] = np.array(mon._spectra.spectra[0])
     for k, mon in enumerate(maps):
@@ -65,9 +70,9 @@ def main():
     sys.path.insert(0, reference)
     sys.path.insert(0, HERE)
     import numpy as np
-    from cases_dft import CASES_DFT
+    from cases_dft import CASES_DFT, CASES_DFT_HZ
     index = {}
-    for spec in CASES_DFT:
+    for spec in CASES_DFT + CASES_DFT_HZ:
         out = run_case(spec)
         np.savez_compressed(os.path.join(HERE, f"{spec['name']}.npz"), **out)
         index[spec['name']] = sorted(out)

@@ -1,5 +1,5 @@
-"""GPU parity of the field-map (running DFT) monitors and field probes of the 2D engines, through the C ABI, against
-open_sol's own outputs (tests/golden/dft_*.npz) and the oracle.  Bar: bit-identical complex64 maps and float32 probe
+"""GPU parity of the field-map (running DFT) monitors and field probes of the 2D E_z and H_z engines, through the C
+ABI, against open_sol's own outputs (tests/golden/dft_*.npz) and the oracle.  Bar: bit-identical complex64 maps and float32 probe
 values (array_equal), for every kernel variant and for chunk boundaries that do and do not fall on sample steps."""
 import hashlib
 import os
@@ -8,9 +8,8 @@ import numpy as np
 import pytest
 
 from cases import apply_ops
-from cases_dft import CASES_DFT
-from oracle.fdtd2d import OracleEz2D
-from test_oracle_golden_dft import run_oracle_dft
+from cases_dft import CASES_DFT, CASES_DFT_HZ
+from test_oracle_golden_dft import field_names, map_keys, map_parts, run_oracle_dft
 
 import opensol_b200 as ob
 from opensol_b200 import serving
@@ -18,6 +17,9 @@ from opensol_b200 import serving
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), 'golden')
 CONFIGS = [(1, 3, 0), (1, 2, 8), (1, 4, 16), (2, 3, 0), (0, 1, 0)]   # (variant, steps per launch, tile rows)
+CONFIGS_HZ = [(1, 1, 0), (1, 1, 16), (0, 1, 0)]
+FIXTURE_RUNS = ([(spec, c) for spec in CASES_DFT for c in CONFIGS] + [(spec, c) for spec in CASES_DFT_HZ
+                                                                      for c in CONFIGS_HZ])
 
 
 def _digest(a):
@@ -34,8 +36,8 @@ def _build(spec, config):
     return sim, fluxes, maps
 
 
-@pytest.mark.parametrize('config', CONFIGS, ids=[f'v{c[0]}_T{c[1]}_r{c[2]}' for c in CONFIGS])
-@pytest.mark.parametrize('spec', CASES_DFT, ids=[c['name'] for c in CASES_DFT])
+@pytest.mark.parametrize('spec,config', FIXTURE_RUNS,
+                         ids=[f"{sp['name']}-v{c[0]}_T{c[1]}_r{c[2]}" for sp, c in FIXTURE_RUNS])
 def test_maps_bit_exact_against_reference(spec, config):
     g = np.load(os.path.join(GOLDEN, f"{spec['name']}.npz"))
     sim, fluxes, maps = _build(spec, config)
@@ -43,12 +45,12 @@ def test_maps_bit_exact_against_reference(spec, config):
     for cp in spec['checkpoints']:
         sim.run(n_steps=cp - done, verbose=False, print_every=0)
         done = cp
-        for name in ('ez', 'hx', 'hy'):
+        for name in field_names(spec):
             assert _digest(sim.em.engine.read_field(name)) == str(g[f'sha_{name}_{cp}']), f'{name} at {cp}'
         for k, mon in enumerate(maps):
-            got = mon.ez_dft
-            assert got.dtype == np.complex64
-            np.testing.assert_array_equal(got, g[f'map{k}_{cp}'])
+            for got, key in zip(map_parts(mon), map_keys(spec, k, cp)):
+                assert got.dtype == np.complex64
+                np.testing.assert_array_equal(got, g[key])
         for k, mon in enumerate(fluxes):
             np.testing.assert_array_equal(mon.spectra()[0], g[f'spec_e{k}_{cp}'])
     for k, probe in enumerate(sim.probes):
@@ -112,7 +114,7 @@ def test_random_maps_and_chunks_match_oracle(seed):
         sim.em.engine.advance(int(cp - done))
         done = cp
         for k, mon in enumerate(maps):
-            np.testing.assert_array_equal(mon.ez_dft, snaps[cp][0][k])
+            np.testing.assert_array_equal(mon.ez_dft, snaps[cp][0][k][0])
     sim.em.engine.close()
 
 
