@@ -161,6 +161,18 @@ int os_fdtd2d_add_dft_map(OsFdtd2D *h, int32_t x_start, int32_t x_stop, int32_t 
  * handle (hz_dft, ex_dft, ey_dft). */
 int os_fdtd2d_read_dft_map(OsFdtd2D *h, int32_t map_id, float *spectra);
 
+/* +x plane wave in vacuum on a total-field box of E_z cells [x0, x1) x [y0, y1): TFSFSource (physics/em/sources.py:
+ * 206-350).  The host computes, as the reference does, the 1D incident line of aux_cells cells (the box's first
+ * column at aux index aux_x0, the soft source at source_index), its H and E coefficients aux_coef_h (aux_cells - 1
+ * hi faces) and aux_coef_e (aux_cells centres), the Mur end coefficients, and the side coefficients coef_h (H_y rows
+ * x0 - 1, x1 - 1; H_x columns y0 - 1, y1 - 1) and coef_e (E_z rows x0, x1 - 1).  Each step: the H side corrections
+ * and the incident H update after the H update, the E side corrections and the incident E update (soft source from
+ * row n_lines + box of the chunk's value table) after the E update and the line sources.  An engine with a box
+ * advances with the per-half-step kernels.  E_z engines only; not in batched advances or the adjoint.  At most 4. */
+int os_fdtd2d_add_tfsf(OsFdtd2D *h, int32_t x0, int32_t x1, int32_t y0, int32_t y1, int32_t aux_cells, int32_t aux_x0,
+                       int32_t source_index, const float *coef_h, const float *coef_e, float mur_lo, float mur_hi,
+                       const float *aux_coef_h, const float *aux_coef_e, int32_t *tfsf_id);
+
 /* Field probe: one component (OS_EZ / OS_HX / OS_HY, or OS_HZ_* on an H_z handle) of cell (ix, iy) recorded after
  * every step from the current one on: FieldProbe.record at t_full (core/monitors.py:194-243, fdtd_2d_base.py:481-487).
  * At most 8.  An advance with probes runs one step per launch.  Not in batched advances; os_fdtd2d_advance_noalloc

@@ -45,6 +45,14 @@ struct ProbeSet {
     int64_t start[OS_MAX_PROBES];
 };
 
+// +x plane-wave TFSF box (TFSFSource): the 1D incident line and the side coefficients, all float32 as computed by
+// the host.
+struct Tfsf2D {
+    int32_t x0, x1, y0, y1, aux_x0, aux_n, source_index;
+    float coef_h[4], coef_e[2], mur_lo, mur_hi;
+    DeviceArray<float> aux_ez, aux_hy, aux_coef_h, aux_coef_e;
+};
+
 struct DftMap2D {                       // field-map running DFT (DFTMonitor)
     int32_t x0, y0, ds, mx, my, nf;     // first sampled cell, stride, samples per axis, frequencies
     bool hz;                            // H_z engine: H_z, E_x, E_y maps (E at the cell centres), two phase tables
@@ -87,6 +95,8 @@ struct OsFdtd2D {
     std::vector<std::unique_ptr<os::FluxLine2D>> fluxes;
     std::vector<std::unique_ptr<os::DftMap2D>> maps;   // field-map DFTs (E_z engines), after the flux lines in a
                                                        // chunk's phase table
+    std::vector<std::unique_ptr<os::Tfsf2D>> tfsf;   // plane-wave boxes (E_z engines; their value rows follow the
+                                                     // line sources' in a chunk's value table)
     os::ProbeSet probes{};                // field probes (recorded after every step)
     os::DeviceArray<float> probe_rows;    // (OS_MAX_PROBES, probe_capacity) values by step
     int64_t probe_capacity = 0;           // rows per probe
@@ -144,6 +154,10 @@ static int zero_state(OsFdtd2D *h) {
         OS_CUDA(cudaMemsetAsync(f->h_acc.ptr, 0, f->h_acc.bytes(), h->stream));
     }
     for (auto &d : h->maps) OS_CUDA(cudaMemsetAsync(d->acc.ptr, 0, d->acc.bytes(), h->stream));
+    for (auto &t : h->tfsf) {
+        OS_CUDA(cudaMemsetAsync(t->aux_ez.ptr, 0, t->aux_ez.bytes(), h->stream));
+        OS_CUDA(cudaMemsetAsync(t->aux_hy.ptr, 0, t->aux_hy.bytes(), h->stream));
+    }
     for (int k = 0; k < h->probes.n; ++k) h->probes.start[k] = 0;   // rows recorded again from step 0
     h->n_step = 0;
     return OS_OK;
@@ -306,6 +320,7 @@ extern "C" int os_fdtd2d_destroy(OsFdtd2D *h) {
         for (auto &l : h->lines) give(l->profile);
         for (auto &f : h->fluxes) give(f->e_acc), give(f->h_acc), give(f->stage);
         for (auto &d : h->maps) give(d->acc);
+        for (auto &t : h->tfsf) give(t->aux_ez), give(t->aux_hy), give(t->aux_coef_h), give(t->aux_coef_e);
         give(h->probe_rows);
         give(h->err), give(h->line_values), give(h->phases);
         pool_events_done(ev);
@@ -1144,7 +1159,26 @@ static int advance_per_step(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, 
     for (int64_t k = 0; k < n_steps; ++k) {
         OS_TRY(prof_begin(h, 3, h->stream));
         ez2d_h_kernel<<<grid, block, 0, h->stream>>>(p);
+        for (auto &t : h->tfsf) {   // TFSFSource.inject_h after the H update (fdtd_ez_2d.py:85-88)
+            const int side = std::max(t->x1 - t->x0, t->y1 - t->y0);
+            ez2d_tfsf_h_kernel<<<(side + 255) / 256, 256, 0, h->stream>>>(
+                p.hx, p.hy, t->aux_ez.ptr, t->x0, t->x1, t->y0, t->y1, t->aux_x0, h->grid.ny, t->coef_h[0],
+                t->coef_h[1], t->coef_h[2], t->coef_h[3]);
+            ez2d_tfsf_aux_h_kernel<<<(t->aux_n + 255) / 256, 256, 0, h->stream>>>(t->aux_ez.ptr, t->aux_coef_h.ptr,
+                                                                                   t->aux_hy.ptr, t->aux_n);
+            h->launches += 2;
+        }
         ez2d_e_kernel<<<grid, block, 0, h->stream>>>(p, values, n_steps, k);
+        for (size_t b = 0; b < h->tfsf.size(); ++b) {   // TFSFSource.inject_e at t + dt/2 (fdtd_ez_2d.py:92-99)
+            Tfsf2D &t = *h->tfsf[b];
+            ez2d_tfsf_e_kernel<<<(t.y1 - t.y0 + 255) / 256, 256, 0, h->stream>>>(
+                p.ez, t.aux_hy.ptr, t.x0, t.x1, t.y0, t.y1, t.aux_x0, h->grid.ny, t.coef_e[0], t.coef_e[1]);
+            // this step's source value: row n_lines + b of the chunk's value table
+            const float *value = values + (h->lines.size() + b) * (size_t)n_steps + (size_t)k;
+            ez2d_tfsf_aux_e_kernel<<<1, 256, 0, h->stream>>>(t.aux_ez.ptr, t.aux_hy.ptr, t.aux_n, t.aux_coef_e.ptr,
+                                                             t.source_index, value, t.mur_lo, t.mur_hi);
+            h->launches += 2;
+        }
         OS_TRY(prof_end(h, h->stream));
         h->launches += 2;
         h->n_step += 1;
@@ -1395,7 +1429,7 @@ static int check_advance(const OsFdtd2D *h, const char *fn, int64_t n_steps, con
         OS_CHECK(!(h->grid.cpml_sides & (1 << s)) || h->cpml_set[s], OS_ERR_STATE,
                  "%s: CPML side %d has no recursion rows", fn, 1 << s);
     if (n_steps == 0) return OS_OK;
-    OS_CHECK(h->lines.empty() || line_values, OS_ERR_INVALID, "%s: line_values is required", fn);
+    OS_CHECK((h->lines.empty() && h->tfsf.empty()) || line_values, OS_ERR_INVALID, "%s: line_values is required", fn);
     const int64_t m = h->sample_interval;
     const int64_t q_first = h->n_step / m + 1, q_last = (h->n_step + n_steps) / m;
     if ((!h->fluxes.empty() || !h->maps.empty()) && q_last >= q_first) {
@@ -1411,9 +1445,11 @@ static int check_advance(const OsFdtd2D *h, const char *fn, int64_t n_steps, con
 static int run_chunk(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples, const float *values,
                      const float *phase_table) {
     OS_CUDA(cudaEventRecord(h->ev_start, h->stream));
+    // a TFSF box corrects H between the H and E updates of every step: the per-half-step kernels run it
     const int rc = h->polarization == 1 ? advance_hz(h, n_steps, first_sample, n_samples, values, phase_table)
-                   : h->variant == 0    ? advance_per_step(h, n_steps, first_sample, n_samples, values, phase_table)
-                                        : advance_blocked(h, n_steps, first_sample, n_samples, values, phase_table);
+                   : (h->variant == 0 || !h->tfsf.empty())
+                       ? advance_per_step(h, n_steps, first_sample, n_samples, values, phase_table)
+                       : advance_blocked(h, n_steps, first_sample, n_samples, values, phase_table);
     if (rc != OS_OK) return rc;
     OS_CUDA(cudaEventRecord(h->ev_stop, h->stream));
     h->timed = true;
@@ -1438,7 +1474,8 @@ extern "C" int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line
     h->prof_used = 0;
     if (n_steps == 0) return OS_OK;
     OS_TRY(bind_device(h));
-    if (!h->lines.empty()) OS_TRY(upload(h->line_values, line_values, h->lines.size() * (size_t)n_steps, h->stream));
+    const size_t value_rows = h->lines.size() + h->tfsf.size();   // line sources, then TFSF boxes
+    if (value_rows) OS_TRY(upload(h->line_values, line_values, value_rows * (size_t)n_steps, h->stream));
     const size_t phase_floats = phase_floats_of(h, n_samples);
     if (phase_floats && phases) OS_TRY(upload(h->phases, phases, phase_floats, h->stream));
     OS_TRY(reserve_probe_rows(h, n_steps));
@@ -1489,7 +1526,7 @@ extern "C" int os_fdtd2d_advance_noalloc(OsFdtd2D *h, int64_t n_steps, const flo
     OS_CHECK(h->probes.n == 0 || h->n_step + n_steps <= h->probe_capacity, OS_ERR_STATE,
              "os_fdtd2d_advance_noalloc: the field probes' rows would have to grow; advance with os_fdtd2d_advance");
     // tables: line values at float 0, phases at the next 64-float (256-byte) boundary
-    const size_t value_floats = n_steps > 0 ? h->lines.size() * (size_t)n_steps : 0;
+    const size_t value_floats = n_steps > 0 ? (h->lines.size() + h->tfsf.size()) * (size_t)n_steps : 0;
     const size_t phase_floats = n_steps > 0 && n_samples > 0 ? phase_floats_of(h, n_samples) : 0;
     const size_t phase_offset = (value_floats + 63) / 64 * 64;
     const size_t need = phase_floats ? phase_offset + phase_floats : value_floats;
@@ -1691,6 +1728,39 @@ extern "C" int os_fdtd2d_add_dft_map(OsFdtd2D *h, int32_t x_start, int32_t x_sto
     OS_CUDA(cudaMemsetAsync(d->acc.ptr, 0, d->acc.bytes(), h->stream));
     if (map_id) *map_id = (int32_t)h->maps.size();
     h->maps.push_back(std::move(d));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_add_tfsf(OsFdtd2D *h, int32_t x0, int32_t x1, int32_t y0, int32_t y1, int32_t aux_cells,
+                                  int32_t aux_x0, int32_t source_index, const float *coef_h, const float *coef_e,
+                                  float mur_lo, float mur_hi, const float *aux_coef_h, const float *aux_coef_e,
+                                  int32_t *tfsf_id) {
+    OS_TRY(require_ez(h, "os_fdtd2d_add_tfsf"));
+    OS_CHECK(coef_h && coef_e && aux_coef_h && aux_coef_e, OS_ERR_INVALID, "os_fdtd2d_add_tfsf: null argument");
+    OS_CHECK(1 <= x0 && x0 < x1 && x1 < h->grid.nx && 1 <= y0 && y0 < y1 && y1 < h->grid.ny, OS_ERR_INVALID,
+             "TFSF box [%d, %d) x [%d, %d) must keep one scattered-field cell on every side of the %d x %d grid", x0,
+             x1, y0, y1, h->grid.nx, h->grid.ny);
+    OS_CHECK(aux_x0 >= 1 && aux_x0 + (x1 - x0) < aux_cells && 1 <= source_index && source_index < aux_cells - 1,
+             OS_ERR_INVALID, "TFSF incident line of %d cells cannot hold the box at %d and the source at %d",
+             aux_cells, aux_x0, source_index);
+    OS_CHECK(h->tfsf.size() < 4, OS_ERR_INVALID, "at most 4 TFSF boxes per engine");
+    OS_CHECK(h->lines.size() + h->tfsf.size() < (size_t)OS_MAX_LINES_2D, OS_ERR_INVALID,
+             "at most %d line sources and TFSF boxes per engine", OS_MAX_LINES_2D);
+    OS_TRY(bind_device(h));
+    std::unique_ptr<Tfsf2D> t(new Tfsf2D());
+    t->x0 = x0, t->x1 = x1, t->y0 = y0, t->y1 = y1;
+    t->aux_n = aux_cells, t->aux_x0 = aux_x0, t->source_index = source_index;
+    for (int k = 0; k < 4; ++k) t->coef_h[k] = coef_h[k];
+    t->coef_e[0] = coef_e[0], t->coef_e[1] = coef_e[1];
+    t->mur_lo = mur_lo, t->mur_hi = mur_hi;
+    OS_TRY(t->aux_ez.alloc((size_t)aux_cells));
+    OS_TRY(t->aux_hy.alloc((size_t)aux_cells));
+    OS_CUDA(cudaMemsetAsync(t->aux_ez.ptr, 0, t->aux_ez.bytes(), h->stream));
+    OS_CUDA(cudaMemsetAsync(t->aux_hy.ptr, 0, t->aux_hy.bytes(), h->stream));
+    OS_TRY(upload(t->aux_coef_h, aux_coef_h, (size_t)aux_cells - 1, h->stream));
+    OS_TRY(upload(t->aux_coef_e, aux_coef_e, (size_t)aux_cells, h->stream));
+    if (tfsf_id) *tfsf_id = (int32_t)h->tfsf.size();
+    h->tfsf.push_back(std::move(t));
     return OS_OK;
 }
 
@@ -1979,9 +2049,9 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
                  "os_fdtd2d_batch_advance: job %d is not on the batch stream (os_fdtd2d_set_stream with "
                  "os_fdtd2d_batch_stream)", q);
         OS_CHECK(!h->profiling, OS_ERR_STATE, "os_fdtd2d_batch_advance: job %d has profiling on", q);
-        OS_CHECK(h->maps.empty() && h->probes.n == 0, OS_ERR_STATE,
-                 "os_fdtd2d_batch_advance: job %d has field-map monitors or field probes (advance it with "
-                 "os_fdtd2d_advance)", q);
+        OS_CHECK(h->maps.empty() && h->probes.n == 0 && h->tfsf.empty(), OS_ERR_STATE,
+                 "os_fdtd2d_batch_advance: job %d has field-map monitors, field probes or a TFSF box (advance it "
+                 "with os_fdtd2d_advance)", q);
     }
     OS_CUDA(cudaSetDevice(b->device));
     // every job's own tables, in its own buffers, as os_fdtd2d_advance uploads them
@@ -2296,6 +2366,7 @@ extern "C" int os_fdtd2d_adjoint_create(OsFdtd2D *h, int32_t box_i0, int32_t box
     OS_CHECK(h && out, OS_ERR_INVALID, "os_fdtd2d_adjoint_create: null argument");
     OS_TRY(require_ez(h, "os_fdtd2d_adjoint_create"));
     *out = nullptr;
+    OS_CHECK(h->tfsf.empty(), OS_ERR_STATE, "os_fdtd2d_adjoint_create: the adjoint does not transpose a TFSF box");
     OS_CHECK(h->has_cb && h->has_spacings, OS_ERR_STATE, "os_fdtd2d_adjoint_create: coefficients and spacings first");
     OS_CHECK(0 <= box_i0 && box_i0 < box_i1 && box_i1 <= h->grid.nx && 0 <= box_j0 && box_j0 < box_j1 &&
                  box_j1 <= h->grid.ny, OS_ERR_INVALID, "os_fdtd2d_adjoint_create: design box outside the grid");

@@ -231,6 +231,62 @@ __global__ void hz2d_dft_map_kernel(const float *__restrict__ hz, const float *_
     }
 }
 
+// ---- +x plane-wave TFSF box (TFSFSource, physics/em/sources.py:35-52,72-186,334-350)
+// Scattered / total-field H corrections after the H update: H_y on rows x0 - 1 (-) and x1 - 1 (+) from the incident
+// E_z at the box's first / last column, H_x on columns y0 - 1 (+) and y1 - 1 (-) from the incident E_z of each row.
+__global__ void ez2d_tfsf_h_kernel(float *__restrict__ hx, float *__restrict__ hy, const float *__restrict__ aux_ez,
+                                   int x0, int x1, int y0, int y1, int aux_x0, int ny, float c_xlo, float c_xhi,
+                                   float c_ylo, float c_yhi) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < y1 - y0) {
+        const int j = y0 + k;
+        hy[(size_t)(x0 - 1) * ny + j] = hy[(size_t)(x0 - 1) * ny + j] - c_xlo * aux_ez[aux_x0];
+        hy[(size_t)(x1 - 1) * ny + j] = hy[(size_t)(x1 - 1) * ny + j] + c_xhi * aux_ez[aux_x0 + (x1 - 1 - x0)];
+    }
+    if (k < x1 - x0) {
+        const size_t row = (size_t)(x0 + k) * ny;
+        const float incident = aux_ez[aux_x0 + k];
+        hx[row + (y0 - 1)] = hx[row + (y0 - 1)] + c_ylo * incident;
+        hx[row + (y1 - 1)] = hx[row + (y1 - 1)] - c_yhi * incident;
+    }
+}
+
+// The incident line's H update: aux_hy[a] += coef[a] (aux_ez[a + 1] - aux_ez[a]), a < n - 1.
+__global__ void ez2d_tfsf_aux_h_kernel(const float *__restrict__ aux_ez, const float *__restrict__ coef,
+                                       float *__restrict__ aux_hy, int n) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < n - 1) aux_hy[a] = aux_hy[a] + coef[a] * (aux_ez[a + 1] - aux_ez[a]);
+}
+
+// Total-field E_z corrections after the E update: rows x0 (-) and x1 - 1 (+) from the incident H_y.
+__global__ void ez2d_tfsf_e_kernel(float *__restrict__ ez, const float *__restrict__ aux_hy, int x0, int x1, int y0,
+                                   int y1, int aux_x0, int ny, float c_xlo, float c_xhi) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= y1 - y0) return;
+    const int j = y0 + k;
+    ez[(size_t)x0 * ny + j] = ez[(size_t)x0 * ny + j] - c_xlo * aux_hy[aux_x0 - 1];
+    ez[(size_t)(x1 - 1) * ny + j] = ez[(size_t)(x1 - 1) * ny + j] + c_xhi * aux_hy[aux_x0 + (x1 - 1 - x0)];
+}
+
+// The incident line's E update (one block): aux_ez[a] += ce[a] (aux_hy[a] - aux_hy[a - 1]) for 0 < a < n - 1, the soft
+// source value at aux cell `src`, then the Mur ends from the ends' values before the update.
+__global__ void ez2d_tfsf_aux_e_kernel(float *__restrict__ aux_ez, const float *__restrict__ aux_hy, int n,
+                                       const float *__restrict__ ce, int src, const float *__restrict__ value,
+                                       float mur_lo, float mur_hi) {
+    __shared__ float edge_old[4];
+    if (threadIdx.x == 0) {
+        edge_old[0] = aux_ez[0], edge_old[1] = aux_ez[1], edge_old[2] = aux_ez[n - 2], edge_old[3] = aux_ez[n - 1];
+    }
+    __syncthreads();
+    for (int a = 1 + threadIdx.x; a < n - 1; a += blockDim.x) aux_ez[a] = aux_ez[a] + ce[a] * (aux_hy[a] - aux_hy[a - 1]);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        aux_ez[src] = aux_ez[src] + *value;
+        aux_ez[0] = edge_old[1] + mur_lo * (aux_ez[1] - edge_old[0]);
+        aux_ez[n - 1] = edge_old[2] + mur_hi * (aux_ez[n - 2] - edge_old[3]);
+    }
+}
+
 // ca / cb from float32 eps_r, sigma_e (fdtd_ez_2d_kernels.py:314-332, T = float); sigma NULL = lossless (ca not
 // written: it is 1).
 __global__ void ez2d_e_coefficients_kernel(const float *__restrict__ eps_r, const float *__restrict__ sigma, float dt,

@@ -43,6 +43,7 @@ class FDTDEngine2D_Ez:
                                    float(self.dt))
         self._handle = None
         self._lines = []          # LineSource objects in add order
+        self._tfsf = []           # TFSFSource boxes in add order (value rows after the line sources')
         self._line_ids = {}       # id(source) -> native id
         self._profiles_sent = {}  # id(source) -> profile array last uploaded
         self._monitors = []       # FluxMonitor objects in add order
@@ -100,6 +101,10 @@ class FDTDEngine2D_Ez:
         self._monitors.append(monitor)
         monitor._reader = lambda m=monitor: self.read_flux_spectra(m)
 
+    def attach_tfsf(self, source):
+        """Register a TFSF plane-wave box; it is created on the device at the next sync."""
+        self._tfsf.append(source)
+
     def attach_probe(self, probe):
         """Register a FieldProbe; it is created on the device at the next sync and records from the step then."""
         if probe.field_component not in self.FIELDS:
@@ -143,6 +148,17 @@ class FDTDEngine2D_Ez:
                 _native.check(lib.os_fdtd2d_add_flux_line(h, normal, monitor.position, monitor.span[0],
                                                           monitor.span[1], monitor.n_freqs, ctypes.byref(mid)))
                 self._monitor_ids[id(monitor)] = mid.value
+        for source in self._tfsf:
+            if id(source) not in self._monitor_ids:
+                tid = ctypes.c_int32()
+                coef_h = np.array(source.coef_h, dtype=DTYPE)
+                coef_e = np.array(source.coef_e, dtype=DTYPE)
+                _native.check(lib.os_fdtd2d_add_tfsf(
+                    h, source.x0, source.x1, source.y0, source.y1, source.aux_cells, source.aux_x0,
+                    source.AUX_SOURCE_INDEX, _native.fptr(coef_h), _native.fptr(coef_e), float(source.mur[0]),
+                    float(source.mur[1]), _native.fptr(source.aux_coef_h), _native.fptr(source.aux_coef_e),
+                    ctypes.byref(tid)))
+                self._monitor_ids[id(source)] = tid.value
         for probe in self._probes:
             if id(probe) not in self._monitor_ids:
                 pid = ctypes.c_int32()
@@ -240,7 +256,8 @@ class FDTDEngine2D_Ez:
             t_half[k] = t + 0.5 * dt
             t = t + dt
             t_full[k] = t
-        values = (np.stack([src.values(t_half) for src in self._lines]) if self._lines
+        rows = self._lines + self._tfsf   # line sources, then TFSF boxes (the device's value-table order)
+        values = (np.stack([src.values(t_half) for src in rows]) if rows
                   else np.zeros((0, n_steps), dtype=np.float32))
         m = self.sample_interval
         first_q = self.n_step // m + 1

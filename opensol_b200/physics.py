@@ -17,7 +17,7 @@ from .boundaries import BoundaryConfig, inverse_spacings
 from .constants import C0, DTYPE
 from .engine2d import FDTDEngine2D_Ez, FDTDEngine2D_Hz
 from .monitors import PROBE_COMPONENTS, DFTMonitor, FieldProbe, FluxMonitor, dft_sample_interval, resolve_frequencies
-from .sources import (LineSource, calibrate_line_source, calibrate_tangential_sheet, carrier_angular_frequency,
+from .sources import (LineSource, TFSFSource, calibrate_line_source, calibrate_tangential_sheet, carrier_angular_frequency,
                       make_temporal, resolve_frequency)
 
 
@@ -235,6 +235,33 @@ class EMPhysics:
         self._calibrations.append((source, carrier_angular_frequency(temporal), normal_width))
         self._calibration_dirty = True
         self.engine.attach_line_source(source)
+        return source
+
+    def add_tfsf(self, x0, y0, x1, y1, wavelength=None, frequency=None, bandwidth=0.5, amplitude=1.0,
+                 waveform='gaussian'):
+        """+x plane wave of incident peak `amplitude` [V/m] (E_z) inside the box (physics/em/__init__.py:475-490 with
+        placement.tfsf_box_cells): the box's cells plus one scattered-field cell on every side lie in the physical
+        window (this engine's boundary presets have no mirror face a box could open onto)."""
+        if self.polarization != 'ez':
+            raise NotImplementedError('TFSF plane waves are built for the E_z engine only')
+        d = self.domain
+        temporal = make_temporal(waveform, resolve_frequency(wavelength, frequency), bandwidth)
+        d.validate_physical_pos(x0, y0, "TFSF box corner 0")
+        d.validate_physical_pos(x1, y1, "TFSF box corner 1")
+        x_lo, x_hi = sorted((x0, x1))
+        y_lo, y_hi = sorted((y0, y1))
+        ix0, ix1 = d.pos_to_cell_x(x_lo), d.pos_to_cell_x(x_hi) + 1
+        iy0, iy1 = d.pos_to_cell_y(y_lo), d.pos_to_cell_y(y_hi) + 1
+        window_x, window_y = d.physical_window()
+        if ix0 <= window_x.start or ix1 >= window_x.stop or iy0 <= window_y.start or iy1 >= window_y.stop:
+            raise ValueError(f"TFSF box cells [{ix0}, {ix1}) x [{iy0}, {iy1}) need at least one scattered-field cell "
+                             f"inside the physical window [{window_x.start}, {window_x.stop}) x "
+                             f"[{window_y.start}, {window_y.stop}) on every side")
+        grid = d.grid
+        widths = (np.full(grid.nx, float(grid.dx)), np.full(grid.ny, float(grid.dy)))   # yee_grid.grid_cell_widths
+        source = TFSFSource(ix0, ix1, iy0, iy1, temporal, float(grid.dt), amplitude, cell_widths=widths)
+        self.sources.append(source)
+        self.engine.attach_tfsf(source)
         return source
 
     # --- monitors ---------------------------------------------------------------------------------------

@@ -205,3 +205,65 @@ def calibrate_tangential_sheet(source, materials, omega, normal_spacing, dt, sha
                                   normal_spacing, dt)
     weight = np.asarray(2.0 * np.ones(hi - lo) / (float(ETA0) * normal_spacing), dtype=DTYPE)
     return (cb_line * admittance * weight).astype(DTYPE)
+
+
+class TFSFSource:
+    """+x plane wave in vacuum on a total-field box of E_z cells [x0, x1) x [y0, y1) (physics/em/sources.py:206-332,
+    _PlaneWaveBox + TFSFSource): a 1D incident line (20 margin cells at the widths of cells x0 - 1 / x1, the box
+    columns between; soft source at aux cell 10 upstream of the box, Mur ends matched to the numerical phase velocity
+    at the carrier) advanced on the device beside the grid, and the scattered / total-field corrections on the box
+    sides: H_y on rows x0 - 1 and x1 - 1, H_x on columns y0 - 1 and y1 - 1 after the H update, E_z on rows x0 and
+    x1 - 1 after the E update.  Incident E_z peak = amplitude [V/m].  The parameters here are host float64 rounded to
+    float32 exactly as the reference rounds them."""
+
+    AUX_MARGIN = 20
+    AUX_SOURCE_INDEX = 10
+
+    def __init__(self, x0, x1, y0, y1, temporal, dt, amplitude=1.0, cell_widths=None):
+        x0, x1, y0, y1 = int(x0), int(x1), int(y0), int(y1)
+        if not (1 <= x0 < x1 and 1 <= y0 < y1):
+            raise ValueError(f"TFSF box [{x0}, {x1}) x [{y0}, {y1}) must be non-empty and keep one scattered-field "
+                             f"cell on the lo sides (x0 >= 1, y0 >= 1)")
+        dx_cells, dy_cells = (np.asarray(w, dtype=np.float64) for w in cell_widths)
+        if x1 >= dx_cells.size or y1 >= dy_cells.size:
+            raise ValueError(f"TFSF box [{x0}, {x1}) x [{y0}, {y1}) needs a scattered-field cell on the hi sides of a "
+                             f"{dx_cells.size} x {dy_cells.size} grid")
+        self.x0, self.x1, self.y0, self.y1 = x0, x1, y0, y1
+        self.temporal = temporal
+        self.amplitude = float(amplitude)
+        dt = float(dt)
+        m = self.AUX_MARGIN
+        up, down = float(dx_cells[x0 - 1]), float(dx_cells[x1])
+        widths = np.concatenate((np.full(m, up), dx_cells[x0:x1], np.full(m, down)))
+        face_spacings = 0.5 * (widths[:-1] + widths[1:])
+        half_omega_dt = 0.5 * carrier_angular_frequency(temporal) * dt
+        courant, cos_half_kappa, mur_lo = _aux_line_terms(up, dt, half_omega_dt)
+        _, _, mur_hi = _aux_line_terms(down, dt, half_omega_dt)
+        self.source_scale = 2.0 * courant * cos_half_kappa * self.amplitude
+        self.mur = (DTYPE(mur_lo), DTYPE(mur_hi))
+        side_widths_x = (float(dx_cells[x0]), float(dx_cells[x1 - 1]))
+        side_spacings = tuple(0.5 * float(w[i] + w[i + 1]) for w, i in ((dx_cells, x0 - 1), (dx_cells, x1 - 1),
+                                                                       (dy_cells, y0 - 1), (dy_cells, y1 - 1)))
+        self.coef_h = tuple(DTYPE(dt / (MU0 * s)) for s in side_spacings)     # H_y x0-1, x1-1; H_x y0-1, y1-1
+        self.coef_e = tuple(DTYPE(dt / (EPS0 * w)) for w in side_widths_x)    # E_z x0, x1-1
+        self.aux_coef_h = np.asarray(dt / (MU0 * face_spacings), dtype=DTYPE)  # (n - 1,) hi faces
+        self.aux_coef_e = np.asarray(dt / (EPS0 * widths), dtype=DTYPE)        # (n,) centres
+        self.aux_x0 = m
+        self.aux_cells = int(widths.size)
+
+    def values(self, t_half):
+        """float32 soft-source value of each step: FP32(source_scale * temporal(t + dt/2))."""
+        return np.array([DTYPE(self.source_scale * self.temporal(float(t))) for t in t_half], dtype=DTYPE)
+
+
+def _aux_line_terms(width, dt, half_omega_dt, index=1.0):
+    """(Courant number, cos(kappa0 / 2), Mur coefficient) of a uniform 1D line at the carrier
+    (physics/em/sources.py:191-204); ValueError when the carrier does not propagate on it."""
+    courant = C0 * float(dt) / (float(index) * float(width))
+    sin_half_kappa = math.sin(half_omega_dt) / courant
+    if sin_half_kappa >= 1.0:
+        raise ValueError(f"TFSF: the centre frequency has no propagating wave on the 1D grid (sin(k dx/2) = "
+                         f"{sin_half_kappa:.3g} >= 1, at most pi cells per wavelength in the medium); refine the mesh")
+    cos_half_kappa = math.sqrt(1.0 - sin_half_kappa ** 2)
+    mur_courant = courant * cos_half_kappa / math.cos(half_omega_dt)
+    return courant, cos_half_kappa, (mur_courant - 1.0) / (mur_courant + 1.0)

@@ -13,6 +13,10 @@
  *                             t + dt/2, n_step += 1, monitors every sample_interval steps: fdtd_2d_base.py:470-488)
  *   - soft line source        open_sol/core/sources.py:146-154,221-229 (target += scale * profile, skipped at 0)
  *   - line DFT accumulation   open_sol/physics/em/monitors.py:45-46 (complex128 += complex64 phase * (double)f)
+ *   - TFSF plane-wave box     open_sol/physics/em/sources.py:35-52 (host twins of the side corrections and the 1D
+ *                             incident line), 334-350 (inject_h after the H update, inject_e after the E update); the
+ *                             E-side corrections run after the line sources (open_sol: sources in add order, which
+ *                             gives the same bits whenever no line source shares a cell with a box side)
  * Every float operation keeps the reference's evaluation order; build with -ffp-contract=off (no FMA contraction).
  * Rows are parallelised with OpenMP: each cell of a half step is independent, so the thread count never changes a
  * result.
@@ -63,7 +67,48 @@ typedef struct {
     int64_t n_samples;
 } OracleFlux;
 
+typedef struct {
+    int32_t x0, x1, y0, y1, aux_x0, aux_n, source_index;
+    real coef_h[4], coef_e[2], mur_lo, mur_hi;
+    real *aux_ez, *aux_hy;                    /* (aux_n,) incident line: cell centres / hi faces */
+    const real *aux_coef_h, *aux_coef_e;      /* (aux_n - 1,) / (aux_n,) */
+    const float *values;                      /* (n_steps,) float32 soft-source value of each step of the chunk */
+} OracleTfsf;
+
 static inline real coef_or(const real *array, size_t idx, real uniform) { return array ? array[idx] : uniform; }
+
+/* TFSFSource.inject_h: H_y / H_x side corrections from the incident E_z, then the incident H update. */
+static void tfsf_h(const OracleEz2D *s, const OracleTfsf *t)
+{
+    const size_t ny = (size_t)s->ny;
+    for (int j = t->y0; j < t->y1; ++j) {
+        s->hy[(size_t)(t->x0 - 1) * ny + j] -= t->coef_h[0] * t->aux_ez[t->aux_x0];
+        s->hy[(size_t)(t->x1 - 1) * ny + j] += t->coef_h[1] * t->aux_ez[t->aux_x0 + (t->x1 - 1 - t->x0)];
+    }
+    for (int i = t->x0; i < t->x1; ++i) {
+        const real incident = t->aux_ez[t->aux_x0 + (i - t->x0)];
+        s->hx[(size_t)i * ny + (t->y0 - 1)] += t->coef_h[2] * incident;
+        s->hx[(size_t)i * ny + (t->y1 - 1)] -= t->coef_h[3] * incident;
+    }
+    for (int a = 0; a < t->aux_n - 1; ++a) t->aux_hy[a] += t->aux_coef_h[a] * (t->aux_ez[a + 1] - t->aux_ez[a]);
+}
+
+/* TFSFSource.inject_e: E_z side corrections from the incident H_y, then the incident E update with the soft source
+ * and the Mur ends (from the ends' values before the update). */
+static void tfsf_e(const OracleEz2D *s, const OracleTfsf *t, int64_t k)
+{
+    const size_t ny = (size_t)s->ny;
+    for (int j = t->y0; j < t->y1; ++j) {
+        s->ez[(size_t)t->x0 * ny + j] -= t->coef_e[0] * t->aux_hy[t->aux_x0 - 1];
+        s->ez[(size_t)(t->x1 - 1) * ny + j] += t->coef_e[1] * t->aux_hy[t->aux_x0 + (t->x1 - 1 - t->x0)];
+    }
+    const int n = t->aux_n;
+    const real old0 = t->aux_ez[0], old1 = t->aux_ez[1], old2 = t->aux_ez[n - 2], old3 = t->aux_ez[n - 1];
+    for (int a = 1; a < n - 1; ++a) t->aux_ez[a] += t->aux_coef_e[a] * (t->aux_hy[a] - t->aux_hy[a - 1]);
+    t->aux_ez[t->source_index] += (real)t->values[k];
+    t->aux_ez[0] = old1 + t->mur_lo * (t->aux_ez[1] - old0);
+    t->aux_ez[n - 1] = old2 + t->mur_hi * (t->aux_ez[n - 2] - old3);
+}
 
 static void update_h(const OracleEz2D *s)
 {
@@ -207,17 +252,20 @@ static void accumulate_flux(const OracleEz2D *s, OracleFlux *m, int64_t sample)
 /* Advance n_steps steps starting after engine step `step0` (the engine's n_step before the chunk).  Line source
  * values are indexed by the step within the chunk; monitors sample when (step0 + k + 1) % sample_interval == 0.
  * Returns 0, or -1 when a monitor's phase table does not cover a sample. */
-int oracle_ez2d_advance(OracleEz2D *s, int64_t step0, int64_t n_steps, int32_t n_lines, const OracleLine *lines,
-                        int32_t n_monitors, OracleFlux *monitors, int64_t sample_interval)
+int oracle_ez2d_advance_tfsf(OracleEz2D *s, int64_t step0, int64_t n_steps, int32_t n_lines, const OracleLine *lines,
+                             int32_t n_monitors, OracleFlux *monitors, int64_t sample_interval, int32_t n_tfsf,
+                             const OracleTfsf *tfsf)
 {
     for (int64_t k = 0; k < n_steps; ++k) {
         update_h(s);
         for (int side = 0; side < 4; ++side)
             if (s->cpml_active[side]) cpml_side(s, side, 0);
+        for (int b = 0; b < n_tfsf; ++b) tfsf_h(s, &tfsf[b]);
         update_e(s);
         for (int side = 0; side < 4; ++side)
             if (s->cpml_active[side]) cpml_side(s, side, 1);
         for (int l = 0; l < n_lines; ++l) inject_line(s, &lines[l], k);
+        for (int b = 0; b < n_tfsf; ++b) tfsf_e(s, &tfsf[b], k);
         const int64_t n_step = step0 + k + 1;
         if (n_monitors > 0 && n_step % sample_interval == 0) {
             const int64_t sample = n_step / sample_interval;
@@ -229,6 +277,12 @@ int oracle_ez2d_advance(OracleEz2D *s, int64_t step0, int64_t n_steps, int32_t n
         }
     }
     return 0;
+}
+
+int oracle_ez2d_advance(OracleEz2D *s, int64_t step0, int64_t n_steps, int32_t n_lines, const OracleLine *lines,
+                        int32_t n_monitors, OracleFlux *monitors, int64_t sample_interval)
+{
+    return oracle_ez2d_advance_tfsf(s, step0, n_steps, n_lines, lines, n_monitors, monitors, sample_interval, 0, 0);
 }
 
 int oracle_ez2d_real_size(void) { return (int)sizeof(real); }

@@ -364,6 +364,18 @@ def _make_structs(real):
     return State, Line, Flux
 
 
+def _make_tfsf_struct(real):
+    R = ctypes.c_float if real == np.float32 else ctypes.c_double
+    P = ctypes.POINTER(R)
+
+    class Tfsf(ctypes.Structure):
+        _fields_ = [('x0', ctypes.c_int32), ('x1', ctypes.c_int32), ('y0', ctypes.c_int32), ('y1', ctypes.c_int32),
+                    ('aux_x0', ctypes.c_int32), ('aux_n', ctypes.c_int32), ('source_index', ctypes.c_int32),
+                    ('coef_h', R * 4), ('coef_e', R * 2), ('mur_lo', R), ('mur_hi', R), ('aux_ez', P), ('aux_hy', P),
+                    ('aux_coef_h', P), ('aux_coef_e', P), ('values', ctypes.POINTER(ctypes.c_float))]
+    return Tfsf
+
+
 _LIBS = {}
 
 
@@ -381,6 +393,13 @@ def load_library(real=np.float32):
         lib.oracle_ez2d_advance.argtypes = [ctypes.POINTER(State), ctypes.c_int64, ctypes.c_int64, ctypes.c_int32,
                                             ctypes.POINTER(Line), ctypes.c_int32, ctypes.POINTER(Flux),
                                             ctypes.c_int64]
+        Tfsf = _make_tfsf_struct(real)
+        lib.oracle_ez2d_advance_tfsf.restype = ctypes.c_int
+        lib.oracle_ez2d_advance_tfsf.argtypes = [ctypes.POINTER(State), ctypes.c_int64, ctypes.c_int64,
+                                                 ctypes.c_int32, ctypes.POINTER(Line), ctypes.c_int32,
+                                                 ctypes.POINTER(Flux), ctypes.c_int64, ctypes.c_int32,
+                                                 ctypes.POINTER(Tfsf)]
+        lib.tfsf_struct = Tfsf
         _LIBS[key] = (lib, State, Line, Flux)
     return _LIBS[key]
 
@@ -390,6 +409,10 @@ def _ptr(array, ctype):
 
 
 # ----------------------------------------------------------------------------------------------- the oracle run
+
+class TfsfBox:
+    """A TFSF plane-wave box of OracleEz2D.add_tfsf: cells, incident line, coefficients, temporal."""
+
 
 class OracleEz2D:
     """The whole 2D E_z path of one simulation on the CPU: geometry, sources and flux monitors as the reference's
@@ -409,6 +432,7 @@ class OracleEz2D:
         self.hy = np.zeros(shape, dtype=self.real)
         self.sources, self.monitors = [], []
         self.maps = []           # field-map DFT monitors (add_dft_monitor)
+        self.tfsf = []           # TFSF plane-wave boxes (add_tfsf)
         self.probes = []         # field probes (add_field_probe): [ix, iy, component, times, values]
         self.n_step = 0
         self.time = 0.0          # engine clock (host float64 accumulation)
@@ -493,6 +517,52 @@ class OracleEz2D:
         self.maps.append(mon)
         return mon
 
+    def add_tfsf(self, x0, y0, x1, y1, wavelength=None, frequency=None, bandwidth=0.5, amplitude=1.0,
+                 waveform='gaussian'):
+        """physics/em/__init__.py:475-490 with placement.tfsf_box_cells (placement.py:108-128) and the +x plane-wave box
+        of physics/em/sources.py:206-332 (_PlaneWaveBox, TFSFSource): 20 margin cells at the widths of cells x0 - 1 /
+        x1 around the box columns, soft source at aux cell 10 scaled by 2 S cos(kappa0/2) amplitude, Mur ends at the
+        numerical phase velocity of the carrier, side coefficients dt / (mu0 or eps0 x spacing) in float32."""
+        if waveform != 'gaussian':
+            raise ValueError('the oracle restates the Gaussian waveform only')
+        d = self.domain
+        f0 = float(frequency) if frequency is not None else C0 / float(wavelength)
+        x_lo, x_hi = sorted((x0, x1))
+        y_lo, y_hi = sorted((y0, y1))
+        ix0, ix1 = d.pos_to_cell_x(x_lo), d.pos_to_cell_x(x_hi) + 1
+        iy0, iy1 = d.pos_to_cell_y(y_lo), d.pos_to_cell_y(y_hi) + 1
+        dt = float(d.dt)
+        dx_cells = np.full(d.nx, float(DTYPE(d.dx)))
+        dy_cells = np.full(d.ny, float(DTYPE(d.dx)))
+        margin, source_index = 20, 10
+        up, down = float(dx_cells[ix0 - 1]), float(dx_cells[ix1])
+        widths = np.concatenate((np.full(margin, up), dx_cells[ix0:ix1], np.full(margin, down)))
+        face_spacings = 0.5 * (widths[:-1] + widths[1:])
+        half = 0.5 * (2.0 * np.pi * float(f0)) * dt
+
+        def line_terms(width):   # _aux_line_terms (sources.py:191-204)
+            courant = C0 * dt / width
+            sin_half_kappa = math.sin(half) / courant
+            cos_half_kappa = math.sqrt(1.0 - sin_half_kappa ** 2)
+            mur_courant = courant * cos_half_kappa / math.cos(half)
+            return courant, cos_half_kappa, (mur_courant - 1.0) / (mur_courant + 1.0)
+
+        courant, cos_half_kappa, mur_lo = line_terms(up)
+        _, _, mur_hi = line_terms(down)
+        spacings = [0.5 * float(w[i] + w[i + 1]) for w, i in ((dx_cells, ix0 - 1), (dx_cells, ix1 - 1),
+                                                              (dy_cells, iy0 - 1), (dy_cells, iy1 - 1))]
+        box = TfsfBox()
+        box.__dict__.update({'cells': (ix0, ix1, iy0, iy1), 'aux_x0': margin, 'source_index': source_index,
+               'temporal': GaussianPulse(f0, bandwidth), 'scale': 2.0 * courant * cos_half_kappa * float(amplitude),
+               'coef_h': [DTYPE(dt / (MU0 * sp)) for sp in spacings],
+               'coef_e': [DTYPE(dt / (EPS0 * float(dx_cells[ix0]))), DTYPE(dt / (EPS0 * float(dx_cells[ix1 - 1])))],
+               'mur': (DTYPE(mur_lo), DTYPE(mur_hi)),
+               'aux_coef_h': np.asarray(dt / (MU0 * face_spacings), dtype=DTYPE),
+               'aux_coef_e': np.asarray(dt / (EPS0 * widths), dtype=DTYPE),
+               'aux_ez': np.zeros(widths.size, dtype=DTYPE), 'aux_hy': np.zeros(widths.size, dtype=DTYPE)})
+        self.tfsf.append(box)
+        return box
+
     def add_field_probe(self, x, y, field_component=None):
         """physics/em/__init__.py:492-498 with placement.probe_cell (placement.py:29-45) and FieldProbe.record at
         t_full after every step (core/monitors.py:226-236, fdtd_2d_base.py:481-487): (times, values) lists."""
@@ -535,7 +605,7 @@ class OracleEz2D:
                                           float(d.dt))
             weight = np.asarray(2.0 * np.ones(src.hi - src.lo) / (float(ETA0) * src.normal_width), dtype=DTYPE)
             src.profile = (self.cb[line] * admittance * weight).astype(DTYPE)
-        self.sample_interval = dft_sample_interval(float(d.dt), self.sources,
+        self.sample_interval = dft_sample_interval(float(d.dt), self.sources + self.tfsf,
                                                    [m.frequencies for m in self.monitors + self.maps])
         for m in self.monitors + self.maps:
             m.sample_interval = self.sample_interval
@@ -634,6 +704,28 @@ class OracleEz2D:
             fluxes[i].first_sample, fluxes[i].n_samples = first_q, n_q
         return fluxes
 
+    def _tfsf_structs(self, Tfsf, R, n_steps):
+        """ctypes records of the TFSF boxes with this chunk's soft-source values FP32(scale * temporal(t + dt/2))."""
+        boxes = (Tfsf * max(1, len(self.tfsf)))()
+        dt = float(self.domain.dt)
+        for b, box in enumerate(self.tfsf):
+            t, values = self.time, np.empty(n_steps, dtype=np.float32)
+            for k in range(n_steps):
+                values[k] = DTYPE(box.scale * box.temporal(t + 0.5 * dt))
+                t = t + dt
+            box.values = values   # kept alive for the call
+            rec = boxes[b]
+            rec.x0, rec.x1, rec.y0, rec.y1 = box.cells
+            rec.aux_x0, rec.aux_n, rec.source_index = box.aux_x0, box.aux_ez.size, box.source_index
+            for i in range(4):
+                rec.coef_h[i] = float(box.coef_h[i])
+            rec.coef_e[0], rec.coef_e[1] = float(box.coef_e[0]), float(box.coef_e[1])
+            rec.mur_lo, rec.mur_hi = float(box.mur[0]), float(box.mur[1])
+            rec.aux_ez, rec.aux_hy = _ptr(box.aux_ez, R), _ptr(box.aux_hy, R)
+            rec.aux_coef_h, rec.aux_coef_e = _ptr(box.aux_coef_h, R), _ptr(box.aux_coef_e, R)
+            rec.values = _ptr(values, ctypes.c_float)
+        return boxes
+
     def _clock_after(self, n_steps, times_full):
         self.n_step += n_steps
         if n_steps:
@@ -676,8 +768,9 @@ class OracleEz2D:
         keep = self._cpml_state(st, R)
         lines = self._line_structs(Line, values)
         fluxes = self._flux_structs(Flux, phase_tables, first_q, n_q)
-        rc = lib.oracle_ez2d_advance(ctypes.byref(st), self.n_step, n_steps, len(self.sources), lines,
-                                     len(self.monitors), fluxes, self.sample_interval)
+        boxes = self._tfsf_structs(lib.tfsf_struct, R, n_steps)
+        rc = lib.oracle_ez2d_advance_tfsf(ctypes.byref(st), self.n_step, n_steps, len(self.sources), lines,
+                                          len(self.monitors), fluxes, self.sample_interval, len(self.tfsf), boxes)
         del keep
         if rc != 0:
             raise RuntimeError('oracle phase table does not cover a sample')

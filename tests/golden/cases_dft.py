@@ -21,6 +21,37 @@ CASES_DFT = [
         'probes': [[0.75e-6, 0.5e-6, 'ez'], [0.12e-6, 0.6e-6, 'hx'], [1.1e-6, 1.15e-6, 'hy']],
         'checkpoints': [250, 500],
     },
+    {   # +x plane wave (TFSF box) on a cylinder, all CPML: a map over the box and the scattered-field ring, a flux
+        # line and a probe outside the box (scattered field only)
+        'name': 'tfsf_cylinder',
+        'sim': {'size_x': 2.0e-6, 'size_y': 1.6e-6, 'dx': 25e-9, 'npml': 12, 'boundaries': 'pml'},
+        'ops': [
+            ['add_dielectric_circle', [1.0e-6, 0.8e-6, 0.25e-6], {'eps_r': 4.0}],
+            ['add_tfsf', [0.4e-6, 0.3e-6, 1.6e-6, 1.3e-6], {'wavelength': 700e-9, 'bandwidth': 0.5}],
+            ['add_flux_monitor', ['y', 1.8e-6, [0.2e-6, 1.4e-6]], {'wavelengths': [650e-9, 750e-9]}],
+        ],
+        'dft': [
+            [0.2e-6, 0.1e-6, 1.85e-6, 1.5e-6, [4.3e14], 2],
+        ],
+        'probes': [[1.8e-6, 0.8e-6, 'ez'], [1.0e-6, 0.35e-6, 'hy']],
+        'checkpoints': [300, 700],
+    },
+    {   # periodic y: a TFSF box beside a line source (no shared cell) and a slab inside the box
+        'name': 'tfsf_periodic_y',
+        'sim': {'size_x': 2.4e-6, 'size_y': 1.0e-6, 'dx': 25e-9, 'npml': 12, 'boundaries': 'periodic_y'},
+        'ops': [
+            ['add_dielectric_rectangle', [1.0e-6, 0.0, 1.2e-6, 1.0e-6], {'eps_r': 2.5}],
+            ['add_tfsf', [0.5e-6, 0.1e-6, 1.6e-6, 0.9e-6], {'frequency': 4.6e14, 'bandwidth': 0.6,
+                                                            'amplitude': 2.0}],
+            ['add_line_source', ['y', 2.0e-6], {'wavelength': 600e-9, 'bandwidth': 0.5, 'amplitude': 0.5}],
+            ['add_flux_monitor', ['y', 2.2e-6, [0.0, 1.0e-6]], {'wavelengths': [600e-9, 650e-9]}],
+        ],
+        'dft': [
+            [0.3e-6, 0.0, 1.9e-6, 0.99e-6, [4.6e14], 3],
+        ],
+        'probes': [[1.7e-6, 0.5e-6, 'ez']],
+        'checkpoints': [350, 600],
+    },
     {   # periodic y, CPML in x: a map crossing the slab and one touching the y edge of the grid
         'name': 'dft_periodic_y',
         'sim': {'size_x': 2.0e-6, 'size_y': 1.0e-6, 'dx': 25e-9, 'npml': 12, 'boundaries': 'periodic_y'},

@@ -1,0 +1,43 @@
+"""Host side of the TFSF plane-wave box (no GPU): the box checks, and the incident line's parameters (side and line
+coefficients, Mur ends, source scale) equal to the oracle's restatement of open_sol's _PlaneWaveBox, which the
+golden fixtures tests/golden/tfsf_*.npz pin to the reference."""
+import numpy as np
+import pytest
+
+from cases_dft import case
+from oracle.fdtd2d import OracleEz2D
+
+import opensol_b200 as ob
+
+
+def _boxes(spec):
+    sim = ob.Simulation(**spec['sim'], verbose=False)
+    o = OracleEz2D(**spec['sim'])
+    for method, args, kwargs in spec['ops']:
+        if method == 'add_tfsf':
+            return getattr(sim.em, method)(*args, **kwargs), getattr(o, method)(*args, **kwargs)
+    raise AssertionError('no TFSF box in the case')
+
+
+@pytest.mark.parametrize('name', ['tfsf_cylinder', 'tfsf_periodic_y'])
+def test_tfsf_parameters_match_oracle(name):
+    src, box = _boxes(case(name))
+    assert (src.x0, src.x1, src.y0, src.y1) == box.cells
+    assert src.aux_x0 == box.aux_x0 and src.AUX_SOURCE_INDEX == box.source_index
+    assert src.aux_cells == box.aux_ez.size
+    assert src.coef_h == tuple(box.coef_h) and src.coef_e == tuple(box.coef_e) and src.mur == box.mur
+    np.testing.assert_array_equal(src.aux_coef_h, box.aux_coef_h)
+    np.testing.assert_array_equal(src.aux_coef_e, box.aux_coef_e)
+    assert src.source_scale == box.scale
+    t = np.linspace(0.0, 4e-14, 7)
+    np.testing.assert_array_equal(src.values(t), [np.float32(box.scale * box.temporal(float(x))) for x in t])
+
+
+def test_tfsf_box_must_keep_a_scattered_ring_inside_the_window():
+    sim = ob.Simulation(size_x=1.0e-6, size_y=1.0e-6, dx=25e-9, npml=10, boundaries='pml', verbose=False)
+    with pytest.raises(ValueError, match='scattered-field'):
+        sim.em.add_tfsf(0.0, 0.2e-6, 0.5e-6, 0.8e-6, wavelength=700e-9)
+    hz = ob.Simulation(size_x=1.0e-6, size_y=1.0e-6, dx=25e-9, npml=10, boundaries='pml', polarization='hz',
+                       verbose=False)
+    with pytest.raises(NotImplementedError):
+        hz.em.add_tfsf(0.2e-6, 0.2e-6, 0.8e-6, 0.8e-6, wavelength=700e-9)
