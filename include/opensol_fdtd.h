@@ -173,6 +173,16 @@ int os_fdtd2d_add_tfsf(OsFdtd2D *h, int32_t x0, int32_t x1, int32_t y0, int32_t 
                        int32_t source_index, const float *coef_h, const float *coef_e, float mur_lo, float mur_hi,
                        const float *aux_coef_h, const float *aux_coef_e, int32_t *tfsf_id);
 
+/* Dispersive pole on the cell box [i0, i1) x [j0, j1) (FDTDEngine2D_Ez.add_drude / add_lorentz, fdtd_ez_2d.py:
+ * 123-163): kind 0 Drude (J += damping J + drive E^n before the E update, E -= cb J_total after it on the union box of
+ * the Drude poles), kind 1 Lorentz (dP += damping dP - restoring P + drive E^n, P += dP; E -= cb inv_dt dP), with the
+ * host's float32 ADE coefficients (DrudePole / LorentzPole.ade_coefficients) and drive = the box's cell mask times the
+ * drive coefficient ((i1 - i0) x (j1 - j0) floats); inv_dt = float32(1 / dt).  Poles act in add order, Drude before
+ * Lorentz, ahead of the line sources.  An engine with poles advances with the per-half-step kernels.  E_z engines only;
+ * not in batched advances or the adjoint.  At most 32. */
+int os_fdtd2d_add_pole(OsFdtd2D *h, int32_t kind, int32_t i0, int32_t i1, int32_t j0, int32_t j1, float damping,
+                       float restoring, const float *drive, float inv_dt, int32_t *pole_id);
+
 /* Field probe: one component (OS_EZ / OS_HX / OS_HY, or OS_HZ_* on an H_z handle) of cell (ix, iy) recorded after
  * every step from the current one on: FieldProbe.record at t_full (core/monitors.py:194-243, fdtd_2d_base.py:481-487).
  * At most 8.  An advance with probes runs one step per launch.  Not in batched advances; os_fdtd2d_advance_noalloc

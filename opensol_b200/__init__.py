@@ -12,9 +12,10 @@ from .monitors import DFTMonitor, FluxMonitor, dft_sample_interval
 from .physics import EMPhysics
 from .physics3d import EMPhysics3D
 from .simulation import MultiphysicsRunner, Simulation
+from .poles import DrudePole, LorentzPole
 from .sources import ContinuousWave, GaussianPulse, LineSource, RickerWavelet
 
-__all__ = ['BCType', 'BoundaryConfig', 'BoundaryConfig3D', 'Domain', 'Domain3D', 'EMPhysics3D', 'Grid2D', 'courant_time_step', 'DFTMonitor', 'FluxMonitor',
+__all__ = ['BCType', 'BoundaryConfig', 'BoundaryConfig3D', 'Domain', 'Domain3D', 'EMPhysics3D', 'Grid2D', 'courant_time_step', 'DFTMonitor', 'DrudePole', 'FluxMonitor', 'LorentzPole',
            'dft_sample_interval', 'EMPhysics', 'MultiphysicsRunner', 'Simulation', 'ContinuousWave',
            'GaussianPulse', 'LineSource', 'RickerWavelet']
 __version__ = '0.1.0'

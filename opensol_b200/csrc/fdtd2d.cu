@@ -53,6 +53,13 @@ struct Tfsf2D {
     DeviceArray<float> aux_ez, aux_hy, aux_coef_h, aux_coef_e;
 };
 
+// Drude (kind 0) or Lorentz (kind 1) pole on a cell box: drive (box, pole drive x cell mask) and its state.
+struct Pole2D {
+    int32_t kind, i0, i1, j0, j1;
+    float damping, restoring;
+    DeviceArray<float> drive, a, b;     // Drude: a = J; Lorentz: a = P, b = dP
+};
+
 struct DftMap2D {                       // field-map running DFT (DFTMonitor)
     int32_t x0, y0, ds, mx, my, nf;     // first sampled cell, stride, samples per axis, frequencies
     bool hz;                            // H_z engine: H_z, E_x, E_y maps (E at the cell centres), two phase tables
@@ -97,6 +104,10 @@ struct OsFdtd2D {
                                                        // chunk's phase table
     std::vector<std::unique_ptr<os::Tfsf2D>> tfsf;   // plane-wave boxes (E_z engines; their value rows follow the
                                                      // line sources' in a chunk's value table)
+    std::vector<std::unique_ptr<os::Pole2D>> poles;   // dispersive poles (E_z engines), in add order
+    os::DeviceArray<float> jz_total;      // (nx, ny) summed Drude J on drude_box
+    int32_t drude_box[4] = {0, 0, 0, 0};  // union box of the Drude poles (i0, i1, j0, j1); empty when i1 == i0
+    float inv_dt = 0.0f;                  // float32 1 / dt of the Lorentz corrections
     os::ProbeSet probes{};                // field probes (recorded after every step)
     os::DeviceArray<float> probe_rows;    // (OS_MAX_PROBES, probe_capacity) values by step
     int64_t probe_capacity = 0;           // rows per probe
@@ -158,6 +169,11 @@ static int zero_state(OsFdtd2D *h) {
         OS_CUDA(cudaMemsetAsync(t->aux_ez.ptr, 0, t->aux_ez.bytes(), h->stream));
         OS_CUDA(cudaMemsetAsync(t->aux_hy.ptr, 0, t->aux_hy.bytes(), h->stream));
     }
+    for (auto &q : h->poles) {
+        OS_CUDA(cudaMemsetAsync(q->a.ptr, 0, q->a.bytes(), h->stream));
+        if (q->b.ptr) OS_CUDA(cudaMemsetAsync(q->b.ptr, 0, q->b.bytes(), h->stream));
+    }
+    if (h->jz_total.ptr) OS_CUDA(cudaMemsetAsync(h->jz_total.ptr, 0, h->jz_total.bytes(), h->stream));
     for (int k = 0; k < h->probes.n; ++k) h->probes.start[k] = 0;   // rows recorded again from step 0
     h->n_step = 0;
     return OS_OK;
@@ -321,6 +337,8 @@ extern "C" int os_fdtd2d_destroy(OsFdtd2D *h) {
         for (auto &f : h->fluxes) give(f->e_acc), give(f->h_acc), give(f->stage);
         for (auto &d : h->maps) give(d->acc);
         for (auto &t : h->tfsf) give(t->aux_ez), give(t->aux_hy), give(t->aux_coef_h), give(t->aux_coef_e);
+        for (auto &q : h->poles) give(q->drive), give(q->a), give(q->b);
+        give(h->jz_total);
         give(h->probe_rows);
         give(h->err), give(h->line_values), give(h->phases);
         pool_events_done(ev);
@@ -1149,11 +1167,63 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
     return OS_OK;
 }
 
+// The poles' J / P updates from E^n (fdtd_ez_2d.py:318-345): the Drude total zeroed on the union box when several
+// Drude poles add into it, each Drude pole in add order, then each Lorentz pole.
+static int pole_updates(OsFdtd2D *h) {
+    const int ny = h->grid.ny, c = h->cur;
+    int n_drude = 0;
+    for (auto &q : h->poles) n_drude += q->kind == 0;
+    const int32_t *u = h->drude_box;
+    if (n_drude > 1)
+        OS_CUDA(cudaMemset2DAsync(h->jz_total.ptr + (size_t)u[0] * ny + u[2], (size_t)ny * sizeof(float), 0,
+                                  (size_t)(u[3] - u[2]) * sizeof(float), (size_t)(u[1] - u[0]), h->stream));
+    for (int pass = 0; pass < 2; ++pass)
+        for (auto &q : h->poles) {
+            if (q->kind != pass) continue;
+            const int64_t cells = (int64_t)(q->i1 - q->i0) * (q->j1 - q->j0);
+            const unsigned blocks = (unsigned)((cells + 255) / 256);
+            if (q->kind == 0)
+                ez2d_drude_j_kernel<<<blocks, 256, 0, h->stream>>>(h->ez[c].ptr, ny, q->i0, q->i1, q->j0, q->j1,
+                                                                   q->damping, q->drive.ptr, q->a.ptr,
+                                                                   h->jz_total.ptr, n_drude == 1);
+            else
+                ez2d_lorentz_p_kernel<<<blocks, 256, 0, h->stream>>>(h->ez[c].ptr, ny, q->i0, q->i1, q->j0, q->j1,
+                                                                     q->damping, q->restoring, q->drive.ptr, q->a.ptr,
+                                                                     q->b.ptr);
+            h->launches += 1;
+        }
+    OS_CUDA(cudaGetLastError());
+    return OS_OK;
+}
+
+// The E corrections after the E update (fdtd_ez_2d.py:347-358): Drude on the union box, then each Lorentz pole.
+static int pole_corrections(OsFdtd2D *h) {
+    const int ny = h->grid.ny, c = h->cur;
+    const int32_t *u = h->drude_box;
+    if (u[1] > u[0]) {
+        const int64_t cells = (int64_t)(u[1] - u[0]) * (u[3] - u[2]);
+        ez2d_pole_correct_kernel<<<(unsigned)((cells + 255) / 256), 256, 0, h->stream>>>(
+            h->ez[c].ptr, ny, u[0], u[1], u[2], u[3], h->cb.ptr, h->jz_total.ptr, nullptr, 0.0f);
+        h->launches += 1;
+    }
+    for (auto &q : h->poles) {
+        if (q->kind != 1) continue;
+        const int64_t cells = (int64_t)(q->i1 - q->i0) * (q->j1 - q->j0);
+        ez2d_pole_correct_kernel<<<(unsigned)((cells + 255) / 256), 256, 0, h->stream>>>(
+            h->ez[c].ptr, ny, q->i0, q->i1, q->j0, q->j1, h->cb.ptr, nullptr, q->b.ptr, h->inv_dt);
+        h->launches += 1;
+    }
+    OS_CUDA(cudaGetLastError());
+    return OS_OK;
+}
+
 // Per-half-step chunk (variant 0): H kernel, E kernel, DFT of sample steps; fields updated in place.
 static int advance_per_step(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples,
                             const float *values, const float *phase_table) {
     const int64_t m = h->sample_interval;
     Ez2DParams p = make_params(h);
+    Ez2DParams p_no_lines = p;
+    p_no_lines.n_lines = 0;
     const dim3 block(EZ2D_BLOCK_X, EZ2D_BLOCK_Y);
     const dim3 grid((unsigned)((h->grid.ny + block.x - 1) / block.x), (unsigned)((h->grid.nx + block.y - 1) / block.y));
     for (int64_t k = 0; k < n_steps; ++k) {
@@ -1168,7 +1238,17 @@ static int advance_per_step(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, 
                                                                                    t->aux_hy.ptr, t->aux_n);
             h->launches += 2;
         }
-        ez2d_e_kernel<<<grid, block, 0, h->stream>>>(p, values, n_steps, k);
+        if (h->poles.empty()) {
+            ez2d_e_kernel<<<grid, block, 0, h->stream>>>(p, values, n_steps, k);
+        } else {
+            // poles (fdtd_ez_2d.py:263-358): J / P from E^n, the E update (its sources held back), the pole
+            // corrections, then the line sources
+            OS_TRY(pole_updates(h));
+            ez2d_e_kernel<<<grid, block, 0, h->stream>>>(p_no_lines, values, n_steps, k);
+            OS_TRY(pole_corrections(h));
+            if (p.n_lines) ez2d_line_inject_kernel<<<grid, block, 0, h->stream>>>(p, values, n_steps, k);
+            h->launches += 1;
+        }
         for (size_t b = 0; b < h->tfsf.size(); ++b) {   // TFSFSource.inject_e at t + dt/2 (fdtd_ez_2d.py:92-99)
             Tfsf2D &t = *h->tfsf[b];
             ez2d_tfsf_e_kernel<<<(t.y1 - t.y0 + 255) / 256, 256, 0, h->stream>>>(
@@ -1445,9 +1525,9 @@ static int check_advance(const OsFdtd2D *h, const char *fn, int64_t n_steps, con
 static int run_chunk(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples, const float *values,
                      const float *phase_table) {
     OS_CUDA(cudaEventRecord(h->ev_start, h->stream));
-    // a TFSF box corrects H between the H and E updates of every step: the per-half-step kernels run it
+    // a TFSF box or a pole acts between the H and E updates of every step: the per-half-step kernels run them
     const int rc = h->polarization == 1 ? advance_hz(h, n_steps, first_sample, n_samples, values, phase_table)
-                   : (h->variant == 0 || !h->tfsf.empty())
+                   : (h->variant == 0 || !h->tfsf.empty() || !h->poles.empty())
                        ? advance_per_step(h, n_steps, first_sample, n_samples, values, phase_table)
                        : advance_blocked(h, n_steps, first_sample, n_samples, values, phase_table);
     if (rc != OS_OK) return rc;
@@ -1764,6 +1844,40 @@ extern "C" int os_fdtd2d_add_tfsf(OsFdtd2D *h, int32_t x0, int32_t x1, int32_t y
     return OS_OK;
 }
 
+extern "C" int os_fdtd2d_add_pole(OsFdtd2D *h, int32_t kind, int32_t i0, int32_t i1, int32_t j0, int32_t j1,
+                                  float damping, float restoring, const float *drive, float inv_dt, int32_t *pole_id) {
+    OS_TRY(require_ez(h, "os_fdtd2d_add_pole"));
+    OS_CHECK(drive, OS_ERR_INVALID, "os_fdtd2d_add_pole: null drive");
+    OS_CHECK(kind == 0 || kind == 1, OS_ERR_INVALID, "pole kind must be 0 (Drude) or 1 (Lorentz), got %d", kind);
+    OS_CHECK(0 <= i0 && i0 < i1 && i1 <= h->grid.nx && 0 <= j0 && j0 < j1 && j1 <= h->grid.ny, OS_ERR_INVALID,
+             "pole box [%d, %d) x [%d, %d) outside the %d x %d grid", i0, i1, j0, j1, h->grid.nx, h->grid.ny);
+    OS_CHECK(h->poles.size() < 32, OS_ERR_INVALID, "at most 32 poles per engine");
+    OS_TRY(bind_device(h));
+    std::unique_ptr<Pole2D> q(new Pole2D());
+    q->kind = kind, q->i0 = i0, q->i1 = i1, q->j0 = j0, q->j1 = j1;
+    q->damping = damping, q->restoring = restoring;
+    const size_t n = (size_t)(i1 - i0) * (size_t)(j1 - j0);
+    OS_TRY(upload(q->drive, drive, n, h->stream));
+    OS_TRY(q->a.alloc(n));
+    OS_CUDA(cudaMemsetAsync(q->a.ptr, 0, q->a.bytes(), h->stream));
+    if (kind == 1) {
+        OS_TRY(q->b.alloc(n));
+        OS_CUDA(cudaMemsetAsync(q->b.ptr, 0, q->b.bytes(), h->stream));
+        h->inv_dt = inv_dt;
+    } else {
+        if (!h->jz_total.ptr) {
+            OS_TRY(h->jz_total.alloc(cells(h)));
+            OS_CUDA(cudaMemsetAsync(h->jz_total.ptr, 0, h->jz_total.bytes(), h->stream));
+        }
+        int32_t *u = h->drude_box;
+        if (u[1] == u[0]) u[0] = i0, u[1] = i1, u[2] = j0, u[3] = j1;
+        else u[0] = std::min(u[0], i0), u[1] = std::max(u[1], i1), u[2] = std::min(u[2], j0), u[3] = std::max(u[3], j1);
+    }
+    if (pole_id) *pole_id = (int32_t)h->poles.size();
+    h->poles.push_back(std::move(q));
+    return OS_OK;
+}
+
 extern "C" int os_fdtd2d_add_probe(OsFdtd2D *h, int32_t ix, int32_t iy, int32_t component, int32_t *probe_id) {
     OS_CHECK(h, OS_ERR_INVALID, "os_fdtd2d_add_probe: null handle");
     OS_CHECK(0 <= ix && ix < h->grid.nx && 0 <= iy && iy < h->grid.ny, OS_ERR_INVALID,
@@ -2049,9 +2163,9 @@ extern "C" int os_fdtd2d_batch_advance(OsFdtd2DBatch *b, OsFdtd2D *const *handle
                  "os_fdtd2d_batch_advance: job %d is not on the batch stream (os_fdtd2d_set_stream with "
                  "os_fdtd2d_batch_stream)", q);
         OS_CHECK(!h->profiling, OS_ERR_STATE, "os_fdtd2d_batch_advance: job %d has profiling on", q);
-        OS_CHECK(h->maps.empty() && h->probes.n == 0 && h->tfsf.empty(), OS_ERR_STATE,
-                 "os_fdtd2d_batch_advance: job %d has field-map monitors, field probes or a TFSF box (advance it "
-                 "with os_fdtd2d_advance)", q);
+        OS_CHECK(h->maps.empty() && h->probes.n == 0 && h->tfsf.empty() && h->poles.empty(), OS_ERR_STATE,
+                 "os_fdtd2d_batch_advance: job %d has field-map monitors, field probes, a TFSF box or poles (advance "
+                 "it with os_fdtd2d_advance)", q);
     }
     OS_CUDA(cudaSetDevice(b->device));
     // every job's own tables, in its own buffers, as os_fdtd2d_advance uploads them
@@ -2366,7 +2480,8 @@ extern "C" int os_fdtd2d_adjoint_create(OsFdtd2D *h, int32_t box_i0, int32_t box
     OS_CHECK(h && out, OS_ERR_INVALID, "os_fdtd2d_adjoint_create: null argument");
     OS_TRY(require_ez(h, "os_fdtd2d_adjoint_create"));
     *out = nullptr;
-    OS_CHECK(h->tfsf.empty(), OS_ERR_STATE, "os_fdtd2d_adjoint_create: the adjoint does not transpose a TFSF box");
+    OS_CHECK(h->tfsf.empty() && h->poles.empty(), OS_ERR_STATE,
+             "os_fdtd2d_adjoint_create: the adjoint does not transpose a TFSF box or a dispersive pole");
     OS_CHECK(h->has_cb && h->has_spacings, OS_ERR_STATE, "os_fdtd2d_adjoint_create: coefficients and spacings first");
     OS_CHECK(0 <= box_i0 && box_i0 < box_i1 && box_i1 <= h->grid.nx && 0 <= box_j0 && box_j0 < box_j1 &&
                  box_j1 <= h->grid.ny, OS_ERR_INVALID, "os_fdtd2d_adjoint_create: design box outside the grid");

@@ -231,6 +231,73 @@ __global__ void hz2d_dft_map_kernel(const float *__restrict__ hz, const float *_
     }
 }
 
+// Soft line sources on E_z after the E update, as the E kernel's own loop adds them: for the per-step path of an
+// engine whose pole corrections must come between the E update and the sources (fdtd_ez_2d.py:90-99).
+__global__ void ez2d_line_inject_kernel(const Ez2DParams p, const float *__restrict__ line_values, int64_t n_steps,
+                                        int64_t k_step) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= p.nx || j >= p.ny) return;
+    const size_t idx = (size_t)i * p.ny + j;
+    float v = p.ez[idx];
+    bool hit = false;
+    for (int l = 0; l < p.n_lines; ++l) {
+        const LineSrcDev &s = p.lines[l];
+        const int along = s.axis == 0 ? i : j, across = s.axis == 0 ? j : i;
+        if (across == s.position && along >= s.lo && along < s.hi) {
+            const float value = line_values[(size_t)l * n_steps + k_step];
+            if (value != 0.0f) {
+                v += value * s.profile[along - s.lo];
+                hit = true;
+            }
+        }
+    }
+    if (hit) p.ez[idx] = v;
+}
+
+// ---- dispersive poles on a cell box [i0, i1) x [j0, j1) (fdtd_ez_2d_kernels.py:190-260, fdtd_ez_2d.py:318-358);
+// box arrays (i1 - i0, j1 - j0), grid arrays (nx, ny).  drive = the pole's drive coefficient times the cell mask, so
+// cells outside the material keep J = 0 / P = 0.
+// Drude J^{n+1/2} = J + (damping J + drive E^n), then jz_total = J (store: one pole) or jz_total += J.
+__global__ void ez2d_drude_j_kernel(const float *__restrict__ ez, int ny, int i0, int i1, int j0, int j1,
+                                    float damping, const float *__restrict__ drive, float *__restrict__ jz,
+                                    float *__restrict__ jz_total, int store) {
+    const int w = j1 - j0;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)(i1 - i0) * w) return;
+    const int i = i0 + (int)(t / w), j = j0 + (int)(t % w);
+    const size_t g = (size_t)i * ny + j;
+    const float jn = jz[t] + (damping * jz[t] + drive[t] * ez[g]);
+    jz[t] = jn;
+    jz_total[g] = store ? jn : jz_total[g] + jn;
+}
+
+// Lorentz in velocity form: dP += damping dP - restoring P^n + drive E^n, then P += dP.
+__global__ void ez2d_lorentz_p_kernel(const float *__restrict__ ez, int ny, int i0, int i1, int j0, int j1,
+                                      float damping, float restoring, const float *__restrict__ drive,
+                                      float *__restrict__ pz, float *__restrict__ dpz) {
+    const int w = j1 - j0;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)(i1 - i0) * w) return;
+    const size_t g = (size_t)(i0 + (int)(t / w)) * ny + (j0 + (int)(t % w));
+    const float dp = dpz[t] + (damping * dpz[t] - restoring * pz[t] + drive[t] * ez[g]);
+    dpz[t] = dp;
+    pz[t] = pz[t] + dp;
+}
+
+// E corrections after the E update: Drude E -= cb jz_total on the union box (dp NULL), Lorentz E -= (cb inv_dt) dP
+// on the pole's box (dp = its box array).
+__global__ void ez2d_pole_correct_kernel(float *__restrict__ ez, int ny, int i0, int i1, int j0, int j1,
+                                         const float *__restrict__ cb, const float *__restrict__ jz_total,
+                                         const float *__restrict__ dp, float inv_dt) {
+    const int w = j1 - j0;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)(i1 - i0) * w) return;
+    const size_t g = (size_t)(i0 + (int)(t / w)) * ny + (j0 + (int)(t % w));
+    if (dp) ez[g] = ez[g] - cb[g] * inv_dt * dp[t];
+    else ez[g] = ez[g] - cb[g] * jz_total[g];
+}
+
 // ---- +x plane-wave TFSF box (TFSFSource, physics/em/sources.py:35-52,72-186,334-350)
 // Scattered / total-field H corrections after the H update: H_y on rows x0 - 1 (-) and x1 - 1 (+) from the incident
 // E_z at the box's first / last column, H_x on columns y0 - 1 (+) and y1 - 1 (-) from the incident E_z of each row.

@@ -44,6 +44,7 @@ class FDTDEngine2D_Ez:
         self._handle = None
         self._lines = []          # LineSource objects in add order
         self._tfsf = []           # TFSFSource boxes in add order (value rows after the line sources')
+        self._poles = []          # (pole, box, cropped mask) in add order
         self._line_ids = {}       # id(source) -> native id
         self._profiles_sent = {}  # id(source) -> profile array last uploaded
         self._monitors = []       # FluxMonitor objects in add order
@@ -101,6 +102,10 @@ class FDTDEngine2D_Ez:
         self._monitors.append(monitor)
         monitor._reader = lambda m=monitor: self.read_flux_spectra(m)
 
+    def attach_pole(self, pole, box, cropped_mask):
+        """Register a Drude / Lorentz pole on a cell box (cropped_mask: its cells); created at the next sync."""
+        self._poles.append((pole, box, np.asarray(cropped_mask, dtype=bool)))
+
     def attach_tfsf(self, source):
         """Register a TFSF plane-wave box; it is created on the device at the next sync."""
         self._tfsf.append(source)
@@ -148,6 +153,18 @@ class FDTDEngine2D_Ez:
                 _native.check(lib.os_fdtd2d_add_flux_line(h, normal, monitor.position, monitor.span[0],
                                                           monitor.span[1], monitor.n_freqs, ctypes.byref(mid)))
                 self._monitor_ids[id(monitor)] = mid.value
+        for entry in self._poles:
+            if id(entry) not in self._monitor_ids:
+                pole, box, cropped = entry
+                coefficients = pole.ade_coefficients(float(self.dt))
+                kind = 0 if len(coefficients) == 2 else 1
+                damping, restoring, drive = ((coefficients[0], 0.0, coefficients[1]) if kind == 0 else coefficients)
+                drive_box = np.ascontiguousarray(cropped.astype(DTYPE) * DTYPE(drive))
+                pid = ctypes.c_int32()
+                _native.check(lib.os_fdtd2d_add_pole(h, kind, box[0].start, box[0].stop, box[1].start, box[1].stop,
+                                                     float(damping), float(restoring), _native.fptr(drive_box),
+                                                     float(DTYPE(1.0 / float(self.dt))), ctypes.byref(pid)))
+                self._monitor_ids[id(entry)] = pid.value
         for source in self._tfsf:
             if id(source) not in self._monitor_ids:
                 tid = ctypes.c_int32()

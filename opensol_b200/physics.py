@@ -16,6 +16,7 @@ import numpy as np
 from .boundaries import BoundaryConfig, inverse_spacings
 from .constants import C0, DTYPE
 from .engine2d import FDTDEngine2D_Ez, FDTDEngine2D_Hz
+from .poles import DrudePole, LorentzPole, bounding_box
 from .monitors import PROBE_COMPONENTS, DFTMonitor, FieldProbe, FluxMonitor, dft_sample_interval, resolve_frequencies
 from .sources import (LineSource, TFSFSource, calibrate_line_source, calibrate_tangential_sheet, carrier_angular_frequency,
                       make_temporal, resolve_frequency)
@@ -59,6 +60,7 @@ class EMPhysics:
             self.engine = FDTDEngine2D_Ez(domain, bc, device=device)
         self.sources = []
         self.monitors = []
+        self.dispersive_regions = []   # (pole, box, cropped bool mask) in add order
         self._calibrations = []       # (source, omega, normal width)
         self._calibration_dirty = False
         self._finalized = False
@@ -146,13 +148,18 @@ class EMPhysics:
         else:
             eps = np.minimum(materials.array('eps_xx'), materials.array('eps_yy'))
         mu = materials.get('mu_r')
-        # uniform grid: the requirement is one value; the worst cell is the smallest eps mu
+        # uniform grid: the light term is one value; the poles add mu_r x their step term on their cells
         requirement = required_x[0] + required_y[0]
+        if self.dispersive_regions:
+            pole_term = np.zeros(eps.shape, dtype=DTYPE)
+            for pole, box, cropped in self.dispersive_regions:
+                pole_term[box] += cropped.astype(DTYPE) * DTYPE(pole.step_term(dt))
+            requirement = requirement + (pole_term if mu is None else mu * pole_term)
         product = eps if mu is None else eps * mu
-        worst = float(product.min() / requirement)
+        worst = float((product / requirement).min())
         if worst >= 1.0 - 1e-6:
             return
-        ix, iy = np.unravel_index(int(np.argmin(product)), product.shape)
+        ix, iy = np.unravel_index(int(np.argmin(product / requirement)), product.shape)
         x_centers, y_centers = self.domain.cell_centers()
         required = light * (1.0 / dx_cells[ix] ** 2 + 1.0 / dy_cells[iy] ** 2)
         stable = math.floor(float(self.domain.grid.courant) * math.sqrt(max(worst, 0.0)) * 1e3) / 1e3
@@ -164,7 +171,8 @@ class EMPhysics:
         dt = float(self.domain.grid.dt)
         for source, omega, width in self._calibrations:
             if self.polarization == 'ez':
-                source.profile = calibrate_line_source(source, self.domain.materials, omega, width, dt)
+                source.profile = calibrate_line_source(source, self.domain.materials, omega, width, dt,
+                                                       self.dispersive_regions)
             else:
                 normal = 1 if source.axis == 'x' else 0
                 source.profile = calibrate_tangential_sheet(
@@ -172,6 +180,40 @@ class EMPhysics:
                     self.engine.shares_y if normal == 1 else self.engine.shares_x,
                     self.domain.kernel_widths()[normal])
         self._calibration_dirty = False
+
+    # --- dispersive poles (E_z) ---------------------------------------------------------------------------
+    def add_drude_rectangle(self, x0, y0, x1, y1, drude):
+        """Drude medium on the cells of the rectangle, its eps_inf written as their eps_r
+        (physics/em/__init__.py:329-340)."""
+        self._add_pole(drude, self.domain.rect_mask(x0, y0, x1, y1), set_background=True)
+
+    def add_drude_circle(self, cx, cy, radius, drude):
+        self._add_pole(drude, self.domain.circle_mask(cx, cy, radius), set_background=True)
+
+    def add_dispersive(self, pole, mask, weights=None):
+        """Drude or Lorentz pole on a cell mask (a full-grid bool array or a domain mask), the permittivity arrays
+        kept as the background (physics/em/__init__.py:342-361); cut-cell weights are not built."""
+        if weights is not None:
+            raise NotImplementedError('conformal pole weights are not built')
+        if not isinstance(pole, (DrudePole, LorentzPole)):
+            raise TypeError(f"add_dispersive needs a DrudePole or LorentzPole, got {type(pole).__name__}")
+        self._add_pole(pole, mask, set_background=False)
+
+    def _add_pole(self, pole, mask, set_background):
+        if self.polarization != 'ez':
+            raise NotImplementedError('dispersive poles are built for the E_z engine only')
+        grid = self.domain.grid
+        full = mask.full((grid.nx, grid.ny)) if hasattr(mask, 'full') else np.asarray(mask, dtype=bool)
+        if full.shape != (grid.nx, grid.ny):
+            raise ValueError(f"Pole mask must have the grid shape {(grid.nx, grid.ny)}, got {full.shape}")
+        box = bounding_box(full)
+        if box is not None:
+            self.engine.attach_pole(pole, box, full[box])
+            self.dispersive_regions.append((pole, box, full[box]))
+        if set_background:
+            self.domain.materials.assign('eps_r', full, pole.eps_inf)
+            self.materials_changed(('eps_r',))
+        self._calibration_dirty = True
 
     # --- material helpers --------------------------------------------------------------------------------
     def add_dielectric_rectangle(self, x0, y0, x1, y1, eps_r, sigma_e=0.0):

@@ -1,0 +1,82 @@
+"""Dispersive poles of the 2D E_z engine: Drude and Lorentz media (physics/em/materials.py:132-190).
+
+The auxiliary-differential-equation coefficients are computed in float64 and rounded to float32 as open_sol rounds
+them; the device steps them in velocity form (J += damping J + drive E, or dP += damping dP - restoring P + drive E,
+P += dP).  susceptibility() gives the continuous-time chi(omega) the sheet-source calibration adds on pole cells.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .constants import DTYPE, EPS0
+
+
+def _scalar_or_array(value):
+    return complex(value) if np.ndim(value) == 0 else value
+
+
+class DrudePole:
+    """dJ/dt + gamma J = eps0 omega_p^2 E, above a background eps_inf (materials.py:132-157)."""
+
+    def __init__(self, omega_p: float, gamma: float, eps_inf: float = 1.0):
+        self.omega_p = DTYPE(omega_p)
+        self.gamma = DTYPE(gamma)
+        self.eps_inf = DTYPE(eps_inf)
+
+    def ade_coefficients(self, dt):
+        """(damping, drive) float32: damping = -gamma dt / (1 + gamma dt / 2), drive = eps0 wp^2 dt / (1 + gamma dt /
+        2)."""
+        dt = float(dt)
+        gamma, wp = float(self.gamma), float(self.omega_p)
+        denom = 1.0 + gamma * dt / 2.0
+        return DTYPE(-gamma * dt / denom), DTYPE((EPS0 * wp ** 2 * dt) / denom)
+
+    def susceptibility(self, omega):
+        omega = np.asarray(omega, dtype=np.float64)
+        wp, gamma = float(self.omega_p), float(self.gamma)
+        return _scalar_or_array(-wp ** 2 / (omega ** 2 - 1j * gamma * omega))
+
+    def step_term(self, dt):
+        """Leap-frog stability term (omega_p dt)^2 / 4 (materials.py:199-211)."""
+        return (float(self.omega_p) * dt) ** 2 / 4.0
+
+
+class LorentzPole:
+    """P'' + gamma P' + omega_0^2 P = eps0 delta_eps omega_0^2 E (materials.py:160-190)."""
+
+    def __init__(self, delta_eps: float, omega_0: float, gamma: float):
+        self.delta_eps = DTYPE(delta_eps)
+        self.omega_0 = DTYPE(omega_0)
+        self.gamma = DTYPE(gamma)
+
+    def ade_coefficients(self, dt):
+        """(damping, restoring, drive) float32 of the velocity-form step."""
+        dt = float(dt)
+        w0, g, de = float(self.omega_0), float(self.gamma), float(self.delta_eps)
+        denom = 1.0 + g * dt / 2.0
+        return (DTYPE(-g * dt / denom), DTYPE(w0 ** 2 * dt ** 2 / denom),
+                DTYPE(EPS0 * de * w0 ** 2 * dt ** 2 / denom))
+
+    def susceptibility(self, omega):
+        omega = np.asarray(omega, dtype=np.float64)
+        w0, gamma, de = float(self.omega_0), float(self.gamma), float(self.delta_eps)
+        return _scalar_or_array(de * w0 ** 2 / (w0 ** 2 - omega ** 2 + 1j * gamma * omega))
+
+    def step_term(self, dt):
+        """delta_eps (omega_0 dt)^2 / (4 - (omega_0 dt)^2); ValueError when omega_0 dt >= 2."""
+        r2 = (float(self.omega_0) * dt) ** 2
+        if r2 >= 4.0:
+            raise ValueError(f'Lorentz pole: omega_0 dt = {math.sqrt(r2):.4g} >= 2, so the Lorentz update is unstable; '
+                             f'lower courant_factor or refine the mesh')
+        return float(self.delta_eps) * r2 / (4.0 - r2)
+
+
+def bounding_box(mask):
+    """(slice, slice) bounding the set cells of a full-grid bool mask, None when none is set."""
+    rows = np.flatnonzero(mask.any(axis=1))
+    if rows.size == 0:
+        return None
+    cols = np.flatnonzero(mask.any(axis=0))
+    return slice(int(rows[0]), int(rows[-1]) + 1), slice(int(cols[0]), int(cols[-1]) + 1)

@@ -150,9 +150,10 @@ def e_coefficients_host(eps_r, sigma_e, dt):
     return (1.0 - k) / denom, (dt / eps) / denom
 
 
-def calibrate_line_source(source, materials, omega, normal_width, dt):
+def calibrate_line_source(source, materials, omega, normal_width, dt, dispersive_regions=()):
     """float32 profile of an E_z sheet current (SheetCurrentCalibration.apply for a LineSource,
-    physics/em/sources.py:582-602): cb * admittance * 2 / (eta0 w_perp) on the line cells."""
+    physics/em/sources.py:582-602): cb * admittance * 2 / (eta0 w_perp) on the line cells; the line's eps(omega)
+    includes the susceptibility of every pole region it crosses (_line_cell_permittivity, :401-427)."""
     lo, hi = source.span
     if source.axis == 'x':
         line = (slice(lo, hi), source.position)
@@ -168,6 +169,15 @@ def calibrate_line_source(source, materials, omega, normal_width, dt):
     eps_line, sigma_line = cells('eps_r'), cells('sigma_e')
     _, cb_line = e_coefficients_host(eps_line, sigma_line, dt)
     line_eps = eps_line.astype(np.complex128) - 1j * sigma_line.astype(np.float64) / (omega * EPS0)
+    for pole, box, cropped in dispersive_regions:
+        chi = complex(pole.susceptibility(omega))
+        along_box, normal_box = (box[0], box[1]) if source.axis == 'x' else (box[1], box[0])
+        start, stop = max(lo, along_box.start), min(hi, along_box.stop)
+        if not (normal_box.start <= source.position < normal_box.stop and start < stop):
+            continue
+        along, normal = slice(start - along_box.start, stop - along_box.start), source.position - normal_box.start
+        mask_line = cropped[along, normal] if source.axis == 'x' else cropped[normal, along]
+        line_eps[start - lo:stop - lo] += chi * mask_line
     admittance = sheet_admittance(line_eps, cells('mu_r'), cells('sigma_m'), omega, normal_width, dt)
     weight = np.asarray(2.0 * np.ones(hi - lo) / (float(ETA0) * normal_width), dtype=DTYPE)
     return (cb_line * admittance * weight).astype(DTYPE)

@@ -13,6 +13,9 @@
  *                             t + dt/2, n_step += 1, monitors every sample_interval steps: fdtd_2d_base.py:470-488)
  *   - soft line source        open_sol/core/sources.py:146-154,221-229 (target += scale * profile, skipped at 0)
  *   - line DFT accumulation   open_sol/physics/em/monitors.py:45-46 (complex128 += complex64 phase * (double)f)
+ *   - dispersive poles        open_sol/physics/em/solvers/fdtd_ez_2d_kernels.py:190-260 (host twins), order of
+ *                             fdtd_ez_2d.py:263-358: Drude J / Lorentz P from E^n before the E update (Drude poles
+ *                             first, each kind in add order), the E corrections after the E update and its CPML
  *   - TFSF plane-wave box     open_sol/physics/em/sources.py:35-52 (host twins of the side corrections and the 1D
  *                             incident line), 334-350 (inject_h after the H update, inject_e after the E update); the
  *                             E-side corrections run after the line sources (open_sol: sources in add order, which
@@ -75,7 +78,67 @@ typedef struct {
     const float *values;                      /* (n_steps,) float32 soft-source value of each step of the chunk */
 } OracleTfsf;
 
+typedef struct {
+    int32_t kind;                             /* 0 Drude, 1 Lorentz */
+    int32_t i0, i1, j0, j1;                   /* cell box */
+    real damping, restoring;
+    const real *drive;                        /* (box) drive coefficient x cell mask */
+    real *a, *b;                              /* Drude: a = J; Lorentz: a = P, b = dP (box) */
+} OraclePole;
+
 static inline real coef_or(const real *array, size_t idx, real uniform) { return array ? array[idx] : uniform; }
+
+/* _pole_updates (fdtd_ez_2d.py:318-345) from E^n; jz_total is zeroed on drude_box first when several Drude poles
+ * add into it (one pole stores J). */
+static void poles_update(const OracleEz2D *s, int32_t n_poles, const OraclePole *poles, real *jz_total,
+                         const int32_t *drude_box)
+{
+    const size_t ny = (size_t)s->ny;
+    int n_drude = 0;
+    for (int q = 0; q < n_poles; ++q) n_drude += poles[q].kind == 0;
+    if (n_drude > 1)
+        for (int i = drude_box[0]; i < drude_box[1]; ++i)
+            for (int j = drude_box[2]; j < drude_box[3]; ++j) jz_total[(size_t)i * ny + j] = 0;
+    for (int pass = 0; pass < 2; ++pass)
+        for (int q = 0; q < n_poles; ++q) {
+            const OraclePole *p = &poles[q];
+            if (p->kind != pass) continue;
+            const int w = p->j1 - p->j0;
+            for (int i = p->i0; i < p->i1; ++i)
+                for (int j = p->j0; j < p->j1; ++j) {
+                    const size_t t = (size_t)(i - p->i0) * w + (j - p->j0), g = (size_t)i * ny + j;
+                    if (p->kind == 0) {
+                        p->a[t] += p->damping * p->a[t] + p->drive[t] * s->ez[g];
+                        jz_total[g] = n_drude == 1 ? p->a[t] : jz_total[g] + p->a[t];
+                    } else {
+                        p->b[t] += p->damping * p->b[t] - p->restoring * p->a[t] + p->drive[t] * s->ez[g];
+                        p->a[t] += p->b[t];
+                    }
+                }
+        }
+}
+
+/* _pole_corrections (fdtd_ez_2d.py:347-358). */
+static void poles_correct(const OracleEz2D *s, int32_t n_poles, const OraclePole *poles, const real *jz_total,
+                          const int32_t *drude_box, real inv_dt)
+{
+    const size_t ny = (size_t)s->ny;
+    for (int i = drude_box[0]; i < drude_box[1]; ++i)
+        for (int j = drude_box[2]; j < drude_box[3]; ++j) {
+            const size_t g = (size_t)i * ny + j;
+            s->ez[g] -= s->cb[g] * jz_total[g];
+        }
+    for (int q = 0; q < n_poles; ++q) {
+        const OraclePole *p = &poles[q];
+        if (p->kind != 1) continue;
+        const int w = p->j1 - p->j0;
+        for (int i = p->i0; i < p->i1; ++i)
+            for (int j = p->j0; j < p->j1; ++j) {
+                const size_t t = (size_t)(i - p->i0) * w + (j - p->j0), g = (size_t)i * ny + j;
+                s->ez[g] -= s->cb[g] * inv_dt * p->b[t];
+            }
+    }
+}
 
 /* TFSFSource.inject_h: H_y / H_x side corrections from the incident E_z, then the incident H update. */
 static void tfsf_h(const OracleEz2D *s, const OracleTfsf *t)
@@ -252,18 +315,21 @@ static void accumulate_flux(const OracleEz2D *s, OracleFlux *m, int64_t sample)
 /* Advance n_steps steps starting after engine step `step0` (the engine's n_step before the chunk).  Line source
  * values are indexed by the step within the chunk; monitors sample when (step0 + k + 1) % sample_interval == 0.
  * Returns 0, or -1 when a monitor's phase table does not cover a sample. */
-int oracle_ez2d_advance_tfsf(OracleEz2D *s, int64_t step0, int64_t n_steps, int32_t n_lines, const OracleLine *lines,
+int oracle_ez2d_advance_full(OracleEz2D *s, int64_t step0, int64_t n_steps, int32_t n_lines, const OracleLine *lines,
                              int32_t n_monitors, OracleFlux *monitors, int64_t sample_interval, int32_t n_tfsf,
-                             const OracleTfsf *tfsf)
+                             const OracleTfsf *tfsf, int32_t n_poles, const OraclePole *poles, real *jz_total,
+                             const int32_t *drude_box, real inv_dt)
 {
     for (int64_t k = 0; k < n_steps; ++k) {
         update_h(s);
         for (int side = 0; side < 4; ++side)
             if (s->cpml_active[side]) cpml_side(s, side, 0);
         for (int b = 0; b < n_tfsf; ++b) tfsf_h(s, &tfsf[b]);
+        if (n_poles) poles_update(s, n_poles, poles, jz_total, drude_box);
         update_e(s);
         for (int side = 0; side < 4; ++side)
             if (s->cpml_active[side]) cpml_side(s, side, 1);
+        if (n_poles) poles_correct(s, n_poles, poles, jz_total, drude_box, inv_dt);
         for (int l = 0; l < n_lines; ++l) inject_line(s, &lines[l], k);
         for (int b = 0; b < n_tfsf; ++b) tfsf_e(s, &tfsf[b], k);
         const int64_t n_step = step0 + k + 1;
@@ -277,6 +343,15 @@ int oracle_ez2d_advance_tfsf(OracleEz2D *s, int64_t step0, int64_t n_steps, int3
         }
     }
     return 0;
+}
+
+int oracle_ez2d_advance_tfsf(OracleEz2D *s, int64_t step0, int64_t n_steps, int32_t n_lines, const OracleLine *lines,
+                             int32_t n_monitors, OracleFlux *monitors, int64_t sample_interval, int32_t n_tfsf,
+                             const OracleTfsf *tfsf)
+{
+    const int32_t no_box[4] = {0, 0, 0, 0};
+    return oracle_ez2d_advance_full(s, step0, n_steps, n_lines, lines, n_monitors, monitors, sample_interval, n_tfsf,
+                                    tfsf, 0, 0, 0, no_box, 0);
 }
 
 int oracle_ez2d_advance(OracleEz2D *s, int64_t step0, int64_t n_steps, int32_t n_lines, const OracleLine *lines,

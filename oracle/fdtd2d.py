@@ -139,6 +139,60 @@ def paint_circle(domain, array, cx, cy, radius, value):
     np.copyto(array[sx, sy], DTYPE(value), where=mask)
 
 
+def rect_mask(domain, x0, y0, x1, y1):
+    """Full-grid bool Domain.rect_mask (core/domain.py:255-260)."""
+    mask = np.zeros((domain.nx, domain.ny), dtype=bool)
+    X, Y = domain.centers_f32
+    x_min, x_max = min(x0, x1), max(x0, x1)
+    y_min, y_max = min(y0, y1), max(y0, y1)
+    sx, sy = _bbox_slices(X, x_min, x_max), _bbox_slices(Y, y_min, y_max)
+    Xb, Yb = X[sx][:, None], Y[sy][None, :]
+    mask[sx, sy] = (Xb >= x_min) & (Xb < x_max) & (Yb >= y_min) & (Yb < y_max)
+    return mask
+
+
+def circle_mask(domain, cx, cy, radius):
+    """Full-grid bool Domain.circle_mask (core/domain.py:262-267)."""
+    mask = np.zeros((domain.nx, domain.ny), dtype=bool)
+    X, Y = domain.centers_f32
+    sx, sy = _bbox_slices(X, cx - radius, cx + radius), _bbox_slices(Y, cy - radius, cy + radius)
+    Xb, Yb = X[sx][:, None], Y[sy][None, :]
+    mask[sx, sy] = (Xb - cx) ** 2 + (Yb - cy) ** 2 <= radius ** 2
+    return mask
+
+
+class OracleDrude:
+    """DrudePole (physics/em/materials.py:132-157): float32 parameters, ADE coefficients, susceptibility."""
+
+    def __init__(self, omega_p, gamma, eps_inf=1.0):
+        self.omega_p, self.gamma, self.eps_inf = DTYPE(omega_p), DTYPE(gamma), DTYPE(eps_inf)
+
+    def coefficients(self, dt):
+        g, wp = float(self.gamma), float(self.omega_p)
+        denom = 1.0 + g * dt / 2.0
+        return DTYPE(-g * dt / denom), DTYPE(0.0), DTYPE((EPS0 * wp ** 2 * dt) / denom)
+
+    def susceptibility(self, omega):
+        wp, g = float(self.omega_p), float(self.gamma)
+        return complex(-wp ** 2 / (omega ** 2 - 1j * g * omega))
+
+
+class OracleLorentz:
+    """LorentzPole (physics/em/materials.py:160-190)."""
+
+    def __init__(self, delta_eps, omega_0, gamma):
+        self.delta_eps, self.omega_0, self.gamma = DTYPE(delta_eps), DTYPE(omega_0), DTYPE(gamma)
+
+    def coefficients(self, dt):
+        w0, g, de = float(self.omega_0), float(self.gamma), float(self.delta_eps)
+        denom = 1.0 + g * dt / 2.0
+        return DTYPE(-g * dt / denom), DTYPE(w0 ** 2 * dt ** 2 / denom), DTYPE(EPS0 * de * w0 ** 2 * dt ** 2 / denom)
+
+    def susceptibility(self, omega):
+        w0, g, de = float(self.omega_0), float(self.gamma), float(self.delta_eps)
+        return complex(de * w0 ** 2 / (w0 ** 2 - omega ** 2 + 1j * g * omega))
+
+
 def e_coefficients(sigma, eps_r, dt, real):
     """fdtd_ez_2d_kernels.py:314-319 (numpy twin), T = real."""
     dt = real(dt)
@@ -376,6 +430,16 @@ def _make_tfsf_struct(real):
     return Tfsf
 
 
+def _make_pole_struct(real):
+    R = ctypes.c_float if real == np.float32 else ctypes.c_double
+    P = ctypes.POINTER(R)
+
+    class Pole(ctypes.Structure):
+        _fields_ = [('kind', ctypes.c_int32), ('i0', ctypes.c_int32), ('i1', ctypes.c_int32), ('j0', ctypes.c_int32),
+                    ('j1', ctypes.c_int32), ('damping', R), ('restoring', R), ('drive', P), ('a', P), ('b', P)]
+    return Pole
+
+
 _LIBS = {}
 
 
@@ -389,6 +453,8 @@ def load_library(real=np.float32):
             raise RuntimeError(f'oracle library {path} is not built (run: make -C oracle)')
         lib = ctypes.CDLL(path)
         State, Line, Flux = _make_structs(real)
+        P = ctypes.POINTER(ctypes.c_float if real == np.float32 else ctypes.c_double)
+        R = ctypes.c_float if real == np.float32 else ctypes.c_double
         lib.oracle_ez2d_advance.restype = ctypes.c_int
         lib.oracle_ez2d_advance.argtypes = [ctypes.POINTER(State), ctypes.c_int64, ctypes.c_int64, ctypes.c_int32,
                                             ctypes.POINTER(Line), ctypes.c_int32, ctypes.POINTER(Flux),
@@ -400,6 +466,14 @@ def load_library(real=np.float32):
                                                  ctypes.POINTER(Flux), ctypes.c_int64, ctypes.c_int32,
                                                  ctypes.POINTER(Tfsf)]
         lib.tfsf_struct = Tfsf
+        Pole = _make_pole_struct(real)
+        lib.oracle_ez2d_advance_full.restype = ctypes.c_int
+        lib.oracle_ez2d_advance_full.argtypes = [ctypes.POINTER(State), ctypes.c_int64, ctypes.c_int64,
+                                                 ctypes.c_int32, ctypes.POINTER(Line), ctypes.c_int32,
+                                                 ctypes.POINTER(Flux), ctypes.c_int64, ctypes.c_int32,
+                                                 ctypes.POINTER(Tfsf), ctypes.c_int32, ctypes.POINTER(Pole), P,
+                                                 ctypes.c_int32 * 4, R]
+        lib.pole_struct = Pole
         _LIBS[key] = (lib, State, Line, Flux)
     return _LIBS[key]
 
@@ -433,6 +507,7 @@ class OracleEz2D:
         self.sources, self.monitors = [], []
         self.maps = []           # field-map DFT monitors (add_dft_monitor)
         self.tfsf = []           # TFSF plane-wave boxes (add_tfsf)
+        self.poles = []          # [pole, (slice, slice) box, cropped bool mask, state arrays] (add order)
         self.probes = []         # field probes (add_field_probe): [ix, iy, component, times, values]
         self.n_step = 0
         self.time = 0.0          # engine clock (host float64 accumulation)
@@ -516,6 +591,27 @@ class OracleEz2D:
                               dtype=np.complex64)
         self.maps.append(mon)
         return mon
+
+    def add_drude_rectangle(self, x0, y0, x1, y1, drude):
+        """physics/em/__init__.py:329-340: the pole on the mask, eps_r = eps_inf under it."""
+        self._add_pole(drude, rect_mask(self.domain, x0, y0, x1, y1), True)
+
+    def add_drude_circle(self, cx, cy, radius, drude):
+        self._add_pole(drude, circle_mask(self.domain, cx, cy, radius), True)
+
+    def add_dispersive(self, pole, mask):
+        self._add_pole(pole, np.asarray(mask, dtype=bool), False)
+
+    def _add_pole(self, pole, mask, set_background):
+        """fdtd_ez_2d.py:123-163 with _bounding_box (fdtd_2d_base.py:29-36): the pole on the bounding box of its
+        mask, drive = mask x drive there."""
+        rows = np.flatnonzero(mask.any(axis=1))
+        if rows.size:
+            cols = np.flatnonzero(mask.any(axis=0))
+            box = (slice(int(rows[0]), int(rows[-1]) + 1), slice(int(cols[0]), int(cols[-1]) + 1))
+            self.poles.append([pole, box, mask[box].copy()])
+        if set_background:
+            self.eps_r[mask] = DTYPE(pole.eps_inf)
 
     def add_tfsf(self, x0, y0, x1, y1, wavelength=None, frequency=None, bandwidth=0.5, amplitude=1.0,
                  waveform='gaussian'):
@@ -601,6 +697,17 @@ class OracleEz2D:
             omega = 2.0 * np.pi * float(src.temporal.f0)
             line_eps = (np.asarray(self.eps_r[line], dtype=np.complex128)
                         - 1j * np.asarray(self.sigma_e[line], dtype=np.float64) / (omega * EPS0))
+            # the susceptibility of every pole region the line crosses (sources.py:401-427)
+            for pole, box, cropped in self.poles:
+                chi = pole.susceptibility(omega)
+                along_box, normal_box = (box[0], box[1]) if src.axis == 'x' else (box[1], box[0])
+                start, stop = max(src.lo, along_box.start), min(src.hi, along_box.stop)
+                if not (normal_box.start <= src.position < normal_box.stop and start < stop):
+                    continue
+                along = slice(start - along_box.start, stop - along_box.start)
+                normal = src.position - normal_box.start
+                mask_line = cropped[along, normal] if src.axis == 'x' else cropped[normal, along]
+                line_eps[start - src.lo:stop - src.lo] += chi * mask_line
             admittance = sheet_admittance(line_eps, self.mu_r[line], self.sigma_m[line], omega, src.normal_width,
                                           float(d.dt))
             weight = np.asarray(2.0 * np.ones(src.hi - src.lo) / (float(ETA0) * src.normal_width), dtype=DTYPE)
@@ -704,6 +811,35 @@ class OracleEz2D:
             fluxes[i].first_sample, fluxes[i].n_samples = first_q, n_q
         return fluxes
 
+    def _pole_structs(self, Pole, R):
+        """ctypes records of the poles (states kept across chunks), the Drude total, its union box, float32 1 / dt."""
+        dt = float(self.domain.dt)
+        records = (Pole * max(1, len(self.poles)))()
+        union = None
+        for q, entry in enumerate(self.poles):
+            pole, box, cropped = entry[:3]
+            if len(entry) == 3:   # first chunk: drive and zero states
+                damping, restoring, drive = pole.coefficients(dt)
+                shape = cropped.shape
+                entry.extend([cropped.astype(DTYPE) * drive, np.zeros(shape, DTYPE), np.zeros(shape, DTYPE),
+                              damping, restoring])
+            drive_box, a, b, damping, restoring = entry[3:]
+            kind = 0 if isinstance(pole, OracleDrude) else 1
+            rec = records[q]
+            rec.kind, rec.damping, rec.restoring = kind, float(damping), float(restoring)
+            rec.i0, rec.i1, rec.j0, rec.j1 = box[0].start, box[0].stop, box[1].start, box[1].stop
+            rec.drive, rec.a, rec.b = _ptr(drive_box, R), _ptr(a, R), _ptr(b, R)
+            if kind == 0:
+                union = (box if union is None else (slice(min(union[0].start, box[0].start),
+                                                          max(union[0].stop, box[0].stop)),
+                                                    slice(min(union[1].start, box[1].start),
+                                                          max(union[1].stop, box[1].stop))))
+        if getattr(self, 'jz_total', None) is None:
+            self.jz_total = np.zeros((self.domain.nx, self.domain.ny), dtype=DTYPE)
+        box4 = (ctypes.c_int32 * 4)(*((union[0].start, union[0].stop, union[1].start, union[1].stop) if union
+                                      else (0, 0, 0, 0)))
+        return records, self.jz_total, box4, float(DTYPE(1.0 / dt))
+
     def _tfsf_structs(self, Tfsf, R, n_steps):
         """ctypes records of the TFSF boxes with this chunk's soft-source values FP32(scale * temporal(t + dt/2))."""
         boxes = (Tfsf * max(1, len(self.tfsf)))()
@@ -769,8 +905,10 @@ class OracleEz2D:
         lines = self._line_structs(Line, values)
         fluxes = self._flux_structs(Flux, phase_tables, first_q, n_q)
         boxes = self._tfsf_structs(lib.tfsf_struct, R, n_steps)
-        rc = lib.oracle_ez2d_advance_tfsf(ctypes.byref(st), self.n_step, n_steps, len(self.sources), lines,
-                                          len(self.monitors), fluxes, self.sample_interval, len(self.tfsf), boxes)
+        poles, jz_total, drude_box, inv_dt = self._pole_structs(lib.pole_struct, R)
+        rc = lib.oracle_ez2d_advance_full(ctypes.byref(st), self.n_step, n_steps, len(self.sources), lines,
+                                          len(self.monitors), fluxes, self.sample_interval, len(self.tfsf), boxes,
+                                          len(self.poles), poles, _ptr(jz_total, R), drude_box, inv_dt)
         del keep
         if rc != 0:
             raise RuntimeError('oracle phase table does not cover a sample')

@@ -27,8 +27,11 @@ def run_case(spec):
     import numpy as np
     from open_sol import Simulation
     from cases import apply_ops
+    from open_sol.physics.em.materials import DrudePole, LorentzPole
+    from cases_dft import apply_poles
     sim = Simulation(**spec['sim'])
     fluxes = apply_ops(sim, spec)
+    apply_poles(sim.em, spec, DrudePole, LorentzPole, sim.domain.circle_mask)
     maps = [sim.em.add_dft_monitor(x0, y0, x1, y1, frequencies=freqs, downsample=ds)
             for x0, y0, x1, y1, freqs, ds in spec['dft']]
     probes = [sim.em.add_field_probe(x, y, comp) for x, y, comp in spec.get('probes', [])]

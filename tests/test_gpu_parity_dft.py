@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from cases import apply_ops
-from cases_dft import CASES_DFT, CASES_DFT_HZ
+from cases_dft import CASES_DFT, CASES_DFT_HZ, apply_poles
 from test_oracle_golden_dft import field_names, map_keys, map_parts, run_oracle_dft
 
 import opensol_b200 as ob
@@ -29,6 +29,7 @@ def _digest(a):
 def _build(spec, config):
     sim = ob.Simulation(**spec['sim'], verbose=False)
     fluxes = apply_ops(sim, spec)
+    apply_poles(sim.em, spec, ob.DrudePole, ob.LorentzPole, sim.em.domain.circle_mask)
     maps = [sim.em.add_dft_monitor(x0, y0, x1, y1, frequencies=f, downsample=ds)
             for x0, y0, x1, y1, f, ds in spec['dft']]
     sim.probes = [sim.em.add_field_probe(x, y, comp) for x, y, comp in spec.get('probes', [])]

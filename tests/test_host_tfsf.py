@@ -41,3 +41,27 @@ def test_tfsf_box_must_keep_a_scattered_ring_inside_the_window():
                        verbose=False)
     with pytest.raises(NotImplementedError):
         hz.em.add_tfsf(0.2e-6, 0.2e-6, 0.8e-6, 0.8e-6, wavelength=700e-9)
+
+
+@pytest.mark.parametrize('params', [(8e15, 5e13, 2.0), (1.37e16, 1e14, 1.0)])
+def test_drude_coefficients_match_oracle(params):
+    from oracle.fdtd2d import OracleDrude
+    dt = 5.8377e-17
+    damping, drive = ob.DrudePole(*params).ade_coefficients(dt)
+    o_damping, _, o_drive = OracleDrude(*params).coefficients(dt)
+    assert (damping, drive) == (o_damping, o_drive)
+    assert ob.DrudePole(*params).susceptibility(2.3e15) == OracleDrude(*params).susceptibility(2.3e15)
+
+
+def test_lorentz_coefficients_match_oracle():
+    from oracle.fdtd2d import OracleLorentz
+    dt = 5.8377e-17
+    assert ob.LorentzPole(1.5, 3e15, 2e14).ade_coefficients(dt) == OracleLorentz(1.5, 3e15, 2e14).coefficients(dt)
+
+
+def test_unstable_drude_is_refused():
+    sim = ob.Simulation(size_x=1.0e-6, size_y=1.0e-6, dx=25e-9, npml=10, boundaries='pml', verbose=False)
+    sim.em.add_drude_rectangle(0.3e-6, 0.3e-6, 0.6e-6, 0.6e-6, ob.DrudePole(1.37e16, 1e14, 1.0))
+    sim.em.add_line_source('y', 0.2e-6, wavelength=700e-9)
+    with pytest.raises(ValueError, match='unstable'):
+        sim.em.finalize_host()

@@ -1,4 +1,4 @@
-"""Pin the oracle's field-map (running DFT) monitors and field probes to open_sol itself: the fixtures of
+"""Pin the oracle's field-map (running DFT) monitors, field probes, TFSF boxes and dispersive poles to open_sol itself: the fixtures of
 tests/golden/dft_*.npz (generated by running the reference's CPU backend, see tests/golden/make_golden_dft.py) must be
 reproduced bit for bit -- the complex64 maps at every checkpoint (E_z; H_z with E_x / E_y at the cell centres), the
 sample boxes, the flux line spectra, the fields' digests and the probes' times and values."""
@@ -9,8 +9,8 @@ import numpy as np
 import pytest
 
 from cases import apply_ops
-from cases_dft import CASES_DFT, CASES_DFT_HZ
-from oracle.fdtd2d import OracleEz2D
+from cases_dft import CASES_DFT, CASES_DFT_HZ, apply_poles
+from oracle.fdtd2d import OracleDrude, OracleEz2D, OracleLorentz, circle_mask
 from oracle.hz2d import OracleHz2D
 
 GOLDEN = os.path.join(os.path.dirname(__file__), 'golden')
@@ -47,6 +47,7 @@ def run_oracle_dft(spec):
     sim.pop('polarization', None)
     o = (OracleHz2D if is_hz(spec) else OracleEz2D)(**sim)
     fluxes = apply_ops(o, spec)
+    apply_poles(o, spec, OracleDrude, OracleLorentz, lambda cx, cy, r: circle_mask(o.domain, cx, cy, r))
     maps = [o.add_dft_monitor(x0, y0, x1, y1, frequencies=f, downsample=ds) for x0, y0, x1, y1, f, ds in spec['dft']]
     for mon in maps:
         mon.polarization = 'hz' if is_hz(spec) else 'ez'
