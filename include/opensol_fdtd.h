@@ -163,12 +163,14 @@ int os_fdtd2d_read_dft_map(OsFdtd2D *h, int32_t map_id, float *spectra);
 
 /* +x plane wave in vacuum on a total-field box of E_z cells [x0, x1) x [y0, y1): TFSFSource (physics/em/sources.py:
  * 206-350).  The host computes, as the reference does, the 1D incident line of aux_cells cells (the box's first
- * column at aux index aux_x0, the soft source at source_index), its H and E coefficients aux_coef_h (aux_cells - 1
- * hi faces) and aux_coef_e (aux_cells centres), the Mur end coefficients, and the side coefficients coef_h (H_y rows
- * x0 - 1, x1 - 1; H_x columns y0 - 1, y1 - 1) and coef_e (E_z rows x0, x1 - 1).  Each step: the H side corrections
- * and the incident H update after the H update, the E side corrections and the incident E update (soft source from
- * row n_lines + box of the chunk's value table) after the E update and the line sources.  An engine with a box
- * advances with the per-half-step kernels.  E_z engines only; not in batched advances or the adjoint.  At most 4. */
+ * column at aux index aux_x0, the soft source at source_index), its H and E coefficients aux_coef_h (aux_cells - 1)
+ * and aux_coef_e (aux_cells), the Mur end coefficients, and the side coefficients, 4 floats each: E_z handle, coef_h
+ * = H_y rows x0 - 1, x1 - 1 and H_x columns y0 - 1, y1 - 1, coef_e[0..1] = E_z rows x0, x1 - 1; H_z handle
+ * (TFSFSourceHz, sources.py:352-379: the incident line holds E_y on its faces and H_z at its centres), coef_h[0..1] =
+ * H_z rows x0, x1 - 1, coef_e = E_y rows x0 - 1, x1 - 1 and E_x columns y0 - 1, y1 - 1.  Each step: the H side
+ * corrections and the incident H update after the H update, the E side corrections and the incident E update (soft
+ * source from row n_lines + box of the chunk's value table) after the E update and the line sources.  An engine with
+ * a box advances with the per-half-step kernels.  Not in batched advances or the adjoint.  At most 4. */
 int os_fdtd2d_add_tfsf(OsFdtd2D *h, int32_t x0, int32_t x1, int32_t y0, int32_t y1, int32_t aux_cells, int32_t aux_x0,
                        int32_t source_index, const float *coef_h, const float *coef_e, float mur_lo, float mur_hi,
                        const float *aux_coef_h, const float *aux_coef_e, int32_t *tfsf_id);

@@ -49,8 +49,8 @@ struct ProbeSet {
 // the host.
 struct Tfsf2D {
     int32_t x0, x1, y0, y1, aux_x0, aux_n, source_index;
-    float coef_h[4], coef_e[2], mur_lo, mur_hi;
-    DeviceArray<float> aux_ez, aux_hy, aux_coef_h, aux_coef_e;
+    float coef_h[4], coef_e[4], mur_lo, mur_hi;
+    DeviceArray<float> aux_ez, aux_hy, aux_coef_h, aux_coef_e;   // H_z boxes: aux_ez = incident E_y, aux_hy = H_z
 };
 
 // Drude (kind 0) or Lorentz (kind 1) pole on a cell box: drive (box, pole drive x cell mask) and its state.
@@ -1458,15 +1458,37 @@ static int advance_hz(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_
                          (unsigned)((nx + cell_block.y - 1) / cell_block.y));
     const HzPlan plan = hz_plan(h);
     for (int64_t k = 0; k < n_steps; ++k) {
-        const int in = h->cur, out = h->variant == 0 ? h->cur : h->cur ^ 1;
+        const int in = h->cur, out = (h->variant == 0 || !h->tfsf.empty()) ? h->cur : h->cur ^ 1;
         Hz2DParams p = make_hz_params(h, in, out);
         p.line_values = values;
         p.values_stride = n_steps;
         p.k_step = k;
-        if (h->variant == 0) {
+        if (h->variant == 0 || !h->tfsf.empty()) {   // a TFSF box acts between the half steps
             OS_TRY(prof_begin(h, 3, h->stream));
             hz2d_h_kernel<<<cell_grid, cell_block, 0, h->stream>>>(p);
+            for (auto &t : h->tfsf) {   // TFSFSourceHz.inject_magnetic (fdtd_hz_2d.py:160-163)
+                hz2d_tfsf_h_kernel<<<(t->y1 - t->y0 + 255) / 256, 256, 0, h->stream>>>(
+                    h->ez[in].ptr, t->aux_ez.ptr, t->x0, t->x1, t->y0, t->y1, t->aux_x0, ny, t->coef_h[0],
+                    t->coef_h[1]);
+                // aux_hz[k] += coef[k - 1] (aux_ey[k] - aux_ey[k - 1]), k >= 1
+                ez2d_tfsf_aux_h_kernel<<<(t->aux_n + 255) / 256, 256, 0, h->stream>>>(
+                    t->aux_ez.ptr, t->aux_coef_h.ptr, t->aux_hy.ptr + 1, t->aux_n);
+                h->launches += 2;
+            }
             hz2d_e_kernel<<<cell_grid, cell_block, 0, h->stream>>>(p);
+            for (size_t b = 0; b < h->tfsf.size(); ++b) {   // TFSFSourceHz.inject_electric (fdtd_hz_2d.py:171-174)
+                Tfsf2D &t = *h->tfsf[b];
+                const int side = std::max(t.x1 - t.x0, t.y1 - t.y0);
+                hz2d_tfsf_e_kernel<<<(side + 255) / 256, 256, 0, h->stream>>>(
+                    h->hx[in].ptr, h->hy[in].ptr, t.aux_hy.ptr, t.x0, t.x1, t.y0, t.y1, t.aux_x0, ny, t.coef_e[0],
+                    t.coef_e[1], t.coef_e[2], t.coef_e[3]);
+                // aux_ey[a] += ce[a] (aux_hz[a + 1] - aux_hz[a]), the soft source, the Mur ends
+                const float *value = values + (h->lines.size() + b) * (size_t)n_steps + (size_t)k;
+                ez2d_tfsf_aux_e_kernel<<<1, 256, 0, h->stream>>>(t.aux_ez.ptr, t.aux_hy.ptr + 1, t.aux_n,
+                                                                 t.aux_coef_e.ptr, t.source_index, value, t.mur_lo,
+                                                                 t.mur_hi);
+                h->launches += 2;
+            }
             OS_TRY(prof_end(h, h->stream));
             h->launches += 2;
         } else {
@@ -1815,7 +1837,7 @@ extern "C" int os_fdtd2d_add_tfsf(OsFdtd2D *h, int32_t x0, int32_t x1, int32_t y
                                   int32_t aux_x0, int32_t source_index, const float *coef_h, const float *coef_e,
                                   float mur_lo, float mur_hi, const float *aux_coef_h, const float *aux_coef_e,
                                   int32_t *tfsf_id) {
-    OS_TRY(require_ez(h, "os_fdtd2d_add_tfsf"));
+    OS_CHECK(h, OS_ERR_INVALID, "os_fdtd2d_add_tfsf: null handle");
     OS_CHECK(coef_h && coef_e && aux_coef_h && aux_coef_e, OS_ERR_INVALID, "os_fdtd2d_add_tfsf: null argument");
     OS_CHECK(1 <= x0 && x0 < x1 && x1 < h->grid.nx && 1 <= y0 && y0 < y1 && y1 < h->grid.ny, OS_ERR_INVALID,
              "TFSF box [%d, %d) x [%d, %d) must keep one scattered-field cell on every side of the %d x %d grid", x0,
@@ -1831,7 +1853,7 @@ extern "C" int os_fdtd2d_add_tfsf(OsFdtd2D *h, int32_t x0, int32_t x1, int32_t y
     t->x0 = x0, t->x1 = x1, t->y0 = y0, t->y1 = y1;
     t->aux_n = aux_cells, t->aux_x0 = aux_x0, t->source_index = source_index;
     for (int k = 0; k < 4; ++k) t->coef_h[k] = coef_h[k];
-    t->coef_e[0] = coef_e[0], t->coef_e[1] = coef_e[1];
+    for (int k = 0; k < 4; ++k) t->coef_e[k] = coef_e[k];
     t->mur_lo = mur_lo, t->mur_hi = mur_hi;
     OS_TRY(t->aux_ez.alloc((size_t)aux_cells));
     OS_TRY(t->aux_hy.alloc((size_t)aux_cells));

@@ -354,6 +354,35 @@ __global__ void ez2d_tfsf_aux_e_kernel(float *__restrict__ aux_ez, const float *
     }
 }
 
+// H_z box (TFSFSourceHz, physics/em/sources.py:55-70,108-172,352-379): total-field H_z corrections after the H_z
+// update on rows x0 (+, from the incident E_y below the box) and x1 - 1 (-); scattered-field E corrections after the
+// E update: E_y on rows x0 - 1 (+) and x1 - 1 (-) from the incident H_z, E_x on columns y0 - 1 (-) and y1 - 1 (+).
+__global__ void hz2d_tfsf_h_kernel(float *__restrict__ hz, const float *__restrict__ aux_ey, int x0, int x1, int y0,
+                                   int y1, int aux_x0, int ny, float c_xlo, float c_xhi) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= y1 - y0) return;
+    const int j = y0 + k;
+    hz[(size_t)x0 * ny + j] = hz[(size_t)x0 * ny + j] + c_xlo * aux_ey[aux_x0 - 1];
+    hz[(size_t)(x1 - 1) * ny + j] = hz[(size_t)(x1 - 1) * ny + j] - c_xhi * aux_ey[aux_x0 + (x1 - 1 - x0)];
+}
+
+__global__ void hz2d_tfsf_e_kernel(float *__restrict__ ex, float *__restrict__ ey, const float *__restrict__ aux_hz,
+                                   int x0, int x1, int y0, int y1, int aux_x0, int ny, float c_xlo, float c_xhi,
+                                   float c_ylo, float c_yhi) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < y1 - y0) {
+        const int j = y0 + k;
+        ey[(size_t)(x0 - 1) * ny + j] = ey[(size_t)(x0 - 1) * ny + j] + c_xlo * aux_hz[aux_x0];
+        ey[(size_t)(x1 - 1) * ny + j] = ey[(size_t)(x1 - 1) * ny + j] - c_xhi * aux_hz[aux_x0 + (x1 - 1 - x0)];
+    }
+    if (k < x1 - x0) {
+        const size_t row = (size_t)(x0 + k) * ny;
+        const float incident = aux_hz[aux_x0 + k];
+        ex[row + (y0 - 1)] = ex[row + (y0 - 1)] - c_ylo * incident;
+        ex[row + (y1 - 1)] = ex[row + (y1 - 1)] + c_yhi * incident;
+    }
+}
+
 // ca / cb from float32 eps_r, sigma_e (fdtd_ez_2d_kernels.py:314-332, T = float); sigma NULL = lossless (ca not
 // written: it is 1).
 __global__ void ez2d_e_coefficients_kernel(const float *__restrict__ eps_r, const float *__restrict__ sigma, float dt,

@@ -168,8 +168,10 @@ class FDTDEngine2D_Ez:
         for source in self._tfsf:
             if id(source) not in self._monitor_ids:
                 tid = ctypes.c_int32()
-                coef_h = np.array(source.coef_h, dtype=DTYPE)
-                coef_e = np.array(source.coef_e, dtype=DTYPE)
+                coef_h = np.zeros(4, dtype=DTYPE)
+                coef_e = np.zeros(4, dtype=DTYPE)
+                coef_h[:len(source.coef_h)] = source.coef_h
+                coef_e[:len(source.coef_e)] = source.coef_e
                 _native.check(lib.os_fdtd2d_add_tfsf(
                     h, source.x0, source.x1, source.y0, source.y1, source.aux_cells, source.aux_x0,
                     source.AUX_SOURCE_INDEX, _native.fptr(coef_h), _native.fptr(coef_e), float(source.mur[0]),

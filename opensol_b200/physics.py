@@ -281,11 +281,9 @@ class EMPhysics:
 
     def add_tfsf(self, x0, y0, x1, y1, wavelength=None, frequency=None, bandwidth=0.5, amplitude=1.0,
                  waveform='gaussian'):
-        """+x plane wave of incident peak `amplitude` [V/m] (E_z) inside the box (physics/em/__init__.py:475-490 with
+        """+x plane wave of incident peak `amplitude` [V/m] (E_z; E_y on hz) inside the box (physics/em/__init__.py:475-490 with
         placement.tfsf_box_cells): the box's cells plus one scattered-field cell on every side lie in the physical
         window (this engine's boundary presets have no mirror face a box could open onto)."""
-        if self.polarization != 'ez':
-            raise NotImplementedError('TFSF plane waves are built for the E_z engine only')
         d = self.domain
         temporal = make_temporal(waveform, resolve_frequency(wavelength, frequency), bandwidth)
         d.validate_physical_pos(x0, y0, "TFSF box corner 0")
@@ -301,7 +299,8 @@ class EMPhysics:
                              f"[{window_y.start}, {window_y.stop}) on every side")
         grid = d.grid
         widths = (np.full(grid.nx, float(grid.dx)), np.full(grid.ny, float(grid.dy)))   # yee_grid.grid_cell_widths
-        source = TFSFSource(ix0, ix1, iy0, iy1, temporal, float(grid.dt), amplitude, cell_widths=widths)
+        source = TFSFSource(ix0, ix1, iy0, iy1, temporal, float(grid.dt), amplitude, cell_widths=widths,
+                            polarization=self.polarization)
         self.sources.append(source)
         self.engine.attach_tfsf(source)
         return source

@@ -218,8 +218,9 @@ def calibrate_tangential_sheet(source, materials, omega, normal_spacing, dt, sha
 
 
 class TFSFSource:
-    """+x plane wave in vacuum on a total-field box of E_z cells [x0, x1) x [y0, y1) (physics/em/sources.py:206-332,
-    _PlaneWaveBox + TFSFSource): a 1D incident line (20 margin cells at the widths of cells x0 - 1 / x1, the box
+    """+x plane wave in vacuum on a total-field box of cells [x0, x1) x [y0, y1) (physics/em/sources.py:206-379,
+    _PlaneWaveBox + TFSFSource, or TFSFSourceHz for polarization 'hz', whose corrections act on H_z rows x0 / x1 - 1
+    and the scattered E_y / E_x faces around the box): a 1D incident line (20 margin cells at the widths of cells x0 - 1 / x1, the box
     columns between; soft source at aux cell 10 upstream of the box, Mur ends matched to the numerical phase velocity
     at the carrier) advanced on the device beside the grid, and the scattered / total-field corrections on the box
     sides: H_y on rows x0 - 1 and x1 - 1, H_x on columns y0 - 1 and y1 - 1 after the H update, E_z on rows x0 and
@@ -229,7 +230,7 @@ class TFSFSource:
     AUX_MARGIN = 20
     AUX_SOURCE_INDEX = 10
 
-    def __init__(self, x0, x1, y0, y1, temporal, dt, amplitude=1.0, cell_widths=None):
+    def __init__(self, x0, x1, y0, y1, temporal, dt, amplitude=1.0, cell_widths=None, polarization='ez'):
         x0, x1, y0, y1 = int(x0), int(x1), int(y0), int(y1)
         if not (1 <= x0 < x1 and 1 <= y0 < y1):
             raise ValueError(f"TFSF box [{x0}, {x1}) x [{y0}, {y1}) must be non-empty and keep one scattered-field "
@@ -254,10 +255,19 @@ class TFSFSource:
         side_widths_x = (float(dx_cells[x0]), float(dx_cells[x1 - 1]))
         side_spacings = tuple(0.5 * float(w[i] + w[i + 1]) for w, i in ((dx_cells, x0 - 1), (dx_cells, x1 - 1),
                                                                        (dy_cells, y0 - 1), (dy_cells, y1 - 1)))
-        self.coef_h = tuple(DTYPE(dt / (MU0 * s)) for s in side_spacings)     # H_y x0-1, x1-1; H_x y0-1, y1-1
-        self.coef_e = tuple(DTYPE(dt / (EPS0 * w)) for w in side_widths_x)    # E_z x0, x1-1
-        self.aux_coef_h = np.asarray(dt / (MU0 * face_spacings), dtype=DTYPE)  # (n - 1,) hi faces
-        self.aux_coef_e = np.asarray(dt / (EPS0 * widths), dtype=DTYPE)        # (n,) centres
+        self.polarization = polarization
+        if polarization == 'ez':
+            self.coef_h = tuple(DTYPE(dt / (MU0 * s)) for s in side_spacings)     # H_y x0-1, x1-1; H_x y0-1, y1-1
+            self.coef_e = tuple(DTYPE(dt / (EPS0 * w)) for w in side_widths_x)    # E_z x0, x1-1
+            self.aux_coef_h = np.asarray(dt / (MU0 * face_spacings), dtype=DTYPE)  # (n - 1,) hi faces
+            self.aux_coef_e = np.asarray(dt / (EPS0 * widths), dtype=DTYPE)        # (n,) centres
+        else:
+            # TFSFSourceHz (sources.py:352-379): the vacuum pair mu dHz/dt = -dEy/dx, eps0 dEy/dt = -dHz/dx, H_z at
+            # the line's centres, E_y on its hi faces (the last face's spacing repeats the last width)
+            self.coef_h = tuple(DTYPE(dt / (MU0 * w)) for w in side_widths_x)     # H_z x0, x1-1
+            self.coef_e = tuple(DTYPE(dt / (EPS0 * s)) for s in side_spacings)    # E_y x0-1, x1-1; E_x y0-1, y1-1
+            self.aux_coef_h = np.asarray(-dt / (MU0 * widths[1:]), dtype=DTYPE)  # H_z centres 1 .. n-1
+            self.aux_coef_e = np.asarray(-dt / (EPS0 * np.append(face_spacings, widths[-1])), dtype=DTYPE)
         self.aux_x0 = m
         self.aux_cells = int(widths.size)
 

@@ -655,7 +655,9 @@ class OracleEz2D:
                'mur': (DTYPE(mur_lo), DTYPE(mur_hi)),
                'aux_coef_h': np.asarray(dt / (MU0 * face_spacings), dtype=DTYPE),
                'aux_coef_e': np.asarray(dt / (EPS0 * widths), dtype=DTYPE),
-               'aux_ez': np.zeros(widths.size, dtype=DTYPE), 'aux_hy': np.zeros(widths.size, dtype=DTYPE)})
+               'aux_ez': np.zeros(widths.size, dtype=DTYPE), 'aux_hy': np.zeros(widths.size, dtype=DTYPE),
+               'widths': widths, 'face_spacings': face_spacings, 'spacings': spacings,
+               'side_widths_x': (float(dx_cells[ix0]), float(dx_cells[ix1 - 1])), 'dt': dt})
         self.tfsf.append(box)
         return box
 

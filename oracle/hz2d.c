@@ -55,6 +55,50 @@ typedef struct {
     int64_t first_sample, n_samples;
 } OracleFluxHz;
 
+/* TFSFSourceHz (open_sol/physics/em/sources.py:55-70,352-379): the incident line holds E_y (aux_ey, hi faces) and
+ * H_z (aux_hz, centres); coef_h[0..1] act on H_z rows x0 / x1 - 1, coef_e on E_y rows x0 - 1 / x1 - 1 and E_x columns
+ * y0 - 1 / y1 - 1. */
+typedef struct {
+    int32_t x0, x1, y0, y1, aux_x0, aux_n, source_index;
+    real coef_h[4], coef_e[4], mur_lo, mur_hi;
+    real *aux_ey, *aux_hz;
+    const real *aux_coef_h, *aux_coef_e;
+    const float *values;
+} OracleTfsfHz;
+
+/* inject_magnetic: H_z corrections from the incident E_y, then aux_hz[k] += coef[k - 1] (aux_ey[k] - aux_ey[k - 1]). */
+static void tfsf_h(const OracleHz2D *s, const OracleTfsfHz *t)
+{
+    const size_t ny = (size_t)s->ny;
+    for (int j = t->y0; j < t->y1; ++j) {
+        s->hz[(size_t)t->x0 * ny + j] += t->coef_h[0] * t->aux_ey[t->aux_x0 - 1];
+        s->hz[(size_t)(t->x1 - 1) * ny + j] -= t->coef_h[1] * t->aux_ey[t->aux_x0 + (t->x1 - 1 - t->x0)];
+    }
+    for (int k = 1; k < t->aux_n; ++k) t->aux_hz[k] += t->aux_coef_h[k - 1] * (t->aux_ey[k] - t->aux_ey[k - 1]);
+}
+
+/* inject_electric: E_y / E_x corrections from the incident H_z, then the incident E_y update (aux_ey[a] += ce[a]
+ * (aux_hz[a + 1] - aux_hz[a])), the soft source and the Mur ends. */
+static void tfsf_e(const OracleHz2D *s, const OracleTfsfHz *t, int64_t k)
+{
+    const size_t ny = (size_t)s->ny;
+    for (int j = t->y0; j < t->y1; ++j) {
+        s->ey[(size_t)(t->x0 - 1) * ny + j] += t->coef_e[0] * t->aux_hz[t->aux_x0];
+        s->ey[(size_t)(t->x1 - 1) * ny + j] -= t->coef_e[1] * t->aux_hz[t->aux_x0 + (t->x1 - 1 - t->x0)];
+    }
+    for (int i = t->x0; i < t->x1; ++i) {
+        const real incident = t->aux_hz[t->aux_x0 + (i - t->x0)];
+        s->ex[(size_t)i * ny + (t->y0 - 1)] -= t->coef_e[2] * incident;
+        s->ex[(size_t)i * ny + (t->y1 - 1)] += t->coef_e[3] * incident;
+    }
+    const int n = t->aux_n;
+    const real old0 = t->aux_ey[0], old1 = t->aux_ey[1], old2 = t->aux_ey[n - 2], old3 = t->aux_ey[n - 1];
+    for (int a = 1; a < n - 1; ++a) t->aux_ey[a] += t->aux_coef_e[a] * (t->aux_hz[a + 1] - t->aux_hz[a]);
+    t->aux_ey[t->source_index] += (real)t->values[k];
+    t->aux_ey[0] = old1 + t->mur_lo * (t->aux_ey[1] - old0);
+    t->aux_ey[n - 1] = old2 + t->mur_hi * (t->aux_ey[n - 2] - old3);
+}
+
 static void update_hz(const OracleHz2D *s) {
     const int nx = s->nx, ny = s->ny;
     const real one = (real)1, zero = (real)0;
@@ -187,16 +231,19 @@ static void accumulate_flux(const OracleHz2D *s, OracleFluxHz *m, int64_t sample
     }
 }
 
-int oracle_hz2d_advance(OracleHz2D *s, int64_t step0, int64_t n_steps, int32_t n_lines, const OracleLineHz *lines,
-                        int32_t n_monitors, OracleFluxHz *monitors, int64_t sample_interval) {
+int oracle_hz2d_advance_tfsf(OracleHz2D *s, int64_t step0, int64_t n_steps, int32_t n_lines,
+                             const OracleLineHz *lines, int32_t n_monitors, OracleFluxHz *monitors,
+                             int64_t sample_interval, int32_t n_tfsf, const OracleTfsfHz *tfsf) {
     for (int64_t k = 0; k < n_steps; ++k) {
         update_hz(s);
         for (int side = 0; side < 4; ++side)
             if (s->cpml_active[side]) cpml_side(s, side, 1);
+        for (int b = 0; b < n_tfsf; ++b) tfsf_h(s, &tfsf[b]);
         update_exy(s);
         for (int side = 0; side < 4; ++side)
             if (s->cpml_active[side]) cpml_side(s, side, 0);
         for (int l = 0; l < n_lines; ++l) inject_line(s, &lines[l], k);
+        for (int b = 0; b < n_tfsf; ++b) tfsf_e(s, &tfsf[b], k);
         const int64_t n_step = step0 + k + 1;
         if (n_monitors > 0 && n_step % sample_interval == 0) {
             const int64_t sample = n_step / sample_interval;
@@ -208,4 +255,9 @@ int oracle_hz2d_advance(OracleHz2D *s, int64_t step0, int64_t n_steps, int32_t n
         }
     }
     return 0;
+}
+
+int oracle_hz2d_advance(OracleHz2D *s, int64_t step0, int64_t n_steps, int32_t n_lines, const OracleLineHz *lines,
+                        int32_t n_monitors, OracleFluxHz *monitors, int64_t sample_interval) {
+    return oracle_hz2d_advance_tfsf(s, step0, n_steps, n_lines, lines, n_monitors, monitors, sample_interval, 0, 0);
 }

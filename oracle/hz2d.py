@@ -28,7 +28,7 @@ import os
 
 import numpy as np
 
-from oracle.fdtd2d import (DTYPE, EPS0, ETA0, LIB_DIR, OracleEz2D, _make_structs, _ptr, build_cpml,
+from oracle.fdtd2d import (DTYPE, EPS0, ETA0, LIB_DIR, MU0, OracleEz2D, _make_structs, _ptr, build_cpml,
                            dft_phases, dft_sample_interval, h_coefficients, paint_circle, paint_rect, sheet_admittance,
                            yee_inverse_spacings)
 
@@ -190,7 +190,7 @@ class OracleHz2D(OracleEz2D):
                                           omega, src.normal_width, float(d.dt))
             weight = np.asarray(2.0 * np.ones(src.hi - src.lo) / (float(ETA0) * src.normal_width), dtype=DTYPE)
             src.profile = (row(cb_face, src.position) * admittance * weight).astype(DTYPE)
-        self.sample_interval = dft_sample_interval(float(d.dt), self.sources,
+        self.sample_interval = dft_sample_interval(float(d.dt), self.sources + self.tfsf,
                                                    [m.frequencies for m in self.monitors + self.maps])
         for m in self.monitors + self.maps:
             m.sample_interval = self.sample_interval
@@ -208,6 +208,49 @@ class OracleHz2D(OracleEz2D):
 
     def add_field_probe(self, x, y, field_component=None):
         return super().add_field_probe(x, y, field_component or 'hz')
+
+    def add_tfsf(self, x0, y0, x1, y1, wavelength=None, frequency=None, bandwidth=0.5, amplitude=1.0,
+                 waveform='gaussian'):
+        """TFSFSourceHz (physics/em/sources.py:352-366): the E_z box's cells, line and source scale, with the H_z
+        side coefficients dt / (mu0 w) on rows x0 / x1 - 1, the E side ones dt / (eps0 s) on the scattered faces, and
+        the incident pair's negated coefficients (H_z at the line's centres 1 .. n-1, E_y on its faces, the last
+        face's spacing repeating the last width).  aux_ez holds the incident E_y, aux_hy the incident H_z."""
+        box = super().add_tfsf(x0, y0, x1, y1, wavelength, frequency, bandwidth, amplitude, waveform)
+        dt = box.dt
+        box.coef_h = [DTYPE(dt / (MU0 * w)) for w in box.side_widths_x] + [DTYPE(0.0), DTYPE(0.0)]
+        box.coef_e = [DTYPE(dt / (EPS0 * sp)) for sp in box.spacings]
+        box.aux_coef_h = np.asarray(-dt / (MU0 * box.widths[1:]), dtype=DTYPE)
+        box.aux_coef_e = np.asarray(-dt / (EPS0 * np.append(box.face_spacings, box.widths[-1])), dtype=DTYPE)
+        return box
+
+    def _tfsf_hz_structs(self, R, n_steps):
+        P = ctypes.POINTER(R)
+
+        class TfsfHz(ctypes.Structure):
+            _fields_ = [('x0', ctypes.c_int32), ('x1', ctypes.c_int32), ('y0', ctypes.c_int32),
+                        ('y1', ctypes.c_int32), ('aux_x0', ctypes.c_int32), ('aux_n', ctypes.c_int32),
+                        ('source_index', ctypes.c_int32), ('coef_h', R * 4), ('coef_e', R * 4), ('mur_lo', R),
+                        ('mur_hi', R), ('aux_ey', P), ('aux_hz', P), ('aux_coef_h', P), ('aux_coef_e', P),
+                        ('values', ctypes.POINTER(ctypes.c_float))]
+
+        boxes = (TfsfHz * max(1, len(self.tfsf)))()
+        dt = float(self.domain.dt)
+        for b, box in enumerate(self.tfsf):
+            t, values = self.time, np.empty(n_steps, dtype=np.float32)
+            for k in range(n_steps):
+                values[k] = DTYPE(box.scale * box.temporal(t + 0.5 * dt))
+                t = t + dt
+            box.values = values
+            rec = boxes[b]
+            rec.x0, rec.x1, rec.y0, rec.y1 = box.cells
+            rec.aux_x0, rec.aux_n, rec.source_index = box.aux_x0, box.aux_ez.size, box.source_index
+            for i in range(4):
+                rec.coef_h[i], rec.coef_e[i] = float(box.coef_h[i]), float(box.coef_e[i])
+            rec.mur_lo, rec.mur_hi = float(box.mur[0]), float(box.mur[1])
+            rec.aux_ey, rec.aux_hz = _ptr(box.aux_ez, R), _ptr(box.aux_hy, R)
+            rec.aux_coef_h, rec.aux_coef_e = _ptr(box.aux_coef_h, R), _ptr(box.aux_coef_e, R)
+            rec.values = _ptr(values, ctypes.c_float)
+        return boxes, TfsfHz
 
     def _fold_maps(self):
         """DFTMonitor.update for 'hz' (monitors.py:281-322): H_z with the phases of t - dt/2, E_x / E_y as the
@@ -246,8 +289,13 @@ class OracleHz2D(OracleEz2D):
         keep = self._cpml_state(st, R)
         lines = self._line_structs(Line, values)
         fluxes = self._flux_structs(Flux, phase_tables, first_q, n_q)
-        rc = lib.oracle_hz2d_advance(ctypes.byref(st), self.n_step, n_steps, len(self.sources), lines,
-                                     len(self.monitors), fluxes, self.sample_interval)
+        boxes, TfsfHz = self._tfsf_hz_structs(R, n_steps)
+        lib.oracle_hz2d_advance_tfsf.restype = ctypes.c_int
+        lib.oracle_hz2d_advance_tfsf.argtypes = [ctypes.POINTER(State), ctypes.c_int64, ctypes.c_int64, ctypes.c_int32,
+                                                 ctypes.POINTER(Line), ctypes.c_int32, ctypes.POINTER(Flux),
+                                                 ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(TfsfHz)]
+        rc = lib.oracle_hz2d_advance_tfsf(ctypes.byref(st), self.n_step, n_steps, len(self.sources), lines,
+                                          len(self.monitors), fluxes, self.sample_interval, len(self.tfsf), boxes)
         del keep
         if rc != 0:
             raise RuntimeError('oracle phase table does not cover a sample')

@@ -123,6 +123,21 @@ CASES_DFT_HZ = [
         'probes': [[0.75e-6, 0.5e-6, 'hz'], [0.5e-6, 0.6e-6, 'ex']],
         'checkpoints': [250, 500],
     },
+    {   # +x plane wave (TFSF box, incident E_y) on a cylinder in H_z, all CPML; flux line, map and probe outside
+        'name': 'tfsf_hz_cylinder',
+        'sim': {'size_x': 2.0e-6, 'size_y': 1.6e-6, 'dx': 25e-9, 'npml': 12, 'boundaries': 'pml',
+                'polarization': 'hz'},
+        'ops': [
+            ['add_dielectric_circle', [1.0e-6, 0.8e-6, 0.25e-6], {'eps_r': 4.0}],
+            ['add_tfsf', [0.4e-6, 0.3e-6, 1.6e-6, 1.3e-6], {'wavelength': 700e-9, 'bandwidth': 0.5}],
+            ['add_flux_monitor', ['y', 1.8e-6, [0.2e-6, 1.4e-6]], {'wavelengths': [650e-9, 750e-9]}],
+        ],
+        'dft': [
+            [0.2e-6, 0.1e-6, 1.85e-6, 1.5e-6, [4.3e14], 2],
+        ],
+        'probes': [[1.8e-6, 0.8e-6, 'hz'], [1.0e-6, 0.35e-6, 'ey']],
+        'checkpoints': [300, 700],
+    },
     {   # periodic y: a full-resolution map from y = 0 (wrapped partner faces) and a 3x-downsampled one
         'name': 'dft_hz_periodic_y',
         'sim': {'size_x': 2.0e-6, 'size_y': 1.0e-6, 'dx': 25e-9, 'npml': 12, 'boundaries': 'periodic_y',

@@ -39,8 +39,8 @@ def test_tfsf_box_must_keep_a_scattered_ring_inside_the_window():
         sim.em.add_tfsf(0.0, 0.2e-6, 0.5e-6, 0.8e-6, wavelength=700e-9)
     hz = ob.Simulation(size_x=1.0e-6, size_y=1.0e-6, dx=25e-9, npml=10, boundaries='pml', polarization='hz',
                        verbose=False)
-    with pytest.raises(NotImplementedError):
-        hz.em.add_tfsf(0.2e-6, 0.2e-6, 0.8e-6, 0.8e-6, wavelength=700e-9)
+    with pytest.raises(ValueError, match='scattered-field'):
+        hz.em.add_tfsf(0.2e-6, 0.0, 0.8e-6, 0.8e-6, wavelength=700e-9)
 
 
 @pytest.mark.parametrize('params', [(8e15, 5e13, 2.0), (1.37e16, 1e14, 1.0)])
