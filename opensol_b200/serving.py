@@ -207,9 +207,10 @@ class ServingLoop:
         the JobResults in completion order.  time_ticks: wait for every tick and add up its device time (device_ms,
         launches), at the price of a host wait per tick.
 
-        Each tick is enqueued first; while the device runs it the host admits arrivals (they join the next tick),
-        makes the next tick's source and phase tables, and only then reads the fluxes of the jobs the tick finished
-        (which waits for it) and releases them.  At most admit_per_tick jobs are set up per tick, so a burst of
+        Each tick is enqueued first; the jobs it finishes go back to their own streams behind it, and their fluxes
+        are read after the next tick is enqueued (so the device never waits for that read); while the device runs the
+        tick the host also admits arrivals (they join the next tick) and makes the next tick's source and phase
+        tables.  At most admit_per_tick jobs are set up per tick, so a burst of
         arrivals starts on the device while the rest of it is still being set up on the host."""
         if realtime:
             pending = deque(sorted(specs, key=lambda s: (s.arrival, s.job_id)))
@@ -239,12 +240,28 @@ class ServingLoop:
                 groups.setdefault(min(self.chunk_steps, a.remaining), []).append(a)
             return sorted(groups.items(), key=lambda kv: -kv[0])
 
-        tables = {}   # id(job) -> its chunk tables for the next tick, made while the device runs the current one
-        while pending or active:
+        def finish(jobs):
+            # the jobs left the batch stream when their last tick was enqueued: their own streams wait for that tick
+            # only, so reading them does not wait for the tick queued after it
+            nonlocal used
+            for a in jobs:
+                fluxes = [m.flux() for m in a.monitors]
+                finished = time.perf_counter() - t0
+                arrival = a.spec.arrival if realtime else 0.0
+                results.append(JobResult(a.spec.job_id, fluxes, arrival, a.admitted, finished, a.spec.steps,
+                                         a.spec.cells()))
+                a.sim.em.engine.close()
+                used -= a.bytes
+
+        tables = {}      # id(job) -> its chunk tables for the next tick, made while the device runs the current one
+        unread = []      # jobs whose last tick is queued; read after the next tick is queued
+        while pending or active or unread:
             if not active:
                 used = admit(active, used)
                 tables = {}
                 if not active:
+                    finish(unread)
+                    unread = []
                     if pending:
                         time.sleep(max(0.0, min(0.005, pending[0].arrival - (time.perf_counter() - t0))))
                     continue
@@ -262,17 +279,14 @@ class ServingLoop:
             self.ticks += 1
             done = [a for a in active if a.remaining == 0]
             survivors = [a for a in active if a.remaining > 0]
+            for a in done:
+                a.sim.em.engine.set_stream(None)   # back to its own stream, behind this tick's work
+            # the jobs of the previous tick, now that this one keeps the device busy
+            finish(unread)
+            unread = done
             # while the device runs the tick: arrivals join the next one, whose tables are made now
             used = admit(survivors, used)
             tables = {id(a): a.sim.em.engine.chunk_tables(min(self.chunk_steps, a.remaining)) for a in survivors}
-            for a in done:
-                fluxes = [m.flux() for m in a.monitors]
-                finished = time.perf_counter() - t0
-                arrival = a.spec.arrival if realtime else 0.0
-                results.append(JobResult(a.spec.job_id, fluxes, arrival, a.admitted, finished, a.spec.steps,
-                                         a.spec.cells()))
-                a.sim.em.engine.close()
-                used -= a.bytes
             active = survivors
         return results
 
