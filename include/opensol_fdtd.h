@@ -385,6 +385,9 @@ int os_fdtd3d_read_flux_pair(OsFdtd3D *h, int32_t pair_id, double *e_spectra, do
 int os_fdtd3d_reset(OsFdtd3D *h);
 int os_fdtd3d_synchronize(OsFdtd3D *h);
 int os_fdtd3d_set_stream(OsFdtd3D *h, void *cuda_stream);
+
+/* x planes each block of the H / E kernels streams (chosen from the grid at create; results do not depend on it). */
+int os_fdtd3d_set_x_chunk(OsFdtd3D *h, int32_t planes);
 int os_fdtd3d_last_advance_ms(OsFdtd3D *h, float *ms);
 int os_fdtd3d_launch_count(OsFdtd3D *h, int64_t *launches);
 int os_fdtd3d_step_count(OsFdtd3D *h, int64_t *n_step);

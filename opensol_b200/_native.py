@@ -121,6 +121,7 @@ SIGNATURES = {
     'os_fdtd3d_reset': [_P],
     'os_fdtd3d_synchronize': [_P],
     'os_fdtd3d_set_stream': [_P, _P],
+    'os_fdtd3d_set_x_chunk': [_P, _I32],
     'os_fdtd3d_last_advance_ms': [_P, ctypes.POINTER(ctypes.c_float)],
     'os_fdtd3d_launch_count': [_P, ctypes.POINTER(_I64)],
     'os_fdtd3d_step_count': [_P, ctypes.POINTER(_I64)],

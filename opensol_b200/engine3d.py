@@ -288,6 +288,10 @@ class FDTDEngine3D:
     def synchronize(self):
         _native.check(_native.load().os_fdtd3d_synchronize(self.handle))
 
+    def set_x_chunk(self, planes):
+        """x planes per block of the H / E kernels (speed only)."""
+        _native.check(_native.load().os_fdtd3d_set_x_chunk(self.handle, int(planes)))
+
     def set_stream(self, cuda_stream):
         _native.check(_native.load().os_fdtd3d_set_stream(self.handle, cuda_stream or None))
 
