@@ -185,6 +185,18 @@ int os_fdtd2d_add_tfsf(OsFdtd2D *h, int32_t x0, int32_t x1, int32_t y0, int32_t 
 int os_fdtd2d_add_pole(OsFdtd2D *h, int32_t kind, int32_t i0, int32_t i1, int32_t j0, int32_t j1, float damping,
                        float restoring, const float *drive, float inv_dt, int32_t *pole_id);
 
+/* Dispersive pole on one E face set of an H_z engine (FDTDEngine2D_Hz.add_drude / add_lorentz, fdtd_hz_2d.py:441-472,
+ * updates and corrections :286-325): component 0 = E_x (hi-y faces), 1 = E_y (hi-x faces), on the face box
+ * [i0, i1) x [j0, j1); drive = float32(drive coefficient) x the face weight of each face of the box (the width-
+ * weighted face average of the pole's cell mask, _pole_faces :547-570).  Kind 0 Drude: J += damping J + drive E^n
+ * before the E update, E -= cb J after it; kind 1 Lorentz: dP += damping dP - restoring P + drive E^n, P += dP,
+ * E -= cb inv_dt dP; cb of the face set.  Face sets act in add order, all Drude sets before all Lorentz ones, the
+ * corrections ahead of the sheet sources.  An engine with poles advances with the per-half-step kernels.  H_z
+ * engines only; not in batched advances.  At most 64 face sets. */
+int os_fdtd2d_hz_add_pole(OsFdtd2D *h, int32_t kind, int32_t component, int32_t i0, int32_t i1, int32_t j0,
+                          int32_t j1, float damping, float restoring, const float *drive, float inv_dt,
+                          int32_t *pole_id);
+
 /* Field probe: one component (OS_EZ / OS_HX / OS_HY, or OS_HZ_* on an H_z handle) of cell (ix, iy) recorded after
  * every step from the current one on: FieldProbe.record at t_full (core/monitors.py:194-243, fdtd_2d_base.py:481-487).
  * At most 8.  An advance with probes runs one step per launch.  Not in batched advances; os_fdtd2d_advance_noalloc

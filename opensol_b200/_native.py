@@ -81,6 +81,8 @@ SIGNATURES = {
     'os_fdtd2d_add_probe': [_P, _I32, _I32, _I32, ctypes.POINTER(_I32)],
     'os_fdtd2d_add_pole': [_P, _I32, _I32, _I32, _I32, _I32, ctypes.c_float, ctypes.c_float, _F, ctypes.c_float,
                            ctypes.POINTER(_I32)],
+    'os_fdtd2d_hz_add_pole': [_P, _I32, _I32, _I32, _I32, _I32, _I32, ctypes.c_float, ctypes.c_float, _F,
+                              ctypes.c_float, ctypes.POINTER(_I32)],
     'os_fdtd2d_add_tfsf': [_P, _I32, _I32, _I32, _I32, _I32, _I32, _I32, _F, _F, ctypes.c_float, ctypes.c_float, _F, _F,
                            ctypes.POINTER(_I32)],
     'os_fdtd2d_read_probe': [_P, _I32, _F, _I64, ctypes.POINTER(_I64)],

@@ -56,6 +56,7 @@ struct Tfsf2D {
 // Drude (kind 0) or Lorentz (kind 1) pole on a cell box: drive (box, pole drive x cell mask) and its state.
 struct Pole2D {
     int32_t kind, i0, i1, j0, j1;
+    int32_t comp = 0;                   // field of an H_z engine's face set: 0 E_x (hi-y faces), 1 E_y (hi-x faces)
     float damping, restoring;
     DeviceArray<float> drive, a, b;     // Drude: a = J; Lorentz: a = P, b = dP
 };
@@ -1217,6 +1218,47 @@ static int pole_corrections(OsFdtd2D *h) {
     return OS_OK;
 }
 
+// H_z engine: J / P of every pole face set from E^n (fdtd_hz_2d.py:286-309), every Drude set in add order, then every
+// Lorentz one; the drive array carries drive x face weight.
+static int hz_pole_updates(OsFdtd2D *h) {
+    const int ny = h->grid.ny, c = h->cur;
+    for (int pass = 0; pass < 2; ++pass)
+        for (auto &q : h->poles) {
+            if (q->kind != pass) continue;
+            const float *e = q->comp == 0 ? h->hx[c].ptr : h->hy[c].ptr;
+            const int64_t cells = (int64_t)(q->i1 - q->i0) * (q->j1 - q->j0);
+            const unsigned blocks = (unsigned)((cells + 255) / 256);
+            if (q->kind == 0)
+                ez2d_drude_j_kernel<<<blocks, 256, 0, h->stream>>>(e, ny, q->i0, q->i1, q->j0, q->j1, q->damping,
+                                                                   q->drive.ptr, q->a.ptr, nullptr, 0);
+            else
+                ez2d_lorentz_p_kernel<<<blocks, 256, 0, h->stream>>>(e, ny, q->i0, q->i1, q->j0, q->j1, q->damping,
+                                                                     q->restoring, q->drive.ptr, q->a.ptr, q->b.ptr);
+            h->launches += 1;
+        }
+    OS_CUDA(cudaGetLastError());
+    return OS_OK;
+}
+
+// H_z engine: the E corrections after the E update (fdtd_hz_2d.py:311-325), face set by face set: Drude
+// E -= cb J (written E - (cb * 1) J, the same bits), then Lorentz E -= cb inv_dt dP, cb of the set's faces.
+static int hz_pole_corrections(OsFdtd2D *h) {
+    const int ny = h->grid.ny, c = h->cur;
+    for (int pass = 0; pass < 2; ++pass)
+        for (auto &q : h->poles) {
+            if (q->kind != pass) continue;
+            float *e = q->comp == 0 ? h->hx[c].ptr : h->hy[c].ptr;
+            const float *cb = q->comp == 0 ? h->cb.ptr : h->cb_y.ptr;
+            const int64_t cells = (int64_t)(q->i1 - q->i0) * (q->j1 - q->j0);
+            ez2d_pole_correct_kernel<<<(unsigned)((cells + 255) / 256), 256, 0, h->stream>>>(
+                e, ny, q->i0, q->i1, q->j0, q->j1, cb, nullptr, q->kind == 0 ? q->a.ptr : q->b.ptr,
+                q->kind == 0 ? 1.0f : h->inv_dt);
+            h->launches += 1;
+        }
+    OS_CUDA(cudaGetLastError());
+    return OS_OK;
+}
+
 // Per-half-step chunk (variant 0): H kernel, E kernel, DFT of sample steps; fields updated in place.
 static int advance_per_step(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples,
                             const float *values, const float *phase_table) {
@@ -1458,12 +1500,13 @@ static int advance_hz(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_
                          (unsigned)((nx + cell_block.y - 1) / cell_block.y));
     const HzPlan plan = hz_plan(h);
     for (int64_t k = 0; k < n_steps; ++k) {
-        const int in = h->cur, out = (h->variant == 0 || !h->tfsf.empty()) ? h->cur : h->cur ^ 1;
+        const bool per_half = h->variant == 0 || !h->tfsf.empty() || !h->poles.empty();
+        const int in = h->cur, out = per_half ? h->cur : h->cur ^ 1;
         Hz2DParams p = make_hz_params(h, in, out);
         p.line_values = values;
         p.values_stride = n_steps;
         p.k_step = k;
-        if (h->variant == 0 || !h->tfsf.empty()) {   // a TFSF box acts between the half steps
+        if (per_half) {   // a TFSF box and the poles act between the half steps
             OS_TRY(prof_begin(h, 3, h->stream));
             hz2d_h_kernel<<<cell_grid, cell_block, 0, h->stream>>>(p);
             for (auto &t : h->tfsf) {   // TFSFSourceHz.inject_magnetic (fdtd_hz_2d.py:160-163)
@@ -1475,7 +1518,21 @@ static int advance_hz(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_
                     t->aux_ez.ptr, t->aux_coef_h.ptr, t->aux_hy.ptr + 1, t->aux_n);
                 h->launches += 2;
             }
-            hz2d_e_kernel<<<cell_grid, cell_block, 0, h->stream>>>(p);
+            if (h->poles.empty()) {
+                hz2d_e_kernel<<<cell_grid, cell_block, 0, h->stream>>>(p);
+            } else {
+                // poles (fdtd_hz_2d.py:233-284): J / P from E^n, the E update (its sheets held back), the pole
+                // corrections, then the sheets
+                Hz2DParams p_no_lines = p;
+                p_no_lines.n_lines = 0;
+                OS_TRY(hz_pole_updates(h));
+                hz2d_e_kernel<<<cell_grid, cell_block, 0, h->stream>>>(p_no_lines);
+                OS_TRY(hz_pole_corrections(h));
+                if (p.n_lines) {
+                    hz2d_line_inject_kernel<<<cell_grid, cell_block, 0, h->stream>>>(p);
+                    h->launches += 1;
+                }
+            }
             for (size_t b = 0; b < h->tfsf.size(); ++b) {   // TFSFSourceHz.inject_electric (fdtd_hz_2d.py:171-174)
                 Tfsf2D &t = *h->tfsf[b];
                 const int side = std::max(t.x1 - t.x0, t.y1 - t.y0);
@@ -1894,6 +1951,35 @@ extern "C" int os_fdtd2d_add_pole(OsFdtd2D *h, int32_t kind, int32_t i0, int32_t
         int32_t *u = h->drude_box;
         if (u[1] == u[0]) u[0] = i0, u[1] = i1, u[2] = j0, u[3] = j1;
         else u[0] = std::min(u[0], i0), u[1] = std::max(u[1], i1), u[2] = std::min(u[2], j0), u[3] = std::max(u[3], j1);
+    }
+    if (pole_id) *pole_id = (int32_t)h->poles.size();
+    h->poles.push_back(std::move(q));
+    return OS_OK;
+}
+
+extern "C" int os_fdtd2d_hz_add_pole(OsFdtd2D *h, int32_t kind, int32_t component, int32_t i0, int32_t i1, int32_t j0,
+                                     int32_t j1, float damping, float restoring, const float *drive, float inv_dt,
+                                     int32_t *pole_id) {
+    OS_TRY(require_hz(h, "os_fdtd2d_hz_add_pole"));
+    OS_CHECK(drive, OS_ERR_INVALID, "os_fdtd2d_hz_add_pole: null drive");
+    OS_CHECK(kind == 0 || kind == 1, OS_ERR_INVALID, "pole kind must be 0 (Drude) or 1 (Lorentz), got %d", kind);
+    OS_CHECK(component == 0 || component == 1, OS_ERR_INVALID, "pole component must be 0 (E_x) or 1 (E_y), got %d",
+             component);
+    OS_CHECK(0 <= i0 && i0 < i1 && i1 <= h->grid.nx && 0 <= j0 && j0 < j1 && j1 <= h->grid.ny, OS_ERR_INVALID,
+             "pole box [%d, %d) x [%d, %d) outside the %d x %d grid", i0, i1, j0, j1, h->grid.nx, h->grid.ny);
+    OS_CHECK(h->poles.size() < 64, OS_ERR_INVALID, "at most 64 pole face sets per engine");
+    OS_TRY(bind_device(h));
+    std::unique_ptr<Pole2D> q(new Pole2D());
+    q->kind = kind, q->comp = component, q->i0 = i0, q->i1 = i1, q->j0 = j0, q->j1 = j1;
+    q->damping = damping, q->restoring = restoring;
+    const size_t n = (size_t)(i1 - i0) * (size_t)(j1 - j0);
+    OS_TRY(upload(q->drive, drive, n, h->stream));
+    OS_TRY(q->a.alloc(n));
+    OS_CUDA(cudaMemsetAsync(q->a.ptr, 0, q->a.bytes(), h->stream));
+    if (kind == 1) {
+        OS_TRY(q->b.alloc(n));
+        OS_CUDA(cudaMemsetAsync(q->b.ptr, 0, q->b.bytes(), h->stream));
+        h->inv_dt = inv_dt;
     }
     if (pole_id) *pole_id = (int32_t)h->poles.size();
     h->poles.push_back(std::move(q));

@@ -191,6 +191,32 @@ __global__ void __launch_bounds__(EZ2D_BLOCK_X *EZ2D_BLOCK_Y) hz2d_e_kernel(cons
     }
 }
 
+// Sheet sources after the E update and the pole corrections (TangentialSheetCurrentSource.inject_electric at
+// t + dt/2): E_x faces (i, position) for axis 0, E_y faces (position, j) for axis 1, each line in add order, a 0 value
+// skipped; the same additions hz2d_ex_at / hz2d_ey_at make inside the E update.
+__global__ void __launch_bounds__(EZ2D_BLOCK_X *EZ2D_BLOCK_Y) hz2d_line_inject_kernel(const Hz2DParams p) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= p.nx || j >= p.ny) return;
+    const size_t idx = (size_t)i * p.ny + j;
+    for (int axis = 0; axis < 2; ++axis) {
+        float *e = axis == 0 ? p.ex_out : p.ey_out;
+        float v = 0.0f;
+        bool hit = false;
+        for (int l = 0; l < p.n_lines; ++l) {
+            const LineSrcDev &L = p.lines[l];
+            if (L.axis != axis) continue;
+            const int along = axis == 0 ? i : j, across = axis == 0 ? j : i;
+            if (across != L.position || along < L.lo || along >= L.hi) continue;
+            const float value = p.line_values[(size_t)l * p.values_stride + p.k_step];
+            if (value == 0.0f) continue;
+            if (!hit) v = e[idx], hit = true;
+            v += value * L.profile[along - L.lo];
+        }
+        if (hit) e[idx] = v;
+    }
+}
+
 // ---------------------------------------------------------------------------------------------- fused step
 
 // cb of a lossless face from the two cells' eps_r and the face shares: the coefficient kernel's arithmetic with

@@ -269,7 +269,7 @@ __global__ void ez2d_drude_j_kernel(const float *__restrict__ ez, int ny, int i0
     const size_t g = (size_t)i * ny + j;
     const float jn = jz[t] + (damping * jz[t] + drive[t] * ez[g]);
     jz[t] = jn;
-    jz_total[g] = store ? jn : jz_total[g] + jn;
+    if (jz_total) jz_total[g] = store ? jn : jz_total[g] + jn;   // NULL: per-pole corrections (H_z face sets)
 }
 
 // Lorentz in velocity form: dP += damping dP - restoring P^n + drive E^n, then P += dP.

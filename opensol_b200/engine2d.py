@@ -16,6 +16,7 @@ from . import _native
 from .boundaries import build_yee_rows, face_shares
 from .constants import DTYPE, EPS0, MU0
 from .monitors import dft_phase_table
+from .poles import pole_face_sets
 
 
 class FDTDEngine2D_Ez:
@@ -106,6 +107,23 @@ class FDTDEngine2D_Ez:
         """Register a Drude / Lorentz pole on a cell box (cropped_mask: its cells); created at the next sync."""
         self._poles.append((pole, box, np.asarray(cropped_mask, dtype=bool)))
 
+    def _pole_coefficients(self, pole):
+        """(kind 0 Drude / 1 Lorentz, damping, restoring, drive) float32 of a pole at this engine's dt."""
+        coefficients = pole.ade_coefficients(float(self.dt))
+        kind = 0 if len(coefficients) == 2 else 1
+        damping, restoring, drive = ((coefficients[0], 0.0, coefficients[1]) if kind == 0 else coefficients)
+        return kind, damping, restoring, drive
+
+    def _create_pole(self, lib, h, pole, box, cropped):
+        """The pole on the device: its cell box with drive = cell mask x drive coefficient."""
+        kind, damping, restoring, drive = self._pole_coefficients(pole)
+        drive_box = np.ascontiguousarray(cropped.astype(DTYPE) * DTYPE(drive))
+        pid = ctypes.c_int32()
+        _native.check(lib.os_fdtd2d_add_pole(h, kind, box[0].start, box[0].stop, box[1].start, box[1].stop,
+                                             float(damping), float(restoring), _native.fptr(drive_box),
+                                             float(DTYPE(1.0 / float(self.dt))), ctypes.byref(pid)))
+        return pid.value
+
     def attach_tfsf(self, source):
         """Register a TFSF plane-wave box; it is created on the device at the next sync."""
         self._tfsf.append(source)
@@ -155,16 +173,7 @@ class FDTDEngine2D_Ez:
                 self._monitor_ids[id(monitor)] = mid.value
         for entry in self._poles:
             if id(entry) not in self._monitor_ids:
-                pole, box, cropped = entry
-                coefficients = pole.ade_coefficients(float(self.dt))
-                kind = 0 if len(coefficients) == 2 else 1
-                damping, restoring, drive = ((coefficients[0], 0.0, coefficients[1]) if kind == 0 else coefficients)
-                drive_box = np.ascontiguousarray(cropped.astype(DTYPE) * DTYPE(drive))
-                pid = ctypes.c_int32()
-                _native.check(lib.os_fdtd2d_add_pole(h, kind, box[0].start, box[0].stop, box[1].start, box[1].stop,
-                                                     float(damping), float(restoring), _native.fptr(drive_box),
-                                                     float(DTYPE(1.0 / float(self.dt))), ctypes.byref(pid)))
-                self._monitor_ids[id(entry)] = pid.value
+                self._monitor_ids[id(entry)] = self._create_pole(lib, h, *entry)
         for source in self._tfsf:
             if id(source) not in self._monitor_ids:
                 tid = ctypes.c_int32()
@@ -423,6 +432,25 @@ class FDTDEngine2D_Hz(FDTDEngine2D_Ez):
         widths_x, widths_y = domain.kernel_widths()
         self.shares_x = face_shares(widths_x, bc.periodic_x)
         self.shares_y = face_shares(widths_y, bc.periodic_y)
+
+    def _create_pole(self, lib, h, pole, box, cropped):
+        """The pole on the device as one face set per E component it reaches (FDTDEngine2D_Hz.add_drude /
+        add_lorentz, fdtd_hz_2d.py:441-472): drive = float32 drive coefficient x face weight on each face box."""
+        kind, damping, restoring, drive = self._pole_coefficients(pole)
+        full = np.zeros((self.nx, self.ny), dtype=bool)
+        full[box] = cropped
+        bc = self.boundary_config
+        ids = []
+        for component, fbox, weight in pole_face_sets(full, self.shares_x, self.shares_y, bc.periodic_x,
+                                                      bc.periodic_y):
+            drive_box = np.ascontiguousarray(DTYPE(drive) * weight)
+            pid = ctypes.c_int32()
+            _native.check(lib.os_fdtd2d_hz_add_pole(h, kind, component, fbox[0].start, fbox[0].stop, fbox[1].start,
+                                                    fbox[1].stop, float(damping), float(restoring),
+                                                    _native.fptr(drive_box), float(DTYPE(1.0 / float(self.dt))),
+                                                    ctypes.byref(pid)))
+            ids.append(pid.value)
+        return tuple(ids)
 
     def _upload_materials(self, lib, h, materials):
         arrays = [materials.get(name) for name in ('eps_xx', 'eps_yy', 'sigma_e', 'mu_r', 'sigma_m')]

@@ -178,10 +178,10 @@ class EMPhysics:
                 source.profile = calibrate_tangential_sheet(
                     source, self.domain.materials, omega, width, dt,
                     self.engine.shares_y if normal == 1 else self.engine.shares_x,
-                    self.domain.kernel_widths()[normal])
+                    self.domain.kernel_widths()[normal], self.dispersive_regions)
         self._calibration_dirty = False
 
-    # --- dispersive poles (E_z) ---------------------------------------------------------------------------
+    # --- dispersive poles ---------------------------------------------------------------------------
     def add_drude_rectangle(self, x0, y0, x1, y1, drude):
         """Drude medium on the cells of the rectangle, its eps_inf written as their eps_r
         (physics/em/__init__.py:329-340)."""
@@ -200,8 +200,9 @@ class EMPhysics:
         self._add_pole(pole, mask, set_background=False)
 
     def _add_pole(self, pole, mask, set_background):
-        if self.polarization != 'ez':
-            raise NotImplementedError('dispersive poles are built for the E_z engine only')
+        """The pole on its mask's bounding box (the E_z engine steps it on the cells, the H_z engine on the face
+        sets of E_x / E_y the mask reaches); set_background writes eps_inf into every permittivity array of the
+        polarisation under the mask (FDTDEngine2D_Ez / _Hz.add_drude)."""
         grid = self.domain.grid
         full = mask.full((grid.nx, grid.ny)) if hasattr(mask, 'full') else np.asarray(mask, dtype=bool)
         if full.shape != (grid.nx, grid.ny):
@@ -211,8 +212,10 @@ class EMPhysics:
             self.engine.attach_pole(pole, box, full[box])
             self.dispersive_regions.append((pole, box, full[box]))
         if set_background:
-            self.domain.materials.assign('eps_r', full, pole.eps_inf)
-            self.materials_changed(('eps_r',))
+            names = ('eps_r',) if self.polarization == 'ez' else ('eps_xx', 'eps_yy')
+            for name in names:
+                self.domain.materials.assign(name, full, pole.eps_inf)
+            self.materials_changed(names)
         self._calibration_dirty = True
 
     # --- material helpers --------------------------------------------------------------------------------

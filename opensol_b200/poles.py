@@ -80,3 +80,28 @@ def bounding_box(mask):
         return None
     cols = np.flatnonzero(mask.any(axis=0))
     return slice(int(rows[0]), int(rows[-1]) + 1), slice(int(cols[0]), int(cols[-1]) + 1)
+
+
+def pole_face_sets(full_mask, shares_x, shares_y, periodic_x, periodic_y):
+    """[(component, face box, float32 face weights on the box)] of a pole's cell mask on the H_z engine's E face sets
+    (_pole_faces, fdtd_hz_2d.py:547-570): component 0 = E_x (hi-y faces), 1 = E_y (hi-x faces); weight = the
+    width-weighted face average of the float32 mask, cell x lower share + partner x upper share (the partner wraps on
+    a periodic axis and is the cell itself on the last face of an open one, yee_grid.py:119-142), boxed on the faces
+    whose weight is > 0; a set without such faces is left out."""
+    cell = np.asarray(full_mask, dtype=bool).astype(DTYPE)
+    nx, ny = cell.shape
+
+    def partners(n, periodic):
+        idx = np.arange(n)
+        return np.roll(idx, -1) if periodic else np.concatenate((idx[1:], idx[-1:]))
+
+    lo_y, up_y = (np.asarray(a, dtype=DTYPE) for a in shares_y)
+    lo_x, up_x = (np.asarray(a, dtype=DTYPE) for a in shares_x)
+    weights = (cell * lo_y + cell[:, partners(ny, periodic_y)] * up_y,
+               cell * lo_x[:, None] + cell[partners(nx, periodic_x)] * up_x[:, None])
+    sets = []
+    for component, weight in enumerate(weights):
+        box = bounding_box(weight > 0)
+        if box is not None:
+            sets.append((component, box, np.ascontiguousarray(weight[box])))
+    return sets

@@ -150,6 +150,21 @@ def e_coefficients_host(eps_r, sigma_e, dt):
     return (1.0 - k) / denom, (dt / eps) / denom
 
 
+def _add_pole_susceptibility(line_eps, axis, position, lo, hi, dispersive_regions, omega):
+    """Add to the complex eps of the cells [lo, hi) of a grid line (axis 'x': along x at y-cell `position`) the
+    susceptibility chi(omega) of every pole region on them, times the region's cell mask there
+    (_line_cell_permittivity, physics/em/sources.py:401-427)."""
+    for pole, box, cropped in dispersive_regions:
+        chi = complex(pole.susceptibility(omega))
+        along_box, normal_box = (box[0], box[1]) if axis == 'x' else (box[1], box[0])
+        start, stop = max(lo, along_box.start), min(hi, along_box.stop)
+        if not (normal_box.start <= position < normal_box.stop and start < stop):
+            continue
+        along, normal = slice(start - along_box.start, stop - along_box.start), position - normal_box.start
+        mask_line = cropped[along, normal] if axis == 'x' else cropped[normal, along]
+        line_eps[start - lo:stop - lo] += chi * mask_line
+
+
 def calibrate_line_source(source, materials, omega, normal_width, dt, dispersive_regions=()):
     """float32 profile of an E_z sheet current (SheetCurrentCalibration.apply for a LineSource,
     physics/em/sources.py:582-602): cb * admittance * 2 / (eta0 w_perp) on the line cells; the line's eps(omega)
@@ -169,25 +184,19 @@ def calibrate_line_source(source, materials, omega, normal_width, dt, dispersive
     eps_line, sigma_line = cells('eps_r'), cells('sigma_e')
     _, cb_line = e_coefficients_host(eps_line, sigma_line, dt)
     line_eps = eps_line.astype(np.complex128) - 1j * sigma_line.astype(np.float64) / (omega * EPS0)
-    for pole, box, cropped in dispersive_regions:
-        chi = complex(pole.susceptibility(omega))
-        along_box, normal_box = (box[0], box[1]) if source.axis == 'x' else (box[1], box[0])
-        start, stop = max(lo, along_box.start), min(hi, along_box.stop)
-        if not (normal_box.start <= source.position < normal_box.stop and start < stop):
-            continue
-        along, normal = slice(start - along_box.start, stop - along_box.start), source.position - normal_box.start
-        mask_line = cropped[along, normal] if source.axis == 'x' else cropped[normal, along]
-        line_eps[start - lo:stop - lo] += chi * mask_line
+    _add_pole_susceptibility(line_eps, source.axis, source.position, lo, hi, dispersive_regions, omega)
     admittance = sheet_admittance(line_eps, cells('mu_r'), cells('sigma_m'), omega, normal_width, dt)
     weight = np.asarray(2.0 * np.ones(hi - lo) / (float(ETA0) * normal_width), dtype=DTYPE)
     return (cb_line * admittance * weight).astype(DTYPE)
 
 
-def calibrate_tangential_sheet(source, materials, omega, normal_spacing, dt, shares, normal_widths):
+def calibrate_tangential_sheet(source, materials, omega, normal_spacing, dt, shares, normal_widths,
+                               dispersive_regions=()):
     """float32 profile of an H_z in-plane sheet current on the hi faces of its line cells (SheetCurrentCalibration.apply
     for a TangentialSheetCurrentSource, physics/em/sources.py:582-602): cb of the E_x (axis 'x') / E_y (axis 'y') faces
     * admittance of the width-weighted face permittivity * 2 / (eta0 w_perp).  `shares` = the (lower, upper) face
-    weights and `normal_widths` the kernel cell widths of the axis across the line."""
+    weights and `normal_widths` the kernel cell widths of the axis across the line; each row's eps(omega) includes the
+    susceptibility of the pole regions on its cells."""
     lo, hi = source.span
     n = len(normal_widths)
     lower_row, upper_row = source.position, (source.position + 1) % n
@@ -206,8 +215,10 @@ def calibrate_tangential_sheet(source, materials, omega, normal_spacing, dt, sha
     _, cb_line = e_coefficients_host(eps_face, sigma_face, dt)
 
     def row_permittivity(r):
-        return (row(eps_name, r).astype(np.complex128)
-                - 1j * row('sigma_e', r).astype(np.float64) / (omega * EPS0))
+        eps = (row(eps_name, r).astype(np.complex128)
+               - 1j * row('sigma_e', r).astype(np.float64) / (omega * EPS0))
+        _add_pole_susceptibility(eps, source.axis, r, lo, hi, dispersive_regions, omega)
+        return eps
 
     w_lo, w_hi = float(normal_widths[lower_row]), float(normal_widths[upper_row])
     line_eps = (row_permittivity(lower_row) * w_lo + row_permittivity(upper_row) * w_hi) / (w_lo + w_hi)

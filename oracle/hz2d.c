@@ -66,6 +66,61 @@ typedef struct {
     const float *values;
 } OracleTfsfHz;
 
+/* A Drude / Lorentz pole on one E face set (fdtd_hz_2d.py:441-472,547-570): comp 0 = E_x (hi-y faces), 1 = E_y
+ * (hi-x faces); drive = the pole's drive coefficient times the face weight (the face average of its cell mask) on
+ * the box, so faces outside the medium keep J = 0 / P = 0. */
+typedef struct {
+    int32_t kind, comp;                       /* kind 0 Drude, 1 Lorentz */
+    int32_t i0, i1, j0, j1;                   /* face box */
+    real damping, restoring;
+    const real *drive;                        /* (box) drive x face weight */
+    real *a, *b;                              /* Drude: a = J; Lorentz: a = P, b = dP (box) */
+} OraclePoleHz;
+
+/* _pole_updates (fdtd_hz_2d.py:286-309) from E^n: every Drude face set in add order, then every Lorentz one. */
+static void hz_poles_update(const OracleHz2D *s, int32_t n_poles, const OraclePoleHz *poles)
+{
+    const size_t ny = (size_t)s->ny;
+    for (int pass = 0; pass < 2; ++pass)
+        for (int q = 0; q < n_poles; ++q) {
+            const OraclePoleHz *p = &poles[q];
+            if (p->kind != pass) continue;
+            const real *e = p->comp == 0 ? s->ex : s->ey;
+            const int w = p->j1 - p->j0;
+            for (int i = p->i0; i < p->i1; ++i)
+                for (int j = p->j0; j < p->j1; ++j) {
+                    const size_t t = (size_t)(i - p->i0) * w + (j - p->j0), g = (size_t)i * ny + j;
+                    if (p->kind == 0) {
+                        p->a[t] += p->damping * p->a[t] + p->drive[t] * e[g];
+                    } else {
+                        p->b[t] += p->damping * p->b[t] - p->restoring * p->a[t] + p->drive[t] * e[g];
+                        p->a[t] += p->b[t];
+                    }
+                }
+        }
+}
+
+/* _pole_corrections (fdtd_hz_2d.py:311-325): E -= cb J per Drude face set, then E -= cb inv_dt dP per Lorentz one,
+ * cb of the face set (cb_x / cb_y). */
+static void hz_poles_correct(const OracleHz2D *s, int32_t n_poles, const OraclePoleHz *poles, real inv_dt)
+{
+    const size_t ny = (size_t)s->ny;
+    for (int pass = 0; pass < 2; ++pass)
+        for (int q = 0; q < n_poles; ++q) {
+            const OraclePoleHz *p = &poles[q];
+            if (p->kind != pass) continue;
+            real *e = p->comp == 0 ? s->ex : s->ey;
+            const real *cb = p->comp == 0 ? s->cb_x : s->cb_y;
+            const int w = p->j1 - p->j0;
+            for (int i = p->i0; i < p->i1; ++i)
+                for (int j = p->j0; j < p->j1; ++j) {
+                    const size_t t = (size_t)(i - p->i0) * w + (j - p->j0), g = (size_t)i * ny + j;
+                    if (p->kind == 0) e[g] -= cb[g] * p->a[t];
+                    else e[g] -= cb[g] * inv_dt * p->b[t];
+                }
+        }
+}
+
 /* inject_magnetic: H_z corrections from the incident E_y, then aux_hz[k] += coef[k - 1] (aux_ey[k] - aux_ey[k - 1]). */
 static void tfsf_h(const OracleHz2D *s, const OracleTfsfHz *t)
 {
@@ -231,17 +286,22 @@ static void accumulate_flux(const OracleHz2D *s, OracleFluxHz *m, int64_t sample
     }
 }
 
-int oracle_hz2d_advance_tfsf(OracleHz2D *s, int64_t step0, int64_t n_steps, int32_t n_lines,
+/* One chunk of FDTDEngine2D_Hz.advance (fdtd_hz_2d.py:143-198, 233-284): H_z + CPML, TFSF H side, pole updates from
+ * E^n, E_x / E_y + CPML, pole corrections, sheet sources, TFSF E side, flux samples. */
+int oracle_hz2d_advance_full(OracleHz2D *s, int64_t step0, int64_t n_steps, int32_t n_lines,
                              const OracleLineHz *lines, int32_t n_monitors, OracleFluxHz *monitors,
-                             int64_t sample_interval, int32_t n_tfsf, const OracleTfsfHz *tfsf) {
+                             int64_t sample_interval, int32_t n_tfsf, const OracleTfsfHz *tfsf, int32_t n_poles,
+                             const OraclePoleHz *poles, real inv_dt) {
     for (int64_t k = 0; k < n_steps; ++k) {
         update_hz(s);
         for (int side = 0; side < 4; ++side)
             if (s->cpml_active[side]) cpml_side(s, side, 1);
         for (int b = 0; b < n_tfsf; ++b) tfsf_h(s, &tfsf[b]);
+        if (n_poles) hz_poles_update(s, n_poles, poles);
         update_exy(s);
         for (int side = 0; side < 4; ++side)
             if (s->cpml_active[side]) cpml_side(s, side, 0);
+        if (n_poles) hz_poles_correct(s, n_poles, poles, inv_dt);
         for (int l = 0; l < n_lines; ++l) inject_line(s, &lines[l], k);
         for (int b = 0; b < n_tfsf; ++b) tfsf_e(s, &tfsf[b], k);
         const int64_t n_step = step0 + k + 1;
@@ -257,7 +317,15 @@ int oracle_hz2d_advance_tfsf(OracleHz2D *s, int64_t step0, int64_t n_steps, int3
     return 0;
 }
 
+int oracle_hz2d_advance_tfsf(OracleHz2D *s, int64_t step0, int64_t n_steps, int32_t n_lines,
+                             const OracleLineHz *lines, int32_t n_monitors, OracleFluxHz *monitors,
+                             int64_t sample_interval, int32_t n_tfsf, const OracleTfsfHz *tfsf) {
+    return oracle_hz2d_advance_full(s, step0, n_steps, n_lines, lines, n_monitors, monitors, sample_interval, n_tfsf,
+                                    tfsf, 0, 0, (real)0);
+}
+
 int oracle_hz2d_advance(OracleHz2D *s, int64_t step0, int64_t n_steps, int32_t n_lines, const OracleLineHz *lines,
                         int32_t n_monitors, OracleFluxHz *monitors, int64_t sample_interval) {
-    return oracle_hz2d_advance_tfsf(s, step0, n_steps, n_lines, lines, n_monitors, monitors, sample_interval, 0, 0);
+    return oracle_hz2d_advance_full(s, step0, n_steps, n_lines, lines, n_monitors, monitors, sample_interval, 0, 0,
+                                    0, 0, (real)0);
 }

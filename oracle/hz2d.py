@@ -28,7 +28,7 @@ import os
 
 import numpy as np
 
-from oracle.fdtd2d import (DTYPE, EPS0, ETA0, LIB_DIR, MU0, OracleEz2D, _make_structs, _ptr, build_cpml,
+from oracle.fdtd2d import (DTYPE, EPS0, ETA0, LIB_DIR, MU0, OracleDrude, OracleEz2D, _make_structs, _ptr, build_cpml,
                            dft_phases, dft_sample_interval, h_coefficients, paint_circle, paint_rect, sheet_admittance,
                            yee_inverse_spacings)
 
@@ -130,6 +130,7 @@ class OracleHz2D(OracleEz2D):
         self.ex = np.zeros(shape, dtype=self.real)
         self.ey = np.zeros(shape, dtype=self.real)
         del self.ez, self.hx, self.hy
+        self.pole_faces = []   # [pole, comp (0 E_x, 1 E_y), face box, weight on the box, + states] in add order
 
     def add_dielectric_rectangle(self, x0, y0, x1, y1, eps_r, sigma_e=0.0):
         for array in (self.eps_xx, self.eps_yy):
@@ -181,9 +182,20 @@ class OracleHz2D(OracleEz2D):
             def row(array, r, src=src):
                 return array[src.lo:src.hi, r] if src.axis == 'x' else array[r, src.lo:src.hi]
 
-            def row_eps(r):
-                return (np.asarray(row(cell_eps, r), dtype=np.complex128)
-                        - 1j * np.asarray(row(self.sigma_e, r), dtype=np.float64) / (omega * EPS0))
+            def row_eps(r, src=src, cell_eps=cell_eps, omega=omega):
+                eps = (np.asarray(row(cell_eps, r), dtype=np.complex128)
+                       - 1j * np.asarray(row(self.sigma_e, r), dtype=np.float64) / (omega * EPS0))
+                # the susceptibility of every pole region on the row's cells (sources.py:401-427)
+                for pole, box, cropped in self.poles:
+                    along_box, normal_box = (box[0], box[1]) if src.axis == 'x' else (box[1], box[0])
+                    start, stop = max(src.lo, along_box.start), min(src.hi, along_box.stop)
+                    if not (normal_box.start <= r < normal_box.stop and start < stop):
+                        continue
+                    along = slice(start - along_box.start, stop - along_box.start)
+                    mask_line = cropped[along, r - normal_box.start] if src.axis == 'x' else \
+                        cropped[r - normal_box.start, along]
+                    eps[start - src.lo:stop - src.lo] += pole.susceptibility(omega) * mask_line
+                return eps
 
             line_eps = (row_eps(lower_row) * w_lo + row_eps(upper_row) * w_hi) / (w_lo + w_hi)
             admittance = sheet_admittance(line_eps, row(self.mu_r, src.position), row(self.sigma_m, src.position),
@@ -197,6 +209,60 @@ class OracleHz2D(OracleEz2D):
         self.psi_e = {s.name: np.zeros(self._psi_shape(s.name), dtype=real) for s in self.cpml_sides}
         self.psi_h = {s.name: np.zeros(self._psi_shape(s.name), dtype=real) for s in self.cpml_sides}
         self._finalized = True
+
+    def _add_pole(self, pole, mask, set_background):
+        """FDTDEngine2D_Hz.add_drude / add_lorentz (fdtd_hz_2d.py:441-472) with _pole_faces (:547-570): the cell region
+        (its bounding box and cropped mask, for the sheet calibration's susceptibility) and, per E face set, the face
+        average of the float32 cell mask (width-weighted hi-face mean, yee_grid.py:128-142) on the bounding box of its
+        positive faces (fdtd_2d_base.py:29-36); set_background writes eps_inf into eps_xx and eps_yy."""
+        mask = np.asarray(mask, dtype=bool)
+        d = self.domain
+        rows = np.flatnonzero(mask.any(axis=1))
+        if rows.size:
+            cols = np.flatnonzero(mask.any(axis=0))
+            box = (slice(int(rows[0]), int(rows[-1]) + 1), slice(int(cols[0]), int(cols[-1]) + 1))
+            self.poles.append([pole, box, mask[box].copy()])
+        cell = mask.astype(DTYPE)
+        lo_y, up_y = face_shares(d.kernel_widths[1], d.periodic_y, DTYPE)
+        lo_x, up_x = face_shares(d.kernel_widths[0], d.periodic_x, DTYPE)
+        pj, pi = partner_index(d.ny, d.periodic_y), partner_index(d.nx, d.periodic_x)
+        weights = (cell * lo_y + cell[:, pj] * up_y, cell * lo_x[:, None] + cell[pi] * up_x[:, None])
+        for comp, weight in enumerate(weights):
+            positive = weight > 0
+            face_rows = np.flatnonzero(positive.any(axis=1))
+            if face_rows.size == 0:
+                continue
+            face_cols = np.flatnonzero(positive.any(axis=0))
+            fbox = (slice(int(face_rows[0]), int(face_rows[-1]) + 1), slice(int(face_cols[0]), int(face_cols[-1]) + 1))
+            self.pole_faces.append([pole, comp, fbox, weight[fbox].copy()])
+        if set_background:
+            self.eps_xx[mask] = DTYPE(pole.eps_inf)
+            self.eps_yy[mask] = DTYPE(pole.eps_inf)
+
+    def _pole_face_structs(self, R):
+        """ctypes records of the pole face sets (states kept across chunks) and float32 1 / dt."""
+        P = ctypes.POINTER(R)
+
+        class PoleHz(ctypes.Structure):
+            _fields_ = [('kind', ctypes.c_int32), ('comp', ctypes.c_int32), ('i0', ctypes.c_int32),
+                        ('i1', ctypes.c_int32), ('j0', ctypes.c_int32), ('j1', ctypes.c_int32), ('damping', R),
+                        ('restoring', R), ('drive', P), ('a', P), ('b', P)]
+
+        dt = float(self.domain.dt)
+        records = (PoleHz * max(1, len(self.pole_faces)))()
+        for q, entry in enumerate(self.pole_faces):
+            pole, comp, box, weight = entry[:4]
+            if len(entry) == 4:   # first chunk: drive x weight and zero states
+                damping, restoring, drive = pole.coefficients(dt)
+                entry.extend([DTYPE(drive) * weight, np.zeros(weight.shape, DTYPE), np.zeros(weight.shape, DTYPE),
+                              damping, restoring])
+            drive_box, a, b, damping, restoring = entry[4:]
+            rec = records[q]
+            rec.kind = 0 if isinstance(pole, OracleDrude) else 1
+            rec.comp, rec.damping, rec.restoring = comp, float(damping), float(restoring)
+            rec.i0, rec.i1, rec.j0, rec.j1 = box[0].start, box[0].stop, box[1].start, box[1].stop
+            rec.drive, rec.a, rec.b = _ptr(drive_box, R), _ptr(a, R), _ptr(b, R)
+        return records, PoleHz, float(DTYPE(1.0 / dt))
 
     def add_dft_monitor(self, x0, y0, x1, y1, wavelengths=None, frequencies=None, downsample=1):
         """DFTMonitor for 'hz' (physics/em/monitors.py:276-284): H_z, E_x and E_y maps of the sampled cells."""
@@ -290,12 +356,15 @@ class OracleHz2D(OracleEz2D):
         lines = self._line_structs(Line, values)
         fluxes = self._flux_structs(Flux, phase_tables, first_q, n_q)
         boxes, TfsfHz = self._tfsf_hz_structs(R, n_steps)
-        lib.oracle_hz2d_advance_tfsf.restype = ctypes.c_int
-        lib.oracle_hz2d_advance_tfsf.argtypes = [ctypes.POINTER(State), ctypes.c_int64, ctypes.c_int64, ctypes.c_int32,
+        poles, PoleHz, inv_dt = self._pole_face_structs(R)
+        lib.oracle_hz2d_advance_full.restype = ctypes.c_int
+        lib.oracle_hz2d_advance_full.argtypes = [ctypes.POINTER(State), ctypes.c_int64, ctypes.c_int64, ctypes.c_int32,
                                                  ctypes.POINTER(Line), ctypes.c_int32, ctypes.POINTER(Flux),
-                                                 ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(TfsfHz)]
-        rc = lib.oracle_hz2d_advance_tfsf(ctypes.byref(st), self.n_step, n_steps, len(self.sources), lines,
-                                          len(self.monitors), fluxes, self.sample_interval, len(self.tfsf), boxes)
+                                                 ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(TfsfHz),
+                                                 ctypes.c_int32, ctypes.POINTER(PoleHz), R]
+        rc = lib.oracle_hz2d_advance_full(ctypes.byref(st), self.n_step, n_steps, len(self.sources), lines,
+                                          len(self.monitors), fluxes, self.sample_interval, len(self.tfsf), boxes,
+                                          len(self.pole_faces), poles, inv_dt)
         del keep
         if rc != 0:
             raise RuntimeError('oracle phase table does not cover a sample')

@@ -154,6 +154,42 @@ CASES_DFT_HZ = [
         'probes': [[1.2e-6, 0.0, 'ey']],
         'checkpoints': [300, 600],
     },
+    {   # H_z poles: a Drude rectangle and a Lorentz circle on E_x / E_y face sets (face-averaged cell masks), all
+        # CPML; the E_y sheet crosses the Lorentz circle (its calibration takes the pole's susceptibility); probes of
+        # E_x / E_y inside the metal
+        'name': 'poles_hz_pml',
+        'sim': {'size_x': 1.6e-6, 'size_y': 1.4e-6, 'dx': 25e-9, 'npml': 10, 'boundaries': 'pml',
+                'polarization': 'hz'},
+        'ops': [
+            ['add_dielectric_circle', [0.5e-6, 0.9e-6, 0.15e-6], {'eps_r': 2.0}],
+            ['add_line_source', ['y', 0.5e-6], {'wavelength': 800e-9, 'bandwidth': 0.5, 'span': [0.2e-6, 1.2e-6]}],
+            ['add_flux_monitor', ['y', 1.4e-6, [0.1e-6, 1.3e-6]], {'wavelengths': [750e-9, 850e-9]}],
+        ],
+        'poles': [['drude_rect', [0.9e-6, 0.4e-6, 1.2e-6, 1.0e-6], [8e15, 5e13, 2.0]],
+                  ['lorentz_circle', [0.5e-6, 0.9e-6, 0.15e-6], [1.5, 3e15, 2e14]]],
+        'dft': [
+            [0.6e-6, 0.2e-6, 1.5e-6, 1.2e-6, [3.8e14], 2],
+        ],
+        'probes': [[1.0e-6, 0.7e-6, 'ex'], [1.1e-6, 0.5e-6, 'ey'], [0.5e-6, 0.9e-6, 'hz']],
+        'checkpoints': [300, 700],
+    },
+    {   # two overlapping Drude media (each face set corrected in turn) on a periodic y axis, one spanning the whole
+        # y range (its last E_x faces pair with the wrapped first cells); an E_x sheet
+        'name': 'poles_hz_periodic_y',
+        'sim': {'size_x': 1.6e-6, 'size_y': 1.2e-6, 'dx': 25e-9, 'npml': 10, 'boundaries': 'periodic_y',
+                'polarization': 'hz'},
+        'ops': [
+            ['add_line_source', ['x', 0.25e-6], {'wavelength': 700e-9, 'bandwidth': 0.6, 'span': [0.1e-6, 1.5e-6]}],
+            ['add_flux_monitor', ['y', 1.3e-6, [0.0, 1.2e-6]], {'wavelengths': [650e-9, 750e-9]}],
+        ],
+        'poles': [['drude_rect', [0.8e-6, 0.0, 1.0e-6, 1.2e-6], [6e15, 3e13, 2.0]],
+                  ['drude_circle', [0.9e-6, 0.6e-6, 0.2e-6], [9e15, 1e14, 2.5]]],
+        'dft': [
+            [0.1e-6, 0.0, 1.5e-6, 1.2e-6, [4.3e14], 1],
+        ],
+        'probes': [[0.9e-6, 0.6e-6, 'ex'], [0.85e-6, 1.18e-6, 'ey']],
+        'checkpoints': [250, 500],
+    },
 ]
 
 

@@ -3,7 +3,7 @@ cases of cases_dft.py.
 
 Run in a container that holds the reference source tree (read-only):
 
-    python tests/golden/make_golden_dft.py /path/to/reference
+    python tests/golden/make_golden_dft.py /path/to/reference [case names]
 
 Each case writes <name>.npz: per field-map monitor its sample boxes (x / y sample slice starts, strides, counts) and
 its complex64 spectra at every checkpoint (E_z; or H_z, E_x, E_y for the H_z cases), the flux monitor's complex128 spectra, the DFT sample interval,
@@ -74,13 +74,20 @@ def main():
     sys.path.insert(0, HERE)
     import numpy as np
     from cases_dft import CASES_DFT, CASES_DFT_HZ
+    only = set(sys.argv[2:])   # case names to regenerate (default: all)
+    index_path = os.path.join(HERE, 'index_dft.json')
     index = {}
+    if only and os.path.exists(index_path):
+        with open(index_path) as f:
+            index = json.load(f)['cases']
     for spec in CASES_DFT + CASES_DFT_HZ:
+        if only and spec['name'] not in only:
+            continue
         out = run_case(spec)
         np.savez_compressed(os.path.join(HERE, f"{spec['name']}.npz"), **out)
         index[spec['name']] = sorted(out)
         print(f"{spec['name']}: {len(out)} entries, m {int(out['sample_interval'])}")
-    with open(os.path.join(HERE, 'index_dft.json'), 'w') as f:
+    with open(index_path, 'w') as f:
         json.dump({'generated_by': 'tests/golden/make_golden_dft.py (open_sol CPU backend)', 'cases': index}, f,
                   indent=1)
 

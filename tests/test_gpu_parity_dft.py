@@ -179,3 +179,39 @@ def test_random_poles_and_tfsf_match_oracle(seed):
     for (ix, iy, _, times, values), probe in zip(o.probe_records, sim.probes):
         np.testing.assert_array_equal(probe.get_data()[1], np.array(values, dtype=np.float32))
     sim.em.engine.close()
+
+
+@pytest.mark.parametrize('seed', [0, 1])
+def test_random_hz_poles_match_oracle(seed):
+    """Seeded Drude / Lorentz media on the H_z engine (face sets of E_x / E_y), a sheet crossing one of them, a map
+    and probes, advanced in chunks of random length, against the oracle (pinned to open_sol on the poles_hz_* cases)."""
+    rng = np.random.default_rng(700 + seed)
+    cx, cy = rng.uniform(0.6e-6, 1.0e-6, 2)
+    spec = {'sim': {'size_x': 1.6e-6, 'size_y': 1.6e-6, 'dx': 25e-9, 'npml': 10,
+                    'boundaries': ['pml', 'periodic_y'][seed], 'polarization': 'hz'},
+            'ops': [['add_dielectric_circle', [0.4e-6, 1.2e-6, 0.12e-6], {'eps_r': 2.0}],
+                    ['add_line_source', ['y', float(cx) - 0.05e-6],
+                     {'wavelength': float(rng.uniform(650e-9, 900e-9)), 'bandwidth': 0.5,
+                      'span': [0.2e-6, 1.4e-6]}],
+                    ['add_flux_monitor', ['y', 1.45e-6, [0.1e-6, 1.5e-6]], {'wavelengths': [700e-9]}]],
+            'poles': [['drude_circle', [float(cx), float(cy), float(rng.uniform(0.08e-6, 0.2e-6))],
+                       [float(rng.uniform(4e15, 9e15)), float(rng.uniform(1e13, 2e14)), 2.0]],
+                      ['lorentz_circle', [0.4e-6, 1.2e-6, 0.12e-6], [1.2, 2.5e15, 1e14]]],
+            'dft': [[0.1e-6, 0.1e-6, 1.5e-6, 1.5e-6, [4.0e14], 2]],
+            'probes': [[float(cx), float(cy), 'ex'], [float(cx), float(cy), 'ey']]}
+    chunks = [int(c) for c in rng.integers(1, 80, 8)]
+    spec['checkpoints'] = list(np.cumsum(chunks))
+    o, _, snaps = run_oracle_dft(spec)
+    sim, _, maps = _build(spec, CONFIGS_HZ[0])
+    sim.em.finalize()
+    done = 0
+    for cp in spec['checkpoints']:
+        sim.em.engine.advance(int(cp - done))
+        done = cp
+        for k, mon in enumerate(maps):
+            for got, want in zip(map_parts(mon), snaps[cp][0][k]):
+                np.testing.assert_array_equal(got, want)
+        assert _digest(sim.em.engine.read_field('hz')) == snaps[cp][2]['hz']
+    for (ix, iy, _, times, values), probe in zip(o.probe_records, sim.probes):
+        np.testing.assert_array_equal(probe.get_data()[1], np.array(values, dtype=np.float32))
+    sim.em.engine.close()

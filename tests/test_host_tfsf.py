@@ -65,3 +65,28 @@ def test_unstable_drude_is_refused():
     sim.em.add_line_source('y', 0.2e-6, wavelength=700e-9)
     with pytest.raises(ValueError, match='unstable'):
         sim.em.finalize_host()
+
+
+@pytest.mark.parametrize('periodic', [False, True])
+def test_hz_pole_face_sets_match_oracle(periodic):
+    """The H_z engine's pole face sets (face-averaged cell masks on E_x / E_y, boxed on positive weights) equal the
+    oracle's, including the faces below / left of the mask, a wrapped partner on a periodic y axis and graded shares."""
+    from oracle.hz2d import OracleHz2D
+    from oracle.fdtd2d import OracleDrude
+    from opensol_b200.boundaries import face_shares
+    from opensol_b200.poles import pole_face_sets
+    o = OracleHz2D(1.2e-6, 1.0e-6, 25e-9, npml=8, boundaries='periodic_y' if periodic else 'pml')
+    d = o.domain
+    mask = np.zeros((d.nx, d.ny), dtype=bool)
+    mask[20:31, 0:6] = True            # touches the y = 0 edge: its E_x partner faces wrap on a periodic axis
+    mask[25:29, d.ny - 3:] = True      # and the last column
+    mask[40:44, 15:22] = True
+    o.add_dispersive(OracleDrude(8e15, 5e13), mask)
+    shares_x = face_shares(d.kernel_widths[0], d.periodic_x)
+    shares_y = face_shares(d.kernel_widths[1], d.periodic_y)
+    sets = pole_face_sets(mask, shares_x, shares_y, d.periodic_x, d.periodic_y)
+    assert [(c, b) for c, b, _ in sets] == [(f[1], f[2]) for f in o.pole_faces]
+    for (_, _, weight), face in zip(sets, o.pole_faces):
+        assert weight.dtype == np.float32
+        np.testing.assert_array_equal(weight, face[3])
+    assert sets[1][1][0].start == 19   # the E_y faces below the mask's first row carry weight too
