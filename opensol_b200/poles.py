@@ -1,8 +1,9 @@
-"""Dispersive poles of the 2D E_z engine: Drude and Lorentz media (physics/em/materials.py:132-190).
+"""Dispersive poles of the 2D engines: Drude and Lorentz media (physics/em/materials.py:132-190).
 
 The auxiliary-differential-equation coefficients are computed in float64 and rounded to float32 as open_sol rounds
 them; the device steps them in velocity form (J += damping J + drive E, or dP += damping dP - restoring P + drive E,
 P += dP).  susceptibility() gives the continuous-time chi(omega) the sheet-source calibration adds on pole cells.
+The E_z engine steps a pole on its cells, the H_z engine on the E_x / E_y face sets of pole_face_sets().
 """
 from __future__ import annotations
 
