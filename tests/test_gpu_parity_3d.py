@@ -87,3 +87,40 @@ def test_field_roundtrip_and_launches():
     m = physics.monitors[0].sample_interval
     assert engine.launch_count() == 2 * 30 + 30 // m
     assert engine.last_advance_ms() > 0.0
+
+
+def test_x_chunk_does_not_change_results():
+    """The number of x planes a block streams is a launch shape only: 1, 5, 24 planes and the whole grid give
+    bit-identical fields and fluxes."""
+    spec = CASES3D[0]
+    physics, _ = build_product(spec)
+    engine = physics.engine
+    n = spec['checkpoints'][0]
+    runs = []
+    for planes in (engine.shape[0], 1, 5, 24):
+        engine.reset()
+        engine.set_x_chunk(planes)
+        physics.run(n)
+        runs.append((engine.state(), [np.asarray(m.flux()) for m in physics.monitors]))
+    for state, fluxes in runs[1:]:
+        for name in FIELDS:
+            np.testing.assert_array_equal(state[name], runs[0][0][name])
+        for f, f0 in zip(fluxes, runs[0][1]):
+            np.testing.assert_array_equal(f, f0)
+
+
+def test_workload_512_deterministic_across_x_chunks():
+    """Size-independent property at the benchmark size (512^3, 500 spheres, dipole, flux box): two runs, with 24- and
+    7-plane x chunks, give bit-identical fields and box flux (no races, no order dependence)."""
+    from opensol_b200 import workloads
+    out = []
+    for planes in (24, 7):
+        physics, box = workloads.roofline_3d_physics()
+        physics.finalize()
+        physics.engine.set_x_chunk(planes)
+        physics.run(200)
+        out.append((physics.engine.read_field('ez'), physics.engine.read_field('hx'), np.asarray(box.flux())))
+        del physics, box
+    assert np.abs(out[0][0]).max() > 0
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, b)
