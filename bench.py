@@ -62,7 +62,8 @@ def parse_args():
 
 
 def dist_env():
-    return int(os.environ.get('RANK', 0)), int(os.environ.get('WORLD_SIZE', 1)), int(os.environ.get('LOCAL_RANK', 0))
+    from opensol_b200.replicas import replica_env
+    return replica_env()
 
 
 def measured_peak_hbm():
@@ -197,24 +198,12 @@ def config_block(args, parallelism):
 
 def run_b200(args):
     import torch
+    from opensol_b200.replicas import ReplicaGroup
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300), device_id=torch.device('cuda', local))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def reduce_max(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device='cuda')
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    # independent replicas: the group only brackets the timed region and takes the max over ranks
+    group = ReplicaGroup('nccl', timeout_s=300)
+    barrier, reduce_max = group.barrier, group.reduce_max
 
     sim, monitors = build_sim(local, args.grid)
     sim.em.engine.configure(args.variant, args.steps_per_launch, args.tile_rows or 128)
@@ -250,7 +239,7 @@ def run_b200(args):
         torch.cuda.synchronize()
     barrier()
     device_ms = reduce_max(start.elapsed_time(stop))
-    value = world * cells * args.sim_steps * args.steps / (device_ms / 1e3) / 1e9
+    value = group.whole_job_rate(cells * args.sim_steps * args.steps, device_ms / 1e3) / 1e9
     flux = [m.flux() for m in monitors]
     if args.sim_steps >= 2000:   # the pulse reaches the first flux line after ~250 steps
         assert any(float(abs(f).max()) > 0 for f in flux), 'every flux is zero: the run did no work'
@@ -311,8 +300,7 @@ def run_b200(args):
         line['cpu_baseline'] = cpu_baseline()
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    group.close()
 
 
 def run_e2e(args, device, world, barrier, reduce_max):
