@@ -244,7 +244,9 @@ def run_b200(args):
     if args.sim_steps >= 2000:   # the pulse reaches the first flux line after ~250 steps
         assert any(float(abs(f).max()) > 0 for f in flux), 'every flux is zero: the run did no work'
 
-    # Dominant kernel: one more run with every launch bracketed by CUDA events on the engine's stream.
+    # Dominant kernel: one more run with every launch bracketed by CUDA events on the engine's stream (the frame
+    # launches then run ahead of the interior launch instead of beside it, so each pair times one kernel alone and
+    # the shares compare with ncu's serialised launch list).
     engine.set_profiling(True)
     engine.reset()
     engine.advance(args.sim_steps, tables)
@@ -267,7 +269,8 @@ def run_b200(args):
     roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
                 'traffic': None, 'peak_source': f'{peak_kind} hbm_gbs (copy bandwidth)', 'kernel': name,
                 'bytes_per_cell_update': BYTES_PER_CELL_UPDATE, 'cell_updates_per_launch': units,
-                'launch_ms': launch_ms, 'steps_per_launch': T,
+                'launch_ms': launch_ms, 'launch_timing': 'CUDA events per launch, each kernel alone',
+                'steps_per_launch': T,
                 'kernel_share': {k: v[0] / sum(t[0] for t in times.values()) for k, v in times.items()}}
     traffic_path = os.path.join(ROOT, 'profiles', 'traffic.json')
     if os.path.exists(traffic_path):

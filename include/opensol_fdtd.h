@@ -245,7 +245,9 @@ int os_fdtd2d_launch_count(OsFdtd2D *h, int64_t *launches);
 
 /* Profiling: with `on`, every kernel of the following advances is bracketed by CUDA events; kernel_times returns the
  * summed device milliseconds and launch count of one kind over the last advance (0 interior blocked kernel, 1 general
- * blocked kernel, 2 DFT kernel, 3 per-step kernel pair).  No open_sol counterpart. */
+ * blocked kernel, 2 DFT kernel, 3 per-step kernel pair).  While profiling, the frame / border kernels run on the
+ * handle's stream ahead of the interior kernel instead of beside it, so each event pair times one kernel alone and the
+ * shares compare with a serialised launch list.  No open_sol counterpart. */
 int os_fdtd2d_set_profiling(OsFdtd2D *h, int32_t on);
 
 /* Autotuner of the interior tile height: times `repeats` launches of steps_per_launch steps for every candidate

@@ -945,7 +945,8 @@ static int launch_tb(OsFdtd2D *h, const TBParams &interior, const TBParams &gene
                      const EzFrameParams *frame_tmpl = nullptr) {
     const dim3 threads(TB_WARPS * 32);
     const bool run_interior = has_interior && interior.n_tiles;
-    const bool fork = run_interior && general.n_tiles;
+    // profiling: no fork, so that each event pair times one kernel alone (shares as in a serialised launch list)
+    const bool fork = run_interior && general.n_tiles && !h->profiling;
     cudaStream_t gstream = fork ? h->side_stream : h->stream;
     if (fork) {
         OS_CUDA(cudaEventRecord(h->ev_fork, h->stream));
@@ -1447,7 +1448,7 @@ static int hz_rows_per_cta(const OsFdtd2D *h, const HzPlan &q) {
 static int launch_hz_step(OsFdtd2D *h, const HzPlan &q, Hz2DParams p) {
     const bool vec = h->grid.ny % 4 == 0;
     const int64_t border_cells = q.rects.first[q.rects.n];
-    const bool fork = q.interior && border_cells > 0;
+    const bool fork = q.interior && border_cells > 0 && !h->profiling;   // profiling: each kernel timed alone
     cudaStream_t bstream = fork ? h->side_stream : h->stream;
     if (fork) {
         OS_CUDA(cudaEventRecord(h->ev_fork, h->stream));
