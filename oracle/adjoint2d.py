@@ -1,7 +1,7 @@
 """ORACLE -- TEST INFRASTRUCTURE ONLY.
 
-Nothing in the product (``opensol_b200``) imports this module.  Only ``tests/`` use it, as the checker of the device
-adjoint.
+Nothing in the product (``opensol_b200``) imports this module.  Only ``tests/`` use it, as the reference the device
+adjoint is compared with.
 
 The discrete adjoint of the 2D E_z time step in float64 numpy, for small grids: the forward step of oracle/ez2d.c
 (the reference's update order: H Yee, H-row CPML per side, E Yee, E-row CPML per side, line injection, DFT sample;

@@ -1,6 +1,6 @@
 /*
  * ORACLE -- TEST INFRASTRUCTURE ONLY.  Nothing in the product (opensol_b200/) links, loads or calls this file;
- * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg do, as the checker.
+ * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg do, as the reference results are compared with.
  *
  * Plain-C restatement of the two fused field updates of open_sol's 3D Yee engine (em_fdtd_3d, Cartesian grid, one
  * real field set, single-precision storage and arithmetic) on the CPU:

@@ -1,6 +1,6 @@
 /*
  * ORACLE -- TEST INFRASTRUCTURE ONLY.  Nothing in the product (opensol_b200/) links, loads or calls this file;
- * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg do, as the checker.
+ * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg do, as the reference results are compared with.
  *
  * Plain-C restatement of open_sol's 2D E_z-polarisation FDTD time step on the CPU, written to reproduce the
  * reference CPU backend's float32 (or float64, -DORACLE_REAL=double) arithmetic bit for bit:

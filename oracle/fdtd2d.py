@@ -1,7 +1,7 @@
 """ORACLE -- TEST INFRASTRUCTURE ONLY.
 
 Nothing in the product (``opensol_b200``) imports this module.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
-CPU-baseline leg of ``bench.py`` use it, as the checker the CUDA engine is compared with.
+CPU-baseline leg of ``bench.py`` use it, as the reference the CUDA engine is compared with.
 
 A CPU restatement of open_sol's 2D E_z FDTD path (``Simulation.run`` -> ``EMPhysics.step`` ->
 ``FDTDEngine2D_Ez.advance``) in two parts:

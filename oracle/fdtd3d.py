@@ -1,7 +1,7 @@
 """ORACLE -- TEST INFRASTRUCTURE ONLY.
 
 Nothing in the product (``opensol_b200``) imports this module.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
-CPU-baseline leg of ``bench.py`` use it, as the checker the CUDA engine is compared with.
+CPU-baseline leg of ``bench.py`` use it, as the reference the CUDA engine is compared with.
 
 A CPU restatement of open_sol's 3D FDTD path (``EMPhysics3D.step`` -> ``FDTDEngine3D.advance``) for a Cartesian
 uniform grid with one real field set and single-precision fields:

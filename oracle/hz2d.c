@@ -1,6 +1,6 @@
 /*
  * ORACLE -- TEST INFRASTRUCTURE ONLY.  Nothing in the product (opensol_b200/) links, loads or calls this file;
- * only tests/ do, as the checker.
+ * only tests/ do, as the reference results are compared with.
  *
  * Plain-C restatement of open_sol's 2D H_z-polarisation FDTD time step on the CPU (H_z at cell centres, E_x on the
  * hi-y faces, E_y on the hi-x faces), float32 or float64 (-DORACLE_REAL=double), in the reference CPU twins' order:

@@ -1,6 +1,6 @@
 """ORACLE -- TEST INFRASTRUCTURE ONLY.
 
-Nothing in the product (``opensol_b200``) imports this module.  Only ``tests/`` use it, as the checker the CUDA H_z
+Nothing in the product (``opensol_b200``) imports this module.  Only ``tests/`` use it, as the reference the CUDA H_z
 engine is compared with.
 
 A CPU restatement of open_sol's 2D H_z-polarisation FDTD path (``Simulation(polarization='hz').run`` ->

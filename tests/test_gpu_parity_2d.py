@@ -1,6 +1,6 @@
 """GPU parity of the 2D E_z engine (the CUDA path through the C ABI) against the oracle and open_sol's own outputs.
 
-Bar: the north star asks for fluxes and field snapshots within 1e-5 relative (float32) of the reference CPU backend.
+Bar: fluxes and field snapshots within 1e-5 relative (float32) of the reference CPU backend.
 The engine evaluates every cell in the reference's order without fused multiply-add, so these tests assert the
 stronger property: bit-identical fields (array_equal, and the SHA-256 digests of open_sol's own fields in
 tests/golden), bit-identical complex128 spectra and fluxes.  FLUX_RTOL documents the contract bar where a
