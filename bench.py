@@ -488,6 +488,13 @@ def run_em3d(args):
                          'kernel': 'em3d_h_kernel + em3d_e_kernel (whole step)'},
             'gpu_launches': launches, 'clocks': clocks.summary(),
             'flux_box_first': float(box.flux()[0])}
+    traffic_path = os.path.join(ROOT, 'profiles', 'traffic.json')
+    if os.path.exists(traffic_path):
+        with open(traffic_path) as f:
+            t = json.load(f).get('em3d_step')
+        if t:
+            line['roofline']['traffic'] = t['dram_bytes_per_cell_update'] * cells   # per step (both kernels)
+            line['roofline']['traffic_note'] = t['note']
     print(json.dumps(line), flush=True)
 
 
