@@ -127,3 +127,48 @@ def test_engine_results_equal_reference_results(name, tmp_path):
     res.save_results(tmp_path, got)
     _assert_same_archive(tmp_path / 'results.npz', _fixture(name))
     sim.em.engine.close()
+
+
+class _FakeEngine:
+    def __init__(self, dt, n_step):
+        self.dt, self.n_step = dt, n_step
+
+
+class _FakeSource:
+    def __init__(self, temporal):
+        self.temporal = temporal
+
+
+class _FakePhysics:
+    def __init__(self, sources, dt=5e-17, n_step=2000):
+        self.sources, self.engine = sources, _FakeEngine(dt, n_step)
+
+
+class _FakeFlux:
+    def __init__(self, frequencies, power):
+        self.frequencies, self._power, self.sample_interval = np.asarray(frequencies), np.asarray(power), 2
+
+    def flux(self):
+        return self._power
+
+
+def test_flux_result_normalisation_branches():
+    """power_per_cw = power / (2 |S|^2) of the shared waveform's sampled spectrum; NaN where |S|^2 is below 1e-6 of
+    the carrier's; a continuous wave keeps only its main lobe; sources with different waveforms give no per-cw entry."""
+    from opensol_b200.sources import ContinuousWave, GaussianPulse
+    pulse = GaussianPulse(4.5e14, 0.3)
+    freqs = [4.5e14, 4.6e14, 1.5e15]                  # the last far outside the pulse's band
+    physics = _FakePhysics([_FakeSource(pulse), _FakeSource(GaussianPulse(4.5e14, 0.3))])
+    mon = _FakeFlux(freqs, [2.0, 1.0, 0.5])
+    result = res.flux_result(mon, physics)
+    assert result['kind'] == 'flux_spectrum' and result['mirror_factor'] == 1.0
+    s = res.sampled_waveform_spectrum(pulse, 5e-17, freqs, 1, 2000, 2)
+    np.testing.assert_allclose(result['power_per_cw'][:2], np.array([2.0, 1.0]) / (2 * np.abs(s[:2]) ** 2),
+                               rtol=1e-12)
+    assert np.isnan(result['power_per_cw'][2])
+    mixed = _FakePhysics([_FakeSource(pulse), _FakeSource(GaussianPulse(5e14, 0.3))])
+    assert 'power_per_cw' not in res.flux_result(mon, mixed)
+    cw = ContinuousWave(4.5e14)
+    run = _FakePhysics([_FakeSource(cw)], n_step=2000)   # 100 fs: main lobe |f - f0| < 1e13 Hz
+    out = res.flux_result(_FakeFlux([4.5e14, 4.7e14], [1.0, 1.0]), run)['power_per_cw']
+    assert np.isfinite(out[0]) and np.isnan(out[1])
