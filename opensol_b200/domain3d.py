@@ -12,8 +12,9 @@ import math
 
 import numpy as np
 
-from .constants import C0, DTYPE
+from .constants import DTYPE
 from .domain import BoxMask, MaterialGrid, containing_cell
+from .grid import uniform_cell_count, yee_time_step
 
 FACES_3D = ('x_lo', 'x_hi', 'y_lo', 'y_hi', 'z_lo', 'z_hi')
 AXES = ('x', 'y', 'z')
@@ -22,20 +23,9 @@ FACE_TYPES_3D = ('cpml', 'pec', 'pmc', 'periodic', *MIRROR_TYPES_3D)
 MIRROR_GHOST_CELLS = 1
 
 
-def uniform_cell_count(length: float, dx: float) -> int:
-    """Cells of width dx covering length (core/grid.py:20-22)."""
-    return int(np.ceil(length / dx - 1e-9))
-
-
 def courant_time_step_3d(dx_min, dy_min, dz_min, courant_factor=None):
-    """EM time step (float32) = courant x the 3D CFL limit of the finest cells (core/grid3d.py:8-17)."""
-    if courant_factor is None:
-        courant_factor = 0.99
-    if not 0.0 < float(courant_factor) <= 1.0:
-        raise ValueError(f"courant must be a fraction of the 3D CFL limit in (0, 1], got {courant_factor} "
-                         f"(0.99 means dt = 0.99 dx / (C0 sqrt(3)) on cubic cells)")
-    inverse_spacing_squared = 1.0 / float(dx_min) ** 2 + 1.0 / float(dy_min) ** 2 + 1.0 / float(dz_min) ** 2
-    return DTYPE(float(courant_factor) / (C0 * np.sqrt(inverse_spacing_squared)))
+    """float32 EM time step of the 3D CFL limit of the finest cells (core/grid3d.py:8-17)."""
+    return yee_time_step(dx_min, dy_min, dz_min, courant=courant_factor)
 
 
 class BoundaryConfig3D:

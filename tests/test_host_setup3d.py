@@ -126,6 +126,26 @@ def test_material_index_requantisation():
             assert deltas[name] == float(g[f'case{case}_delta_{name}'])
 
 
+def test_material_ids_are_lexicographic_ranks_of_level_tuples():
+    """With exact levels, a cell's id is the rank of its tuple of level numbers (arrays that vary, in order) among the
+    occurring tuples, and the tables give back each array's value: checked against numpy's row-wise unique for one
+    to six varying arrays (four or more take the ranked radix groups)."""
+    rng = np.random.default_rng(12)
+    names = ('eps_r', 'sigma_e', 'mu_r', 'eps_xx', 'eps_yy', 'sigma_m')
+    for k in range(1, 7):
+        shape = (9, 7, 11)
+        arrays = {n: rng.choice(rng.uniform(1.0, 9.0, 4).astype(np.float32), size=shape) for n in names[:k]}
+        arrays['mu_r'] = arrays.get('mu_r', np.ones(shape, np.float32))
+        ids, tables, errors, _ = build_material_index(arrays, shape)
+        varying = [n for n in arrays if np.unique(arrays[n]).size > 1]
+        tuples = np.stack([np.searchsorted(np.unique(arrays[n]), arrays[n].ravel()) for n in varying], axis=1)
+        _, expected = np.unique(tuples, axis=0, return_inverse=True)
+        np.testing.assert_array_equal(ids.ravel(), expected.ravel())
+        for n, a in arrays.items():
+            np.testing.assert_array_equal(tables[n][ids], a)
+        assert errors == {}
+
+
 def test_face_shares_uniform_and_graded():
     lo, hi = face_shares(np.full(5, 3.0), periodic=False)
     assert np.all(lo == 0.5) and np.all(hi == 0.5)
