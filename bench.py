@@ -178,7 +178,7 @@ def run_reference(args):
         'impl': 'reference', 'metric': 'FDTD Gcell-updates/s', 'value': value, 'unit': 'Gcell-updates/s',
         'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total / args.steps * 1e3,
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-        'config': config_block(args, 'replicas'),
+        'config': config_block(args, 'replicas' if world > 1 else 'single'),
         'cpu_baseline': {'value': value, 'unit': 'Gcell-updates/s', 'cores': os.cpu_count(), 'kind': 'port',
                          'sample': f'{sample} Yee steps of the 8192x8192 roofline grid per bench step (oracle: C '
                                    f'restatement of open_sol\'s CPU step, OpenMP on {os.cpu_count()} threads)'},

@@ -73,7 +73,10 @@ def material_index(arrays, limit=MAX_MATERIAL_IDS - 1):
     if not order:
         return np.zeros(shape, np.uint16), {name: levels[name][:1].copy() for name in names}
     codes = np.stack([np.searchsorted(levels[name], arrays[name].ravel()) for name in order], axis=1)
-    tuples, ids = np.unique(codes, axis=0, return_inverse=True)
+    if len(order) == 1:   # one varying array: its level codes are already the ranks
+        tuples, ids = np.arange(levels[order[0]].size)[:, None], codes[:, 0]
+    else:
+        tuples, ids = np.unique(codes, axis=0, return_inverse=True)
     if tuples.shape[0] > limit:
         raise ValueError('joint material count exceeds the exact index of the oracle')
     tables = {}
@@ -178,41 +181,54 @@ class FluxBox:
 
 # ----------------------------------------------------------------------------------------------- ctypes binding
 
-_P = ctypes.POINTER(ctypes.c_float)
 _I = ctypes.POINTER(ctypes.c_int32)
+_REALS = {'single': (np.float32, ctypes.c_float, 'libem3d_oracle.so'),
+          'double': (np.float64, ctypes.c_double, 'libem3d_oracle_f64.so')}
 
 
-class _State(ctypes.Structure):
-    _fields_ = [('nx', ctypes.c_int32), ('ny', ctypes.c_int32), ('nz', ctypes.c_int32),
-                ('px', ctypes.c_int32), ('py', ctypes.c_int32), ('pz', ctypes.c_int32)] + \
-               [(name, _P) for name in ('ex', 'ey', 'ez', 'hx', 'hy', 'hz')] + \
-               [('mat', ctypes.POINTER(ctypes.c_uint16))] + \
-               [(name, _P) for name in ('t_ex', 't_ey', 't_ez', 't_sig', 't_mu', 't_sm', 'iex', 'iey', 'iez', 'ihx',
-                                         'ihy', 'ihz', 'wlx', 'wux', 'wly', 'wuy', 'wlz', 'wuz')] + \
-               [('dt', ctypes.c_float), ('nr', ctypes.c_int32 * 3), ('rm_h', _I * 3), ('rm_e', _I * 3),
-                ('b_h', _P * 3), ('g_h', _P * 3), ('b_e', _P * 3), ('g_e', _P * 3),
-                ('ph_first', _P * 3), ('ph_second', _P * 3), ('pe_first', _P * 3), ('pe_second', _P * 3)]
+def _state_type(ctype):
+    """The C struct OracleEM3D for arithmetic type ctype (float or double build of oracle/em3d.c)."""
+    P = ctypes.POINTER(ctype)
+
+    class State(ctypes.Structure):
+        _fields_ = [('nx', ctypes.c_int32), ('ny', ctypes.c_int32), ('nz', ctypes.c_int32),
+                    ('px', ctypes.c_int32), ('py', ctypes.c_int32), ('pz', ctypes.c_int32)] + \
+                   [(name, P) for name in ('ex', 'ey', 'ez', 'hx', 'hy', 'hz')] + \
+                   [('mat', ctypes.POINTER(ctypes.c_uint16))] + \
+                   [(name, P) for name in ('t_ex', 't_ey', 't_ez', 't_sig', 't_mu', 't_sm', 'iex', 'iey', 'iez',
+                                            'ihx', 'ihy', 'ihz', 'wlx', 'wux', 'wly', 'wuy', 'wlz', 'wuz')] + \
+                   [('dt', ctype), ('nr', ctypes.c_int32 * 3), ('rm_h', _I * 3), ('rm_e', _I * 3),
+                    ('b_h', P * 3), ('g_h', P * 3), ('b_e', P * 3), ('g_e', P * 3),
+                    ('ph_first', P * 3), ('ph_second', P * 3), ('pe_first', P * 3), ('pe_second', P * 3)]
+    return State
 
 
 _LIB = {}
 
 
-def load_library():
-    if 'lib' not in _LIB:
-        if not os.path.exists(LIB_PATH):
-            raise RuntimeError(f'oracle library {LIB_PATH} is not built (run: make -C oracle)')
-        lib = ctypes.CDLL(LIB_PATH)
-        lib.oracle_em3d_update_h.argtypes = [ctypes.POINTER(_State)]
-        lib.oracle_em3d_update_e.argtypes = [ctypes.POINTER(_State)]
-        lib.oracle_em3d_face_cb.argtypes = [ctypes.POINTER(_State), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+def load_library(precision='single'):
+    """(library, State struct type) of the float ('single') or double build."""
+    if precision not in _LIB:
+        _, ctype, name = _REALS[precision]
+        path = os.path.join(_HERE, '_build', name)
+        if not os.path.exists(path):
+            raise RuntimeError(f'oracle library {path} is not built (run: make -C oracle)')
+        lib = ctypes.CDLL(path)
+        State = _state_type(ctype)
+        lib.oracle_em3d_update_h.argtypes = [ctypes.POINTER(State)]
+        lib.oracle_em3d_update_e.argtypes = [ctypes.POINTER(State)]
+        lib.oracle_em3d_face_cb.argtypes = [ctypes.POINTER(State), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_int]
-        lib.oracle_em3d_face_cb.restype = ctypes.c_float
-        _LIB['lib'] = lib
-    return _LIB['lib']
+        lib.oracle_em3d_face_cb.restype = ctype
+        _LIB[precision] = (lib, State)
+    return _LIB[precision]
 
 
 def _fp(a):
-    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float)) if a is not None else None
+    if a is None:
+        return None
+    ctype = ctypes.c_double if a.dtype == np.float64 else ctypes.c_float
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
 
 
 # ----------------------------------------------------------------------------------------------- the oracle run
@@ -221,9 +237,14 @@ class OracleEM3D:
     """The 3D FDTD path on the CPU for a uniform grid: Domain3D.uniform(size_x, size_y, size_z, dx, npml_sides,
     boundary_config) with face types over FACES_3D (cpml / pec / pmc / periodic), float32 material arrays written by
     the caller (eps_r, sigma_e, mu_r, optional sigma_m), then add_dipole / add_flux_box / add_flux_plane, finalize(),
-    run(n_steps)."""
+    run(n_steps).  precision='double' steps float64 fields with float64 coefficient and CPML rows (the float32
+    materials, dt and face shares promoted): the run the float32 results' error is stated against."""
 
-    def __init__(self, size_x, size_y, size_z, dx, faces=None, npml=15, courant=None):
+    def __init__(self, size_x, size_y, size_z, dx, faces=None, npml=15, courant=None, precision='single'):
+        if precision not in _REALS:
+            raise ValueError(f"precision must be 'single' or 'double', got {precision!r}")
+        self.precision = precision
+        self.real = _REALS[precision][0]
         self.faces = {face: (faces or {}).get(face, 'cpml') for face in FACES_3D}
         self.npml = int(npml)
         self.sides = {face: self.npml if kind == 'cpml' else 0 for face, kind in self.faces.items()}
@@ -242,7 +263,7 @@ class OracleEM3D:
         self.edges = tuple((np.arange(n + 1) - o) * self.dx for n, o in zip(self.shape, self.origins))
         self.materials = {'eps_r': np.ones(self.shape, DTYPE), 'sigma_e': np.zeros(self.shape, DTYPE),
                           'mu_r': np.ones(self.shape, DTYPE)}
-        self.fields = {name: np.zeros(self.shape, DTYPE) for name in ('ex', 'ey', 'ez', 'hx', 'hy', 'hz')}
+        self.fields = {name: np.zeros(self.shape, self.real) for name in ('ex', 'ey', 'ez', 'hx', 'hy', 'hz')}
         self.sources, self.monitors = [], []
         self.time, self.n_step = 0.0, 0
         self._build_rows()
@@ -261,8 +282,8 @@ class OracleEM3D:
             n = self.shape[axis_index]
             se, ke, ae, sh, kh, ah = cpml_axis_profile(self.faces, n, axis, self.npml, pml_sizes[axis_index])
             inverse_e, inverse_h = bulk[axis_index]
-            self.inv_e.append((inverse_e / ke).astype(DTYPE))
-            self.inv_h.append((inverse_h / kh).astype(DTYPE))
+            self.inv_e.append((inverse_e / ke).astype(self.real))
+            self.inv_h.append((inverse_h / kh).astype(self.real))
             sides = []
             for side in ('lo', 'hi'):
                 if self.faces[f'{axis}_{side}'] == 'cpml':
@@ -278,18 +299,19 @@ class OracleEM3D:
                     selected = rows[kind_index]
                     row_map[selected] = np.arange(len(decays) * self.npml, (len(decays) + 1) * self.npml,
                                                   dtype=np.int32)
-                    a, b = cpml_recursion(sigma[selected], kappa[selected], alpha[selected], self.dt, DTYPE)
-                    inverse = (inverse_e if kind == 'e' else inverse_h)[selected].astype(DTYPE)
+                    a, b = cpml_recursion(sigma[selected], kappa[selected], alpha[selected], self.dt, self.real)
+                    inverse = (inverse_e if kind == 'e' else inverse_h)[selected].astype(self.real)
                     decays.append(b)
                     gains.append(a * inverse)
                 n_rows = self.npml * len(sides)
                 psi_shape = list(self.shape)
                 psi_shape[axis_index] = n_rows
                 self.layers[(axis_index, kind)] = {
-                    'row_map': row_map, 'b': np.concatenate(decays).astype(DTYPE),
-                    'gain': np.concatenate(gains).astype(DTYPE), 'n_rows': n_rows,
-                    'first': np.zeros(psi_shape, DTYPE), 'second': np.zeros(psi_shape, DTYPE)}
-        self.shares = [face_shares(w, p) for w, p in zip(self.widths, self.periodic)]
+                    'row_map': row_map, 'b': np.concatenate(decays).astype(self.real),
+                    'gain': np.concatenate(gains).astype(self.real), 'n_rows': n_rows,
+                    'first': np.zeros(psi_shape, self.real), 'second': np.zeros(psi_shape, self.real)}
+        self.shares = [tuple(np.asarray(w, self.real) for w in face_shares(widths, p))
+                       for widths, p in zip(self.widths, self.periodic)]
 
     # ---- placement (domain3d.py:123-140, physics3d.py:403-497)
     def pos_to_cell(self, position):
@@ -317,14 +339,15 @@ class OracleEM3D:
         self.sources.append(source)
         return source
 
-    def add_flux_box(self, lo, hi, wavelengths):
+    def add_flux_box(self, lo, hi, wavelengths=None, frequencies=None):
         bounds = []
         for axis in range(3):
             first = self.nearest_edge(axis, min(lo[axis], hi[axis]))
             last = self.nearest_edge(axis, max(lo[axis], hi[axis]))
             bounds.append((first, last))
-        box = FluxBox(bounds, C0 / np.asarray(wavelengths, dtype=np.float64), self.dt, self.widths, self.shape,
-                      self.periodic)
+        freqs = (np.asarray(frequencies, dtype=np.float64) if frequencies is not None
+                 else C0 / np.asarray(wavelengths, dtype=np.float64))
+        box = FluxBox(bounds, freqs, self.dt, self.widths, self.shape, self.periodic)
         self.monitors.append(box)
         return box
 
@@ -344,7 +367,7 @@ class OracleEM3D:
         pec_id = np.uint16(tables['eps_r'].size)
 
         def with_pec(values, pec_value):
-            return np.concatenate((values, np.full(1, pec_value, DTYPE))).astype(DTYPE)
+            return np.concatenate((values, np.full(1, pec_value, DTYPE))).astype(self.real)
         self.t_ez = with_pec(tables['eps_r'], -1.0)
         self.t_ex = with_pec(tables.get('eps_xx', tables['eps_r']), -1.0)
         self.t_ey = with_pec(tables.get('eps_yy', tables['eps_r']), -1.0)
@@ -359,10 +382,10 @@ class OracleEM3D:
                     key[axis] = slice(layer, layer + 1)
                     self.material_id[tuple(key)] = pec_id
         self._state = self._make_state()
-        lib = load_library()
+        lib, _ = load_library(self.precision)
         for source in self.sources:
             cb = lib.oracle_em3d_face_cb(ctypes.byref(self._state), source['axis'], *source['cell'])
-            source['weight'] = np.float32(np.float32(cb) * DTYPE(source['moment'] / source['volume']))
+            source['weight'] = self.real(self.real(cb) * self.real(source['moment'] / source['volume']))
         interval = dft_sample_interval(self.dt, [_SourceView(s) for s in self.sources],
                                        [m.frequencies for m in self.monitors])
         for monitor in self.monitors:
@@ -371,7 +394,7 @@ class OracleEM3D:
                 plane.sample_interval = interval
 
     def _make_state(self):
-        st = _State()
+        st = load_library(self.precision)[1]()
         st.nx, st.ny, st.nz = self.shape
         st.px, st.py, st.pz = (int(p) for p in self.periodic)
         for name, arr in self.fields.items():
@@ -385,7 +408,7 @@ class OracleEM3D:
             setattr(st, f'ih{a}', _fp(self.inv_h[axis]))
             setattr(st, f'wl{a}', _fp(self.shares[axis][0]))
             setattr(st, f'wu{a}', _fp(self.shares[axis][1]))
-        st.dt = DTYPE(self.dt)
+        st.dt = self.real(DTYPE(self.dt))
         for axis in range(3):
             h, e = self.layers.get((axis, 'h')), self.layers.get((axis, 'e'))
             st.nr[axis] = h['n_rows'] if h else 0
@@ -400,10 +423,10 @@ class OracleEM3D:
 
     # ---- stepping (engine3d.py:497-554)
     def source_value(self, source, t_half):
-        return DTYPE(source['temporal'](t_half))
+        return self.real(source['temporal'](t_half))
 
     def run(self, n_steps):
-        lib = load_library()
+        lib, _ = load_library(self.precision)
         for _ in range(int(n_steps)):
             t = self.time
             lib.oracle_em3d_update_h(ctypes.byref(self._state))
@@ -413,7 +436,7 @@ class OracleEM3D:
                 value = self.source_value(source, t_half)
                 field = self.fields['e' + 'xyz'[source['axis']]]
                 i, j, k = source['cell']
-                field[i, j, k] = np.float32(field[i, j, k] + np.float32(value * source['weight']))
+                field[i, j, k] = self.real(field[i, j, k] + self.real(value * source['weight']))
             self.time = t + self.dt
             self.n_step += 1
             for monitor in self.monitors:

@@ -107,3 +107,42 @@ def paint(spec):
 def boundary_faces(spec):
     """Face type per FACES_3D face (missing = cpml)."""
     return {f'{axis}_{side}': spec['faces'].get(f'{axis}_{side}', 'cpml') for axis in 'xyz' for side in ('lo', 'hi')}
+
+
+def roofline_3d_oracle(precision='single', total_cells=512, npml=12, n_spheres=500, seed=2025):
+    """(OracleEM3D, flux box) of the 3D benchmark workload (opensol_b200.workloads.roofline_3d_physics: a
+    total_cells^3 grid incl. npml CPML cells per face, n_spheres seeded dielectric spheres painted in draw order on the
+    cells whose centre lies within the radius, a centred z dipole, a closed 8-frequency flux box), finalized.  The
+    spheres are painted here, over each sphere's bounding box of cell centres, from the same seeded draws as the
+    workload."""
+    from oracle.fdtd3d import OracleEM3D
+    from opensol_b200 import workloads
+    from opensol_b200.constants import C0
+    spec = workloads.ROOFLINE_3D
+    dx = spec['dx']
+    window = (total_cells - 2 * npml) * dx
+    o = OracleEM3D(window, window, window, dx, npml=npml, precision=precision)
+    rng = np.random.default_rng(seed)
+    radius = rng.uniform(*spec['radius'], n_spheres)
+    centres = rng.uniform(0.15 * window, 0.85 * window, (n_spheres, 3))
+    eps = rng.uniform(*spec['eps_r'], n_spheres)
+    cell_centres = [0.5 * (e[:-1] + e[1:]) for e in o.edges]
+    eps_r = o.materials['eps_r']
+    for centre, r, e in zip(centres, radius, eps):
+        box = []
+        for a in range(3):
+            lo = int(np.searchsorted(cell_centres[a], centre[a] - r, side='left'))
+            hi = int(np.searchsorted(cell_centres[a], centre[a] + r, side='right'))
+            box.append(slice(lo, hi))
+        x, y, z = (cell_centres[a][box[a]] for a in range(3))
+        inside = ((x[:, None, None] - centre[0]) ** 2 + (y[None, :, None] - centre[1]) ** 2
+                  + (z[None, None, :] - centre[2]) ** 2) <= r * r
+        eps_r[tuple(box)][inside] = np.float32(e)
+    o.add_dipole(0.5 * window, 0.5 * window, 0.5 * window, orientation='z', dipole_moment=1e-12,
+                 wavelength=spec['wavelength'], bandwidth=spec['bandwidth'])
+    f0 = C0 / spec['wavelength']
+    bw = spec['bandwidth']
+    freqs = np.linspace(f0 * (1 - bw / 2), f0 * (1 + bw / 2), spec['n_freqs'])
+    box = o.add_flux_box((0.2 * window,) * 3, (0.8 * window,) * 3, frequencies=freqs)
+    o.finalize()
+    return o, box

@@ -256,24 +256,31 @@ def test_duration_run_matches_reference_ticks_and_flux():
 
 
 def test_roofline_workload_full_size_bit_exact():
-    """The 8192^2 benchmark grid (2000 cylinders, 4 x 16-frequency lines) for 26 steps (one DFT sample) against the
-    oracle on the host: every field bit-identical at full size."""
+    """The 8192^2 benchmark grid (2000 cylinders, 4 x 16-frequency lines) for 600 steps against the oracle on the host:
+    every field and every monitor's complex128 E / H spectra bit-identical at full size.  By step 600 the pulse has
+    crossed the lo-x flux line and reached the first cylinders, and 23 DFT samples have been taken."""
     args = workloads.roofline_2d_sim_args()
     ops = workloads.roofline_2d_ops()
     sim = ob.Simulation(**args, verbose=False)
     mons = workloads.apply(sim, ops)
     o = OracleEz2D(**args)
     omons = workloads.apply(o, ops)
-    n = 27
+    n = 600
     sim.run(n_steps=n, verbose=False)
     o.run(n_steps=n)
     assert sim.grid.nx == sim.grid.ny == 8192
     assert mons[0].sample_interval == o.sample_interval
     for name, arr in _fields(sim).items():
         np.testing.assert_array_equal(arr, getattr(o, name))
+    crossed = 0
     for mon, omon in zip(mons, omons):
-        e, _ = mon.spectra()
+        e, h = mon.spectra()
         np.testing.assert_array_equal(e, omon.e_acc)
+        np.testing.assert_array_equal(h, omon.h_acc)
+        np.testing.assert_array_equal(mon.flux(), omon.flux())
+        crossed += bool(np.abs(e).max() > 0)
+    assert crossed >= 1
+    sim.clear()
 
 
 def test_roofline_workload_linearity():

@@ -124,3 +124,28 @@ def test_workload_512_deterministic_across_x_chunks():
     assert np.abs(out[0][0]).max() > 0
     for a, b in zip(out[0], out[1]):
         np.testing.assert_array_equal(a, b)
+
+
+def test_workload_512_against_oracle():
+    """The 3D benchmark workload at its full size (512^3 incl. CPML 12, 500 spheres, z dipole, 8-frequency flux box)
+    for 200 steps (7 DFT samples) against the oracle on the host: the painted eps_r, all six fields, every plane's
+    complex128 spectra and the box flux bit-identical."""
+    from cases3d import roofline_3d_oracle
+    from opensol_b200 import workloads
+    physics, box = workloads.roofline_3d_physics()
+    physics.finalize()
+    o, obox = roofline_3d_oracle()
+    np.testing.assert_array_equal(physics.domain.materials.array('eps_r'), o.materials['eps_r'])
+    assert box.sample_interval == obox.sample_interval
+    n = 200
+    physics.run(n)
+    o.run(n)
+    engine = physics.engine
+    for name in FIELDS:
+        np.testing.assert_array_equal(engine.read_field(name), o.fields[name], err_msg=name)
+    assert np.abs(o.fields['ez']).max() > 0
+    for plane, oplane in zip(box.planes(), obox.planes()):
+        for (e, h), opair in zip(plane.spectra(), oplane.pairs):
+            np.testing.assert_array_equal(e, opair['e_dft'])
+            np.testing.assert_array_equal(h, opair['h_dft'])
+    np.testing.assert_array_equal(np.asarray(box.flux()), np.asarray(obox.flux()))
