@@ -49,6 +49,9 @@ def parse_args():
                    'workload; smaller grids scale the sphere count with the volume, for profiling)')
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-e2e', action='store_true')
+    p.add_argument('--no-replay', action='store_true', help='skip the reference-kernel replay leg')
+    p.add_argument('--no-secondary', action='store_true',
+                   help='skip the H_z, 3D, serving and adjoint figures that follow the headline')
     p.add_argument('--variant', type=int, default=1, help='1: temporally blocked kernels (default), 0: per step')
     p.add_argument('--steps-per-launch', type=int, default=3)
     p.add_argument('--tile-rows', type=int, default=0, help='rows per interior tile (0: autotune)')
@@ -151,6 +154,35 @@ def cpu_baseline(sample_steps=CPU_SAMPLE_STEPS):
             'sample': f'{sample_steps} Yee steps of the 8192x8192 roofline grid after 2 warm-up steps, '
                       f'C restatement with OpenMP on {os.cpu_count()} threads',
             'wall_s': wall}
+
+
+def gpu_reference_replay(args, device, value, warmup_steps=50, timed_steps=2000):
+    """open_sol's own GPU step on the same workload: the reference-kernel replay (its update_h / update_e RawKernels
+    compiled unchanged for sm_100a, the CPML, source and DFT launches of its step sequence, H and E blocks replayed
+    as CUDA graphs), timed with CUDA events over timed_steps steps after warmup_steps; ratio = this engine's value
+    over the replay's."""
+    from oracle import replay_ez2d
+    ok, why = replay_ez2d.available()
+    if not ok:
+        return {'unavailable': why}
+    from oracle.fdtd2d import OracleEz2D
+    from opensol_b200 import workloads
+    o = OracleEz2D(**workloads.roofline_2d_sim_args(total_cells=args.grid))
+    workloads.apply(o, workloads.roofline_2d_ops(total_cells=args.grid))
+    o.finalize()
+    replay = replay_ez2d.ReferenceReplayEz2D(o, device)
+    try:
+        replay.run(warmup_steps)
+        replay.reset()
+        ms = replay.run(timed_steps)
+    finally:
+        replay.close()
+    rate = o.domain.nx * o.domain.ny * timed_steps / (ms / 1e3) / 1e9
+    return {'value': rate, 'unit': 'Gcell-updates/s', 'steps': timed_steps, 'ms': ms, 'ratio': value / rate,
+            'kind': 'reference-kernel replay',
+            'what': "open_sol's update_h_kernel / update_e_kernel (fdtd_ez_2d_kernels.py:23-122) compiled unchanged "
+                    'for sm_100a with (32, 8, 1) blocks, its CPML psi / source / DFT elementwise launches restated, '
+                    'the H and E blocks replayed as CUDA graphs per step as its _fixed_block does'}
 
 
 def run_reference(args):
@@ -301,6 +333,10 @@ def run_b200(args):
     sim.clear()
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.grid == 8192:
         line['cpu_baseline'] = cpu_baseline()
+    if rank == 0 and world == 1 and not args.no_replay:
+        line['gpu_reference_replay'] = gpu_reference_replay(args, local, value)
+    if rank == 0 and world == 1 and not args.no_secondary and args.grid == 8192:
+        line['secondary'] = secondary_workloads(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     group.close()
@@ -418,7 +454,7 @@ def run_hz2d(args):
     sim.clear()
     if not args.no_cpu_baseline and args.grid == 8192:
         line['cpu_baseline'] = cpu_baseline_hz()
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def cpu_baseline_hz(sample_steps=CPU_SAMPLE_STEPS):
@@ -495,7 +531,7 @@ def run_em3d(args):
         if t:
             line['roofline']['traffic'] = t['dram_bytes_per_cell_update'] * cells   # per step (both kernels)
             line['roofline']['traffic_note'] = t['note']
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_serving(args):
@@ -545,11 +581,14 @@ def run_serving(args):
             'cell_updates_per_s_batched': work / t_batch, 'fluxes_equal_alone_and_batched': bool(same),
             'latency_p50_s': p50, 'latency_p99_s': p99, 'realtime_makespan_s': t_rt,
             'timing': 'host wall clock (synchronised), one process, one B200'}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_adjoint(args):
-    """The adjoint workload (opensol_b200/workloads.py adjoint_2d_problem): wall(forward + gradient) / wall(forward)."""
+    """The adjoint workload (opensol_b200/workloads.py adjoint_2d_problem): the cost of one gradient (forward with
+    checkpoints + backward) over the cost of one plain forward of the same problem through the public API
+    (Simulation.run of all its steps from rest + flux()).  Both are host wall clock around synchronized calls; the
+    device time of each (CUDA events on the engine's stream) is reported beside it."""
     import numpy as np
     import torch
     from opensol_b200 import workloads
@@ -557,32 +596,89 @@ def run_adjoint(args):
     torch.cuda.set_device(0)
     spec = workloads.ADJOINT_2D
     sim, monitor, box, eps = workloads.adjoint_2d_problem()
-    sim.em.engine.configure(tile_rows=32)
+    engine = sim.em.engine
+    stream = torch.cuda.Stream()
+    engine.set_stream(stream.cuda_stream)
     adj = FluxAdjoint2D(sim, monitor, 0, box, spec['steps'], checkpoint_every=spec['checkpoint_every'])
-    adj.forward()
-    adj.backward()
-    fw, bw = [], []
-    for _ in range(max(1, args.steps)):
-        t0 = time.perf_counter()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def plain_forward():
+        engine.reset()
+        sim.run(n_steps=spec['steps'], verbose=False, print_every=0)
+        return float(monitor.flux()[0])
+
+    def gradient():
         J = adj.forward()
-        sim.em.engine.synchronize()
-        t1 = time.perf_counter()
-        grad = adj.backward()
-        t2 = time.perf_counter()
-        fw.append(t1 - t0)
-        bw.append(t2 - t1)
-    f, b = min(fw), min(bw)
-    line = {'metric': 'adjoint gradient cost / forward cost', 'value': (f + b) / f, 'unit': 'x',
-            'n_gpus': 1, 'steps': len(fw), 'warmup': 1, 'ms_per_step': (f + b) * 1e3, 'higher_is_better': False,
+        return J, adj.backward()
+
+    plain_forward()
+    gradient()
+    torch.cuda.synchronize()
+    plain, plain_dev, grad_wall, grad_dev, fw_wall = [], [], [], [], []
+    with ClockSampler(0) as clocks:
+        for _ in range(max(3, args.steps)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            start.record(stream)
+            J_plain = plain_forward()
+            stop.record(stream)
+            torch.cuda.synchronize()
+            plain.append(time.perf_counter() - t0)
+            plain_dev.append(start.elapsed_time(stop) / 1e3)
+            t0 = time.perf_counter()
+            start.record(stream)
+            J = adj.forward()
+            engine.synchronize()
+            t1 = time.perf_counter()
+            grad = adj.backward()
+            stop.record(stream)
+            torch.cuda.synchronize()
+            grad_wall.append(time.perf_counter() - t0)
+            fw_wall.append(t1 - t0)
+            grad_dev.append(start.elapsed_time(stop) / 1e3)
+    assert J == J_plain, 'the checkpointed forward differs from the plain run'
+    p, g = statistics.median(plain), statistics.median(grad_wall)
+    cells = engine.nx * engine.ny
+    line = {'metric': 'adjoint gradient cost / plain forward cost', 'value': g / p, 'unit': 'x',
+            'n_gpus': 1, 'steps': len(plain), 'warmup': 1, 'ms_per_step': g * 1e3, 'higher_is_better': False,
             'scaling': 'strong', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-            'config': {'workload': f'adjoint: {sim.em.engine.nx}^2 total grid incl. 20 CPML cells/side, dx 20 nm, '
+            'config': {'workload': f'adjoint: {engine.nx}^2 total grid incl. 20 CPML cells/side, dx 20 nm, '
                                    f'{box[1] - box[0]}x{box[3] - box[2]} design box eps_r U(1,12.1), 1550 nm line '
                                    f'source, flux objective at 1550 nm after {spec["steps"]} steps, checkpoints '
                                    f'every {spec["checkpoint_every"]}'},
-            'forward_s': f, 'backward_s': b, 'objective': J, 'grad_abs_max': float(np.abs(grad).max()),
-            'forward_gcell_updates_per_s': sim.em.engine.nx * sim.em.engine.ny * spec['steps'] / f / 1e9,
-            'timing': 'host wall clock (synchronised), best of the timed repeats'}
-    print(json.dumps(line), flush=True)
+            'plain_forward_s': p, 'gradient_s': g, 'checkpointed_forward_s': statistics.median(fw_wall),
+            'plain_forward_device_s': statistics.median(plain_dev), 'gradient_device_s': statistics.median(grad_dev),
+            'device_ratio': statistics.median(grad_dev) / statistics.median(plain_dev),
+            'plain_forward_gcell_updates_per_s': cells * spec['steps'] / p / 1e9,
+            'objective': J, 'grad_abs_max': float(np.abs(grad).max()), 'clocks': clocks.summary(),
+            'timing': 'host wall clock around synchronized calls (median of the repeats); device time by CUDA events '
+                      'on the engine stream'}
+    return line
+
+
+def secondary_workloads(args):
+    """The other benchmark configurations, each run once in this process after the headline and reported inside its
+    JSON line with its own clock record: the same grid in the H_z polarisation, the 512^3 3D run, the serving stream
+    against one-at-a-time runs, and the adjoint gradient against a plain forward."""
+    import copy
+    import torch
+    out = {}
+    plans = [('hz2d', run_hz2d, {'steps': 2, 'warmup': 1, 'sim_steps': SIM_STEPS, 'no_cpu_baseline': True}),
+             ('em3d', run_em3d, {'steps': 1, 'warmup': 1, 'sim_steps': SIM_STEPS}),
+             ('adjoint', run_adjoint, {'steps': 3, 'warmup': 1}),
+             ('serving', run_serving, {'jobs': 32})]
+    for name, fn, overrides in plans:
+        a = copy.copy(args)
+        for key, value in overrides.items():
+            setattr(a, key, value)
+        try:
+            line = fn(a)
+            out[name] = {k: v for k, v in line.items() if k not in ('n_gpus', 'data', 'vs_baseline')}
+        except Exception as error:   # a failing secondary figure is reported, the headline stands
+            out[name] = {'error': f'{type(error).__name__}: {error}'}
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return out
 
 
 def main():
@@ -590,16 +686,11 @@ def main():
     if args.impl == 'reference':
         run_reference(args)
         return
-    if args.workload == 'em3d':
-        run_em3d(args)
-    elif args.workload == 'hz2d':
-        run_hz2d(args)
-    elif args.workload == 'serving':
-        run_serving(args)
-    elif args.workload == 'adjoint':
-        run_adjoint(args)
-    else:
+    if args.workload == 'roofline_2d':
         run_b200(args)
+        return
+    fn = {'em3d': run_em3d, 'hz2d': run_hz2d, 'serving': run_serving, 'adjoint': run_adjoint}[args.workload]
+    print(json.dumps(fn(args)), flush=True)
 
 
 if __name__ == '__main__':

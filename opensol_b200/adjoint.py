@@ -43,6 +43,7 @@ class FluxAdjoint2D:
                                                               ctypes.byref(out)))
         self._handle = out
         self._tables = None
+        self._slot_tables = None   # per checkpoint segment: the chunk tables of its steps (clock from rest)
 
     def close(self):
         if self._handle is not None:
@@ -64,21 +65,36 @@ class FluxAdjoint2D:
         materials.version += 1   # an in-place write: the engine re-uploads the coefficients at the next sync
         self.sim.em.materials_changed(('eps_r',))
 
+    def _prepare_tables(self):
+        """The source values and DFT phases of the whole run and of each checkpoint segment, for a run from rest.
+        They depend on the clock, the sources' waveforms and the monitors' frequencies only, not on eps_r, so they are
+        built once and reused by every forward."""
+        engine = self.engine
+        engine.reset()
+        self._tables = engine.chunk_tables(self.n_steps)
+        slots = []
+        for slot in range(self.n_slots):
+            n = min(self.K, self.n_steps - slot * self.K)
+            tables = engine.chunk_tables(n)
+            slots.append(tables)
+            engine.n_step += n          # the clock of the next segment's tables (no device work)
+            engine.time = tables[-1]
+        engine.reset()
+        self._slot_tables = slots
+
     def forward(self, eps_box=None):
         """Run from rest; returns J."""
         if eps_box is not None:
             self.set_design(eps_box)
         engine = self.engine
-        engine.reset()
         self.sim.em.finalize()
-        self._tables = engine.chunk_tables(self.n_steps)   # the whole run's source values and phases (no state)
+        if self._slot_tables is None:
+            self._prepare_tables()
+        engine.reset()
         lib = _native.load()
-        done = 0
         for slot in range(self.n_slots):
             _native.check(lib.os_fdtd2d_adjoint_save(self._handle, slot))
-            n = min(self.K, self.n_steps - done)
-            engine.advance(n)
-            done += n
+            engine.advance(min(self.K, self.n_steps - slot * self.K), self._slot_tables[slot])
         return float(self.monitor.flux()[self.freq_index])
 
     # ---- backward
