@@ -126,8 +126,10 @@ class EMPhysics:
 
     def materials_changed(self, names) -> None:
         """Materials were rewritten: the device coefficients follow at the next step (the engine tracks the
-        MaterialGrid version) and the sources recalibrate (physics/em/__init__.py:205-209)."""
+        MaterialGrid version, bumped here for writes made in place on the arrays) and the sources recalibrate
+        (physics/em/__init__.py:205-209)."""
         if frozenset(names) & {'eps_r', 'eps_xx', 'eps_yy', 'sigma_e', 'mu_r', 'sigma_m'}:
+            self.domain.materials.version += 1
             self._calibration_dirty = True
 
     def renderer(self):
