@@ -224,11 +224,13 @@ int os_fdtd2d_advance(OsFdtd2D *h, int64_t n_steps, const float *line_values, in
 /* os_fdtd2d_advance without any device allocation; no open_sol counterpart.  Same arguments, checks and results as os_fdtd2d_advance, but the chunk's tables go
  * to a fixed file-scope device array of OS_FDTD_NOALLOC_MAX_FLOATS floats instead of the handle's grow-only
  * buffers: for callers that must not allocate mid-run (jobs sharing a GPU on several streams, where cudaFree's
- * device-wide wait would stall the others; jobs held to a fixed memory budget).  Limits: n_sources * n_steps
- * source values plus the phase floats (rounded to 64 after the values) must fit, else OS_ERR_INVALID and nothing
- * runs; profiling must be off.  The first call per device looks the array up (it may load the module), so make it
- * before any stream capture.  One array per device and process: calls whose device work may overlap (unordered
- * streams) race on it. */
+ * device-wide wait would stall the others; jobs held to a fixed memory budget).  Refusals, each with nothing run:
+ * n_sources * n_steps source values plus the phase floats (counted only when phases is given, rounded to 64 after
+ * the values) must fit, else OS_ERR_INVALID; profiling must be off, and field probes must already have rows for the
+ * chunk (advance once with os_fdtd2d_advance to reserve them), else OS_ERR_STATE.  The first call per device looks
+ * the array up (it may load the module), so make it before any stream capture; the address is kept for the life of
+ * the process, so do not call it again on a device after cudaDeviceReset.  One array per device and process: calls
+ * whose device work may overlap (unordered streams) race on it. */
 int os_fdtd2d_advance_noalloc(OsFdtd2D *h, int64_t n_steps, const float *line_values, int64_t first_sample,
                               int64_t n_samples, const float *phases);
 
@@ -402,6 +404,19 @@ int os_fdtd3d_set_stream(OsFdtd3D *h, void *cuda_stream);
 
 /* x planes each block of the H / E kernels streams (chosen from the grid at create; results do not depend on it). */
 int os_fdtd3d_set_x_chunk(OsFdtd3D *h, int32_t planes);
+
+/* Step form (results bit-identical; no counterpart in open_sol, which has one form): 0 (the default) = the H and
+ * the E kernel over the whole grid in place; 1 = one fused H + E kernel over every cell but the outermost layer of
+ * each axis plus the two-kernel update of that layer, on two field sets and two CPML psi sets swapped every step
+ * (twice the field memory, a third less DRAM traffic per step). */
+int os_fdtd3d_set_variant(OsFdtd3D *h, int32_t variant);
+
+/* Launch shape of the fused kernel, 0..4 (tile rows 16 or 8 and the blocks per SM its registers are cut for; 3 by
+ * default); speed only, results bit-identical. */
+int os_fdtd3d_set_fused_config(OsFdtd3D *h, int32_t config);
+
+/* The fused box (i0, i1, j0, j1, k0, k1) and whether the next advance uses it (*fused = 1). */
+int os_fdtd3d_interior(OsFdtd3D *h, int32_t *box6, int32_t *fused);
 int os_fdtd3d_last_advance_ms(OsFdtd3D *h, float *ms);
 int os_fdtd3d_launch_count(OsFdtd3D *h, int64_t *launches);
 int os_fdtd3d_step_count(OsFdtd3D *h, int64_t *n_step);

@@ -109,6 +109,9 @@ SIGNATURES = {
     'os_fdtd3d_set_rows': [_P, _F, _F, _F, _F, _F, _F, _F],
     'os_fdtd3d_set_materials': [_P, ctypes.POINTER(ctypes.c_uint16), _I32, _F, _F, _F, _F, _F, _F, ctypes.c_float],
     'os_fdtd3d_set_cpml_axis': [_P, _I32, _I32, ctypes.POINTER(_I32), _F, _F, ctypes.POINTER(_I32), _F, _F],
+    'os_fdtd3d_set_variant': [_P, _I32],
+    'os_fdtd3d_set_fused_config': [_P, _I32],
+    'os_fdtd3d_interior': [_P, ctypes.POINTER(_I32), ctypes.POINTER(_I32)],
     'os_fdtd3d_face_cb': [_P, _I32, _I32, _I32, _I32, _F],
     'os_fdtd3d_add_dipole': [_P, _I32, _I32, _I32, _I32, ctypes.c_float, ctypes.POINTER(_I32)],
     'os_fdtd3d_set_dipole_weight': [_P, _I32, ctypes.c_float],

@@ -1,8 +1,15 @@
 // 3D FDTD engine for sm_100a: device state, launches and the os_fdtd3d_* C ABI (replaces open_sol's FDTDEngine3D,
 // physics/em3d/engine3d.py:157-554, for a Cartesian grid with one real field set and float32 fields).
 //
-// One Yee step = em3d_h_kernel (H with its CPML) then em3d_e_kernel (E with its CPML and the dipole injection), the
-// reference's own step order (engine3d.py:497-554); on DFT sample steps em3d_flux_kernel accumulates every flux pair.
+// One Yee step follows the reference's own order (engine3d.py:497-554): H with its CPML, then E with its CPML and the
+// dipole injection; on DFT sample steps em3d_flux_kernel accumulates every flux pair.  Two forms, bit-identical:
+//   variant 1: two field sets and two CPML psi sets, read one, write the other, swapped after every step.
+//     em3d_fused_kernel does H and E of every cell but the outermost layer of each axis in one pass (each field and
+//     psi read and written once); that layer (where samples cross the grid edge) runs em3d_h_kernel over its six
+//     faces, then em3d_e_kernel, which reads the new H of both parts;
+//   variant 0 (default): em3d_h_kernel then em3d_e_kernel over the whole grid, in place on one field set.
+// Variant 1 moves 52.8 B per cell-update against variant 0's 79.5 (ncu, 256^3) but issues from fewer resident warps
+// (one barrier per plane, 80 registers a thread), and on 512^3 it runs 42.6 G cell-updates/s against 44.8.
 // A chunk of n steps is enqueued with no host synchronisation: per-step dipole amplitudes and per-sample DFT phases
 // arrive as small tables computed on the host in float64 and rounded as open_sol rounds them.
 #include "common.cuh"
@@ -19,6 +26,10 @@ struct OsFdtd3D {
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     bool timed = false;
     os::DeviceArray<float> field[6];            // ex, ey, ez, hx, hy, hz
+    os::DeviceArray<float> field2[6];           // the second field set of variant 1 (allocated on first use)
+    int cur = 0;                                // the set holding the current state (0: field, 1: field2)
+    int32_t variant = 0;                        // the faster form on 512^3 (44.8 vs 42.6 G cell-updates/s)
+    int32_t fused_config = 3;                   // tile rows / blocks per SM of em3d_fused_kernel (speed only)
     os::DeviceArray<uint16_t> mat;
     os::DeviceArray<float> tables;              // t_ex, t_ey, t_ez, t_sig, t_da, t_db (6 * n_ids)
     os::DeviceArray<float> same;                // same-id face ca, cb per component (6 * n_ids)
@@ -33,6 +44,7 @@ struct OsFdtd3D {
         os::DeviceArray<int32_t> rm;            // rm_e (n), rm_h (n)
         os::DeviceArray<float> coef;            // b_e, g_e, b_h, g_h (nr each)
         os::DeviceArray<float> psi;             // pe_first, pe_second, ph_first, ph_second
+        os::DeviceArray<float> psi2;            // the second psi set of variant 1 (allocated on first use)
         size_t psi_count = 0;
     } cpml[3];
     struct Dipole {
@@ -64,6 +76,23 @@ static int bind3(OsFdtd3D *h) {
 
 static size_t cells3(const OsFdtd3D *h) { return (size_t)h->grid.nx * h->grid.ny * h->grid.nz; }
 
+// Component c (ex, ey, ez, hx, hy, hz) of field set `set`.
+static float *fset(const OsFdtd3D *h, int set, int c) { return set ? h->field2[c].ptr : h->field[c].ptr; }
+
+// x chunks of box b along x.
+static int32_t box_chunks(const Em3DBox &b, int32_t x_chunk) {
+    return b.i1 > b.i0 ? (b.i1 - b.i0 + x_chunk - 1) / x_chunk : 0;
+}
+
+// Boxes of em3d_h_kernel / em3d_e_kernel: one box, the whole grid.
+static void whole_grid_boxes(const OsFdtd3D *h, Em3DParams &p) {
+    const OsGrid3D &g = h->grid;
+    p.n_boxes = 1;
+    p.boxes[0] = Em3DBox{0, g.nx, 0, g.ny, 0, g.nz};
+    p.zbase[0] = 0;
+    p.zbase[1] = box_chunks(p.boxes[0], p.x_chunk);
+}
+
 static Em3DParams make_params3(const OsFdtd3D *h) {
     Em3DParams p{};
     const OsGrid3D &g = h->grid;
@@ -74,12 +103,13 @@ static Em3DParams make_params3(const OsFdtd3D *h) {
     p.py = g.periodic[1];
     p.pz = g.periodic[2];
     p.x_chunk = h->x_chunk;
-    p.ex = h->field[0].ptr;
-    p.ey = h->field[1].ptr;
-    p.ez = h->field[2].ptr;
-    p.hx = h->field[3].ptr;
-    p.hy = h->field[4].ptr;
-    p.hz = h->field[5].ptr;
+    p.ex = p.oex = fset(h, h->cur, 0);
+    p.ey = p.oey = fset(h, h->cur, 1);
+    p.ez = p.oez = fset(h, h->cur, 2);
+    p.hx = p.ohx = fset(h, h->cur, 3);
+    p.hy = p.ohy = fset(h, h->cur, 4);
+    p.hz = p.ohz = fset(h, h->cur, 5);
+    whole_grid_boxes(h, p);
     p.mat = h->mat.ptr;
     const int n = h->n_ids;
     const float *t = h->tables.ptr;
@@ -123,10 +153,11 @@ static Em3DParams make_params3(const OsFdtd3D *h) {
         q.g_e = c.coef.ptr + c.nr;
         q.b_h = c.coef.ptr + 2 * c.nr;
         q.g_h = c.coef.ptr + 3 * c.nr;
-        q.pe_first = c.psi.ptr;
-        q.pe_second = c.psi.ptr + c.psi_count;
-        q.ph_first = c.psi.ptr + 2 * c.psi_count;
-        q.ph_second = c.psi.ptr + 3 * c.psi_count;
+        float *psi = h->cur ? c.psi2.ptr : c.psi.ptr;
+        q.pe_first = q.ope_first = psi;
+        q.pe_second = q.ope_second = psi + c.psi_count;
+        q.ph_first = q.oph_first = psi + 2 * c.psi_count;
+        q.ph_second = q.oph_second = psi + 3 * c.psi_count;
     }
     p.n_dip = (int32_t)h->dipoles.size();
     for (size_t d = 0; d < h->dipoles.size(); ++d) {
@@ -139,6 +170,7 @@ static Em3DParams make_params3(const OsFdtd3D *h) {
 }
 
 static int zero_state3(OsFdtd3D *h) {
+    h->cur = 0;
     for (auto &f : h->field) OS_CUDA(cudaMemsetAsync(f.ptr, 0, f.bytes(), h->stream));
     for (auto &c : h->cpml)
         if (c.psi.ptr) OS_CUDA(cudaMemsetAsync(c.psi.ptr, 0, c.psi.bytes(), h->stream));
@@ -147,9 +179,95 @@ static int zero_state3(OsFdtd3D *h) {
     return OS_OK;
 }
 
-static dim3 grid3(const OsFdtd3D *h) {
-    return dim3((unsigned)((h->grid.nz + EM3D_BZ - 1) / EM3D_BZ), (unsigned)((h->grid.ny + EM3D_BY - 1) / EM3D_BY),
-                (unsigned)((h->grid.nx + h->x_chunk - 1) / h->x_chunk));
+// Launch grid of em3d_h_kernel / em3d_e_kernel with bz x by blocks over p's boxes.
+static dim3 box_grid(const Em3DParams &p, int bz = EM3D_BZ, int by = EM3D_BY) {
+    int32_t nj = 0, nk = 0;
+    for (int b = 0; b < p.n_boxes; ++b) {
+        nj = std::max(nj, p.boxes[b].j1 - p.boxes[b].j0);
+        nk = std::max(nk, p.boxes[b].k1 - p.boxes[b].k0);
+    }
+    return dim3((unsigned)((nk + bz - 1) / bz), (unsigned)((nj + by - 1) / by), (unsigned)p.zbase[p.n_boxes]);
+}
+
+// variant 1's fused box: every cell but the outermost layer of each axis.
+static Em3DBox fused_box(const OsFdtd3D *h) {
+    const OsGrid3D &g = h->grid;
+    return Em3DBox{1, g.nx - 1, 1, g.ny - 1, 1, g.nz - 1};
+}
+
+static bool fused_active(const OsFdtd3D *h) {
+    const OsGrid3D &g = h->grid;
+    return h->variant == 1 && g.nx >= 3 && g.ny >= 3 && g.nz >= 3;
+}
+
+// The outermost layer around the fused box: the x and y faces (coalesced along k: 32 x 8 blocks) or the z faces
+// (one k per face: blocks of 256 threads along j).
+static void face_boxes(const OsFdtd3D *h, Em3DParams &p, bool z_faces) {
+    const OsGrid3D &g = h->grid;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const Em3DBox xy[4] = {{0, 1, 0, ny, 0, nz}, {nx - 1, nx, 0, ny, 0, nz},
+                           {1, nx - 1, 0, 1, 0, nz}, {1, nx - 1, ny - 1, ny, 0, nz}};
+    const Em3DBox zf[2] = {{1, nx - 1, 1, ny - 1, 0, 1}, {1, nx - 1, 1, ny - 1, nz - 1, nz}};
+    const Em3DBox *all = z_faces ? zf : xy;
+    const int n = z_faces ? 2 : 4;
+    p.n_boxes = 0;
+    p.zbase[0] = 0;
+    for (int q = 0; q < n; ++q) {
+        const Em3DBox &b = all[q];
+        p.boxes[p.n_boxes] = b;
+        p.zbase[p.n_boxes + 1] = p.zbase[p.n_boxes] + box_chunks(b, p.x_chunk);
+        ++p.n_boxes;
+    }
+}
+
+// Point the psi of p's CPML axes: read set `in`, write set `out`.
+static void point_psi(const OsFdtd3D *h, Em3DParams &p, int in, int out) {
+    for (int a = 0; a < 3; ++a) {
+        const auto &c = h->cpml[a];
+        if (!c.nr) continue;
+        float *pi = in ? c.psi2.ptr : c.psi.ptr, *po = out ? c.psi2.ptr : c.psi.ptr;
+        Em3DCpmlAxis &q = p.cpml[a];
+        q.pe_first = pi;
+        q.pe_second = pi + c.psi_count;
+        q.ph_first = pi + 2 * c.psi_count;
+        q.ph_second = pi + 3 * c.psi_count;
+        q.ope_first = po;
+        q.ope_second = po + c.psi_count;
+        q.oph_first = po + 2 * c.psi_count;
+        q.oph_second = po + 3 * c.psi_count;
+    }
+}
+
+// em3d_fused_kernel configurations: (tile rows, blocks per SM the register budget is cut for).
+constexpr int FUSED_CONFIGS = 5;
+static int fused_rows(int config) { return config == 0 || config == 1 ? 16 : 8; }
+
+static int launch_fused(int config, dim3 grid, const Em3DParams &p, const Em3DBox &in, cudaStream_t s) {
+    switch (config) {
+        case 0: em3d_fused_kernel<16, 1><<<grid, dim3(EM3D_FZ, 16), 0, s>>>(p, in); break;
+        case 1: em3d_fused_kernel<16, 2><<<grid, dim3(EM3D_FZ, 16), 0, s>>>(p, in); break;
+        case 2: em3d_fused_kernel<8, 2><<<grid, dim3(EM3D_FZ, 8), 0, s>>>(p, in); break;
+        case 3: em3d_fused_kernel<8, 3><<<grid, dim3(EM3D_FZ, 8), 0, s>>>(p, in); break;
+        default: em3d_fused_kernel<8, 4><<<grid, dim3(EM3D_FZ, 8), 0, s>>>(p, in); break;
+    }
+    OS_CUDA(cudaGetLastError());
+    return OS_OK;
+}
+
+// Point p's inputs at set `in` and its outputs at set `out` (components from c0 to c0 + 2 of each, or all).
+static void point_sets(const OsFdtd3D *h, Em3DParams &p, int e_in, int h_in, int e_out, int h_out) {
+    p.ex = fset(h, e_in, 0);
+    p.ey = fset(h, e_in, 1);
+    p.ez = fset(h, e_in, 2);
+    p.hx = fset(h, h_in, 3);
+    p.hy = fset(h, h_in, 4);
+    p.hz = fset(h, h_in, 5);
+    p.oex = fset(h, e_out, 0);
+    p.oey = fset(h, e_out, 1);
+    p.oez = fset(h, e_out, 2);
+    p.ohx = fset(h, h_out, 3);
+    p.ohy = fset(h, h_out, 4);
+    p.ohz = fset(h, h_out, 5);
 }
 
 }  // namespace os
@@ -285,6 +403,7 @@ extern "C" int os_fdtd3d_set_cpml_axis(OsFdtd3D *h, int32_t axis, int32_t n_rows
         OS_CHECK(row_map_e[r] >= -1 && row_map_e[r] < n_rows && row_map_h[r] >= -1 && row_map_h[r] < n_rows,
                  OS_ERR_INVALID, "os_fdtd3d_set_cpml_axis: row map entry %d out of [-1, %d)", r, n_rows);
     }
+
     auto &c = h->cpml[axis];
     c.nr = n_rows;
     OS_TRY(c.rm.alloc(2 * (size_t)n));
@@ -426,21 +545,61 @@ extern "C" int os_fdtd3d_advance(OsFdtd3D *h, int64_t n_steps, const float *dipo
         OS_TRY(upload(h->pairs_dev, h->pairs.data(), h->pairs.size(), h->stream));
         h->pairs_dirty = false;
     }
+    const bool fused = fused_active(h);
+    if (fused) {
+        for (auto &f : h->field2)
+            if (!f.ptr) OS_TRY(f.alloc(cells3(h)));
+        for (auto &c : h->cpml)
+            if (c.nr && !c.psi2.ptr) OS_TRY(c.psi2.alloc(4 * c.psi_count));
+    }
     Em3DParams p = make_params3(h);
     p.dip_values = h->values.ptr;
     p.values_stride = n_steps;
-    const dim3 grid = grid3(h), block(EM3D_BZ, EM3D_BY);
+    Em3DParams pz = p;   // the z faces
+    if (fused) {
+        face_boxes(h, p, false);
+        face_boxes(h, pz, true);
+    }
+    const Em3DBox in = fused_box(h);
+    const int ty = fused_rows(h->fused_config);
+    const dim3 block(EM3D_BZ, EM3D_BY), zblock(1, 256);
+    const dim3 fused_grid((unsigned)((in.k1 - in.k0 + EM3D_FZ - 2) / (EM3D_FZ - 1)),
+                          (unsigned)((in.j1 - in.j0 + ty - 2) / (ty - 1)),
+                          (unsigned)((in.i1 - in.i0 + p.x_chunk - 1) / p.x_chunk));
     OS_CUDA(cudaEventRecord(h->ev_start, h->stream));
     for (int64_t k = 0; k < n_steps; ++k) {
         p.k_step = k;
-        em3d_h_kernel<<<grid, block, 0, h->stream>>>(p);
-        em3d_e_kernel<<<grid, block, 0, h->stream>>>(p);
-        h->launches += 2;
+        pz.k_step = k;
+        if (fused) {
+            const int a = h->cur, b = a ^ 1;
+            // faces H: E^n, H^{n-1/2}, psi of set a -> H^{n+1/2}, psi' of set b
+            point_sets(h, p, a, a, b, b);
+            point_psi(h, p, a, b);
+            point_sets(h, pz, a, a, b, b);
+            point_psi(h, pz, a, b);
+            em3d_h_kernel<EM3D_BZ, EM3D_BY><<<box_grid(p), block, 0, h->stream>>>(p);
+            em3d_h_kernel<1, 256><<<box_grid(pz, 1, 256), zblock, 0, h->stream>>>(pz);
+            OS_TRY(launch_fused(h->fused_config, fused_grid, p, in, h->stream));
+            // faces E: E^n and psi of set a, H^{n+1/2} of set b -> E^{n+1}, psi' of set b
+            point_sets(h, p, a, b, b, b);
+            point_sets(h, pz, a, b, b, b);
+            em3d_e_kernel<EM3D_BZ, EM3D_BY><<<box_grid(p), block, 0, h->stream>>>(p);
+            em3d_e_kernel<1, 256><<<box_grid(pz, 1, 256), zblock, 0, h->stream>>>(pz);
+            h->launches += 5;
+            h->cur = b;
+        } else {
+            const dim3 grid = box_grid(p);
+            em3d_h_kernel<EM3D_BZ, EM3D_BY><<<grid, block, 0, h->stream>>>(p);
+            em3d_e_kernel<EM3D_BZ, EM3D_BY><<<grid, block, 0, h->stream>>>(p);
+            h->launches += 2;
+        }
         h->n_step += 1;
         if (!h->pairs.empty() && h->n_step % m == 0) {
             const int64_t q = h->n_step / m;
             const dim3 fgrid((unsigned)((h->max_pair_cells + 255) / 256), (unsigned)h->pairs.size());
-            em3d_flux_kernel<<<fgrid, 256, 0, h->stream>>>(h->pairs_dev.ptr, p.ex, p.ey, p.ez, p.hx, p.hy, p.hz,
+            const int c = h->cur;
+            em3d_flux_kernel<<<fgrid, 256, 0, h->stream>>>(h->pairs_dev.ptr, fset(h, c, 0), fset(h, c, 1),
+                                                            fset(h, c, 2), fset(h, c, 3), fset(h, c, 4), fset(h, c, 5),
                                                             h->grid.ny, h->grid.nz,
                                                             h->phases.ptr + (size_t)(q - first_sample) * row_floats);
             h->launches += 1;
@@ -455,7 +614,7 @@ extern "C" int os_fdtd3d_advance(OsFdtd3D *h, int64_t n_steps, const float *dipo
 extern "C" int os_fdtd3d_read_field(OsFdtd3D *h, int32_t component, float *out) {
     OS_CHECK(h && out && component >= 0 && component < 6, OS_ERR_INVALID, "os_fdtd3d_read_field: bad argument");
     OS_TRY(bind3(h));
-    OS_CUDA(cudaMemcpyAsync(out, h->field[component].ptr, h->field[component].bytes(), cudaMemcpyDeviceToHost,
+    OS_CUDA(cudaMemcpyAsync(out, fset(h, h->cur, component), h->field[component].bytes(), cudaMemcpyDeviceToHost,
                             h->stream));
     OS_CUDA(cudaStreamSynchronize(h->stream));
     return OS_OK;
@@ -464,7 +623,7 @@ extern "C" int os_fdtd3d_read_field(OsFdtd3D *h, int32_t component, float *out) 
 extern "C" int os_fdtd3d_write_field(OsFdtd3D *h, int32_t component, const float *in) {
     OS_CHECK(h && in && component >= 0 && component < 6, OS_ERR_INVALID, "os_fdtd3d_write_field: bad argument");
     OS_TRY(bind3(h));
-    OS_CUDA(cudaMemcpyAsync(h->field[component].ptr, in, h->field[component].bytes(), cudaMemcpyHostToDevice,
+    OS_CUDA(cudaMemcpyAsync(fset(h, h->cur, component), in, h->field[component].bytes(), cudaMemcpyHostToDevice,
                             h->stream));
     OS_CUDA(cudaStreamSynchronize(h->stream));
     return OS_OK;
@@ -509,6 +668,31 @@ extern "C" int os_fdtd3d_set_x_chunk(OsFdtd3D *h, int32_t planes) {
     OS_CHECK(h, OS_ERR_INVALID, "os_fdtd3d_set_x_chunk: null handle");
     OS_CHECK(planes >= 1, OS_ERR_INVALID, "x chunk must be >= 1 plane, got %d", planes);
     h->x_chunk = planes;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_set_variant(OsFdtd3D *h, int32_t variant) {
+    OS_CHECK(h, OS_ERR_INVALID, "os_fdtd3d_set_variant: null handle");
+    OS_CHECK(variant == 0 || variant == 1, OS_ERR_INVALID,
+             "variant must be 0 (two in-place kernels) or 1 (fused interior, two field sets), got %d", variant);
+    h->variant = variant;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_set_fused_config(OsFdtd3D *h, int32_t config) {
+    OS_CHECK(h, OS_ERR_INVALID, "os_fdtd3d_set_fused_config: null handle");
+    OS_CHECK(config >= 0 && config < FUSED_CONFIGS, OS_ERR_INVALID, "fused kernel configuration must be in [0, %d), got %d",
+             FUSED_CONFIGS, config);
+    h->fused_config = config;
+    return OS_OK;
+}
+
+extern "C" int os_fdtd3d_interior(OsFdtd3D *h, int32_t *box6, int32_t *fused) {
+    OS_CHECK(h && box6 && fused, OS_ERR_INVALID, "os_fdtd3d_interior: null argument");
+    const Em3DBox b = fused_box(h);
+    const int32_t v[6] = {b.i0, b.i1, b.j0, b.j1, b.k0, b.k1};
+    for (int q = 0; q < 6; ++q) box6[q] = v[q];
+    *fused = fused_active(h) ? 1 : 0;
     return OS_OK;
 }
 

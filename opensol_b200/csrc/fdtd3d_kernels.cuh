@@ -26,14 +26,28 @@ constexpr int EM3D_MAX_DIPOLES = 16;
 struct Em3DCpmlAxis {
     const int32_t *rm_h, *rm_e;        // grid row -> psi row (-1 outside the layers)
     const float *b_h, *g_h, *b_e, *g_e;
-    float *ph_first, *ph_second, *pe_first, *pe_second;
+    float *ph_first, *ph_second, *pe_first, *pe_second;       // psi read
+    float *oph_first, *oph_second, *ope_first, *ope_second;   // psi written (the same arrays for an in-place step)
     int32_t nr;                        // psi rows of the axis (0: no CPML on it)
 };
+
+// A box of cells [i0, i1) x [j0, j1) x [k0, k1).
+struct Em3DBox {
+    int32_t i0, i1, j0, j1, k0, k1;
+};
+
+constexpr int EM3D_MAX_BOXES = 6;
 
 struct Em3DParams {
     int32_t nx, ny, nz, px, py, pz;
     int32_t x_chunk;                   // x planes per block
-    float *ex, *ey, *ez, *hx, *hy, *hz;
+    float *ex, *ey, *ez, *hx, *hy, *hz;        // the fields a kernel reads
+    float *oex, *oey, *oez, *ohx, *ohy, *ohz;  // where it writes them (the same arrays for an in-place step)
+    // em3d_h_kernel / em3d_e_kernel: the cells they update, as boxes; blockIdx.z runs over the boxes' x chunks
+    // (zbase[b] = first z block of box b), blockIdx.x / y over the largest box's k / j extent
+    int32_t n_boxes;
+    Em3DBox boxes[EM3D_MAX_BOXES];
+    int32_t zbase[EM3D_MAX_BOXES + 1];
     const uint16_t *mat;
     const float *t_ex, *t_ey, *t_ez, *t_sig;   // E tables per material id
     const float *t_da, *t_db;                  // H coefficients per material id
@@ -58,9 +72,11 @@ struct Em3DParams {
 
 __device__ __forceinline__ float em3d_wrapped(float v) { return __fadd_rn(__fmul_rn(1.0f, v), __fmul_rn(0.0f, v)); }
 
-__device__ __forceinline__ float em3d_psi(float *psi, size_t p, float b, float g, float difference) {
-    const float value = b * psi[p] + g * difference;
-    psi[p] = value;
+// psi' = b psi + g difference, written to psi_out (psi_in itself for an in-place step); returns psi'.
+__device__ __forceinline__ float em3d_psi(const float *psi_in, float *psi_out, size_t p, float b, float g,
+                                          float difference) {
+    const float value = b * psi_in[p] + g * difference;
+    psi_out[p] = value;
     return value;
 }
 
@@ -68,19 +84,34 @@ __device__ __forceinline__ float em3d_psi(float *psi, size_t p, float b, float g
 // Thread (j, k) streams x-planes i0 .. i1 - 1.  The loads of plane i + 1 (its next plane, its y / z neighbours, its
 // own H) are issued before plane i is computed, so every warp keeps two planes of loads in flight; fields the kernel
 // only reads go through the read-only path.  In-plane offsets are 32-bit (ny nz < 2^31 is checked at create).
-__global__ void __launch_bounds__(EM3D_BZ * EM3D_BY) em3d_h_kernel(const Em3DParams p) {
-    const int k = blockIdx.x * EM3D_BZ + threadIdx.x;
-    const int j = blockIdx.y * EM3D_BY + threadIdx.y;
-    if (j >= p.ny || k >= p.nz) return;
-    const int i0 = blockIdx.z * p.x_chunk;
-    const int i1 = min(p.nx, i0 + p.x_chunk);
+// The box of this block and its x chunk (boxes of em3d_h_kernel / em3d_e_kernel; blocks of BZ x BY threads along
+// k and j).
+template <int BZ, int BY>
+__device__ __forceinline__ bool em3d_block_box(const Em3DParams &p, int &j, int &k, int &i0, int &i1) {
+    int b = 0;
+    while (b + 1 < p.n_boxes && (int)blockIdx.z >= p.zbase[b + 1]) ++b;
+    const Em3DBox bx = p.boxes[b];
+    k = bx.k0 + blockIdx.x * BZ + threadIdx.x;
+    j = bx.j0 + blockIdx.y * BY + threadIdx.y;
+    i0 = bx.i0 + ((int)blockIdx.z - p.zbase[b]) * p.x_chunk;
+    i1 = min(bx.i1, i0 + p.x_chunk);
+    return j < bx.j1 && k < bx.k1 && i0 < i1;
+}
+
+template <int BZ = EM3D_BZ, int BY = EM3D_BY>
+__global__ void __launch_bounds__(BZ * BY) em3d_h_kernel(const Em3DParams p) {
+    int j, k, i0, i1;
+    if (!em3d_block_box<BZ, BY>(p, j, k, i0, i1)) return;
     const size_t sx = (size_t)p.ny * p.nz;
     const float *__restrict__ ex = p.ex;
     const float *__restrict__ ey = p.ey;
     const float *__restrict__ ez = p.ez;
-    float *__restrict__ hx = p.hx;
-    float *__restrict__ hy = p.hy;
-    float *__restrict__ hz = p.hz;
+    const float *hx = p.hx;   // H in, H out: the same arrays when the step runs in place
+    const float *hy = p.hy;
+    const float *hz = p.hz;
+    float *ohx = p.ohx;
+    float *ohy = p.ohy;
+    float *ohz = p.ohz;
     const bool wy = j + 1 == p.ny, wz = k + 1 == p.nz;
     const int o = j * p.nz + k;
     const int oy = wy ? k : o + p.nz;             // hi y neighbour (row 0 across the edge)
@@ -137,25 +168,25 @@ __global__ void __launch_bounds__(EM3D_BZ * EM3D_BY) em3d_h_kernel(const Em3DPar
             if (r >= 0) {   // x layers: H_y from E_z (+), H_z from E_y (-)
                 const Em3DCpmlAxis &c = p.cpml[0];
                 const size_t q = (size_t)r * sx + o;
-                vy += db * em3d_psi(c.ph_first, q, c.b_h[r], c.g_h[r], dez_x);
-                vz -= db * em3d_psi(c.ph_second, q, c.b_h[r], c.g_h[r], dey_x);
+                vy += db * em3d_psi(c.ph_first, c.oph_first, q, c.b_h[r], c.g_h[r], dez_x);
+                vz -= db * em3d_psi(c.ph_second, c.oph_second, q, c.b_h[r], c.g_h[r], dey_x);
             }
         }
         if (ry >= 0) {   // y layers: H_x from E_z (-), H_z from E_x (+)
             const Em3DCpmlAxis &c = p.cpml[1];
             const size_t q = ((size_t)i * c.nr + ry) * p.nz + k;
-            vx -= db * em3d_psi(c.ph_first, q, c.b_h[ry], c.g_h[ry], dez_y);
-            vz += db * em3d_psi(c.ph_second, q, c.b_h[ry], c.g_h[ry], dex_y);
+            vx -= db * em3d_psi(c.ph_first, c.oph_first, q, c.b_h[ry], c.g_h[ry], dez_y);
+            vz += db * em3d_psi(c.ph_second, c.oph_second, q, c.b_h[ry], c.g_h[ry], dex_y);
         }
         if (rz >= 0) {   // z layers: H_x from E_y (+), H_y from E_x (-)
             const Em3DCpmlAxis &c = p.cpml[2];
             const size_t q = ((size_t)i * p.ny + j) * c.nr + rz;
-            vx += db * em3d_psi(c.ph_first, q, c.b_h[rz], c.g_h[rz], dey_z);
-            vy -= db * em3d_psi(c.ph_second, q, c.b_h[rz], c.g_h[rz], dex_z);
+            vx += db * em3d_psi(c.ph_first, c.oph_first, q, c.b_h[rz], c.g_h[rz], dey_z);
+            vy -= db * em3d_psi(c.ph_second, c.oph_second, q, c.b_h[rz], c.g_h[rz], dex_z);
         }
-        hx[b + o] = vx;
-        hy[b + o] = vy;
-        hz[b + o] = vz;
+        ohx[b + o] = vx;
+        ohy[b + o] = vy;
+        ohz[b + o] = vz;
         ex0 = exn;
         ey0 = eyn;
         ez0 = ezn;
@@ -228,19 +259,20 @@ __device__ __forceinline__ float em3d_lo_diff(float f0, float lo, bool first_row
     return periodic ? f0 - em3d_wrapped(lo) : f0;
 }
 
-__global__ void __launch_bounds__(EM3D_BZ * EM3D_BY, 4) em3d_e_kernel(const Em3DParams p) {
-    const int k = blockIdx.x * EM3D_BZ + threadIdx.x;
-    const int j = blockIdx.y * EM3D_BY + threadIdx.y;
-    if (j >= p.ny || k >= p.nz) return;
-    const int i0 = blockIdx.z * p.x_chunk;
-    const int i1 = min(p.nx, i0 + p.x_chunk);
+template <int BZ = EM3D_BZ, int BY = EM3D_BY>
+__global__ void __launch_bounds__(BZ * BY, 3) em3d_e_kernel(const Em3DParams p) {
+    int j, k, i0, i1;
+    if (!em3d_block_box<BZ, BY>(p, j, k, i0, i1)) return;
     const size_t sx = (size_t)p.ny * p.nz;
     const float *__restrict__ hx = p.hx;
     const float *__restrict__ hy = p.hy;
     const float *__restrict__ hz = p.hz;
-    float *__restrict__ ex = p.ex;
-    float *__restrict__ ey = p.ey;
-    float *__restrict__ ez = p.ez;
+    const float *ex = p.ex;   // E in, E out: the same arrays when the step runs in place
+    const float *ey = p.ey;
+    const float *ez = p.ez;
+    float *oex = p.oex;
+    float *oey = p.oey;
+    float *oez = p.oez;
     const uint16_t *__restrict__ mat = p.mat;
     const bool fy = j == 0, fz = k == 0;
     const int o = j * p.nz + k;
@@ -306,21 +338,21 @@ __global__ void __launch_bounds__(EM3D_BZ * EM3D_BY, 4) em3d_e_kernel(const Em3D
             if (r >= 0) {   // x layers: E_y from H_z (-), E_z from H_y (+)
                 const Em3DCpmlAxis &c = p.cpml[0];
                 const size_t q = (size_t)r * sx + o;
-                vy -= cby * em3d_psi(c.pe_first, q, c.b_e[r], c.g_e[r], dhz_x);
-                vz += cbz * em3d_psi(c.pe_second, q, c.b_e[r], c.g_e[r], dhy_x);
+                vy -= cby * em3d_psi(c.pe_first, c.ope_first, q, c.b_e[r], c.g_e[r], dhz_x);
+                vz += cbz * em3d_psi(c.pe_second, c.ope_second, q, c.b_e[r], c.g_e[r], dhy_x);
             }
         }
         if (ry >= 0) {   // y layers: E_x from H_z (+), E_z from H_x (-)
             const Em3DCpmlAxis &c = p.cpml[1];
             const size_t q = ((size_t)i * c.nr + ry) * p.nz + k;
-            vx += cbx * em3d_psi(c.pe_first, q, c.b_e[ry], c.g_e[ry], dhz_y);
-            vz -= cbz * em3d_psi(c.pe_second, q, c.b_e[ry], c.g_e[ry], dhx_y);
+            vx += cbx * em3d_psi(c.pe_first, c.ope_first, q, c.b_e[ry], c.g_e[ry], dhz_y);
+            vz -= cbz * em3d_psi(c.pe_second, c.ope_second, q, c.b_e[ry], c.g_e[ry], dhx_y);
         }
         if (rz >= 0) {   // z layers: E_x from H_y (-), E_y from H_x (+)
             const Em3DCpmlAxis &c = p.cpml[2];
             const size_t q = ((size_t)i * p.ny + j) * c.nr + rz;
-            vx -= cbx * em3d_psi(c.pe_first, q, c.b_e[rz], c.g_e[rz], dhy_z);
-            vy += cby * em3d_psi(c.pe_second, q, c.b_e[rz], c.g_e[rz], dhx_z);
+            vx -= cbx * em3d_psi(c.pe_first, c.ope_first, q, c.b_e[rz], c.g_e[rz], dhy_z);
+            vy += cby * em3d_psi(c.pe_second, c.ope_second, q, c.b_e[rz], c.g_e[rz], dhx_z);
         }
         // dipoles (DipoleSource3D.inject, sources3d.py:69-75): E += FP32(s(t + dt/2)) * weight after the update
         for (int d = 0; d < p.n_dip; ++d) {
@@ -330,9 +362,9 @@ __global__ void __launch_bounds__(EM3D_BZ * EM3D_BY, 4) em3d_e_kernel(const Em3D
             else if (p.dip_comp[d] == 1) vy = vy + add;
             else vz = vz + add;
         }
-        ex[b + o] = vx;
-        ey[b + o] = vy;
-        ez[b + o] = vz;
+        oex[b + o] = vx;
+        oey[b + o] = vy;
+        oez[b + o] = vz;
         hy_m = hy0;
         hz_m = hz0;
         hx0 = hx2;
@@ -350,6 +382,241 @@ __global__ void __launch_bounds__(EM3D_BZ * EM3D_BY, 4) em3d_e_kernel(const Em3D
         my = my2;
         mz = mz2;
         b = bn;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------- fused step
+// One whole Yee step (H then E) of the cells of box `in` -- every cell but the outermost layer of each axis, where a
+// sample would cross the grid edge -- in one pass that reads E^n, H^{n-1/2} and the CPML psi once and writes E^{n+1},
+// H^{n+1/2} and psi' once: two field sets and two psi sets, read one, write the other, swapped after each step.  A
+// block is a 32 x TY tile of (k, j) columns streaming a chunk of x planes; lane 0 of each warp is the column k0 - 1
+// and warp 0 the row j0 - 1, whose H the tile's E update needs: they compute H only (the halo, never stored; a halo
+// cell in a CPML layer reads the old psi and stores nothing).  Per plane every thread updates H of its column, then E
+// takes H^{n+1/2} of the k - 1 neighbour from the next lower lane (a shuffle), of the j - 1 neighbour through shared
+// memory (double-buffered by plane parity, one barrier per plane) and of the i - 1 plane from the thread's own
+// previous iteration (the chunk starts one plane early, with H only).  The arithmetic of every cell, CPML terms
+// included, is em3d_h_kernel's and em3d_e_kernel's term for term, so the results are those of the two-kernel step
+// bit for bit.
+constexpr int EM3D_FZ = 32;   // lanes along k (lane 0: the halo column)
+
+template <int TY, int MINB>
+__global__ void __launch_bounds__(EM3D_FZ * TY, MINB) em3d_fused_kernel(const Em3DParams p, const Em3DBox in) {
+    __shared__ float s_hz[2][TY][EM3D_FZ];
+    __shared__ float s_hx[2][TY][EM3D_FZ];
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int kk = in.k0 - 1 + (int)blockIdx.x * (EM3D_FZ - 1) + lane;
+    const int jj = in.j0 - 1 + (int)blockIdx.y * (TY - 1) + w;
+    const bool e_thread = lane > 0 && w > 0;                    // not a halo lane or row
+    const bool emit = e_thread && kk < in.k1 && jj < in.j1;     // stores its column's results
+    // a column past the box computes a discarded copy of the box's last column (every address stays inside)
+    const int k = min(kk, in.k1 - 1), j = min(jj, in.j1 - 1);
+    const int i_first = in.i0 + (int)blockIdx.z * p.x_chunk;
+    const int i_last = min(in.i1, i_first + p.x_chunk);
+    const size_t sx = (size_t)p.ny * p.nz;
+    const int o = j * p.nz + k;
+    const int oy = o + p.nz, oz = o + 1;
+    const float *__restrict__ ex = p.ex;
+    const float *__restrict__ ey = p.ey;
+    const float *__restrict__ ez = p.ez;
+    const float *__restrict__ hx = p.hx;
+    const float *__restrict__ hy = p.hy;
+    const float *__restrict__ hz = p.hz;
+    float *__restrict__ oex = p.oex;
+    float *__restrict__ oey = p.oey;
+    float *__restrict__ oez = p.oez;
+    float *__restrict__ ohx = p.ohx;
+    float *__restrict__ ohy = p.ohy;
+    float *__restrict__ ohz = p.ohz;
+    const uint16_t *__restrict__ mat = p.mat;
+    const float ihy = p.ihy[j], ihz = p.ihz[k];
+    const float iey = p.iey[j], iez = p.iez[k];
+    const float wly = p.wly[j], wuy = p.wuy[j], wlz = p.wlz[k], wuz = p.wuz[k];
+    // CPML rows of this column on y and z (-1: outside the layers)
+    const int32_t ryh = p.cpml[1].nr ? p.cpml[1].rm_h[j] : -1, rye = p.cpml[1].nr ? p.cpml[1].rm_e[j] : -1;
+    const int32_t rzh = p.cpml[2].nr ? p.cpml[2].rm_h[k] : -1, rze = p.cpml[2].nr ? p.cpml[2].rm_e[k] : -1;
+    // plane i = i_first - 1 (the halo plane), its loads
+    int i = i_first - 1;
+    size_t b = (size_t)i * sx;
+    size_t bn = b + sx;
+    float ex0 = __ldg(ex + b + o), ey0 = __ldg(ey + b + o), ez0 = __ldg(ez + b + o);
+    float exn = __ldg(ex + bn + o), eyn = __ldg(ey + bn + o), ezn = __ldg(ez + bn + o);
+    float exy = __ldg(ex + b + oy), ezy = __ldg(ez + b + oy);
+    float exz = __ldg(ex + b + oz), eyz = __ldg(ey + b + oz);
+    float hx0 = __ldg(hx + b + o), hy0 = __ldg(hy + b + o), hz0 = __ldg(hz + b + o);
+    uint16_t m0 = __ldg(mat + b + o), mx = __ldg(mat + bn + o);
+    uint16_t my = __ldg(mat + b + oy), mz = __ldg(mat + b + oz);
+    float hy_m = 0.0f, hz_m = 0.0f;   // H^{n+1/2} of plane i - 1 of this column
+    int par = 0;
+    for (; i < i_last; ++i) {
+        const bool more = i + 1 < i_last;
+        const size_t bnn = bn + sx;
+        float exn2 = 0.0f, eyn2 = 0.0f, ezn2 = 0.0f, exy2 = 0.0f, ezy2 = 0.0f, exz2 = 0.0f, eyz2 = 0.0f;
+        float hx2 = 0.0f, hy2 = 0.0f, hz2 = 0.0f;
+        uint16_t mx2 = 0, my2 = 0, mz2 = 0;
+        if (more) {   // plane i + 1's loads (plane i + 2 <= i_last <= in.i1 <= nx - 1)
+            exn2 = __ldg(ex + bnn + o);
+            eyn2 = __ldg(ey + bnn + o);
+            ezn2 = __ldg(ez + bnn + o);
+            exy2 = __ldg(ex + bn + oy);
+            ezy2 = __ldg(ez + bn + oy);
+            exz2 = __ldg(ex + bn + oz);
+            eyz2 = __ldg(ey + bn + oz);
+            hx2 = __ldg(hx + bn + o);
+            hy2 = __ldg(hy + bn + o);
+            hz2 = __ldg(hz + bn + o);
+            mx2 = __ldg(mat + bnn + o);
+            my2 = __ldg(mat + bn + oy);
+            mz2 = __ldg(mat + bn + oz);
+        }
+        const bool inside = i >= i_first;
+        const bool store = emit && inside;
+        // H^{n+1/2} of (i, j, k): em3d_h_kernel's update (no sample crosses the grid edge in the box)
+        float da, db;
+        if (p.h_uniform) {
+            da = p.da_u;
+            db = p.db_u;
+        } else {
+            da = p.t_da[m0];
+            db = p.t_db[m0];
+        }
+        const float ihx = p.ihx[i];
+        const float dez_y = ezy - ez0, dey_z = eyz - ey0, dex_z = exz - ex0, dez_x = ezn - ez0;
+        const float dey_x = eyn - ey0, dex_y = exy - ex0;
+        float vhx = da * hx0 - db * (dez_y * ihy - dey_z * ihz);
+        float vhy = da * hy0 - db * (dex_z * ihz - dez_x * ihx);
+        float vhz = da * hz0 - db * (dey_x * ihx - dex_y * ihy);
+        const int32_t rxh = p.cpml[0].nr ? p.cpml[0].rm_h[i] : -1;
+        if (rxh >= 0) {   // x layers: H_y from E_z (+), H_z from E_y (-)
+            const Em3DCpmlAxis &c = p.cpml[0];
+            const size_t q = (size_t)rxh * sx + o;
+            const float f = c.b_h[rxh] * c.ph_first[q] + c.g_h[rxh] * dez_x;
+            const float g = c.b_h[rxh] * c.ph_second[q] + c.g_h[rxh] * dey_x;
+            if (store) {
+                c.oph_first[q] = f;
+                c.oph_second[q] = g;
+            }
+            vhy += db * f;
+            vhz -= db * g;
+        }
+        if (ryh >= 0) {   // y layers: H_x from E_z (-), H_z from E_x (+)
+            const Em3DCpmlAxis &c = p.cpml[1];
+            const size_t q = ((size_t)i * c.nr + ryh) * p.nz + k;
+            const float f = c.b_h[ryh] * c.ph_first[q] + c.g_h[ryh] * dez_y;
+            const float g = c.b_h[ryh] * c.ph_second[q] + c.g_h[ryh] * dex_y;
+            if (store) {
+                c.oph_first[q] = f;
+                c.oph_second[q] = g;
+            }
+            vhx -= db * f;
+            vhz += db * g;
+        }
+        if (rzh >= 0) {   // z layers: H_x from E_y (+), H_y from E_x (-)
+            const Em3DCpmlAxis &c = p.cpml[2];
+            const size_t q = ((size_t)i * p.ny + j) * c.nr + rzh;
+            const float f = c.b_h[rzh] * c.ph_first[q] + c.g_h[rzh] * dey_z;
+            const float g = c.b_h[rzh] * c.ph_second[q] + c.g_h[rzh] * dex_z;
+            if (store) {
+                c.oph_first[q] = f;
+                c.oph_second[q] = g;
+            }
+            vhx += db * f;
+            vhy -= db * g;
+        }
+        if (store) {
+            ohx[b + o] = vhx;
+            ohy[b + o] = vhy;
+            ohz[b + o] = vhz;
+        }
+        s_hz[par][w][lane] = vhz;
+        s_hx[par][w][lane] = vhx;
+        const float hy_z = __shfl_up_sync(0xffffffffu, vhy, 1);   // H^{n+1/2} of (i, j, k - 1)
+        const float hx_z = __shfl_up_sync(0xffffffffu, vhx, 1);
+        __syncthreads();
+        if (e_thread && inside) {
+            const float hz_y = s_hz[par][w - 1][lane];            // H^{n+1/2} of (i, j - 1, k)
+            const float hx_y = s_hx[par][w - 1][lane];
+            const float dhz_y = vhz - hz_y, dhy_z = vhy - hy_z, dhx_z = vhx - hx_z;
+            const float dhz_x = vhz - hz_m, dhy_x = vhy - hy_m, dhx_y = vhx - hx_y;
+            float ca, cbx, cby, cbz;
+            const float iex = p.iex[i];
+            em3d_face_fast(p, 0, p.t_ex, m0, mx, p.wlx[i], p.wux[i], ca, cbx);
+            float vx = ca * ex0 + cbx * (dhz_y * iey - dhy_z * iez);
+            em3d_face_fast(p, 1, p.t_ey, m0, my, wly, wuy, ca, cby);
+            float vy = ca * ey0 + cby * (dhx_z * iez - dhz_x * iex);
+            em3d_face_fast(p, 2, p.t_ez, m0, mz, wlz, wuz, ca, cbz);
+            float vz = ca * ez0 + cbz * (dhy_x * iex - dhx_y * iey);
+            const int32_t rxe = p.cpml[0].nr ? p.cpml[0].rm_e[i] : -1;
+            if (rxe >= 0) {   // x layers: E_y from H_z (-), E_z from H_y (+)
+                const Em3DCpmlAxis &c = p.cpml[0];
+                const size_t q = (size_t)rxe * sx + o;
+                const float f = c.b_e[rxe] * c.pe_first[q] + c.g_e[rxe] * dhz_x;
+                const float g = c.b_e[rxe] * c.pe_second[q] + c.g_e[rxe] * dhy_x;
+                if (emit) {
+                    c.ope_first[q] = f;
+                    c.ope_second[q] = g;
+                }
+                vy -= cby * f;
+                vz += cbz * g;
+            }
+            if (rye >= 0) {   // y layers: E_x from H_z (+), E_z from H_x (-)
+                const Em3DCpmlAxis &c = p.cpml[1];
+                const size_t q = ((size_t)i * c.nr + rye) * p.nz + k;
+                const float f = c.b_e[rye] * c.pe_first[q] + c.g_e[rye] * dhz_y;
+                const float g = c.b_e[rye] * c.pe_second[q] + c.g_e[rye] * dhx_y;
+                if (emit) {
+                    c.ope_first[q] = f;
+                    c.ope_second[q] = g;
+                }
+                vx += cbx * f;
+                vz -= cbz * g;
+            }
+            if (rze >= 0) {   // z layers: E_x from H_y (-), E_y from H_x (+)
+                const Em3DCpmlAxis &c = p.cpml[2];
+                const size_t q = ((size_t)i * p.ny + j) * c.nr + rze;
+                const float f = c.b_e[rze] * c.pe_first[q] + c.g_e[rze] * dhy_z;
+                const float g = c.b_e[rze] * c.pe_second[q] + c.g_e[rze] * dhx_z;
+                if (emit) {
+                    c.ope_first[q] = f;
+                    c.ope_second[q] = g;
+                }
+                vx -= cbx * f;
+                vy += cby * g;
+            }
+            for (int d = 0; d < p.n_dip; ++d) {   // dipoles: E += FP32(s(t + dt/2)) * weight after the update
+                if (p.dip_o[d] != o || p.dip_i[d] != i) continue;
+                const float add = p.dip_values[d * p.values_stride + p.k_step] * p.dip_weight[d];
+                if (p.dip_comp[d] == 0) vx = vx + add;
+                else if (p.dip_comp[d] == 1) vy = vy + add;
+                else vz = vz + add;
+            }
+            if (emit) {
+                oex[b + o] = vx;
+                oey[b + o] = vy;
+                oez[b + o] = vz;
+            }
+        }
+        hy_m = vhy;
+        hz_m = vhz;
+        ex0 = exn;
+        ey0 = eyn;
+        ez0 = ezn;
+        exn = exn2;
+        eyn = eyn2;
+        ezn = ezn2;
+        exy = exy2;
+        ezy = ezy2;
+        exz = exz2;
+        eyz = eyz2;
+        hx0 = hx2;
+        hy0 = hy2;
+        hz0 = hz2;
+        m0 = mx;
+        mx = mx2;
+        my = my2;
+        mz = mz2;
+        b = bn;
+        bn = bnn;
+        par ^= 1;
     }
 }
 

@@ -292,6 +292,22 @@ class FDTDEngine3D:
         """x planes per block of the H / E kernels (speed only)."""
         _native.check(_native.load().os_fdtd3d_set_x_chunk(self.handle, int(planes)))
 
+    def set_variant(self, variant):
+        """Step form (speed and memory only; results are bit-identical): 0 = the two in-place kernels (the default),
+        1 = the fused kernel on two field and psi sets."""
+        _native.check(_native.load().os_fdtd3d_set_variant(self.handle, int(variant)))
+
+    def set_fused_config(self, config):
+        """Launch shape of the fused step kernel (0..4; speed only, results bit-identical)."""
+        _native.check(_native.load().os_fdtd3d_set_fused_config(self.handle, int(config)))
+
+    def interior(self):
+        """((i0, i1, j0, j1, k0, k1) of the fused interior box, whether the next advance uses it)."""
+        box = (ctypes.c_int32 * 6)()
+        fused = ctypes.c_int32()
+        _native.check(_native.load().os_fdtd3d_interior(self.handle, box, ctypes.byref(fused)))
+        return tuple(int(v) for v in box), bool(fused.value)
+
     def set_stream(self, cuda_stream):
         _native.check(_native.load().os_fdtd3d_set_stream(self.handle, cuda_stream or None))
 

@@ -81,12 +81,43 @@ def test_field_roundtrip_and_launches():
     values = rng.standard_normal(engine.shape).astype(np.float32)
     engine.write_field('hy', values)
     np.testing.assert_array_equal(engine.read_field('hy'), values)
+    engine.set_variant(1)
     engine.reset()
     physics.run(30)
     engine.synchronize()
     m = physics.monitors[0].sample_interval
+    _, fused = engine.interior()
+    assert fused   # the fused kernel, and H then E of the faces in two block shapes each: 5 launches per step
+    assert engine.launch_count() == 5 * 30 + 30 // m
+    engine.set_variant(0)
+    engine.reset()
+    physics.run(30)
     assert engine.launch_count() == 2 * 30 + 30 // m
     assert engine.last_advance_ms() > 0.0
+
+
+@pytest.mark.parametrize('spec', CASES3D, ids=[c['name'] for c in CASES3D])
+def test_step_forms_bit_identical(spec):
+    """The fused form (two field and psi sets) in every launch shape and the in-place two-kernel form give
+    bit-identical fields and fluxes, chunked into uneven advances (the set holding the current state alternates
+    between chunks)."""
+    runs = []
+    for variant, config in ((0, 0), (1, 0), (1, 1), (1, 2), (1, 3), (1, 4)):
+        physics, monitors = build_product(spec)
+        engine = physics.engine
+        engine.set_variant(variant)
+        engine.set_fused_config(config)
+        box, fused = engine.interior()
+        assert fused == (variant == 1)
+        assert all(hi > lo for lo, hi in zip(box[::2], box[1::2]))
+        for n in (7, 1, 12, 5):
+            physics.run(n)
+        runs.append((engine.state(), [np.asarray(m.flux()) for m in monitors]))
+    for run in runs[1:]:
+        for name in FIELDS:
+            np.testing.assert_array_equal(runs[0][0][name], run[0][name], err_msg=name)
+        for f0, f1 in zip(runs[0][1], run[1]):
+            np.testing.assert_array_equal(f0, f1)
 
 
 def test_x_chunk_does_not_change_results():
