@@ -10,6 +10,8 @@
 // CPU backend.  The CPML corrections of a cell are applied in FACES order (x sides, then y sides), as open_sol's one
 // launch per side does.
 #include "common.cuh"
+
+#include <functional>
 #include "fdtd2d_kernels.cuh"
 #include "fdtd2d_tb.cuh"
 #include "fdtd2d_interior.cuh"
@@ -1657,7 +1659,10 @@ static __device__ __align__(256) float g_noalloc_scratch[OS_FDTD_NOALLOC_MAX_FLO
 namespace os {
 
 // Device address of g_noalloc_scratch on the current device, looked up once per device (the first lookup may load
-// the module onto the device, so the first call for a device belongs before any stream capture).
+// the module onto the device, so the first call for a device belongs before any stream capture).  The cached address
+// belongs to the device's primary context as it was at the lookup: a process that resets the device
+// (cudaDeviceReset) or tears its primary context down must not call os_fdtd2d_advance_noalloc on it afterwards; the
+// engines of that context are gone with it anyway.
 static int noalloc_scratch(int device, float **out) {
     static std::mutex mu;
     static float *addr[OS_FDTD_MAX_DEVICES] = {};
@@ -1685,9 +1690,22 @@ extern "C" int os_fdtd2d_advance_noalloc(OsFdtd2D *h, int64_t n_steps, const flo
              "os_fdtd2d_advance_noalloc: profiling is on (its event pool grows on demand); turn it off first");
     OS_CHECK(h->probes.n == 0 || h->n_step + n_steps <= h->probe_capacity, OS_ERR_STATE,
              "os_fdtd2d_advance_noalloc: the field probes' rows would have to grow; advance with os_fdtd2d_advance");
-    // tables: line values at float 0, phases at the next 64-float (256-byte) boundary
-    const size_t value_floats = n_steps > 0 ? (h->lines.size() + h->tfsf.size()) * (size_t)n_steps : 0;
-    const size_t phase_floats = n_steps > 0 && n_samples > 0 ? phase_floats_of(h, n_samples) : 0;
+    // tables: line values at float 0, phases at the next 64-float (256-byte) boundary.  Step and sample counts are
+    // bounded before they multiply anything, so no product below can wrap around.
+    const size_t value_rows = h->lines.size() + h->tfsf.size();
+    size_t sample_floats = 0;   // phase floats per DFT sample, over every flux line and field map
+    for (auto &f : h->fluxes) sample_floats += (size_t)f->nf * 2;
+    for (auto &d : h->maps) sample_floats += (size_t)d->nf * 2 * (d->hz ? 2 : 1);
+    OS_CHECK(value_rows == 0 || n_steps <= (int64_t)(OS_FDTD_NOALLOC_MAX_FLOATS / value_rows), OS_ERR_INVALID,
+             "os_fdtd2d_advance_noalloc: %lld steps of %zu source rows exceed the fixed scratch of %d floats; advance "
+             "fewer steps per call", (long long)n_steps, value_rows, OS_FDTD_NOALLOC_MAX_FLOATS);
+    const bool with_phases = n_steps > 0 && n_samples > 0 && phases;   // uploaded only when given, as advance does
+    OS_CHECK(!with_phases || sample_floats == 0 ||
+                 n_samples <= (int64_t)(OS_FDTD_NOALLOC_MAX_FLOATS / sample_floats), OS_ERR_INVALID,
+             "os_fdtd2d_advance_noalloc: %lld DFT samples of %zu phase floats exceed the fixed scratch of %d floats; "
+             "advance fewer steps per call", (long long)n_samples, sample_floats, OS_FDTD_NOALLOC_MAX_FLOATS);
+    const size_t value_floats = n_steps > 0 ? value_rows * (size_t)n_steps : 0;
+    const size_t phase_floats = with_phases ? (size_t)n_samples * sample_floats : 0;
     const size_t phase_offset = (value_floats + 63) / 64 * 64;
     const size_t need = phase_floats ? phase_offset + phase_floats : value_floats;
     OS_CHECK(need <= (size_t)OS_FDTD_NOALLOC_MAX_FLOATS, OS_ERR_INVALID,
@@ -1703,7 +1721,7 @@ extern "C" int os_fdtd2d_advance_noalloc(OsFdtd2D *h, int64_t n_steps, const flo
     if (value_floats)
         OS_CUDA(cudaMemcpyAsync(scratch, line_values, value_floats * sizeof(float), cudaMemcpyHostToDevice,
                                 h->stream));
-    if (phase_floats && phases)
+    if (phase_floats)
         OS_CUDA(cudaMemcpyAsync(scratch + phase_offset, phases, phase_floats * sizeof(float),
                                 cudaMemcpyHostToDevice, h->stream));
     return run_chunk(h, n_steps, first_sample, n_samples, scratch, scratch + phase_offset);
@@ -2515,12 +2533,19 @@ struct OsAdjoint2D {
     os::DeviceArray<float> le[2], lhx[2], lhy[2];
     os::DeviceArray<float> lpe[2][4], lph[2][4];
     int e_par = 0;                                     // live parity of lambda_E and the psi adjoints
-    os::DeviceArray<float> rec;                        // (seg_steps + 1) x box
+    // Backward pipeline: the recomputation of segment s (engine stream) records E over the box into rec[s & 1] while
+    // the transposed sweep of segment s + 1 (adjoint stream) reads rec[(s + 1) & 1]; ev_rec[b] marks a recording into
+    // rec[b] done, ev_swept[b] a sweep of rec[b] done (the next recording into it waits for that).
+    os::DeviceArray<float> rec[2];                     // (seg_steps + 1) x box each
     os::DeviceArray<double> grad;                      // box
     os::DeviceArray<float> values, src_e, src_h;
     os::DeviceArray<int32_t> src_row;                  // per step of the segment: row of its adjoint source, or -1
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};     // full-segment body, per starting parity
-    int graph_monitor[2] = {-1, -1};
+    cudaStream_t adj_stream = nullptr;
+    cudaEvent_t ev_rec[2] = {nullptr, nullptr}, ev_swept[2] = {nullptr, nullptr};
+    bool swept_pending[2] = {false, false};
+    cudaGraphExec_t rec_graph[2] = {nullptr, nullptr};           // full-length recomputation, per rec buffer
+    cudaGraphExec_t sweep_graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // per rec buffer and parity
+    int sweep_monitor[2][2] = {{-1, -1}, {-1, -1}};
     int64_t graph_launches = 0;
 };
 
@@ -2619,8 +2644,13 @@ extern "C" int os_fdtd2d_adjoint_create(OsFdtd2D *h, int32_t box_i0, int32_t box
             OS_TRY(a->lph[b][s].alloc(h->psi_h[0][s].count));
         }
     }
-    OS_TRY(a->rec.alloc((size_t)(segment_steps + 1) * adj_box(a.get())));
+    for (auto &r : a->rec) OS_TRY(r.alloc((size_t)(segment_steps + 1) * adj_box(a.get())));
     OS_TRY(a->grad.alloc(adj_box(a.get())));
+    OS_CUDA(cudaStreamCreateWithFlags(&a->adj_stream, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+        OS_CUDA(cudaEventCreateWithFlags(&a->ev_rec[b], cudaEventDisableTiming));
+        OS_CUDA(cudaEventCreateWithFlags(&a->ev_swept[b], cudaEventDisableTiming));
+    }
     *out = a.release();
     return OS_OK;
 }
@@ -2629,8 +2659,15 @@ extern "C" int os_fdtd2d_adjoint_destroy(OsAdjoint2D *a) {
     if (!a) return OS_OK;
     cudaSetDevice(a->h->device);
     cudaStreamSynchronize(a->h->stream);
-    for (cudaGraphExec_t g : a->graph)
-        if (g) cudaGraphExecDestroy(g);
+    if (a->adj_stream) cudaStreamSynchronize(a->adj_stream);
+    for (int b = 0; b < 2; ++b) {
+        if (a->rec_graph[b]) cudaGraphExecDestroy(a->rec_graph[b]);
+        for (cudaGraphExec_t g : a->sweep_graph[b])
+            if (g) cudaGraphExecDestroy(g);
+        if (a->ev_rec[b]) cudaEventDestroy(a->ev_rec[b]);
+        if (a->ev_swept[b]) cudaEventDestroy(a->ev_swept[b]);
+    }
+    if (a->adj_stream) cudaStreamDestroy(a->adj_stream);
     delete a;
     return OS_OK;
 }
@@ -2664,6 +2701,12 @@ extern "C" int os_fdtd2d_adjoint_reset(OsAdjoint2D *a) {
     }
     OS_CUDA(cudaMemsetAsync(a->grad.ptr, 0, a->grad.bytes(), s));
     a->e_par = 0;
+    // the adjoint stream's next sweep must also follow these zeroings and every earlier sweep: one wait on the engine
+    // stream, which a sweep's own wait for its recording orders anyway; earlier sweeps are joined here
+    for (int b = 0; b < 2; ++b) {
+        if (a->swept_pending[b]) OS_CUDA(cudaStreamWaitEvent(s, a->ev_swept[b], 0));
+        a->swept_pending[b] = false;
+    }
     return OS_OK;
 }
 
@@ -2684,8 +2727,11 @@ extern "C" int os_fdtd2d_adjoint_segment(OsAdjoint2D *a, int32_t slot, int64_t s
         OS_CHECK(source_steps[q] >= 0 && source_steps[q] < n_steps && (q == 0 || source_steps[q] > source_steps[q - 1]),
                  OS_ERR_INVALID, "os_fdtd2d_adjoint_segment: source steps must be increasing within the segment");
     OS_TRY(bind_device(h));
-    cudaStream_t s = h->stream;
-    // restore the checkpoint into the live buffers
+    cudaStream_t s = h->stream, as = a->adj_stream;
+    const int rb = slot & 1;   // the record buffer of this segment
+    const size_t box = adj_box(a);
+    // ---- engine stream: recompute the segment from its checkpoint, recording E over the box into rec[rb]
+    if (a->swept_pending[rb]) OS_CUDA(cudaStreamWaitEvent(s, a->ev_swept[rb], 0));   // its last reader is done
     {
         std::vector<std::pair<float *, size_t>> pieces;
         adj_pieces(a, pieces);
@@ -2700,6 +2746,47 @@ extern "C" int os_fdtd2d_adjoint_segment(OsAdjoint2D *a, int32_t slot, int64_t s
         OS_CUDA(cudaMemcpyAsync(a->values.ptr, line_values, h->lines.size() * (size_t)n_steps * sizeof(float),
                                 cudaMemcpyHostToDevice, s));
     }
+    auto recompute = [&](int32_t steps) -> int {
+        const int box_blocks = (int)((box + 255) / 256);
+        Ez2DParams p = make_params(h);
+        const dim3 block(EZ2D_BLOCK_X, EZ2D_BLOCK_Y);
+        const dim3 grid((unsigned)((h->grid.ny + block.x - 1) / block.x),
+                        (unsigned)((h->grid.nx + block.y - 1) / block.y));
+        float *rec = a->rec[rb].ptr;
+        ez2d_record_box_kernel<<<box_blocks, 256, 0, s>>>(p.ez, h->grid.ny, a->bi0, a->bi1, a->bj0, a->bj1, rec);
+        for (int32_t k = 0; k < steps; ++k) {
+            ez2d_h_kernel<<<grid, block, 0, s>>>(p);
+            ez2d_e_kernel<<<grid, block, 0, s>>>(p, a->values.ptr, steps, k);
+            ez2d_record_box_kernel<<<box_blocks, 256, 0, s>>>(p.ez, h->grid.ny, a->bi0, a->bi1, a->bj0, a->bj1,
+                                                              rec + (size_t)(k + 1) * box);
+        }
+        return OS_OK;
+    };
+    // a full-length segment replays a captured graph (its arguments are the same for every segment using rec[rb])
+    auto run_captured = [&](cudaStream_t stream, cudaGraphExec_t &exec, const std::function<int()> &body) -> int {
+        if (!exec) {
+            cudaGraph_t g = nullptr;
+            OS_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            const int rc = body();
+            const cudaError_t end = cudaStreamEndCapture(stream, &g);
+            if (rc != OS_OK) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            OS_CUDA(end);
+            const cudaError_t inst = cudaGraphInstantiate(&exec, g, 0);
+            cudaGraphDestroy(g);
+            OS_CUDA(inst);
+        }
+        OS_CUDA(cudaGraphLaunch(exec, stream));
+        a->graph_launches += 1;
+        return OS_OK;
+    };
+    if (n_steps == a->seg_steps) OS_TRY(run_captured(s, a->rec_graph[rb], [&] { return recompute(n_steps); }));
+    else OS_TRY(recompute(n_steps));
+    OS_CUDA(cudaEventRecord(a->ev_rec[rb], s));
+    // ---- adjoint stream: the transposed steps backward over rec[rb], the monitor's DFT samples as sources
+    OS_CUDA(cudaStreamWaitEvent(as, a->ev_rec[rb], 0));
     const FluxLine2D &mon = *h->fluxes[monitor_id];
     const int n_line = mon.hi - mon.lo;
     {   // source rows and the per-step row table
@@ -2707,40 +2794,27 @@ extern "C" int os_fdtd2d_adjoint_segment(OsAdjoint2D *a, int32_t slot, int64_t s
         for (int32_t q = 0; q < n_sources; ++q) rows[(size_t)source_steps[q]] = q;
         OS_TRY(a->src_row.alloc((size_t)a->seg_steps));
         OS_CUDA(cudaMemcpyAsync(a->src_row.ptr, rows.data(), rows.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
-                                s));
+                                as));
         OS_TRY(a->src_e.alloc((size_t)a->seg_steps * n_line));
         OS_TRY(a->src_h.alloc((size_t)a->seg_steps * n_line));
         if (n_sources) {
             OS_CUDA(cudaMemcpyAsync(a->src_e.ptr, source_e, (size_t)n_sources * n_line * sizeof(float),
-                                    cudaMemcpyHostToDevice, s));
+                                    cudaMemcpyHostToDevice, as));
             OS_CUDA(cudaMemcpyAsync(a->src_h.ptr, source_h, (size_t)n_sources * n_line * sizeof(float),
-                                    cudaMemcpyHostToDevice, s));
+                                    cudaMemcpyHostToDevice, as));
         }
+        OS_CUDA(cudaStreamSynchronize(as));   // the host rows above are released on return
     }
-    // the body: recompute the segment recording E over the box, then the transposed steps backward; a full-length
-    // segment replays one captured graph (its arguments are the same for every segment of that parity)
-    auto body = [&](int32_t steps) -> int {
-        const size_t box = adj_box(a);
-        const int box_blocks = (int)((box + 255) / 256);
-        Ez2DParams p = make_params(h);
-        const dim3 block(EZ2D_BLOCK_X, EZ2D_BLOCK_Y);
-        const dim3 grid((unsigned)((h->grid.ny + block.x - 1) / block.x),
-                        (unsigned)((h->grid.nx + block.y - 1) / block.y));
-        ez2d_record_box_kernel<<<box_blocks, 256, 0, s>>>(p.ez, h->grid.ny, a->bi0, a->bi1, a->bj0, a->bj1,
-                                                          a->rec.ptr);
-        for (int32_t k = 0; k < steps; ++k) {
-            ez2d_h_kernel<<<grid, block, 0, s>>>(p);
-            ez2d_e_kernel<<<grid, block, 0, s>>>(p, a->values.ptr, steps, k);
-            ez2d_record_box_kernel<<<box_blocks, 256, 0, s>>>(p.ez, h->grid.ny, a->bi0, a->bi1, a->bj0, a->bj1,
-                                                              a->rec.ptr + (size_t)(k + 1) * box);
-        }
+    const int par = a->e_par;
+    auto sweep = [&](int32_t steps) -> int {
         Ez2DAdjParams q = adj_params(a);
         const dim3 ablock(32, 8);
         const dim3 agrid((unsigned)((h->grid.ny + 31) / 32), (unsigned)((h->grid.nx + 7) / 8));
-        int e = a->e_par;
+        const float *rec = a->rec[rb].ptr;
+        int e = par;
         for (int32_t k = steps - 1; k >= 0; --k) {
             float *lh = mon.normal_axis == 0 ? a->lhy[0].ptr : a->lhx[0].ptr;
-            ez2d_adj_source_kernel<<<(n_line + 127) / 128, 128, 0, s>>>(
+            ez2d_adj_source_kernel<<<(n_line + 127) / 128, 128, 0, as>>>(
                 a->le[e].ptr, lh, h->grid.ny, mon.normal_axis, mon.position, mon.lo, n_line, a->src_row.ptr, k,
                 a->src_e.ptr, a->src_h.ptr);
             q.le_in = a->le[e].ptr;
@@ -2754,43 +2828,32 @@ extern "C" int os_fdtd2d_adjoint_segment(OsAdjoint2D *a, int32_t slot, int64_t s
                 q.lph_in[sd] = a->lph[e][sd].ptr;
                 q.lph_out[sd] = a->lph[e ^ 1][sd].ptr;
             }
-            q.e_next = a->rec.ptr + (size_t)(k + 1) * box;
-            q.e_prev = a->rec.ptr + (size_t)k * box;
-            ez2d_adj_e_kernel<<<agrid, ablock, 0, s>>>(q);
+            q.e_next = rec + (size_t)(k + 1) * box;
+            q.e_prev = rec + (size_t)k * box;
+            ez2d_adj_e_kernel<<<agrid, ablock, 0, as>>>(q);
             q.lhx_in = a->lhx[1].ptr;
             q.lhy_in = a->lhy[1].ptr;
             q.lhx_out = a->lhx[0].ptr;
             q.lhy_out = a->lhy[0].ptr;
             q.le_out = a->le[e ^ 1].ptr;
-            ez2d_adj_h_kernel<<<agrid, ablock, 0, s>>>(q);
+            ez2d_adj_h_kernel<<<agrid, ablock, 0, as>>>(q);
             e ^= 1;
         }
         return OS_OK;
     };
-    const int par = a->e_par;
     if (n_steps == a->seg_steps) {
-        if (!a->graph[par] || a->graph_monitor[par] != monitor_id) {
-            if (a->graph[par]) OS_CUDA(cudaGraphExecDestroy(a->graph[par]));
-            a->graph[par] = nullptr;
-            cudaGraph_t g = nullptr;
-            OS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-            const int rc = body(n_steps);
-            const cudaError_t end = cudaStreamEndCapture(s, &g);
-            if (rc != OS_OK) {
-                if (g) cudaGraphDestroy(g);
-                return rc;
-            }
-            OS_CUDA(end);
-            const cudaError_t inst = cudaGraphInstantiate(&a->graph[par], g, 0);
-            cudaGraphDestroy(g);
-            OS_CUDA(inst);
-            a->graph_monitor[par] = monitor_id;
+        cudaGraphExec_t &exec = a->sweep_graph[rb][par];
+        if (exec && a->sweep_monitor[rb][par] != monitor_id) {
+            OS_CUDA(cudaGraphExecDestroy(exec));
+            exec = nullptr;
         }
-        OS_CUDA(cudaGraphLaunch(a->graph[par], s));
-        a->graph_launches += 1;
+        a->sweep_monitor[rb][par] = monitor_id;
+        OS_TRY(run_captured(as, exec, [&] { return sweep(n_steps); }));
     } else {
-        OS_TRY(body(n_steps));
+        OS_TRY(sweep(n_steps));
     }
+    OS_CUDA(cudaEventRecord(a->ev_swept[rb], as));
+    a->swept_pending[rb] = true;
     a->e_par = (par + (int)(n_steps & 1)) & 1;
     OS_CUDA(cudaGetLastError());
     h->n_step = step0 + n_steps;   // the live buffers hold the recomputed state at the segment's end
@@ -2801,7 +2864,8 @@ extern "C" int os_fdtd2d_adjoint_gradient(OsAdjoint2D *a, double *out) {
     using namespace os;
     OS_CHECK(a && out, OS_ERR_INVALID, "os_fdtd2d_adjoint_gradient: null argument");
     OS_TRY(bind_device(a->h));
-    OS_CUDA(cudaMemcpyAsync(out, a->grad.ptr, a->grad.bytes(), cudaMemcpyDeviceToHost, a->h->stream));
+    OS_CUDA(cudaMemcpyAsync(out, a->grad.ptr, a->grad.bytes(), cudaMemcpyDeviceToHost, a->adj_stream));
+    OS_CUDA(cudaStreamSynchronize(a->adj_stream));
     OS_CUDA(cudaStreamSynchronize(a->h->stream));
     return OS_OK;
 }

@@ -260,7 +260,7 @@ __device__ __forceinline__ float em3d_lo_diff(float f0, float lo, bool first_row
 }
 
 template <int BZ = EM3D_BZ, int BY = EM3D_BY>
-__global__ void __launch_bounds__(BZ * BY, 3) em3d_e_kernel(const Em3DParams p) {
+__global__ void __launch_bounds__(BZ * BY, 4) em3d_e_kernel(const Em3DParams p) {
     int j, k, i0, i1;
     if (!em3d_block_box<BZ, BY>(p, j, k, i0, i1)) return;
     const size_t sx = (size_t)p.ny * p.nz;
