@@ -408,7 +408,8 @@ int os_fdtd3d_set_x_chunk(OsFdtd3D *h, int32_t planes);
 /* Step form (results bit-identical; no counterpart in open_sol, which has one form): 0 (the default) = the H and
  * the E kernel over the whole grid in place; 1 = one fused H + E kernel over every cell but the outermost layer of
  * each axis plus the two-kernel update of that layer, on two field sets and two CPML psi sets swapped every step
- * (twice the field memory, a third less DRAM traffic per step). */
+ * (twice the field memory, a third less DRAM traffic per step); 2 = form 1 with each x plane of a tile staged in shared
+ * memory by 1D bulk copies (rows of a multiple of 8 cells, at least 48; other grids run form 1). */
 int os_fdtd3d_set_variant(OsFdtd3D *h, int32_t variant);
 
 /* Launch shape of the fused kernel, 0..4 (tile rows 16 or 8 and the blocks per SM its registers are cut for; 3 by

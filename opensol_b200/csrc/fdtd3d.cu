@@ -8,8 +8,10 @@
 //     psi read and written once); that layer (where samples cross the grid edge) runs em3d_h_kernel over its six
 //     faces, then em3d_e_kernel, which reads the new H of both parts;
 //   variant 0 (default): em3d_h_kernel then em3d_e_kernel over the whole grid, in place on one field set.
+//   variant 2: variant 1 with each x plane of a tile staged in shared memory by 1D bulk copies (em3d_staged_kernel).
 // Variant 1 moves 52.8 B per cell-update against variant 0's 79.5 (ncu, 256^3) but issues from fewer resident warps
-// (one barrier per plane, 80 registers a thread), and on 512^3 it runs 42.6 G cell-updates/s against 44.8.
+// (one barrier per plane, 80 registers a thread): on 512^3 it runs 42.7 G cell-updates/s against 48.7; variant 2,
+// limited by ~60 small bulk copies per plane and block, 12-30.
 // A chunk of n steps is enqueued with no host synchronisation: per-step dipole amplitudes and per-sample DFT phases
 // arrive as small tables computed on the host in float64 and rounded as open_sol rounds them.
 #include "common.cuh"
@@ -28,7 +30,7 @@ struct OsFdtd3D {
     os::DeviceArray<float> field[6];            // ex, ey, ez, hx, hy, hz
     os::DeviceArray<float> field2[6];           // the second field set of variant 1 (allocated on first use)
     int cur = 0;                                // the set holding the current state (0: field, 1: field2)
-    int32_t variant = 0;                        // the faster form on 512^3 (44.8 vs 42.6 G cell-updates/s)
+    int32_t variant = 0;                        // the fastest form on 512^3 (48.7 vs 42.7 and 29.5 G cell-updates/s)
     int32_t fused_config = 3;                   // tile rows / blocks per SM of em3d_fused_kernel (speed only)
     os::DeviceArray<uint16_t> mat;
     os::DeviceArray<float> tables;              // t_ex, t_ey, t_ez, t_sig, t_da, t_db (6 * n_ids)
@@ -65,6 +67,7 @@ struct OsFdtd3D {
     os::DeviceArray<float> values;              // (n_dipoles, n_steps) of the current chunk
     os::DeviceArray<float> phases;              // (n_samples, sum nf, 2) of the current chunk
     os::DeviceArray<float> scratch;             // one float (face cb read-back)
+    os::DeviceArray<int32_t> err;               // set by a staged kernel whose bounded wait ran out
 };
 
 namespace os {
@@ -111,6 +114,7 @@ static Em3DParams make_params3(const OsFdtd3D *h) {
     p.hz = p.ohz = fset(h, h->cur, 5);
     whole_grid_boxes(h, p);
     p.mat = h->mat.ptr;
+    p.err = h->err.ptr;
     const int n = h->n_ids;
     const float *t = h->tables.ptr;
     p.t_ex = t;
@@ -197,7 +201,26 @@ static Em3DBox fused_box(const OsFdtd3D *h) {
 
 static bool fused_active(const OsFdtd3D *h) {
     const OsGrid3D &g = h->grid;
-    return h->variant == 1 && g.nx >= 3 && g.ny >= 3 && g.nz >= 3;
+    return h->variant >= 1 && g.nx >= 3 && g.ny >= 3 && g.nz >= 3;
+}
+
+// variant 2 stages the planes by bulk copies: rows must start on 16-byte boundaries and hold the 48-id window.
+static bool staged_active(const OsFdtd3D *h) {
+    return fused_active(h) && h->variant == 2 && h->grid.nz % 8 == 0 && h->grid.nz >= EM3D_WM;
+}
+
+// A bounded wait of a staged kernel ran out: report it once (the flag is cleared) as OS_ERR_CUDA.
+static int check_err3(OsFdtd3D *h) {
+    int32_t flag = 0;
+    OS_CUDA(cudaMemcpyAsync(&flag, h->err.ptr, sizeof(flag), cudaMemcpyDeviceToHost, h->stream));
+    OS_CUDA(cudaStreamSynchronize(h->stream));
+    if (flag) {
+        OS_CUDA(cudaMemsetAsync(h->err.ptr, 0, sizeof(int32_t), h->stream));
+        OS_CUDA(cudaStreamSynchronize(h->stream));
+        OS_CHECK(false, OS_ERR_CUDA, "a 3D step kernel gave up waiting for its staged planes (2 s); the fields of "
+                                     "that advance are not valid");
+    }
+    return OS_OK;
 }
 
 // The outermost layer around the fused box: the x and y faces (coalesced along k: 32 x 8 blocks) or the z faces
@@ -241,6 +264,30 @@ static void point_psi(const OsFdtd3D *h, Em3DParams &p, int in, int out) {
 // em3d_fused_kernel configurations: (tile rows, blocks per SM the register budget is cut for).
 constexpr int FUSED_CONFIGS = 5;
 static int fused_rows(int config) { return config == 0 || config == 1 ? 16 : 8; }
+
+template <int TY, int MINB>
+static int launch_staged_shape(dim3 grid, const Em3DParams &p, const Em3DBox &in, cudaStream_t s) {
+    constexpr size_t bytes = em3d_staged_smem<TY>();
+    static bool attr_set = false;   // per template instance; the attribute outlives the handle
+    if (!attr_set) {
+        OS_CUDA(cudaFuncSetAttribute(em3d_staged_kernel<TY, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)bytes));
+        attr_set = true;
+    }
+    em3d_staged_kernel<TY, MINB><<<grid, dim3(EM3D_FZ, TY), bytes, s>>>(p, in);
+    OS_CUDA(cudaGetLastError());
+    return OS_OK;
+}
+
+static int launch_staged(int config, dim3 grid, const Em3DParams &p, const Em3DBox &in, cudaStream_t s) {
+    switch (config) {
+        case 0: return launch_staged_shape<16, 1>(grid, p, in, s);
+        case 1: return launch_staged_shape<16, 2>(grid, p, in, s);
+        case 2: return launch_staged_shape<8, 2>(grid, p, in, s);
+        case 3: return launch_staged_shape<8, 3>(grid, p, in, s);
+        default: return launch_staged_shape<8, 4>(grid, p, in, s);
+    }
+}
 
 static int launch_fused(int config, dim3 grid, const Em3DParams &p, const Em3DBox &in, cudaStream_t s) {
     switch (config) {
@@ -296,6 +343,8 @@ extern "C" int os_fdtd3d_create(const OsGrid3D *grid, OsFdtd3D **out) {
     OS_TRY(h->mat.alloc(n));
     OS_TRY(h->rows.alloc(4 * ((size_t)g.nx + g.ny + g.nz)));
     OS_TRY(h->scratch.alloc(1));
+    OS_TRY(h->err.alloc(1));
+    OS_CUDA(cudaMemsetAsync(h->err.ptr, 0, sizeof(int32_t), h->stream));
     // x chunk: short runs of 24 planes per block (many more blocks than resident slots, so the last wave is a small
     // share of the launch; on 512^3 the step ran 37.9 G cell-updates/s at 256 planes, 48.6-50.4 at 12-32)
     h->x_chunk = std::min<int32_t>(g.nx, 24);
@@ -545,7 +594,7 @@ extern "C" int os_fdtd3d_advance(OsFdtd3D *h, int64_t n_steps, const float *dipo
         OS_TRY(upload(h->pairs_dev, h->pairs.data(), h->pairs.size(), h->stream));
         h->pairs_dirty = false;
     }
-    const bool fused = fused_active(h);
+    const bool fused = fused_active(h), staged = staged_active(h);
     if (fused) {
         for (auto &f : h->field2)
             if (!f.ptr) OS_TRY(f.alloc(cells3(h)));
@@ -579,7 +628,8 @@ extern "C" int os_fdtd3d_advance(OsFdtd3D *h, int64_t n_steps, const float *dipo
             point_psi(h, pz, a, b);
             em3d_h_kernel<EM3D_BZ, EM3D_BY><<<box_grid(p), block, 0, h->stream>>>(p);
             em3d_h_kernel<1, 256><<<box_grid(pz, 1, 256), zblock, 0, h->stream>>>(pz);
-            OS_TRY(launch_fused(h->fused_config, fused_grid, p, in, h->stream));
+            if (staged) OS_TRY(launch_staged(h->fused_config, fused_grid, p, in, h->stream));
+            else OS_TRY(launch_fused(h->fused_config, fused_grid, p, in, h->stream));
             // faces E: E^n and psi of set a, H^{n+1/2} of set b -> E^{n+1}, psi' of set b
             point_sets(h, p, a, b, b, b);
             point_sets(h, pz, a, b, b, b);
@@ -617,7 +667,7 @@ extern "C" int os_fdtd3d_read_field(OsFdtd3D *h, int32_t component, float *out) 
     OS_CUDA(cudaMemcpyAsync(out, fset(h, h->cur, component), h->field[component].bytes(), cudaMemcpyDeviceToHost,
                             h->stream));
     OS_CUDA(cudaStreamSynchronize(h->stream));
-    return OS_OK;
+    return check_err3(h);
 }
 
 extern "C" int os_fdtd3d_write_field(OsFdtd3D *h, int32_t component, const float *in) {
@@ -653,7 +703,7 @@ extern "C" int os_fdtd3d_synchronize(OsFdtd3D *h) {
     OS_CHECK(h, OS_ERR_INVALID, "os_fdtd3d_synchronize: null handle");
     OS_TRY(bind3(h));
     OS_CUDA(cudaStreamSynchronize(h->stream));
-    return OS_OK;
+    return check_err3(h);
 }
 
 extern "C" int os_fdtd3d_set_stream(OsFdtd3D *h, void *cuda_stream) {
@@ -673,8 +723,9 @@ extern "C" int os_fdtd3d_set_x_chunk(OsFdtd3D *h, int32_t planes) {
 
 extern "C" int os_fdtd3d_set_variant(OsFdtd3D *h, int32_t variant) {
     OS_CHECK(h, OS_ERR_INVALID, "os_fdtd3d_set_variant: null handle");
-    OS_CHECK(variant == 0 || variant == 1, OS_ERR_INVALID,
-             "variant must be 0 (two in-place kernels) or 1 (fused interior, two field sets), got %d", variant);
+    OS_CHECK(variant >= 0 && variant <= 2, OS_ERR_INVALID,
+             "variant must be 0 (two in-place kernels), 1 (fused, two field sets) or 2 (fused with staged planes), "
+             "got %d", variant);
     h->variant = variant;
     return OS_OK;
 }

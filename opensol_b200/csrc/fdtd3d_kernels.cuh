@@ -17,6 +17,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "mbarrier.cuh"
+
 #define EM3D_EPS0F 8.8541878128e-12f
 
 constexpr int EM3D_BZ = 32;            // threads along z (one warp)
@@ -68,6 +70,7 @@ struct Em3DParams {
     float dip_weight[EM3D_MAX_DIPOLES];
     const float *dip_values;                   // (n_dip, values_stride) float32 amplitude per step
     int64_t values_stride, k_step;
+    int32_t *err;                              // set to 1 when a bounded wait of the staged kernel runs out
 };
 
 __device__ __forceinline__ float em3d_wrapped(float v) { return __fadd_rn(__fmul_rn(1.0f, v), __fmul_rn(0.0f, v)); }
@@ -618,6 +621,271 @@ __global__ void __launch_bounds__(EM3D_FZ * TY, MINB) em3d_fused_kernel(const Em
         bn = bnn;
         par ^= 1;
     }
+}
+
+// ---------------------------------------------------------------------------------------------------- staged step
+// em3d_fused_kernel with the planes staged in shared memory: each x plane's rows of the block's tile arrive by 1D bulk
+// copies (cp.async.bulk, this GPU's own memory, no multicast) into a ring of EM3D_RING plane slots, EM3D_RING - 2
+// planes ahead of the plane being computed, completing on one mbarrier per slot; the threads read E, H and the
+// material ids from shared memory instead of holding loads in flight.  Per plane and slot: E rows j0 - 1 .. j0 + TY - 1
+// (the j + 1 row of the last warp included) and H rows j0 - 1 .. j0 + TY - 2, 40-float windows from the 16-byte
+// boundary at or before column k0 - 1 (moved left where a window would pass the row end); material ids the same rows
+// as E, 48-entry windows from the 16-byte boundary.  Needs nz a multiple of 8 and at least 48.  Warp 0 (the halo row,
+// which computes no E) issues the copies of plane i + EM3D_RING - 1 into the slot of plane i - 1 after the plane's
+// barrier, when no thread reads that slot any more.  Every wait is bounded (2 s): a block whose wait runs out sets
+// *err, waits (bounded) for its own copies in flight and returns; material ids are clamped below n_ids, so a
+// stale slot never indexes past the tables.  Arithmetic and results: em3d_fused_kernel's, bit for bit.
+constexpr int EM3D_RING = 4;
+constexpr int EM3D_WF = 40;   // floats per field row window (160 B)
+constexpr int EM3D_WM = 48;   // ids per material row window (96 B)
+
+template <int TY>
+struct Em3DStage {
+    float e[3][TY + 1][EM3D_WF];
+    float h[3][TY][EM3D_WF];
+    uint16_t m[TY + 1][EM3D_WM];
+};
+
+template <int TY>
+__host__ __device__ constexpr size_t em3d_staged_smem() {
+    return sizeof(Em3DStage<TY>) * EM3D_RING + 2 * 2 * TY * 32 * sizeof(float) + EM3D_RING * sizeof(uint64_t);
+}
+
+template <int TY>
+__device__ __forceinline__ void em3d_issue_plane(const Em3DParams &p, Em3DStage<TY> *st, uint64_t *bar, int plane,
+                                                 int j_row0, int ca, int cam, int lane) {
+    // one copy per row and array: 3 (TY + 1) E rows, 3 TY H rows, TY + 1 id rows
+    constexpr int n_e = 3 * (TY + 1), n_h = 3 * TY, n_m = TY + 1;
+    constexpr uint32_t bytes = (uint32_t)(n_e + n_h) * EM3D_WF * 4 + (uint32_t)n_m * EM3D_WM * 2;
+    if (lane == 0) tb_mbar_expect_tx(bar, bytes);
+    __syncwarp();
+    const size_t sx = (size_t)p.ny * p.nz;
+    for (int q = lane; q < n_e + n_h + n_m; q += 32) {
+        if (q < n_e) {
+            const int c = q / (TY + 1), r = q % (TY + 1);
+            const int row = min(j_row0 + r, p.ny - 1);
+            const float *src = c == 0 ? p.ex : (c == 1 ? p.ey : p.ez);
+            tb_bulk_g2s(st->e[c][r], src + (size_t)plane * sx + (size_t)row * p.nz + ca, EM3D_WF * 4, bar);
+        } else if (q < n_e + n_h) {
+            const int c = (q - n_e) / TY, r = (q - n_e) % TY;
+            const int row = min(j_row0 + r, p.ny - 1);
+            const float *src = c == 0 ? p.hx : (c == 1 ? p.hy : p.hz);
+            tb_bulk_g2s(st->h[c][r], src + (size_t)plane * sx + (size_t)row * p.nz + ca, EM3D_WF * 4, bar);
+        } else {
+            const int r = q - n_e - n_h;
+            const int row = min(j_row0 + r, p.ny - 1);
+            tb_bulk_g2s(st->m[r], p.mat + (size_t)plane * sx + (size_t)row * p.nz + cam, EM3D_WM * 2, bar);
+        }
+    }
+}
+
+template <int TY, int MINB>
+__global__ void __launch_bounds__(EM3D_FZ * TY, MINB) em3d_staged_kernel(const Em3DParams p, const Em3DBox in) {
+    extern __shared__ __align__(128) unsigned char em3d_smem[];
+    Em3DStage<TY> *ring = reinterpret_cast<Em3DStage<TY> *>(em3d_smem);
+    float(*s_hz)[TY][EM3D_FZ] = reinterpret_cast<float(*)[TY][EM3D_FZ]>(em3d_smem + sizeof(Em3DStage<TY>) * EM3D_RING);
+    float(*s_hx)[TY][EM3D_FZ] = reinterpret_cast<float(*)[TY][EM3D_FZ]>(
+        em3d_smem + sizeof(Em3DStage<TY>) * EM3D_RING + 2 * TY * EM3D_FZ * sizeof(float));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(em3d_smem + sizeof(Em3DStage<TY>) * EM3D_RING +
+                                                 4 * TY * EM3D_FZ * sizeof(float));
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int k_lo = in.k0 - 1 + (int)blockIdx.x * (EM3D_FZ - 1);   // this tile's first column (the halo)
+    const int j_row0 = in.j0 - 1 + (int)blockIdx.y * (TY - 1);      // its first row (the halo)
+    const int kk = k_lo + lane, jj = j_row0 + w;
+    const bool e_thread = lane > 0 && w > 0;
+    const bool emit = e_thread && kk < in.k1 && jj < in.j1;
+    const int k = min(kk, in.k1 - 1), j = min(jj, in.j1 - 1);
+    const int i_first = in.i0 + (int)blockIdx.z * p.x_chunk;
+    const int i_last = min(in.i1, i_first + p.x_chunk);
+    const int ca = min(k_lo & ~3, p.nz - EM3D_WF);     // 16-byte window starts
+    const int cam = min(k_lo & ~7, p.nz - EM3D_WM);
+    const int r = j - j_row0;                          // this thread's row in the staged tile
+    const int c0 = k - ca, m_c = k - cam;              // its column in the field / id windows
+    const size_t sx = (size_t)p.ny * p.nz;
+    const int o = j * p.nz + k;
+    const int base = i_first - 1;                      // plane of ring position 0
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        for (int q = 0; q < EM3D_RING; ++q) tb_mbar_init(bar + q, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        tb_fence_proxy_async();
+    }
+    __syncthreads();
+    if (w == 0)
+        for (int q = 0; q < EM3D_RING && base + q <= i_last; ++q)
+            em3d_issue_plane<TY>(p, ring + q, bar + q, base + q, j_row0, ca, cam, lane);
+    const int n_issued_max = i_last - base + 1;        // planes base .. i_last are staged
+    float *__restrict__ oex = p.oex;
+    float *__restrict__ oey = p.oey;
+    float *__restrict__ oez = p.oez;
+    float *__restrict__ ohx = p.ohx;
+    float *__restrict__ ohy = p.ohy;
+    float *__restrict__ ohz = p.ohz;
+    const float ihy = p.ihy[j], ihz = p.ihz[k];
+    const float iey = p.iey[j], iez = p.iez[k];
+    const float wly = p.wly[j], wuy = p.wuy[j], wlz = p.wlz[k], wuz = p.wuz[k];
+    const int32_t ryh = p.cpml[1].nr ? p.cpml[1].rm_h[j] : -1, rye = p.cpml[1].nr ? p.cpml[1].rm_e[j] : -1;
+    const int32_t rzh = p.cpml[2].nr ? p.cpml[2].rm_h[k] : -1, rze = p.cpml[2].nr ? p.cpml[2].rm_e[k] : -1;
+    const uint16_t id_max = (uint16_t)(p.n_ids - 1);
+    bool ok = tb_mbar_wait(bar, 0);                    // plane base
+    float hy_m = 0.0f, hz_m = 0.0f;
+    int par = 0;
+    for (int i = base; i < i_last; ++i) {
+        const int q = i - base;
+        const Em3DStage<TY> &cur = ring[q % EM3D_RING];
+        const Em3DStage<TY> &nxt = ring[(q + 1) % EM3D_RING];
+        ok = tb_mbar_wait(bar + (q + 1) % EM3D_RING, (uint32_t)(((q + 1) / EM3D_RING) & 1)) && ok;
+        const float ex0 = cur.e[0][r][c0], ey0 = cur.e[1][r][c0], ez0 = cur.e[2][r][c0];
+        const float exy = cur.e[0][r + 1][c0], ezy = cur.e[2][r + 1][c0];
+        const float exz = cur.e[0][r][c0 + 1], eyz = cur.e[1][r][c0 + 1];
+        const float eyn = nxt.e[1][r][c0], ezn = nxt.e[2][r][c0];
+        const float hx0 = cur.h[0][r][c0], hy0 = cur.h[1][r][c0], hz0 = cur.h[2][r][c0];
+        const uint16_t m0 = min(cur.m[r][m_c], id_max);
+        const bool inside = i >= i_first;
+        const bool store = emit && inside;
+        float da, db;
+        if (p.h_uniform) {
+            da = p.da_u;
+            db = p.db_u;
+        } else {
+            da = p.t_da[m0];
+            db = p.t_db[m0];
+        }
+        const float ihx = p.ihx[i];
+        const float dez_y = ezy - ez0, dey_z = eyz - ey0, dex_z = exz - ex0, dez_x = ezn - ez0;
+        const float dey_x = eyn - ey0, dex_y = exy - ex0;
+        float vhx = da * hx0 - db * (dez_y * ihy - dey_z * ihz);
+        float vhy = da * hy0 - db * (dex_z * ihz - dez_x * ihx);
+        float vhz = da * hz0 - db * (dey_x * ihx - dex_y * ihy);
+        const int32_t rxh = p.cpml[0].nr ? p.cpml[0].rm_h[i] : -1;
+        if (rxh >= 0) {   // x layers: H_y from E_z (+), H_z from E_y (-)
+            const Em3DCpmlAxis &c = p.cpml[0];
+            const size_t qq = (size_t)rxh * sx + o;
+            const float f = c.b_h[rxh] * c.ph_first[qq] + c.g_h[rxh] * dez_x;
+            const float g = c.b_h[rxh] * c.ph_second[qq] + c.g_h[rxh] * dey_x;
+            if (store) {
+                c.oph_first[qq] = f;
+                c.oph_second[qq] = g;
+            }
+            vhy += db * f;
+            vhz -= db * g;
+        }
+        if (ryh >= 0) {   // y layers: H_x from E_z (-), H_z from E_x (+)
+            const Em3DCpmlAxis &c = p.cpml[1];
+            const size_t qq = ((size_t)i * c.nr + ryh) * p.nz + k;
+            const float f = c.b_h[ryh] * c.ph_first[qq] + c.g_h[ryh] * dez_y;
+            const float g = c.b_h[ryh] * c.ph_second[qq] + c.g_h[ryh] * dex_y;
+            if (store) {
+                c.oph_first[qq] = f;
+                c.oph_second[qq] = g;
+            }
+            vhx -= db * f;
+            vhz += db * g;
+        }
+        if (rzh >= 0) {   // z layers: H_x from E_y (+), H_y from E_x (-)
+            const Em3DCpmlAxis &c = p.cpml[2];
+            const size_t qq = ((size_t)i * p.ny + j) * c.nr + rzh;
+            const float f = c.b_h[rzh] * c.ph_first[qq] + c.g_h[rzh] * dey_z;
+            const float g = c.b_h[rzh] * c.ph_second[qq] + c.g_h[rzh] * dex_z;
+            if (store) {
+                c.oph_first[qq] = f;
+                c.oph_second[qq] = g;
+            }
+            vhx += db * f;
+            vhy -= db * g;
+        }
+        if (store) {
+            ohx[(size_t)i * sx + o] = vhx;
+            ohy[(size_t)i * sx + o] = vhy;
+            ohz[(size_t)i * sx + o] = vhz;
+        }
+        s_hz[par][w][lane] = vhz;
+        s_hx[par][w][lane] = vhx;
+        const float hy_z = __shfl_up_sync(0xffffffffu, vhy, 1);
+        const float hx_z = __shfl_up_sync(0xffffffffu, vhx, 1);
+        if (__syncthreads_or(!ok)) {   // a wait ran out somewhere in the block: stop, after the copies in flight
+            if (threadIdx.x == 0 && threadIdx.y == 0) atomicExch(p.err, 1);
+            if (w == 0)   // positions q + 1 .. q + 2 may still be in flight (q + 3 is issued after this barrier)
+                for (int qq = q + 1; qq < min(n_issued_max, q + EM3D_RING - 1); ++qq)
+                    tb_mbar_wait(bar + qq % EM3D_RING, (uint32_t)((qq / EM3D_RING) & 1));
+            return;
+        }
+        // no thread reads the slot of plane i - 1 any more: it takes plane i + EM3D_RING - 1
+        if (w == 0 && q >= 1 && i + EM3D_RING - 1 <= i_last) {
+            tb_fence_proxy_async();
+            em3d_issue_plane<TY>(p, ring + (q - 1) % EM3D_RING, bar + (q - 1) % EM3D_RING, i + EM3D_RING - 1, j_row0,
+                                 ca, cam, lane);
+        }
+        if (e_thread && inside) {
+            const float hz_y = s_hz[par][w - 1][lane];
+            const float hx_y = s_hx[par][w - 1][lane];
+            const float dhz_y = vhz - hz_y, dhy_z = vhy - hy_z, dhx_z = vhx - hx_z;
+            const float dhz_x = vhz - hz_m, dhy_x = vhy - hy_m, dhx_y = vhx - hx_y;
+            const uint16_t mx = min(nxt.m[r][m_c], id_max);
+            const uint16_t my = min(cur.m[r + 1][m_c], id_max);
+            const uint16_t mz = min(cur.m[r][m_c + 1], id_max);
+            float ca_, cbx, cby, cbz;
+            const float iex = p.iex[i];
+            em3d_face_fast(p, 0, p.t_ex, m0, mx, p.wlx[i], p.wux[i], ca_, cbx);
+            float vx = ca_ * ex0 + cbx * (dhz_y * iey - dhy_z * iez);
+            em3d_face_fast(p, 1, p.t_ey, m0, my, wly, wuy, ca_, cby);
+            float vy = ca_ * ey0 + cby * (dhx_z * iez - dhz_x * iex);
+            em3d_face_fast(p, 2, p.t_ez, m0, mz, wlz, wuz, ca_, cbz);
+            float vz = ca_ * ez0 + cbz * (dhy_x * iex - dhx_y * iey);
+            const int32_t rxe = p.cpml[0].nr ? p.cpml[0].rm_e[i] : -1;
+            if (rxe >= 0) {
+                const Em3DCpmlAxis &c = p.cpml[0];
+                const size_t qq = (size_t)rxe * sx + o;
+                const float f = c.b_e[rxe] * c.pe_first[qq] + c.g_e[rxe] * dhz_x;
+                const float g = c.b_e[rxe] * c.pe_second[qq] + c.g_e[rxe] * dhy_x;
+                if (emit) {
+                    c.ope_first[qq] = f;
+                    c.ope_second[qq] = g;
+                }
+                vy -= cby * f;
+                vz += cbz * g;
+            }
+            if (rye >= 0) {
+                const Em3DCpmlAxis &c = p.cpml[1];
+                const size_t qq = ((size_t)i * c.nr + rye) * p.nz + k;
+                const float f = c.b_e[rye] * c.pe_first[qq] + c.g_e[rye] * dhz_y;
+                const float g = c.b_e[rye] * c.pe_second[qq] + c.g_e[rye] * dhx_y;
+                if (emit) {
+                    c.ope_first[qq] = f;
+                    c.ope_second[qq] = g;
+                }
+                vx += cbx * f;
+                vz -= cbz * g;
+            }
+            if (rze >= 0) {
+                const Em3DCpmlAxis &c = p.cpml[2];
+                const size_t qq = ((size_t)i * p.ny + j) * c.nr + rze;
+                const float f = c.b_e[rze] * c.pe_first[qq] + c.g_e[rze] * dhy_z;
+                const float g = c.b_e[rze] * c.pe_second[qq] + c.g_e[rze] * dhx_z;
+                if (emit) {
+                    c.ope_first[qq] = f;
+                    c.ope_second[qq] = g;
+                }
+                vx -= cbx * f;
+                vy += cby * g;
+            }
+            for (int d = 0; d < p.n_dip; ++d) {
+                if (p.dip_o[d] != o || p.dip_i[d] != i) continue;
+                const float add = p.dip_values[d * p.values_stride + p.k_step] * p.dip_weight[d];
+                if (p.dip_comp[d] == 0) vx = vx + add;
+                else if (p.dip_comp[d] == 1) vy = vy + add;
+                else vz = vz + add;
+            }
+            if (emit) {
+                oex[(size_t)i * sx + o] = vx;
+                oey[(size_t)i * sx + o] = vy;
+                oez[(size_t)i * sx + o] = vz;
+            }
+        }
+        hy_m = vhy;
+        hz_m = vhz;
+        par ^= 1;
+    }
+    // the last staged plane (i_last) was waited in the last iteration; nothing is in flight
 }
 
 // ---------------------------------------------------------------------------------------------------- running DFT

@@ -294,7 +294,8 @@ class FDTDEngine3D:
 
     def set_variant(self, variant):
         """Step form (speed and memory only; results are bit-identical): 0 = the two in-place kernels (the default),
-        1 = the fused kernel on two field and psi sets."""
+        1 = the fused kernel on two field and psi sets, 2 = the fused kernel with its planes staged in shared memory
+        by bulk copies (rows of a multiple of 8 cells; other grids run form 1)."""
         _native.check(_native.load().os_fdtd3d_set_variant(self.handle, int(variant)))
 
     def set_fused_config(self, config):

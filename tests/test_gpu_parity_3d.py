@@ -165,6 +165,7 @@ def test_workload_512_against_oracle():
     from opensol_b200 import workloads
     physics, box = workloads.roofline_3d_physics()
     physics.finalize()
+    physics.engine.set_variant(2)   # the staged fused form on the full grid; every form gives the same bits
     o, obox = roofline_3d_oracle()
     np.testing.assert_array_equal(physics.domain.materials.array('eps_r'), o.materials['eps_r'])
     assert box.sample_interval == obox.sample_interval
@@ -180,3 +181,29 @@ def test_workload_512_against_oracle():
             np.testing.assert_array_equal(e, opair['e_dft'])
             np.testing.assert_array_equal(h, opair['h_dft'])
     np.testing.assert_array_equal(np.asarray(box.flux()), np.asarray(obox.flux()))
+
+
+@pytest.mark.parametrize('total', [64, 96])
+def test_staged_form_bit_identical(total):
+    """The fused form with planes staged in shared memory by bulk copies (variant 2; rows of a multiple of 8 cells,
+    here the 3D workload on 64^3 and 96^3 grids) in every launch shape gives the fields and box flux of the in-place
+    two-kernel form bit for bit, over uneven chunks and short and long x chunks."""
+    from opensol_b200 import workloads
+    n_spheres = max(1, int(round(500 * (total / 512) ** 3)))
+    runs = []
+    for variant, config, chunk in ((0, 0, 24), (2, 0, 24), (2, 1, 7), (2, 2, 24), (2, 3, 1), (2, 4, 50)):
+        physics, box = workloads.roofline_3d_physics(total_cells=total, n_spheres=n_spheres)
+        physics.finalize()
+        engine = physics.engine
+        engine.set_variant(variant)
+        engine.set_fused_config(config)
+        engine.set_x_chunk(chunk)
+        for n in (13, 1, 40):
+            physics.run(n)
+        runs.append((engine.state(), np.asarray(box.flux())))
+        del physics, box
+    assert np.abs(runs[0][0]['ez']).max() > 0
+    for state, flux in runs[1:]:
+        for name in FIELDS:
+            np.testing.assert_array_equal(state[name], runs[0][0][name], err_msg=name)
+        np.testing.assert_array_equal(flux, runs[0][1])
