@@ -98,6 +98,7 @@ struct OsFdtd2D {
     int32_t gen_tile_rows = 16;           // rows per general tile
     int64_t launches = 0;                 // kernels launched by the last advance
     bool profiling = false;               // bracket every kernel with events (os_fdtd2d_kernel_times)
+    int64_t stall_probe_ns = 0;           // test hook of the bounded waits (os_fdtd2d_set_stall_probe)
     std::vector<cudaEvent_t> prof_events; // pool, grown on demand
     std::vector<int> prof_kind;           // kind of each recorded pair: 0 interior, 1 general, 2 DFT, 3 per-step
     size_t prof_used = 0;
@@ -818,6 +819,7 @@ static void fill_common(const OsFdtd2D *h, TBParams &q) {
     }
     q.m = h->sample_interval;
     q.err = h->err.ptr;
+    q.stall_probe_ns = h->stall_probe_ns;
 }
 
 template <int T, bool CA, bool PX, bool PY, bool VEC>
@@ -1725,6 +1727,14 @@ extern "C" int os_fdtd2d_advance_noalloc(OsFdtd2D *h, int64_t n_steps, const flo
         OS_CUDA(cudaMemcpyAsync(scratch + phase_offset, phases, phase_floats * sizeof(float),
                                 cudaMemcpyHostToDevice, h->stream));
     return run_chunk(h, n_steps, first_sample, n_samples, scratch, scratch + phase_offset);
+}
+
+extern "C" int os_fdtd2d_set_stall_probe(OsFdtd2D *h, int64_t wait_ns) {
+    OS_CHECK(h, OS_ERR_INVALID, "os_fdtd2d_set_stall_probe: null handle");
+    OS_CHECK(wait_ns >= 0 && wait_ns <= (int64_t)TB_WAIT_NS, OS_ERR_INVALID,
+             "os_fdtd2d_set_stall_probe: the wait must be within [0, %llu] ns", (unsigned long long)TB_WAIT_NS);
+    h->stall_probe_ns = wait_ns;
+    return OS_OK;
 }
 
 extern "C" int os_fdtd2d_configure(OsFdtd2D *h, int32_t variant, int32_t steps_per_launch, int32_t tile_rows) {

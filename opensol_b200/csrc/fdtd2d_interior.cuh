@@ -472,6 +472,24 @@ __device__ __forceinline__ void ez2d_interior_tile(const TBParams &p, int w, uns
 template <int T, bool CA, bool PX, bool PY, bool VEC>
 __global__ void __launch_bounds__(TB_WARPS * 32, 4) ez2d_interior_kernel(const TBParams p) {
     extern __shared__ __align__(16) unsigned char tb_smem[];
+    if (p.stall_probe_ns && blockIdx.x == 0 && threadIdx.x < 32) {
+        // test hook: a wait on an mbarrier that no copy and no thread ever completes, bounded like every real wait;
+        // when it runs out the warp sets the error flag and leaves its tile unwritten, as a real timeout does (it has
+        // issued no copy yet, so nothing is in flight)
+        __shared__ uint64_t probe_bar;
+        if (threadIdx.x == 0) {
+            tb_mbar_init(&probe_bar, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncwarp();
+        bool done = tb_mbar_try_wait(&probe_bar, 0);
+        const uint64_t t0 = tb_globaltimer();
+        while (!done && tb_globaltimer() - t0 <= (uint64_t)p.stall_probe_ns) done = tb_mbar_try_wait(&probe_bar, 0);
+        if (!__all_sync(0xffffffffu, done)) {
+            if (threadIdx.x == 0) atomicExch(p.err, 1);
+            return;
+        }
+    }
     ez2d_interior_tile<T, CA, PX, PY, VEC, true>(p, blockIdx.x * TB_WARPS + (threadIdx.x >> 5), tb_smem);
 }
 

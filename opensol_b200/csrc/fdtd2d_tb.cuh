@@ -86,6 +86,10 @@ struct TBParams {
     TBRect rects[TB_MAX_RECTS];
     int32_t tile_w, tile_rows, n_tiles;
     int32_t *err;   // set to 1 when a bounded wait runs out (read by the host after the launch)
+    // test hook of the bounded waits (0: off): warp 0 of block 0 of the interior kernel first waits on an mbarrier
+    // that nothing completes, at most this many nanoseconds, and then gives up as a real wait does
+    int64_t stall_probe_ns;
+    int64_t reserved;
 };
 
 // Shared memory of one warp of the interior variant: field ring (TB_AHEAD + 1 slots x E, H_x, H_y rows), coefficient

@@ -8,10 +8,11 @@
 //     psi read and written once); that layer (where samples cross the grid edge) runs em3d_h_kernel over its six
 //     faces, then em3d_e_kernel, which reads the new H of both parts;
 //   variant 0 (default): em3d_h_kernel then em3d_e_kernel over the whole grid, in place on one field set.
-//   variant 2: variant 1 with each x plane of a tile staged in shared memory by 1D bulk copies (em3d_staged_kernel).
+//   variant 2: variant 1 with each x plane of a tile staged in shared memory by tiled tensor copies
+//     (em3d_staged_kernel).
 // Variant 1 moves 52.8 B per cell-update against variant 0's 79.5 (ncu, 256^3) but issues from fewer resident warps
-// (one barrier per plane, 80 registers a thread): on 512^3 it runs 42.7 G cell-updates/s against 48.7; variant 2,
-// limited by ~60 small bulk copies per plane and block, 12-30.
+// (one barrier per plane, 80 registers a thread): on 512^3 it runs 42.7 G cell-updates/s against 48.6; variant 2 runs
+// 48.4 (issue- and barrier-bound once the loads are staged).
 // A chunk of n steps is enqueued with no host synchronisation: per-step dipole amplitudes and per-sample DFT phases
 // arrive as small tables computed on the host in float64 and rounded as open_sol rounds them.
 #include "common.cuh"
@@ -30,7 +31,7 @@ struct OsFdtd3D {
     os::DeviceArray<float> field[6];            // ex, ey, ez, hx, hy, hz
     os::DeviceArray<float> field2[6];           // the second field set of variant 1 (allocated on first use)
     int cur = 0;                                // the set holding the current state (0: field, 1: field2)
-    int32_t variant = 0;                        // the fastest form on 512^3 (48.7 vs 42.7 and 29.5 G cell-updates/s)
+    int32_t variant = 0;                        // on 512^3: 48.6 G cell-updates/s, variant 1 42.7, variant 2 48.4
     int32_t fused_config = 3;                   // tile rows / blocks per SM of em3d_fused_kernel (speed only)
     os::DeviceArray<uint16_t> mat;
     os::DeviceArray<float> tables;              // t_ex, t_ey, t_ez, t_sig, t_da, t_db (6 * n_ids)
@@ -68,6 +69,8 @@ struct OsFdtd3D {
     os::DeviceArray<float> phases;              // (n_samples, sum nf, 2) of the current chunk
     os::DeviceArray<float> scratch;             // one float (face cb read-back)
     os::DeviceArray<int32_t> err;               // set by a staged kernel whose bounded wait ran out
+    Em3DMaps maps[2][2];                        // staged form: tensor maps per field set read and tile height (8, 16)
+    bool maps_ok[2][2] = {{false, false}, {false, false}};
 };
 
 namespace os {
@@ -265,8 +268,60 @@ static void point_psi(const OsFdtd3D *h, Em3DParams &p, int in, int out) {
 constexpr int FUSED_CONFIGS = 5;
 static int fused_rows(int config) { return config == 0 || config == 1 ? 16 : 8; }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the library does not link libcuda itself).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static int encode_tiled_fn(EncodeTiledFn *out) {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *ptr = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        OS_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q));
+        OS_CHECK(ptr && q == cudaDriverEntryPointSuccess, OS_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+        fn = (EncodeTiledFn)ptr;
+    }
+    *out = fn;
+    return OS_OK;
+}
+
+// A map of one (nx, ny, nz) array, z contiguous, with boxes of box_k x box_j x 1 (zero fill outside the array).
+static int encode_box(CUtensorMap *map, const void *base, CUtensorMapDataType type, size_t elem, const OsGrid3D &g,
+                      uint32_t box_k, uint32_t box_j) {
+    EncodeTiledFn fn;
+    OS_TRY(encode_tiled_fn(&fn));
+    const cuuint64_t dims[3] = {(cuuint64_t)g.nz, (cuuint64_t)g.ny, (cuuint64_t)g.nx};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.nz * elem, (cuuint64_t)g.ny * g.nz * elem};
+    const cuuint32_t box[3] = {box_k, box_j, 1};
+    const cuuint32_t element_strides[3] = {1, 1, 1};
+    const CUresult r = fn(map, type, 3, const_cast<void *>(base), dims, strides, box, element_strides,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    OS_CHECK(r == CUDA_SUCCESS, OS_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return OS_OK;
+}
+
+// The staged launch's maps for field set `set` and tile height ty (made once per handle).
+static int staged_maps(OsFdtd3D *h, int set, int ty, const Em3DMaps **out) {
+    const int t = ty == 16 ? 1 : 0;
+    if (!h->maps_ok[set][t]) {
+        Em3DMaps &m = h->maps[set][t];
+        for (int c = 0; c < 3; ++c) {
+            OS_TRY(encode_box(&m.e[c], fset(h, set, c), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->grid, EM3D_WF, ty + 1));
+            OS_TRY(encode_box(&m.h[c], fset(h, set, 3 + c), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->grid, EM3D_WF,
+                              ty));
+        }
+        OS_TRY(encode_box(&m.m, h->mat.ptr, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, h->grid, EM3D_WM, ty + 1));
+        h->maps_ok[set][t] = true;
+    }
+    *out = &h->maps[set][t];
+    return OS_OK;
+}
+
 template <int TY, int MINB>
-static int launch_staged_shape(dim3 grid, const Em3DParams &p, const Em3DBox &in, cudaStream_t s) {
+static int launch_staged_shape(dim3 grid, const Em3DParams &p, const Em3DBox &in, const Em3DMaps &maps,
+                               cudaStream_t s) {
     constexpr size_t bytes = em3d_staged_smem<TY>();
     static bool attr_set = false;   // per template instance; the attribute outlives the handle
     if (!attr_set) {
@@ -274,18 +329,21 @@ static int launch_staged_shape(dim3 grid, const Em3DParams &p, const Em3DBox &in
                                      (int)bytes));
         attr_set = true;
     }
-    em3d_staged_kernel<TY, MINB><<<grid, dim3(EM3D_FZ, TY), bytes, s>>>(p, in);
+    em3d_staged_kernel<TY, MINB><<<grid, dim3(EM3D_FZ, TY), bytes, s>>>(p, in, maps);
     OS_CUDA(cudaGetLastError());
     return OS_OK;
 }
 
-static int launch_staged(int config, dim3 grid, const Em3DParams &p, const Em3DBox &in, cudaStream_t s) {
+static int launch_staged(OsFdtd3D *h, int set, dim3 grid, const Em3DParams &p, const Em3DBox &in, cudaStream_t s) {
+    const int config = h->fused_config;
+    const Em3DMaps *maps = nullptr;
+    OS_TRY(staged_maps(h, set, fused_rows(config), &maps));
     switch (config) {
-        case 0: return launch_staged_shape<16, 1>(grid, p, in, s);
-        case 1: return launch_staged_shape<16, 2>(grid, p, in, s);
-        case 2: return launch_staged_shape<8, 2>(grid, p, in, s);
-        case 3: return launch_staged_shape<8, 3>(grid, p, in, s);
-        default: return launch_staged_shape<8, 4>(grid, p, in, s);
+        case 0: return launch_staged_shape<16, 1>(grid, p, in, *maps, s);
+        case 1: return launch_staged_shape<16, 2>(grid, p, in, *maps, s);
+        case 2: return launch_staged_shape<8, 2>(grid, p, in, *maps, s);
+        case 3: return launch_staged_shape<8, 3>(grid, p, in, *maps, s);
+        default: return launch_staged_shape<8, 4>(grid, p, in, *maps, s);
     }
 }
 
@@ -628,7 +686,7 @@ extern "C" int os_fdtd3d_advance(OsFdtd3D *h, int64_t n_steps, const float *dipo
             point_psi(h, pz, a, b);
             em3d_h_kernel<EM3D_BZ, EM3D_BY><<<box_grid(p), block, 0, h->stream>>>(p);
             em3d_h_kernel<1, 256><<<box_grid(pz, 1, 256), zblock, 0, h->stream>>>(pz);
-            if (staged) OS_TRY(launch_staged(h->fused_config, fused_grid, p, in, h->stream));
+            if (staged) OS_TRY(launch_staged(h, a, fused_grid, p, in, h->stream));
             else OS_TRY(launch_fused(h->fused_config, fused_grid, p, in, h->stream));
             // faces E: E^n and psi of set a, H^{n+1/2} of set b -> E^{n+1}, psi' of set b
             point_sets(h, p, a, b, b, b);

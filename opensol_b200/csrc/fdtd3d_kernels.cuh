@@ -14,6 +14,7 @@
 // non-periodic axis the last row's inverse spacing is 0.  The missing lo H below row 0 of a non-periodic axis is 0.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -624,70 +625,75 @@ __global__ void __launch_bounds__(EM3D_FZ * TY, MINB) em3d_fused_kernel(const Em
 }
 
 // ---------------------------------------------------------------------------------------------------- staged step
-// em3d_fused_kernel with the planes staged in shared memory: each x plane's rows of the block's tile arrive by 1D bulk
-// copies (cp.async.bulk, this GPU's own memory, no multicast) into a ring of EM3D_RING plane slots, EM3D_RING - 2
-// planes ahead of the plane being computed, completing on one mbarrier per slot; the threads read E, H and the
-// material ids from shared memory instead of holding loads in flight.  Per plane and slot: E rows j0 - 1 .. j0 + TY - 1
-// (the j + 1 row of the last warp included) and H rows j0 - 1 .. j0 + TY - 2, 40-float windows from the 16-byte
-// boundary at or before column k0 - 1 (moved left where a window would pass the row end); material ids the same rows
-// as E, 48-entry windows from the 16-byte boundary.  Needs nz a multiple of 8 and at least 48.  Warp 0 (the halo row,
-// which computes no E) issues the copies of plane i + EM3D_RING - 1 into the slot of plane i - 1 after the plane's
-// barrier, when no thread reads that slot any more.  Every wait is bounded (2 s): a block whose wait runs out sets
-// *err, waits (bounded) for its own copies in flight and returns; material ids are clamped below n_ids, so a
-// stale slot never indexes past the tables.  Arithmetic and results: em3d_fused_kernel's, bit for bit.
+// em3d_fused_kernel with the planes staged in shared memory: each x plane of the block's tile arrives by tiled tensor
+// copies (cp.async.bulk.tensor, one per array: the three E boxes of TY + 1 rows, the three H boxes of TY rows, the
+// material-id box of TY + 1 rows; this GPU's own memory, no multicast) into a ring of EM3D_RING plane slots,
+// EM3D_RING - 2 planes ahead of the plane being computed, completing on one mbarrier per slot; the threads read E, H
+// and the material ids from shared memory instead of holding loads in flight.  Boxes start at row j0 - 1 and at the
+// 16-byte boundary at or before column k0 - 1 (moved left where a box would pass the row end): 40 floats or 48 ids
+// wide; rows past the grid are filled with zeros by the copy and read only by threads whose results are discarded.
+// Needs nz a multiple of 8 and at least 48.  Warp 0 (the halo row, which computes no E) issues the copies of plane
+// i + EM3D_RING - 1 into the slot of plane i - 1 after the plane's barrier, when no thread reads that slot any more.
+// Every wait is bounded (2 s): a block whose wait runs out sets *err, waits (bounded) for its own copies in flight and
+// returns; material ids are clamped below n_ids, so a stale slot never indexes past the tables.  Arithmetic and
+// results: em3d_fused_kernel's, bit for bit.
 constexpr int EM3D_RING = 4;
-constexpr int EM3D_WF = 40;   // floats per field row window (160 B)
-constexpr int EM3D_WM = 48;   // ids per material row window (96 B)
+constexpr int EM3D_WF = 40;   // floats per field box row (160 B)
+constexpr int EM3D_WM = 48;   // ids per material box row (96 B)
+
+// Tensor maps of one staged launch: E and H components of the field set read (boxes of TY + 1 and TY rows), ids.
+struct Em3DMaps {
+    CUtensorMap e[3], h[3], m;
+};
+
+__host__ __device__ constexpr int em3d_round128(int bytes) { return (bytes + 127) / 128 * 128; }
 
 template <int TY>
-struct Em3DStage {
-    float e[3][TY + 1][EM3D_WF];
-    float h[3][TY][EM3D_WF];
-    uint16_t m[TY + 1][EM3D_WM];
+struct Em3DStageLayout {   // byte offsets inside one ring slot, every box on a 128-byte boundary
+    static constexpr int e_bytes = em3d_round128((TY + 1) * EM3D_WF * 4);
+    static constexpr int h_bytes = em3d_round128(TY * EM3D_WF * 4);
+    static constexpr int m_bytes = em3d_round128((TY + 1) * EM3D_WM * 2);
+    static constexpr int e_off = 0, h_off = 3 * e_bytes, m_off = h_off + 3 * h_bytes;
+    static constexpr int slot = m_off + m_bytes;
+    static constexpr uint32_t tx = (uint32_t)((TY + 1) * EM3D_WF * 4 * 3 + TY * EM3D_WF * 4 * 3 + (TY + 1) * EM3D_WM * 2);
 };
 
 template <int TY>
 __host__ __device__ constexpr size_t em3d_staged_smem() {
-    return sizeof(Em3DStage<TY>) * EM3D_RING + 2 * 2 * TY * 32 * sizeof(float) + EM3D_RING * sizeof(uint64_t);
+    return (size_t)Em3DStageLayout<TY>::slot * EM3D_RING + 2 * 2 * TY * 32 * sizeof(float) + EM3D_RING * sizeof(uint64_t);
 }
 
+__device__ __forceinline__ void em3d_tensor_g2s(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                                uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(tb_smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(tb_smem_addr(bar))
+        : "memory");
+}
+
+// The seven copies of one plane into one slot (warp 0; lane 0 arms the barrier first).
 template <int TY>
-__device__ __forceinline__ void em3d_issue_plane(const Em3DParams &p, Em3DStage<TY> *st, uint64_t *bar, int plane,
+__device__ __forceinline__ void em3d_issue_plane(const Em3DMaps &maps, unsigned char *slot, uint64_t *bar, int plane,
                                                  int j_row0, int ca, int cam, int lane) {
-    // one copy per row and array: 3 (TY + 1) E rows, 3 TY H rows, TY + 1 id rows
-    constexpr int n_e = 3 * (TY + 1), n_h = 3 * TY, n_m = TY + 1;
-    constexpr uint32_t bytes = (uint32_t)(n_e + n_h) * EM3D_WF * 4 + (uint32_t)n_m * EM3D_WM * 2;
-    if (lane == 0) tb_mbar_expect_tx(bar, bytes);
+    using L = Em3DStageLayout<TY>;
+    if (lane == 0) tb_mbar_expect_tx(bar, L::tx);
     __syncwarp();
-    const size_t sx = (size_t)p.ny * p.nz;
-    for (int q = lane; q < n_e + n_h + n_m; q += 32) {
-        if (q < n_e) {
-            const int c = q / (TY + 1), r = q % (TY + 1);
-            const int row = min(j_row0 + r, p.ny - 1);
-            const float *src = c == 0 ? p.ex : (c == 1 ? p.ey : p.ez);
-            tb_bulk_g2s(st->e[c][r], src + (size_t)plane * sx + (size_t)row * p.nz + ca, EM3D_WF * 4, bar);
-        } else if (q < n_e + n_h) {
-            const int c = (q - n_e) / TY, r = (q - n_e) % TY;
-            const int row = min(j_row0 + r, p.ny - 1);
-            const float *src = c == 0 ? p.hx : (c == 1 ? p.hy : p.hz);
-            tb_bulk_g2s(st->h[c][r], src + (size_t)plane * sx + (size_t)row * p.nz + ca, EM3D_WF * 4, bar);
-        } else {
-            const int r = q - n_e - n_h;
-            const int row = min(j_row0 + r, p.ny - 1);
-            tb_bulk_g2s(st->m[r], p.mat + (size_t)plane * sx + (size_t)row * p.nz + cam, EM3D_WM * 2, bar);
-        }
-    }
+    if (lane < 3) em3d_tensor_g2s(slot + L::e_off + lane * L::e_bytes, &maps.e[lane], ca, j_row0, plane, bar);
+    else if (lane < 6) em3d_tensor_g2s(slot + L::h_off + (lane - 3) * L::h_bytes, &maps.h[lane - 3], ca, j_row0, plane,
+                                       bar);
+    else if (lane == 6) em3d_tensor_g2s(slot + L::m_off, &maps.m, cam, j_row0, plane, bar);
 }
 
 template <int TY, int MINB>
-__global__ void __launch_bounds__(EM3D_FZ * TY, MINB) em3d_staged_kernel(const Em3DParams p, const Em3DBox in) {
+__global__ void __launch_bounds__(EM3D_FZ * TY, MINB)
+    em3d_staged_kernel(const Em3DParams p, const Em3DBox in, const __grid_constant__ Em3DMaps maps) {
+    using L = Em3DStageLayout<TY>;
     extern __shared__ __align__(128) unsigned char em3d_smem[];
-    Em3DStage<TY> *ring = reinterpret_cast<Em3DStage<TY> *>(em3d_smem);
-    float(*s_hz)[TY][EM3D_FZ] = reinterpret_cast<float(*)[TY][EM3D_FZ]>(em3d_smem + sizeof(Em3DStage<TY>) * EM3D_RING);
+    float(*s_hz)[TY][EM3D_FZ] = reinterpret_cast<float(*)[TY][EM3D_FZ]>(em3d_smem + L::slot * EM3D_RING);
     float(*s_hx)[TY][EM3D_FZ] = reinterpret_cast<float(*)[TY][EM3D_FZ]>(
-        em3d_smem + sizeof(Em3DStage<TY>) * EM3D_RING + 2 * TY * EM3D_FZ * sizeof(float));
-    uint64_t *bar = reinterpret_cast<uint64_t *>(em3d_smem + sizeof(Em3DStage<TY>) * EM3D_RING +
-                                                 4 * TY * EM3D_FZ * sizeof(float));
+        em3d_smem + L::slot * EM3D_RING + 2 * TY * EM3D_FZ * sizeof(float));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(em3d_smem + L::slot * EM3D_RING + 4 * TY * EM3D_FZ * sizeof(float));
     const int lane = threadIdx.x, w = threadIdx.y;
     const int k_lo = in.k0 - 1 + (int)blockIdx.x * (EM3D_FZ - 1);   // this tile's first column (the halo)
     const int j_row0 = in.j0 - 1 + (int)blockIdx.y * (TY - 1);      // its first row (the halo)
@@ -712,7 +718,7 @@ __global__ void __launch_bounds__(EM3D_FZ * TY, MINB) em3d_staged_kernel(const E
     __syncthreads();
     if (w == 0)
         for (int q = 0; q < EM3D_RING && base + q <= i_last; ++q)
-            em3d_issue_plane<TY>(p, ring + q, bar + q, base + q, j_row0, ca, cam, lane);
+            em3d_issue_plane<TY>(maps, em3d_smem + q * L::slot, bar + q, base + q, j_row0, ca, cam, lane);
     const int n_issued_max = i_last - base + 1;        // planes base .. i_last are staged
     float *__restrict__ oex = p.oex;
     float *__restrict__ oey = p.oey;
@@ -731,15 +737,23 @@ __global__ void __launch_bounds__(EM3D_FZ * TY, MINB) em3d_staged_kernel(const E
     int par = 0;
     for (int i = base; i < i_last; ++i) {
         const int q = i - base;
-        const Em3DStage<TY> &cur = ring[q % EM3D_RING];
-        const Em3DStage<TY> &nxt = ring[(q + 1) % EM3D_RING];
+        const unsigned char *cur = em3d_smem + (q % EM3D_RING) * L::slot;
+        const unsigned char *nxt = em3d_smem + ((q + 1) % EM3D_RING) * L::slot;
         ok = tb_mbar_wait(bar + (q + 1) % EM3D_RING, (uint32_t)(((q + 1) / EM3D_RING) & 1)) && ok;
-        const float ex0 = cur.e[0][r][c0], ey0 = cur.e[1][r][c0], ez0 = cur.e[2][r][c0];
-        const float exy = cur.e[0][r + 1][c0], ezy = cur.e[2][r + 1][c0];
-        const float exz = cur.e[0][r][c0 + 1], eyz = cur.e[1][r][c0 + 1];
-        const float eyn = nxt.e[1][r][c0], ezn = nxt.e[2][r][c0];
-        const float hx0 = cur.h[0][r][c0], hy0 = cur.h[1][r][c0], hz0 = cur.h[2][r][c0];
-        const uint16_t m0 = min(cur.m[r][m_c], id_max);
+        const float *ce0 = reinterpret_cast<const float *>(cur + L::e_off);
+        const float *ce1 = reinterpret_cast<const float *>(cur + L::e_off + L::e_bytes);
+        const float *ce2 = reinterpret_cast<const float *>(cur + L::e_off + 2 * L::e_bytes);
+        const float *ch = reinterpret_cast<const float *>(cur + L::h_off);
+        const uint16_t *cm = reinterpret_cast<const uint16_t *>(cur + L::m_off);
+        const int at = r * EM3D_WF + c0, below = at + EM3D_WF;   // (row r, col c0) and the row after it
+        const float ex0 = ce0[at], ey0 = ce1[at], ez0 = ce2[at];
+        const float exy = ce0[below], ezy = ce2[below];
+        const float exz = ce0[at + 1], eyz = ce1[at + 1];
+        const float eyn = reinterpret_cast<const float *>(nxt + L::e_off + L::e_bytes)[at];
+        const float ezn = reinterpret_cast<const float *>(nxt + L::e_off + 2 * L::e_bytes)[at];
+        const float hx0 = ch[at], hy0 = ch[L::h_bytes / 4 + at], hz0 = ch[2 * (L::h_bytes / 4) + at];
+        const int m_at = r * EM3D_WM + m_c;
+        const uint16_t m0 = min(cm[m_at], id_max);
         const bool inside = i >= i_first;
         const bool store = emit && inside;
         float da, db;
@@ -812,17 +826,17 @@ __global__ void __launch_bounds__(EM3D_FZ * TY, MINB) em3d_staged_kernel(const E
         // no thread reads the slot of plane i - 1 any more: it takes plane i + EM3D_RING - 1
         if (w == 0 && q >= 1 && i + EM3D_RING - 1 <= i_last) {
             tb_fence_proxy_async();
-            em3d_issue_plane<TY>(p, ring + (q - 1) % EM3D_RING, bar + (q - 1) % EM3D_RING, i + EM3D_RING - 1, j_row0,
-                                 ca, cam, lane);
+            em3d_issue_plane<TY>(maps, em3d_smem + ((q - 1) % EM3D_RING) * L::slot, bar + (q - 1) % EM3D_RING,
+                                 i + EM3D_RING - 1, j_row0, ca, cam, lane);
         }
         if (e_thread && inside) {
             const float hz_y = s_hz[par][w - 1][lane];
             const float hx_y = s_hx[par][w - 1][lane];
             const float dhz_y = vhz - hz_y, dhy_z = vhy - hy_z, dhx_z = vhx - hx_z;
             const float dhz_x = vhz - hz_m, dhy_x = vhy - hy_m, dhx_y = vhx - hx_y;
-            const uint16_t mx = min(nxt.m[r][m_c], id_max);
-            const uint16_t my = min(cur.m[r + 1][m_c], id_max);
-            const uint16_t mz = min(cur.m[r][m_c + 1], id_max);
+            const uint16_t mx = min(reinterpret_cast<const uint16_t *>(nxt + L::m_off)[m_at], id_max);
+            const uint16_t my = min(cm[m_at + EM3D_WM], id_max);
+            const uint16_t mz = min(cm[m_at + 1], id_max);
             float ca_, cbx, cby, cbz;
             const float iex = p.iex[i];
             em3d_face_fast(p, 0, p.t_ex, m0, mx, p.wlx[i], p.wux[i], ca_, cbx);
