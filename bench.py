@@ -61,6 +61,10 @@ def parse_args():
                         'em3d: the 512^3 3D run; serving: the batched job stream against one-at-a-time runs; '
                         'adjoint: gradient cost against one forward run')
     p.add_argument('--jobs', type=int, default=64, help='serving: jobs of the request stream')
+    p.add_argument('--form3d', type=int, default=0, choices=[0, 1, 2],
+                   help='em3d: step form (0 two in-place kernels, 1 fused on two field sets, 2 fused with staged '
+                        'planes); results are the same bits')
+    p.add_argument('--fused-config', type=int, default=3, help='em3d: launch shape of the fused forms (0..4)')
     return p.parse_args()
 
 
@@ -489,6 +493,8 @@ def run_em3d(args):
                                                  device=local)
     physics.finalize()
     engine = physics.engine
+    engine.set_variant(args.form3d)
+    engine.set_fused_config(args.fused_config)
     # a stream of its own (torch's default stream is handle 0, which os_fdtd*_set_stream reads as "the engine's own
     # stream"): the engine launches on it and the timing events are recorded on it
     stream = torch.cuda.Stream()
@@ -518,7 +524,8 @@ def run_em3d(args):
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
             'config': {'workload': f'em3d: {engine.nx}^3 total grid incl. 12 CPML cells/face, dx 20 nm, 500 seeded '
                                    'spheres eps_r U(2,12), z dipole 1310 nm at the centre, 8-frequency flux box, '
-                                   f'{steps} Yee steps per bench step', 'l2': 'fields 6 x 537 MB, no flush'},
+                                   f'{steps} Yee steps per bench step', 'l2': 'fields 6 x 537 MB, no flush',
+                       'step_form': args.form3d, 'fused_config': args.fused_config},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
                          'traffic': None, 'peak_source': f'{peak_kind} hbm_gbs', 'bytes_per_cell_update': 52,
                          'kernel': 'em3d_h_kernel + em3d_e_kernel (whole step)'},
