@@ -670,7 +670,9 @@ def secondary_workloads(args):
     import copy
     import torch
     out = {}
-    plans = [('hz2d', run_hz2d, {'steps': 2, 'warmup': 1, 'sim_steps': SIM_STEPS, 'no_cpu_baseline': True}),
+    # tile_rows 0: each engine picks its own (the headline run stored the E_z autotuner's choice in args)
+    plans = [('hz2d', run_hz2d, {'steps': 2, 'warmup': 1, 'sim_steps': SIM_STEPS, 'no_cpu_baseline': True,
+                                 'tile_rows': 0}),
              ('em3d', run_em3d, {'steps': 1, 'warmup': 1, 'sim_steps': SIM_STEPS}),
              ('adjoint', run_adjoint, {'steps': 3, 'warmup': 1}),
              ('serving', run_serving, {'jobs': 32})]
