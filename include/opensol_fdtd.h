@@ -242,6 +242,13 @@ int os_fdtd2d_advance_noalloc(OsFdtd2D *h, int64_t n_steps, const float *line_va
  * Every choice gives bit-identical results.  No open_sol counterpart (open_sol launches per half step). */
 int os_fdtd2d_configure(OsFdtd2D *h, int32_t variant, int32_t steps_per_launch, int32_t tile_rows);
 
+/* Test hook of the bounded waits, no open_sol counterpart (0, the default: off).  With wait_ns > 0 the next blocked
+ * advances make one warp of the interior kernel wait on an mbarrier that nothing completes, for at most wait_ns
+ * nanoseconds (<= 2 s), and give up as a real wait does: the handle's error flag is set, that warp's tile is not
+ * written, and the next synchronising call returns OS_ERR_CUDA (the flag cleared).  The context stays usable: reset
+ * and advance again. */
+int os_fdtd2d_set_stall_probe(OsFdtd2D *h, int64_t wait_ns);
+
 /* Kernels the last os_fdtd2d_advance launched. */
 int os_fdtd2d_launch_count(OsFdtd2D *h, int64_t *launches);
 

@@ -104,6 +104,7 @@ SIGNATURES = {
     'os_fdtd2d_adjoint_reset': [_P],
     'os_fdtd2d_adjoint_segment': [_P, _I32, _I64, _I32, _F, _I32, _I32, ctypes.POINTER(_I32), _F, _F],
     'os_fdtd2d_adjoint_gradient': [_P, _D],
+    'os_fdtd2d_set_stall_probe': [_P, _I64],
     'os_fdtd3d_create': [ctypes.POINTER(OsGrid3D), ctypes.POINTER(_P)],
     'os_fdtd3d_destroy': [_P],
     'os_fdtd3d_set_rows': [_P, _F, _F, _F, _F, _F, _F, _F],

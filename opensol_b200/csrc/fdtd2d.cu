@@ -2764,11 +2764,10 @@ extern "C" int os_fdtd2d_adjoint_segment(OsAdjoint2D *a, int32_t slot, int64_t s
                         (unsigned)((h->grid.nx + block.y - 1) / block.y));
         float *rec = a->rec[rb].ptr;
         ez2d_record_box_kernel<<<box_blocks, 256, 0, s>>>(p.ez, h->grid.ny, a->bi0, a->bi1, a->bj0, a->bj1, rec);
-        for (int32_t k = 0; k < steps; ++k) {
+        for (int32_t k = 0; k < steps; ++k) {   // the E kernel records the box of its own step
             ez2d_h_kernel<<<grid, block, 0, s>>>(p);
-            ez2d_e_kernel<<<grid, block, 0, s>>>(p, a->values.ptr, steps, k);
-            ez2d_record_box_kernel<<<box_blocks, 256, 0, s>>>(p.ez, h->grid.ny, a->bi0, a->bi1, a->bj0, a->bj1,
-                                                              rec + (size_t)(k + 1) * box);
+            ez2d_e_kernel<<<grid, block, 0, s>>>(p, a->values.ptr, steps, k, rec + (size_t)(k + 1) * box, a->bi0,
+                                                 a->bi1, a->bj0, a->bj1);
         }
         return OS_OK;
     };

@@ -92,8 +92,11 @@ __global__ void __launch_bounds__(EZ2D_BLOCK_X *EZ2D_BLOCK_Y) ez2d_h_kernel(cons
 // E half step of cell (i, j): fdtd_ez_2d_kernels.py:103-120, then the E-row CPML x sides (ez += cb psi) and y sides
 // (ez += (-cb) psi) (boundaries.py:757-760), then the soft line sources in add order (core/sources.py:221-229: skipped
 // when the step's float32 value is 0, else ez += value * profile).
+// rec (optional): the new E_z of the cells of box [bi0, bi1) x [bj0, bj1) is also written to rec, row by row (the
+// adjoint's recomputation records the design box this way, in the step's own launch).
 __global__ void __launch_bounds__(EZ2D_BLOCK_X *EZ2D_BLOCK_Y)
-    ez2d_e_kernel(const Ez2DParams p, const float *__restrict__ line_values, int64_t n_steps, int64_t k_step) {
+    ez2d_e_kernel(const Ez2DParams p, const float *__restrict__ line_values, int64_t n_steps, int64_t k_step,
+                  float *__restrict__ rec = nullptr, int bi0 = 0, int bi1 = 0, int bj0 = 0, int bj1 = 0) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= p.nx || j >= p.ny) return;
@@ -160,6 +163,7 @@ __global__ void __launch_bounds__(EZ2D_BLOCK_X *EZ2D_BLOCK_Y)
         }
     }
     p.ez[idx] = v;
+    if (rec && i >= bi0 && i < bi1 && j >= bj0 && j < bj1) rec[(size_t)(i - bi0) * (bj1 - bj0) + (j - bj0)] = v;
 }
 
 // Line DFT of a flux monitor at one sample (physics/em/monitors.py:45-46,84-90): acc[f, c] += complex128(phase_f) *

@@ -261,6 +261,11 @@ class FDTDEngine2D_Ez:
     def set_profiling(self, on):
         _native.check(_native.load().os_fdtd2d_set_profiling(self.handle, int(bool(on))))
 
+    def set_stall_probe(self, wait_ns):
+        """Test hook of the bounded waits (0: off): one warp of the next blocked advances waits on a barrier nothing
+        completes, at most wait_ns ns, and gives up; the next synchronising call raises RuntimeError."""
+        _native.check(_native.load().os_fdtd2d_set_stall_probe(self.handle, int(wait_ns)))
+
     def kernel_times(self):
         """{kernel kind name: (total device ms, launches)} of the last advance (profiling on)."""
         out = {}
