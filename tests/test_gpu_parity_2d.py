@@ -319,3 +319,35 @@ def test_roofline_workload_deterministic():
     np.testing.assert_array_equal(out[0][1], out[1][1])
     for f1, f2 in zip(out[0][2], out[1][2]):
         np.testing.assert_array_equal(f1, f2)
+
+
+FP64_FLUX_RTOL = 1e-5   # float32 run against the float64 oracle run, relative to each monitor's peak flux
+
+
+def test_roofline_workload_full_run_against_fixture():
+    """The whole 10,000-step 8192^2 benchmark run against tests/golden/c2_full.npz (open_sol's own float32 run and
+    the oracle's, which agree byte for byte; tests/golden/make_golden_c2_full.py): E_z, H_x, H_y and every monitor's
+    complex128 E / H spectra bit-identical (SHA-256) at steps 600 and 10,000, the four 16-frequency fluxes equal.  The
+    error of those float32 fluxes against the float64 oracle run is stated and held to FP64_FLUX_RTOL."""
+    g = np.load(os.path.join(GOLDEN, 'c2_full.npz'))
+    sim = ob.Simulation(**workloads.roofline_2d_sim_args(), verbose=False)
+    mons = workloads.apply(sim, workloads.roofline_2d_ops())
+    done = 0
+    for cp in (600, 10_000):
+        sim.run(n_steps=cp - done, verbose=False, print_every=0)
+        done = cp
+        for name, arr in _fields(sim).items():
+            assert _digest(arr) == str(g[f'sha_{name}_{cp}']), f'{name} at step {cp}'
+        for k, mon in enumerate(mons):
+            e, h = mon.spectra()
+            assert _digest(e) == str(g[f'sha_spec_e{k}_{cp}']), f'E spectra of monitor {k} at step {cp}'
+            assert _digest(h) == str(g[f'sha_spec_h{k}_{cp}']), f'H spectra of monitor {k} at step {cp}'
+            np.testing.assert_array_equal(mon.flux(), g[f'flux{k}_{cp}'])
+    assert int(g['sample_interval']) == mons[0].sample_interval
+    errors = []
+    for k, mon in enumerate(mons):
+        f64 = g[f'f64_flux{k}_10000']
+        errors.append(float(np.abs(mon.flux() - f64).max() / np.abs(f64).max()))
+    print(f'float32 vs float64 flux error per monitor (relative to its peak): {errors}')
+    assert max(errors) <= FP64_FLUX_RTOL
+    sim.clear()
