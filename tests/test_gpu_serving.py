@@ -56,3 +56,20 @@ def test_batched_fields_equal_single_advance():
             np.testing.assert_array_equal(sim.em.engine.read_field(name), ref.em.engine.read_field(name))
         assert sim.em.engine.n_step == ref.em.engine.n_step == 131
     batch.close()
+
+
+def test_mix_equals_alone_at_stream_sizes():
+    """Ten jobs of the serving stream's own kind at sizes 256-1024 cells a side (+30 CPML cells: row lengths that are
+    not multiples of 4 included), 600-1500 steps, served together with at most 6 active at once and 256-step ticks
+    (jobs join and leave mid-run): every job's fluxes bit-identical to its run alone."""
+    specs = serving.make_job_specs(n_jobs=10, rate=0.0, seed=11, side_range=(256, 1024), steps_range=(600, 1500))
+    assert any((s.side + 2 * s.npml) % 4 for s in specs)
+    loop = serving.ServingLoop(max_active=6, chunk_steps=256)
+    results = {r.job_id: r for r in loop.run(specs, realtime=False)}
+    loop.close()
+    assert sorted(results) == [s.job_id for s in specs]
+    assert loop.peak_active == 6
+    for spec in specs:
+        alone, _ = serving.run_alone(spec)
+        for mine, ref in zip(results[spec.job_id].fluxes, alone):
+            np.testing.assert_array_equal(mine, ref)
