@@ -61,10 +61,11 @@ def parse_args():
                         'em3d: the 512^3 3D run; serving: the batched job stream against one-at-a-time runs; '
                         'adjoint: gradient cost against one forward run')
     p.add_argument('--jobs', type=int, default=64, help='serving: jobs of the request stream')
-    p.add_argument('--form3d', type=int, default=0, choices=[0, 1, 2],
+    p.add_argument('--form3d', type=int, default=3, choices=[0, 1, 2, 3],
                    help='em3d: step form (0 two in-place kernels, 1 fused on two field sets, 2 fused with staged '
-                        'planes); results are the same bits')
-    p.add_argument('--fused-config', type=int, default=3, help='em3d: launch shape of the fused forms (0..4)')
+                        'planes, 3 lean staged fused pass); results are the same bits')
+    p.add_argument('--fused-config', type=int, default=-1,
+                   help="em3d: launch shape of the fused forms (0..4; -1: the form's default)")
     return p.parse_args()
 
 

@@ -412,15 +412,17 @@ int os_fdtd3d_set_stream(OsFdtd3D *h, void *cuda_stream);
 /* x planes each block of the H / E kernels streams (chosen from the grid at create; results do not depend on it). */
 int os_fdtd3d_set_x_chunk(OsFdtd3D *h, int32_t planes);
 
-/* Step form (results bit-identical; no counterpart in open_sol, which has one form): 0 (the default) = the H and
- * the E kernel over the whole grid in place; 1 = one fused H + E kernel over every cell but the outermost layer of
- * each axis plus the two-kernel update of that layer, on two field sets and two CPML psi sets swapped every step
- * (twice the field memory, a third less DRAM traffic per step); 2 = form 1 with each x plane of a tile staged in shared
- * memory by 1D bulk copies (rows of a multiple of 8 cells, at least 48; other grids run form 1). */
+/* Step form (results bit-identical; no counterpart in open_sol, which has one form): 0 = the H and the E kernel over
+ * the whole grid in place; 1 = one fused H + E kernel over every cell but the outermost layer of each axis plus the
+ * two-kernel update of that layer, on two field sets and two CPML psi sets swapped every step (twice the field memory,
+ * a third less DRAM traffic per step); 2 = form 1 with each x plane of a tile staged in shared memory by tensor copies
+ * (rows of a multiple of 8 cells, at least 48; other grids run form 1); 3 (the default) = form 1 with the lean staged
+ * kernel (four cells a thread; z rows of a multiple of 4 cells and at least 144, y at least 17, at most 255 z CPML
+ * rows; other grids run form 0). */
 int os_fdtd3d_set_variant(OsFdtd3D *h, int32_t variant);
 
-/* Launch shape of the fused kernel, 0..4 (tile rows 16 or 8 and the blocks per SM its registers are cut for; 3 by
- * default); speed only, results bit-identical. */
+/* Launch shape of the fused kernel of forms 1-3, -1..4 (tile rows and the blocks per SM its registers are cut for;
+ * -1: the form's default); speed only, results bit-identical. */
 int os_fdtd3d_set_fused_config(OsFdtd3D *h, int32_t config);
 
 /* The fused box (i0, i1, j0, j1, k0, k1) and whether the next advance uses it (*fused = 1). */

@@ -2,21 +2,24 @@
 // physics/em3d/engine3d.py:157-554, for a Cartesian grid with one real field set and float32 fields).
 //
 // One Yee step follows the reference's own order (engine3d.py:497-554): H with its CPML, then E with its CPML and the
-// dipole injection; on DFT sample steps em3d_flux_kernel accumulates every flux pair.  Two forms, bit-identical:
-//   variant 1: two field sets and two CPML psi sets, read one, write the other, swapped after every step.
-//     em3d_fused_kernel does H and E of every cell but the outermost layer of each axis in one pass (each field and
-//     psi read and written once); that layer (where samples cross the grid edge) runs em3d_h_kernel over its six
-//     faces, then em3d_e_kernel, which reads the new H of both parts;
-//   variant 0 (default): em3d_h_kernel then em3d_e_kernel over the whole grid, in place on one field set.
+// dipole injection; on DFT sample steps em3d_flux_kernel accumulates every flux pair.  Four forms, bit-identical:
+//   variant 3 (default): two field sets and two CPML psi sets, read one, write the other, swapped after every step;
+//     em3d_lean_kernel (fdtd3d_lean.cuh) does H and E of every cell but the outermost x and y layers (and the z faces
+//     too on an open z axis) in one pass over tensor-copy-staged planes, four cells a thread; the outer layers run
+//     em3d_h_kernel, then em3d_e_kernel, per face in block shapes of their own; em3d_dipole_kernel adds the dipoles.
+//     Rows of a multiple of 4 cells, at least 144; other grids run variant 0;
+//   variant 0: em3d_h_kernel then em3d_e_kernel over the whole grid, in place on one field set;
+//   variant 1: variant 3's schedule with em3d_fused_kernel, one cell a thread (every cell but the outermost layer of
+//     each axis), the faces by the face kernels;
 //   variant 2: variant 1 with each x plane of a tile staged in shared memory by tiled tensor copies
 //     (em3d_staged_kernel).
-// Variant 1 moves 52.8 B per cell-update against variant 0's 79.5 (ncu, 256^3) but issues from fewer resident warps
-// (one barrier per plane, 80 registers a thread): on 512^3 it runs 42.7 G cell-updates/s against 48.6; variant 2 runs
-// 48.4 (issue- and barrier-bound once the loads are staged).
+// On 512^3: variant 3 65.3 G cell-updates/s (52 B of algorithmic traffic a cell-update: 0.52 of the measured copy
+// bandwidth), variant 0 48.3 (two kernels re-reading the fields, ~76 B), variant 1 42.7, variant 2 46.4.
 // A chunk of n steps is enqueued with no host synchronisation: per-step dipole amplitudes and per-sample DFT phases
 // arrive as small tables computed on the host in float64 and rounded as open_sol rounds them.
 #include "common.cuh"
 #include "fdtd3d_kernels.cuh"
+#include "fdtd3d_lean.cuh"
 
 #include <algorithm>
 #include <memory>
@@ -31,8 +34,8 @@ struct OsFdtd3D {
     os::DeviceArray<float> field[6];            // ex, ey, ez, hx, hy, hz
     os::DeviceArray<float> field2[6];           // the second field set of variant 1 (allocated on first use)
     int cur = 0;                                // the set holding the current state (0: field, 1: field2)
-    int32_t variant = 0;                        // on 512^3: 48.6 G cell-updates/s, variant 1 42.7, variant 2 48.4
-    int32_t fused_config = 3;                   // tile rows / blocks per SM of em3d_fused_kernel (speed only)
+    int32_t variant = 3;                        // on 512^3: 65.3 G cell-updates/s; variant 0 48.3, 1 42.7, 2 46.4
+    int32_t fused_config = -1;                  // launch shape of the fused form's kernel (speed only; -1: default)
     os::DeviceArray<uint16_t> mat;
     os::DeviceArray<float> tables;              // t_ex, t_ey, t_ez, t_sig, t_da, t_db (6 * n_ids)
     os::DeviceArray<float> same;                // same-id face ca, cb per component (6 * n_ids)
@@ -71,6 +74,9 @@ struct OsFdtd3D {
     os::DeviceArray<int32_t> err;               // set by a staged kernel whose bounded wait ran out
     Em3DMaps maps[2][2];                        // staged form: tensor maps per field set read and tile height (8, 16)
     bool maps_ok[2][2] = {{false, false}, {false, false}};
+    Em3DLeanMaps lean_maps[2][3];               // lean form: per field set read and tile height (4, 8, 16)
+    bool lean_maps_ok[2][3] = {{false, false, false}, {false, false, false}};
+    bool ca_one = true;                         // every face's ca is 1 (no conductivity, no perfect conductor)
 };
 
 namespace os {
@@ -202,14 +208,35 @@ static Em3DBox fused_box(const OsFdtd3D *h) {
     return Em3DBox{1, g.nx - 1, 1, g.ny - 1, 1, g.nz - 1};
 }
 
+// variant 3's lean kernel: rows of a multiple of 4 cells (16-byte vectors), boxes no larger than the grid (the id box
+// is 144 cells wide, the tallest 17 rows), z CPML rows that fit one byte.
+static bool lean_ok(const OsFdtd3D *h) {
+    return h->grid.nz % 4 == 0 && h->grid.nz >= Em3DLeanLayout<16>::WM && h->grid.ny >= 17 &&
+           h->cpml[2].nr <= EM3D_LEAN_MAX_ZROWS;
+}
+
+// The step runs on two field sets (variants 1, 2; variant 3 where its kernel applies, else the in-place form).
 static bool fused_active(const OsFdtd3D *h) {
     const OsGrid3D &g = h->grid;
-    return h->variant >= 1 && g.nx >= 3 && g.ny >= 3 && g.nz >= 3;
+    const bool form = h->variant == 1 || h->variant == 2 || (h->variant == 3 && lean_ok(h));
+    return form && g.nx >= 3 && g.ny >= 3 && g.nz >= 3;
 }
 
 // variant 2 stages the planes by bulk copies: rows must start on 16-byte boundaries and hold the 48-id window.
 static bool staged_active(const OsFdtd3D *h) {
     return fused_active(h) && h->variant == 2 && h->grid.nz % 8 == 0 && h->grid.nz >= EM3D_WM;
+}
+
+static bool lean_active(const OsFdtd3D *h) { return h->variant == 3 && fused_active(h); }
+
+// The lean kernel's box: the fused box, and along a non-periodic z axis rows 0 and nz - 1 too (the z faces).
+static Em3DBox lean_box(const OsFdtd3D *h) {
+    Em3DBox b = fused_box(h);
+    if (!h->grid.periodic[2]) {
+        b.k0 = 0;
+        b.k1 = h->grid.nz;
+    }
+    return b;
 }
 
 // A bounded wait of a staged kernel ran out: report it once (the flag is cleared) as OS_ERR_CUDA.
@@ -226,24 +253,41 @@ static int check_err3(OsFdtd3D *h) {
     return OS_OK;
 }
 
-// The outermost layer around the fused box: the x and y faces (coalesced along k: 32 x 8 blocks) or the z faces
-// (one k per face: blocks of 256 threads along j).
-static void face_boxes(const OsFdtd3D *h, Em3DParams &p, bool z_faces) {
+// The outermost layer around the fused box, in three launches of their own block shapes, each block streaming one x
+// plane (a face holds one or two cells across, so short chunks give the launch its threads): 0 = the x faces (32 x 8
+// blocks along k and j), 1 = the y faces (rows of 128 along k), 2 = the z faces (256 along j: one k per face).
+enum { FACES_X = 0, FACES_Y = 1, FACES_Z = 2 };
+static void face_boxes(const OsFdtd3D *h, Em3DParams &p, int which) {
     const OsGrid3D &g = h->grid;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const Em3DBox xy[4] = {{0, 1, 0, ny, 0, nz}, {nx - 1, nx, 0, ny, 0, nz},
-                           {1, nx - 1, 0, 1, 0, nz}, {1, nx - 1, ny - 1, ny, 0, nz}};
+    const Em3DBox xf[2] = {{0, 1, 0, ny, 0, nz}, {nx - 1, nx, 0, ny, 0, nz}};
+    const Em3DBox yf[2] = {{1, nx - 1, 0, 1, 0, nz}, {1, nx - 1, ny - 1, ny, 0, nz}};
     const Em3DBox zf[2] = {{1, nx - 1, 1, ny - 1, 0, 1}, {1, nx - 1, 1, ny - 1, nz - 1, nz}};
-    const Em3DBox *all = z_faces ? zf : xy;
-    const int n = z_faces ? 2 : 4;
+    const Em3DBox *all = which == FACES_X ? xf : (which == FACES_Y ? yf : zf);
+    p.x_chunk = 1;
     p.n_boxes = 0;
     p.zbase[0] = 0;
-    for (int q = 0; q < n; ++q) {
+    for (int q = 0; q < 2; ++q) {
         const Em3DBox &b = all[q];
         p.boxes[p.n_boxes] = b;
         p.zbase[p.n_boxes + 1] = p.zbase[p.n_boxes] + box_chunks(b, p.x_chunk);
         ++p.n_boxes;
     }
+}
+
+// H (e = false) or E (e = true) of the face launches (the z faces unless the interior kernel covers them); returns
+// the number of launches.
+static int launch_faces(const OsFdtd3D *h, const Em3DParams (&f)[3], bool e, bool z_faces) {
+    if (e) {
+        em3d_e_kernel<32, 8><<<box_grid(f[0], 32, 8), dim3(32, 8), 0, h->stream>>>(f[0]);
+        em3d_e_kernel<128, 1><<<box_grid(f[1], 128, 1), dim3(128, 1), 0, h->stream>>>(f[1]);
+        if (z_faces) em3d_e_kernel<1, 256><<<box_grid(f[2], 1, 256), dim3(1, 256), 0, h->stream>>>(f[2]);
+    } else {
+        em3d_h_kernel<32, 8><<<box_grid(f[0], 32, 8), dim3(32, 8), 0, h->stream>>>(f[0]);
+        em3d_h_kernel<128, 1><<<box_grid(f[1], 128, 1), dim3(128, 1), 0, h->stream>>>(f[1]);
+        if (z_faces) em3d_h_kernel<1, 256><<<box_grid(f[2], 1, 256), dim3(1, 256), 0, h->stream>>>(f[2]);
+    }
+    return z_faces ? 3 : 2;
 }
 
 // Point the psi of p's CPML axes: read set `in`, write set `out`.
@@ -267,6 +311,7 @@ static void point_psi(const OsFdtd3D *h, Em3DParams &p, int in, int out) {
 // em3d_fused_kernel configurations: (tile rows, blocks per SM the register budget is cut for).
 constexpr int FUSED_CONFIGS = 5;
 static int fused_rows(int config) { return config == 0 || config == 1 ? 16 : 8; }
+static int fused_cfg(const OsFdtd3D *h) { return h->fused_config < 0 ? 3 : h->fused_config; }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (the library does not link libcuda itself).
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -319,6 +364,66 @@ static int staged_maps(OsFdtd3D *h, int set, int ty, const Em3DMaps **out) {
     return OS_OK;
 }
 
+// em3d_lean_kernel configurations: (tile rows, ring slots, blocks per SM).
+constexpr int LEAN_CONFIGS = 4;
+static int lean_rows(int config) { return config == 0 ? 16 : 8; }
+static int lean_ty_index(int ty) { return ty == 4 ? 0 : (ty == 8 ? 1 : 2); }
+
+// The lean launch's maps for field set `set` and tile height ty (made once per handle).
+static int lean_maps(OsFdtd3D *h, int set, int ty, const Em3DLeanMaps **out) {
+    const int t = lean_ty_index(ty);
+    if (!h->lean_maps_ok[set][t]) {
+        using L = Em3DLeanLayout<8>;
+        Em3DLeanMaps &m = h->lean_maps[set][t];
+        for (int c = 0; c < 3; ++c) {
+            OS_TRY(encode_box(&m.e[c], fset(h, set, c), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->grid, L::WE, ty + 1));
+            OS_TRY(encode_box(&m.h[c], fset(h, set, 3 + c), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->grid, L::WH, ty));
+        }
+        OS_TRY(encode_box(&m.m, h->mat.ptr, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, h->grid, L::WM, ty + 1));
+        h->lean_maps_ok[set][t] = true;
+    }
+    *out = &h->lean_maps[set][t];
+    return OS_OK;
+}
+
+template <int TY, int RING, int MINB, bool CA1>
+static int launch_lean_shape(const Em3DParams &p, const Em3DBox &in, const Em3DLeanMaps &maps, cudaStream_t s) {
+    static bool attr_set = false;   // per template instance; the attribute outlives the handle
+    if (!attr_set) {
+        OS_CUDA(cudaFuncSetAttribute(em3d_lean_kernel<TY, RING, MINB, CA1>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)em3d_lean_smem<TY, RING>(EM3D_LEAN_MAX_ZROWS)));
+        attr_set = true;
+    }
+    const dim3 grid((unsigned)((in.k1 - (in.k0 & ~3) + EM3D_LTILE - 1) / EM3D_LTILE),
+                    (unsigned)((in.j1 - in.j0 + TY - 2) / (TY - 1)),
+                    (unsigned)((in.i1 - in.i0 + p.x_chunk - 1) / p.x_chunk));
+    em3d_lean_kernel<TY, RING, MINB, CA1>
+        <<<grid, dim3(32, TY), em3d_lean_smem<TY, RING>(p.cpml[2].nr), s>>>(p, in, maps);
+    OS_CUDA(cudaGetLastError());
+    return OS_OK;
+}
+
+template <bool CA1>
+static int launch_lean_ca(int config, const Em3DParams &p, const Em3DBox &in, const Em3DLeanMaps &maps,
+                          cudaStream_t s) {
+    switch (config) {
+        case 0: return launch_lean_shape<16, 3, 1, CA1>(p, in, maps, s);
+        case 1: return launch_lean_shape<8, 3, 2, CA1>(p, in, maps, s);
+        case 2: return launch_lean_shape<8, 4, 1, CA1>(p, in, maps, s);
+        default: return launch_lean_shape<8, 3, 1, CA1>(p, in, maps, s);
+    }
+}
+
+// The lean kernel streams chunks of at most EM3D_LEAN_MAX_PLANES - 1 planes (its per-plane table).
+static int launch_lean(OsFdtd3D *h, int set, Em3DParams p, const Em3DBox &in, cudaStream_t s) {
+    const int config = h->fused_config < 0 ? 1 : h->fused_config % LEAN_CONFIGS;
+    const Em3DLeanMaps *maps = nullptr;
+    OS_TRY(lean_maps(h, set, lean_rows(config), &maps));
+    p.x_chunk = std::min<int32_t>(p.x_chunk, EM3D_LEAN_MAX_PLANES - 1);
+    return h->ca_one ? launch_lean_ca<true>(config, p, in, *maps, s) : launch_lean_ca<false>(config, p, in, *maps, s);
+}
+
 template <int TY, int MINB>
 static int launch_staged_shape(dim3 grid, const Em3DParams &p, const Em3DBox &in, const Em3DMaps &maps,
                                cudaStream_t s) {
@@ -335,7 +440,7 @@ static int launch_staged_shape(dim3 grid, const Em3DParams &p, const Em3DBox &in
 }
 
 static int launch_staged(OsFdtd3D *h, int set, dim3 grid, const Em3DParams &p, const Em3DBox &in, cudaStream_t s) {
-    const int config = h->fused_config;
+    const int config = fused_cfg(h);
     const Em3DMaps *maps = nullptr;
     OS_TRY(staged_maps(h, set, fused_rows(config), &maps));
     switch (config) {
@@ -487,6 +592,9 @@ extern "C" int os_fdtd3d_set_materials(OsFdtd3D *h, const uint16_t *material_id,
     h->e_lossless = true;
     for (int32_t m = 0; m < n_ids; ++m)
         if (t_sig[m] != 0.0f) h->e_lossless = false;
+    h->ca_one = h->e_lossless;   // a face between two perfect conductors has ca = 0
+    for (int32_t m = 0; m < n_ids; ++m)
+        if (t_ex[m] < 0.0f || t_ey[m] < 0.0f || t_ez[m] < 0.0f) h->ca_one = false;
     OS_TRY(h->same.alloc(6 * (size_t)n_ids));
     Em3DParams q = make_params3(h);
     em3d_same_tables_kernel<<<(n_ids + 255) / 256, 256, 0, h->stream>>>(q, h->same.ptr);
@@ -652,7 +760,7 @@ extern "C" int os_fdtd3d_advance(OsFdtd3D *h, int64_t n_steps, const float *dipo
         OS_TRY(upload(h->pairs_dev, h->pairs.data(), h->pairs.size(), h->stream));
         h->pairs_dirty = false;
     }
-    const bool fused = fused_active(h), staged = staged_active(h);
+    const bool fused = fused_active(h), staged = staged_active(h), lean = lean_active(h);
     if (fused) {
         for (auto &f : h->field2)
             if (!f.ptr) OS_TRY(f.alloc(cells3(h)));
@@ -662,38 +770,44 @@ extern "C" int os_fdtd3d_advance(OsFdtd3D *h, int64_t n_steps, const float *dipo
     Em3DParams p = make_params3(h);
     p.dip_values = h->values.ptr;
     p.values_stride = n_steps;
-    Em3DParams pz = p;   // the z faces
-    if (fused) {
-        face_boxes(h, p, false);
-        face_boxes(h, pz, true);
-    }
-    const Em3DBox in = fused_box(h);
-    const int ty = fused_rows(h->fused_config);
-    const dim3 block(EM3D_BZ, EM3D_BY), zblock(1, 256);
+    Em3DParams pd = p;   // the lean form adds the dipoles after the step, in em3d_dipole_kernel
+    if (lean) p.n_dip = 0;
+    Em3DParams faces[3] = {p, p, p};
+    if (fused)
+        for (int f = 0; f < 3; ++f) face_boxes(h, faces[f], f);
+    const Em3DBox in = lean ? lean_box(h) : fused_box(h);
+    const bool z_faces = in.k0 > 0;   // the z faces need launches of their own
+    const int ty = fused_rows(fused_cfg(h));
+    const dim3 block(EM3D_BZ, EM3D_BY);
     const dim3 fused_grid((unsigned)((in.k1 - in.k0 + EM3D_FZ - 2) / (EM3D_FZ - 1)),
                           (unsigned)((in.j1 - in.j0 + ty - 2) / (ty - 1)),
                           (unsigned)((in.i1 - in.i0 + p.x_chunk - 1) / p.x_chunk));
     OS_CUDA(cudaEventRecord(h->ev_start, h->stream));
     for (int64_t k = 0; k < n_steps; ++k) {
         p.k_step = k;
-        pz.k_step = k;
+        for (auto &f : faces) f.k_step = k;
+        pd.k_step = k;
         if (fused) {
             const int a = h->cur, b = a ^ 1;
             // faces H: E^n, H^{n-1/2}, psi of set a -> H^{n+1/2}, psi' of set b
             point_sets(h, p, a, a, b, b);
             point_psi(h, p, a, b);
-            point_sets(h, pz, a, a, b, b);
-            point_psi(h, pz, a, b);
-            em3d_h_kernel<EM3D_BZ, EM3D_BY><<<box_grid(p), block, 0, h->stream>>>(p);
-            em3d_h_kernel<1, 256><<<box_grid(pz, 1, 256), zblock, 0, h->stream>>>(pz);
-            if (staged) OS_TRY(launch_staged(h, a, fused_grid, p, in, h->stream));
-            else OS_TRY(launch_fused(h->fused_config, fused_grid, p, in, h->stream));
+            for (auto &f : faces) {
+                point_sets(h, f, a, a, b, b);
+                point_psi(h, f, a, b);
+            }
+            h->launches += launch_faces(h, faces, false, z_faces);
+            if (lean) OS_TRY(launch_lean(h, a, p, in, h->stream));
+            else if (staged) OS_TRY(launch_staged(h, a, fused_grid, p, in, h->stream));
+            else OS_TRY(launch_fused(fused_cfg(h), fused_grid, p, in, h->stream));
             // faces E: E^n and psi of set a, H^{n+1/2} of set b -> E^{n+1}, psi' of set b
-            point_sets(h, p, a, b, b, b);
-            point_sets(h, pz, a, b, b, b);
-            em3d_e_kernel<EM3D_BZ, EM3D_BY><<<box_grid(p), block, 0, h->stream>>>(p);
-            em3d_e_kernel<1, 256><<<box_grid(pz, 1, 256), zblock, 0, h->stream>>>(pz);
-            h->launches += 5;
+            for (auto &f : faces) point_sets(h, f, a, b, b, b);
+            h->launches += launch_faces(h, faces, true, z_faces) + 1;
+            if (lean && pd.n_dip) {
+                point_sets(h, pd, a, b, b, b);
+                em3d_dipole_kernel<<<1, 1, 0, h->stream>>>(pd);
+                h->launches += 1;
+            }
             h->cur = b;
         } else {
             const dim3 grid = box_grid(p);
@@ -781,24 +895,24 @@ extern "C" int os_fdtd3d_set_x_chunk(OsFdtd3D *h, int32_t planes) {
 
 extern "C" int os_fdtd3d_set_variant(OsFdtd3D *h, int32_t variant) {
     OS_CHECK(h, OS_ERR_INVALID, "os_fdtd3d_set_variant: null handle");
-    OS_CHECK(variant >= 0 && variant <= 2, OS_ERR_INVALID,
-             "variant must be 0 (two in-place kernels), 1 (fused, two field sets) or 2 (fused with staged planes), "
-             "got %d", variant);
+    OS_CHECK(variant >= 0 && variant <= 3, OS_ERR_INVALID,
+             "variant must be 0 (two in-place kernels), 1 (fused, two field sets), 2 (fused with staged planes) or 3 "
+             "(lean staged fused pass), got %d", variant);
     h->variant = variant;
     return OS_OK;
 }
 
 extern "C" int os_fdtd3d_set_fused_config(OsFdtd3D *h, int32_t config) {
     OS_CHECK(h, OS_ERR_INVALID, "os_fdtd3d_set_fused_config: null handle");
-    OS_CHECK(config >= 0 && config < FUSED_CONFIGS, OS_ERR_INVALID, "fused kernel configuration must be in [0, %d), got %d",
-             FUSED_CONFIGS, config);
+    OS_CHECK(config >= -1 && config < FUSED_CONFIGS, OS_ERR_INVALID,
+             "fused kernel configuration must be in [-1, %d), got %d", FUSED_CONFIGS, config);
     h->fused_config = config;
     return OS_OK;
 }
 
 extern "C" int os_fdtd3d_interior(OsFdtd3D *h, int32_t *box6, int32_t *fused) {
     OS_CHECK(h && box6 && fused, OS_ERR_INVALID, "os_fdtd3d_interior: null argument");
-    const Em3DBox b = fused_box(h);
+    const Em3DBox b = lean_active(h) ? lean_box(h) : fused_box(h);
     const int32_t v[6] = {b.i0, b.i1, b.j0, b.j1, b.k0, b.k1};
     for (int q = 0; q < 6; ++q) box6[q] = v[q];
     *fused = fused_active(h) ? 1 : 0;

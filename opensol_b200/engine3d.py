@@ -293,13 +293,16 @@ class FDTDEngine3D:
         _native.check(_native.load().os_fdtd3d_set_x_chunk(self.handle, int(planes)))
 
     def set_variant(self, variant):
-        """Step form (speed and memory only; results are bit-identical): 0 = the two in-place kernels (the default),
-        1 = the fused kernel on two field and psi sets, 2 = the fused kernel with its planes staged in shared memory
-        by bulk copies (rows of a multiple of 8 cells; other grids run form 1)."""
+        """Step form (speed and memory only; results are bit-identical): 0 = the two in-place kernels, 1 = the fused
+        kernel on two field and psi sets, 2 = the fused kernel with its planes staged in shared memory by tensor
+        copies (rows of a multiple of 8 cells; other grids run form 1), 3 = the lean staged fused kernel (the default:
+        four cells a thread, packed arithmetic; z rows of a multiple of 4 cells and at least 144, y at least 17; other
+        grids run form 0)."""
         _native.check(_native.load().os_fdtd3d_set_variant(self.handle, int(variant)))
 
     def set_fused_config(self, config):
-        """Launch shape of the fused step kernel (0..4; speed only, results bit-identical)."""
+        """Launch shape of the fused step kernel of forms 1-3 (0..4, -1 for the form's default; speed only, results
+        bit-identical)."""
         _native.check(_native.load().os_fdtd3d_set_fused_config(self.handle, int(config)))
 
     def interior(self):

@@ -87,8 +87,13 @@ def test_field_roundtrip_and_launches():
     engine.synchronize()
     m = physics.monitors[0].sample_interval
     _, fused = engine.interior()
-    assert fused   # the fused kernel, and H then E of the faces in two block shapes each: 5 launches per step
-    assert engine.launch_count() == 5 * 30 + 30 // m
+    assert fused   # the fused kernel, and H then E of the x, y and z faces in three launches each: 7 per step
+    assert engine.launch_count() == 7 * 30 + 30 // m
+    engine.set_variant(3)   # the lean form needs rows of at least 144 cells: this grid runs the in-place form
+    engine.reset()
+    physics.run(30)
+    assert not engine.interior()[1]
+    assert engine.launch_count() == 2 * 30 + 30 // m
     engine.set_variant(0)
     engine.reset()
     physics.run(30)
@@ -96,19 +101,28 @@ def test_field_roundtrip_and_launches():
     assert engine.last_advance_ms() > 0.0
 
 
-@pytest.mark.parametrize('spec', CASES3D, ids=[c['name'] for c in CASES3D])
+# c3_mixed with a z extent of 160 cells (a multiple of 4, at least 144): the lean form runs on it, with lossy and
+# magnetic blocks (every coefficient path), a periodic axis and pec / pmc faces
+MIXED_NZ160 = dict(CASES3D[1], name='c3_mixed_nz160', window=(16, 20, 150))
+FORM_SPECS = CASES3D + [MIXED_NZ160]
+
+
+@pytest.mark.parametrize('spec', FORM_SPECS, ids=[c['name'] for c in FORM_SPECS])
 def test_step_forms_bit_identical(spec):
-    """The fused form (two field and psi sets) in every launch shape and the in-place two-kernel form give
-    bit-identical fields and fluxes, chunked into uneven advances (the set holding the current state alternates
-    between chunks)."""
+    """The fused forms (two field and psi sets; the lean form where the z extent is a multiple of 4, else the
+    in-place form) in every launch shape and the in-place two-kernel form give bit-identical fields and fluxes,
+    chunked into uneven advances (the set holding the current state alternates between chunks)."""
+    from cases3d import grid_shape
+    shape = grid_shape(spec)
+    lean = shape[2] % 4 == 0 and shape[2] >= 144 and shape[1] >= 17
     runs = []
-    for variant, config in ((0, 0), (1, 0), (1, 1), (1, 2), (1, 3), (1, 4)):
+    for variant, config in ((0, 0), (1, 0), (1, 1), (1, 2), (1, 3), (1, 4), (3, 0), (3, 1), (3, 2), (3, 3)):
         physics, monitors = build_product(spec)
         engine = physics.engine
         engine.set_variant(variant)
         engine.set_fused_config(config)
         box, fused = engine.interior()
-        assert fused == (variant == 1)
+        assert fused == (variant == 1 or (variant == 3 and lean))
         assert all(hi > lo for lo, hi in zip(box[::2], box[1::2]))
         for n in (7, 1, 12, 5):
             physics.run(n)
@@ -185,9 +199,9 @@ def test_workload_512_against_oracle():
 
 @pytest.mark.parametrize('total', [64, 96])
 def test_staged_form_bit_identical(total):
-    """The fused form with planes staged in shared memory by bulk copies (variant 2; rows of a multiple of 8 cells,
-    here the 3D workload on 64^3 and 96^3 grids) in every launch shape gives the fields and box flux of the in-place
-    two-kernel form bit for bit, over uneven chunks and short and long x chunks."""
+    """The fused form with planes staged in shared memory by tensor copies (variant 2; here the 3D workload on 64^3
+    and 96^3 grids) in every launch shape gives the fields and box flux of the in-place two-kernel form bit for bit,
+    over uneven chunks and short and long x chunks."""
     from opensol_b200 import workloads
     n_spheres = max(1, int(round(500 * (total / 512) ** 3)))
     runs = []
@@ -198,6 +212,64 @@ def test_staged_form_bit_identical(total):
         engine.set_variant(variant)
         engine.set_fused_config(config)
         engine.set_x_chunk(chunk)
+        for n in (13, 1, 40):
+            physics.run(n)
+        runs.append((engine.state(), np.asarray(box.flux())))
+        del physics, box
+    assert np.abs(runs[0][0]['ez']).max() > 0
+    for state, flux in runs[1:]:
+        for name in FIELDS:
+            np.testing.assert_array_equal(state[name], runs[0][0][name], err_msg=name)
+        np.testing.assert_array_equal(flux, runs[0][1])
+
+
+FP64_FLUX_RTOL_3D = 1e-5   # float32 box flux against the float64 3D oracle run, relative to its peak
+
+
+def test_workload_512_full_run_against_fixture():
+    """The whole 2000-step 512^3 workload against tests/golden/c3_full.npz (the oracle's float32 and float64 runs,
+    tests/golden/make_golden_c3_full.py): the six fields and every plane's complex128 spectra bit-identical (SHA-256)
+    at steps 200 and 2000, the box flux equal; the error of the float32 box flux against the float64 run is stated and
+    held to FP64_FLUX_RTOL_3D."""
+    from opensol_b200 import workloads
+    g = np.load(os.path.join(GOLDEN, 'c3_full.npz'))
+    physics, box = workloads.roofline_3d_physics()
+    physics.finalize()
+    assert box.sample_interval == int(g['sample_interval'])
+    engine = physics.engine
+    done = 0
+    for cp in (200, 2000):
+        physics.run(cp - done)
+        done = cp
+        for name in FIELDS:
+            assert _digest(engine.read_field(name)) == str(g[f'sha_{name}_{cp}']), (name, cp)
+        for p_, plane in enumerate(box.planes()):
+            for q, (e, h) in enumerate(plane.spectra()):
+                assert _digest(e) == str(g[f'sha_spec_e{p_}{q}_{cp}']), (p_, q, cp)
+                assert _digest(h) == str(g[f'sha_spec_h{p_}{q}_{cp}']), (p_, q, cp)
+        np.testing.assert_array_equal(np.asarray(box.flux()), g[f'flux_{cp}'])
+    f64 = g['f64_flux_2000']
+    error = float(np.abs(np.asarray(box.flux()) - f64).max() / np.abs(f64).max())
+    print(f'float32 vs float64 box flux error (relative to its peak): {error:.3e}')
+    assert error <= FP64_FLUX_RTOL_3D
+
+
+@pytest.mark.parametrize('total', [160, 200])
+def test_lean_form_bit_identical(total):
+    """The lean staged fused form (variant 3: four cells a thread, packed arithmetic; here the 3D workload on 160^3
+    and 200^3 grids, two and three tiles along z with partial last tiles) in every launch shape gives the fields and
+    box flux of the in-place two-kernel form bit for bit, over uneven chunks and short and long x chunks."""
+    from opensol_b200 import workloads
+    n_spheres = max(1, int(round(500 * (total / 512) ** 3)))
+    runs = []
+    for variant, config, chunk in ((0, 0, 24), (3, 0, 24), (3, 1, 7), (3, 2, 1), (3, 3, 50), (3, 0, 2)):
+        physics, box = workloads.roofline_3d_physics(total_cells=total, n_spheres=n_spheres)
+        physics.finalize()
+        engine = physics.engine
+        engine.set_variant(variant)
+        engine.set_fused_config(config)
+        engine.set_x_chunk(chunk)
+        assert engine.interior()[1] == (variant == 3)
         for n in (13, 1, 40):
             physics.run(n)
         runs.append((engine.state(), np.asarray(box.flux())))
