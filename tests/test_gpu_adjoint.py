@@ -86,3 +86,33 @@ def test_torch_autograd_function():
     (2.0 * J).backward()
     np.testing.assert_allclose(x.grad.numpy(), 2.0 * adj.backward(), rtol=0, atol=0)
     adj.close()
+
+
+def test_adjoint_c5_against_open_sols_float64_finite_differences():
+    """The adjoint workload at its stated size (1024^2 incl. 20 CPML cells per side, a 200 x 200 design box of seeded
+    eps_r, the 1550 nm flux objective after 8,000 steps, checkpoints every 256) against the reference-computed
+    gradient: central finite differences of open_sol's own float64 stepper on 32 seeded cells of the box
+    (tests/golden/adjoint_c5_fd.npz, made by tests/golden/make_golden_adjoint.py).  Bar: GRAD_RTOL relative, as the
+    norm of the difference over the 32 cells and cell by cell against the largest of them."""
+    import hashlib
+    import os
+    from opensol_b200 import workloads
+    g = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'adjoint_c5_fd.npz'))
+    spec = workloads.ADJOINT_2D
+    sim, monitor, box, eps = workloads.adjoint_2d_problem()
+    assert hashlib.sha256(eps.tobytes()).hexdigest() == str(g['eps_sha'])
+    assert tuple(box) == tuple(int(v) for v in g['box'])
+    adj = FluxAdjoint2D(sim, monitor, 0, box, spec['steps'], checkpoint_every=spec['checkpoint_every'])
+    J = adj.forward()
+    grad = adj.backward()
+    cells = g['cells']
+    fd = g['fd']
+    got = grad[cells[:, 0], cells[:, 1]]
+    norm_error = float(np.linalg.norm(got - fd) / np.linalg.norm(fd))
+    cell_error = float(np.abs(got - fd).max() / np.abs(fd).max())
+    print(f'J float32 {J!r} vs open_sol float64 {float(g["J"])!r}; gradient error: norm {norm_error:.2e}, '
+          f'worst cell {cell_error:.2e}')
+    assert abs(J - float(g['J'])) <= 1e-4 * abs(float(g['J']))
+    assert norm_error <= GRAD_RTOL
+    assert cell_error <= GRAD_RTOL
+    adj.close()
