@@ -64,6 +64,7 @@ def parse_args():
     p.add_argument('--form3d', type=int, default=3, choices=[0, 1, 2, 3],
                    help='em3d: step form (0 two in-place kernels, 1 fused on two field sets, 2 fused with staged '
                         'planes, 3 lean staged fused pass); results are the same bits')
+    p.add_argument('--x-chunk', type=int, default=0, help='em3d: x planes per block (0: the engine\'s choice)')
     p.add_argument('--fused-config', type=int, default=-1,
                    help="em3d: launch shape of the fused forms (0..4; -1: the form's default)")
     return p.parse_args()
@@ -496,6 +497,8 @@ def run_em3d(args):
     engine = physics.engine
     engine.set_variant(args.form3d)
     engine.set_fused_config(args.fused_config)
+    if args.x_chunk > 0:
+        engine.set_x_chunk(args.x_chunk)
     # a stream of its own (torch's default stream is handle 0, which os_fdtd*_set_stream reads as "the engine's own
     # stream"): the engine launches on it and the timing events are recorded on it
     stream = torch.cuda.Stream()
@@ -526,7 +529,7 @@ def run_em3d(args):
             'config': {'workload': f'em3d: {engine.nx}^3 total grid incl. 12 CPML cells/face, dx 20 nm, 500 seeded '
                                    'spheres eps_r U(2,12), z dipole 1310 nm at the centre, 8-frequency flux box, '
                                    f'{steps} Yee steps per bench step', 'l2': 'fields 6 x 537 MB, no flush',
-                       'step_form': args.form3d, 'fused_config': args.fused_config},
+                       'step_form': args.form3d, 'fused_config': args.fused_config, 'x_chunk': args.x_chunk},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
                          'traffic': None, 'peak_source': f'{peak_kind} hbm_gbs', 'bytes_per_cell_update': 52,
                          'kernel': 'em3d_h_kernel + em3d_e_kernel (whole step)'},

@@ -364,8 +364,9 @@ static int staged_maps(OsFdtd3D *h, int set, int ty, const Em3DMaps **out) {
     return OS_OK;
 }
 
-// em3d_lean_kernel configurations: (tile rows, ring slots, blocks per SM).
-constexpr int LEAN_CONFIGS = 4;
+// em3d_lean_kernel configurations: 0 = 16 tile rows, 3 ring slots, one block per SM; 1 (the default) = 8 rows, 3
+// slots, two blocks per SM.
+constexpr int LEAN_CONFIGS = 2;
 static int lean_rows(int config) { return config == 0 ? 16 : 8; }
 static int lean_ty_index(int ty) { return ty == 4 ? 0 : (ty == 8 ? 1 : 2); }
 
@@ -386,11 +387,11 @@ static int lean_maps(OsFdtd3D *h, int set, int ty, const Em3DLeanMaps **out) {
     return OS_OK;
 }
 
-template <int TY, int RING, int MINB, bool CA1>
+template <int TY, int RING, int MINB, bool CA1, bool HU>
 static int launch_lean_shape(const Em3DParams &p, const Em3DBox &in, const Em3DLeanMaps &maps, cudaStream_t s) {
     static bool attr_set = false;   // per template instance; the attribute outlives the handle
     if (!attr_set) {
-        OS_CUDA(cudaFuncSetAttribute(em3d_lean_kernel<TY, RING, MINB, CA1>,
+        OS_CUDA(cudaFuncSetAttribute(em3d_lean_kernel<TY, RING, MINB, CA1, HU>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)em3d_lean_smem<TY, RING>(EM3D_LEAN_MAX_ZROWS)));
         attr_set = true;
@@ -398,21 +399,17 @@ static int launch_lean_shape(const Em3DParams &p, const Em3DBox &in, const Em3DL
     const dim3 grid((unsigned)((in.k1 - (in.k0 & ~3) + EM3D_LTILE - 1) / EM3D_LTILE),
                     (unsigned)((in.j1 - in.j0 + TY - 2) / (TY - 1)),
                     (unsigned)((in.i1 - in.i0 + p.x_chunk - 1) / p.x_chunk));
-    em3d_lean_kernel<TY, RING, MINB, CA1>
+    em3d_lean_kernel<TY, RING, MINB, CA1, HU>
         <<<grid, dim3(32, TY), em3d_lean_smem<TY, RING>(p.cpml[2].nr), s>>>(p, in, maps);
     OS_CUDA(cudaGetLastError());
     return OS_OK;
 }
 
-template <bool CA1>
+template <bool CA1, bool HU>
 static int launch_lean_ca(int config, const Em3DParams &p, const Em3DBox &in, const Em3DLeanMaps &maps,
                           cudaStream_t s) {
-    switch (config) {
-        case 0: return launch_lean_shape<16, 3, 1, CA1>(p, in, maps, s);
-        case 1: return launch_lean_shape<8, 3, 2, CA1>(p, in, maps, s);
-        case 2: return launch_lean_shape<8, 4, 1, CA1>(p, in, maps, s);
-        default: return launch_lean_shape<8, 3, 1, CA1>(p, in, maps, s);
-    }
+    if (config == 0) return launch_lean_shape<16, 3, 1, CA1, HU>(p, in, maps, s);
+    return launch_lean_shape<8, 3, 2, CA1, HU>(p, in, maps, s);
 }
 
 // The lean kernel streams chunks of at most EM3D_LEAN_MAX_PLANES - 1 planes (its per-plane table).
@@ -421,7 +418,11 @@ static int launch_lean(OsFdtd3D *h, int set, Em3DParams p, const Em3DBox &in, cu
     const Em3DLeanMaps *maps = nullptr;
     OS_TRY(lean_maps(h, set, lean_rows(config), &maps));
     p.x_chunk = std::min<int32_t>(p.x_chunk, EM3D_LEAN_MAX_PLANES - 1);
-    return h->ca_one ? launch_lean_ca<true>(config, p, in, *maps, s) : launch_lean_ca<false>(config, p, in, *maps, s);
+    if (h->ca_one)
+        return h->h_uniform ? launch_lean_ca<true, true>(config, p, in, *maps, s)
+                            : launch_lean_ca<true, false>(config, p, in, *maps, s);
+    return h->h_uniform ? launch_lean_ca<false, true>(config, p, in, *maps, s)
+                        : launch_lean_ca<false, false>(config, p, in, *maps, s);
 }
 
 template <int TY, int MINB>

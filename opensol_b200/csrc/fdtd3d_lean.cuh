@@ -16,7 +16,8 @@
 // Arithmetic: products and plain differences in packed FP32 pairs (__fmul2_rn, __fadd2_rn; x - y as x + (-y)), and
 // every add or subtract with a product operand per lane with the scalar __fadd_rn, which the code generator never
 // merges into a fused multiply-add: each lane rounds exactly like em3d_h_kernel's / em3d_e_kernel's scalar code.
-// With CA1 (every face's ca is 1: no conductivity, no perfect conductor) ca * E is E itself and is not multiplied.
+// With CA1 (every face's ca is 1: no conductivity, no perfect conductor) ca * E is E itself and is not multiplied;
+// with HU every id has the same H coefficients (da_u, db_u) and the ids are not read for H.
 // Neighbours along k come from the next / previous lane (shuffles) or, for lane 31's k + 1, from the staged box; along
 // j from the staged row above (E) or the row below's new H through shared memory (one barrier per plane); along x
 // from the next slot (E) or the thread's previous plane (H).  The coefficients of a face between two cells of one id
@@ -59,12 +60,21 @@ struct Em3DLeanLayout {   // byte offsets inside one ring slot, every box on a 1
 constexpr int EM3D_LEAN_MAX_PLANES = 64;       // x planes of one block's chunk, the halo plane included
 constexpr int EM3D_LEAN_MAX_ZROWS = 255;       // z CPML rows (one byte per cell row index, 0xff: none)
 
-// Shared memory of one lean block: ring, exchanged H (two parities), mbarriers, per-plane scalars, z CPML coefficients.
+// Shared memory of one lean block, every region on a 16-byte boundary (the ring on 128): ring, exchanged H (two
+// parities), mbarriers, z CPML coefficients (b_h, g_h, b_e, g_e per z row; 16-byte vectors of four rows), per-plane
+// scalars.
+template <int TY, int RING>
+struct Em3DLeanSmem {
+    static constexpr size_t xch = Em3DLeanLayout<TY>::slot * (size_t)RING;
+    static constexpr size_t bars = xch + 2 * (size_t)Em3DLeanLayout<TY>::xch;
+    static constexpr size_t zc = bars + (RING * sizeof(uint64_t) + 15) / 16 * 16;
+    __host__ __device__ static constexpr size_t plane(int z_rows) { return zc + 16 * (size_t)z_rows; }
+    __host__ __device__ static constexpr size_t bytes(int z_rows) { return plane(z_rows) + EM3D_LEAN_MAX_PLANES * 40; }
+};
+
 template <int TY, int RING>
 __host__ __device__ constexpr size_t em3d_lean_smem(int z_rows) {
-    using L = Em3DLeanLayout<TY>;
-    return (size_t)L::slot * RING + 2 * (size_t)L::xch + RING * sizeof(uint64_t) + EM3D_LEAN_MAX_PLANES * 40 +
-           4 * (size_t)z_rows * sizeof(float);
+    return Em3DLeanSmem<TY, RING>::bytes(z_rows);
 }
 
 // Tensor maps of one lean launch: E and H components of the field set read, ids.
@@ -168,17 +178,18 @@ __device__ __forceinline__ void lv_store(float *ptr, const float2 (&v)[2], unsig
         if (mask & (1u << c)) ptr[c] = lv_get(v, c);
 }
 
-template <int TY, int RING, int MINB, bool CA1>
+template <int TY, int RING, int MINB, bool CA1, bool HU>
 __global__ void __launch_bounds__(32 * TY, MINB)
     em3d_lean_kernel(const Em3DParams p, const Em3DBox in, const __grid_constant__ Em3DLeanMaps maps) {
     using L = Em3DLeanLayout<TY>;
     extern __shared__ __align__(128) unsigned char em3d_lean_smem_buf[];
     unsigned char *const ring = em3d_lean_smem_buf;
-    float *const s_hx = reinterpret_cast<float *>(ring + L::slot * RING);   // [2][TY][128]
+    using S = Em3DLeanSmem<TY, RING>;
+    float *const s_hx = reinterpret_cast<float *>(ring + S::xch);   // [2][TY][128]
     float *const s_hz = s_hx + 2 * TY * 128;
-    uint64_t *const bar = reinterpret_cast<uint64_t *>(s_hz + 2 * TY * 128);
-    Em3DLeanPlane *const s_plane = reinterpret_cast<Em3DLeanPlane *>(bar + RING);   // [EM3D_LEAN_MAX_PLANES]
-    float *const s_zc = reinterpret_cast<float *>(s_plane + EM3D_LEAN_MAX_PLANES);  // b_h, g_h, b_e, g_e per z row
+    uint64_t *const bar = reinterpret_cast<uint64_t *>(ring + S::bars);
+    float *const s_zc = reinterpret_cast<float *>(ring + S::zc);    // [4][nrz]
+    Em3DLeanPlane *const s_plane = reinterpret_cast<Em3DLeanPlane *>(ring + S::plane(p.cpml[2].nr));
     const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
     const int kt0 = (in.k0 & ~3) + (int)blockIdx.x * EM3D_LTILE;  // the tile's first cell
     const int kv = kt0 + EM3D_LV * lane;                         // this thread's first cell (may be off the grid)
@@ -255,6 +266,9 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     }
     const float ihz_h = p.ihz[max(kt0 - 1, 0)];
     const int32_t zr_h = nrz ? p.cpml[2].rm_h[max(kt0 - 1, 0)] : -1;
+    // z rows r0 .. r0 + 3 on a multiple of 4 (and a multiple of 4 rows): one 16-byte psi vector for the four cells
+    const bool zvh = nrz % 4 == 0 && (zrh & 3u) == 0 && zrh == (zrh & 0xffu) * 0x01010101u + 0x03020100u;
+    const bool zve = nrz % 4 == 0 && (zre & 3u) == 0 && zre == (zre & 0xffu) * 0x01010101u + 0x03020100u;
     const int32_t ryh = p.cpml[1].nr ? p.cpml[1].rm_h[j] : -1, rye = p.cpml[1].nr ? p.cpml[1].rm_e[j] : -1;
     const float2 byh = lp_dup(ryh >= 0 ? p.cpml[1].b_h[ryh] : 0.0f), gyh = lp_dup(ryh >= 0 ? p.cpml[1].g_h[ryh] : 0.0f);
     const float2 bye = lp_dup(rye >= 0 ? p.cpml[1].b_e[rye] : 0.0f), gye = lp_dup(rye >= 0 ? p.cpml[1].g_e[rye] : 0.0f);
@@ -306,7 +320,7 @@ __global__ void __launch_bounds__(32 * TY, MINB)
         }
         lv_up(ex0, exn4, exk);
         lv_up(ey0, eyn4, eyk);
-        const bool hu = p.h_uniform;
+        constexpr bool hu = HU;
         float2 dav[2], dbv[2];
         if (hu) {
             dav[0] = dav[1] = lp_dup(p.da_u);
@@ -372,7 +386,25 @@ __global__ void __launch_bounds__(32 * TY, MINB)
             lv_store(c.oph_first + qq, f, smask, vec);
             lv_store(c.oph_second + qq, g, smask, vec);
         }
-        if (zrh != 0xffffffffu) {   // z layers, per cell: H_x from E_y (+), H_y from E_x (-)
+        if (zvh) {   // z layers, four consecutive rows: H_x from E_y (+), H_y from E_x (-)
+            const Em3DCpmlAxis &c = p.cpml[2];
+            const int r0 = (int)(zrh & 0xffu);
+            const size_t qq = ((size_t)i * p.ny + j) * nrz + r0;
+            float2 pf[2], pg[2], bz[2], gz[2], f[2], g[2];
+            lv_ldg(c.ph_first + qq, pf);
+            lv_ldg(c.ph_second + qq, pg);
+            lv_lds(s_zc + r0, bz);
+            lv_lds(s_zc + nrz + r0, gz);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                f[h] = ls_add(lp_mul(bz[h], pf[h]), lp_mul(gz[h], dey_z[h]));
+                g[h] = ls_add(lp_mul(bz[h], pg[h]), lp_mul(gz[h], dex_z[h]));
+                vhx[h] = ls_add(vhx[h], lp_mul(dbv[h], f[h]));
+                vhy[h] = ls_sub(vhy[h], lp_mul(dbv[h], g[h]));
+            }
+            lv_store(c.oph_first + qq, f, smask, smask == 0u || smask == 0xFu);
+            lv_store(c.oph_second + qq, g, smask, smask == 0u || smask == 0xFu);
+        } else if (zrh != 0xffffffffu) {   // z layers, per cell
             const Em3DCpmlAxis &c = p.cpml[2];
             const size_t zb = ((size_t)i * p.ny + j) * nrz;
 #pragma unroll
@@ -541,7 +573,25 @@ __global__ void __launch_bounds__(32 * TY, MINB)
                 lv_store(c.ope_first + qq, f, kmask, vec);
                 lv_store(c.ope_second + qq, g, kmask, vec);
             }
-            if (zre != 0xffffffffu) {   // z layers, per cell: E_x from H_y (-), E_y from H_x (+)
+            if (zve) {   // z layers, four consecutive rows: E_x from H_y (-), E_y from H_x (+)
+                const Em3DCpmlAxis &c = p.cpml[2];
+                const int r0 = (int)(zre & 0xffu);
+                const size_t qq = ((size_t)i * p.ny + j) * nrz + r0;
+                float2 pf[2], pg[2], bz[2], gz[2], f[2], g[2];
+                lv_ldg(c.pe_first + qq, pf);
+                lv_ldg(c.pe_second + qq, pg);
+                lv_lds(s_zc + 2 * nrz + r0, bz);
+                lv_lds(s_zc + 3 * nrz + r0, gz);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    f[h] = ls_add(lp_mul(bz[h], pf[h]), lp_mul(gz[h], dhy_z[h]));
+                    g[h] = ls_add(lp_mul(bz[h], pg[h]), lp_mul(gz[h], dhx_z[h]));
+                    vx[h] = ls_sub(vx[h], lp_mul(cbx[h], f[h]));
+                    vy[h] = ls_add(vy[h], lp_mul(cby[h], g[h]));
+                }
+                lv_store(c.ope_first + qq, f, kmask, kmask == 0u || kmask == 0xFu);
+                lv_store(c.ope_second + qq, g, kmask, kmask == 0u || kmask == 0xFu);
+            } else if (zre != 0xffffffffu) {   // z layers, per cell
                 const Em3DCpmlAxis &c = p.cpml[2];
                 const size_t zb = ((size_t)i * p.ny + j) * nrz;
 #pragma unroll
