@@ -13,7 +13,7 @@
 //     each axis), the faces by the face kernels;
 //   variant 2: variant 1 with each x plane of a tile staged in shared memory by tiled tensor copies
 //     (em3d_staged_kernel).
-// On 512^3: variant 3 65.3 G cell-updates/s (52 B of algorithmic traffic a cell-update: 0.52 of the measured copy
+// On 512^3: variant 3 71.7 G cell-updates/s (52 B of algorithmic traffic a cell-update: 0.57 of the measured copy
 // bandwidth), variant 0 48.3 (two kernels re-reading the fields, ~76 B), variant 1 42.7, variant 2 46.4.
 // A chunk of n steps is enqueued with no host synchronisation: per-step dipole amplitudes and per-sample DFT phases
 // arrive as small tables computed on the host in float64 and rounded as open_sol rounds them.
@@ -34,7 +34,7 @@ struct OsFdtd3D {
     os::DeviceArray<float> field[6];            // ex, ey, ez, hx, hy, hz
     os::DeviceArray<float> field2[6];           // the second field set of variant 1 (allocated on first use)
     int cur = 0;                                // the set holding the current state (0: field, 1: field2)
-    int32_t variant = 3;                        // on 512^3: 65.3 G cell-updates/s; variant 0 48.3, 1 42.7, 2 46.4
+    int32_t variant = 3;                        // on 512^3: 71.7 G cell-updates/s; variant 0 48.3, 1 42.7, 2 46.4
     int32_t fused_config = -1;                  // launch shape of the fused form's kernel (speed only; -1: default)
     os::DeviceArray<uint16_t> mat;
     os::DeviceArray<float> tables;              // t_ex, t_ey, t_ez, t_sig, t_da, t_db (6 * n_ids)
@@ -74,7 +74,7 @@ struct OsFdtd3D {
     os::DeviceArray<int32_t> err;               // set by a staged kernel whose bounded wait ran out
     Em3DMaps maps[2][2];                        // staged form: tensor maps per field set read and tile height (8, 16)
     bool maps_ok[2][2] = {{false, false}, {false, false}};
-    Em3DLeanMaps lean_maps[2][3];               // lean form: per field set read and tile height (4, 8, 16)
+    Em3DLeanMaps lean_maps[2][3];               // lean form: per field set read and tile height (6, 8, 16)
     bool lean_maps_ok[2][3] = {{false, false, false}, {false, false, false}};
     bool ca_one = true;                         // every face's ca is 1 (no conductivity, no perfect conductor)
 };
@@ -364,11 +364,13 @@ static int staged_maps(OsFdtd3D *h, int set, int ty, const Em3DMaps **out) {
     return OS_OK;
 }
 
-// em3d_lean_kernel configurations: 0 = 16 tile rows, 3 ring slots, one block per SM; 1 (the default) = 8 rows, 3
-// slots, two blocks per SM.
-constexpr int LEAN_CONFIGS = 2;
-static int lean_rows(int config) { return config == 0 ? 16 : 8; }
-static int lean_ty_index(int ty) { return ty == 4 ? 0 : (ty == 8 ? 1 : 2); }
+// em3d_lean_kernel configurations (on 512^3): 0 = 16 tile rows, 3 ring slots, one block per SM (67.7 G
+// cell-updates/s); 1 = 8 rows, 3 slots, two blocks per SM, each plane's copies issued after its exchange barrier
+// (70.2); 2 (the default) = 1 with the copies issued at the top of the plane behind a second barrier, a whole plane
+// ahead (71.7); 3 = 6 rows, 4 slots, two blocks per SM, early copies (58.3: fewer warps).
+constexpr int LEAN_CONFIGS = 4;
+static int lean_rows(int config) { return config == 0 ? 16 : (config == 3 ? 6 : 8); }
+static int lean_ty_index(int ty) { return ty == 6 ? 0 : (ty == 8 ? 1 : 2); }
 
 // The lean launch's maps for field set `set` and tile height ty (made once per handle).
 static int lean_maps(OsFdtd3D *h, int set, int ty, const Em3DLeanMaps **out) {
@@ -387,11 +389,11 @@ static int lean_maps(OsFdtd3D *h, int set, int ty, const Em3DLeanMaps **out) {
     return OS_OK;
 }
 
-template <int TY, int RING, int MINB, bool CA1, bool HU>
+template <int TY, int RING, int MINB, bool CA1, bool HU, bool EARLY>
 static int launch_lean_shape(const Em3DParams &p, const Em3DBox &in, const Em3DLeanMaps &maps, cudaStream_t s) {
     static bool attr_set = false;   // per template instance; the attribute outlives the handle
     if (!attr_set) {
-        OS_CUDA(cudaFuncSetAttribute(em3d_lean_kernel<TY, RING, MINB, CA1, HU>,
+        OS_CUDA(cudaFuncSetAttribute(em3d_lean_kernel<TY, RING, MINB, CA1, HU, EARLY>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)em3d_lean_smem<TY, RING>(EM3D_LEAN_MAX_ZROWS)));
         attr_set = true;
@@ -399,7 +401,7 @@ static int launch_lean_shape(const Em3DParams &p, const Em3DBox &in, const Em3DL
     const dim3 grid((unsigned)((in.k1 - (in.k0 & ~3) + EM3D_LTILE - 1) / EM3D_LTILE),
                     (unsigned)((in.j1 - in.j0 + TY - 2) / (TY - 1)),
                     (unsigned)((in.i1 - in.i0 + p.x_chunk - 1) / p.x_chunk));
-    em3d_lean_kernel<TY, RING, MINB, CA1, HU>
+    em3d_lean_kernel<TY, RING, MINB, CA1, HU, EARLY>
         <<<grid, dim3(32, TY), em3d_lean_smem<TY, RING>(p.cpml[2].nr), s>>>(p, in, maps);
     OS_CUDA(cudaGetLastError());
     return OS_OK;
@@ -408,13 +410,15 @@ static int launch_lean_shape(const Em3DParams &p, const Em3DBox &in, const Em3DL
 template <bool CA1, bool HU>
 static int launch_lean_ca(int config, const Em3DParams &p, const Em3DBox &in, const Em3DLeanMaps &maps,
                           cudaStream_t s) {
-    if (config == 0) return launch_lean_shape<16, 3, 1, CA1, HU>(p, in, maps, s);
-    return launch_lean_shape<8, 3, 2, CA1, HU>(p, in, maps, s);
+    if (config == 0) return launch_lean_shape<16, 3, 1, CA1, HU, false>(p, in, maps, s);
+    if (config == 2) return launch_lean_shape<8, 3, 2, CA1, HU, true>(p, in, maps, s);
+    if (config == 3) return launch_lean_shape<6, 4, 2, CA1, HU, true>(p, in, maps, s);
+    return launch_lean_shape<8, 3, 2, CA1, HU, false>(p, in, maps, s);
 }
 
 // The lean kernel streams chunks of at most EM3D_LEAN_MAX_PLANES - 1 planes (its per-plane table).
 static int launch_lean(OsFdtd3D *h, int set, Em3DParams p, const Em3DBox &in, cudaStream_t s) {
-    const int config = h->fused_config < 0 ? 1 : h->fused_config % LEAN_CONFIGS;
+    const int config = h->fused_config < 0 ? 2 : h->fused_config % LEAN_CONFIGS;
     const Em3DLeanMaps *maps = nullptr;
     OS_TRY(lean_maps(h, set, lean_rows(config), &maps));
     p.x_chunk = std::min<int32_t>(p.x_chunk, EM3D_LEAN_MAX_PLANES - 1);

@@ -62,14 +62,15 @@ constexpr int EM3D_LEAN_MAX_ZROWS = 255;       // z CPML rows (one byte per cell
 
 // Shared memory of one lean block, every region on a 16-byte boundary (the ring on 128): ring, exchanged H (two
 // parities), mbarriers, z CPML coefficients (b_h, g_h, b_e, g_e per z row; 16-byte vectors of four rows), per-plane
-// scalars.
+// scalars, the tile's z inverse spacings (H then E).
 template <int TY, int RING>
 struct Em3DLeanSmem {
     static constexpr size_t xch = Em3DLeanLayout<TY>::slot * (size_t)RING;
     static constexpr size_t bars = xch + 2 * (size_t)Em3DLeanLayout<TY>::xch;
     static constexpr size_t zc = bars + (RING * sizeof(uint64_t) + 15) / 16 * 16;
     __host__ __device__ static constexpr size_t plane(int z_rows) { return zc + 16 * (size_t)z_rows; }
-    __host__ __device__ static constexpr size_t bytes(int z_rows) { return plane(z_rows) + EM3D_LEAN_MAX_PLANES * 40; }
+    __host__ __device__ static constexpr size_t kz(int z_rows) { return plane(z_rows) + EM3D_LEAN_MAX_PLANES * 40; }
+    __host__ __device__ static constexpr size_t bytes(int z_rows) { return kz(z_rows) + 2 * EM3D_LTILE * 4; }
 };
 
 template <int TY, int RING>
@@ -178,7 +179,7 @@ __device__ __forceinline__ void lv_store(float *ptr, const float2 (&v)[2], unsig
         if (mask & (1u << c)) ptr[c] = lv_get(v, c);
 }
 
-template <int TY, int RING, int MINB, bool CA1, bool HU>
+template <int TY, int RING, int MINB, bool CA1, bool HU, bool EARLY>
 __global__ void __launch_bounds__(32 * TY, MINB)
     em3d_lean_kernel(const Em3DParams p, const Em3DBox in, const __grid_constant__ Em3DLeanMaps maps) {
     using L = Em3DLeanLayout<TY>;
@@ -190,6 +191,7 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     uint64_t *const bar = reinterpret_cast<uint64_t *>(ring + S::bars);
     float *const s_zc = reinterpret_cast<float *>(ring + S::zc);    // [4][nrz]
     Em3DLeanPlane *const s_plane = reinterpret_cast<Em3DLeanPlane *>(ring + S::plane(p.cpml[2].nr));
+    float *const s_kz = reinterpret_cast<float *>(ring + S::kz(p.cpml[2].nr));   // [2][128]
     const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
     const int kt0 = (in.k0 & ~3) + (int)blockIdx.x * EM3D_LTILE;  // the tile's first cell
     const int kv = kt0 + EM3D_LV * lane;                         // this thread's first cell (may be off the grid)
@@ -237,6 +239,11 @@ __global__ void __launch_bounds__(32 * TY, MINB)
         pl.ge = pl.re >= 0 ? p.cpml[0].g_e[pl.re] : 0.0f;
         s_plane[q] = pl;
     }
+    for (int c = tid; c < EM3D_LTILE; c += 32 * TY) {
+        const int kc = min(kt0 + c, p.nz - 1);
+        s_kz[c] = p.ihz[kc];
+        s_kz[EM3D_LTILE + c] = p.iez[kc];
+    }
     const int nrz = p.cpml[2].nr;
     for (int r = tid; r < nrz; r += 32 * TY) {
         s_zc[r] = p.cpml[2].b_h[r];
@@ -251,13 +258,10 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     const int n_issued_max = i_last - base + 1;
     // per-row and per-cell spacings; CPML rows of the row (y) and of the cells (z, one byte each, 0xff: none)
     const float2 ihy2 = lp_dup(p.ihy[j]), iey2 = lp_dup(p.iey[j]);
-    float2 ihz[2], iez[2];
     uint32_t zrh = 0xffffffffu, zre = 0xffffffffu;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
         const int kc = min(max(kv + c, 0), p.nz - 1);
-        lv_set(ihz, c, p.ihz[kc]);
-        lv_set(iez, c, p.iez[kc]);
         if (nrz) {
             const int32_t rh = p.cpml[2].rm_h[kc], re = p.cpml[2].rm_e[kc];
             if (rh >= 0) zrh = (zrh & ~(0xffu << (8 * c))) | ((uint32_t)rh << (8 * c));
@@ -290,6 +294,16 @@ __global__ void __launch_bounds__(32 * TY, MINB)
         const int q = i - base;
         const unsigned char *cur = ring + cs * L::slot;
         const unsigned char *nxt = ring + ns * L::slot;
+        if (EARLY) {
+            // every warp is done with plane i - 1: its slot takes plane i + RING - 1 now, a whole plane before it is
+            // read
+            __syncthreads();
+            if (w == 0 && q >= 1 && i + RING - 1 <= i_last) {
+                const int ps = cs == 0 ? RING - 1 : cs - 1;
+                tb_fence_proxy_async();
+                em3d_lean_issue<TY>(maps, ring + ps * L::slot, bar + ps, i + RING - 1, j_row0, ke, km, lane);
+            }
+        }
         ok = tb_mbar_wait(bar + ns, nph) && ok;
         const Em3DLeanPlane pl = s_plane[q];
         const float *ce0 = reinterpret_cast<const float *>(cur + L::e_off);
@@ -337,7 +351,8 @@ __global__ void __launch_bounds__(32 * TY, MINB)
         }
         const float2 ihx2 = lp_dup(pl.ihx);
         float2 dez_y[2], dey_z[2], dex_z[2], dez_x[2], dey_x[2], dex_y[2];
-        float2 vhx[2], vhy[2], vhz[2];
+        float2 vhx[2], vhy[2], vhz[2], ihz[2];
+        lv_lds(s_kz + EM3D_LV * lane, ihz);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             dez_y[h] = lp_sub(ezy[h], ez0[h]);
@@ -472,7 +487,7 @@ __global__ void __launch_bounds__(32 * TY, MINB)
             return;
         }
         // no thread reads the slot of plane i - 1 any more: it takes plane i + RING - 1
-        if (w == 0 && q >= 1 && i + RING - 1 <= i_last) {
+        if (!EARLY && w == 0 && q >= 1 && i + RING - 1 <= i_last) {
             const int ps = cs == 0 ? RING - 1 : cs - 1;
             tb_fence_proxy_async();
             em3d_lean_issue<TY>(maps, ring + ps * L::slot, bar + ps, i + RING - 1, j_row0, ke, km, lane);
@@ -524,7 +539,12 @@ __global__ void __launch_bounds__(32 * TY, MINB)
                 }
             }
             const float2 iex2 = lp_dup(pl.iex);
-            float2 dhz_y[2], dhy_z[2], dhx_z[2], dhz_x[2], dhy_x[2], dhx_y[2], vx[2], vy[2], vz[2];
+            float2 dhz_y[2], dhy_z[2], dhx_z[2], dhz_x[2], dhy_x[2], dhx_y[2], vx[2], vy[2], vz[2], iez[2];
+            float2 ex0[2], ey0[2], ez0[2];   // E^n of the cells, read again from the slot
+            lv_lds(s_kz + EM3D_LTILE + EM3D_LV * lane, iez);
+            lv_lds(ce0 + at_e, ex0);
+            lv_lds(ce1 + at_e, ey0);
+            lv_lds(ce2 + at_e, ez0);
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 dhz_y[h] = lp_sub(vhz[h], hzy[h]);
