@@ -74,8 +74,8 @@ struct OsFdtd3D {
     os::DeviceArray<int32_t> err;               // set by a staged kernel whose bounded wait ran out
     Em3DMaps maps[2][2];                        // staged form: tensor maps per field set read and tile height (8, 16)
     bool maps_ok[2][2] = {{false, false}, {false, false}};
-    Em3DLeanMaps lean_maps[2][3];               // lean form: per field set read and tile height (6, 8, 16)
-    bool lean_maps_ok[2][3] = {{false, false, false}, {false, false, false}};
+    Em3DLeanMaps lean_maps[2][8];               // lean form: per field set read and launch configuration
+    bool lean_maps_ok[2][8] = {};
     bool ca_one = true;                         // every face's ca is 1 (no conductivity, no perfect conductor)
 };
 
@@ -367,66 +367,69 @@ static int staged_maps(OsFdtd3D *h, int set, int ty, const Em3DMaps **out) {
 // em3d_lean_kernel configurations (on 512^3): 0 = 16 tile rows, 3 ring slots, one block per SM (67.7 G
 // cell-updates/s); 1 = 8 rows, 3 slots, two blocks per SM, each plane's copies issued after its exchange barrier
 // (70.2); 2 (the default) = 1 with the copies issued at the top of the plane behind a second barrier, a whole plane
-// ahead (71.7); 3 = 6 rows, 4 slots, two blocks per SM, early copies (58.3: fewer warps).
-constexpr int LEAN_CONFIGS = 4;
-static int lean_rows(int config) { return config == 0 ? 16 : (config == 3 ? 6 : 8); }
-static int lean_ty_index(int ty) { return ty == 6 ? 0 : (ty == 8 ? 1 : 2); }
+// ahead (71.7); 3 = 6 rows, 4 slots, two blocks per SM, early copies (58.3: fewer warps); 4 = 2 with no exchange:
+// every warp computes H_x, H_z of the row below its own (8 output rows a block, one barrier per plane; 69.6: the
+// extra H work costs more than the barrier and the halo warp it saves).
+constexpr int LEAN_CONFIGS = 5;
+static_assert(LEAN_CONFIGS <= 8, "lean map cache");
 
-// The lean launch's maps for field set `set` and tile height ty (made once per handle).
-static int lean_maps(OsFdtd3D *h, int set, int ty, const Em3DLeanMaps **out) {
-    const int t = lean_ty_index(ty);
-    if (!h->lean_maps_ok[set][t]) {
-        using L = Em3DLeanLayout<8>;
-        Em3DLeanMaps &m = h->lean_maps[set][t];
+template <int TY, bool NX>
+static int lean_maps(OsFdtd3D *h, int set, int config, const Em3DLeanMaps **out) {
+    if (!h->lean_maps_ok[set][config]) {
+        using L = Em3DLeanLayout<TY, NX>;
+        Em3DLeanMaps &m = h->lean_maps[set][config];
         for (int c = 0; c < 3; ++c) {
-            OS_TRY(encode_box(&m.e[c], fset(h, set, c), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->grid, L::WE, ty + 1));
-            OS_TRY(encode_box(&m.h[c], fset(h, set, 3 + c), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->grid, L::WH, ty));
+            OS_TRY(encode_box(&m.e[c], fset(h, set, c), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->grid, L::WE, L::ER));
+            OS_TRY(encode_box(&m.h[c], fset(h, set, 3 + c), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->grid, L::WH, L::HR));
         }
-        OS_TRY(encode_box(&m.m, h->mat.ptr, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, h->grid, L::WM, ty + 1));
-        h->lean_maps_ok[set][t] = true;
+        OS_TRY(encode_box(&m.m, h->mat.ptr, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, h->grid, L::WM, L::MR));
+        h->lean_maps_ok[set][config] = true;
     }
-    *out = &h->lean_maps[set][t];
+    *out = &h->lean_maps[set][config];
     return OS_OK;
 }
 
-template <int TY, int RING, int MINB, bool CA1, bool HU, bool EARLY>
-static int launch_lean_shape(const Em3DParams &p, const Em3DBox &in, const Em3DLeanMaps &maps, cudaStream_t s) {
+template <int TY, int RING, int MINB, bool CA1, bool HU, bool EARLY, bool NX>
+static int launch_lean_shape(OsFdtd3D *h, int set, int config, const Em3DParams &p, const Em3DBox &in,
+                             cudaStream_t s) {
     static bool attr_set = false;   // per template instance; the attribute outlives the handle
     if (!attr_set) {
-        OS_CUDA(cudaFuncSetAttribute(em3d_lean_kernel<TY, RING, MINB, CA1, HU, EARLY>,
+        OS_CUDA(cudaFuncSetAttribute(em3d_lean_kernel<TY, RING, MINB, CA1, HU, EARLY, NX>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)em3d_lean_smem<TY, RING>(EM3D_LEAN_MAX_ZROWS)));
+                                     (int)em3d_lean_smem<TY, RING, NX>(EM3D_LEAN_MAX_ZROWS)));
         attr_set = true;
     }
+    const Em3DLeanMaps *maps = nullptr;
+    OS_TRY((lean_maps<TY, NX>(h, set, config, &maps)));
     const dim3 grid((unsigned)((in.k1 - (in.k0 & ~3) + EM3D_LTILE - 1) / EM3D_LTILE),
-                    (unsigned)((in.j1 - in.j0 + TY - 2) / (TY - 1)),
+                    (unsigned)(NX ? (in.j1 - in.j0 + TY - 1) / TY : (in.j1 - in.j0 + TY - 2) / (TY - 1)),
                     (unsigned)((in.i1 - in.i0 + p.x_chunk - 1) / p.x_chunk));
-    em3d_lean_kernel<TY, RING, MINB, CA1, HU, EARLY>
-        <<<grid, dim3(32, TY), em3d_lean_smem<TY, RING>(p.cpml[2].nr), s>>>(p, in, maps);
+    em3d_lean_kernel<TY, RING, MINB, CA1, HU, EARLY, NX>
+        <<<grid, dim3(32, TY), em3d_lean_smem<TY, RING, NX>(p.cpml[2].nr), s>>>(p, in, *maps);
     OS_CUDA(cudaGetLastError());
     return OS_OK;
 }
 
 template <bool CA1, bool HU>
-static int launch_lean_ca(int config, const Em3DParams &p, const Em3DBox &in, const Em3DLeanMaps &maps,
-                          cudaStream_t s) {
-    if (config == 0) return launch_lean_shape<16, 3, 1, CA1, HU, false>(p, in, maps, s);
-    if (config == 2) return launch_lean_shape<8, 3, 2, CA1, HU, true>(p, in, maps, s);
-    if (config == 3) return launch_lean_shape<6, 4, 2, CA1, HU, true>(p, in, maps, s);
-    return launch_lean_shape<8, 3, 2, CA1, HU, false>(p, in, maps, s);
+static int launch_lean_ca(OsFdtd3D *h, int set, int config, const Em3DParams &p, const Em3DBox &in, cudaStream_t s) {
+    switch (config) {
+        case 0: return launch_lean_shape<16, 3, 1, CA1, HU, false, false>(h, set, config, p, in, s);
+        case 1: return launch_lean_shape<8, 3, 2, CA1, HU, false, false>(h, set, config, p, in, s);
+        case 3: return launch_lean_shape<6, 4, 2, CA1, HU, true, false>(h, set, config, p, in, s);
+        case 4: return launch_lean_shape<8, 3, 2, CA1, HU, true, true>(h, set, config, p, in, s);
+        default: return launch_lean_shape<8, 3, 2, CA1, HU, true, false>(h, set, config, p, in, s);
+    }
 }
 
 // The lean kernel streams chunks of at most EM3D_LEAN_MAX_PLANES - 1 planes (its per-plane table).
 static int launch_lean(OsFdtd3D *h, int set, Em3DParams p, const Em3DBox &in, cudaStream_t s) {
     const int config = h->fused_config < 0 ? 2 : h->fused_config % LEAN_CONFIGS;
-    const Em3DLeanMaps *maps = nullptr;
-    OS_TRY(lean_maps(h, set, lean_rows(config), &maps));
     p.x_chunk = std::min<int32_t>(p.x_chunk, EM3D_LEAN_MAX_PLANES - 1);
     if (h->ca_one)
-        return h->h_uniform ? launch_lean_ca<true, true>(config, p, in, *maps, s)
-                            : launch_lean_ca<true, false>(config, p, in, *maps, s);
-    return h->h_uniform ? launch_lean_ca<false, true>(config, p, in, *maps, s)
-                        : launch_lean_ca<false, false>(config, p, in, *maps, s);
+        return h->h_uniform ? launch_lean_ca<true, true>(h, set, config, p, in, s)
+                            : launch_lean_ca<true, false>(h, set, config, p, in, s);
+    return h->h_uniform ? launch_lean_ca<false, true>(h, set, config, p, in, s)
+                        : launch_lean_ca<false, false>(h, set, config, p, in, s);
 }
 
 template <int TY, int MINB>

@@ -45,16 +45,19 @@
 constexpr int EM3D_LV = 4;                     // cells per thread along k
 constexpr int EM3D_LTILE = 32 * EM3D_LV;       // cells of a warp row (128)
 
-template <int TY>
+// Boxes of one plane: E and ids TY + 1 rows, H TY rows from the tile's first row (its halo row j0 - 1); with NX (no
+// exchange: every warp computes the H of the row below its own) one more row of each.
+template <int TY, bool NX = false>
 struct Em3DLeanLayout {   // byte offsets inside one ring slot, every box on a 128-byte boundary
     static constexpr int WE = 136, WH = 132, WM = 144;
-    static constexpr int e_bytes = em3d_round128((TY + 1) * WE * 4);
-    static constexpr int h_bytes = em3d_round128(TY * WH * 4);
-    static constexpr int m_bytes = em3d_round128((TY + 1) * WM * 2);
+    static constexpr int ER = TY + 1 + (NX ? 1 : 0), HR = TY + (NX ? 1 : 0), MR = ER;   // box rows
+    static constexpr int e_bytes = em3d_round128(ER * WE * 4);
+    static constexpr int h_bytes = em3d_round128(HR * WH * 4);
+    static constexpr int m_bytes = em3d_round128(MR * WM * 2);
     static constexpr int e_off = 0, h_off = 3 * e_bytes, m_off = h_off + 3 * h_bytes;
     static constexpr int slot = m_off + m_bytes;
-    static constexpr uint32_t tx = (uint32_t)(3 * (TY + 1) * WE * 4 + 3 * TY * WH * 4 + (TY + 1) * WM * 2);
-    static constexpr int xch = 2 * TY * 128 * 4;   // one parity of one exchanged H component
+    static constexpr uint32_t tx = (uint32_t)(3 * ER * WE * 4 + 3 * HR * WH * 4 + MR * WM * 2);
+    static constexpr int xch = NX ? 0 : 2 * TY * 128 * 4;   // one parity of one exchanged H component
 };
 
 constexpr int EM3D_LEAN_MAX_PLANES = 64;       // x planes of one block's chunk, the halo plane included
@@ -63,19 +66,19 @@ constexpr int EM3D_LEAN_MAX_ZROWS = 255;       // z CPML rows (one byte per cell
 // Shared memory of one lean block, every region on a 16-byte boundary (the ring on 128): ring, exchanged H (two
 // parities), mbarriers, z CPML coefficients (b_h, g_h, b_e, g_e per z row; 16-byte vectors of four rows), per-plane
 // scalars, the tile's z inverse spacings (H then E).
-template <int TY, int RING>
+template <int TY, int RING, bool NX = false>
 struct Em3DLeanSmem {
-    static constexpr size_t xch = Em3DLeanLayout<TY>::slot * (size_t)RING;
-    static constexpr size_t bars = xch + 2 * (size_t)Em3DLeanLayout<TY>::xch;
+    static constexpr size_t xch = Em3DLeanLayout<TY, NX>::slot * (size_t)RING;
+    static constexpr size_t bars = xch + 2 * (size_t)Em3DLeanLayout<TY, NX>::xch;
     static constexpr size_t zc = bars + (RING * sizeof(uint64_t) + 15) / 16 * 16;
     __host__ __device__ static constexpr size_t plane(int z_rows) { return zc + 16 * (size_t)z_rows; }
     __host__ __device__ static constexpr size_t kz(int z_rows) { return plane(z_rows) + EM3D_LEAN_MAX_PLANES * 40; }
     __host__ __device__ static constexpr size_t bytes(int z_rows) { return kz(z_rows) + 2 * EM3D_LTILE * 4; }
 };
 
-template <int TY, int RING>
+template <int TY, int RING, bool NX = false>
 __host__ __device__ constexpr size_t em3d_lean_smem(int z_rows) {
-    return Em3DLeanSmem<TY, RING>::bytes(z_rows);
+    return Em3DLeanSmem<TY, RING, NX>::bytes(z_rows);
 }
 
 // Tensor maps of one lean launch: E and H components of the field set read, ids.
@@ -138,10 +141,10 @@ __device__ __forceinline__ void lv_down(const float2 (&v)[2], float prev, float2
 }
 
 // The seven copies of one plane into one slot (warp 0; lane 0 arms the barrier first).
-template <int TY>
+template <int TY, bool NX>
 __device__ __forceinline__ void em3d_lean_issue(const Em3DLeanMaps &maps, unsigned char *slot, uint64_t *bar,
                                                 int plane, int j_row0, int ke, int km, int lane) {
-    using L = Em3DLeanLayout<TY>;
+    using L = Em3DLeanLayout<TY, NX>;
     if (lane == 0) tb_mbar_expect_tx(bar, L::tx);
     __syncwarp();
     if (lane < 3) em3d_tensor_g2s(slot + L::e_off + lane * L::e_bytes, &maps.e[lane], ke, j_row0, plane, bar);
@@ -179,13 +182,13 @@ __device__ __forceinline__ void lv_store(float *ptr, const float2 (&v)[2], unsig
         if (mask & (1u << c)) ptr[c] = lv_get(v, c);
 }
 
-template <int TY, int RING, int MINB, bool CA1, bool HU, bool EARLY>
+template <int TY, int RING, int MINB, bool CA1, bool HU, bool EARLY, bool NX>
 __global__ void __launch_bounds__(32 * TY, MINB)
     em3d_lean_kernel(const Em3DParams p, const Em3DBox in, const __grid_constant__ Em3DLeanMaps maps) {
-    using L = Em3DLeanLayout<TY>;
+    using L = Em3DLeanLayout<TY, NX>;
     extern __shared__ __align__(128) unsigned char em3d_lean_smem_buf[];
     unsigned char *const ring = em3d_lean_smem_buf;
-    using S = Em3DLeanSmem<TY, RING>;
+    using S = Em3DLeanSmem<TY, RING, NX>;
     float *const s_hx = reinterpret_cast<float *>(ring + S::xch);   // [2][TY][128]
     float *const s_hz = s_hx + 2 * TY * 128;
     uint64_t *const bar = reinterpret_cast<uint64_t *>(ring + S::bars);
@@ -196,8 +199,10 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     const int kt0 = (in.k0 & ~3) + (int)blockIdx.x * EM3D_LTILE;  // the tile's first cell
     const int kv = kt0 + EM3D_LV * lane;                         // this thread's first cell (may be off the grid)
     const int ks = min(max(kv, 0), p.nz - EM3D_LV);              // the same, clamped: global addresses
-    const int j_row0 = in.j0 - 1 + (int)blockIdx.y * (TY - 1);   // the tile's first row (the halo)
-    const int jj = j_row0 + w;
+    // the boxes' first row: the halo row below the tile's first output row
+    const int j_row0 = in.j0 - 1 + (int)blockIdx.y * (NX ? TY : TY - 1);
+    const int rb = NX ? w + 1 : w;                               // this warp's row in the boxes
+    const int jj = j_row0 + rb;
     const int j = min(jj, in.j1 - 1);
     const int i_first = in.i0 + (int)blockIdx.z * p.x_chunk;
     const int i_last = min(in.i1, i_first + p.x_chunk);
@@ -208,15 +213,15 @@ __global__ void __launch_bounds__(32 * TY, MINB)
 #pragma unroll
     for (int c = 0; c < 4; ++c)
         if (kv + c >= in.k0 && kv + c < in.k1) kmask |= 1u << c;
-    if (w == 0 || jj >= in.j1) kmask = 0;
+    if ((!NX && w == 0) || jj >= in.j1) kmask = 0;
     const bool vec = __all_sync(0xffffffffu, kmask == 0u || kmask == 0xFu);
     // the box reaches the z edges only on an open z axis: the thread holding row 0 / row nz - 1
     const bool first = in.k0 == 0 && kv == 0, last = in.k1 == p.nz && kv + EM3D_LV == p.nz;
     const size_t sx = (size_t)p.ny * p.nz;
     const int o = j * p.nz + ks;                                 // in-plane offset of the thread's vector
-    const int at_e = w * L::WE + EM3D_LV + EM3D_LV * lane;       // the vector in an E box row
-    const int at_h = w * L::WH + EM3D_LV + EM3D_LV * lane;
-    const int at_m = w * L::WM + (kt0 - km) + EM3D_LV * lane;
+    const int at_e = rb * L::WE + EM3D_LV + EM3D_LV * lane;      // the vector in an E box row
+    const int at_h = rb * L::WH + EM3D_LV + EM3D_LV * lane;
+    const int at_m = rb * L::WM + (kt0 - km) + EM3D_LV * lane;
     const bool halo = lane == 0 && kt0 > 0;                      // lane 0 also computes H_x, H_y of cell kt0 - 1
     const int base = i_first - 1;
     if (tid == 0) {
@@ -254,7 +259,7 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     __syncthreads();
     if (w == 0)
         for (int q = 0; q < RING && base + q <= i_last; ++q)
-            em3d_lean_issue<TY>(maps, ring + q * L::slot, bar + q, base + q, j_row0, ke, km, lane);
+            em3d_lean_issue<TY, NX>(maps, ring + q * L::slot, bar + q, base + q, j_row0, ke, km, lane);
     const int n_issued_max = i_last - base + 1;
     // per-row and per-cell spacings; CPML rows of the row (y) and of the cells (z, one byte each, 0xff: none)
     const float2 ihy2 = lp_dup(p.ihy[j]), iey2 = lp_dup(p.iey[j]);
@@ -276,6 +281,11 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     const int32_t ryh = p.cpml[1].nr ? p.cpml[1].rm_h[j] : -1, rye = p.cpml[1].nr ? p.cpml[1].rm_e[j] : -1;
     const float2 byh = lp_dup(ryh >= 0 ? p.cpml[1].b_h[ryh] : 0.0f), gyh = lp_dup(ryh >= 0 ? p.cpml[1].g_h[ryh] : 0.0f);
     const float2 bye = lp_dup(rye >= 0 ? p.cpml[1].b_e[rye] : 0.0f), gye = lp_dup(rye >= 0 ? p.cpml[1].g_e[rye] : 0.0f);
+    // NX: the row below (j - 1): its inverse spacing and y CPML row (H map)
+    const int jb = max(j - 1, 0);
+    const float ihyb = NX ? p.ihy[jb] : 0.0f;
+    const int32_t ryb = NX && p.cpml[1].nr ? p.cpml[1].rm_h[jb] : -1;
+    const float byb = ryb >= 0 ? p.cpml[1].b_h[ryb] : 0.0f, gyb = ryb >= 0 ? p.cpml[1].g_h[ryb] : 0.0f;
     const uint32_t id_max = (uint32_t)(p.n_ids - 1);
     const float *__restrict__ t_same = p.t_same;
     float *__restrict__ oex = p.oex;
@@ -294,14 +304,29 @@ __global__ void __launch_bounds__(32 * TY, MINB)
         const int q = i - base;
         const unsigned char *cur = ring + cs * L::slot;
         const unsigned char *nxt = ring + ns * L::slot;
-        if (EARLY) {
+        if (NX) {
+            // every warp is done with plane i - 1 (and every wait so far succeeded): its slot takes plane
+            // i + RING - 1 now, a whole plane before it is read
+            if (__syncthreads_or(!ok)) {   // a wait ran out somewhere in the block: stop, after the copies in flight
+                if (tid == 0) atomicExch(p.err, 1);
+                if (w == 0)   // positions q (its wait ran out, maybe) .. q + RING - 2 may be in flight
+                    for (int qq = q; qq < min(n_issued_max, q + RING - 1); ++qq)
+                        tb_mbar_wait(bar + qq % RING, (uint32_t)((qq / RING) & 1));
+                return;
+            }
+            if (w == 0 && q >= 1 && i + RING - 1 <= i_last) {
+                const int ps = cs == 0 ? RING - 1 : cs - 1;
+                tb_fence_proxy_async();
+                em3d_lean_issue<TY, NX>(maps, ring + ps * L::slot, bar + ps, i + RING - 1, j_row0, ke, km, lane);
+            }
+        } else if (EARLY) {
             // every warp is done with plane i - 1: its slot takes plane i + RING - 1 now, a whole plane before it is
             // read
             __syncthreads();
             if (w == 0 && q >= 1 && i + RING - 1 <= i_last) {
                 const int ps = cs == 0 ? RING - 1 : cs - 1;
                 tb_fence_proxy_async();
-                em3d_lean_issue<TY>(maps, ring + ps * L::slot, bar + ps, i + RING - 1, j_row0, ke, km, lane);
+                em3d_lean_issue<TY, NX>(maps, ring + ps * L::slot, bar + ps, i + RING - 1, j_row0, ke, km, lane);
             }
         }
         ok = tb_mbar_wait(bar + ns, nph) && ok;
@@ -441,10 +466,12 @@ __global__ void __launch_bounds__(32 * TY, MINB)
         lv_store(ohy + bo, vhy, smask, vec);
         lv_store(ohz + bo, vhz, smask, vec);
         float *const xhx = s_hx + par * TY * 128, *const xhz = s_hz + par * TY * 128;
-        *reinterpret_cast<float4 *>(xhx + w * 128 + EM3D_LV * lane) = make_float4(vhx[0].x, vhx[0].y, vhx[1].x,
-                                                                                 vhx[1].y);
-        *reinterpret_cast<float4 *>(xhz + w * 128 + EM3D_LV * lane) = make_float4(vhz[0].x, vhz[0].y, vhz[1].x,
-                                                                                 vhz[1].y);
+        if constexpr (!NX) {
+            *reinterpret_cast<float4 *>(xhx + w * 128 + EM3D_LV * lane) = make_float4(vhx[0].x, vhx[0].y, vhx[1].x,
+                                                                                     vhx[1].y);
+            *reinterpret_cast<float4 *>(xhz + w * 128 + EM3D_LV * lane) = make_float4(vhz[0].x, vhz[0].y, vhz[1].x,
+                                                                                     vhz[1].y);
+        }
         // H^{n+1/2} of cell k - 1 (lane - 1; lane 0: the halo cell kt0 - 1); below row 0 of the open z axis, 0:
         // F - 0 is F, em3d_lo_diff's value
         float hx_prev = __shfl_up_sync(0xffffffffu, vhx[1].y, 1);
@@ -479,24 +506,109 @@ __global__ void __launch_bounds__(32 * TY, MINB)
             hx_prev = hx;
             hy_prev = hy;
         }
-        if (__syncthreads_or(!ok)) {   // a wait ran out somewhere in the block: stop, after the copies in flight
-            if (tid == 0) atomicExch(p.err, 1);
-            if (w == 0)
-                for (int qq = q + 1; qq < min(n_issued_max, q + RING - 1); ++qq)
-                    tb_mbar_wait(bar + qq % RING, (uint32_t)((qq / RING) & 1));
-            return;
+        float2 hzy[2], hxy[2];   // H^{n+1/2} of row j - 1 (H_z, H_x)
+        if constexpr (NX) {   // evaluated here from the staged row below (its psi read, not stored)
+            float2 exb[2], eyb[2], ezb[2], eynb[2], hxb0[2], hzb0[2], eykb[2];
+            lv_lds(ce0 + at_e - L::WE, exb);
+            lv_lds(ce1 + at_e - L::WE, eyb);
+            lv_lds(ce2 + at_e - L::WE, ezb);
+            lv_lds(ne1 + at_e - L::WE, eynb);
+            lv_lds(ch + at_h - L::WH, hxb0);
+            lv_lds(ch + 2 * (L::h_bytes / 4) + at_h - L::WH, hzb0);
+            float eyn4b = ce1[at_e - L::WE + 4];
+            if (last) eyn4b = em3d_wrapped(__ldg(p.ey + (bo - ks - p.nz)));
+            lv_up(eyb, eyn4b, eykb);
+            float2 dab[2], dbb[2];
+            if (hu) {
+                dab[0] = dab[1] = lp_dup(p.da_u);
+                dbb[0] = dbb[1] = lp_dup(p.db_u);
+            } else {
+                const uint2 mbv = *reinterpret_cast<const uint2 *>(
+                    reinterpret_cast<const uint16_t *>(cur + L::m_off) + at_m - L::WM);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const uint32_t m = min(lv_id(mbv, c), id_max);
+                    lv_set(dab, c, __ldg(p.t_da + m));
+                    lv_set(dbb, c, __ldg(p.t_db + m));
+                }
+            }
+            const float2 ihyb2 = lp_dup(ihyb);
+            float2 dez_yb[2], dey_zb[2], dey_xb[2], dex_yb[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                dez_yb[h] = lp_sub(ez0[h], ezb[h]);
+                dey_zb[h] = lp_sub(eykb[h], eyb[h]);
+                dey_xb[h] = lp_sub(eynb[h], eyb[h]);
+                dex_yb[h] = lp_sub(ex0[h], exb[h]);
+                hxy[h] = ls_sub(lp_mul(dab[h], hxb0[h]),
+                                lp_mul(dbb[h], ls_sub(lp_mul(dez_yb[h], ihyb2), lp_mul(dey_zb[h], ihz[h]))));
+                hzy[h] = ls_sub(lp_mul(dab[h], hzb0[h]),
+                                lp_mul(dbb[h], ls_sub(lp_mul(dey_xb[h], ihx2), lp_mul(dex_yb[h], ihyb2))));
+            }
+            if (pl.rh >= 0) {   // x layers: H_z from E_y (-)
+                const size_t qq = (size_t)pl.rh * sx + (o - p.nz);
+                const float2 bb = lp_dup(pl.bh), gg = lp_dup(pl.gh);
+                float2 pg[2];
+                lv_ldg(p.cpml[0].ph_second + qq, pg);
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                    hzy[h] = ls_sub(hzy[h], lp_mul(dbb[h], ls_add(lp_mul(bb, pg[h]), lp_mul(gg, dey_xb[h]))));
+            }
+            if (ryb >= 0) {   // y layers: H_x from E_z (-), H_z from E_x (+)
+                const size_t qq = ((size_t)i * p.cpml[1].nr + ryb) * p.nz + ks;
+                const float2 bb = lp_dup(byb), gg = lp_dup(gyb);
+                float2 pf[2], pg[2];
+                lv_ldg(p.cpml[1].ph_first + qq, pf);
+                lv_ldg(p.cpml[1].ph_second + qq, pg);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    hxy[h] = ls_sub(hxy[h], lp_mul(dbb[h], ls_add(lp_mul(bb, pf[h]), lp_mul(gg, dez_yb[h]))));
+                    hzy[h] = ls_add(hzy[h], lp_mul(dbb[h], ls_add(lp_mul(bb, pg[h]), lp_mul(gg, dex_yb[h]))));
+                }
+            }
+            if (zvh) {   // z layers, four consecutive rows: H_x from E_y (+)
+                const int r0 = (int)(zrh & 0xffu);
+                const size_t qq = ((size_t)i * p.ny + jb) * nrz + r0;
+                float2 pf[2], bz[2], gz[2];
+                lv_ldg(p.cpml[2].ph_first + qq, pf);
+                lv_lds(s_zc + r0, bz);
+                lv_lds(s_zc + nrz + r0, gz);
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                    hxy[h] = ls_add(hxy[h], lp_mul(dbb[h], ls_add(lp_mul(bz[h], pf[h]), lp_mul(gz[h], dey_zb[h]))));
+            } else if (zrh != 0xffffffffu) {   // z layers, per cell
+                const size_t zb = ((size_t)i * p.ny + jb) * nrz;
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) {
+                    const uint32_t r = (zrh >> (8 * cc)) & 0xffu;
+                    if (r == 0xffu) continue;
+                    const float f = __fadd_rn(__fmul_rn(s_zc[r], p.cpml[2].ph_first[zb + r]),
+                                              __fmul_rn(s_zc[nrz + r], lv_get(dey_zb, cc)));
+                    lv_set(hxy, cc, __fadd_rn(lv_get(hxy, cc), __fmul_rn(lv_get(dbb, cc), f)));
+                }
+            }
+        } else {
+            if (__syncthreads_or(!ok)) {   // a wait ran out somewhere in the block: stop, after the copies in flight
+                if (tid == 0) atomicExch(p.err, 1);
+                if (w == 0)
+                    for (int qq = q + 1; qq < min(n_issued_max, q + RING - 1); ++qq)
+                        tb_mbar_wait(bar + qq % RING, (uint32_t)((qq / RING) & 1));
+                return;
+            }
+            // no thread reads the slot of plane i - 1 any more: it takes plane i + RING - 1
+            if (!EARLY && w == 0 && q >= 1 && i + RING - 1 <= i_last) {
+                const int ps = cs == 0 ? RING - 1 : cs - 1;
+                tb_fence_proxy_async();
+                em3d_lean_issue<TY, NX>(maps, ring + ps * L::slot, bar + ps, i + RING - 1, j_row0, ke, km, lane);
+            }
+            if (w > 0) {
+                lv_lds(xhz + (w - 1) * 128 + EM3D_LV * lane, hzy);   // H^{n+1/2} of row j - 1, from the warp below
+                lv_lds(xhx + (w - 1) * 128 + EM3D_LV * lane, hxy);
+            }
         }
-        // no thread reads the slot of plane i - 1 any more: it takes plane i + RING - 1
-        if (!EARLY && w == 0 && q >= 1 && i + RING - 1 <= i_last) {
-            const int ps = cs == 0 ? RING - 1 : cs - 1;
-            tb_fence_proxy_async();
-            em3d_lean_issue<TY>(maps, ring + ps * L::slot, bar + ps, i + RING - 1, j_row0, ke, km, lane);
-        }
-        if (w > 0 && inside) {
+        if ((NX || w > 0) && inside) {
             // ---- E^{n+1} of the thread's four cells
-            float2 hzy[2], hxy[2], hxk[2], hyk[2];
-            lv_lds(xhz + (w - 1) * 128 + EM3D_LV * lane, hzy);   // H^{n+1/2} of row j - 1
-            lv_lds(xhx + (w - 1) * 128 + EM3D_LV * lane, hxy);
+            float2 hxk[2], hyk[2];
             lv_down(vhx, hx_prev, hxk);
             lv_down(vhy, hy_prev, hyk);
             const uint16_t *cm = reinterpret_cast<const uint16_t *>(cur + L::m_off);
@@ -641,6 +753,14 @@ __global__ void __launch_bounds__(32 * TY, MINB)
         cs = ns;
         ns = ns + 1 == RING ? 0 : ns + 1;
         nph ^= ns == 0 ? 1u : 0u;
+    }
+    if constexpr (NX) {   // the last plane's wait is checked here
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicExch(p.err, 1);
+            if (w == 0)
+                for (int qq = max(0, n_issued_max - RING); qq < n_issued_max; ++qq)
+                    tb_mbar_wait(bar + qq % RING, (uint32_t)((qq / RING) & 1));
+        }
     }
     // the last staged plane (i_last) was waited in the last iteration; nothing is in flight
 }

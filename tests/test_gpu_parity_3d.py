@@ -116,7 +116,7 @@ def test_step_forms_bit_identical(spec):
     shape = grid_shape(spec)
     lean = shape[2] % 4 == 0 and shape[2] >= 144 and shape[1] >= 17
     runs = []
-    for variant, config in ((0, 0), (1, 0), (1, 1), (1, 2), (1, 3), (1, 4), (3, 0), (3, 1), (3, 2), (3, 3)):
+    for variant, config in ((0, 0), (1, 0), (1, 1), (1, 2), (1, 3), (1, 4), (3, 0), (3, 1), (3, 2), (3, 3), (3, 4)):
         physics, monitors = build_product(spec)
         engine = physics.engine
         engine.set_variant(variant)
@@ -262,7 +262,8 @@ def test_lean_form_bit_identical(total):
     from opensol_b200 import workloads
     n_spheres = max(1, int(round(500 * (total / 512) ** 3)))
     runs = []
-    for variant, config, chunk in ((0, 0, 24), (3, 0, 24), (3, 1, 7), (3, 2, 1), (3, 3, 50), (3, -1, 2), (3, 3, 63)):
+    for variant, config, chunk in ((0, 0, 24), (3, 0, 24), (3, 1, 7), (3, 2, 1), (3, 3, 50), (3, -1, 2), (3, 3, 63),
+                                   (3, 4, 24), (3, 4, 1), (3, 4, 63)):
         physics, box = workloads.roofline_3d_physics(total_cells=total, n_spheres=n_spheres)
         physics.finalize()
         engine = physics.engine
