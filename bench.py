@@ -65,6 +65,7 @@ def parse_args():
                    help='em3d: step form (0 two in-place kernels, 1 fused on two field sets, 2 fused with staged '
                         'planes, 3 lean staged fused pass); results are the same bits')
     p.add_argument('--x-chunk', type=int, default=0, help='em3d: x planes per block (0: the engine\'s choice)')
+    p.add_argument('--hz-steps', type=int, default=1, choices=[1, 2], help='hz2d: Yee steps per interior launch')
     p.add_argument('--fused-config', type=int, default=-1,
                    help="em3d: launch shape of the fused forms (0..4; -1: the form's default)")
     return p.parse_args()
@@ -391,7 +392,7 @@ def run_hz2d(args):
     sim = ob.Simulation(**workloads.roofline_2d_sim_args(total_cells=args.grid), polarization='hz', verbose=False)
     monitors = workloads.apply(sim, workloads.roofline_2d_ops(total_cells=args.grid))
     variant = args.variant if args.variant in (0, 1) else 1
-    sim.em.engine.configure(variant=variant, steps_per_launch=1, tile_rows=args.tile_rows)
+    sim.em.engine.configure(variant=variant, steps_per_launch=args.hz_steps, tile_rows=args.tile_rows)
     sim.em.finalize()
     engine = sim.em.engine
     # a stream of its own (torch's default stream is handle 0, which os_fdtd*_set_stream reads as "the engine's own
@@ -428,7 +429,7 @@ def run_hz2d(args):
     interior_cells, border_cells = engine.hz_plan()
     if engine.variant == 1 and interior_cells:
         name = engine.KERNEL_KINDS[0]
-        units = interior_cells
+        units = interior_cells * engine.steps_per_launch   # cell-updates of one interior launch
     else:
         name = engine.KERNEL_KINDS[3 if engine.variant == 0 else 1]
         units = cells
@@ -454,7 +455,8 @@ def run_hz2d(args):
                                    'dx 20 nm, 2000 seeded cylinders eps_r U(2,12), 1550 nm E_y sheet source, '
                                    f'4 x 16-frequency flux lines, {args.sim_steps} Yee steps per bench step',
                        'grid': [args.grid, args.grid], 'sim_steps': args.sim_steps,
-                       'kernel': {'variant': engine.variant, 'rows_per_cta': engine.tile_rows},
+                       'kernel': {'variant': engine.variant, 'rows_per_cta': engine.tile_rows,
+                                  'steps_per_launch': engine.steps_per_launch},
                        'l2': 'inputs larger than L2 (fields 3 x 268 MB), no flush'},
             'roofline': roofline, 'gpu_launches': launches, 'clocks': clocks.summary()}
     sim.clear()

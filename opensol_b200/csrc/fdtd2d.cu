@@ -16,6 +16,7 @@
 #include "fdtd2d_tb.cuh"
 #include "fdtd2d_interior.cuh"
 #include "fdtd2d_hz.cuh"
+#include "fdtd2d_hz2.cuh"
 #include "fdtd2d_frame.cuh"
 
 #include <algorithm>
@@ -1494,8 +1495,113 @@ static int launch_hz_step(OsFdtd2D *h, const HzPlan &q, Hz2DParams p) {
     return OS_OK;
 }
 
+// The two-step H_z launch's split: the interior box of hz2d_interior2_kernel (the single-step box less one row and four
+// columns on each side, so that its two-step cone holds plain updates only) and the border's two regions: step 1 over
+// the grid minus the box shrunk by one cell (its step-1 state, which step 2 reads around every cell it updates, goes to
+// the scratch set), step 2 over the grid minus the box.
+struct HzPlan2 {
+    bool interior = false;
+    int ia = 0, ib = 0, jc0 = 0, jc1 = 0;
+    HzBorderRects rects1{}, rects2{};
+};
+
+// The grid minus rows [r0, r1) x columns [c0, c1) as up to four rectangles (the whole grid when the box is empty).
+static HzBorderRects hz_frame_rects(const OsFdtd2D *h, int r0, int r1, int c0, int c1) {
+    const int nx = h->grid.nx, ny = h->grid.ny;
+    HzBorderRects q{};
+    int n = 0;
+    auto add = [&](int a0, int a1, int b0, int b1) {
+        if (a1 <= a0 || b1 <= b0) return;
+        q.r0[n] = a0, q.r1[n] = a1, q.c0[n] = b0, q.c1[n] = b1;
+        ++n;
+    };
+    if (r1 > r0 && c1 > c0) {
+        add(0, r0, 0, ny);
+        add(r1, nx, 0, ny);
+        add(r0, r1, 0, c0);
+        add(r0, r1, c1, ny);
+    } else {
+        add(0, nx, 0, ny);
+    }
+    q.n = n;
+    q.first[0] = 0;
+    for (int k = 0; k < n; ++k)
+        q.first[k + 1] = q.first[k] + (int64_t)(q.r1[k] - q.r0[k]) * (q.c1[k] - q.c0[k]);
+    for (int k = n; k < 4; ++k) q.first[k + 1] = q.first[n];
+    return q;
+}
+
+static HzPlan2 hz_plan2(const OsFdtd2D *h) {
+    const HzPlan q1 = hz_plan(h);
+    HzPlan2 q;
+    q.ia = q1.ia + 1;
+    q.ib = q1.ib - 1;
+    q.jc0 = q1.jc0 + 4;
+    q.jc1 = q1.jc1 - 4;
+    // the kernel's form: lossless (face coefficients from eps_r), rows a multiple of 4 cells (TMA-staged windows)
+    q.interior = q1.interior && q.ib > q.ia && q.jc1 > q.jc0 && h->hz_eps && h->grid.ny % 4 == 0;
+    if (q.interior) {
+        q.rects1 = hz_frame_rects(h, q.ia + 1, q.ib - 1, q.jc0 + 1, q.jc1 - 1);
+        q.rects2 = hz_frame_rects(h, q.ia, q.ib, q.jc0, q.jc1);
+    }
+    return q;
+}
+
+// Two fused H_z steps from set `in` to set `out` (p.k_step: the first step's column of the source tables): the
+// border's two single steps through the scratch set on the side stream, the interior's two-step kernel on the main
+// stream; they write disjoint cells of the output set.
+static int launch_hz_step2(OsFdtd2D *h, const HzPlan2 &q, const Hz2DParams &p) {
+    const bool fork = !h->profiling;   // profiling: each kernel timed alone
+    cudaStream_t bstream = fork ? h->side_stream : h->stream;
+    if (fork) {
+        OS_CUDA(cudaEventRecord(h->ev_fork, h->stream));
+        OS_CUDA(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
+    }
+    Hz2DParams b1 = p, b2 = p;
+    b1.hz_out = h->sez[0].ptr, b1.ex_out = h->shx[0].ptr, b1.ey_out = h->shy[0].ptr;
+    b2.hz_in = h->sez[0].ptr, b2.ex_in = h->shx[0].ptr, b2.ey_in = h->shy[0].ptr;
+    b2.k_step = p.k_step + 1;
+    for (int sd = 0; sd < 4; ++sd) {
+        if (!(p.cpml_mask & (1 << sd))) continue;
+        b1.psi_e_out[sd] = h->spsi_e[0][sd].ptr, b1.psi_h_out[sd] = h->spsi_h[0][sd].ptr;
+        b2.psi_e_in[sd] = h->spsi_e[0][sd].ptr, b2.psi_h_in[sd] = h->spsi_h[0][sd].ptr;
+    }
+    const Hz2DParams *bp[2] = {&b1, &b2};
+    const HzBorderRects *br[2] = {&q.rects1, &q.rects2};
+    for (int st = 0; st < 2; ++st) {
+        const int64_t cells_b = br[st]->first[br[st]->n];
+        if (cells_b <= 0) continue;
+        OS_TRY(prof_begin(h, 1, bstream));
+        hz2d_border_kernel<true><<<(unsigned)((cells_b + 255) / 256), 256, 0, bstream>>>(*bp[st], *br[st]);
+        OS_TRY(prof_end(h, bstream));
+        h->launches += 1;
+    }
+    Hz2DParams pi = p;
+    pi.ia = q.ia, pi.ib = q.ib, pi.jc0 = q.jc0, pi.jc1 = q.jc1;
+    {
+        const int64_t warps = (q.jc1 - q.jc0 + 127) / 128;
+        const int64_t ctas_x = (warps + HZ_THREADS / 32 - 1) / (HZ_THREADS / 32);
+        const int64_t want = (int64_t)h->sm_count * 4 * 4;   // about four waves of four CTAs per SM
+        int64_t rows = h->hz_rows > 0 ? h->hz_rows : ((int64_t)(q.ib - q.ia) * ctas_x + want - 1) / want;
+        pi.rows_per_cta = (int32_t)std::max<int64_t>(h->hz_rows > 0 ? 1 : 16, std::min<int64_t>(128, rows));
+    }
+    const dim3 grid((unsigned)((q.jc1 - q.jc0 + 128 * (HZ_THREADS / 32) - 1) / (128 * (HZ_THREADS / 32))),
+                    (unsigned)((q.ib - q.ia + pi.rows_per_cta - 1) / pi.rows_per_cta));
+    OS_TRY(prof_begin(h, 0, h->stream));
+    hz2d_interior2_kernel<<<grid, HZ_THREADS, (HZ_THREADS / 32) * hz_warp_smem_bytes(), h->stream>>>(pi, h->err.ptr);
+    OS_TRY(prof_end(h, h->stream));
+    h->launches += 1;
+    if (fork) {
+        OS_CUDA(cudaEventRecord(h->ev_join, h->side_stream));
+        OS_CUDA(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+    }
+    return OS_OK;
+}
+
 // H_z chunk: variant 0 launches the in-place H and E kernels per step, otherwise one fused step kernel per step
-// (buffers swapped after each); the flux lines are sampled after every step that is a sample step.
+// (buffers swapped after each), or with steps_per_launch 2 two steps per launch wherever the next step is not a
+// sampled one (the flux lines and field maps are sampled after every sample step, so a sample step ends a launch);
+// field probes, which record every step, keep one step per launch.
 static int advance_hz(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples, const float *values,
                       const float *phase_table) {
     const int64_t m = h->sample_interval;
@@ -1504,14 +1610,23 @@ static int advance_hz(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_
     const dim3 cell_grid((unsigned)((ny + cell_block.x - 1) / cell_block.x),
                          (unsigned)((nx + cell_block.y - 1) / cell_block.y));
     const HzPlan plan = hz_plan(h);
+    const bool per_half = h->variant == 0 || !h->tfsf.empty() || !h->poles.empty();
+    const bool sampled = !h->fluxes.empty() || !h->maps.empty();
+    HzPlan2 plan2;
+    const bool two = !per_half && h->steps_per_launch == 2 && h->sez[0].ptr && h->probes.n == 0 &&
+                     (plan2 = hz_plan2(h)).interior;
     for (int64_t k = 0; k < n_steps; ++k) {
-        const bool per_half = h->variant == 0 || !h->tfsf.empty() || !h->poles.empty();
         const int in = h->cur, out = per_half ? h->cur : h->cur ^ 1;
         Hz2DParams p = make_hz_params(h, in, out);
         p.line_values = values;
         p.values_stride = n_steps;
         p.k_step = k;
-        if (per_half) {   // a TFSF box and the poles act between the half steps
+        int64_t advanced = 1;
+        if (two && k + 1 < n_steps && !(sampled && (h->n_step + 1) % m == 0)) {   // steps k and k + 1 in one launch
+            OS_TRY(launch_hz_step2(h, plan2, p));
+            advanced = 2;
+            k += 1;
+        } else if (per_half) {   // a TFSF box and the poles act between the half steps
             OS_TRY(prof_begin(h, 3, h->stream));
             hz2d_h_kernel<<<cell_grid, cell_block, 0, h->stream>>>(p);
             for (auto &t : h->tfsf) {   // TFSFSourceHz.inject_magnetic (fdtd_hz_2d.py:160-163)
@@ -1557,7 +1672,7 @@ static int advance_hz(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_
             OS_TRY(launch_hz_step(h, plan, p));
         }
         h->cur = out;
-        h->n_step += 1;
+        h->n_step += advanced;
         if (!h->maps.empty() && h->n_step % m == 0)
             OS_TRY(fold_maps(h, nullptr, h->n_step / m, first_sample, n_samples, phase_table));
         if (h->probes.n) OS_TRY(record_probes(h));
@@ -1625,6 +1740,14 @@ static int run_chunk(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t
 extern "C" int os_fdtd2d_hz_plan(OsFdtd2D *h, int64_t *interior_cells, int64_t *border_cells) {
     OS_TRY(require_hz(h, "os_fdtd2d_hz_plan"));
     OS_CHECK(interior_cells && border_cells, OS_ERR_INVALID, "os_fdtd2d_hz_plan: null argument");
+    if (h->steps_per_launch == 2 && h->sez[0].ptr) {   // the two-step box (border: the cells outside it)
+        const HzPlan2 q = hz_plan2(h);
+        if (q.interior) {
+            *interior_cells = (int64_t)(q.ib - q.ia) * (q.jc1 - q.jc0);
+            *border_cells = q.rects2.first[q.rects2.n];
+            return OS_OK;
+        }
+    }
     const HzPlan q = hz_plan(h);
     *interior_cells = q.interior ? (int64_t)(q.ib - q.ia) * (q.jc1 - q.jc0) : 0;
     *border_cells = q.rects.first[q.rects.n];
@@ -1744,11 +1867,27 @@ extern "C" int os_fdtd2d_configure(OsFdtd2D *h, int32_t variant, int32_t steps_p
     OS_CHECK(steps_per_launch >= 1 && steps_per_launch <= TB_MAX_T, OS_ERR_INVALID,
              "steps_per_launch must be in [1, %d], got %d", TB_MAX_T, steps_per_launch);
     if (h->polarization == 1) {
-        // H_z: variant 0 per-half-step kernels, 1 the fused step kernel with tile_rows rows per CTA (0: per grid)
-        OS_CHECK(variant <= 1 && steps_per_launch == 1 && tile_rows >= 0, OS_ERR_INVALID,
-                 "an H_z engine takes variant 0 or 1, steps_per_launch 1 and tile_rows >= 0, got %d, %d, %d", variant,
-                 steps_per_launch, tile_rows);
+        // H_z: variant 0 per-half-step kernels, 1 the fused step kernel with tile_rows rows per CTA (0: per grid);
+        // steps_per_launch 2: the interior box advances two steps per launch (hz2d_interior2_kernel) where it applies
+        OS_CHECK(variant <= 1 && (steps_per_launch == 1 || steps_per_launch == 2) && tile_rows >= 0, OS_ERR_INVALID,
+                 "an H_z engine takes variant 0 or 1, steps_per_launch 1 or 2 and tile_rows >= 0, got %d, %d, %d",
+                 variant, steps_per_launch, tile_rows);
+        if (steps_per_launch == 2 && !h->sez[0].ptr) {   // the border's step-1 state (made here, not in an advance)
+            OS_TRY(bind_device(h));
+            const size_t n = cells(h);
+            OS_TRY(h->sez[0].alloc(n));
+            OS_TRY(h->shx[0].alloc(n));
+            OS_TRY(h->shy[0].alloc(n));
+            const OsGrid2D &g = h->grid;
+            for (int sd = 0; sd < 4; ++sd) {
+                if (!(g.cpml_sides & (1 << sd))) continue;
+                const size_t slab = (sd < 2 ? (size_t)g.ny : (size_t)g.nx) * (size_t)g.npml;
+                OS_TRY(h->spsi_e[0][sd].alloc(slab));
+                OS_TRY(h->spsi_h[0][sd].alloc(slab));
+            }
+        }
         h->variant = variant;
+        h->steps_per_launch = steps_per_launch;
         h->hz_rows = tile_rows;
         return OS_OK;
     }

@@ -1,0 +1,307 @@
+// Two-step interior kernel of the fused H_z step (lossless form, rows a multiple of 4 cells): two Yee steps per launch
+// for the cells of an interior box, reading field set a and writing set b, with every intermediate value in registers.
+//
+// The same warp strips, lanes and TMA row ring as hz2d_interior_kernel, and the same arithmetic term for term, in a
+// skewed two-stage pipeline: while streaming row r, stage 1 makes step 1 of row r (H_z^1(r), E_x^1(r)) and E_y^1 of
+// row r - 1; stage 2 makes step 2 one row behind (H_z^2(r - 1), E_x^2(r - 1), E_y^2(r - 2)).  A block streams rows
+// r0 - 1 .. r1 + 1 and stores step 2 of its rows [r0, r1).  Step 2's columns need step 1 one column beyond the strip
+// on each side: lane 0 makes H_z^1 and E_x^1 of column jw - 1, the strip's last lane H_z^1 of columns j_end and
+// j_end + 1, E_x^1 and E_y^1 of column j_end, and H_z^2 of column j_end; none of these is stored.  The sheet sources
+// of each step are added to the E values of that step, the halo columns' included.  A face's cb, computed by stage 1,
+// is kept for stage 2 one row later.  The host chooses the box so that every update in this cone is the plain one (no
+// CPML row, edge or wrap): the single-step box less one row and four columns on each side.  Every wait is bounded
+// (the ring's tb_mbar_wait).
+#pragma once
+
+#include "fdtd2d_hz.cuh"
+
+// Sheet sources of step `k` on the E_x face (r, j) (axis 0 lines: faces (r, position), r in [lo, hi)), added in line
+// order after the update, a zero value skipped, as hz_plain_e adds them.
+__device__ __forceinline__ float hz2_src_x(const Hz2DParams &p, int64_t k, int r, int j, float v) {
+    for (int l = 0; l < p.n_lines; ++l) {
+        const LineSrcDev &L = p.lines[l];
+        if (L.axis != 0 || L.position != j || r < L.lo || r >= L.hi) continue;
+        const float value = p.line_values[(size_t)l * p.values_stride + k];
+        if (value != 0.0f) v += value * L.profile[r - L.lo];
+    }
+    return v;
+}
+
+// The same on the E_y face (re, j) (axis 1 lines: faces (position, j), j in [lo, hi)).
+__device__ __forceinline__ float hz2_src_y(const Hz2DParams &p, int64_t k, int re, int j, float v) {
+    for (int l = 0; l < p.n_lines; ++l) {
+        const LineSrcDev &L = p.lines[l];
+        if (L.axis != 1 || L.position != re || j < L.lo || j >= L.hi) continue;
+        const float value = p.line_values[(size_t)l * p.values_stride + k];
+        if (value != 0.0f) v += value * L.profile[j - L.lo];
+    }
+    return v;
+}
+
+// The same for the lane's four E_x faces of row r (columns jt .. jt + 3) and four E_y faces of row re: each line is
+// tested once per row.
+__device__ __forceinline__ void hz2_src_x4(const Hz2DParams &p, int64_t k, int r, int jt, float (&v)[4]) {
+    for (int l = 0; l < p.n_lines; ++l) {
+        const LineSrcDev &L = p.lines[l];
+        if (L.axis != 0 || L.position < jt || L.position >= jt + 4 || r < L.lo || r >= L.hi) continue;
+        const float value = p.line_values[(size_t)l * p.values_stride + k];
+        if (value == 0.0f) continue;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            if (jt + c == L.position) v[c] += value * L.profile[r - L.lo];
+    }
+}
+__device__ __forceinline__ void hz2_src_y4(const Hz2DParams &p, int64_t k, int re, int jt, float (&v)[4]) {
+    for (int l = 0; l < p.n_lines; ++l) {
+        const LineSrcDev &L = p.lines[l];
+        if (L.axis != 1 || L.position != re || jt + 3 < L.lo || jt >= L.hi) continue;
+        const float value = p.line_values[(size_t)l * p.values_stride + k];
+        if (value == 0.0f) continue;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            if (jt + c >= L.lo && jt + c < L.hi) v[c] += value * L.profile[jt + c - L.lo];
+    }
+}
+
+// One plain H_z update: da H + db ((E_x - E_x left) iye - (E_y - E_y below) ixe).
+__device__ __forceinline__ float hz2_h(float da, float db, float h, float ex, float ex_left, float ey, float ey_below,
+                                       float iye, float ixe) {
+    const float dex = ex - ex_left;
+    const float dey = ey - ey_below;
+    float curl = dex * iye;
+    curl -= dey * ixe;
+    return da * h + db * curl;
+}
+
+// Plain E_x (lossless form): 1 E_x + cb (H_z right - H_z) iyh; cb = hz_cb_lossless of the face.
+__device__ __forceinline__ float hz2_ex(float ex, float bx, float h, float h_right, float iyh) {
+    const float dx = h_right - h;
+    return 1.0f * ex + bx * dx * iyh;
+}
+
+// Plain E_y (lossless form) of row re: 1 E_y - cb (H_z above - H_z) ixh.
+__device__ __forceinline__ float hz2_ey(float ey, float by, float h, float h_above, float ixh) {
+    const float dy = h_above - h;
+    return 1.0f * ey - by * dy * ixh;
+}
+
+__global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2DParams p, int32_t *err) {
+    extern __shared__ __align__(16) unsigned char hz_smem[];
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int jw = p.jc0 + (blockIdx.x * (HZ_THREADS / 32) + warp) * 128;
+    if (jw >= p.jc1) return;   // whole warp (its barriers are never used)
+    const int jt = jw + 4 * lane;
+    const int ny = p.ny;
+    const int r0 = p.ia + blockIdx.y * p.rows_per_cta;
+    if (r0 >= p.ib) return;
+    const int r1 = min(p.ib, r0 + p.rows_per_cta);
+    const int j_end = min(jw + 128, p.jc1);             // the strip's columns [jw, j_end)
+    const bool active = jt < j_end;
+    const int last_lane = (j_end - 1 - jw) / 4;
+    const bool halo_lane = lane == last_lane;
+    const bool left_lane = lane == 0;
+    const int R0 = r0 - 1, R1 = r1 + 1;                 // streamed rows R0 .. R1
+
+    HzStage st;
+    {
+        unsigned char *mine = hz_smem + warp * hz_warp_smem_bytes();
+        st.ring = reinterpret_cast<float *>(mine);
+        st.bar = reinterpret_cast<uint64_t *>(mine + HZ_SLOTS * 4 * HZ_WIN * 4);
+        st.jw = jw;
+        st.c_lo = max(jw - 4, 0);
+        st.c_hi = min(jw + 132, ny);
+        if (lane == 0) {
+            for (int s = 0; s < HZ_SLOTS; ++s) tb_mbar_init(st.bar + s, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            tb_fence_proxy_async();
+            for (int R = R0; R <= min(R1, R0 + HZ_AHEAD); ++R) st.issue(p, R, (R - R0) % HZ_SLOTS);
+        }
+        __syncwarp();
+    }
+
+    // per-column constants: the lane's four columns, lane 0's column jw - 1, the last lane's j_end and j_end + 1
+    float iye[4], iyh[4], lo_y[4], up_y[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int jc = active ? jt + c : jw;
+        iye[c] = __ldg(p.iye + jc);
+        iyh[c] = __ldg(p.iyh + jc);
+        lo_y[c] = __ldg(p.lo_y + jc);
+        up_y[c] = __ldg(p.up_y + jc);
+    }
+    const int jl = jw - 1;
+    const float iye_l = __ldg(p.iye + jl), iyh_l = __ldg(p.iyh + jl);
+    const float lo_y_l = __ldg(p.lo_y + jl), up_y_l = __ldg(p.up_y + jl);
+    const float iye_h = __ldg(p.iye + j_end), iye_h1 = __ldg(p.iye + j_end + 1), iyh_h = __ldg(p.iyh + j_end);
+    const float lo_y_h = __ldg(p.lo_y + j_end), up_y_h = __ldg(p.up_y + j_end);
+    const float da = p.da_u, db = p.db_u;
+
+    // carried state (stage 1 of the previous row, stage 2 of the row before)
+    float ey0p[4] = {}, h1p[4] = {}, epp[4] = {}, e1xp[4] = {}, e1ypp[4] = {}, h2p[4] = {};
+    float cbxp[4] = {}, cbypp[4] = {};   // face cb of stage 1's previous rows: E_x of row r - 1, E_y of row r - 2
+    float ey0p_l = 0.0f, e1xp_l = 0.0f;                                  // lane 0, column jw - 1
+    float ey0p_h = 0.0f, ey0p_h1 = 0.0f, h1p_h = 0.0f, epp_h = 0.0f;    // last lane, columns j_end, j_end + 1
+    float e1xp_h = 0.0f, e1ypp_h = 0.0f;
+    {   // old E_y of row R0 - 1
+        const size_t row = (size_t)(R0 - 1) * ny;
+        if (active) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) ey0p[c] = __ldg(p.ey_in + row + jt + c);
+        }
+        if (left_lane) ey0p_l = __ldg(p.ey_in + row + jl);
+        if (halo_lane) ey0p_h = __ldg(p.ey_in + row + j_end), ey0p_h1 = __ldg(p.ey_in + row + j_end + 1);
+    }
+
+    for (int r = R0; r <= R1; ++r) {
+        const int k = r - R0, s = k % HZ_SLOTS;
+        if (!tb_mbar_wait(st.bar + s, (uint32_t)((k / HZ_SLOTS) & 1))) {
+            if (lane == 0) atomicExch(err, 1);
+            for (int q = r; q <= min(R1, r + HZ_AHEAD); ++q) {   // copies still in flight, this row's included
+                const int kq = q - R0;
+                tb_mbar_wait(st.bar + kq % HZ_SLOTS, (uint32_t)((kq / HZ_SLOTS) & 1));
+            }
+            return;
+        }
+        float hzo[4] = {}, exo[4] = {}, eyo[4] = {}, ep[4] = {};
+        float ex_l = 0.0f, ex_l2 = 0.0f, ey_l = 0.0f, hz_l = 0.0f, ep_l = 0.0f;             // columns jw - 1, jw - 2
+        float hz_h = 0.0f, ex_h = 0.0f, ey_h = 0.0f, ep_h = 0.0f;                           // column j_end
+        float hz_h1 = 0.0f, ex_h1 = 0.0f, ey_h1 = 0.0f, ep_h1 = 0.0f;                       // column j_end + 1
+        if (active) {
+            const int o = 4 + 4 * lane;
+            const float4 a = *reinterpret_cast<const float4 *>(st.slot(s, 0) + o);
+            const float4 bx = *reinterpret_cast<const float4 *>(st.slot(s, 1) + o);
+            const float4 by = *reinterpret_cast<const float4 *>(st.slot(s, 2) + o);
+            const float4 be = *reinterpret_cast<const float4 *>(st.slot(s, 3) + o);
+            hzo[0] = a.x, hzo[1] = a.y, hzo[2] = a.z, hzo[3] = a.w;
+            exo[0] = bx.x, exo[1] = bx.y, exo[2] = bx.z, exo[3] = bx.w;
+            eyo[0] = by.x, eyo[1] = by.y, eyo[2] = by.z, eyo[3] = by.w;
+            ep[0] = be.x, ep[1] = be.y, ep[2] = be.z, ep[3] = be.w;
+            if (left_lane) {
+                hz_l = st.slot(s, 0)[o - 1];
+                ex_l = st.slot(s, 1)[o - 1];
+                ex_l2 = st.slot(s, 1)[o - 2];
+                ey_l = st.slot(s, 2)[o - 1];
+                ep_l = st.slot(s, 3)[o - 1];
+            }
+            if (halo_lane) {
+                hz_h = st.slot(s, 0)[o + 4], ex_h = st.slot(s, 1)[o + 4], ey_h = st.slot(s, 2)[o + 4];
+                ep_h = st.slot(s, 3)[o + 4];
+                hz_h1 = st.slot(s, 0)[o + 5], ex_h1 = st.slot(s, 1)[o + 5], ey_h1 = st.slot(s, 2)[o + 5];
+                ep_h1 = st.slot(s, 3)[o + 5];
+            }
+        }
+        __syncwarp();
+        if (lane == 0 && r + HZ_AHEAD + 1 <= R1) {
+            tb_fence_proxy_async();
+            st.issue(p, r + HZ_AHEAD + 1, s);
+        }
+        const float left = __shfl_up_sync(FULL, exo[3], 1);   // old E_x of column jt - 1
+        const float ex_left = left_lane ? ex_l : left;
+
+        // ---- stage 1: step 1 of row r (H_z, E_x) and E_y of row r - 1
+        const float ixe = __ldg(p.ixe + r);
+        float h1[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            h1[c] = hz2_h(da, db, hzo[c], exo[c], c == 0 ? ex_left : exo[c - 1], eyo[c], ey0p[c], iye[c], ixe);
+        float h1_l = 0.0f, h1_h = 0.0f, h1_h1 = 0.0f;
+        if (left_lane) h1_l = hz2_h(da, db, hz_l, ex_l, ex_l2, ey_l, ey0p_l, iye_l, ixe);
+        if (halo_lane) {
+            h1_h = hz2_h(da, db, hz_h, ex_h, exo[3], ey_h, ey0p_h, iye_h, ixe);
+            h1_h1 = hz2_h(da, db, hz_h1, ex_h1, ex_h, ey_h1, ey0p_h1, iye_h1, ixe);
+        }
+        float h1_next = __shfl_down_sync(FULL, h1[0], 1), e_next = __shfl_down_sync(FULL, ep[0], 1);
+        if (halo_lane) h1_next = h1_h, e_next = ep_h;
+        const int64_t k1 = p.k_step, k2 = p.k_step + 1;
+        float e1x[4], cbx[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            cbx[c] = hz_cb_lossless(ep[c], c < 3 ? ep[c + 1] : e_next, lo_y[c], up_y[c], p.dt, p.eps0);
+            e1x[c] = hz2_ex(exo[c], cbx[c], h1[c], c < 3 ? h1[c + 1] : h1_next, iyh[c]);
+        }
+        if (p.n_lines) hz2_src_x4(p, k1, r, jt, e1x);
+        float e1x_l = 0.0f, e1x_h = 0.0f;
+        if (left_lane) {
+            e1x_l = hz2_ex(ex_l, hz_cb_lossless(ep_l, ep[0], lo_y_l, up_y_l, p.dt, p.eps0), h1_l, h1[0], iyh_l);
+            if (p.n_lines) e1x_l = hz2_src_x(p, k1, r, jl, e1x_l);
+        }
+        if (halo_lane) {
+            e1x_h = hz2_ex(ex_h, hz_cb_lossless(ep_h, ep_h1, lo_y_h, up_y_h, p.dt, p.eps0), h1_h, h1_h1, iyh_h);
+            if (p.n_lines) e1x_h = hz2_src_x(p, k1, r, j_end, e1x_h);
+        }
+        // E_y^1 of row r - 1 (rows r0 - 1 .. r1)
+        float e1y[4] = {}, cby[4] = {}, e1y_h = 0.0f;
+        if (r > R0) {
+            const int re = r - 1;
+            const float lo_x = __ldg(p.lo_x + re), up_x = __ldg(p.up_x + re), ixh = __ldg(p.ixh + re);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                cby[c] = hz_cb_lossless(epp[c], ep[c], lo_x, up_x, p.dt, p.eps0);
+                e1y[c] = hz2_ey(ey0p[c], cby[c], h1p[c], h1[c], ixh);
+            }
+            if (p.n_lines) hz2_src_y4(p, k1, re, jt, e1y);
+            if (halo_lane) {
+                e1y_h = hz2_ey(ey0p_h, hz_cb_lossless(epp_h, ep_h, lo_x, up_x, p.dt, p.eps0), h1p_h, h1_h, ixh);
+                if (p.n_lines) e1y_h = hz2_src_y(p, k1, re, j_end, e1y_h);
+            }
+        }
+
+        // ---- stage 2: step 2 of row r - 1 (H_z, E_x) and E_y of row r - 2
+        float h2[4] = {};
+        if (r >= r0 + 1) {
+            const int rs = r - 1;
+            const float ixe_s = __ldg(p.ixe + rs);
+            const float e1x_left_lane = __shfl_up_sync(FULL, e1xp[3], 1);
+            const float e1x_left = left_lane ? e1xp_l : e1x_left_lane;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                h2[c] = hz2_h(da, db, h1p[c], e1xp[c], c == 0 ? e1x_left : e1xp[c - 1], e1y[c], e1ypp[c], iye[c],
+                              ixe_s);
+            float h2_h = 0.0f;
+            if (halo_lane) h2_h = hz2_h(da, db, h1p_h, e1xp_h, e1xp[3], e1y_h, e1ypp_h, iye_h, ixe_s);
+            float h2_next = __shfl_down_sync(FULL, h2[0], 1);
+            if (halo_lane) h2_next = h2_h;
+            const bool own = rs < r1;   // rows r0 .. r1 - 1 are stored; row r1 is the halo of E_y
+            if (own && active) {
+                float e2x[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c)   // the faces of row r - 1: stage 1's cb of the previous row
+                    e2x[c] = hz2_ex(e1xp[c], cbxp[c], h2[c], c < 3 ? h2[c + 1] : h2_next, iyh[c]);
+                if (p.n_lines) hz2_src_x4(p, k2, rs, jt, e2x);
+                const size_t row = (size_t)rs * ny + jt;
+                hz_st4<true>(p.hz_out, row, h2);
+                hz_st4<true>(p.ex_out, row, e2x);
+            }
+            if (r >= r0 + 2 && active) {   // E_y^2 of row r - 2
+                const int re = r - 2;
+                const float ixh = __ldg(p.ixh + re);
+                float e2y[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c)   // the faces of row r - 2: stage 1's cb two rows back
+                    e2y[c] = hz2_ey(e1ypp[c], cbypp[c], h2p[c], h2[c], ixh);
+                if (p.n_lines) hz2_src_y4(p, k2, re, jt, e2y);
+                hz_st4<true>(p.ey_out, (size_t)re * ny + jt, e2y);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            ey0p[c] = eyo[c];
+            h2p[c] = h2[c];
+            h1p[c] = h1[c];
+            epp[c] = ep[c];
+            e1xp[c] = e1x[c];
+            e1ypp[c] = e1y[c];
+            cbxp[c] = cbx[c];
+            cbypp[c] = cby[c];
+        }
+        ey0p_l = ey_l;
+        e1xp_l = e1x_l;
+        ey0p_h = ey_h, ey0p_h1 = ey_h1;
+        h1p_h = h1_h;
+        epp_h = ep_h;
+        e1xp_h = e1x_h;
+        e1ypp_h = e1y_h;
+    }
+}

@@ -481,7 +481,8 @@ class FDTDEngine2D_Hz(FDTDEngine2D_Ez):
         raise NotImplementedError('the H_z engine has no blocked-kernel plan (hz_plan gives its split)')
 
     def hz_plan(self):
-        """(interior cells, border cells) of the variant-1 step."""
+        """(interior cells, border cells) of the variant-1 step (of the two-step launch's box with
+        steps_per_launch 2, where it applies)."""
         self.sync_device()
         a, b = ctypes.c_int64(), ctypes.c_int64()
         _native.check(_native.load().os_fdtd2d_hz_plan(self.handle, ctypes.byref(a), ctypes.byref(b)))

@@ -34,18 +34,19 @@ def _oracle_kwargs(spec):
     return {k: v for k, v in spec['sim'].items() if k != 'polarization'}
 
 
-# (variant, rows per CTA): the per-half-step kernels, and the interior + border kernels with the per-grid choice and
-# with interior runs of 1, 2, 7 and 64 rows (ragged last runs, halo rows on every run)
-HZ_CONFIGS = [(0, 0), (1, 0), (1, 1), (1, 2), (1, 7), (1, 64)]
+# (variant, rows per CTA, steps per launch): the per-half-step kernels, and the interior + border kernels with the
+# per-grid choice and with interior runs of 1, 2, 7 and 64 rows (ragged last runs, halo rows on every run), one step
+# per launch and two (where the two-step interior box fits the grid)
+HZ_CONFIGS = [(0, 0, 1), (1, 0, 1), (1, 1, 1), (1, 2, 1), (1, 7, 1), (1, 64, 1), (1, 0, 2), (1, 16, 2), (1, 1, 2)]
 
 
-@pytest.mark.parametrize('config', HZ_CONFIGS, ids=[f'v{v}_rows{r}' for v, r in HZ_CONFIGS])
+@pytest.mark.parametrize('config', HZ_CONFIGS, ids=[f'v{v}_rows{r}_T{t}' for v, r, t in HZ_CONFIGS])
 @pytest.mark.parametrize('spec', HZ_CASES, ids=[c['name'] for c in HZ_CASES])
 def test_hz_cases_bit_exact_against_reference_fixtures(spec, config):
     g = np.load(os.path.join(GOLDEN, f"{spec['name']}.npz"))
     sim = ob.Simulation(**spec['sim'], verbose=False)
     mons = apply_ops(sim, spec)
-    sim.em.engine.configure(variant=config[0], steps_per_launch=1, tile_rows=config[1])
+    sim.em.engine.configure(variant=config[0], steps_per_launch=config[2], tile_rows=config[1])
     done = 0
     for cp in spec['checkpoints']:
         sim.run(n_steps=cp - done, verbose=False)
@@ -112,19 +113,21 @@ def _random_spec(seed):
         ops.append(['add_flux_monitor', [axis, pos, span],
                     {'wavelengths': rng.uniform(400e-9, 1600e-9, int(rng.integers(1, 5))).tolist()}])
     rows = int(rng.choice([0, 1, 3, 16, 100]))
-    return {'sim': {'size_x': size_x, 'size_y': size_y, 'dx': dx, 'npml': npml, 'boundaries': boundaries},
+    spec = {'sim': {'size_x': size_x, 'size_y': size_y, 'dx': dx, 'npml': npml, 'boundaries': boundaries},
             'ops': ops, 'steps': int(rng.integers(1, 200)), 'rows': rows, 'variant': int(rng.random() < 0.8)}
+    spec['T'] = 2 if spec['variant'] == 1 and rng.random() < 0.5 else 1
+    return spec
 
 
 @pytest.mark.parametrize('seed', range(24))
 def test_hz_random_geometries_bit_exact(seed):
     """Every boundary preset, grids from the 2 npml + 2 minimum to 300+ cells (several column strips, ragged and
     exact multiples of the strip), lossless and lossy, 1-3 sheets (spans cut to the CPML), 0-2 flux lines, 1-199
-    steps in two chunks, variant 0 or the fused kernel with various row runs."""
+    steps in two chunks, variant 0 or the fused kernel with various row runs, one or two steps per launch."""
     spec = _random_spec(seed)
     sim = ob.Simulation(**spec['sim'], polarization='hz', verbose=False)
     mons = apply_ops(sim, spec)
-    sim.em.engine.configure(variant=spec['variant'], steps_per_launch=1, tile_rows=spec['rows'])
+    sim.em.engine.configure(variant=spec['variant'], steps_per_launch=spec['T'], tile_rows=spec['rows'])
     o = OracleHz2D(**spec['sim'])
     omons = apply_ops(o, spec)
     first = spec['steps'] // 3
@@ -196,3 +199,46 @@ def test_hz_field_write_read_roundtrip_and_launch_count():
     m = sim.em.engine.sample_interval
     # per step the interior kernel and the border kernel, plus one DFT launch per sample step
     assert sim.em.engine.launch_count() == 12 * 2 + 12 // m
+
+
+@pytest.mark.parametrize('size, npml, boundaries, rows', [((4.0e-6, 3.2e-6), 10, 'pml', 0),
+                                                          ((3.0e-6, 5.12e-6), 12, 'pml', 16),
+                                                          ((4.4e-6, 2.88e-6), 8, 'periodic_y', 5),
+                                                          ((2.6e-6, 4.0e-6), 10, 'periodic_x', 0)])
+def test_hz_two_steps_per_launch(size, npml, boundaries, rows):
+    """Two steps per launch (hz2d_interior2_kernel on the interior box, the border in two single steps through the
+    scratch set) on lossless grids whose rows are a multiple of 4 cells: dielectric blocks, sheets along both axes
+    crossing the interior, two flux lines (a sample step always ends a launch), uneven chunks -- every field, spectrum
+    and flux bit-identical to one step per launch and to the oracle, in fewer launches."""
+    ops = [['add_dielectric_rectangle', [0.8e-6, 0.4e-6, 1.6e-6, 1.9e-6], {'eps_r': 4.0}],
+           ['add_dielectric_circle', [2.0e-6, 1.4e-6, 0.5e-6], {'eps_r': 2.1}],
+           ['add_line_source', ['y', 0.45e-6], {'wavelength': 700e-9, 'bandwidth': 0.6}],
+           ['add_line_source', ['x', 1.1e-6], {'wavelength': 900e-9, 'bandwidth': 0.5, 'amplitude': 2.0}],
+           ['add_flux_monitor', ['y', 2.3e-6, [0.2e-6, 2.4e-6]], {'wavelengths': [650e-9, 800e-9, 1000e-9]}],
+           ['add_flux_monitor', ['x', 0.7e-6, [0.2e-6, 2.4e-6]], {'wavelengths': [900e-9]}]]
+    args = {'size_x': size[0], 'size_y': size[1], 'dx': 20e-9, 'npml': npml, 'boundaries': boundaries}
+    runs = []
+    for T in (1, 2):
+        sim = ob.Simulation(**args, polarization='hz', verbose=False)
+        mons = apply_ops(sim, {'ops': ops})
+        sim.em.engine.configure(variant=1, steps_per_launch=T, tile_rows=rows)
+        assert sim.grid.ny % 4 == 0
+        launches = 0
+        for n in (37, 1, 2, 160):
+            sim.run(n_steps=n, verbose=False)
+            launches += sim.em.engine.launch_count()
+        assert sim.em.engine.lossless_form()
+        runs.append((_fields(sim), [m.spectra() for m in mons], [m.flux() for m in mons], launches))
+    o = OracleHz2D(**args)
+    omons = apply_ops(o, {'ops': ops})
+    o.run(n_steps=200)
+    assert runs[1][3] < runs[0][3]   # the two-step launches ran
+    for name in runs[0][0]:
+        np.testing.assert_array_equal(runs[1][0][name], runs[0][0][name], err_msg=name)
+        np.testing.assert_array_equal(runs[1][0][name], getattr(o, name), err_msg=name)
+    for (e1, h1), (e2, h2), omon in zip(runs[0][1], runs[1][1], omons):
+        np.testing.assert_array_equal(e2, e1)
+        np.testing.assert_array_equal(h2, h1)
+        np.testing.assert_array_equal(e2, omon.e_acc)
+    for f1, f2 in zip(runs[0][2], runs[1][2]):
+        np.testing.assert_array_equal(f2, f1)
