@@ -65,7 +65,7 @@ def parse_args():
                    help='em3d: step form (0 two in-place kernels, 1 fused on two field sets, 2 fused with staged '
                         'planes, 3 lean staged fused pass); results are the same bits')
     p.add_argument('--x-chunk', type=int, default=0, help='em3d: x planes per block (0: the engine\'s choice)')
-    p.add_argument('--hz-steps', type=int, default=1, choices=[1, 2], help='hz2d: Yee steps per interior launch')
+    p.add_argument('--hz-steps', type=int, default=2, choices=[1, 2], help='hz2d: Yee steps per interior launch')
     p.add_argument('--fused-config', type=int, default=-1,
                    help="em3d: launch shape of the fused forms (0..4; -1: the form's default)")
     return p.parse_args()

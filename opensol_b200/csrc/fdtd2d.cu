@@ -1538,8 +1538,9 @@ static HzPlan2 hz_plan2(const OsFdtd2D *h) {
     q.ib = q1.ib - 1;
     q.jc0 = q1.jc0 + 4;
     q.jc1 = q1.jc1 - 4;
-    // the kernel's form: lossless (face coefficients from eps_r), rows a multiple of 4 cells (TMA-staged windows)
-    q.interior = q1.interior && q.ib > q.ia && q.jc1 > q.jc0 && h->hz_eps && h->grid.ny % 4 == 0;
+    // the kernel's form: ca = 1 and uniform da / db (no conductivity, no magnetic cells; cb from the stored arrays),
+    // rows a multiple of 4 cells (TMA-staged windows)
+    q.interior = q1.interior && q.ib > q.ia && q.jc1 > q.jc0 && !h->has_ca && !h->has_dadb && h->grid.ny % 4 == 0;
     if (q.interior) {
         q.rects1 = hz_frame_rects(h, q.ia + 1, q.ib - 1, q.jc0 + 1, q.jc1 - 1);
         q.rects2 = hz_frame_rects(h, q.ia, q.ib, q.jc0, q.jc1);
@@ -1572,7 +1573,8 @@ static int launch_hz_step2(OsFdtd2D *h, const HzPlan2 &q, const Hz2DParams &p) {
         const int64_t cells_b = br[st]->first[br[st]->n];
         if (cells_b <= 0) continue;
         OS_TRY(prof_begin(h, 1, bstream));
-        hz2d_border_kernel<true><<<(unsigned)((cells_b + 255) / 256), 256, 0, bstream>>>(*bp[st], *br[st]);
+        if (h->hz_eps) hz2d_border_kernel<true><<<(unsigned)((cells_b + 255) / 256), 256, 0, bstream>>>(*bp[st], *br[st]);
+        else hz2d_border_kernel<false><<<(unsigned)((cells_b + 255) / 256), 256, 0, bstream>>>(*bp[st], *br[st]);
         OS_TRY(prof_end(h, bstream));
         h->launches += 1;
     }
@@ -1588,7 +1590,7 @@ static int launch_hz_step2(OsFdtd2D *h, const HzPlan2 &q, const Hz2DParams &p) {
     const dim3 grid((unsigned)((q.jc1 - q.jc0 + 128 * (HZ_THREADS / 32) - 1) / (128 * (HZ_THREADS / 32))),
                     (unsigned)((q.ib - q.ia + pi.rows_per_cta - 1) / pi.rows_per_cta));
     OS_TRY(prof_begin(h, 0, h->stream));
-    hz2d_interior2_kernel<<<grid, HZ_THREADS, (HZ_THREADS / 32) * hz_warp_smem_bytes(), h->stream>>>(pi, h->err.ptr);
+    hz2d_interior2_kernel<<<grid, HZ_THREADS, (HZ_THREADS / 32) * hz2_warp_smem_bytes(), h->stream>>>(pi, h->err.ptr);
     OS_TRY(prof_end(h, h->stream));
     h->launches += 1;
     if (fork) {

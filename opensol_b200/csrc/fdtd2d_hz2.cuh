@@ -1,5 +1,6 @@
-// Two-step interior kernel of the fused H_z step (lossless form, rows a multiple of 4 cells): two Yee steps per launch
-// for the cells of an interior box, reading field set a and writing set b, with every intermediate value in registers.
+// Two-step interior kernel of the fused H_z step (no conductivity, no magnetic cells, rows a multiple of 4 cells): two
+// Yee steps per launch for the cells of an interior box, reading field set a and writing set b, with every
+// intermediate value in registers.
 //
 // The same warp strips, lanes and TMA row ring as hz2d_interior_kernel, and the same arithmetic term for term, in a
 // skewed two-stage pipeline: while streaming row r, stage 1 makes step 1 of row r (H_z^1(r), E_x^1(r)) and E_y^1 of
@@ -7,10 +8,11 @@
 // r0 - 1 .. r1 + 1 and stores step 2 of its rows [r0, r1).  Step 2's columns need step 1 one column beyond the strip
 // on each side: lane 0 makes H_z^1 and E_x^1 of column jw - 1, the strip's last lane H_z^1 of columns j_end and
 // j_end + 1, E_x^1 and E_y^1 of column j_end, and H_z^2 of column j_end; none of these is stored.  The sheet sources
-// of each step are added to the E values of that step, the halo columns' included.  A face's cb, computed by stage 1,
-// is kept for stage 2 one row later.  The host chooses the box so that every update in this cone is the plain one (no
-// CPML row, edge or wrap): the single-step box less one row and four columns on each side.  Every wait is bounded
-// (the ring's tb_mbar_wait).
+// of each step are added to the E values of that step, the halo columns' included.  The faces' cb are read from the
+// stored coefficient arrays (hz2d_face_coefficients_kernel: with no conductivity the denominator is exactly 1, so
+// they are the lossless form's dt / (face eps eps0) as well), staged with the fields, and kept for stage 2.  The host
+// chooses the box so that every update in this cone is the plain one (no CPML row, edge or wrap): the single-step box
+// less one row and four columns on each side.  Every wait is bounded (the ring's tb_mbar_wait).
 #pragma once
 
 #include "fdtd2d_hz.cuh"
@@ -73,17 +75,43 @@ __device__ __forceinline__ float hz2_h(float da, float db, float h, float ex, fl
     return da * h + db * curl;
 }
 
-// Plain E_x (lossless form): 1 E_x + cb (H_z right - H_z) iyh; cb = hz_cb_lossless of the face.
+// Plain E_x (ca = 1): 1 E_x + cb (H_z right - H_z) iyh.
 __device__ __forceinline__ float hz2_ex(float ex, float bx, float h, float h_right, float iyh) {
     const float dx = h_right - h;
     return 1.0f * ex + bx * dx * iyh;
 }
 
-// Plain E_y (lossless form) of row re: 1 E_y - cb (H_z above - H_z) ixh.
+// Plain E_y (ca = 1) of row re: 1 E_y - cb (H_z above - H_z) ixh.
 __device__ __forceinline__ float hz2_ey(float ey, float by, float h, float h_above, float ixh) {
     const float dy = h_above - h;
     return 1.0f * ey - by * dy * ixh;
 }
+
+// Row staging of the two-step kernel: like HzStage, five arrays per row (H_z, E_x, E_y in, the stored face cb of E_x
+// and of E_y) in a per-warp ring of HZ_SLOTS slots by 1D bulk copies (cp.async.bulk, no multicast).
+constexpr int HZ2_ARRAYS = 5;
+__host__ __device__ constexpr int hz2_warp_smem_bytes() { return HZ_SLOTS * HZ2_ARRAYS * HZ_WIN * 4 + HZ_SLOTS * 8; }
+
+struct Hz2Stage {
+    float *ring;          // [slot][array][HZ_WIN]
+    uint64_t *bar;        // [slot]
+    int jw, c_lo, c_hi;
+
+    __device__ __forceinline__ float *slot(int s, int a) const { return ring + (s * HZ2_ARRAYS + a) * HZ_WIN; }
+
+    // lane 0: copy row r into slot s
+    __device__ __forceinline__ void issue(const Hz2DParams &p, int r, int s) const {
+        const uint32_t bytes = (uint32_t)(c_hi - c_lo) * 4u;
+        tb_mbar_expect_tx(bar + s, HZ2_ARRAYS * bytes);
+        const size_t src = (size_t)r * p.ny + c_lo;
+        const int off = c_lo - (jw - 4);
+        tb_bulk_g2s(slot(s, 0) + off, p.hz_in + src, bytes, bar + s);
+        tb_bulk_g2s(slot(s, 1) + off, p.ex_in + src, bytes, bar + s);
+        tb_bulk_g2s(slot(s, 2) + off, p.ey_in + src, bytes, bar + s);
+        tb_bulk_g2s(slot(s, 3) + off, p.cb_x + src, bytes, bar + s);
+        tb_bulk_g2s(slot(s, 4) + off, p.cb_y + src, bytes, bar + s);
+    }
+};
 
 __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2DParams p, int32_t *err) {
     extern __shared__ __align__(16) unsigned char hz_smem[];
@@ -104,11 +132,11 @@ __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2
     const bool left_lane = lane == 0;
     const int R0 = r0 - 1, R1 = r1 + 1;                 // streamed rows R0 .. R1
 
-    HzStage st;
+    Hz2Stage st;
     {
-        unsigned char *mine = hz_smem + warp * hz_warp_smem_bytes();
+        unsigned char *mine = hz_smem + warp * hz2_warp_smem_bytes();
         st.ring = reinterpret_cast<float *>(mine);
-        st.bar = reinterpret_cast<uint64_t *>(mine + HZ_SLOTS * 4 * HZ_WIN * 4);
+        st.bar = reinterpret_cast<uint64_t *>(mine + HZ_SLOTS * HZ2_ARRAYS * HZ_WIN * 4);
         st.jw = jw;
         st.c_lo = max(jw - 4, 0);
         st.c_hi = min(jw + 132, ny);
@@ -121,28 +149,24 @@ __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2
         __syncwarp();
     }
 
-    // per-column constants: the lane's four columns, lane 0's column jw - 1, the last lane's j_end and j_end + 1
-    float iye[4], iyh[4], lo_y[4], up_y[4];
+    // per-column inverse spacings: the lane's four columns, lane 0's column jw - 1, the last lane's j_end, j_end + 1
+    float iye[4], iyh[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
         const int jc = active ? jt + c : jw;
         iye[c] = __ldg(p.iye + jc);
         iyh[c] = __ldg(p.iyh + jc);
-        lo_y[c] = __ldg(p.lo_y + jc);
-        up_y[c] = __ldg(p.up_y + jc);
     }
     const int jl = jw - 1;
     const float iye_l = __ldg(p.iye + jl), iyh_l = __ldg(p.iyh + jl);
-    const float lo_y_l = __ldg(p.lo_y + jl), up_y_l = __ldg(p.up_y + jl);
     const float iye_h = __ldg(p.iye + j_end), iye_h1 = __ldg(p.iye + j_end + 1), iyh_h = __ldg(p.iyh + j_end);
-    const float lo_y_h = __ldg(p.lo_y + j_end), up_y_h = __ldg(p.up_y + j_end);
     const float da = p.da_u, db = p.db_u;
 
-    // carried state (stage 1 of the previous row, stage 2 of the row before)
-    float ey0p[4] = {}, h1p[4] = {}, epp[4] = {}, e1xp[4] = {}, e1ypp[4] = {}, h2p[4] = {};
-    float cbxp[4] = {}, cbypp[4] = {};   // face cb of stage 1's previous rows: E_x of row r - 1, E_y of row r - 2
+    // carried state (stage 1 of the previous row, stage 2 of the row before) and the face cb of earlier rows
+    float ey0p[4] = {}, h1p[4] = {}, e1xp[4] = {}, e1ypp[4] = {}, h2p[4] = {};
+    float cbxp[4] = {}, cbyp[4] = {}, cbypp[4] = {};   // cb of E_x of row r - 1, of E_y of rows r - 1 and r - 2
     float ey0p_l = 0.0f, e1xp_l = 0.0f;                                  // lane 0, column jw - 1
-    float ey0p_h = 0.0f, ey0p_h1 = 0.0f, h1p_h = 0.0f, epp_h = 0.0f;    // last lane, columns j_end, j_end + 1
+    float ey0p_h = 0.0f, ey0p_h1 = 0.0f, h1p_h = 0.0f, cbyp_h = 0.0f;   // last lane, columns j_end, j_end + 1
     float e1xp_h = 0.0f, e1ypp_h = 0.0f;
     {   // old E_y of row R0 - 1
         const size_t row = (size_t)(R0 - 1) * ny;
@@ -164,32 +188,33 @@ __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2
             }
             return;
         }
-        float hzo[4] = {}, exo[4] = {}, eyo[4] = {}, ep[4] = {};
-        float ex_l = 0.0f, ex_l2 = 0.0f, ey_l = 0.0f, hz_l = 0.0f, ep_l = 0.0f;             // columns jw - 1, jw - 2
-        float hz_h = 0.0f, ex_h = 0.0f, ey_h = 0.0f, ep_h = 0.0f;                           // column j_end
-        float hz_h1 = 0.0f, ex_h1 = 0.0f, ey_h1 = 0.0f, ep_h1 = 0.0f;                       // column j_end + 1
+        float hzo[4] = {}, exo[4] = {}, eyo[4] = {}, cbx[4] = {}, cby[4] = {};
+        float ex_l = 0.0f, ex_l2 = 0.0f, ey_l = 0.0f, hz_l = 0.0f, cbx_l = 0.0f;             // columns jw - 1, jw - 2
+        float hz_h = 0.0f, ex_h = 0.0f, ey_h = 0.0f, cbx_h = 0.0f, cby_h = 0.0f;             // column j_end
+        float hz_h1 = 0.0f, ex_h1 = 0.0f, ey_h1 = 0.0f;                                      // column j_end + 1
         if (active) {
             const int o = 4 + 4 * lane;
             const float4 a = *reinterpret_cast<const float4 *>(st.slot(s, 0) + o);
             const float4 bx = *reinterpret_cast<const float4 *>(st.slot(s, 1) + o);
             const float4 by = *reinterpret_cast<const float4 *>(st.slot(s, 2) + o);
-            const float4 be = *reinterpret_cast<const float4 *>(st.slot(s, 3) + o);
+            const float4 cx = *reinterpret_cast<const float4 *>(st.slot(s, 3) + o);
+            const float4 cy = *reinterpret_cast<const float4 *>(st.slot(s, 4) + o);
             hzo[0] = a.x, hzo[1] = a.y, hzo[2] = a.z, hzo[3] = a.w;
             exo[0] = bx.x, exo[1] = bx.y, exo[2] = bx.z, exo[3] = bx.w;
             eyo[0] = by.x, eyo[1] = by.y, eyo[2] = by.z, eyo[3] = by.w;
-            ep[0] = be.x, ep[1] = be.y, ep[2] = be.z, ep[3] = be.w;
+            cbx[0] = cx.x, cbx[1] = cx.y, cbx[2] = cx.z, cbx[3] = cx.w;
+            cby[0] = cy.x, cby[1] = cy.y, cby[2] = cy.z, cby[3] = cy.w;
             if (left_lane) {
                 hz_l = st.slot(s, 0)[o - 1];
                 ex_l = st.slot(s, 1)[o - 1];
                 ex_l2 = st.slot(s, 1)[o - 2];
                 ey_l = st.slot(s, 2)[o - 1];
-                ep_l = st.slot(s, 3)[o - 1];
+                cbx_l = st.slot(s, 3)[o - 1];
             }
             if (halo_lane) {
                 hz_h = st.slot(s, 0)[o + 4], ex_h = st.slot(s, 1)[o + 4], ey_h = st.slot(s, 2)[o + 4];
-                ep_h = st.slot(s, 3)[o + 4];
+                cbx_h = st.slot(s, 3)[o + 4], cby_h = st.slot(s, 4)[o + 4];
                 hz_h1 = st.slot(s, 0)[o + 5], ex_h1 = st.slot(s, 1)[o + 5], ey_h1 = st.slot(s, 2)[o + 5];
-                ep_h1 = st.slot(s, 3)[o + 5];
             }
         }
         __syncwarp();
@@ -212,38 +237,32 @@ __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2
             h1_h = hz2_h(da, db, hz_h, ex_h, exo[3], ey_h, ey0p_h, iye_h, ixe);
             h1_h1 = hz2_h(da, db, hz_h1, ex_h1, ex_h, ey_h1, ey0p_h1, iye_h1, ixe);
         }
-        float h1_next = __shfl_down_sync(FULL, h1[0], 1), e_next = __shfl_down_sync(FULL, ep[0], 1);
-        if (halo_lane) h1_next = h1_h, e_next = ep_h;
+        float h1_next = __shfl_down_sync(FULL, h1[0], 1);
+        if (halo_lane) h1_next = h1_h;
         const int64_t k1 = p.k_step, k2 = p.k_step + 1;
-        float e1x[4], cbx[4];
+        float e1x[4];
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            cbx[c] = hz_cb_lossless(ep[c], c < 3 ? ep[c + 1] : e_next, lo_y[c], up_y[c], p.dt, p.eps0);
-            e1x[c] = hz2_ex(exo[c], cbx[c], h1[c], c < 3 ? h1[c + 1] : h1_next, iyh[c]);
-        }
+        for (int c = 0; c < 4; ++c) e1x[c] = hz2_ex(exo[c], cbx[c], h1[c], c < 3 ? h1[c + 1] : h1_next, iyh[c]);
         if (p.n_lines) hz2_src_x4(p, k1, r, jt, e1x);
         float e1x_l = 0.0f, e1x_h = 0.0f;
         if (left_lane) {
-            e1x_l = hz2_ex(ex_l, hz_cb_lossless(ep_l, ep[0], lo_y_l, up_y_l, p.dt, p.eps0), h1_l, h1[0], iyh_l);
+            e1x_l = hz2_ex(ex_l, cbx_l, h1_l, h1[0], iyh_l);
             if (p.n_lines) e1x_l = hz2_src_x(p, k1, r, jl, e1x_l);
         }
         if (halo_lane) {
-            e1x_h = hz2_ex(ex_h, hz_cb_lossless(ep_h, ep_h1, lo_y_h, up_y_h, p.dt, p.eps0), h1_h, h1_h1, iyh_h);
+            e1x_h = hz2_ex(ex_h, cbx_h, h1_h, h1_h1, iyh_h);
             if (p.n_lines) e1x_h = hz2_src_x(p, k1, r, j_end, e1x_h);
         }
-        // E_y^1 of row r - 1 (rows r0 - 1 .. r1)
-        float e1y[4] = {}, cby[4] = {}, e1y_h = 0.0f;
+        // E_y^1 of row r - 1 (rows r0 - 1 .. r1), with that row's stored cb
+        float e1y[4] = {}, e1y_h = 0.0f;
         if (r > R0) {
             const int re = r - 1;
-            const float lo_x = __ldg(p.lo_x + re), up_x = __ldg(p.up_x + re), ixh = __ldg(p.ixh + re);
+            const float ixh = __ldg(p.ixh + re);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                cby[c] = hz_cb_lossless(epp[c], ep[c], lo_x, up_x, p.dt, p.eps0);
-                e1y[c] = hz2_ey(ey0p[c], cby[c], h1p[c], h1[c], ixh);
-            }
+            for (int c = 0; c < 4; ++c) e1y[c] = hz2_ey(ey0p[c], cbyp[c], h1p[c], h1[c], ixh);
             if (p.n_lines) hz2_src_y4(p, k1, re, jt, e1y);
             if (halo_lane) {
-                e1y_h = hz2_ey(ey0p_h, hz_cb_lossless(epp_h, ep_h, lo_x, up_x, p.dt, p.eps0), h1p_h, h1_h, ixh);
+                e1y_h = hz2_ey(ey0p_h, cbyp_h, h1p_h, h1_h, ixh);
                 if (p.n_lines) e1y_h = hz2_src_y(p, k1, re, j_end, e1y_h);
             }
         }
@@ -267,7 +286,7 @@ __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2
             if (own && active) {
                 float e2x[4];
 #pragma unroll
-                for (int c = 0; c < 4; ++c)   // the faces of row r - 1: stage 1's cb of the previous row
+                for (int c = 0; c < 4; ++c)
                     e2x[c] = hz2_ex(e1xp[c], cbxp[c], h2[c], c < 3 ? h2[c + 1] : h2_next, iyh[c]);
                 if (p.n_lines) hz2_src_x4(p, k2, rs, jt, e2x);
                 const size_t row = (size_t)rs * ny + jt;
@@ -279,8 +298,7 @@ __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2
                 const float ixh = __ldg(p.ixh + re);
                 float e2y[4];
 #pragma unroll
-                for (int c = 0; c < 4; ++c)   // the faces of row r - 2: stage 1's cb two rows back
-                    e2y[c] = hz2_ey(e1ypp[c], cbypp[c], h2p[c], h2[c], ixh);
+                for (int c = 0; c < 4; ++c) e2y[c] = hz2_ey(e1ypp[c], cbypp[c], h2p[c], h2[c], ixh);
                 if (p.n_lines) hz2_src_y4(p, k2, re, jt, e2y);
                 hz_st4<true>(p.ey_out, (size_t)re * ny + jt, e2y);
             }
@@ -290,17 +308,17 @@ __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2
             ey0p[c] = eyo[c];
             h2p[c] = h2[c];
             h1p[c] = h1[c];
-            epp[c] = ep[c];
             e1xp[c] = e1x[c];
             e1ypp[c] = e1y[c];
             cbxp[c] = cbx[c];
-            cbypp[c] = cby[c];
+            cbypp[c] = cbyp[c];
+            cbyp[c] = cby[c];
         }
         ey0p_l = ey_l;
         e1xp_l = e1x_l;
         ey0p_h = ey_h, ey0p_h1 = ey_h1;
         h1p_h = h1_h;
-        epp_h = ep_h;
+        cbyp_h = cby_h;
         e1xp_h = e1x_h;
         e1ypp_h = e1y_h;
     }

@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(32 * TY, MINB)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         tb_fence_proxy_async();
     }
-    for (int q = tid; q <= i_last - base; q += 32 * TY) {
+    for (int q = tid; q < i_last - base; q += 32 * TY) {   // planes base .. i_last - 1, the ones the loop steps
         const int i = base + q;
         Em3DLeanPlane pl;
         pl.ihx = p.ihx[i];

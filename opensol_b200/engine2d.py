@@ -422,7 +422,8 @@ class FDTDEngine2D_Hz(FDTDEngine2D_Ez):
     """Device engine of one 2D H_z simulation (FDTDEngine2D_Hz, open_sol/physics/em/solvers/fdtd_hz_2d.py:12): H_z at
     the cell centres, E_x / E_y on the hi-y / hi-x faces, face-averaged eps_xx / eps_yy / sigma_e.  Per Yee step an
     interior kernel over the box of plain cells (tile_rows rows per CTA, 0 = chosen per grid) and a border kernel over
-    the rest (variant 1), or the in-place per-half-step kernels (variant 0); both give bit-identical fields."""
+    the rest (variant 1), by default two steps per interior launch where the grid allows it, or the in-place
+    per-half-step kernels (variant 0); every choice gives bit-identical fields."""
 
     polarization = 'hz'
     FIELDS = {'hz': _native.OS_HZ_HZ, 'ex': _native.OS_HZ_EX, 'ey': _native.OS_HZ_EY}
@@ -432,7 +433,7 @@ class FDTDEngine2D_Hz(FDTDEngine2D_Ez):
 
     def __init__(self, domain, boundary_config, device: int = 0):
         super().__init__(domain, boundary_config, device)
-        self.variant, self.steps_per_launch, self.tile_rows = 1, 1, 0
+        self.variant, self.steps_per_launch, self.tile_rows = 1, 2, 0
         bc = boundary_config
         widths_x, widths_y = domain.kernel_widths()
         self.shares_x = face_shares(widths_x, bc.periodic_x)
@@ -471,7 +472,10 @@ class FDTDEngine2D_Hz(FDTDEngine2D_Ez):
 
     def configure(self, variant=None, steps_per_launch=None, tile_rows=None):
         """variant 1 (default): interior + border kernel per step, tile_rows interior rows per CTA (0 = chosen per
-        grid); variant 0: one H_z and one E kernel per step.  steps_per_launch is 1."""
+        grid); variant 0: one H_z and one E kernel per step.  steps_per_launch 2 (default) or 1: with 2, where the grid
+        has no conductivity, no magnetic cells and rows of a multiple of 4 cells, the interior box advances two steps
+        per launch (the border two single steps through a scratch field set, made here) except where the next step is
+        a sampled one; field probes, a TFSF box or poles keep one step per launch."""
         super().configure(variant, steps_per_launch, tile_rows)
 
     def autotune(self, candidates=None, repeats=4):

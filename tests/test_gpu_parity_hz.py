@@ -190,6 +190,7 @@ def test_hz_field_write_read_roundtrip_and_launch_count():
     sim = ob.Simulation(1e-6, 0.5e-6, 25e-9, npml=8, polarization='hz', verbose=False)
     sim.add_flux_monitor('y', 0.5e-6, (0.1e-6, 0.4e-6), wavelengths=[700e-9])
     sim.add_line_source('x', 0.2e-6, wavelength=700e-9)
+    sim.em.engine.configure(variant=1, steps_per_launch=1, tile_rows=0)
     sim.em.finalize()
     rng = np.random.default_rng(3)
     values = rng.standard_normal((sim.grid.nx, sim.grid.ny)).astype(np.float32)
