@@ -101,7 +101,10 @@ int os_fdtd2d_read_cb(OsFdtd2D *h, float *cb);
  * (FluxMonitor 'hz', physics/em/monitors.py:350-362); field components are OS_HZ_HZ / OS_HZ_EX / OS_HZ_EY.
  * os_fdtd2d_configure takes variant 1 (default: per step an interior kernel over the box of plain cells, tile_rows
  * rows per CTA, 0 = chosen per grid, and a border kernel over the rest) or 0 (one H_z and one E kernel per step) with
- * steps_per_launch 1.  The E_z-only calls (set_materials,
+ * steps_per_launch 1 or 2: with 2, on a grid without conductivity or magnetic cells whose rows are a multiple of 4
+ * cells, the interior box advances two steps per launch and the border two single steps through a scratch field set
+ * (allocated by this call), except where the next step is a DFT sample step or field probes are set; results are
+ * bit-identical either way.  The E_z-only calls (set_materials,
  * set_coefficients, read_cb, autotune, plan_info, batch, adjoint) return OS_ERR_STATE on an H_z handle and the
  * H_z-only calls below on an E_z handle.
  * ---------------------------------------------------------------------------------------------------------------- */
