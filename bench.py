@@ -442,9 +442,12 @@ def run_hz2d(args):
                 'border_cells': border_cells, 'launch_ms': launch_ms, 'lossless_form': engine.lossless_form(),
                 'kernel_share': {k: v[0] / sum(t[0] for t in times.values()) for k, v in times.items()}}
     traffic_path = os.path.join(ROOT, 'profiles', 'traffic.json')
+    two_step = engine.variant == 1 and interior_cells and engine.steps_per_launch == 2
+    if two_step:
+        roofline['kernel'] = 'hz2d_interior2_kernel (two steps per launch)'
     if os.path.exists(traffic_path):
         with open(traffic_path) as f:
-            t = json.load(f).get('hz2d_interior_kernel')
+            t = json.load(f).get('hz2d_interior2_kernel' if two_step else 'hz2d_interior_kernel')
         if t:
             roofline['traffic'] = t['dram_bytes_per_cell_update'] * units
             roofline['traffic_note'] = t['note']
@@ -534,15 +537,16 @@ def run_em3d(args):
                        'step_form': args.form3d, 'fused_config': args.fused_config, 'x_chunk': args.x_chunk},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
                          'traffic': None, 'peak_source': f'{peak_kind} hbm_gbs', 'bytes_per_cell_update': 52,
-                         'kernel': 'em3d_h_kernel + em3d_e_kernel (whole step)'},
+                         'kernel': 'em3d_lean_kernel + x / y face kernels (whole step)' if engine.interior()[1]
+                         and args.form3d == 3 else 'em3d_h_kernel + em3d_e_kernel (whole step)'},
             'gpu_launches': launches, 'clocks': clocks.summary(),
             'flux_box_first': float(box.flux()[0])}
     traffic_path = os.path.join(ROOT, 'profiles', 'traffic.json')
     if os.path.exists(traffic_path):
         with open(traffic_path) as f:
-            t = json.load(f).get('em3d_step')
+            t = json.load(f).get('em3d_lean_step' if engine.interior()[1] and args.form3d == 3 else 'em3d_step')
         if t:
-            line['roofline']['traffic'] = t['dram_bytes_per_cell_update'] * cells   # per step (both kernels)
+            line['roofline']['traffic'] = t['dram_bytes_per_cell_update'] * cells   # per step
             line['roofline']['traffic_note'] = t['note']
     return line
 
