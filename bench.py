@@ -32,6 +32,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_CELL_UPDATE = 28          # 3 float32 fields read + written, one float32 material word read
+HZ2_BYTES_PER_CELL_UPDATE = 16      # H_z two steps per launch: 5 float32 arrays read, 3 written, per two steps
 SIM_STEPS = 10_000
 CPU_SAMPLE_STEPS = 24
 
@@ -435,16 +436,21 @@ def run_hz2d(args):
         units = cells
     total_ms, n_launch = times[name]
     launch_ms = total_ms / n_launch
-    achieved = BYTES_PER_CELL_UPDATE * units / (launch_ms / 1e3) / 1e9
+    two_step = engine.variant == 1 and interior_cells and engine.steps_per_launch == 2
+    # algorithmic bytes per cell-update of the timed kernel: one step reads and writes the three fields and reads one
+    # eps word (28 B); the two-step pass reads H_z, E_x, E_y and the stored faces cb_x, cb_y and writes the three
+    # fields once per two steps (32 B per cell, 16 B per cell-update)
+    bpc = HZ2_BYTES_PER_CELL_UPDATE if two_step else BYTES_PER_CELL_UPDATE
+    achieved = bpc * units / (launch_ms / 1e3) / 1e9
     roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
                 'traffic': None, 'peak_source': f'{peak_kind} hbm_gbs (copy bandwidth)', 'kernel': name,
-                'bytes_per_cell_update': BYTES_PER_CELL_UPDATE, 'cell_updates_per_launch': units,
+                'bytes_per_cell_update': bpc, 'cell_updates_per_launch': units,
                 'border_cells': border_cells, 'launch_ms': launch_ms, 'lossless_form': engine.lossless_form(),
                 'kernel_share': {k: v[0] / sum(t[0] for t in times.values()) for k, v in times.items()}}
     traffic_path = os.path.join(ROOT, 'profiles', 'traffic.json')
-    two_step = engine.variant == 1 and interior_cells and engine.steps_per_launch == 2
     if two_step:
         roofline['kernel'] = 'hz2d_interior2_kernel (two steps per launch)'
+        roofline['one_step_equivalent_gbs'] = BYTES_PER_CELL_UPDATE * units / (launch_ms / 1e3) / 1e9
     if os.path.exists(traffic_path):
         with open(traffic_path) as f:
             t = json.load(f).get('hz2d_interior2_kernel' if two_step else 'hz2d_interior_kernel')

@@ -1581,13 +1581,13 @@ static int launch_hz_step2(OsFdtd2D *h, const HzPlan2 &q, const Hz2DParams &p) {
     Hz2DParams pi = p;
     pi.ia = q.ia, pi.ib = q.ib, pi.jc0 = q.jc0, pi.jc1 = q.jc1;
     {
-        const int64_t warps = (q.jc1 - q.jc0 + 127) / 128;
+        const int64_t warps = (q.jc1 - q.jc0 + HZ2_OUT - 1) / HZ2_OUT;
         const int64_t ctas_x = (warps + HZ_THREADS / 32 - 1) / (HZ_THREADS / 32);
         const int64_t want = (int64_t)h->sm_count * 4 * 4;   // about four waves of four CTAs per SM
         int64_t rows = h->hz_rows > 0 ? h->hz_rows : ((int64_t)(q.ib - q.ia) * ctas_x + want - 1) / want;
         pi.rows_per_cta = (int32_t)std::max<int64_t>(h->hz_rows > 0 ? 1 : 16, std::min<int64_t>(128, rows));
     }
-    const dim3 grid((unsigned)((q.jc1 - q.jc0 + 128 * (HZ_THREADS / 32) - 1) / (128 * (HZ_THREADS / 32))),
+    const dim3 grid((unsigned)((q.jc1 - q.jc0 + HZ2_OUT * (HZ_THREADS / 32) - 1) / (HZ2_OUT * (HZ_THREADS / 32))),
                     (unsigned)((q.ib - q.ia + pi.rows_per_cta - 1) / pi.rows_per_cta));
     OS_TRY(prof_begin(h, 0, h->stream));
     hz2d_interior2_kernel<<<grid, HZ_THREADS, (HZ_THREADS / 32) * hz2_warp_smem_bytes(), h->stream>>>(pi, h->err.ptr);

@@ -6,9 +6,9 @@
 // skewed two-stage pipeline: while streaming row r, stage 1 makes step 1 of row r (H_z^1(r), E_x^1(r)) and E_y^1 of
 // row r - 1; stage 2 makes step 2 one row behind (H_z^2(r - 1), E_x^2(r - 1), E_y^2(r - 2)).  A block streams rows
 // r0 - 1 .. r1 + 1 and stores step 2 of its rows [r0, r1).  Step 2's columns need step 1 one column beyond the strip
-// on each side: lane 0 makes H_z^1 and E_x^1 of column jw - 1, the strip's last lane H_z^1 of columns j_end and
-// j_end + 1, E_x^1 and E_y^1 of column j_end, and H_z^2 of column j_end; none of these is stored.  The sheet sources
-// of each step are added to the E values of that step, the halo columns' included.  The faces' cb are read from the
+// on each side: a warp holds 128 columns and stores the middle 120, its first and last lanes computing the halo
+// columns with the same code as the rest.  The sheet sources of each step are added to the E values of that step,
+// the halo columns' included.  The faces' cb are read from the
 // stored coefficient arrays (hz2d_face_coefficients_kernel: with no conductivity the denominator is exactly 1, so
 // they are the lossless form's dt / (face eps eps0) as well), staged with the fields, and kept for stage 2.  The host
 // chooses the box so that every update in this cone is the plain one (no CPML row, edge or wrap): the single-step box
@@ -17,31 +17,9 @@
 
 #include "fdtd2d_hz.cuh"
 
-// Sheet sources of step `k` on the E_x face (r, j) (axis 0 lines: faces (r, position), r in [lo, hi)), added in line
-// order after the update, a zero value skipped, as hz_plain_e adds them.
-__device__ __forceinline__ float hz2_src_x(const Hz2DParams &p, int64_t k, int r, int j, float v) {
-    for (int l = 0; l < p.n_lines; ++l) {
-        const LineSrcDev &L = p.lines[l];
-        if (L.axis != 0 || L.position != j || r < L.lo || r >= L.hi) continue;
-        const float value = p.line_values[(size_t)l * p.values_stride + k];
-        if (value != 0.0f) v += value * L.profile[r - L.lo];
-    }
-    return v;
-}
-
-// The same on the E_y face (re, j) (axis 1 lines: faces (position, j), j in [lo, hi)).
-__device__ __forceinline__ float hz2_src_y(const Hz2DParams &p, int64_t k, int re, int j, float v) {
-    for (int l = 0; l < p.n_lines; ++l) {
-        const LineSrcDev &L = p.lines[l];
-        if (L.axis != 1 || L.position != re || j < L.lo || j >= L.hi) continue;
-        const float value = p.line_values[(size_t)l * p.values_stride + k];
-        if (value != 0.0f) v += value * L.profile[j - L.lo];
-    }
-    return v;
-}
-
-// The same for the lane's four E_x faces of row r (columns jt .. jt + 3) and four E_y faces of row re: each line is
-// tested once per row.
+// Sheet sources of step `k` on the lane's four E_x faces of row r (columns jt .. jt + 3; axis 0 lines: faces
+// (r, position), r in [lo, hi)) and four E_y faces of row re (axis 1 lines: faces (position, j), j in [lo, hi)), added
+// in line order after the update, a zero value skipped, as hz_plain_e adds them; each line is tested once per row.
 __device__ __forceinline__ void hz2_src_x4(const Hz2DParams &p, int64_t k, int r, int jt, float (&v)[4]) {
     for (int l = 0; l < p.n_lines; ++l) {
         const LineSrcDev &L = p.lines[l];
@@ -87,15 +65,17 @@ __device__ __forceinline__ float hz2_ey(float ey, float by, float h, float h_abo
     return 1.0f * ey - by * dy * ixh;
 }
 
-// Row staging of the two-step kernel: like HzStage, five arrays per row (H_z, E_x, E_y in, the stored face cb of E_x
-// and of E_y) in a per-warp ring of HZ_SLOTS slots by 1D bulk copies (cp.async.bulk, no multicast).
+// Row staging of the two-step kernel: five arrays per row (H_z, E_x, E_y in, the stored face cb of E_x and of E_y),
+// each a window of HZ_WIN columns from jw - 8 (clipped to the grid), in a per-warp ring of HZ_SLOTS slots by 1D bulk
+// copies (cp.async.bulk, no multicast).
 constexpr int HZ2_ARRAYS = 5;
+constexpr int HZ2_OUT = 120;   // output columns of a warp strip: lanes 1..30 (lanes 0 and 31 are halo lanes)
 __host__ __device__ constexpr int hz2_warp_smem_bytes() { return HZ_SLOTS * HZ2_ARRAYS * HZ_WIN * 4 + HZ_SLOTS * 8; }
 
 struct Hz2Stage {
     float *ring;          // [slot][array][HZ_WIN]
     uint64_t *bar;        // [slot]
-    int jw, c_lo, c_hi;
+    int jw, c_lo, c_hi;   // window columns [c_lo, c_hi) of the grid at slot offset c_lo - (jw - 8)
 
     __device__ __forceinline__ float *slot(int s, int a) const { return ring + (s * HZ2_ARRAYS + a) * HZ_WIN; }
 
@@ -104,7 +84,7 @@ struct Hz2Stage {
         const uint32_t bytes = (uint32_t)(c_hi - c_lo) * 4u;
         tb_mbar_expect_tx(bar + s, HZ2_ARRAYS * bytes);
         const size_t src = (size_t)r * p.ny + c_lo;
-        const int off = c_lo - (jw - 4);
+        const int off = c_lo - (jw - 8);
         tb_bulk_g2s(slot(s, 0) + off, p.hz_in + src, bytes, bar + s);
         tb_bulk_g2s(slot(s, 1) + off, p.ex_in + src, bytes, bar + s);
         tb_bulk_g2s(slot(s, 2) + off, p.ey_in + src, bytes, bar + s);
@@ -113,24 +93,25 @@ struct Hz2Stage {
     }
 };
 
+// Lane l holds columns jw - 4 + 4 l .. + 3, the whole warp the same vector code: lanes 1..30 own the strip's 120
+// output columns [jw, j_end); lane 0 (columns jw - 4 .. jw - 1) and the lane after the last output lane are halo
+// lanes whose step-1 values at jw - 1 and j_end, j_end + 1 (and step-2 H_z at j_end) the output lanes read by
+// shuffle; a halo lane's other values miss a neighbour and are never read.  Only output columns are stored.
 __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2DParams p, int32_t *err) {
     extern __shared__ __align__(16) unsigned char hz_smem[];
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int jw = p.jc0 + (blockIdx.x * (HZ_THREADS / 32) + warp) * 128;
+    const int jw = p.jc0 + (blockIdx.x * (HZ_THREADS / 32) + warp) * HZ2_OUT;
     if (jw >= p.jc1) return;   // whole warp (its barriers are never used)
-    const int jt = jw + 4 * lane;
+    const int jt = jw - 4 + 4 * lane;
     const int ny = p.ny;
     const int r0 = p.ia + blockIdx.y * p.rows_per_cta;
     if (r0 >= p.ib) return;
     const int r1 = min(p.ib, r0 + p.rows_per_cta);
-    const int j_end = min(jw + 128, p.jc1);             // the strip's columns [jw, j_end)
-    const bool active = jt < j_end;
-    const int last_lane = (j_end - 1 - jw) / 4;
-    const bool halo_lane = lane == last_lane;
-    const bool left_lane = lane == 0;
-    const int R0 = r0 - 1, R1 = r1 + 1;                 // streamed rows R0 .. R1
+    const int j_end = min(jw + HZ2_OUT, p.jc1);          // the strip's output columns [jw, j_end)
+    const bool out_lane = jt >= jw && jt < j_end;
+    const int R0 = r0 - 1, R1 = r1 + 1;                  // streamed rows R0 .. R1
 
     Hz2Stage st;
     {
@@ -138,8 +119,8 @@ __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2
         st.ring = reinterpret_cast<float *>(mine);
         st.bar = reinterpret_cast<uint64_t *>(mine + HZ_SLOTS * HZ2_ARRAYS * HZ_WIN * 4);
         st.jw = jw;
-        st.c_lo = max(jw - 4, 0);
-        st.c_hi = min(jw + 132, ny);
+        st.c_lo = max(jw - 8, 0);
+        st.c_hi = min(jw + 128, ny);
         if (lane == 0) {
             for (int s = 0; s < HZ_SLOTS; ++s) tb_mbar_init(st.bar + s, 1);
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -149,34 +130,24 @@ __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2
         __syncwarp();
     }
 
-    // per-column inverse spacings: the lane's four columns, lane 0's column jw - 1, the last lane's j_end, j_end + 1
     float iye[4], iyh[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-        const int jc = active ? jt + c : jw;
+        const int jc = min(max(jt + c, 0), ny - 1);
         iye[c] = __ldg(p.iye + jc);
         iyh[c] = __ldg(p.iyh + jc);
     }
-    const int jl = jw - 1;
-    const float iye_l = __ldg(p.iye + jl), iyh_l = __ldg(p.iyh + jl);
-    const float iye_h = __ldg(p.iye + j_end), iye_h1 = __ldg(p.iye + j_end + 1), iyh_h = __ldg(p.iyh + j_end);
     const float da = p.da_u, db = p.db_u;
 
     // carried state (stage 1 of the previous row, stage 2 of the row before) and the face cb of earlier rows
     float ey0p[4] = {}, h1p[4] = {}, e1xp[4] = {}, e1ypp[4] = {}, h2p[4] = {};
     float cbxp[4] = {}, cbyp[4] = {}, cbypp[4] = {};   // cb of E_x of row r - 1, of E_y of rows r - 1 and r - 2
-    float ey0p_l = 0.0f, e1xp_l = 0.0f;                                  // lane 0, column jw - 1
-    float ey0p_h = 0.0f, ey0p_h1 = 0.0f, h1p_h = 0.0f, cbyp_h = 0.0f;   // last lane, columns j_end, j_end + 1
-    float e1xp_h = 0.0f, e1ypp_h = 0.0f;
     {   // old E_y of row R0 - 1
         const size_t row = (size_t)(R0 - 1) * ny;
-        if (active) {
 #pragma unroll
-            for (int c = 0; c < 4; ++c) ey0p[c] = __ldg(p.ey_in + row + jt + c);
-        }
-        if (left_lane) ey0p_l = __ldg(p.ey_in + row + jl);
-        if (halo_lane) ey0p_h = __ldg(p.ey_in + row + j_end), ey0p_h1 = __ldg(p.ey_in + row + j_end + 1);
+        for (int c = 0; c < 4; ++c) ey0p[c] = __ldg(p.ey_in + row + min(max(jt + c, 0), ny - 1));
     }
+    const int o = 4 + 4 * lane;   // the lane's first column in a window (window column 0 = grid column jw - 8)
 
     for (int r = R0; r <= R1; ++r) {
         const int k = r - R0, s = k % HZ_SLOTS;
@@ -188,12 +159,8 @@ __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2
             }
             return;
         }
-        float hzo[4] = {}, exo[4] = {}, eyo[4] = {}, cbx[4] = {}, cby[4] = {};
-        float ex_l = 0.0f, ex_l2 = 0.0f, ey_l = 0.0f, hz_l = 0.0f, cbx_l = 0.0f;             // columns jw - 1, jw - 2
-        float hz_h = 0.0f, ex_h = 0.0f, ey_h = 0.0f, cbx_h = 0.0f, cby_h = 0.0f;             // column j_end
-        float hz_h1 = 0.0f, ex_h1 = 0.0f, ey_h1 = 0.0f;                                      // column j_end + 1
-        if (active) {
-            const int o = 4 + 4 * lane;
+        float hzo[4], exo[4], eyo[4], cbx[4], cby[4];
+        {
             const float4 a = *reinterpret_cast<const float4 *>(st.slot(s, 0) + o);
             const float4 bx = *reinterpret_cast<const float4 *>(st.slot(s, 1) + o);
             const float4 by = *reinterpret_cast<const float4 *>(st.slot(s, 2) + o);
@@ -204,67 +171,33 @@ __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2
             eyo[0] = by.x, eyo[1] = by.y, eyo[2] = by.z, eyo[3] = by.w;
             cbx[0] = cx.x, cbx[1] = cx.y, cbx[2] = cx.z, cbx[3] = cx.w;
             cby[0] = cy.x, cby[1] = cy.y, cby[2] = cy.z, cby[3] = cy.w;
-            if (left_lane) {
-                hz_l = st.slot(s, 0)[o - 1];
-                ex_l = st.slot(s, 1)[o - 1];
-                ex_l2 = st.slot(s, 1)[o - 2];
-                ey_l = st.slot(s, 2)[o - 1];
-                cbx_l = st.slot(s, 3)[o - 1];
-            }
-            if (halo_lane) {
-                hz_h = st.slot(s, 0)[o + 4], ex_h = st.slot(s, 1)[o + 4], ey_h = st.slot(s, 2)[o + 4];
-                cbx_h = st.slot(s, 3)[o + 4], cby_h = st.slot(s, 4)[o + 4];
-                hz_h1 = st.slot(s, 0)[o + 5], ex_h1 = st.slot(s, 1)[o + 5], ey_h1 = st.slot(s, 2)[o + 5];
-            }
         }
+        const float ex_l0 = st.slot(s, 1)[o - 1];   // old E_x left of the lane (lane 0: from the window)
         __syncwarp();
         if (lane == 0 && r + HZ_AHEAD + 1 <= R1) {
             tb_fence_proxy_async();
             st.issue(p, r + HZ_AHEAD + 1, s);
         }
-        const float left = __shfl_up_sync(FULL, exo[3], 1);   // old E_x of column jt - 1
-        const float ex_left = left_lane ? ex_l : left;
 
         // ---- stage 1: step 1 of row r (H_z, E_x) and E_y of row r - 1
         const float ixe = __ldg(p.ixe + r);
         float h1[4];
 #pragma unroll
         for (int c = 0; c < 4; ++c)
-            h1[c] = hz2_h(da, db, hzo[c], exo[c], c == 0 ? ex_left : exo[c - 1], eyo[c], ey0p[c], iye[c], ixe);
-        float h1_l = 0.0f, h1_h = 0.0f, h1_h1 = 0.0f;
-        if (left_lane) h1_l = hz2_h(da, db, hz_l, ex_l, ex_l2, ey_l, ey0p_l, iye_l, ixe);
-        if (halo_lane) {
-            h1_h = hz2_h(da, db, hz_h, ex_h, exo[3], ey_h, ey0p_h, iye_h, ixe);
-            h1_h1 = hz2_h(da, db, hz_h1, ex_h1, ex_h, ey_h1, ey0p_h1, iye_h1, ixe);
-        }
-        float h1_next = __shfl_down_sync(FULL, h1[0], 1);
-        if (halo_lane) h1_next = h1_h;
+            h1[c] = hz2_h(da, db, hzo[c], exo[c], c == 0 ? ex_l0 : exo[c - 1], eyo[c], ey0p[c], iye[c], ixe);
+        const float h1_next = __shfl_down_sync(FULL, h1[0], 1);   // H_z^1 right of the lane (lane 31: unused)
         const int64_t k1 = p.k_step, k2 = p.k_step + 1;
         float e1x[4];
 #pragma unroll
         for (int c = 0; c < 4; ++c) e1x[c] = hz2_ex(exo[c], cbx[c], h1[c], c < 3 ? h1[c + 1] : h1_next, iyh[c]);
         if (p.n_lines) hz2_src_x4(p, k1, r, jt, e1x);
-        float e1x_l = 0.0f, e1x_h = 0.0f;
-        if (left_lane) {
-            e1x_l = hz2_ex(ex_l, cbx_l, h1_l, h1[0], iyh_l);
-            if (p.n_lines) e1x_l = hz2_src_x(p, k1, r, jl, e1x_l);
-        }
-        if (halo_lane) {
-            e1x_h = hz2_ex(ex_h, cbx_h, h1_h, h1_h1, iyh_h);
-            if (p.n_lines) e1x_h = hz2_src_x(p, k1, r, j_end, e1x_h);
-        }
-        // E_y^1 of row r - 1 (rows r0 - 1 .. r1), with that row's stored cb
-        float e1y[4] = {}, e1y_h = 0.0f;
-        if (r > R0) {
+        float e1y[4] = {};
+        if (r > R0) {   // E_y^1 of row r - 1 (rows r0 - 1 .. r1), with that row's stored cb
             const int re = r - 1;
             const float ixh = __ldg(p.ixh + re);
 #pragma unroll
             for (int c = 0; c < 4; ++c) e1y[c] = hz2_ey(ey0p[c], cbyp[c], h1p[c], h1[c], ixh);
             if (p.n_lines) hz2_src_y4(p, k1, re, jt, e1y);
-            if (halo_lane) {
-                e1y_h = hz2_ey(ey0p_h, cbyp_h, h1p_h, h1_h, ixh);
-                if (p.n_lines) e1y_h = hz2_src_y(p, k1, re, j_end, e1y_h);
-            }
         }
 
         // ---- stage 2: step 2 of row r - 1 (H_z, E_x) and E_y of row r - 2
@@ -272,18 +205,13 @@ __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2
         if (r >= r0 + 1) {
             const int rs = r - 1;
             const float ixe_s = __ldg(p.ixe + rs);
-            const float e1x_left_lane = __shfl_up_sync(FULL, e1xp[3], 1);
-            const float e1x_left = left_lane ? e1xp_l : e1x_left_lane;
+            const float e1x_left = __shfl_up_sync(FULL, e1xp[3], 1);   // lane 0: unused
 #pragma unroll
             for (int c = 0; c < 4; ++c)
                 h2[c] = hz2_h(da, db, h1p[c], e1xp[c], c == 0 ? e1x_left : e1xp[c - 1], e1y[c], e1ypp[c], iye[c],
                               ixe_s);
-            float h2_h = 0.0f;
-            if (halo_lane) h2_h = hz2_h(da, db, h1p_h, e1xp_h, e1xp[3], e1y_h, e1ypp_h, iye_h, ixe_s);
-            float h2_next = __shfl_down_sync(FULL, h2[0], 1);
-            if (halo_lane) h2_next = h2_h;
-            const bool own = rs < r1;   // rows r0 .. r1 - 1 are stored; row r1 is the halo of E_y
-            if (own && active) {
+            const float h2_next = __shfl_down_sync(FULL, h2[0], 1);
+            if (rs < r1 && out_lane) {   // rows r0 .. r1 - 1 are stored; row r1 is the halo of E_y
                 float e2x[4];
 #pragma unroll
                 for (int c = 0; c < 4; ++c)
@@ -293,7 +221,7 @@ __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2
                 hz_st4<true>(p.hz_out, row, h2);
                 hz_st4<true>(p.ex_out, row, e2x);
             }
-            if (r >= r0 + 2 && active) {   // E_y^2 of row r - 2
+            if (r >= r0 + 2 && out_lane) {   // E_y^2 of row r - 2
                 const int re = r - 2;
                 const float ixh = __ldg(p.ixh + re);
                 float e2y[4];
@@ -314,12 +242,5 @@ __global__ void __launch_bounds__(HZ_THREADS, 4) hz2d_interior2_kernel(const Hz2
             cbypp[c] = cbyp[c];
             cbyp[c] = cby[c];
         }
-        ey0p_l = ey_l;
-        e1xp_l = e1x_l;
-        ey0p_h = ey_h, ey0p_h1 = ey_h1;
-        h1p_h = h1_h;
-        cbyp_h = cby_h;
-        e1xp_h = e1x_h;
-        e1ypp_h = e1y_h;
     }
 }
