@@ -202,7 +202,9 @@ int os_fdtd2d_hz_add_pole(OsFdtd2D *h, int32_t kind, int32_t component, int32_t 
 
 /* Field probe: one component (OS_EZ / OS_HX / OS_HY, or OS_HZ_* on an H_z handle) of cell (ix, iy) recorded after
  * every step from the current one on: FieldProbe.record at t_full (core/monitors.py:194-243, fdtd_2d_base.py:481-487).
- * At most 8.  An advance with probes runs one step per launch.  Not in batched advances; os_fdtd2d_advance_noalloc
+ * At most 8.  On an E_z handle the blocked launches stage the probes' cells at every step (same values as one step
+ * per launch) while flux lines and probes together number at most 8, else an advance with probes runs one step per
+ * launch, as it always does on an H_z handle.  Not in batched advances; os_fdtd2d_advance_noalloc
  * refuses a chunk for which the probes' rows would have to grow. */
 int os_fdtd2d_add_probe(OsFdtd2D *h, int32_t ix, int32_t iy, int32_t component, int32_t *probe_id);
 

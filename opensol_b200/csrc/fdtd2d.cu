@@ -115,6 +115,7 @@ struct OsFdtd2D {
     float inv_dt = 0.0f;                  // float32 1 / dt of the Lorentz corrections
     os::ProbeSet probes{};                // field probes (recorded after every step)
     os::DeviceArray<float> probe_rows;    // (OS_MAX_PROBES, probe_capacity) values by step
+    os::DeviceArray<float> probe_stage;   // (OS_MAX_PROBES, TB_MAX_T, 2) the probes' cells at each step of a launch
     int64_t probe_capacity = 0;           // rows per probe
     int64_t sample_interval = 1;
     int64_t n_step = 0;
@@ -344,7 +345,7 @@ extern "C" int os_fdtd2d_destroy(OsFdtd2D *h) {
         for (auto &t : h->tfsf) give(t->aux_ez), give(t->aux_hy), give(t->aux_coef_h), give(t->aux_coef_e);
         for (auto &q : h->poles) give(q->drive), give(q->a), give(q->b);
         give(h->jz_total);
-        give(h->probe_rows);
+        give(h->probe_rows), give(h->probe_stage);
         give(h->err), give(h->line_values), give(h->phases);
         pool_events_done(ev);
     }
@@ -854,6 +855,11 @@ static int launch_interior_any(OsFdtd2D *h, const TBParams &q) {
     return h->has_ca ? launch_interior_ca<T, true>(h, q) : launch_interior_ca<T, false>(h, q);
 }
 
+// The staging slot of frame step k (1..T) of a launch with the sample mask of `q` (-1: not a staging step).
+static void set_frame_slots(EzFrameParams &f, const TBParams &q, int k) {
+    f.sample_slot = ((q.sample_mask >> (k - 1)) & 1u) ? __builtin_popcount(q.sample_mask & ((1u << (k - 1)) - 1u)) : -1;
+}
+
 // Parameters of frame step k (1..T) of one blocked launch of T steps from buffer set in_set to out_set: the region
 // is the grid minus the interior rectangle `in` (NULL: none) shrunk by T - k cells on each non-periodic side; it
 // reads the state of step k - 1 (the input set for k = 1, else a scratch set) and writes that of step k (a scratch
@@ -888,7 +894,7 @@ static EzFrameParams make_frame_params(const OsFdtd2D *h, int T, int k, const TB
     f.k_col = q.k0 + (k - 1);
     f.n_mons = q.n_mons;
     for (int m = 0; m < q.n_mons; ++m) f.mons[m] = q.mons[m];
-    f.sample_slot = ((q.sample_mask >> (k - 1)) & 1u) ? __builtin_popcount(q.sample_mask & ((1u << (k - 1)) - 1u)) : -1;
+    set_frame_slots(f, q, k);
     Rect sh{0, 0, 0, 0};
     if (in) {
         f.in_r0 = in->r0, f.in_r1 = in->r1, f.in_c0 = in->c0, f.in_c1 = in->c1;
@@ -932,8 +938,7 @@ static int launch_frame_chain(OsFdtd2D *h, int T, const TBParams &q, const Rect 
         f.line_values = q.line_values;
         f.values_stride = q.values_stride;
         f.k_col = q.k0 + (k - 1);
-        f.sample_slot = ((q.sample_mask >> (k - 1)) & 1u) ? __builtin_popcount(q.sample_mask & ((1u << (k - 1)) - 1u))
-                                                         : -1;
+        set_frame_slots(f, q, k);
         if (f.first[f.n_rects] == 0) continue;
         OS_TRY(prof_begin(h, 1, s));
         ez2d_frame_step_kernel<<<(unsigned)frame_blocks(f), 256, 0, s>>>(f);
@@ -1069,6 +1074,48 @@ static int record_probes(OsFdtd2D *h) {
     return OS_OK;
 }
 
+// The probes' values after steps n0 + 1 .. n0 + T of a blocked launch, from the cells the launch's kernels staged
+// (slot s - 1 of step s: E_z, then the tangential H: H_y of a cell staged as an x-normal line, H_x as a y-normal
+// one).  Thread k * TB_MAX_T + s: probe k, step s + 1.
+__global__ void ez2d_probe_staged_kernel(ProbeSet ps, const float *stage, float *rows, int64_t capacity, int64_t n0,
+                                         int T) {
+    const int k = threadIdx.x / TB_MAX_T, s = threadIdx.x % TB_MAX_T;
+    if (k >= ps.n || s >= T) return;
+    const int64_t row = n0 + s;
+    if (row < ps.start[k]) return;
+    rows[(size_t)k * capacity + row] = stage[((size_t)k * TB_MAX_T + s) * 2 + (ps.comp[k] == 0 ? 0 : 1)];
+}
+
+static int record_probes_staged(OsFdtd2D *h, int T, int64_t n0) {
+    OS_TRY(prof_begin(h, 2, h->stream));
+    ez2d_probe_staged_kernel<<<1, OS_MAX_PROBES * TB_MAX_T, 0, h->stream>>>(h->probes, h->probe_stage.ptr,
+                                                                             h->probe_rows.ptr, h->probe_capacity,
+                                                                             n0, T);
+    OS_TRY(prof_end(h, h->stream));
+    h->launches += 1;
+    OS_CUDA(cudaGetLastError());
+    return OS_OK;
+}
+
+// The field probes as monitors of the blocked E_z kernels, after the flux lines: each probe's cell is a staged line of
+// one cell (E_z and H_y probes x-normal, whose stage holds E_z then H_y; H_x probes y-normal, E_z then H_x).  A launch
+// with probes marks every step as a staging step, so the kernels stage step s in slot s - 1 and the flux lines' DFT
+// reads its sample steps' slots from there.
+static bool probes_fit_mons(const OsFdtd2D *h) {
+    return h->probe_stage.ptr && h->fluxes.size() + (size_t)h->probes.n <= (size_t)TB_MAX_MONS;
+}
+static void add_probe_mons(const OsFdtd2D *h, TBParams &q) {
+    for (int k = 0; k < h->probes.n; ++k) {
+        TBMon &M = q.mons[q.n_mons++];
+        const bool hx = h->probes.comp[k] == 1;
+        M.normal_axis = hx ? 1 : 0;
+        M.position = hx ? h->probes.iy[k] : h->probes.ix[k];
+        M.lo = hx ? h->probes.ix[k] : h->probes.iy[k];
+        M.hi = M.lo + 1;
+        M.stage = h->probe_stage.ptr + (size_t)k * TB_MAX_T * 2;
+    }
+}
+
 // Room for the probes' rows of the next n_steps steps: the rows grow by doubling, the recorded ones copied over on
 // the handle's stream and the old block given to the pool behind that copy.
 static int reserve_probe_rows(OsFdtd2D *h, int64_t n_steps) {
@@ -1094,6 +1141,7 @@ static int reserve_probe_rows(OsFdtd2D *h, int64_t n_steps) {
 static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples,
                            const float *values, const float *phase_table) {
     const int64_t m = h->sample_interval;
+    const bool staged_probes = h->probes.n > 0 && probes_fit_mons(h);
     // The plan of a launch depends only on its length T (the full steps_per_launch, or a shorter last one): tiles,
     // coefficients, sources, monitors, and the frame steps' regions for both buffer parities.  Each launch then only
     // sets its buffers, first step and sample mask.
@@ -1112,6 +1160,7 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
         plan_tiles(h, T, pl.interior, pl.general, pl.has_interior);
         fill_common(h, pl.interior);
         fill_common(h, pl.general);
+        if (staged_probes) add_probe_mons(h, pl.interior), add_probe_mons(h, pl.general);
         if (h->variant == 1 && pl.general.n_tiles) {
             const bool run_interior = pl.has_interior && pl.interior.n_tiles;
             const Rect box = run_interior ? Rect{pl.interior.rects[0].r0, pl.interior.rects[0].r1,
@@ -1127,9 +1176,10 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
     int64_t k = 0;
     while (k < n_steps) {
         int T = (int)std::min<int64_t>(h->steps_per_launch, n_steps - k);
-        // field maps read E_z between launches: a launch ends on every sample step; probes record every step
+        // field maps read E_z between launches: a launch ends on every sample step; field probes are staged by the
+        // launch's kernels at every step (one step per launch when they do not fit among the monitors)
         if (!h->maps.empty()) T = (int)std::min<int64_t>(T, m - h->n_step % m);
-        if (h->probes.n) T = 1;
+        if (h->probes.n && !staged_probes) T = 1;
         LaunchPlan &pl = plan_for(T);
         TBParams interior = pl.interior, general = pl.general;
         const int in = h->cur, out = h->cur ^ 1;
@@ -1144,6 +1194,7 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
             for (int st = 1; st <= T; ++st)
                 if ((h->n_step + st) % m == 0) q->sample_mask |= 1u << (st - 1);
             if (h->fluxes.empty()) q->sample_mask = 0;
+            if (staged_probes) q->sample_mask = (1u << T) - 1u;   // every step staged (slot s - 1)
         }
         OS_TRY(launch_tb_any(h, T, interior, general, pl.has_interior,
                              pl.frame[in].empty() ? nullptr : pl.frame[in].data()));
@@ -1157,19 +1208,23 @@ static int advance_blocked(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, i
                 const int n = f->hi - f->lo;
                 const int total = n * f->nf;
                 OS_TRY(prof_begin(h, 2, h->stream));
+                // sample q_lo is step q_lo * m of the run: its slot, then every m-th, when every step was staged
+                const int slot0 = staged_probes ? (int)(q_lo * m - h->n_step - 1) : 0;
+                const int stride = staged_probes ? (int)m : 1;
                 ez2d_flux_staged_kernel<<<(total + 255) / 256, 256, 0, h->stream>>>(
-                    f->stage.ptr, n, f->nf, (int)(q_hi - q_lo + 1), ph, f->e_acc.ptr, f->h_acc.ptr);
+                    f->stage.ptr, n, f->nf, (int)(q_hi - q_lo + 1), slot0, stride, ph, f->e_acc.ptr, f->h_acc.ptr);
                 OS_TRY(prof_end(h, h->stream));
                 h->launches += 1;
                 offset += (size_t)n_samples * f->nf * 2;
             }
             OS_CUDA(cudaGetLastError());
         }
+        if (staged_probes) OS_TRY(record_probes_staged(h, T, h->n_step));
         h->n_step += T;
         k += T;
         if (!h->maps.empty() && h->n_step % m == 0)
             OS_TRY(fold_maps(h, h->ez[h->cur].ptr, h->n_step / m, first_sample, n_samples, phase_table));
-        if (h->probes.n) OS_TRY(record_probes(h));
+        if (h->probes.n && !staged_probes) OS_TRY(record_probes(h));
     }
     return OS_OK;
 }
@@ -2162,6 +2217,10 @@ extern "C" int os_fdtd2d_add_probe(OsFdtd2D *h, int32_t ix, int32_t iy, int32_t 
              "field probe cell (%d, %d) outside the %d x %d grid", ix, iy, h->grid.nx, h->grid.ny);
     OS_CHECK(component >= 0 && component <= 2, OS_ERR_INVALID, "unknown field component %d", component);
     OS_CHECK(h->probes.n < OS_MAX_PROBES, OS_ERR_INVALID, "at most %d field probes per engine", OS_MAX_PROBES);
+    if (!h->probe_stage.ptr) {
+        OS_TRY(bind_device(h));
+        OS_TRY(h->probe_stage.alloc((size_t)OS_MAX_PROBES * TB_MAX_T * 2));
+    }
     const int k = h->probes.n++;
     h->probes.ix[k] = ix, h->probes.iy[k] = iy, h->probes.comp[k] = component;
     h->probes.start[k] = h->n_step;

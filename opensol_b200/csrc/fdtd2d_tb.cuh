@@ -706,17 +706,20 @@ __global__ void __launch_bounds__(TB_WARPS * 32) ez2d_tb_batch_kernel(const TBPa
     ez2d_tb_tile<T, C, GEN, CA>(jobs[job], g - tile_start[job], tb_smem);
 }
 
-// Running DFTs of one flux line from the staged samples of one launch, in sample order (monitors.py:45-46,84-90).
+// Running DFTs of one flux line from the staged samples of one launch, in sample order (monitors.py:45-46,84-90):
+// sample q of the launch in staging slot slot0 + q * slot_stride (0 and 1 when only the sample steps were staged;
+// the first sample step's slot and the sample interval when every step was).
 __device__ __forceinline__ void ez2d_flux_staged(int t, const float *__restrict__ stage, int n, int nf, int n_q,
-                                                 const float *__restrict__ phases, double *__restrict__ e_acc,
-                                                 double *__restrict__ h_acc) {
+                                                 int slot0, int slot_stride, const float *__restrict__ phases,
+                                                 double *__restrict__ e_acc, double *__restrict__ h_acc) {
     if (t >= n * nf) return;
     const int f = t / n, c = t - f * n;
     const size_t a = ((size_t)f * n + c) * 2;
     double er = e_acc[a], ei = e_acc[a + 1], hr = h_acc[a], hi = h_acc[a + 1];
     for (int q = 0; q < n_q; ++q) {
         const double pr = (double)phases[((size_t)q * nf + f) * 2], pi = (double)phases[((size_t)q * nf + f) * 2 + 1];
-        const double e = (double)stage[((size_t)q * 2) * n + c], hv = (double)stage[((size_t)q * 2 + 1) * n + c];
+        const size_t slot = (size_t)(slot0 + q * slot_stride);
+        const double e = (double)stage[(slot * 2) * n + c], hv = (double)stage[(slot * 2 + 1) * n + c];
         er += pr * e;
         ei += pi * e;
         hr += pr * hv;
@@ -728,10 +731,11 @@ __device__ __forceinline__ void ez2d_flux_staged(int t, const float *__restrict_
     h_acc[a + 1] = hi;
 }
 
-__global__ void ez2d_flux_staged_kernel(const float *__restrict__ stage, int n, int nf, int n_q,
-                                        const float *__restrict__ phases, double *__restrict__ e_acc,
+__global__ void ez2d_flux_staged_kernel(const float *__restrict__ stage, int n, int nf, int n_q, int slot0,
+                                        int slot_stride, const float *__restrict__ phases, double *__restrict__ e_acc,
                                         double *__restrict__ h_acc) {
-    ez2d_flux_staged(blockIdx.x * blockDim.x + threadIdx.x, stage, n, nf, n_q, phases, e_acc, h_acc);
+    ez2d_flux_staged(blockIdx.x * blockDim.x + threadIdx.x, stage, n, nf, n_q, slot0, slot_stride, phases, e_acc,
+                     h_acc);
 }
 
 // One flux line of one simulation in a batched launch.
@@ -744,6 +748,6 @@ struct FluxBatchItem {
 
 __global__ void ez2d_flux_staged_batch_kernel(const FluxBatchItem *__restrict__ items) {
     const FluxBatchItem it = items[blockIdx.y];
-    ez2d_flux_staged(blockIdx.x * blockDim.x + threadIdx.x, it.stage, it.n, it.nf, it.n_q, it.phases, it.e_acc,
+    ez2d_flux_staged(blockIdx.x * blockDim.x + threadIdx.x, it.stage, it.n, it.nf, it.n_q, 0, 1, it.phases, it.e_acc,
                      it.h_acc);
 }

@@ -88,6 +88,71 @@ def test_hz_probes_record_every_step():
     eng.close()
 
 
+def _ez_probe_run(config, n_probes, flux, chunks, late=None):
+    """An E_z run on a 136 x 496 grid (CPML 8) whose probes sit in the interior box, in the CPML slabs and on the grid
+    corners; `late` (a chunk index) adds one more probe, near the interior box's edge, after that chunk.  (probe data,
+    launches per chunk, interior cells of the plan)."""
+    from opensol_b200.monitors import FieldProbe
+    spec = {'sim': {'size_x': 3.0e-6, 'size_y': 12.0e-6, 'dx': 25e-9, 'npml': 8, 'boundaries': 'pml'},
+            'ops': [['add_dielectric_circle', [1.5e-6, 6.0e-6, 0.6e-6], {'eps_r': 4.0}],
+                    ['add_line_source', ['y', 0.6e-6], {'wavelength': 700e-9, 'bandwidth': 0.6}]]}
+    if flux:
+        spec['ops'].append(['add_flux_monitor', ['y', 2.4e-6, [0.5e-6, 11.0e-6]],
+                            {'wavelengths': [650e-9, 750e-9]}])
+    sim = ob.Simulation(**spec['sim'], verbose=False)
+    apply_ops(sim, spec)
+    eng = sim.em.engine
+    nx, ny = eng.nx, eng.ny
+    cells = [(nx // 2, ny // 2, 'ez'), (nx // 2 + 1, 250, 'hx'), (40, 300, 'hy'), (3, 100, 'ez'),
+             (nx // 2, 2, 'hy'), (0, 0, 'ez'), (nx - 1, ny - 1, 'hx')][:n_probes]
+    probes = []
+    for ix, iy, comp in cells:
+        probes.append(FieldProbe(ix, iy, comp))
+        eng.attach_probe(probes[-1])
+    eng.configure(variant=config[0], steps_per_launch=config[1], tile_rows=config[2])
+    sim.em.finalize()
+    launches = []
+    for k, n in enumerate(chunks):
+        eng.advance(n)
+        launches.append(eng.launch_count())
+        if late is not None and k == late:
+            probes.append(FieldProbe(11, 130, 'hy'))
+            eng.attach_probe(probes[-1])
+    out = [p.get_data() for p in probes]
+    interior = eng.plan_info()[0]
+    eng.close()
+    return out, launches, interior
+
+
+EZ_PROBE_CONFIGS = [(1, 3, 0), (1, 4, 16), (1, 2, 8), (2, 3, 0)]
+
+
+@pytest.mark.parametrize('config', EZ_PROBE_CONFIGS, ids=[f'v{c[0]}_T{c[1]}_r{c[2]}' for c in EZ_PROBE_CONFIGS])
+@pytest.mark.parametrize('n_probes,flux', [(7, False), (6, True), (7, True)],
+                         ids=['8probes', '7probes_flux', '8probes_flux_one_step'])
+def test_ez_probes_in_blocked_launches(config, n_probes, flux):
+    """E_z probes are staged by the blocked kernels at every step of a launch (interior, frame and general tiles):
+    the values equal a one-step-per-launch run's of the same kernel variant, which reads each probe's cell from the
+    field after every step.  A
+    probe is added between chunks.  Eight probes and a flux line exceed the monitors a launch stages: from then on
+    that run keeps one step per launch."""
+    chunks = [7, 13, 1, 40, 9]
+    ref, ref_launches, _ = _ez_probe_run((config[0], 1, config[2]), n_probes, flux, chunks, late=1)
+    got, launches, interior = _ez_probe_run(config, n_probes, flux, chunks, late=1)
+    if config[0] == 1:
+        assert interior > 0, 'the plan has no interior box: the interior kernel is not exercised'
+    for (t0, v0), (t1, v1) in zip(ref, got):
+        assert v0.shape == v1.shape and v0.shape[0] > 0
+        np.testing.assert_array_equal(t1, t0)
+        np.testing.assert_array_equal(v1, v0)
+    assert got[-1][1].shape == (sum(chunks) - sum(chunks[:2]),)   # the late probe records from its step on
+    assert launches[0] < ref_launches[0]   # before the late probe: blocked launches
+    if n_probes + 1 + flux <= 8:
+        assert launches[3] < ref_launches[3]
+    else:
+        assert launches[3] == ref_launches[3]
+
+
 @pytest.mark.parametrize('seed', [0, 1, 2])
 def test_random_maps_and_chunks_match_oracle(seed):
     """Seeded boxes and downsample factors; the run advances in chunks of random length, so chunk ends fall both on
