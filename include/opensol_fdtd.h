@@ -204,7 +204,8 @@ int os_fdtd2d_hz_add_pole(OsFdtd2D *h, int32_t kind, int32_t component, int32_t 
  * every step from the current one on: FieldProbe.record at t_full (core/monitors.py:194-243, fdtd_2d_base.py:481-487).
  * At most 8.  On an E_z handle the blocked launches stage the probes' cells at every step (same values as one step
  * per launch) while flux lines and probes together number at most 8, else an advance with probes runs one step per
- * launch, as it always does on an H_z handle.  Not in batched advances; os_fdtd2d_advance_noalloc
+ * launch; on an H_z handle two-step launches record the first step by stepping the probe cells again from the
+ * launch's input.  Not in batched advances; os_fdtd2d_advance_noalloc
  * refuses a chunk for which the probes' rows would have to grow. */
 int os_fdtd2d_add_probe(OsFdtd2D *h, int32_t ix, int32_t iy, int32_t component, int32_t *probe_id);
 

@@ -1606,6 +1606,38 @@ static HzPlan2 hz_plan2(const OsFdtd2D *h) {
 // Two fused H_z steps from set `in` to set `out` (p.k_step: the first step's column of the source tables): the
 // border's two single steps through the scratch set on the side stream, the interior's two-step kernel on the main
 // stream; they write disjoint cells of the output set.
+// Field probes after the first step of a two-step H_z launch, a state no buffer holds inside the box: a cell outside
+// the box shrunk by one (the region the border's first step covers) is read from the scratch set that step wrote; a
+// cell inside it (plain: no CPML row, edge or wrap in reach) is stepped here from the launch's input set with the
+// border's per-cell functions (no psi written: none of them is in a CPML layer), its faces' cb from the stored
+// arrays (the two-step launch needs no ca).  `p` holds the first step's inputs and value column; `row` is the step's
+// row in the probe rows.  Thread k: probe k.
+__global__ void hz2d_probe_mid_kernel(const Hz2DParams p, ProbeSet ps, int i0, int i1, int j0, int j1,
+                                      const float *shz, const float *sex, const float *sey, float *rows,
+                                      int64_t capacity, int64_t row) {
+    const int k = threadIdx.x;
+    if (k >= ps.n || row < ps.start[k]) return;
+    const int i = ps.ix[k], j = ps.iy[k], comp = ps.comp[k];
+    const size_t idx = (size_t)i * p.ny + j;
+    float v;
+    if (!(i >= i0 && i < i1 && j >= j0 && j < j1)) {
+        v = (comp == 0 ? shz : comp == 1 ? sex : sey)[idx];
+    } else {
+        float exo, eyo, sx, sy;
+        const float hz = hz2d_hz_at(p, i, j, false, exo, eyo);
+        if (comp == 0) {
+            v = hz;
+        } else if (comp == 1) {
+            const float up = hz2d_hz_at(p, i, j + 1, false, sx, sy);
+            v = hz2d_ex_at(p, i, j, exo, 1.0f, __ldg(p.cb_x + idx), hz, up);
+        } else {
+            const float up = hz2d_hz_at(p, i + 1, j, false, sx, sy);
+            v = hz2d_ey_at(p, i, j, eyo, 1.0f, __ldg(p.cb_y + idx), hz, up);
+        }
+    }
+    rows[(size_t)k * capacity + row] = v;
+}
+
 static int launch_hz_step2(OsFdtd2D *h, const HzPlan2 &q, const Hz2DParams &p) {
     const bool fork = !h->profiling;   // profiling: each kernel timed alone
     cudaStream_t bstream = fork ? h->side_stream : h->stream;
@@ -1652,13 +1684,22 @@ static int launch_hz_step2(OsFdtd2D *h, const HzPlan2 &q, const Hz2DParams &p) {
         OS_CUDA(cudaEventRecord(h->ev_join, h->side_stream));
         OS_CUDA(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
     }
+    if (h->probes.n) {   // the first step's values (the second's are read from the output set after the launch)
+        OS_TRY(prof_begin(h, 2, h->stream));
+        hz2d_probe_mid_kernel<<<1, 32, 0, h->stream>>>(b1, h->probes, q.ia + 1, q.ib - 1, q.jc0 + 1, q.jc1 - 1,
+                                                       h->sez[0].ptr, h->shx[0].ptr, h->shy[0].ptr,
+                                                       h->probe_rows.ptr, h->probe_capacity, h->n_step);
+        OS_TRY(prof_end(h, h->stream));
+        h->launches += 1;
+        OS_CUDA(cudaGetLastError());
+    }
     return OS_OK;
 }
 
 // H_z chunk: variant 0 launches the in-place H and E kernels per step, otherwise one fused step kernel per step
 // (buffers swapped after each), or with steps_per_launch 2 two steps per launch wherever the next step is not a
 // sampled one (the flux lines and field maps are sampled after every sample step, so a sample step ends a launch);
-// field probes, which record every step, keep one step per launch.
+// field probes record the first step of a two-step launch with hz2d_probe_mid_kernel and the second from the output.
 static int advance_hz(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_t n_samples, const float *values,
                       const float *phase_table) {
     const int64_t m = h->sample_interval;
@@ -1670,8 +1711,7 @@ static int advance_hz(OsFdtd2D *h, int64_t n_steps, int64_t first_sample, int64_
     const bool per_half = h->variant == 0 || !h->tfsf.empty() || !h->poles.empty();
     const bool sampled = !h->fluxes.empty() || !h->maps.empty();
     HzPlan2 plan2;
-    const bool two = !per_half && h->steps_per_launch == 2 && h->sez[0].ptr && h->probes.n == 0 &&
-                     (plan2 = hz_plan2(h)).interior;
+    const bool two = !per_half && h->steps_per_launch == 2 && h->sez[0].ptr && (plan2 = hz_plan2(h)).interior;
     for (int64_t k = 0; k < n_steps; ++k) {
         const int in = h->cur, out = per_half ? h->cur : h->cur ^ 1;
         Hz2DParams p = make_hz_params(h, in, out);

@@ -475,7 +475,7 @@ class FDTDEngine2D_Hz(FDTDEngine2D_Ez):
         grid); variant 0: one H_z and one E kernel per step.  steps_per_launch 2 (default) or 1: with 2, where the grid
         has no conductivity, no magnetic cells and rows of a multiple of 4 cells, the interior box advances two steps
         per launch (the border two single steps through a scratch field set, made here) except where the next step is
-        a sampled one; field probes, a TFSF box or poles keep one step per launch."""
+        a sampled one; a TFSF box or poles keep one step per launch."""
         super().configure(variant, steps_per_launch, tile_rows)
 
     def autotune(self, candidates=None, repeats=4):

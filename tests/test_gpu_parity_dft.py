@@ -17,7 +17,7 @@ from opensol_b200 import serving
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), 'golden')
 CONFIGS = [(1, 3, 0), (1, 2, 8), (1, 4, 16), (2, 3, 0), (0, 1, 0)]   # (variant, steps per launch, tile rows)
-CONFIGS_HZ = [(1, 1, 0), (1, 1, 16), (0, 1, 0)]
+CONFIGS_HZ = [(1, 1, 0), (1, 1, 16), (0, 1, 0), (1, 2, 0)]
 FIXTURE_RUNS = ([(spec, c) for spec in CASES_DFT for c in CONFIGS] + [(spec, c) for spec in CASES_DFT_HZ
                                                                       for c in CONFIGS_HZ])
 

@@ -243,3 +243,49 @@ def test_hz_two_steps_per_launch(size, npml, boundaries, rows):
         np.testing.assert_array_equal(e2, omon.e_acc)
     for f1, f2 in zip(runs[0][2], runs[1][2]):
         np.testing.assert_array_equal(f2, f1)
+
+
+def test_hz_probes_two_steps_per_launch():
+    """Field probes with two steps per launch: the first step's value of a cell inside the two-step box comes from
+    hz2d_probe_mid_kernel (stepped again from the launch's input), of a cell in the border's first-step region from
+    the scratch set.  Probes of each component in the box, on the box's outer ring, in the CPML and on the grid
+    corners, one added between chunks: the series equal one step per launch bit for bit, in fewer launches."""
+    from opensol_b200.monitors import FieldProbe
+    ops = [['add_dielectric_rectangle', [0.8e-6, 0.4e-6, 1.6e-6, 1.9e-6], {'eps_r': 4.0}],
+           ['add_line_source', ['y', 0.45e-6], {'wavelength': 700e-9, 'bandwidth': 0.6}],
+           ['add_line_source', ['x', 1.1e-6], {'wavelength': 900e-9, 'bandwidth': 0.5, 'amplitude': 2.0}],
+           ['add_flux_monitor', ['y', 2.3e-6, [0.2e-6, 2.4e-6]], {'wavelengths': [650e-9, 800e-9]}]]
+    args = {'size_x': 4.0e-6, 'size_y': 3.2e-6, 'dx': 20e-9, 'npml': 10, 'boundaries': 'pml'}
+    runs = []
+    for T in (1, 2):
+        sim = ob.Simulation(**args, polarization='hz', verbose=False)
+        apply_ops(sim, {'ops': ops})
+        eng = sim.em.engine
+        nx, ny = sim.grid.nx, sim.grid.ny
+        cells = [(nx // 2, ny // 2, 'hz'), (nx // 2 + 1, ny // 2 + 1, 'ex'), (100, 60, 'ey'), (12, 50, 'hz'),
+                 (110, 16, 'ex'), (110, 163, 'ey'), (3, 40, 'ey')]
+        probes = []
+        for ix, iy, comp in cells:
+            probes.append(FieldProbe(ix, iy, comp))
+            eng.attach_probe(probes[-1])
+        eng.configure(variant=1, steps_per_launch=T, tile_rows=0)
+        launches = 0
+        for k, n in enumerate((37, 1, 2, 160)):
+            sim.run(n_steps=n, verbose=False)
+            launches += eng.launch_count()
+            if k == 0:
+                probes.append(FieldProbe(0, 0, 'hz'))
+                eng.attach_probe(probes[-1])
+        assert eng.lossless_form() and ny % 4 == 0
+        if T == 2:
+            assert eng.hz_plan()[0] > 0
+        runs.append(([p.get_data() for p in probes], launches, _fields(sim)))
+        eng.close()
+    assert runs[1][1] < runs[0][1]   # the two-step launches ran
+    for (t0, v0), (t1, v1) in zip(runs[0][0], runs[1][0]):
+        assert v0.shape == v1.shape and v0.shape[0] > 0
+        np.testing.assert_array_equal(t1, t0)
+        np.testing.assert_array_equal(v1, v0)
+    assert runs[1][0][-1][1].shape == (163,)
+    for name in runs[0][2]:
+        np.testing.assert_array_equal(runs[1][2][name], runs[0][2][name], err_msg=name)
