@@ -305,10 +305,15 @@ def run_b200(args):
         total_ms, n_launch = times[name]
         units = cells * (1 if engine.variant == 0 else T)
         launch_ms = reduce_max(total_ms / n_launch)
-    achieved = BYTES_PER_CELL_UPDATE * units / (launch_ms / 1e3) / 1e9
+    # algorithmic bytes of a launch of T steps: the three fields and cb read once and the fields written once per cell
+    # (28 B), i.e. 28 / T per cell-update; the one-step figure (28 B per cell-update) is kept beside it
+    steps_in_launch = 1 if engine.variant == 0 else T
+    bpc = BYTES_PER_CELL_UPDATE / steps_in_launch
+    achieved = bpc * units / (launch_ms / 1e3) / 1e9
     roofline = {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
                 'traffic': None, 'peak_source': f'{peak_kind} hbm_gbs (copy bandwidth)', 'kernel': name,
-                'bytes_per_cell_update': BYTES_PER_CELL_UPDATE, 'cell_updates_per_launch': units,
+                'bytes_per_cell_update': bpc, 'cell_updates_per_launch': units,
+                'one_step_equivalent_gbs': BYTES_PER_CELL_UPDATE * units / (launch_ms / 1e3) / 1e9,
                 'launch_ms': launch_ms, 'launch_timing': 'CUDA events per launch, each kernel alone',
                 'steps_per_launch': T,
                 'kernel_share': {k: v[0] / sum(t[0] for t in times.values()) for k, v in times.items()}}
